@@ -1,0 +1,9 @@
+"""cuwaves: B200 engine for the CP-PAW wavefunction hot path (host-side binding).
+
+The compute path is the CUDA library lib/libcuwaves.so behind the C ABI of
+include/cuwaves.h; this package only binds it (capi) and builds seeded model
+inputs (systems).
+"""
+from . import systems  # noqa: F401
+from .capi import (CUW_HPSI, CUW_OPSI, CUW_PREC_FP64, CUW_PREC_MIXED, CUW_PSI0,  # noqa: F401
+                   CUW_PSIM, Waves, WavesError, bind, engine, load_library, open_waves)

@@ -1,0 +1,351 @@
+"""ctypes binding of the C ABI in include/cuwaves.h.
+
+`Waves` mirrors the reference's WAVES object for one (k-point, spin) set:
+its methods carry the names of the reference routines they replace
+(hpsi, projections, propagate, orthogonalize, switch, ekin, force, ...), take
+the same arguments and raise `WavesError` where the reference calls
+ERROR$STOP (src/paw_error.f90:221).  The same class drives any library that
+exports the ABI under another symbol prefix.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+CUW_MAXSP = 16
+CUW_MAXLN = 8
+CUW_PSI0, CUW_PSIM, CUW_HPSI, CUW_OPSI = 0, 1, 2, 3
+CUW_PREC_FP64, CUW_PREC_MIXED = 0, 1
+
+ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
+          5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
+
+
+class WavesError(RuntimeError):
+    def __init__(self, code: int, routine: str, message: str):
+        self.code = code
+        self.routine = routine
+        super().__init__(f"{routine}: {ERRORS.get(code, code)}: {message}")
+
+
+class Dims(C.Structure):
+    _fields_ = [
+        ("ngl", C.c_int), ("ndim", C.c_int), ("nb", C.c_int), ("nbh", C.c_int), ("tinv", C.c_int),
+        ("nr1", C.c_int), ("nr2", C.c_int), ("nr3", C.c_int), ("nat", C.c_int), ("nsp", C.c_int),
+        ("lmx", C.c_int), ("precision", C.c_int),
+        ("lnx", C.c_int * CUW_MAXSP), ("lox", (C.c_int * CUW_MAXLN) * CUW_MAXSP),
+        ("isp", C.POINTER(C.c_int)),
+    ]
+
+
+# (name, argtypes) of every entry point; handle pointers are c_void_p
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+SIGNATURES = {
+    "create": [C.POINTER(Dims), C.POINTER(C.c_void_p)],
+    "destroy": [_P],
+    "last_error": [_P, C.c_char_p, C.c_int],
+    "set_gset": [_P, _I, _I, _D, _D, _D, _D, _D, _D, _D, C.c_double],
+    "set_potential": [_P, _D],
+    "set_dh": [_P, C.c_int, _D],
+    "set_do": [_P, C.c_int, _D],
+    "set_atoms": [_P, _D, _D],
+    "reset_atoms": [_P, _D],
+    "set_occ": [_P, _D],
+    "set_dynamics": [_P, C.c_double, C.c_double],
+    "upload_psi": [_P, C.c_int, _D],
+    "download_psi": [_P, C.c_int, _D],
+    "get_proj": [_P, _D],
+    "set_proj": [_P, _D],
+    "get_rlam0": [_P, _D],
+    "set_rlam0": [_P, _D],
+    "gramschmidt": [_P, C.c_int, _D],
+    "projections": [_P],
+    "hpsi": [_P],
+    "ekin": [_P, _D],
+    "expectation": [_P, _D],
+    "wavekinetic": [_P, _D, _D],
+    "force": [_P, _D],
+    "propagate": [_P],
+    "orthogonalize": [_P, C.c_int, C.c_double, _I],
+    "switch": [_P],
+    "stop": [_P],
+    "cp_step": [_P, C.c_int, _D, C.c_int, C.c_double, _D, _D],
+}
+OPTIONAL = {
+    "set_async": [_P, C.c_int],
+    "synchronize": [_P],
+    "get_atoms": [_P, _D, _D, _D],
+    "set_threads": [_P, C.c_int],
+}
+
+
+def _dptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_D)
+
+
+def _iptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_I)
+
+
+def bind(lib: C.CDLL, prefix: str) -> dict:
+    fns = {}
+    for name, args in list(SIGNATURES.items()) + list(OPTIONAL.items()):
+        sym = prefix + name
+        if not hasattr(lib, sym):
+            if name in OPTIONAL:
+                continue
+            raise OSError(f"{sym} not exported")
+        f = getattr(lib, sym)
+        f.argtypes = args
+        f.restype = C.c_int
+        fns[name] = f
+    return fns
+
+
+class Waves:
+    """One wave-function set on an engine that implements the C ABI."""
+
+    def __init__(self, fns: dict, inputs: dict, precision: int = CUW_PREC_FP64):
+        self._f = fns
+        self.inp = inputs
+        d = Dims()
+        d.ngl = inputs["ngl"]
+        d.ndim = 1
+        d.nb = inputs["nb"]
+        d.nbh = inputs["nbh"]
+        d.tinv = 1
+        d.nr1, d.nr2, d.nr3 = inputs["grid"]
+        d.nat = inputs["nat"]
+        d.nsp = inputs["nsp"]
+        d.lmx = inputs["lmx"]
+        d.precision = precision
+        for s in range(inputs["nsp"]):
+            d.lnx[s] = inputs["lnx"][s]
+            for ln, l in enumerate(inputs["lox"][s]):
+                d.lox[s][ln] = l
+        self._isp = np.ascontiguousarray(inputs["isp"], dtype=np.int32)
+        d.isp = _iptr(self._isp)
+        self.dims = d
+        h = C.c_void_p()
+        rc = fns["create"](C.byref(d), C.byref(h))
+        if rc:
+            raise WavesError(rc, "create", "invalid dimensions")
+        self.h = h
+        self.ngl, self.nb, self.nbh, self.nat = d.ngl, d.nb, d.nbh, d.nat
+        self.npro = sum(sum(2 * l + 1 for l in inputs["lox"][s - 1]) for s in self._isp.tolist())
+
+    # -- error handling ------------------------------------------------------
+    def _chk(self, rc: int, routine: str):
+        if rc:
+            buf = C.create_string_buffer(512)
+            self._f["last_error"](self.h, buf, 512)
+            raise WavesError(rc, routine, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._f["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- set-up ----------------------------------------------------------------
+    def setup(self, psi0: Optional[np.ndarray] = None, psim: Optional[np.ndarray] = None):
+        """Loads G-set, potential, one-centre matrices, atoms, occupations and
+        dynamics parameters from the inputs dictionary."""
+        i = self.inp
+        self._keep = dict(
+            igvec=np.ascontiguousarray(i["igvec"], dtype=np.int32),
+            minusg=np.ascontiguousarray(i["minusg"], dtype=np.int32),
+            gbas=np.asfortranarray(i["gbas"], dtype=np.float64),
+            gvec=np.ascontiguousarray(i["gvec"], dtype=np.float64),
+            g2=np.ascontiguousarray(i["g2"], dtype=np.float64),
+            pro=np.ascontiguousarray(i["pro"], dtype=np.float64),
+            ylm=np.ascontiguousarray(i["ylm"], dtype=np.float64),
+            mpsi=np.ascontiguousarray(i["mpsi"], dtype=np.float64),
+        )
+        k = self._keep
+        self._chk(self._f["set_gset"](self.h, _iptr(k["igvec"]), _iptr(k["minusg"]), _dptr(k["gbas"]),
+                                      _dptr(k["gvec"]), _dptr(k["g2"]), _dptr(k["pro"]), _dptr(k["ylm"]),
+                                      _dptr(k["mpsi"]), None, float(i["omega"])), "set_gset")
+        self.set_potential(i["v"])
+        self.set_dh(i["dh"])
+        self.set_do(i["dover"])
+        self.reset_atoms(i["r0"])
+        self.set_occ(i["occ"])
+        self.set_dynamics(i["delt"], i["annee"])
+        p0 = i["psi"] if psi0 is None else psi0
+        self.upload_psi(CUW_PSI0, p0)
+        self.upload_psi(CUW_PSIM, p0 if psim is None else psim)
+        return self
+
+    def set_potential(self, v):
+        a = np.ascontiguousarray(v, dtype=np.float64)
+        self._chk(self._f["set_potential"](self.h, _dptr(a)), "set_potential")
+
+    def set_dh(self, dh):
+        a = np.ascontiguousarray(dh, dtype=np.complex128)
+        self._chk(self._f["set_dh"](self.h, int(a.shape[-1]), a.ctypes.data_as(_D)), "set_dh")
+
+    def set_do(self, dover):
+        a = np.ascontiguousarray(dover, dtype=np.float64)
+        self._chk(self._f["set_do"](self.h, int(a.shape[-1]), _dptr(a)), "set_do")
+
+    def set_atoms(self, r0=None, rp=None):
+        a = None if r0 is None else np.ascontiguousarray(r0, dtype=np.float64)
+        b = None if rp is None else np.ascontiguousarray(rp, dtype=np.float64)
+        self._chk(self._f["set_atoms"](self.h, _dptr(a), _dptr(b)), "set_atoms")
+
+    def reset_atoms(self, r0):
+        a = np.ascontiguousarray(r0, dtype=np.float64)
+        self._chk(self._f["reset_atoms"](self.h, _dptr(a)), "reset_atoms")
+
+    def set_occ(self, occ):
+        a = np.ascontiguousarray(occ, dtype=np.float64)
+        self._chk(self._f["set_occ"](self.h, _dptr(a)), "set_occ")
+
+    def set_dynamics(self, delt, annee=0.0):
+        self._chk(self._f["set_dynamics"](self.h, float(delt), float(annee)), "set_dynamics")
+
+    # -- data movement -------------------------------------------------------
+    def upload_psi(self, which: int, psi):
+        a = np.ascontiguousarray(psi, dtype=np.complex128)
+        assert a.size == self.ngl * self.nbh
+        self._chk(self._f["upload_psi"](self.h, which, a.ctypes.data_as(_D)), "upload_psi")
+
+    def download_psi(self, which: int) -> np.ndarray:
+        a = np.empty((self.nbh, self.ngl), dtype=np.complex128)
+        self._chk(self._f["download_psi"](self.h, which, a.ctypes.data_as(_D)), "download_psi")
+        return a
+
+    def get_proj(self) -> np.ndarray:
+        """PROJ(1,NBH,NPRO) returned with shape (NPRO, NBH)."""
+        a = np.empty((self.npro, self.nbh), dtype=np.complex128)
+        self._chk(self._f["get_proj"](self.h, a.ctypes.data_as(_D)), "get_proj")
+        return a
+
+    def set_proj(self, proj):
+        a = np.ascontiguousarray(proj, dtype=np.complex128)
+        self._chk(self._f["set_proj"](self.h, a.ctypes.data_as(_D)), "set_proj")
+
+    def get_rlam0(self) -> np.ndarray:
+        """RLAM0(NB,NB) returned with shape (NB, NB) indexed [j, i]."""
+        a = np.empty((self.nb, self.nb), dtype=np.complex128)
+        self._chk(self._f["get_rlam0"](self.h, a.ctypes.data_as(_D)), "get_rlam0")
+        return a
+
+    def set_rlam0(self, r):
+        a = np.ascontiguousarray(r, dtype=np.complex128)
+        self._chk(self._f["set_rlam0"](self.h, a.ctypes.data_as(_D)), "set_rlam0")
+
+    # -- the WAVES operations --------------------------------------------------
+    def gramschmidt(self, which: int, r):
+        a = np.ascontiguousarray(r, dtype=np.float64)
+        self._chk(self._f["gramschmidt"](self.h, which, _dptr(a)), "WAVES_GRAMSCHMIDT")
+
+    def projections(self):
+        self._chk(self._f["projections"](self.h), "WAVES$PROJECTIONS")
+
+    def hpsi(self):
+        self._chk(self._f["hpsi"](self.h), "WAVES$HPSI")
+
+    def ekin(self) -> float:
+        x = C.c_double()
+        self._chk(self._f["ekin"](self.h, C.byref(x)), "WAVES$EKIN")
+        return x.value
+
+    def expectation(self) -> np.ndarray:
+        a = np.empty(self.nb)
+        self._chk(self._f["expectation"](self.h, _dptr(a)), "WAVES$ETOT")
+        return a
+
+    def wavekinetic(self):
+        x = C.c_double()
+        a = np.empty(self.nb)
+        self._chk(self._f["wavekinetic"](self.h, C.byref(x), _dptr(a)), "WAVES_WAVEKINETIC")
+        return x.value, a
+
+    def force(self) -> np.ndarray:
+        a = np.empty((self.nat, 3))
+        self._chk(self._f["force"](self.h, _dptr(a)), "WAVES$FORCE")
+        return a
+
+    def propagate(self):
+        self._chk(self._f["propagate"](self.h), "WAVES$PROPAGATE")
+
+    def orthogonalize(self, max_iter: int = 200, eps: float = 1e-8) -> int:
+        it = C.c_int()
+        self._chk(self._f["orthogonalize"](self.h, max_iter, eps, C.byref(it)), "WAVES$ORTHOGONALIZE")
+        return it.value
+
+    def switch(self):
+        self._chk(self._f["switch"](self.h), "WAVES$SWITCH")
+
+    def stop(self):
+        self._chk(self._f["stop"](self.h), "WAVES$STOP")
+
+    def cp_step(self, move_atoms: bool = False, max_iter: int = 200, eps: float = 1e-8, want_force=True):
+        out = np.zeros(8)
+        f = np.zeros((self.nat, 3)) if want_force else None
+        m = np.ascontiguousarray(self.inp["masses"], dtype=np.float64)
+        self._chk(self._f["cp_step"](self.h, int(move_atoms), _dptr(m), max_iter, eps, _dptr(out), _dptr(f)),
+                  "TIMESTEP")
+        return out, f
+
+    def set_async(self, flag: bool):
+        if "set_async" in self._f:
+            self._chk(self._f["set_async"](self.h, int(flag)), "set_async")
+
+    def synchronize(self):
+        if "synchronize" in self._f:
+            self._chk(self._f["synchronize"](self.h), "synchronize")
+
+    def initialize(self, gram_schmidt: bool = True):
+        """Start-up of WAVES$ETOT at TFIRST (src/paw_waves1.f90:1733-1748):
+        Gram-Schmidt of PSI0 (at R(0)) and PSIM (at R(-)), then PROJ of PSI0."""
+        if gram_schmidt:
+            r = self.inp["r0"]
+            self.gramschmidt(CUW_PSI0, r)
+            self.gramschmidt(CUW_PSIM, r)
+        self.projections()
+        return self
+
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(os.path.dirname(PKG_DIR), "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libcuwaves.so")
+
+
+def load_library(path: Optional[str] = None) -> C.CDLL:
+    """Loads the B200 engine.  There is no fallback: a missing library or a
+    machine without a CUDA device raises."""
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OSError(f"libcuwaves.so not built: {p} (run __graft_entry__.build())")
+    return C.CDLL(p, mode=C.RTLD_GLOBAL)
+
+
+_engine_fns = None
+
+
+def engine() -> dict:
+    global _engine_fns
+    if _engine_fns is None:
+        _engine_fns = bind(load_library(), "cuwaves_")
+    return _engine_fns
+
+
+def open_waves(inputs: dict, precision: int = CUW_PREC_FP64) -> Waves:
+    return Waves(engine(), inputs, precision)

@@ -1,0 +1,152 @@
+/*
+ * cuwaves.h -- C ABI of the B200 wavefunction engine for the CP-PAW WAVES object.
+ *
+ * One handle holds the device-resident state of ONE wave-function set of the
+ * reference's WAVES_MODULE (one (k-point, spin) pair, src/paw_waves1.f90:176-193
+ * WVSET_TYPE) together with its G-set (GSET_TYPE, :156-175) and projector map
+ * (MAP_TYPE, :142-154).  The Fortran host selects a handle where the reference
+ * calls WAVES_SELECTWV (src/paw_waves1.f90:252-276).
+ *
+ * Conventions (all identical to the reference's Fortran arrays):
+ *  - arrays are column-major; complex numbers are pairs of doubles (COMPLEX(8));
+ *  - PSI(NGL,NDIM,NBH), PROJ(NDIM,NBH,NPRO), RLAM0(NB,NB);
+ *  - IGVEC(3,NGL) in the order of PLANEWAVE_GETIG (src/paw_fft.f90:1211-1327),
+ *    MINUSG(NGL) 1-based (src/paw_fft.f90:1157-1208);
+ *  - the real-space grid is x-fastest, NR1*NR2*NR3 (src/paw_fft.f90:2162-2174);
+ *  - projector index IPRO runs over atoms, then LN, then M (src/paw_waves1.f90:6070-6109).
+ *
+ * Every entry point returns CUW_OK (0) or an error code; the message is
+ * available from cuwaves_last_error.  The reference stops the program instead
+ * (ERROR$STOP, src/paw_error.f90:221); a Fortran shim maps a nonzero status
+ * onto ERROR$STOP.  Calls are synchronous on the handle's own CUDA stream
+ * unless the handle was put into asynchronous mode with cuwaves_set_async.
+ */
+#ifndef CUWAVES_H
+#define CUWAVES_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUW_OK                 0
+#define CUW_ERR_ARG            1  /* invalid argument or size */
+#define CUW_ERR_CUDA           2  /* CUDA runtime error */
+#define CUW_ERR_STATE          3  /* call out of order (e.g. propagate before hpsi) */
+#define CUW_ERR_NOT_CONVERGED  4  /* orthogonalisation loop not converged */
+#define CUW_ERR_DIVERGED       5  /* orthogonalisation loop diverged (max|overlap-1|>1e200) */
+#define CUW_ERR_UNSUPPORTED    6  /* configuration outside the implemented path */
+#define CUW_ERR_NAN            7  /* non-finite value detected */
+#define CUW_ERR_NOMEM          8  /* device allocation failed */
+
+#define CUW_PSI0 0   /* THIS%PSI0 */
+#define CUW_PSIM 1   /* THIS%PSIM */
+#define CUW_HPSI 2   /* THIS%HPSI */
+#define CUW_OPSI 3   /* THIS%OPSI (mass-scaled O|psi0>, valid inside a step) */
+
+#define CUW_PREC_FP64  0  /* every product in FP64 */
+#define CUW_PREC_MIXED 1  /* FP32 FFT/V.psi, split-BF16 tensor-core contractions, FP64 solves */
+
+#define CUW_MAXSP 16
+#define CUW_MAXLN 8
+
+typedef struct cuw_handle cuw_handle;
+
+/* Sizes and projector map of one wave-function set (MAP_TYPE + WVSET sizes). */
+typedef struct cuw_dims {
+  int ngl;        /* #G vectors of the full sphere 0.5|G|^2 <= EPWPSI */
+  int ndim;       /* spinor components; 1 is implemented */
+  int nb;         /* #bands */
+  int nbh;        /* #stored functions: (nb+1)/2 with tinv, else nb */
+  int tinv;       /* 1: Gamma point, super wave functions (src/paw_fft.f90:35-55) */
+  int nr1, nr2, nr3;  /* FFT grid */
+  int nat;        /* #atoms */
+  int nsp;        /* #species */
+  int lmx;        /* #real spherical harmonics in YLM(NGL,LMX) */
+  int precision;  /* CUW_PREC_* */
+  int lnx[CUW_MAXSP];             /* MAP%LNX */
+  int lox[CUW_MAXSP][CUW_MAXLN];  /* MAP%LOX(LN,ISP) stored as lox[isp-1][ln-1] */
+  const int* isp;                 /* [nat] MAP%ISP, 1-based */
+} cuw_dims;
+
+/* Replaces the WVSET allocation of WAVES$INITIALIZE (src/paw_waves1.f90:1187-1450). */
+int cuwaves_create(const cuw_dims* dims, cuw_handle** out);
+int cuwaves_destroy(cuw_handle* h);
+/* Copies the last error message (NUL-terminated, truncated to len). */
+int cuwaves_last_error(const cuw_handle* h, char* buf, int len);
+/* 0: every call waits for its work (default); 1: calls only enqueue. */
+int cuwaves_set_async(cuw_handle* h, int async);
+int cuwaves_synchronize(cuw_handle* h);
+
+/* G-set of PLANEWAVE$INITIALIZE + WAVES_UPDATEGSET (src/paw_fft.f90:872-1110;
+ * src/paw_waves1.f90:6237-6353): igvec(3,NGL), minusg(NGL) (1-based, required
+ * when tinv), gbas(3,3) reciprocal lattice vectors (THIS%GBAS of PLANEWAVE),
+ * gvec(3,NGL) and g2(NGL) as PLANEWAVE$GETR8A('GVEC'/'G2'),
+ * pro(NGL,NBAREPRO) = GSET%PRO, ylm(NGL,LMX) = GSET%YLM, mpsi(NGL) = GSET%MPSI,
+ * bucket(NGL) = GSET%BUCKET or NULL (no bucket potential), gweight = cell volume. */
+int cuwaves_set_gset(cuw_handle* h, const int* igvec, const int* minusg,
+                     const double* gbas, const double* gvec, const double* g2, const double* pro,
+                     const double* ylm, const double* mpsi, const double* bucket,
+                     double gweight);
+/* Local potential V(r) on the FFT grid (the RHO argument of WAVES$HPSI, src/paw_waves1.f90:4793). */
+int cuwaves_set_potential(cuw_handle* h, const double* v);
+/* One-centre Hamiltonian DH(LMNXX,LMNXX,NAT) of this spin, complex (WAVES$HPSI argument). */
+int cuwaves_set_dh(cuw_handle* h, int lmnxx, const double* dh);
+/* One-centre overlap DO(LNXX,LNXX,NSP) as SETUP$GETR8A('DO') per species. */
+int cuwaves_set_do(cuw_handle* h, int lnxx, const double* dover);
+/* Atomic positions R(0) and R(+) (ATOMLIST 'R(0)', 'R(+)'), each (3,NAT). */
+int cuwaves_set_atoms(cuw_handle* h, const double* r0, const double* rp);
+/* Occupations OCC(NB) of this (k,spin) as WAVES_DYNOCCGETR8A('OCC'). */
+int cuwaves_set_occ(cuw_handle* h, const double* occ);
+/* DELT and ANNEE (friction) of WAVES_MODULE (src/paw_waves1.f90:216-218). */
+int cuwaves_set_dynamics(cuw_handle* h, double delt, double annee);
+
+int cuwaves_upload_psi(cuw_handle* h, int which, const double* psi);
+int cuwaves_download_psi(cuw_handle* h, int which, double* psi);
+int cuwaves_get_proj(cuw_handle* h, double* proj);
+int cuwaves_set_proj(cuw_handle* h, const double* proj);
+int cuwaves_get_rlam0(cuw_handle* h, double* rlam0);
+int cuwaves_set_rlam0(cuw_handle* h, const double* rlam0);
+
+/* WAVES_GRAMSCHMIDT (src/paw_waves2.f90:2025-2177) of PSI0 or PSIM with atoms at r(3,NAT). */
+int cuwaves_gramschmidt(cuw_handle* h, int which, const double* r);
+/* WAVES$PROJECTIONS('PSI0') (src/paw_waves1.f90:2681-2726): PROJ = <p(R0)|PSI0>. */
+int cuwaves_projections(cuw_handle* h);
+/* WAVES$HPSI (src/paw_waves1.f90:4793-4916): HPSI = H|PSI0> from V, DH and PROJ. */
+int cuwaves_hpsi(cuw_handle* h);
+/* WAVES$EKIN without stress (src/paw_waves1.f90:2729-2954). */
+int cuwaves_ekin(cuw_handle* h, double* ekin);
+/* Expectation values <psi_n|H|psi_n> of WAVES$ETOT (src/paw_waves1.f90:2094-2123), eig(NB). */
+int cuwaves_expectation(cuw_handle* h, double* eig);
+/* WAVES_WAVEKINETIC (src/paw_waves1.f90:6713-6847); eig(NB) may be NULL. */
+int cuwaves_wavekinetic(cuw_handle* h, double* ekin, double* eig);
+/* WAVES$FORCE without stress (src/paw_waves1.f90:4570-4739), force(3,NAT). */
+int cuwaves_force(cuw_handle* h, double* force);
+/* WAVES$PROPAGATE without cell dynamics (src/paw_waves1.f90:6479-6592). */
+int cuwaves_propagate(cuw_handle* h);
+/* WAVES$ORTHOGONALIZE with SAFEORTHO=T at the Gamma point (src/paw_waves2.f90:11-494,
+ * WAVES_ORTHO_X :1844-2022).  max_iter and eps replace the PARAMETERs MAX=200 and
+ * EPS=1e-8; iters (may be NULL) receives the iteration count. */
+int cuwaves_orthogonalize(cuw_handle* h, int max_iter, double eps, int* iters);
+/* WAVES$SWITCH (src/paw_waves2.f90:2180-2317): PSI0<->PSIM, Lagrange extrapolation. */
+int cuwaves_switch(cuw_handle* h);
+/* WAVES$STOP (src/paw_waves1.f90:6445-6476): PSIM = PSI0, history of RLAM dropped. */
+int cuwaves_stop(cuw_handle* h);
+
+/* One Car-Parrinello time step in the order of TIMESTEP (src/paw_driver.f90:280-561)
+ * for a fixed potential: energies and forces at R(0), H|psi>, Verlet propagation,
+ * orthogonalisation at R(+), switch.  When move_atoms is nonzero the step also
+ * advances the nuclei with the Verlet rule of ATOMS$PROPAGATE without friction,
+ * R(+) = 2R(0) - R(-) + dt^2 F/M, using mass(NAT) in electron masses, and keeps
+ * R(-), R(0), R(+) on the device; otherwise R(+) is the one last set.  out[8]
+ * receives: [0] total energy sum_n f_n <psi_n|H|psi_n>, [1] kinetic energy,
+ * [2] fictitious kinetic energy 0.5*(EKIN1+EKIN2), [3] ionic kinetic energy,
+ * [4] orthogonalisation iterations, [5..7] reserved.  force (3,NAT) may be NULL. */
+int cuwaves_cp_step(cuw_handle* h, int move_atoms, const double* mass,
+                    int max_iter, double eps, double* out, double* force);
+/* Resets the nuclear history so that R(-) = R(0) (start from rest). */
+int cuwaves_reset_atoms(cuw_handle* h, const double* r0);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUWAVES_H */
