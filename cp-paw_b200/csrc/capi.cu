@@ -1,0 +1,828 @@
+// C ABI of the engine (include/cuwaves.h): handle management, data movement
+// and the WAVES operations, each a sequence of device kernels on the handle's
+// stream.  No operation has a host compute path: results are produced by the
+// kernels in fft.cu, gemm.cu and ortho.cu and by the small kernels below.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cuwaves_internal.cuh"
+
+namespace cuw {
+
+int unravel_run(Handle* h, const double2* pw, const double2* oc, int npair, double* o0, double* o1, double* o2);
+int jacobi_run(Handle* h, const double* s_dev, double* u, double* e);
+int lambda_init_run(Handle* h);
+int store_lambda_run(Handle* h);
+int ortho_y_run(Handle* h, const double* s, double* x);
+int fold_x_run(Handle* h, const double* x, double2* x1, double2* x2);
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// band sums over G (partials per block, deterministic final combination)
+// mode 0 (EKIN, src/paw_waves1.f90:2790-2954):
+//   q0 = sum g2 |x|^2, q1 = sum g2 Re(conj x(g) conj x(-g)), q2/q3 same with bucket
+// mode 1 (WAVEKINETIC, :6713-6847), d = x - y:
+//   q0 = sum m |d|^2, q1 = sum m (Re d Re d~ + Im d Im d~), d~ = conj d(-g)
+// mode 2 (expectation values, :2094-2123):
+//   q0 + i q1 = sum conj(x) y, q2 + i q3 = sum x(g) y(-g)
+// ---------------------------------------------------------------------------
+constexpr int RB = 256;
+constexpr int RG = 2048;  // g per block
+
+__global__ void k_band_sums(int mode, const double2* __restrict__ x, const double2* __restrict__ y, int ldg, int ngl,
+                            const double* __restrict__ w1, const double* __restrict__ w2,
+                            const int* __restrict__ minusg, double* __restrict__ part, int nblk) {
+  const int b = blockIdx.y, blk = blockIdx.x;
+  const double2* xb = x + (size_t)ldg * b;
+  const double2* yb = y ? y + (size_t)ldg * b : nullptr;
+  double q[4] = {0.0, 0.0, 0.0, 0.0};
+  const int g0 = blk * RG, g1 = min(ngl, g0 + RG);
+  for (int g = g0 + threadIdx.x; g < g1; g += RB) {
+    int mg = minusg[g];
+    if (mode == 0) {
+      double2 a = xb[g], c = xb[mg];
+      double n2 = a.x * a.x + a.y * a.y;
+      double cr = a.x * c.x - a.y * c.y;  // Re(conj(a) conj(c)) = Re(a c)
+      q[0] += w1[g] * n2;
+      q[1] += w1[g] * cr;
+      if (w2) {
+        q[2] += w2[g] * n2;
+        q[3] += w2[g] * cr;
+      }
+    } else if (mode == 1) {
+      double2 d = csub(xb[g], yb[g]);
+      double2 dm = csub(xb[mg], yb[mg]);
+      q[0] += w1[g] * (d.x * d.x + d.y * d.y);
+      q[1] += w1[g] * (d.x * dm.x - d.y * dm.y);
+    } else {
+      double2 a = xb[g], hv = yb[g], hm = yb[mg];
+      q[0] += a.x * hv.x + a.y * hv.y;
+      q[1] += a.x * hv.y - a.y * hv.x;
+      q[2] += a.x * hm.x - a.y * hm.y;
+      q[3] += a.x * hm.y + a.y * hm.x;
+    }
+  }
+  __shared__ double red[4][RB];
+  for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = q[k];
+  __syncthreads();
+  for (int s = RB / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[((size_t)b * nblk + blk) * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// final: res[b*4+k] = sum over blocks
+__global__ void k_band_final(const double* __restrict__ part, int nbh, int nblk, double* __restrict__ res) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbh * 4) return;
+  int b = i / 4, k = i % 4;
+  double s = 0.0;
+  for (int t = 0; t < nblk; ++t) s += part[((size_t)b * nblk + t) * 4 + k];
+  res[i] = s;
+}
+
+// scalar results from band sums and occupations (one thread)
+//   out[0] EKIN or WAVEKINETIC energy; out[1 + i] per-band values
+__global__ void k_energy_final(int mode, const double* __restrict__ res, const double* __restrict__ occ, int nbh,
+                               double gweight, double dt2, int tbucket, double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double e = 0.0;
+  for (int b = 0; b < nbh; ++b) {
+    double f1 = occ[2 * b], f2 = occ[2 * b + 1];
+    const double* q = res + 4 * b;
+    if (mode == 0) {
+      double fp = 0.5 * (f1 + f2), fm = 0.5 * (f1 - f2);
+      if (fp == 0.0 && fm == 0.0) continue;
+      double t = 0.5 * fp * q[0] + (tbucket ? fp * q[2] : 0.0);
+      if (fabs(fm) >= 1e-12) t += 0.5 * fm * q[1] + (tbucket ? fm * q[3] : 0.0);
+      e += t;
+    } else if (mode == 1) {
+      double ev1 = 0.0, ev2 = 0.0;
+      if (!(f1 == 0.0 && f2 == 0.0)) {
+        double sum = q[0] / dt2;
+        ev1 = 0.5 * sum;
+        ev2 = 0.5 * sum;
+        e += sum * 0.5 * (f1 + f2);
+        if (f1 - f2 != 0.0) {
+          double s2 = q[1] / dt2;
+          ev1 += 0.5 * s2;
+          ev2 -= 0.5 * s2;
+          e += s2 * 0.5 * (f1 - f2);
+        }
+      }
+      out[1 + 2 * b] = ev1;
+      out[2 + 2 * b] = ev2;
+    } else {
+      double tp = q[0] * gweight, tm = q[2] * gweight;
+      out[1 + 2 * b] = 0.5 * tp + 0.5 * tm;
+      out[2 + 2 * b] = 0.5 * tp - 0.5 * tm;
+      e += f1 * out[1 + 2 * b] + f2 * out[2 + 2 * b];
+    }
+  }
+  out[0] = (mode == 2) ? e : e * gweight;
+}
+
+// WAVES$PROPAGATE (src/paw_waves1.f90:6575-6583)
+__global__ void k_propagate(const double2* __restrict__ psi0, double2* __restrict__ psim,
+                            const double2* __restrict__ hpsi, const double* __restrict__ mpsi, int ldg, int ngl,
+                            int nbh, double a1, double a2, double a3) {
+  size_t n = (size_t)ldg * nbh;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int g = (int)(k % ldg);
+    if (g >= ngl) continue;
+    double c = a3 / mpsi[g];
+    double2 p0 = psi0[k], pm = psim[k], hv = hpsi[k];
+    psim[k] = make_double2(a1 * p0.x + a2 * pm.x + c * hv.x, a1 * p0.y + a2 * pm.y + c * hv.y);
+  }
+}
+
+// DEDPROJ = F1 HPROJ + F2 conj(HPROJ) per super wave function (src/paw_waves1.f90:5644-5668)
+__global__ void k_dedproj(double2* __restrict__ hp, const double* __restrict__ occ, int nbh, int npro) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)nbh * npro) return;
+  int b = (int)(i % nbh);
+  double f1 = 0.5 * (occ[2 * b] + occ[2 * b + 1]), f2 = 0.5 * (occ[2 * b] - occ[2 * b + 1]);
+  double2 c = hp[i];
+  hp[i] = make_double2(f1 * c.x + f2 * c.x, f1 * c.y - f2 * c.y);
+}
+
+// lambda(i,j) = -Re RLAM0(i,j) * 0.5 (f_i + f_j)   (src/paw_waves1.f90:5673-5680)
+__global__ void k_force_lambda(const double2* __restrict__ rlam0, const double* __restrict__ occ, int nb,
+                               double* __restrict__ lam) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nb * nb) return;
+  int i = idx % nb, j = idx / nb;
+  lam[idx] = -rlam0[idx].x * 0.5 * (occ[i] + occ[j]);
+}
+
+// R(+) = 2R(0) - R(-) + dt^2 F/M  (ATOMS$PROPAGATE without friction)
+__global__ void k_atoms_verlet(const double* __restrict__ r0, const double* __restrict__ rm, double* __restrict__ rp,
+                               const double* __restrict__ f, const double* __restrict__ mass, int nat, double dt2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * nat) return;
+  rp[i] = 2.0 * r0[i] - rm[i] + dt2 * f[i] / mass[i / 3];
+}
+
+__global__ void k_ion_ekin(const double* __restrict__ rp, const double* __restrict__ rm,
+                           const double* __restrict__ mass, int nat, double dt, double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double e = 0.0;
+  for (int i = 0; i < 3 * nat; ++i) {
+    double v = (rp[i] - rm[i]) / (2.0 * dt);
+    e += 0.5 * mass[i / 3] * v * v;
+  }
+  out[0] = e;
+}
+
+__global__ void k_copy_psi(const double2* __restrict__ src, double2* __restrict__ dst, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    dst[k] = src[k];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// band reductions: results in h->g.scal (device): [0] energy, [1..nb] per band
+// ---------------------------------------------------------------------------
+static int band_sums_run(Handle* h, int mode, const double2* x, const double2* y, const double* w1, const double* w2,
+                         double* res_dev) {
+  const int nblk = ceil_div(h->d.ngl, RG);
+  k_band_sums<<<dim3(nblk, h->d.nbh), RB, 0, h->stream>>>(mode, x, y, h->ldg, h->d.ngl, w1, w2, h->g.minusg,
+                                                          h->g.red, nblk);
+  CUW_LAUNCH_CHECK("k_band_sums");
+  k_band_final<<<ceil_div(4 * h->d.nbh, 128), 128, 0, h->stream>>>(h->g.red, h->d.nbh, nblk, res_dev);
+  CUW_LAUNCH_CHECK("k_band_final");
+  return CUW_OK;
+}
+
+// mode: RED_EKIN / RED_WAVEKIN / RED_EXPECT; result vector at out_dev
+static int energy_run(Handle* h, int mode, double* out_dev) {
+  Device& g = h->g;
+  double* res = g.red + (size_t)4 * h->d.nbh * ceil_div(h->d.ngl, RG);
+  if (mode == RED_EKIN) CUW_RET(band_sums_run(h, 0, g.psi0, nullptr, g.g2, h->tbucket ? g.bucket : nullptr, res));
+  else if (mode == RED_WAVEKIN) CUW_RET(band_sums_run(h, 1, g.psi0, g.psim, g.mpsi, nullptr, res));
+  else CUW_RET(band_sums_run(h, 2, g.psi0, g.hpsi, nullptr, nullptr, res));
+  k_energy_final<<<1, 1, 0, h->stream>>>(mode == RED_EKIN ? 0 : (mode == RED_WAVEKIN ? 1 : 2), res, g.occ, h->d.nbh,
+                                         h->gweight, h->delt * h->delt, h->tbucket ? 1 : 0, out_dev);
+  CUW_LAUNCH_CHECK("k_energy_final");
+  return CUW_OK;
+}
+
+int band_reduce(Handle* h, int what, double* out_host, double* eig_host) {
+  double* out_dev = h->g.scal;
+  CUW_RET(energy_run(h, what, out_dev));
+  std::vector<double> tmp(1 + h->d.nb);
+  CUW_TRY(cudaMemcpyAsync(tmp.data(), out_dev, sizeof(double) * (1 + h->d.nb), cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  if (out_host) *out_host = tmp[0];
+  if (eig_host) std::memcpy(eig_host, tmp.data() + 1, sizeof(double) * h->d.nb);
+  return CUW_OK;
+}
+
+int propagate_run(Handle* h) {
+  const double a1 = 2.0 / (1.0 + h->annee), a2 = 1.0 - a1, a3 = -h->delt * h->delt / (1.0 + h->annee);
+  k_propagate<<<4 * h->nsm, 256, 0, h->stream>>>(h->g.psi0, h->g.psim, h->g.hpsi, h->g.mpsi, h->ldg, h->d.ngl,
+                                                 h->d.nbh, a1, a2, a3);
+  CUW_LAUNCH_CHECK("k_propagate");
+  return CUW_OK;
+}
+
+// DEDPROJ in h->g.hproj, then forces into force_dev (uses eigr of R(0))
+static int force_dev_run(Handle* h, double* force_dev) {
+  Device& g = h->g;
+  const int nbh = h->d.nbh, npro = h->npro, nb = h->d.nb;
+  CUW_RET(hproj_compute(h, g.proj, g.hproj));
+  CUW_RET(oproj_compute(h, g.proj, g.oproj));
+  size_t n = (size_t)nbh * npro;
+  k_dedproj<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(g.hproj, g.occ, nbh, npro);
+  CUW_LAUNCH_CHECK("k_dedproj");
+  k_force_lambda<<<ceil_div(nb * nb, 256), 256, 0, h->stream>>>(g.rlam0, g.occ, nb, g.wk2);
+  CUW_LAUNCH_CHECK("k_force_lambda");
+  CUW_RET(lambda12_run(h, g.wk2, g.lam1c, g.lam2c));
+  CUW_RET(addoproj_run(h, g.hproj, g.oproj, g.lam1c, g.lam2c));
+  CUW_RET(force_gemm(h, g.hproj, force_dev));
+  return CUW_OK;
+}
+
+// the part of WAVES$ORTHOGONALIZE after OPSI is formed (src/paw_waves2.f90:242-490)
+static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
+  Device& g = h->g;
+  // projections of PSIBAR and OPSI at R(+)
+  CUW_RET(eigr_compute(h, g.rp));
+  CUW_RET(proj_compute(h, g.psim, g.proj, g.opsi, g.oproj));
+  // DO*PROJ and DO*OPROJ
+  CUW_RET(oproj_compute(h, g.proj, g.hproj));
+  CUW_RET(oproj_compute(h, g.oproj, g.pbuf));
+  const size_t mn = (size_t)h->d.nbh * h->d.nbh;
+  double2* pw = g.tmat;
+  double2* oc = g.tmat + 6 * mn;
+  GramPair pc[3] = {{g.proj, g.hproj}, {g.oproj, g.hproj}, {g.oproj, g.pbuf}};
+  CUW_RET(gram_projections(h, pc, 3, oc));
+  GramPair pp[3] = {{g.psim, g.psim}, {g.opsi, g.psim}, {g.opsi, g.opsi}};
+  CUW_RET(gram_planewave(h, pp, 3, pw));
+  CUW_RET(unravel_run(h, pw, oc, 3, g.mat, g.omat, g.oomat));
+  CUW_RET(lambda_init_run(h));
+  int it = 0;
+  int st = ortho_solve(h, max_iter, eps, &it);
+  if (iters) *iters = it;
+  if (st != CUW_OK) return st;
+  CUW_RET(lambda12_run(h, g.lam, g.lam1c, g.lam2c));
+  CUW_RET(addopsi_run(h, g.psim, g.opsi, g.lam1c, g.lam2c));
+  CUW_RET(addoproj_run(h, g.proj, g.oproj, g.lam1c, g.lam2c));
+  CUW_RET(store_lambda_run(h));
+  h->have_opsi = false;
+  return CUW_OK;
+}
+
+}  // namespace cuw
+
+using namespace cuw;
+
+// ---------------------------------------------------------------------------
+// extern "C" entry points
+// ---------------------------------------------------------------------------
+#define H(hp) Handle* h = reinterpret_cast<Handle*>(hp)
+#define NEED(cond, code, msg) \
+  do {                        \
+    if (!(cond)) return h->fail(code, msg); \
+  } while (0)
+
+static int dev_alloc(Handle* h, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) return h->fail(CUW_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  e = cudaMemset(*p, 0, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) return h->fail(CUW_ERR_CUDA, cudaGetErrorString(e));
+  return CUW_OK;
+}
+#define ALLOC(ptr, bytes) CUW_RET(dev_alloc(h, reinterpret_cast<void**>(&(ptr)), (bytes)))
+
+static void free_all(Handle* h) {
+  Device& g = h->g;
+  void* ptrs[] = {g.psi0, g.psim, g.hpsi, g.opsi, g.proj, g.oproj, g.hproj, g.pbuf, g.rlam0, g.rlamm, g.igvec,
+                  g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_off,
+                  g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
+                  g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.u, g.eig, g.haux, g.gamn,
+                  g.work, g.wk2, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
+                  g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  h->g = Device();
+}
+
+extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
+  if (!dims || !out) return CUW_ERR_ARG;
+  *out = nullptr;
+  const cuw_dims& d = *dims;
+  if (d.ngl <= 0 || d.nb <= 0 || d.nat < 0 || d.nsp <= 0 || d.nsp > CUW_MAXSP || d.nr1 <= 0 || d.nr2 <= 0 ||
+      d.nr3 <= 0 || d.lmx <= 0 || (d.nat > 0 && !d.isp))
+    return CUW_ERR_ARG;
+  if (d.ndim != 1 || !d.tinv || (d.nb % 2) || d.nbh != d.nb / 2) return CUW_ERR_UNSUPPORTED;
+  if (d.precision != CUW_PREC_FP64 && d.precision != CUW_PREC_MIXED) return CUW_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CUW_ERR_CUDA;
+  }
+  Handle* h = new Handle();
+  h->d = d;
+  h->d.isp = nullptr;
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
+  h->isp.resize(d.nat);
+  for (int a = 0; a < d.nat; ++a) {
+    h->isp[a] = dims->isp[a] - 1;
+    if (h->isp[a] < 0 || h->isp[a] >= d.nsp) {
+      delete h;
+      return CUW_ERR_ARG;
+    }
+  }
+  h->lmnx.resize(d.nsp);
+  h->ibpro.resize(d.nsp);
+  int nbare = 0;
+  for (int s = 0; s < d.nsp; ++s) {
+    if (d.lnx[s] <= 0 || d.lnx[s] > CUW_MAXLN) { delete h; return CUW_ERR_ARG; }
+    int n = 0;
+    for (int ln = 0; ln < d.lnx[s]; ++ln) {
+      int l = d.lox[s][ln];
+      if (l < 0 || (l + 1) * (l + 1) > d.lmx) { delete h; return CUW_ERR_ARG; }
+      n += 2 * l + 1;
+    }
+    h->lmnx[s] = n;
+    h->lmnxx = std::max(h->lmnxx, n);
+    h->lnxx = std::max(h->lnxx, d.lnx[s]);
+    h->ibpro[s] = nbare;
+    nbare += d.lnx[s];
+  }
+  h->nbarepro = nbare;
+  h->ipro0.resize(d.nat);
+  for (int a = 0; a < d.nat; ++a) {
+    int s = h->isp[a];
+    h->ipro0[a] = h->npro;
+    for (int ln = 0; ln < d.lnx[s]; ++ln) {
+      int l = d.lox[s][ln];
+      for (int m = 0; m < 2 * l + 1; ++m) h->pdesc.push_back(ProDesc{a, h->ibpro[s] + ln, l * l + m, l});
+    }
+    h->npro += h->lmnx[s];
+  }
+  h->ldg = ceil_div(d.ngl, 32) * 32;
+  h->nr = (size_t)d.nr1 * d.nr2 * d.nr3;
+  h->occ_h.assign(d.nb, 0.0);
+  int rc = CUW_OK;
+  do {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = CUW_ERR_CUDA; break; }
+    Device& g = h->g;
+    const size_t nps = (size_t)h->ldg * d.nbh * sizeof(double2);
+    const size_t npj = (size_t)d.nbh * std::max(1, h->npro) * sizeof(double2);
+    const size_t nn = (size_t)d.nb * d.nb;
+    const size_t mn = (size_t)d.nbh * d.nbh;
+#define TRYA(p, b) \
+  if ((rc = dev_alloc(h, reinterpret_cast<void**>(&(p)), (b))) != CUW_OK) break
+    TRYA(g.psi0, nps); TRYA(g.psim, nps); TRYA(g.hpsi, nps); TRYA(g.opsi, nps);
+    TRYA(g.proj, npj); TRYA(g.oproj, npj); TRYA(g.hproj, npj); TRYA(g.pbuf, npj);
+    TRYA(g.rlam0, nn * sizeof(double2)); TRYA(g.rlamm, nn * sizeof(double2));
+    TRYA(g.igvec, sizeof(int) * 3 * d.ngl); TRYA(g.minusg, sizeof(int) * d.ngl);
+    TRYA(g.gx, sizeof(double) * d.ngl); TRYA(g.gy, sizeof(double) * d.ngl); TRYA(g.gz, sizeof(double) * d.ngl);
+    TRYA(g.g2, sizeof(double) * d.ngl); TRYA(g.mpsi, sizeof(double) * d.ngl);
+    TRYA(g.pro, sizeof(double) * d.ngl * (size_t)nbare); TRYA(g.ylm, sizeof(double) * d.ngl * (size_t)d.lmx);
+    TRYA(g.pdesc, sizeof(ProDesc) * std::max(1, h->npro));
+    TRYA(g.v, sizeof(double) * h->nr);
+    TRYA(g.r0, sizeof(double) * 3 * std::max(1, d.nat)); TRYA(g.rp, sizeof(double) * 3 * std::max(1, d.nat));
+    TRYA(g.rm, sizeof(double) * 3 * std::max(1, d.nat)); TRYA(g.force, sizeof(double) * 3 * std::max(1, d.nat));
+    TRYA(g.mass, sizeof(double) * std::max(1, d.nat));
+    TRYA(g.eigr, sizeof(double2) * d.ngl * (size_t)std::max(1, d.nat));
+    TRYA(g.dh, sizeof(double2) * (size_t)h->lmnxx * h->lmnxx * std::max(1, d.nat));
+    TRYA(g.dover, sizeof(double) * (size_t)h->lnxx * h->lnxx * d.nsp);
+    TRYA(g.occ, sizeof(double) * d.nb);
+    TRYA(g.mat, sizeof(double) * nn); TRYA(g.omat, sizeof(double) * nn); TRYA(g.oomat, sizeof(double) * nn);
+    TRYA(g.lam, sizeof(double) * nn); TRYA(g.lam2, sizeof(double) * nn); TRYA(g.u, sizeof(double) * nn);
+    TRYA(g.eig, sizeof(double) * d.nb); TRYA(g.haux, sizeof(double) * nn); TRYA(g.gamn, sizeof(double) * nn);
+    TRYA(g.work, sizeof(double) * nn); TRYA(g.wk2, sizeof(double) * nn);
+    TRYA(g.maxpart, sizeof(double) * 64); TRYA(g.ostatus, sizeof(int) * 16);
+    TRYA(g.lam1c, sizeof(double2) * mn); TRYA(g.lam2c, sizeof(double2) * mn);
+    TRYA(g.tmat, sizeof(double2) * 12 * mn);
+    TRYA(g.red, sizeof(double) * (4 * (size_t)d.nbh * (ceil_div(d.ngl, RG) + 1) + 8));
+    TRYA(g.scal, sizeof(double) * (size_t)(2 * d.nb + 16));
+#undef TRYA
+    if (rc != CUW_OK) break;
+    if (cudaMemcpy(g.pdesc, h->pdesc.data(), sizeof(ProDesc) * h->npro, cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = CUW_ERR_CUDA;
+      break;
+    }
+    rc = small_tables_setup(h);
+  } while (0);
+  if (rc != CUW_OK) {
+    free_all(h);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return rc;
+  }
+  *out = reinterpret_cast<cuw_handle*>(h);
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_destroy(cuw_handle* hp) {
+  if (!hp) return CUW_OK;
+  H(hp);
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_last_error(const cuw_handle* hp, char* buf, int len) {
+  if (!buf || len <= 0) return CUW_ERR_ARG;
+  const Handle* h = reinterpret_cast<const Handle*>(hp);
+  std::snprintf(buf, (size_t)len, "%s", h ? h->err.c_str() : "null handle");
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_async(cuw_handle* hp, int async) {
+  H(hp);
+  h->async = async != 0;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_synchronize(cuw_handle* hp) {
+  H(hp);
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* minusg, const double* gbas,
+                                const double* gvec, const double* g2, const double* pro, const double* ylm,
+                                const double* mpsi, const double* bucket, double gweight) {
+  H(hp);
+  NEED(igvec && minusg && gbas && gvec && g2 && pro && ylm && mpsi, CUW_ERR_ARG, "null argument");
+  NEED(gweight > 0.0, CUW_ERR_ARG, "gweight must be the positive cell volume");
+  const int ngl = h->d.ngl;
+  Device& g = h->g;
+  std::vector<int> mg(ngl);
+  for (int i = 0; i < ngl; ++i) {
+    mg[i] = minusg[i] - 1;
+    NEED(mg[i] >= 0 && mg[i] < ngl, CUW_ERR_ARG, "minusg out of range");
+    NEED(minusg[mg[i]] - 1 == i, CUW_ERR_ARG, "minusg is not an involution");
+  }
+  std::vector<double> x(ngl), y(ngl), z(ngl);
+  for (int i = 0; i < ngl; ++i) {
+    x[i] = gvec[3 * i];
+    y[i] = gvec[3 * i + 1];
+    z[i] = gvec[3 * i + 2];
+  }
+  std::memcpy(h->gbas, gbas, sizeof(h->gbas));
+  h->gweight = gweight;
+  CUW_TRY(cudaMemcpy(g.igvec, igvec, sizeof(int) * 3 * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.minusg, mg.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.gx, x.data(), sizeof(double) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.gy, y.data(), sizeof(double) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.gz, z.data(), sizeof(double) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.g2, g2, sizeof(double) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.pro, pro, sizeof(double) * ngl * (size_t)h->nbarepro, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.ylm, ylm, sizeof(double) * ngl * (size_t)h->d.lmx, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.mpsi, mpsi, sizeof(double) * ngl, cudaMemcpyHostToDevice));
+  if (bucket) {
+    if (!g.bucket) CUW_TRY(cudaMalloc(&g.bucket, sizeof(double) * ngl));
+    CUW_TRY(cudaMemcpy(g.bucket, bucket, sizeof(double) * ngl, cudaMemcpyHostToDevice));
+    h->tbucket = true;
+  } else {
+    h->tbucket = false;
+  }
+  CUW_RET(fft_setup(h, igvec));
+  h->have_gset = true;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_potential(cuw_handle* hp, const double* v) {
+  H(hp);
+  NEED(v, CUW_ERR_ARG, "null potential");
+  CUW_TRY(cudaMemcpy(h->g.v, v, sizeof(double) * h->nr, cudaMemcpyHostToDevice));
+  h->have_v = true;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_dh(cuw_handle* hp, int lmnxx, const double* dh) {
+  H(hp);
+  NEED(dh && lmnxx >= h->lmnxx, CUW_ERR_ARG, "DH: lmnxx smaller than the largest LMNX");
+  const int L = h->lmnxx, nat = h->d.nat;
+  std::vector<double2> t((size_t)L * L * std::max(1, nat));
+  for (int a = 0; a < nat; ++a)
+    for (int j = 0; j < L; ++j)
+      for (int i = 0; i < L; ++i) {
+        size_t src = 2 * ((size_t)i + (size_t)lmnxx * (j + (size_t)lmnxx * a));
+        t[i + (size_t)L * (j + (size_t)L * a)] = make_double2(dh[src], dh[src + 1]);
+      }
+  CUW_TRY(cudaMemcpy(h->g.dh, t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice));
+  h->have_dh = true;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_do(cuw_handle* hp, int lnxx, const double* dover) {
+  H(hp);
+  NEED(dover && lnxx >= h->lnxx, CUW_ERR_ARG, "DO: lnxx smaller than the largest LNX");
+  const int L = h->lnxx, nsp = h->d.nsp;
+  std::vector<double> t((size_t)L * L * nsp);
+  for (int s = 0; s < nsp; ++s)
+    for (int j = 0; j < L; ++j)
+      for (int i = 0; i < L; ++i) t[i + (size_t)L * (j + (size_t)L * s)] = dover[i + (size_t)lnxx * (j + (size_t)lnxx * s)];
+  CUW_TRY(cudaMemcpy(h->g.dover, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+  h->have_do = true;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_atoms(cuw_handle* hp, const double* r0, const double* rp) {
+  H(hp);
+  const size_t n = sizeof(double) * 3 * h->d.nat;
+  if (r0) CUW_TRY(cudaMemcpy(h->g.r0, r0, n, cudaMemcpyHostToDevice));
+  if (rp) CUW_TRY(cudaMemcpy(h->g.rp, rp, n, cudaMemcpyHostToDevice));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_reset_atoms(cuw_handle* hp, const double* r0) {
+  H(hp);
+  NEED(r0, CUW_ERR_ARG, "null positions");
+  const size_t n = sizeof(double) * 3 * h->d.nat;
+  CUW_TRY(cudaMemcpy(h->g.r0, r0, n, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(h->g.rp, r0, n, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(h->g.rm, r0, n, cudaMemcpyHostToDevice));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_get_atoms(cuw_handle* hp, double* rm, double* r0, double* rp) {
+  H(hp);
+  const size_t n = sizeof(double) * 3 * h->d.nat;
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  if (rm) CUW_TRY(cudaMemcpy(rm, h->g.rm, n, cudaMemcpyDeviceToHost));
+  if (r0) CUW_TRY(cudaMemcpy(r0, h->g.r0, n, cudaMemcpyDeviceToHost));
+  if (rp) CUW_TRY(cudaMemcpy(rp, h->g.rp, n, cudaMemcpyDeviceToHost));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_occ(cuw_handle* hp, const double* occ) {
+  H(hp);
+  NEED(occ, CUW_ERR_ARG, "null occupations");
+  h->occ_h.assign(occ, occ + h->d.nb);
+  CUW_TRY(cudaMemcpy(h->g.occ, occ, sizeof(double) * h->d.nb, cudaMemcpyHostToDevice));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_dynamics(cuw_handle* hp, double delt, double annee) {
+  H(hp);
+  NEED(delt > 0.0 && annee > -1.0, CUW_ERR_ARG, "DELT must be positive and ANNEE > -1");
+  h->delt = delt;
+  h->annee = annee;
+  return CUW_OK;
+}
+
+static double2* psi_ptr(Handle* h, int which) {
+  switch (which) {
+    case CUW_PSI0: return h->g.psi0;
+    case CUW_PSIM: return h->g.psim;
+    case CUW_HPSI: return h->g.hpsi;
+    case CUW_OPSI: return h->g.opsi;
+  }
+  return nullptr;
+}
+
+extern "C" int cuwaves_upload_psi(cuw_handle* hp, int which, const double* psi) {
+  H(hp);
+  double2* d = psi_ptr(h, which);
+  NEED(d && psi, CUW_ERR_ARG, "bad wave-function selector or null pointer");
+  CUW_TRY(cudaMemcpy2DAsync(d, sizeof(double2) * h->ldg, psi, sizeof(double2) * h->d.ngl,
+                            sizeof(double2) * h->d.ngl, h->d.nbh, cudaMemcpyHostToDevice, h->stream));
+  if (which == CUW_HPSI) h->have_hpsi = true;
+  return h->sync();
+}
+
+extern "C" int cuwaves_download_psi(cuw_handle* hp, int which, double* psi) {
+  H(hp);
+  double2* d = psi_ptr(h, which);
+  NEED(d && psi, CUW_ERR_ARG, "bad wave-function selector or null pointer");
+  CUW_TRY(cudaMemcpy2DAsync(psi, sizeof(double2) * h->d.ngl, d, sizeof(double2) * h->ldg,
+                            sizeof(double2) * h->d.ngl, h->d.nbh, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_get_proj(cuw_handle* hp, double* proj) {
+  H(hp);
+  CUW_TRY(cudaMemcpyAsync(proj, h->g.proj, sizeof(double2) * h->d.nbh * h->npro, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_proj(cuw_handle* hp, const double* proj) {
+  H(hp);
+  CUW_TRY(cudaMemcpyAsync(h->g.proj, proj, sizeof(double2) * h->d.nbh * h->npro, cudaMemcpyHostToDevice, h->stream));
+  return h->sync();
+}
+
+extern "C" int cuwaves_get_rlam0(cuw_handle* hp, double* r) {
+  H(hp);
+  CUW_TRY(cudaMemcpyAsync(r, h->g.rlam0, sizeof(double2) * h->d.nb * h->d.nb, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_rlam0(cuw_handle* hp, const double* r) {
+  H(hp);
+  CUW_TRY(cudaMemcpyAsync(h->g.rlam0, r, sizeof(double2) * h->d.nb * h->d.nb, cudaMemcpyHostToDevice, h->stream));
+  return h->sync();
+}
+
+extern "C" int cuwaves_projections(cuw_handle* hp) {
+  H(hp);
+  NEED(h->have_gset, CUW_ERR_STATE, "G set not loaded");
+  CUW_RET(eigr_compute(h, h->g.r0));
+  CUW_RET(proj_compute(h, h->g.psi0, h->g.proj, nullptr, nullptr));
+  return h->sync();
+}
+
+extern "C" int cuwaves_hpsi(cuw_handle* hp) {
+  H(hp);
+  NEED(h->have_gset && h->have_v && h->have_dh, CUW_ERR_STATE, "G set, potential or DH not loaded");
+  CUW_RET(fft_vpsi(h, h->g.psi0, h->g.hpsi, true));
+  CUW_RET(hproj_compute(h, h->g.proj, h->g.hproj));
+  CUW_RET(eigr_compute(h, h->g.r0));
+  CUW_RET(addpro_run(h, ADDPRO_HPSI, h->g.hproj, nullptr));
+  h->have_hpsi = true;
+  return h->sync();
+}
+
+extern "C" int cuwaves_ekin(cuw_handle* hp, double* ekin) {
+  H(hp);
+  NEED(h->have_gset && ekin, CUW_ERR_STATE, "G set not loaded");
+  return band_reduce(h, RED_EKIN, ekin, nullptr);
+}
+
+extern "C" int cuwaves_expectation(cuw_handle* hp, double* eig) {
+  H(hp);
+  NEED(h->have_hpsi, CUW_ERR_STATE, "HPSI NOT AVAILABLE");
+  NEED(eig, CUW_ERR_ARG, "null eig");
+  return band_reduce(h, RED_EXPECT, nullptr, eig);
+}
+
+extern "C" int cuwaves_wavekinetic(cuw_handle* hp, double* ekin, double* eig) {
+  H(hp);
+  NEED(h->have_gset, CUW_ERR_STATE, "G set not loaded");
+  double e = 0.0;
+  CUW_RET(band_reduce(h, RED_WAVEKIN, &e, eig));
+  if (ekin) *ekin = e;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_force(cuw_handle* hp, double* force) {
+  H(hp);
+  NEED(h->have_gset && h->have_dh && h->have_do, CUW_ERR_STATE, "G set, DH or DO not loaded");
+  NEED(force, CUW_ERR_ARG, "null force");
+  CUW_RET(eigr_compute(h, h->g.r0));
+  CUW_RET(force_dev_run(h, h->g.force));
+  CUW_TRY(cudaMemcpyAsync(force, h->g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_propagate(cuw_handle* hp) {
+  H(hp);
+  NEED(h->have_hpsi, CUW_ERR_STATE, "HPSI NOT AVAILABLE: EITHER WAVES$ETOT HAS NOT BEEN CALLED OR WAVES$PROPAGATE HAS BEEN CALLED PREVIOUSLY");
+  CUW_RET(propagate_run(h));
+  h->have_hpsi = false;
+  return h->sync();
+}
+
+extern "C" int cuwaves_orthogonalize(cuw_handle* hp, int max_iter, double eps, int* iters) {
+  H(hp);
+  NEED(h->have_gset && h->have_do, CUW_ERR_STATE, "G set or DO not loaded");
+  NEED(max_iter > 0 && eps > 0.0, CUW_ERR_ARG, "max_iter and eps must be positive");
+  // OPSI = (PSI0 + |p>DO<p|PSI0>) * dt^2/((1+annee) m_G) with PROJ at R(0)
+  CUW_RET(oproj_compute(h, h->g.proj, h->g.oproj));
+  CUW_RET(eigr_compute(h, h->g.r0));
+  CUW_RET(addpro_run(h, ADDPRO_OPSI, nullptr, h->g.oproj));
+  CUW_RET(ortho_core(h, max_iter, eps, iters));
+  // second part of the fictitious kinetic energy (src/paw_waves2.f90:490)
+  double e2 = 0.0;
+  CUW_RET(band_reduce(h, RED_WAVEKIN, &e2, nullptr));
+  h->waveekin2 = e2;
+  return h->sync();
+}
+
+extern "C" int cuwaves_switch(cuw_handle* hp) {
+  H(hp);
+  std::swap(h->g.psi0, h->g.psim);
+  CUW_RET(switch_lambda_run(h));
+  h->waveekin1 = h->waveekin2 = 0.0;
+  return h->sync();
+}
+
+extern "C" int cuwaves_stop(cuw_handle* hp) {
+  H(hp);
+  CUW_TRY(cudaMemcpyAsync(h->g.psim, h->g.psi0, sizeof(double2) * h->ldg * h->d.nbh, cudaMemcpyDeviceToDevice,
+                          h->stream));
+  h->have_rlamm = false;
+  return h->sync();
+}
+
+extern "C" int cuwaves_gramschmidt(cuw_handle* hp, int which, const double* r) {
+  H(hp);
+  NEED(h->have_gset && h->have_do, CUW_ERR_STATE, "G set or DO not loaded");
+  NEED(which == CUW_PSI0 || which == CUW_PSIM, CUW_ERR_ARG, "Gram-Schmidt acts on PSI0 or PSIM");
+  NEED(r, CUW_ERR_ARG, "null positions");
+  Device& g = h->g;
+  double2* psi = psi_ptr(h, which);
+  // atom positions r -> rm slot is not touched: use force buffer as scratch for r
+  double* rd = g.force;
+  CUW_TRY(cudaMemcpyAsync(rd, r, sizeof(double) * 3 * h->d.nat, cudaMemcpyHostToDevice, h->stream));
+  CUW_RET(eigr_compute(h, rd));
+  CUW_RET(proj_compute(h, psi, g.hproj, nullptr, nullptr));
+  CUW_RET(oproj_compute(h, g.hproj, g.pbuf));
+  const size_t mn = (size_t)h->d.nbh * h->d.nbh;
+  double2* pw = g.tmat;
+  double2* oc = g.tmat + 6 * mn;
+  GramPair pc[1] = {{g.hproj, g.pbuf}};
+  CUW_RET(gram_projections(h, pc, 1, oc));
+  GramPair pp[1] = {{psi, psi}};
+  CUW_RET(gram_planewave(h, pp, 1, pw));
+  CUW_RET(unravel_run(h, pw, oc, 1, g.mat, nullptr, nullptr));
+  CUW_RET(ortho_y_run(h, g.mat, g.wk2));
+  CUW_RET(fold_x_run(h, g.wk2, g.lam1c, g.lam2c));
+  // PSIINV = PSI (copy into OPSI), PSI += PSIINV X1 + PSIINV(-) X2
+  size_t n = (size_t)h->ldg * h->d.nbh;
+  k_copy_psi<<<4 * h->nsm, 256, 0, h->stream>>>(psi, g.opsi, n);
+  CUW_LAUNCH_CHECK("k_copy_psi");
+  CUW_RET(addopsi_run(h, psi, g.opsi, g.lam1c, g.lam2c));
+  int st = 0;
+  CUW_TRY(cudaMemcpyAsync(&st, g.ostatus, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  if (st != CUW_OK) return h->fail(st, "NAN DETECTED in WAVES_ORTHO_Y_C");
+  return CUW_OK;
+}
+
+// One CP step (see the header).  Kernel order:
+//   EKIN, WAVEKINETIC(1) | EIGR(R0) | forces | FFT V.psi | DH.PROJ, DO.PROJ |
+//   fused ADDPRO (HPSI, OPSI, PROPAGATE) | <psi|H|psi> | atoms |
+//   ORTHOGONALIZE at R(+) | WAVEKINETIC(2) | SWITCH
+extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mass, int max_iter, double eps,
+                               double* out, double* force) {
+  H(hp);
+  NEED(h->have_gset && h->have_v && h->have_dh && h->have_do, CUW_ERR_STATE, "inputs not loaded");
+  NEED(!move_atoms || mass, CUW_ERR_ARG, "masses required to move atoms");
+  Device& g = h->g;
+  double* sc = g.scal;  // [0] ekin [1] etot [2] ekin1 [3] ekin2 [4] eion ; per-band scratch after 8
+  double* tmpv = g.scal + 8;
+  CUW_RET(energy_run(h, RED_EKIN, tmpv));
+  CUW_TRY(cudaMemcpyAsync(sc + 0, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
+  CUW_TRY(cudaMemcpyAsync(sc + 2, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(eigr_compute(h, g.r0));
+  CUW_RET(force_dev_run(h, g.force));
+  CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
+  CUW_RET(hproj_compute(h, g.proj, g.hproj));
+  CUW_RET(oproj_compute(h, g.proj, g.oproj));
+  CUW_RET(addpro_run(h, ADDPRO_FUSED, g.hproj, g.oproj));
+  CUW_RET(energy_run(h, RED_EXPECT, tmpv));
+  CUW_TRY(cudaMemcpyAsync(sc + 1, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  if (move_atoms) {
+    CUW_TRY(cudaMemcpyAsync(g.mass, mass, sizeof(double) * h->d.nat, cudaMemcpyHostToDevice, h->stream));
+    k_atoms_verlet<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(g.r0, g.rm, g.rp, g.force, g.mass, h->d.nat,
+                                                                       h->delt * h->delt);
+    CUW_LAUNCH_CHECK("k_atoms_verlet");
+  }
+  int iters = 0;
+  CUW_RET(ortho_core(h, max_iter, eps, &iters));
+  CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
+  CUW_TRY(cudaMemcpyAsync(sc + 3, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  if (move_atoms) {
+    k_ion_ekin<<<1, 1, 0, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
+    CUW_LAUNCH_CHECK("k_ion_ekin");
+    // ATOMS$SWITCH: R(-) <- R(0), R(0) <- R(+)
+    std::swap(g.rm, g.r0);
+    std::swap(g.r0, g.rp);
+    CUW_TRY(cudaMemcpyAsync(g.rp, g.r0, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToDevice, h->stream));
+  } else {
+    CUW_TRY(cudaMemsetAsync(sc + 4, 0, sizeof(double), h->stream));
+  }
+  std::swap(g.psi0, g.psim);
+  CUW_RET(switch_lambda_run(h));
+  h->have_hpsi = false;
+  double hs[5];
+  CUW_TRY(cudaMemcpyAsync(hs, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+  if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  if (out) {
+    out[0] = hs[1];
+    out[1] = hs[0];
+    out[2] = 0.5 * (hs[2] + hs[3]);
+    out[3] = hs[4];
+    out[4] = iters;
+    out[5] = out[6] = out[7] = 0.0;
+  }
+  return CUW_OK;
+}

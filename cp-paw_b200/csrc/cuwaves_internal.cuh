@@ -1,0 +1,220 @@
+// Internal state and device helpers of the cuwaves engine (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/cuwaves.h"
+
+namespace cuw {
+
+// ---------------------------------------------------------------------------
+// error handling: every CUDA call is checked and turned into a status code
+// ---------------------------------------------------------------------------
+struct Status {
+  int code = CUW_OK;
+  std::string msg;
+};
+
+#define CUW_TRY(expr)                                              \
+  do {                                                             \
+    cudaError_t e__ = (expr);                                      \
+    if (e__ != cudaSuccess) {                                      \
+      return h->fail(CUW_ERR_CUDA, std::string(#expr) + ": " +     \
+                                       cudaGetErrorString(e__));   \
+    }                                                              \
+  } while (0)
+
+#define CUW_LAUNCH_CHECK(name)                                      \
+  do {                                                              \
+    cudaError_t e__ = cudaGetLastError();                           \
+    if (e__ != cudaSuccess)                                         \
+      return h->fail(CUW_ERR_CUDA, std::string(name) + ": " +       \
+                                       cudaGetErrorString(e__));    \
+  } while (0)
+
+#define CUW_RET(expr)            \
+  do {                           \
+    int r__ = (expr);            \
+    if (r__ != CUW_OK) return r__; \
+  } while (0)
+
+// Projector descriptor: IPRO -> (atom, bare projector column, LM, L)
+struct ProDesc {
+  int iat;
+  int ibare;
+  int lm;
+  int l;
+};
+
+// FFT plan of one grid axis: radix sequence of a Stockham transform
+struct AxisPlan {
+  int n = 0;
+  int nstage = 0;
+  int radix[8] = {0};
+};
+
+// Device arrays of one wave-function set.
+struct Device {
+  // wave functions (ld = ldg complex numbers per band)
+  double2 *psi0 = nullptr, *psim = nullptr, *hpsi = nullptr, *opsi = nullptr;
+  double2 *proj = nullptr;       // (NBH, NPRO)
+  double2 *oproj = nullptr;      // (NBH, NPRO) scratch
+  double2 *hproj = nullptr;      // (NBH, NPRO) scratch
+  double2 *pbuf = nullptr;       // (NBH, NPRO) scratch
+  double2 *rlam0 = nullptr;      // (NB, NB) complex, Fortran layout
+  double2 *rlamm = nullptr;
+  // g-set
+  int *igvec = nullptr;          // (3, NGL)
+  int *minusg = nullptr;         // (NGL) 0-based
+  double *gx = nullptr, *gy = nullptr, *gz = nullptr, *g2 = nullptr;
+  double *pro = nullptr;         // (NGL, NBAREPRO)
+  double *ylm = nullptr;         // (NGL, LMX)
+  double *mpsi = nullptr;        // (NGL)
+  double *bucket = nullptr;      // (NGL) or null
+  ProDesc *pdesc = nullptr;      // (NPRO)
+  // FFT
+  int *plane_iz = nullptr;       // (nzp) occupied z planes
+  int *plane_off = nullptr;      // (nzp+1) CSR offsets of the G lists
+  int *plane_g = nullptr;        // (NGL) G index, grouped by plane
+  int *plane_pos = nullptr;      // (NGL) ix + NR1*iy of that G
+  int *zslot = nullptr;          // (NR3) compact plane index or -1
+  double *v = nullptr;           // (NR1*NR2*NR3) local potential
+  double2 *grid = nullptr;       // (batch, nzp, NR2, NR1) work grid
+  double2 *tw1 = nullptr, *tw2 = nullptr, *tw3 = nullptr;  // twiddles exp(+2 pi i k/n)
+  // atoms and one-centre data
+  double *r0 = nullptr, *rp = nullptr, *rm = nullptr;  // (3, NAT)
+  double *force = nullptr;       // (3, NAT)
+  double *mass = nullptr;        // (NAT)
+  double2 *eigr = nullptr;       // (NGL, NAT) structure factors of the last position set
+  double2 *dh = nullptr;         // (LMNXX, LMNXX, NAT)
+  double *dover = nullptr;       // (LNXX, LNXX, NSP)
+  double *occ = nullptr;         // (NB)
+  // orthogonalisation (real NB x NB)
+  double *mat = nullptr, *omat = nullptr, *oomat = nullptr;
+  double *lam = nullptr, *lam2 = nullptr;
+  double *u = nullptr, *eig = nullptr;
+  double *haux = nullptr, *gamn = nullptr, *work = nullptr, *wk2 = nullptr;
+  double *maxpart = nullptr;
+  int *ostatus = nullptr;        // [0] status, [1] iterations
+  double2 *lam1c = nullptr, *lam2c = nullptr;  // (NBH, NBH) folded multipliers
+  double2 *tmat = nullptr;       // 12 (NBH, NBH) reduced Gram products
+  // scratch for split-K partial sums and band reductions
+  double2 *part = nullptr;
+  size_t part_bytes = 0;
+  double *red = nullptr;         // reductions
+  double *scal = nullptr;        // small scalar results
+  // projector-map tables: first IPRO and #LMN per atom, species per atom,
+  // (LN, M) of each IPRO, first LMN of each (species, LN), LOX (-1 = none)
+  int *t_ipro0 = nullptr, *t_nlmn = nullptr, *t_isp = nullptr, *t_lnofp = nullptr, *t_mofp = nullptr,
+      *t_lmn0ln = nullptr, *t_lox = nullptr;
+};
+
+struct Handle {
+  cuw_dims d{};
+  std::vector<int> isp;          // 0-based
+  std::vector<int> lmnx, ibpro, ipro0;
+  std::vector<ProDesc> pdesc;
+  int npro = 0, nbarepro = 0, lmnxx = 0, lnxx = 0;
+  int ldg = 0;                   // leading dimension of wave-function arrays
+  double gweight = 0.0;
+  double gbas[9] = {0};
+  double delt = 0.0, annee = 0.0;
+  bool have_gset = false, have_v = false, have_dh = false, have_do = false;
+  bool have_hpsi = false, have_rlamm = false, have_opsi = false, have_u = false;
+  bool tbucket = false;
+  bool async = false;
+  int nzp = 0;                   // occupied z planes
+  int batch = 0;                 // bands per FFT batch
+  AxisPlan ax[3];
+  size_t nr = 0;
+  std::vector<double> occ_h;
+  double waveekin1 = 0.0, waveekin2 = 0.0;
+  cudaStream_t stream = nullptr;
+  int device = 0, nsm = 148;
+  Device g;
+  std::string err;
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int sync() {
+    if (async) return CUW_OK;
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return fail(CUW_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+    return CUW_OK;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// (-i)^l
+__device__ __forceinline__ double2 mipow(int l) {
+  switch (l & 3) {
+    case 0: return make_double2(1.0, 0.0);
+    case 1: return make_double2(0.0, -1.0);
+    case 2: return make_double2(-1.0, 0.0);
+    default: return make_double2(0.0, 1.0);
+  }
+}
+
+// FP64 tensor-core MMA, m8n8k4, A row-major / B column-major fragments:
+//   a = A[lane>>2][lane&3], b = B[lane&3][lane>>2],
+//   c[0..1] = C[lane>>2][2*(lane&3)+0..1]
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+// host helpers implemented in the .cu files
+int fft_setup(Handle* h, const int* igvec_host);
+int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic);
+int eigr_compute(Handle* h, const double* r_dev);
+int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* psiB, double2* projB);
+int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc);
+int hproj_compute(Handle* h, const double2* proj, double2* out);
+int oproj_compute(Handle* h, const double2* proj, double2* out);
+int gram_overlaps(Handle* h, double2* projP, double2* projO);
+int ortho_solve(Handle* h, int max_iter, double eps, int* iters);
+int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* l1, const double2* l2);
+int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* l1, const double2* l2);
+int lambda12_run(Handle* h, const double* lam_real, double2* l1, double2* l2);
+int band_reduce(Handle* h, int what, double* out_host, double* eig_host);
+int force_run(Handle* h, double* force_host);
+int force_gemm(Handle* h, const double2* ded, double* force_dev);
+int small_tables_setup(Handle* h);
+struct GramPair {
+  const double2* x;
+  const double2* y;
+};
+int gram_planewave(Handle* h, const GramPair* pairs, int npair, double2* dst);
+int gram_projections(Handle* h, const GramPair* pairs, int npair, double2* dst);
+int propagate_run(Handle* h);
+int opsi_scale_run(Handle* h);
+int switch_lambda_run(Handle* h);
+int gramschmidt_run(Handle* h, double2* psi, const double* r_dev);
+int atoms_verlet_run(Handle* h, const double* mass_dev);
+
+enum { ADDPRO_HPSI = 0, ADDPRO_OPSI = 1, ADDPRO_FUSED = 2 };
+enum { RED_EKIN = 0, RED_WAVEKIN = 1, RED_EXPECT = 2 };
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace cuw

@@ -1,0 +1,457 @@
+// Band-batched 3-D FFT with the local potential fused in (WAVES_VPSI).
+//
+// Reference: WAVES_VPSI (src/paw_waves1.f90:5099-5194) runs, per band, the
+// three 1-D passes of PLANEWAVE_FFTGTOR (src/paw_fft.f90:2012-2177), multiplies
+// by V(r), and runs the three passes of PLANEWAVE_FFTRTOG (:2180-2341).
+// Conventions (src/paw_library.f90:2635-2728): G->r is exp(+iGr) and unscaled;
+// r->G is exp(-iGr) with 1/N.  Like the reference, only the z-planes that hold
+// G vectors are transformed in x and y (its NR3END1/NR3END2 pruning).
+//
+// B200 layout: three kernels per band batch.
+//   gtor_plane : sphere -> xy-plane in shared memory, x then y transforms,
+//                plane written to the work grid (only occupied planes).
+//   zcol_v     : z columns of 16 x-points: inverse z transform, V(r) and the
+//                1/N scale, forward z transform, in shared memory.
+//   rtog_plane : forward y then x transforms of a plane, gathered back onto
+//                the sphere with 1/2|G|^2 (+bucket) psi added.
+// Each 1-D transform is a mixed-radix Stockham autosort (radix 2,3,4,5,7,8,11)
+// whose butterflies run in registers; every stage reads all of its inputs into
+// registers before a barrier and writes after it, so it works in place.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "cuwaves_internal.cuh"
+
+namespace cuw {
+
+namespace {
+
+constexpr int kMaxV = 16;  // complex values per thread per stage
+
+// --- radix butterflies: v <- DFT_R(v) with exp(sign*2*pi*i*q*s/R) -----------
+__device__ __forceinline__ double2 mul_i(double2 a, double sgn) {  // a * (sgn*i)
+  return make_double2(-sgn * a.y, sgn * a.x);
+}
+
+template <int R>
+struct Bfly;
+
+template <>
+struct Bfly<2> {
+  __device__ __forceinline__ static void run(double2 (&v)[2], double, const double2*, int) {
+    double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <>
+struct Bfly<3> {
+  __device__ __forceinline__ static void run(double2 (&v)[3], double sgn, const double2*, int) {
+    const double h = 0.86602540378443864676;  // sqrt(3)/2
+    double2 a = v[0], t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    double2 u = mul_i(cscale(d, h), sgn);
+    double2 m = make_double2(a.x - 0.5 * t.x, a.y - 0.5 * t.y);
+    v[0] = cadd(a, t);
+    v[1] = cadd(m, u);
+    v[2] = csub(m, u);
+  }
+};
+
+template <>
+struct Bfly<4> {
+  __device__ __forceinline__ static void run(double2 (&v)[4], double sgn, const double2*, int) {
+    double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    double2 t2 = cadd(v[1], v[3]), t3 = mul_i(csub(v[1], v[3]), sgn);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  }
+};
+
+template <>
+struct Bfly<5> {
+  __device__ __forceinline__ static void run(double2 (&v)[5], double sgn, const double2*, int) {
+    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+    double2 a = v[0];
+    double2 p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
+    double2 p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
+    double2 r1 = make_double2(a.x + c1 * p1.x + c2 * p2.x, a.y + c1 * p1.y + c2 * p2.y);
+    double2 r2 = make_double2(a.x + c2 * p1.x + c1 * p2.x, a.y + c2 * p1.y + c1 * p2.y);
+    double2 i1 = mul_i(make_double2(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y), sgn);
+    double2 i2 = mul_i(make_double2(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y), sgn);
+    v[0] = make_double2(a.x + p1.x + p2.x, a.y + p1.y + p2.y);
+    v[1] = cadd(r1, i1);
+    v[4] = csub(r1, i1);
+    v[2] = cadd(r2, i2);
+    v[3] = csub(r2, i2);
+  }
+};
+
+template <>
+struct Bfly<8> {
+  __device__ __forceinline__ static void run(double2 (&v)[8], double sgn, const double2*, int) {
+    const double q = 0.70710678118654752440;
+    double2 e[4] = {v[0], v[2], v[4], v[6]};
+    double2 o[4] = {v[1], v[3], v[5], v[7]};
+    Bfly<4>::run(e, sgn, nullptr, 0);
+    Bfly<4>::run(o, sgn, nullptr, 0);
+    // twiddles W8^k = exp(sgn*i*pi*k/4)
+    double2 w1 = make_double2(q, sgn * q), w3 = make_double2(-q, sgn * q);
+    double2 o1 = cmul(o[1], w1), o2 = mul_i(o[2], sgn), o3 = cmul(o[3], w3);
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+  }
+};
+
+// generic prime radix through the twiddle table of the axis (tw[k] = W_N^k)
+template <int R>
+struct BflyGeneric {
+  __device__ __forceinline__ static void run(double2 (&v)[R], double, const double2* tw, int n) {
+    double2 out[R];
+    const int step = n / R;
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      double2 acc = v[0];
+#pragma unroll
+      for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], tw[((q * s) % R) * step]));
+      out[s] = acc;
+    }
+#pragma unroll
+    for (int s = 0; s < R; ++s) v[s] = out[s];
+  }
+};
+template <>
+struct Bfly<7> : BflyGeneric<7> {};
+template <>
+struct Bfly<11> : BflyGeneric<11> {};
+
+// One Stockham stage on `nlines` lines of length n held in shared memory:
+// element e of line L lives at buf[L*ls + e*es].  tw[k] = exp(sgn*2 pi i k/n).
+// jfast selects the thread mapping (consecutive threads -> consecutive j).
+template <int R>
+__device__ __noinline__ void stage(double2* buf, int n, int ns, int nlines, int ls, int es, bool jfast,
+                      const double2* tw, double sgn) {
+  constexpr int BPT = kMaxV / R;
+  const int nq = n / R;
+  const int total = nlines * nq;
+  double2 v[BPT][R];
+  int line_[BPT], j_[BPT];
+#pragma unroll
+  for (int t = 0; t < BPT; ++t) {
+    int bf = threadIdx.x + t * blockDim.x;
+    line_[t] = -1;
+    if (bf < total) {
+      int line, j;
+      if (jfast) { j = bf % nq; line = bf / nq; }
+      else { line = bf % nlines; j = bf / nlines; }
+      line_[t] = line;
+      j_[t] = j;
+      const int k = j % ns;
+      const int tstep = n / (ns * R);
+      double2* base = buf + (size_t)line * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        double2 x = base[(size_t)(j + r * nq) * es];
+        if (r && k) x = cmul(x, tw[(r * k * tstep) % n]);
+        v[t][r] = x;
+      }
+      Bfly<R>::run(v[t], sgn, tw, n);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < BPT; ++t) {
+    if (line_[t] >= 0) {
+      const int j = j_[t], k = j % ns;
+      const int idxd = (j / ns) * ns * R + k;
+      double2* base = buf + (size_t)line_[t] * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[(size_t)(idxd + r * ns) * es] = v[t][r];
+    }
+  }
+  __syncthreads();
+}
+
+struct AxisArg {
+  int n;
+  int nstage;
+  int radix[8];
+};
+
+__device__ void transform(double2* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast,
+                          const double2* tw, double sgn) {
+  int ns = 1;
+  for (int s = 0; s < ax.nstage; ++s) {
+    switch (ax.radix[s]) {
+      case 2: stage<2>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+      case 3: stage<3>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+      case 4: stage<4>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+      case 5: stage<5>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+      case 7: stage<7>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+      case 8: stage<8>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+      case 11: stage<11>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+    }
+    ns *= ax.radix[s];
+  }
+}
+
+// load twiddles exp(sgn*2 pi i k/n) from the table exp(+2 pi i k/n)
+__device__ void load_tw(double2* dst, const double2* src, int n, double sgn) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    double2 w = src[k];
+    dst[k] = make_double2(w.x, sgn * w.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
+                             const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
+                             double2* __restrict__ grid, int nzp, AxisArg a1, AxisArg a2,
+                             const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
+  extern __shared__ double2 sm[];
+  const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2;
+  double2* plane = sm;
+  double2* tw1 = sm + npl;
+  double2* tw2 = tw1 + nr1;
+  const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = make_double2(0.0, 0.0);
+  load_tw(tw1, tw1g, nr1, +1.0);
+  load_tw(tw2, tw2g, nr2, +1.0);
+  __syncthreads();
+  const double2* src = psi + (size_t)ldg * b;
+  for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x)
+    plane[plane_pos[k]] = src[plane_g[k]];
+  __syncthreads();
+  transform(plane, a1, nr2, nr1, 1, true, tw1, +1.0);   // x lines
+  transform(plane, a2, nr1, 1, nr1, false, tw2, +1.0);  // y lines
+  double2* dst = grid + ((size_t)bl * nzp + p) * npl;
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i];
+}
+
+constexpr int kTX = 16;  // x columns per z-column block
+
+__global__ void k_zcol_v(double2* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot,
+                         int nzp, int nr1, int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
+  extern __shared__ double2 sm[];
+  const int nr3 = a3.n;
+  double2* tile = sm;             // [nr3][kTX]
+  double2* tw = sm + nr3 * kTX;
+  const int nxb = (nr1 + kTX - 1) / kTX;
+  const int iy = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * kTX;
+  const int bl = blockIdx.y;
+  const size_t npl = (size_t)nr1 * nr2;
+  double2* gb = grid + (size_t)bl * nzp * npl;
+  load_tw(tw, tw3g, nr3, +1.0);
+  for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
+    int iz = i / kTX, x = i % kTX;
+    int s = zslot[iz];
+    double2 val = make_double2(0.0, 0.0);
+    if (s >= 0 && x0 + x < nr1) val = gb[(size_t)s * npl + (size_t)iy * nr1 + x0 + x];
+    tile[i] = val;
+  }
+  __syncthreads();
+  transform(tile, a3, kTX, 1, kTX, false, tw, +1.0);
+  for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
+    int iz = i / kTX, x = i % kTX;
+    double vv = 0.0;
+    if (x0 + x < nr1) vv = v[(size_t)x0 + x + (size_t)nr1 * (iy + (size_t)nr2 * iz)] * scale;
+    tile[i] = cscale(tile[i], vv);
+  }
+  __syncthreads();
+  // forward transform: conjugated twiddles
+  for (int k = threadIdx.x; k < nr3; k += blockDim.x) tw[k].y = -tw[k].y;
+  __syncthreads();
+  transform(tile, a3, kTX, 1, kTX, false, tw, -1.0);
+  for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
+    int iz = i / kTX, x = i % kTX;
+    int s = zslot[iz];
+    if (s >= 0 && x0 + x < nr1) gb[(size_t)s * npl + (size_t)iy * nr1 + x0 + x] = tile[i];
+  }
+}
+
+__global__ void k_rtog_plane(const double2* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
+                             const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
+                             double2* __restrict__ out, const double2* __restrict__ psi, int ldg, int b0,
+                             const double* __restrict__ g2, const double* __restrict__ bucket, int add_kin,
+                             AxisArg a1, AxisArg a2, const double2* __restrict__ tw1g,
+                             const double2* __restrict__ tw2g) {
+  extern __shared__ double2 sm[];
+  const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2;
+  double2* plane = sm;
+  double2* tw1 = sm + npl;
+  double2* tw2 = tw1 + nr1;
+  const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
+  const double2* srcp = grid + ((size_t)bl * nzp + p) * npl;
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = srcp[i];
+  load_tw(tw1, tw1g, nr1, -1.0);
+  load_tw(tw2, tw2g, nr2, -1.0);
+  __syncthreads();
+  transform(plane, a2, nr1, 1, nr1, false, tw2, -1.0);  // y lines
+  transform(plane, a1, nr2, nr1, 1, true, tw1, -1.0);   // x lines
+  double2* dst = out + (size_t)ldg * b;
+  const double2* ps = psi + (size_t)ldg * b;
+  for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
+    int g = plane_g[k];
+    double2 val = plane[plane_pos[k]];
+    if (add_kin) {
+      double kin = 0.5 * g2[g] + (bucket ? bucket[g] : 0.0);
+      double2 c = ps[g];
+      val.x += kin * c.x;
+      val.y += kin * c.y;
+    }
+    dst[g] = val;
+  }
+}
+
+AxisArg make_axis(const AxisPlan& p) {
+  AxisArg a;
+  a.n = p.n;
+  a.nstage = p.nstage;
+  for (int i = 0; i < 8; ++i) a.radix[i] = p.radix[i];
+  return a;
+}
+
+bool plan_axis(int n, AxisPlan& p) {
+  p.n = n;
+  p.nstage = 0;
+  int m = n;
+  const int order[] = {8, 4, 2, 3, 5, 7, 11};
+  for (int r : order) {
+    while (m % r == 0 && p.nstage < 8) {
+      p.radix[p.nstage++] = r;
+      m /= r;
+    }
+  }
+  // prefer a radix-8 stage over 4*2
+  return m == 1;
+}
+
+int plane_threads(int npl) {
+  // values per thread per stage must stay below kMaxV for every radix
+  int t = 128;
+  while (t < 1024 && (npl + t - 1) / t > kMaxV / 2) t *= 2;
+  return t;
+}
+
+}  // namespace
+
+int fft_setup(Handle* h, const int* igvec) {
+  const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3, ngl = h->d.ngl;
+  for (int a = 0; a < 3; ++a) {
+    int n = a == 0 ? nr1 : (a == 1 ? nr2 : nr3);
+    if (!plan_axis(n, h->ax[a]))
+      return h->fail(CUW_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has a prime factor above 11");
+  }
+  const size_t npl = (size_t)nr1 * nr2;
+  if (npl + nr1 + nr2 > (size_t)(220 * 1024) / sizeof(double2) || npl > (size_t)kMaxV / 2 * 1024 ||
+      (size_t)nr3 * kTX + nr3 > 14000)
+    return h->fail(CUW_ERR_UNSUPPORTED, "FFT plane too large for shared memory");
+  // occupied planes and the per-plane G lists
+  std::vector<int> cnt(nr3, 0);
+  std::vector<int> iz_of(ngl), pos_of(ngl);
+  for (int g = 0; g < ngl; ++g) {
+    int i1 = ((igvec[3 * g] % nr1) + nr1) % nr1;
+    int i2 = ((igvec[3 * g + 1] % nr2) + nr2) % nr2;
+    int i3 = ((igvec[3 * g + 2] % nr3) + nr3) % nr3;
+    iz_of[g] = i3;
+    pos_of[g] = i1 + nr1 * i2;
+    cnt[i3]++;
+  }
+  std::vector<int> zslot(nr3, -1), plane_iz, off(1, 0);
+  for (int z = 0; z < nr3; ++z)
+    if (cnt[z]) {
+      zslot[z] = (int)plane_iz.size();
+      plane_iz.push_back(z);
+      off.push_back(off.back() + cnt[z]);
+    }
+  const int nzp = (int)plane_iz.size();
+  std::vector<int> fill(off.begin(), off.end() - 1), pg(ngl), pp(ngl);
+  for (int g = 0; g < ngl; ++g) {
+    int s = zslot[iz_of[g]];
+    int k = fill[s]++;
+    pg[k] = g;
+    pp[k] = pos_of[g];
+  }
+  h->nzp = nzp;
+  // band batch: keep the work grid near 48 MB so that it stays in L2
+  const size_t per_band = (size_t)nzp * npl * sizeof(double2);
+  int batch = (int)std::max<size_t>(1, (48u << 20) / per_band);
+  batch = std::min(batch, h->d.nbh);
+  h->batch = batch;
+  Device& g = h->g;
+  if (g.plane_off) {
+    cudaFree(g.plane_off); cudaFree(g.plane_g); cudaFree(g.plane_pos); cudaFree(g.zslot); cudaFree(g.plane_iz);
+    cudaFree(g.grid); cudaFree(g.tw1); cudaFree(g.tw2); cudaFree(g.tw3);
+  }
+  CUW_TRY(cudaMalloc(&g.plane_off, sizeof(int) * (nzp + 1)));
+  CUW_TRY(cudaMalloc(&g.plane_g, sizeof(int) * ngl));
+  CUW_TRY(cudaMalloc(&g.plane_pos, sizeof(int) * ngl));
+  CUW_TRY(cudaMalloc(&g.zslot, sizeof(int) * nr3));
+  CUW_TRY(cudaMalloc(&g.plane_iz, sizeof(int) * nzp));
+  CUW_TRY(cudaMalloc(&g.grid, per_band * batch));
+  CUW_TRY(cudaMemcpy(g.plane_off, off.data(), sizeof(int) * (nzp + 1), cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.plane_g, pg.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.plane_pos, pp.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.zslot, zslot.data(), sizeof(int) * nr3, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.plane_iz, plane_iz.data(), sizeof(int) * nzp, cudaMemcpyHostToDevice));
+  double2** tws[3] = {&g.tw1, &g.tw2, &g.tw3};
+  for (int a = 0; a < 3; ++a) {
+    int n = h->ax[a].n;
+    std::vector<double2> t(n);
+    for (int k = 0; k < n; ++k) {
+      double ang = 2.0 * M_PI * (double)k / (double)n;
+      t[k] = make_double2(std::cos(ang), std::sin(ang));
+    }
+    CUW_TRY(cudaMalloc(tws[a], sizeof(double2) * n));
+    CUW_TRY(cudaMemcpy(*tws[a], t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+  }
+  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(double2));
+  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(double2));
+  CUW_TRY(cudaFuncSetAttribute(k_gtor_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+  CUW_TRY(cudaFuncSetAttribute(k_rtog_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+  CUW_TRY(cudaFuncSetAttribute(k_zcol_v, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  return CUW_OK;
+}
+
+// out = FFT_RTOG[ V * FFT_GTOR[psi] ] (+ 1/2 G^2 psi + bucket psi when add_kinetic)
+int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
+  const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
+  const size_t npl = (size_t)nr1 * nr2;
+  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(double2));
+  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(double2));
+  const int tp = plane_threads((int)npl);
+  const int tz = plane_threads(nr3 * kTX);
+  AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
+  const double scale = 1.0 / ((double)nr1 * nr2 * nr3);
+  Device& g = h->g;
+  for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
+    const int nb = std::min(h->batch, h->d.nbh - b0);
+    k_gtor_plane<<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
+                                                                   g.plane_pos, g.grid, h->nzp, a1, a2, g.tw1,
+                                                                   g.tw2);
+    CUW_LAUNCH_CHECK("k_gtor_plane");
+    const int nxb = (nr1 + kTX - 1) / kTX;
+    k_zcol_v<<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(g.grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
+                                                             scale);
+    CUW_LAUNCH_CHECK("k_zcol_v");
+    k_rtog_plane<<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(g.grid, h->nzp, g.plane_off, g.plane_g,
+                                                                   g.plane_pos, out, psi, h->ldg, b0, g.g2,
+                                                                   g.bucket, add_kinetic ? 1 : 0, a1, a2,
+                                                                   g.tw1, g.tw2);
+    CUW_LAUNCH_CHECK("k_rtog_plane");
+  }
+  return CUW_OK;
+}
+
+}  // namespace cuw

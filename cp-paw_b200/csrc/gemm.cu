@@ -1,0 +1,845 @@
+// Complex FP64 contractions of the WAVES path on the FP64 tensor cores
+// (mma.sync m8n8k4 f64), with the projector functions generated in the tile
+// loaders instead of being stored.
+//
+// Reference routines and the contraction each kernel replaces:
+//   k_proj      WAVES_PROJECTIONS (src/paw_waves1.f90:5746-5905):
+//               PROJ(b,p) = Omega sum_G conj(PRO(G,p)) psi(G,b)      [split-K]
+//   k_addpro    WAVES_ADDPRO (src/paw_waves1.f90:5908-6067):
+//               psi(G,b) += sum_p PRO(G,p) C(p,b)
+//               with the epilogues of WAVES$HPSI (:4793-4916), WAVES_OPSI
+//               (:5043-5096), the mass scaling of WAVES$ORTHOGONALIZE
+//               (src/paw_waves2.f90:140-162) and WAVES$PROPAGATE (:6575-6583)
+//   k_gram      PLANEWAVE$SCALARPRODUCT ' '/'='/'-' (src/paw_fft.f90:2344-2422)
+//               as used by WAVES_OVERLAP (src/paw_waves2.f90:761-853) and the
+//               projector sums of WAVES_1COVERLAP (:856-1022)         [split-K]
+//   k_addx      WAVES_ADDOPSI (src/paw_waves2.f90:547-615), WAVES_ADDOPROJ
+//               (:687-758) and the PSI update of WAVES_GRAMSCHMIDT (:2131-2136)
+//   k_force     WAVES_DEDPRO + WAVES_PROFORCE (src/paw_waves1.f90:5694-5743,
+//               6112-6234) fused: the (NGL,NPRO) array DEDPRO is never stored.
+//
+// PRO(G,p) = Y_lm(G) P_ln(|G|) (-i)^l exp(-iG.R_a)   (WAVES_EXPANDPRO :6070-6109)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "cuwaves_internal.cuh"
+
+namespace cuw {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 8, LDS = 12, NT = 256;
+
+// ---------------------------------------------------------------------------
+// warp-level complex MMA over one BK slice held in shared memory:
+// As[m][k], Bs[n][k] (real and imaginary parts separately).
+// Warp (wm, wn) in a 2x4 layout owns a 32x16 block: 4 x 2 tiles of 8x8.
+// conjA: use conj(A).
+// ---------------------------------------------------------------------------
+struct Acc {
+  double r[4][2][2];
+  double i[4][2][2];
+  __device__ void zero() {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        r[a][b][0] = r[a][b][1] = 0.0;
+        i[a][b][0] = i[a][b][1] = 0.0;
+      }
+  }
+};
+
+template <bool CONJA>
+__device__ __forceinline__ void mma_slice(Acc& acc, const double (*Ar)[LDS], const double (*Ai)[LDS],
+                                          const double (*Br)[LDS], const double (*Bi)[LDS], int wm, int wn,
+                                          int lane) {
+  const int r8 = lane >> 2, c4 = lane & 3;
+#pragma unroll
+  for (int ks = 0; ks < BK / 4; ++ks) {
+    double ar[4], ai[4], nai[4], br[2], bi[2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      ar[mi] = Ar[wm * 32 + mi * 8 + r8][ks * 4 + c4];
+      double t = Ai[wm * 32 + mi * 8 + r8][ks * 4 + c4];
+      ai[mi] = CONJA ? -t : t;
+      nai[mi] = -ai[mi];
+    }
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni) {
+      br[ni] = Br[wn * 16 + ni * 8 + r8][ks * 4 + c4];
+      bi[ni] = Bi[wn * 16 + ni * 8 + r8][ks * 4 + c4];
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        dmma(acc.r[mi][ni], ar[mi], br[ni]);
+        dmma(acc.r[mi][ni], nai[mi], bi[ni]);
+        dmma(acc.i[mi][ni], ar[mi], bi[ni]);
+        dmma(acc.i[mi][ni], ai[mi], br[ni]);
+      }
+  }
+}
+
+// coordinates of accumulator element (mi, ni, e) of this lane
+__device__ __forceinline__ void acc_mn(int wm, int wn, int lane, int mi, int ni, int e, int& m, int& n) {
+  m = wm * 32 + mi * 8 + (lane >> 2);
+  n = wn * 16 + ni * 8 + 2 * (lane & 3) + e;
+}
+
+// PRO(g,p) generated from the tables
+__device__ __forceinline__ double2 gen_pro(int g, int ngl, const ProDesc& d, const double* __restrict__ ylm,
+                                           const double* __restrict__ pro, const double2* __restrict__ eigr) {
+  double s = ylm[(size_t)g + (size_t)ngl * d.lm] * pro[(size_t)g + (size_t)ngl * d.ibare];
+  double2 e = cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]);
+  return make_double2(s * e.x, s * e.y);
+}
+
+// ---------------------------------------------------------------------------
+// EIGR(g,a) = exp(-i G.R_a)   (PLANEWAVE_STRUCTUREFACTOR, src/paw_fft.f90:1597-1695)
+// ---------------------------------------------------------------------------
+__global__ void k_eigr(const double* __restrict__ gx, const double* __restrict__ gy, const double* __restrict__ gz,
+                       const double* __restrict__ r, int ngl, int nat, double2* __restrict__ eigr) {
+  const int a = blockIdx.y;
+  const double rx = r[3 * a], ry = r[3 * a + 1], rz = r[3 * a + 2];
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngl; g += gridDim.x * blockDim.x) {
+    double ph = gx[g] * rx + gy[g] * ry + gz[g] * rz;
+    double s, c;
+    sincos(ph, &s, &c);
+    eigr[(size_t)g + (size_t)ngl * a] = make_double2(c, -s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Projections: part[z][b + nbh*p] = sum_{g in split z} conj(PRO(g,p)) X(g,b)
+// for one or two operands X (psiA -> part, psiB -> part + stride).
+// M = bands (blockIdx.y), N = projectors (blockIdx.x), K = g (blockIdx.z).
+// ---------------------------------------------------------------------------
+template <bool DUAL>
+__global__ void __launch_bounds__(NT) k_proj(const double2* __restrict__ psiA, const double2* __restrict__ psiB,
+                                             int ldg, int ngl, int nbh, int npro, int kchunk,
+                                             const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+                                             const double* __restrict__ pro, const double2* __restrict__ eigr,
+                                             double2* __restrict__ part, size_t dual_stride) {
+  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS];
+  __shared__ double A2r[DUAL ? BM : 1][LDS], A2i[DUAL ? BM : 1][LDS];
+  __shared__ ProDesc sd[BN];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+  const int kbeg = blockIdx.z * kchunk, kend = min(ngl, kbeg + kchunk);
+  if (tid < BN) {
+    int p = n0 + tid;
+    sd[tid] = p < npro ? pdesc[p] : ProDesc{0, 0, 0, 0};
+  }
+  Acc acc, acc2;
+  acc.zero();
+  if (DUAL) acc2.zero();
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    __syncthreads();
+    // A tiles: X(g, b) -> As[b][g], coalesced along g
+    for (int i = tid; i < BM * BK; i += NT) {
+      int kk = i % BK, mm = i / BK;
+      int g = k0 + kk, b = m0 + mm;
+      double2 x = make_double2(0.0, 0.0), y = x;
+      if (g < kend && b < nbh) {
+        x = psiA[(size_t)g + (size_t)ldg * b];
+        if (DUAL) y = psiB[(size_t)g + (size_t)ldg * b];
+      }
+      Ar[mm][kk] = x.x;
+      Ai[mm][kk] = x.y;
+      if (DUAL) {
+        A2r[mm][kk] = y.x;
+        A2i[mm][kk] = y.y;
+      }
+    }
+    // B tile: conj(PRO(g, p)) -> Bs[p][g]
+    for (int i = tid; i < BN * BK; i += NT) {
+      int kk = i % BK, nn = i / BK;
+      int g = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (g < kend && n0 + nn < npro) v = gen_pro(g, ngl, sd[nn], ylm, pro, eigr);
+      Br[nn][kk] = v.x;
+      Bi[nn][kk] = -v.y;
+    }
+    __syncthreads();
+    mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
+    if (DUAL) mma_slice<false>(acc2, A2r, A2i, Br, Bi, wm, wn, lane);
+  }
+  double2* out = part + (size_t)blockIdx.z * nbh * npro;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int m, n;
+        acc_mn(wm, wn, lane, mi, ni, e, m, n);
+        int b = m0 + m, p = n0 + n;
+        if (b < nbh && p < npro) {
+          out[(size_t)b + (size_t)nbh * p] = make_double2(acc.r[mi][ni][e], acc.i[mi][ni][e]);
+          if (DUAL) out[dual_stride + (size_t)b + (size_t)nbh * p] = make_double2(acc2.r[mi][ni][e], acc2.i[mi][ni][e]);
+        }
+      }
+}
+
+// out[i] = scale * sum_z part[z*stride + i]   (deterministic order)
+__global__ void k_reduce_parts(const double2* __restrict__ part, int nz, size_t stride, size_t n, double scale,
+                               double2* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 s = make_double2(0.0, 0.0);
+    for (int z = 0; z < nz; ++z) {
+      double2 v = part[(size_t)z * stride + i];
+      s.x += v.x;
+      s.y += v.y;
+    }
+    out[i] = make_double2(s.x * scale, s.y * scale);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ADDPRO with the step epilogues.  M = g (blockIdx.x), N = bands (blockIdx.y),
+// K = projectors.  Operands C1 (hproj) and/or C2 (oproj), layout (NBH, NPRO).
+// mode ADDPRO_HPSI : hpsi += PRO*C1                     (vpsi already in hpsi)
+// mode ADDPRO_OPSI : opsi  = (psi0 + PRO*C2) * dt^2/((1+annee) m_G)
+// mode ADDPRO_FUSED: both, then psim = a1 psi0 + a2 psim + a3/m_G hpsi
+// ---------------------------------------------------------------------------
+struct StepCoef {
+  double a1, a2, a3, oscale;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(NT) k_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi,
+                                               const double2* __restrict__ psi0, double2* __restrict__ psim,
+                                               const double* __restrict__ mpsi, int ldg, int ngl, int nbh,
+                                               int npro, const double2* __restrict__ c1,
+                                               const double2* __restrict__ c2, const ProDesc* __restrict__ pdesc,
+                                               const double* __restrict__ ylm, const double* __restrict__ pro,
+                                               const double2* __restrict__ eigr, StepCoef sc) {
+  constexpr bool USE_H = (MODE != ADDPRO_OPSI);
+  constexpr bool USE_O = (MODE != ADDPRO_HPSI);
+  __shared__ double Ar[BM][LDS], Ai[BM][LDS];
+  __shared__ double Br[USE_H ? BN : 1][LDS], Bi[USE_H ? BN : 1][LDS];
+  __shared__ double B2r[USE_O ? BN : 1][LDS], B2i[USE_O ? BN : 1][LDS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  Acc acc, acc2;
+  if (USE_H) acc.zero();
+  if (USE_O) acc2.zero();
+  for (int k0 = 0; k0 < npro; k0 += BK) {
+    __syncthreads();
+    // A tile: PRO(g, p) -> As[g][p]
+    for (int i = tid; i < BM * BK; i += NT) {
+      int mm = i % BM, kk = i / BM;
+      int g = m0 + mm, p = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (g < ngl && p < npro) v = gen_pro(g, ngl, pdesc[p], ylm, pro, eigr);
+      Ar[mm][kk] = v.x;
+      Ai[mm][kk] = v.y;
+    }
+    // B tiles: C(p, b) stored C[b + nbh*p] -> Bs[b][p]
+    for (int i = tid; i < BN * BK; i += NT) {
+      int nn = i % BN, kk = i / BN;
+      int b = n0 + nn, p = k0 + kk;
+      bool ok = (b < nbh && p < npro);
+      if (USE_H) {
+        double2 v = ok ? c1[(size_t)b + (size_t)nbh * p] : make_double2(0.0, 0.0);
+        Br[nn][kk] = v.x;
+        Bi[nn][kk] = v.y;
+      }
+      if (USE_O) {
+        double2 v = ok ? c2[(size_t)b + (size_t)nbh * p] : make_double2(0.0, 0.0);
+        B2r[nn][kk] = v.x;
+        B2i[nn][kk] = v.y;
+      }
+    }
+    __syncthreads();
+    if (USE_H) mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
+    if (USE_O) mma_slice<false>(acc2, Ar, Ai, B2r, B2i, wm, wn, lane);
+  }
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int m, n;
+        acc_mn(wm, wn, lane, mi, ni, e, m, n);
+        int g = m0 + m, b = n0 + n;
+        if (g >= ngl || b >= nbh) continue;
+        size_t k = (size_t)g + (size_t)ldg * b;
+        double2 hv = make_double2(0.0, 0.0);
+        if (USE_H) {
+          hv = hpsi[k];
+          hv.x += acc.r[mi][ni][e];
+          hv.y += acc.i[mi][ni][e];
+          hpsi[k] = hv;
+        }
+        if (USE_O) {
+          double2 p0 = psi0[k];
+          double s = sc.oscale / mpsi[g];
+          opsi[k] = make_double2((p0.x + acc2.r[mi][ni][e]) * s, (p0.y + acc2.i[mi][ni][e]) * s);
+        }
+        if (MODE == ADDPRO_FUSED) {
+          double2 p0 = psi0[k], pm = psim[k];
+          double a3 = sc.a3 / mpsi[g];
+          psim[k] = make_double2(sc.a1 * p0.x + sc.a2 * pm.x + a3 * hv.x, sc.a1 * p0.y + sc.a2 * pm.y + a3 * hv.y);
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Gram products for one or more (X, Y) pairs (blockIdx.z = split*npair + pair):
+//   T1(m,n) = sum_k conj(X(k,m)) Y(k,n)
+//   T2(m,n) = sum_k X(k,m) Y(-k,n)    (MINUS: k -> minusg[k])
+//           = sum_k X(k,m) Y(k,n)     (otherwise)
+// Layout: element (k, m) of an operand at ptr[k*sk + m*sm].
+// part[((split*npair + pair)*2 + t)*nm*nn + m + nm*n]
+// ---------------------------------------------------------------------------
+struct GramArgs {
+  GramPair pair[3];
+  int npair;
+  int nk, nm, nn;   // K, M, N extents
+  size_t sk, sm;    // strides of k and of m/n
+  int kchunk;
+};
+
+template <bool MINUS>
+__global__ void __launch_bounds__(NT) k_gram(GramArgs a, const int* __restrict__ minusg, double2* __restrict__ part) {
+  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS], B2r[BN][LDS], B2i[BN][LDS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  const int pair = blockIdx.z % a.npair, split = blockIdx.z / a.npair;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const double2* X = a.pair[pair].x;
+  const double2* Y = a.pair[pair].y;
+  const int kbeg = split * a.kchunk, kend = min(a.nk, kbeg + a.kchunk);
+  Acc t1, t2;
+  t1.zero();
+  t2.zero();
+  const bool kfast = (a.sk == 1);
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    __syncthreads();
+    for (int i = tid; i < BM * BK; i += NT) {
+      int kk, mm;
+      if (kfast) { kk = i % BK; mm = i / BK; }
+      else { mm = i % BM; kk = i / BM; }
+      int k = k0 + kk;
+      bool okk = k < kend;
+      double2 x = make_double2(0.0, 0.0);
+      if (okk && m0 + mm < a.nm) x = X[(size_t)k * a.sk + (size_t)(m0 + mm) * a.sm];
+      Ar[mm][kk] = x.x;
+      Ai[mm][kk] = x.y;
+      double2 y = make_double2(0.0, 0.0), y2 = y;
+      if (okk && n0 + mm < a.nn) {
+        y = Y[(size_t)k * a.sk + (size_t)(n0 + mm) * a.sm];
+        if (MINUS) y2 = Y[(size_t)minusg[k] * a.sk + (size_t)(n0 + mm) * a.sm];
+        else y2 = y;
+      }
+      Br[mm][kk] = y.x;
+      Bi[mm][kk] = y.y;
+      B2r[mm][kk] = y2.x;
+      B2i[mm][kk] = y2.y;
+    }
+    __syncthreads();
+    mma_slice<true>(t1, Ar, Ai, Br, Bi, wm, wn, lane);
+    mma_slice<false>(t2, Ar, Ai, B2r, B2i, wm, wn, lane);
+  }
+  const size_t mn = (size_t)a.nm * a.nn;
+  double2* o1 = part + ((size_t)blockIdx.z * 2 + 0) * mn;
+  double2* o2 = part + ((size_t)blockIdx.z * 2 + 1) * mn;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int m, n;
+        acc_mn(wm, wn, lane, mi, ni, e, m, n);
+        m += m0;
+        n += n0;
+        if (m < a.nm && n < a.nn) {
+          o1[(size_t)m + (size_t)a.nm * n] = make_double2(t1.r[mi][ni][e], t1.i[mi][ni][e]);
+          o2[(size_t)m + (size_t)a.nm * n] = make_double2(t2.r[mi][ni][e], t2.i[mi][ni][e]);
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// out(m, n) += sum_k X(k... see below
+//   ADDOPSI form (XMINUS): out(g,n) += sum_k X(g,k) L1(k,n) + conj(X(-g,k)) L2(k,n)
+//   ADDOPROJ form       : out(p,n) += sum_k X(p,k) L1(k,n) + conj(X(p,k)) L2(k,n)
+// X element (m, k) at X[m*sxm + k*sxk]; out element (m, n) at out[m*som + n*son];
+// L1/L2 (nk, nn) column-major complex.  M = blockIdx.x, N = blockIdx.y.
+// ---------------------------------------------------------------------------
+struct AddXArgs {
+  double2* out;
+  const double2* x;
+  const double2* l1;
+  const double2* l2;
+  int nm, nn, nk;
+  size_t sxm, sxk, som, son;
+};
+
+template <bool XMINUS>
+__global__ void __launch_bounds__(NT) k_addx(AddXArgs a, const int* __restrict__ minusg) {
+  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  Acc acc;
+  acc.zero();
+  const int ktot = 2 * a.nk;
+  const bool mfast = (a.sxm == 1);
+  for (int k0 = 0; k0 < ktot; k0 += BK) {
+    __syncthreads();
+    for (int i = tid; i < BM * BK; i += NT) {
+      int mm, kk;
+      if (mfast) { mm = i % BM; kk = i / BM; }
+      else { kk = i % BK; mm = i / BK; }
+      int kg = k0 + kk, m = m0 + mm;
+      double2 v = make_double2(0.0, 0.0);
+      if (m < a.nm && kg < ktot) {
+        if (kg < a.nk) v = a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
+        else {
+          int k = kg - a.nk;
+          int mm2 = XMINUS ? minusg[m] : m;
+          v = cconj(a.x[(size_t)mm2 * a.sxm + (size_t)k * a.sxk]);
+        }
+      }
+      Ar[mm][kk] = v.x;
+      Ai[mm][kk] = v.y;
+    }
+    for (int i = tid; i < BN * BK; i += NT) {
+      int kk = i % BK, nn = i / BK;
+      int kg = k0 + kk, n = n0 + nn;
+      double2 v = make_double2(0.0, 0.0);
+      if (n < a.nn && kg < ktot) {
+        if (kg < a.nk) v = a.l1[(size_t)kg + (size_t)a.nk * n];
+        else v = a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
+      }
+      Br[nn][kk] = v.x;
+      Bi[nn][kk] = v.y;
+    }
+    __syncthreads();
+    mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
+  }
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int m, n;
+        acc_mn(wm, wn, lane, mi, ni, e, m, n);
+        m += m0;
+        n += n0;
+        if (m < a.nm && n < a.nn) {
+          size_t k = (size_t)m * a.som + (size_t)n * a.son;
+          double2 o = a.out[k];
+          a.out[k] = make_double2(o.x + acc.r[mi][ni][e], o.y + acc.i[mi][ni][e]);
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Forces: D(g,p) = sum_b psi0(g,b) conj(E(b,p)); then per projector
+//   f_p += Re[ i P(g) (-i)^l EIGR(g) conj(D(g,p)) ] Y_lm(g) G(g)
+// reduced over the g tile into fpart[blockIdx.x][p][3].  M = g, N = p, K = b.
+// The TINV symmetrisation of WAVES_DEDPRO (src/paw_waves1.f90:5730-5738)
+// cancels in this sum (c(-G) = -conj(c(G)) for c = i Y P (-i)^l EIGR over the
+// full sphere), so it is not applied.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_force(const double2* __restrict__ psi0, int ldg, int ngl, int nbh, int npro,
+                                              const double2* __restrict__ ded, const ProDesc* __restrict__ pdesc,
+                                              const double* __restrict__ ylm, const double* __restrict__ pro,
+                                              const double2* __restrict__ eigr, const double* __restrict__ gx,
+                                              const double* __restrict__ gy, const double* __restrict__ gz,
+                                              double* __restrict__ fpart) {
+  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS];
+  __shared__ double fred[BN][3][4];  // per projector, per warp row-group (wm) x 2 halves
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  Acc acc;
+  acc.zero();
+  for (int k0 = 0; k0 < nbh; k0 += BK) {
+    __syncthreads();
+    for (int i = tid; i < BM * BK; i += NT) {
+      int mm = i % BM, kk = i / BM;
+      int g = m0 + mm, b = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (g < ngl && b < nbh) v = psi0[(size_t)g + (size_t)ldg * b];
+      Ar[mm][kk] = v.x;
+      Ai[mm][kk] = v.y;
+    }
+    for (int i = tid; i < BN * BK; i += NT) {
+      int kk = i % BK, nn = i / BK;
+      int b = k0 + kk, p = n0 + nn;
+      double2 v = make_double2(0.0, 0.0);
+      if (b < nbh && p < npro) v = ded[(size_t)b + (size_t)nbh * p];
+      Br[nn][kk] = v.x;
+      Bi[nn][kk] = -v.y;
+    }
+    __syncthreads();
+    mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
+  }
+  // epilogue: per (g, p) contribution, reduced over g
+  double f[2][2][3];
+#pragma unroll
+  for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) f[ni][e][0] = f[ni][e][1] = f[ni][e][2] = 0.0;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int m, n;
+        acc_mn(wm, wn, lane, mi, ni, e, m, n);
+        int g = m0 + m, p = n0 + n;
+        if (g < ngl && p < npro) {
+          ProDesc d = pdesc[p];
+          double pr = pro[(size_t)g + (size_t)ngl * d.ibare];
+          double y = ylm[(size_t)g + (size_t)ngl * d.lm];
+          // cw = i * P * (-i)^l * EIGR
+          double2 cw = cmul(make_double2(0.0, pr), cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]));
+          double2 dd = make_double2(acc.r[mi][ni][e], acc.i[mi][ni][e]);
+          double sv = (cw.x * dd.x + cw.y * dd.y) * y;  // Re(cw * conj(dd)) * Y
+          f[ni][e][0] += sv * gx[g];
+          f[ni][e][1] += sv * gy[g];
+          f[ni][e][2] += sv * gz[g];
+        }
+      }
+  // reduce across the 8 lanes that share (lane & 3) (different g rows)
+#pragma unroll
+  for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double v = f[ni][e][c];
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        f[ni][e][c] = v;
+      }
+  __syncthreads();
+  if (lane < 4) {
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int n = wn * 16 + ni * 8 + 2 * lane + e;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fred[n][c][wm] = f[ni][e][c];
+      }
+  }
+  __syncthreads();
+  for (int i = tid; i < BN * 3; i += NT) {
+    int n = i / 3, c = i % 3;
+    int p = n0 + n;
+    if (p < npro) fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = fred[n][c][0] + fred[n][c][1];
+  }
+}
+
+// force(c, iat) = 2 * Omega * sum over g tiles and projectors of atom iat
+__global__ void k_force_final(const double* __restrict__ fpart, int ntile, int npro, const int* __restrict__ ipro0,
+                              const int* __restrict__ nlmn, int nat, double gweight, double* __restrict__ force) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * nat) return;
+  int a = i / 3, c = i % 3;
+  double s = 0.0;
+  for (int p = ipro0[a]; p < ipro0[a] + nlmn[a]; ++p)
+    for (int t = 0; t < ntile; ++t) s += fpart[((size_t)t * npro + p) * 3 + c];
+  force[i] = gweight * 2.0 * s;
+}
+
+// ---------------------------------------------------------------------------
+// one-centre operations on projections (small, one thread per output)
+// HPROJ = DH * PROJ per atom (WAVES_HPROJ, src/paw_waves1.f90:4919-4973)
+// OPROJ = DO * PROJ per atom (WAVES_OPROJ, src/paw_waves2.f90:497-544)
+// ---------------------------------------------------------------------------
+__global__ void k_hproj(const double2* __restrict__ proj, const double2* __restrict__ dh, int lmnxx,
+                        const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0,
+                        const int* __restrict__ nlmn, int nbh, int npro, double2* __restrict__ out) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)nbh * npro) return;
+  int b = (int)(i % nbh), p = (int)(i / nbh);
+  int a = pdesc[p].iat;
+  int l1 = p - ipro0[a];
+  double2 s = make_double2(0.0, 0.0);
+  for (int l2 = 0; l2 < nlmn[a]; ++l2) {
+    double2 d = dh[(size_t)l1 + (size_t)lmnxx * (l2 + (size_t)lmnxx * a)];
+    double2 c = proj[(size_t)b + (size_t)nbh * (ipro0[a] + l2)];
+    s = cadd(s, cmul(d, c));
+  }
+  out[i] = s;
+}
+
+__global__ void k_oproj(const double2* __restrict__ proj, const double* __restrict__ dover, int lnxx,
+                        const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0, const int* __restrict__ isp,
+                        const int* __restrict__ lnofp, const int* __restrict__ mofp, const int* __restrict__ lmn0ln,
+                        const int* __restrict__ lox, int maxln, int nbh, int npro, double2* __restrict__ out) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)nbh * npro) return;
+  int b = (int)(i % nbh), p = (int)(i / nbh);
+  int a = pdesc[p].iat, s = isp[a];
+  int ln1 = lnofp[p], m = mofp[p], l1 = pdesc[p].l;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int ln2 = 0; ln2 < maxln; ++ln2) {
+    int l2 = lox[s * maxln + ln2];
+    if (l2 < 0) break;
+    if (l2 != l1) continue;
+    double dv = dover[(size_t)ln1 + (size_t)lnxx * (ln2 + (size_t)lnxx * s)];
+    double2 c = proj[(size_t)b + (size_t)nbh * (ipro0[a] + lmn0ln[s * maxln + ln2] + m)];
+    acc.x += dv * c.x;
+    acc.y += dv * c.y;
+  }
+  out[i] = acc;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+static int ensure_part(Handle* h, size_t bytes) {
+  if (bytes <= h->g.part_bytes) return CUW_OK;
+  if (h->g.part) cudaFree(h->g.part);
+  h->g.part = nullptr;
+  h->g.part_bytes = 0;
+  CUW_TRY(cudaMalloc(&h->g.part, bytes));
+  h->g.part_bytes = bytes;
+  return CUW_OK;
+}
+
+static int choose_split(Handle* h, int tiles, int nk, int minchunk) {
+  int want = std::max(1, ceil_div(2 * h->nsm, std::max(1, tiles)));
+  int maxs = std::max(1, ceil_div(nk, minchunk));
+  return std::min(want, maxs);
+}
+
+int eigr_compute(Handle* h, const double* r_dev) {
+  dim3 grid(std::min(ceil_div(h->d.ngl, 256), 64), h->d.nat);
+  k_eigr<<<grid, 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz, r_dev, h->d.ngl, h->d.nat, h->g.eigr);
+  CUW_LAUNCH_CHECK("k_eigr");
+  return CUW_OK;
+}
+
+// projA = Omega <p|psiA>, projB likewise when psiB != null; uses h->g.eigr
+int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* psiB, double2* projB) {
+  const int nbh = h->d.nbh, npro = h->npro, ngl = h->d.ngl;
+  const int tn = ceil_div(npro, BN), tm = ceil_div(nbh, BM);
+  int ks = choose_split(h, tn * tm, ngl, 256);
+  int kchunk = ceil_div(ceil_div(ngl, ks), BK) * BK;
+  ks = ceil_div(ngl, kchunk);
+  const size_t one = (size_t)ks * nbh * npro;
+  const bool dual = (psiB != nullptr);
+  CUW_RET(ensure_part(h, sizeof(double2) * one * (dual ? 2 : 1)));
+  dim3 grid(tn, tm, ks);
+  if (dual)
+    k_proj<true><<<grid, NT, 0, h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
+                                             h->g.pro, h->g.eigr, h->g.part, one);
+  else
+    k_proj<false><<<grid, NT, 0, h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
+                                              h->g.pro, h->g.eigr, h->g.part, 0);
+  CUW_LAUNCH_CHECK("k_proj");
+  const size_t n = (size_t)nbh * npro;
+  const int rb = std::min(ceil_div((int)std::min<size_t>(n, 1 << 30), 256), 4 * h->nsm);
+  k_reduce_parts<<<rb, 256, 0, h->stream>>>(h->g.part, ks, n, n, h->gweight, projA);
+  CUW_LAUNCH_CHECK("k_reduce_parts");
+  if (dual) {
+    k_reduce_parts<<<rb, 256, 0, h->stream>>>(h->g.part + one, ks, n, n, h->gweight, projB);
+    CUW_LAUNCH_CHECK("k_reduce_parts");
+  }
+  return CUW_OK;
+}
+
+int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
+  const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
+  dim3 grid(ceil_div(ngl, BM), ceil_div(nbh, BN));
+  StepCoef sc;
+  sc.a1 = 2.0 / (1.0 + h->annee);  // WAVES$PROPAGATE (src/paw_waves1.f90:6557-6566)
+  sc.a2 = 1.0 - sc.a1;
+  sc.a3 = -h->delt * h->delt / (1.0 + h->annee);
+  sc.oscale = h->delt * h->delt / (1.0 + h->annee);  // src/paw_waves2.f90:148-156
+  Device& g = h->g;
+  switch (mode) {
+    case ADDPRO_HPSI:
+      k_addpro<ADDPRO_HPSI><<<grid, NT, 0, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
+                                                         hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
+      break;
+    case ADDPRO_OPSI:
+      k_addpro<ADDPRO_OPSI><<<grid, NT, 0, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
+                                                         hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
+      break;
+    default:
+      k_addpro<ADDPRO_FUSED><<<grid, NT, 0, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh,
+                                                          npro, hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
+  }
+  CUW_LAUNCH_CHECK("k_addpro");
+  return CUW_OK;
+}
+
+// tables of the projector map on the device (Device::t_*)
+struct TabView {
+  const int *ipro0, *nlmn, *isp, *lnofp, *mofp, *lmn0ln, *lox;
+};
+static TabView tables(Handle* h) {
+  const Device& g = h->g;
+  return TabView{g.t_ipro0, g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox};
+}
+
+int hproj_compute(Handle* h, const double2* proj, double2* out) {
+  TabView t = tables(h);
+  size_t n = (size_t)h->d.nbh * h->npro;
+  k_hproj<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(proj, h->g.dh, h->lmnxx, h->g.pdesc, t.ipro0, t.nlmn,
+                                                              h->d.nbh, h->npro, out);
+  CUW_LAUNCH_CHECK("k_hproj");
+  return CUW_OK;
+}
+
+int oproj_compute(Handle* h, const double2* proj, double2* out) {
+  TabView t = tables(h);
+  size_t n = (size_t)h->d.nbh * h->npro;
+  k_oproj<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(proj, h->g.dover, h->lnxx, h->g.pdesc, t.ipro0, t.isp,
+                                                              t.lnofp, t.mofp, t.lmn0ln, t.lox, CUW_MAXLN, h->d.nbh,
+                                                              h->npro, out);
+  CUW_LAUNCH_CHECK("k_oproj");
+  return CUW_OK;
+}
+
+// T(pair) products into h->g.part region [pair][t][nbh*nbh] after reduction at
+// offset `dst` (complex), scaled by `scale`.
+static int gram_run(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
+                    double scale, double2* dst) {
+  GramArgs a;
+  for (int i = 0; i < npair; ++i) a.pair[i] = pairs[i];
+  a.npair = npair;
+  a.nk = nk;
+  a.nm = nm;
+  a.nn = nm;
+  a.sk = sk;
+  a.sm = sm;
+  const int tiles = ceil_div(nm, BM) * ceil_div(nm, BN) * npair;
+  int ks = choose_split(h, tiles, nk, 128);
+  a.kchunk = ceil_div(ceil_div(nk, ks), BK) * BK;
+  ks = ceil_div(nk, a.kchunk);
+  const size_t mn = (size_t)nm * nm;
+  CUW_RET(ensure_part(h, sizeof(double2) * mn * 2 * npair * ks));
+  dim3 grid(ceil_div(nm, BN), ceil_div(nm, BM), ks * npair);
+  if (minus) k_gram<true><<<grid, NT, 0, h->stream>>>(a, h->g.minusg, h->g.part);
+  else k_gram<false><<<grid, NT, 0, h->stream>>>(a, h->g.minusg, h->g.part);
+  CUW_LAUNCH_CHECK("k_gram");
+  // reduce over splits: layout part[(split*npair+pair)*2+t] -> dst[(pair*2+t)]
+  const size_t n = mn * 2 * npair;
+  const int rb = std::min(ceil_div((int)n, 256), 4 * h->nsm);
+  k_reduce_parts<<<rb, 256, 0, h->stream>>>(h->g.part, ks, n, n, scale, dst);
+  CUW_LAUNCH_CHECK("k_reduce_parts");
+  return CUW_OK;
+}
+
+int gram_planewave(Handle* h, const GramPair* pairs, int npair, double2* dst) {
+  return gram_run(h, pairs, npair, true, h->d.ngl, h->d.nbh, 1, (size_t)h->ldg, h->gweight, dst);
+}
+
+int gram_projections(Handle* h, const GramPair* pairs, int npair, double2* dst) {
+  return gram_run(h, pairs, npair, false, h->npro, h->d.nbh, (size_t)h->d.nbh, 1, 1.0, dst);
+}
+
+int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* l1, const double2* l2) {
+  AddXArgs a;
+  a.out = psibar;
+  a.x = opsi;
+  a.l1 = l1;
+  a.l2 = l2;
+  a.nm = h->d.ngl;
+  a.nn = h->d.nbh;
+  a.nk = h->d.nbh;
+  a.sxm = 1;
+  a.sxk = (size_t)h->ldg;
+  a.som = 1;
+  a.son = (size_t)h->ldg;
+  dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
+  k_addx<true><<<grid, NT, 0, h->stream>>>(a, h->g.minusg);
+  CUW_LAUNCH_CHECK("k_addx");
+  return CUW_OK;
+}
+
+int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* l1, const double2* l2) {
+  AddXArgs a;
+  a.out = proj;
+  a.x = oproj;
+  a.l1 = l1;
+  a.l2 = l2;
+  a.nm = h->npro;
+  a.nn = h->d.nbh;
+  a.nk = h->d.nbh;
+  a.sxm = (size_t)h->d.nbh;  // X(m=p, k=b) at b + nbh*p
+  a.sxk = 1;
+  a.som = (size_t)h->d.nbh;  // out(m=p, n=b) at b + nbh*p
+  a.son = 1;
+  dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
+  k_addx<false><<<grid, NT, 0, h->stream>>>(a, h->g.minusg);
+  CUW_LAUNCH_CHECK("k_addx");
+  return CUW_OK;
+}
+
+int force_gemm(Handle* h, const double2* ded, double* force_dev) {
+  const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
+  const int tm = ceil_div(ngl, BM), tn = ceil_div(npro, BN);
+  CUW_RET(ensure_part(h, sizeof(double) * 3 * (size_t)tm * npro));
+  double* fpart = reinterpret_cast<double*>(h->g.part);
+  k_force<<<dim3(tm, tn), NT, 0, h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro,
+                                              h->g.eigr, h->g.gx, h->g.gy, h->g.gz, fpart);
+  CUW_LAUNCH_CHECK("k_force");
+  TabView t = tables(h);
+  k_force_final<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(fpart, tm, npro, t.ipro0, t.nlmn, h->d.nat,
+                                                                     h->gweight, force_dev);
+  CUW_LAUNCH_CHECK("k_force_final");
+  return CUW_OK;
+}
+
+int small_tables_setup(Handle* h) {
+  Device& t = h->g;
+  const int nat = h->d.nat, nsp = h->d.nsp, npro = h->npro;
+  std::vector<int> ipro0(nat), nlmn(nat), lnofp(npro), mofp(npro), lmn0ln(nsp * CUW_MAXLN, 0),
+      lox(nsp * CUW_MAXLN, -1);
+  for (int s = 0; s < nsp; ++s) {
+    int off = 0;
+    for (int ln = 0; ln < h->d.lnx[s]; ++ln) {
+      lox[s * CUW_MAXLN + ln] = h->d.lox[s][ln];
+      lmn0ln[s * CUW_MAXLN + ln] = off;
+      off += 2 * h->d.lox[s][ln] + 1;
+    }
+  }
+  for (int a = 0; a < nat; ++a) {
+    ipro0[a] = h->ipro0[a];
+    nlmn[a] = h->lmnx[h->isp[a]];
+    int s = h->isp[a], p = ipro0[a];
+    for (int ln = 0; ln < h->d.lnx[s]; ++ln)
+      for (int m = 0; m < 2 * h->d.lox[s][ln] + 1; ++m) {
+        lnofp[p] = ln;
+        mofp[p] = m;
+        ++p;
+      }
+  }
+  auto up = [&](int** dst, const std::vector<int>& src) -> int {
+    if (*dst) cudaFree(*dst);
+    CUW_TRY(cudaMalloc(dst, sizeof(int) * std::max<size_t>(1, src.size())));
+    CUW_TRY(cudaMemcpy(*dst, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice));
+    return CUW_OK;
+  };
+  CUW_RET(up(&t.t_ipro0, ipro0));
+  CUW_RET(up(&t.t_nlmn, nlmn));
+  CUW_RET(up(&t.t_isp, h->isp));
+  CUW_RET(up(&t.t_lnofp, lnofp));
+  CUW_RET(up(&t.t_mofp, mofp));
+  CUW_RET(up(&t.t_lmn0ln, lmn0ln));
+  CUW_RET(up(&t.t_lox, lox));
+  return CUW_OK;
+}
+
+}  // namespace cuw

@@ -1,0 +1,669 @@
+// Orthonormality constraint of the CP step on the device (FP64 throughout).
+//
+//   k_unravel       WAVES_OVERLAP + WAVES_1COVERLAP unravelling of super wave
+//                   functions into real NB x NB matrices (src/paw_waves2.f90:797-848,
+//                   999-1020) and their sum (:262-289)
+//   k_lambda_init   symmetrisation and occupation scaling of RLAM0 (:295-303, 352-359)
+//   k_jacobi        eigenpairs of 0.5*(CHIPSI+CHIPSI^T) (LIB$DIAGR8 -> DSYEV,
+//                   src/paw_library.f90:572-631, 1555-1620) by parallel cyclic Jacobi
+//   k_ortho_x       the iteration of WAVES_ORTHO_X (src/paw_waves2.f90:1844-2022)
+//                   as one thread-block cluster; every wait is a hardware cluster
+//                   barrier and the loop is bounded by max_iter
+//   k_lambda12      LAMBDA1/LAMBDA2 of WAVES_ADDOPSI (:583-595)
+//   k_switch_lambda Lagrange extrapolation of WAVES$SWITCH (:2249-2296)
+//   k_ortho_y       WAVES_ORTHO_Y_C (:1025-1338) for WAVES_GRAMSCHMIDT (:2025-2177);
+//                   its matrices are real at the Gamma point, so it runs in real
+//                   arithmetic
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "cuwaves_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace cuw {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// T[pair][t] (NBH x NBH complex) -> real (NB x NB) matrices
+//   pw : plane-wave part, t=0 <X|Y>, t=1 sum X(G) Y(-G)     (both times Omega)
+//   oc : one-centre part, t=0 CMAT1, t=1 CMAT2
+// ---------------------------------------------------------------------------
+__global__ void k_unravel(const double2* __restrict__ pw, const double2* __restrict__ oc, int npair, int nbh,
+                          double* __restrict__ out0, double* __restrict__ out1, double* __restrict__ out2) {
+  const int nb = 2 * nbh;
+  const size_t mn = (size_t)nbh * nbh;
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int pair = blockIdx.y;
+  if (idx >= (int)mn || pair >= npair) return;
+  int i = idx % nbh, j = idx / nbh;
+  double* out = pair == 0 ? out0 : (pair == 1 ? out1 : out2);
+  double2 t1 = pw[(pair * 2 + 0) * mn + idx], t2 = pw[(pair * 2 + 1) * mn + idx];
+  double2 c1 = oc[(pair * 2 + 0) * mn + idx], c2 = oc[(pair * 2 + 1) * mn + idx];
+  // one-centre: cs1 = 0.5(C1+C2), cs2 = 0.5(C1-C2)
+  double cs1r = 0.5 * (c1.x + c2.x), cs1i = 0.5 * (c1.y + c2.y);
+  double cs2r = 0.5 * (c1.x - c2.x), cs2i = 0.5 * (c1.y - c2.y);
+  double re = 0.5 * t1.x, im = 0.5 * t1.y, re2 = 0.5 * t2.x, im2 = 0.5 * t2.y;
+  const int a = 2 * i, b = 2 * j;
+  out[a + (size_t)nb * b] = cs1r + (re + re2);
+  out[a + (size_t)nb * (b + 1)] = cs1i + (im + im2);
+  out[(a + 1) + (size_t)nb * b] = -cs2i + (-im + im2);
+  out[(a + 1) + (size_t)nb * (b + 1)] = cs2r + (re - re2);
+}
+
+// Lambda = sym(RLAM0) scaled by 0.5*f_i/(f_i+f_j); real part
+__global__ void k_lambda_init(const double2* __restrict__ rlam0, const double* __restrict__ occ, int nb,
+                              double* __restrict__ lam) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nb * nb) return;
+  int i = idx % nb, j = idx / nb;
+  double2 a = rlam0[i + (size_t)nb * j];
+  double2 v = a;
+  if (i != j) {
+    double2 b = rlam0[j + (size_t)nb * i];
+    v = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+  }
+  double oi = occ[i], oj = occ[j];
+  if (oi + oj < 1e-12) oj = 1e-12;
+  lam[idx] = v.x * 0.5 * oi / (oi + oj);
+}
+
+// 0.5*(A + A^T)
+__global__ void k_symmetrize(const double* __restrict__ a, int n, double* __restrict__ s) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  int i = idx % n, j = idx / n;
+  s[idx] = 0.5 * (a[i + (size_t)n * j] + a[j + (size_t)n * i]);
+}
+
+// ---------------------------------------------------------------------------
+// Parallel cyclic Jacobi on a symmetric n x n matrix (n even), one CTA.
+// A is held packed (upper triangle) in shared memory, V (eigenvectors) in
+// shared memory when it fits, else in global memory.  Rounds follow the
+// round-robin tournament ordering so that the n/2 rotations of a round act on
+// disjoint index pairs; each 2x2 block [P,Q] is updated by one thread as
+// J_P^T A[P,Q] J_Q.  At most max_sweeps sweeps.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pk(int i, int j) { return i <= j ? (j * (j + 1)) / 2 + i : (i * (i + 1)) / 2 + j; }
+
+__global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in, int n, double* __restrict__ u_out,
+                                                 double* __restrict__ e_out, double* __restrict__ vglob,
+                                                 int v_in_smem, int max_sweeps, int* __restrict__ info) {
+  extern __shared__ double sm[];
+  const int np = n / 2;
+  double* A = sm;                                        // packed n(n+1)/2
+  double* rc = A + (size_t)n * (n + 1) / 2;              // np cosines
+  double* rs = rc + np;                                  // np sines
+  int* pp = reinterpret_cast<int*>(rs + np);             // np
+  int* pq = pp + np;                                     // np
+  int* flag = pq + np;                                   // 1
+  double* V = v_in_smem ? reinterpret_cast<double*>(flag + 2) : vglob;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int j = tid; j < n; j += nt)
+    for (int i = 0; i <= j; ++i) A[pk(i, j)] = s_in[i + (size_t)n * j];
+  for (size_t k = tid; k < (size_t)n * n; k += nt) {
+    int i = (int)(k % n), j = (int)(k / n);
+    V[k] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    if (tid == 0) *flag = 0;
+    __syncthreads();
+    for (int r = 0; r < n - 1; ++r) {
+      if (tid < np) {
+        int a, b;
+        if (tid == 0) { a = n - 1; b = r; }
+        else { a = (r + tid) % (n - 1); b = (r - tid + (n - 1)) % (n - 1); }
+        int p = min(a, b), q = max(a, b);
+        pp[tid] = p;
+        pq[tid] = q;
+        double apq = A[pk(p, q)], app = A[pk(p, p)], aqq = A[pk(q, q)];
+        double c = 1.0, s = 0.0;
+        if (apq != 0.0 && fabs(apq) > 1e-17 * sqrt(fabs(app * aqq))) {
+          double theta = (aqq - app) / (2.0 * apq);
+          double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          c = 1.0 / sqrt(t * t + 1.0);
+          s = t * c;
+          *flag = 1;
+        }
+        rc[tid] = c;
+        rs[tid] = s;
+      }
+      __syncthreads();
+      // 2x2 blocks between pair P and pair Q (P <= Q), np*(np+1)/2 of them
+      const int nblk = np * (np + 1) / 2;
+      for (int k = tid; k < nblk; k += nt) {
+        // decode k -> (P, Q) with P <= Q
+        int Q = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+        while ((Q + 1) * (Q + 2) / 2 <= k) ++Q;
+        while (Q * (Q + 1) / 2 > k) --Q;
+        int P = k - Q * (Q + 1) / 2;
+        int p = pp[P], q = pq[P], r2 = pp[Q], s2 = pq[Q];
+        double cP = rc[P], sP = rs[P], cQ = rc[Q], sQ = rs[Q];
+        if (P == Q) {
+          double apq = A[pk(p, q)], app = A[pk(p, p)], aqq = A[pk(q, q)];
+          if (sP != 0.0) {
+            double t = sP / cP;
+            A[pk(p, p)] = app - t * apq;
+            A[pk(q, q)] = aqq + t * apq;
+            A[pk(p, q)] = 0.0;
+          }
+        } else {
+          double a_pr = A[pk(p, r2)], a_ps = A[pk(p, s2)], a_qr = A[pk(q, r2)], a_qs = A[pk(q, s2)];
+          // rows: J_P^T
+          double b_pr = cP * a_pr - sP * a_qr, b_ps = cP * a_ps - sP * a_qs;
+          double b_qr = sP * a_pr + cP * a_qr, b_qs = sP * a_ps + cP * a_qs;
+          // columns: J_Q
+          A[pk(p, r2)] = cQ * b_pr - sQ * b_ps;
+          A[pk(p, s2)] = sQ * b_pr + cQ * b_ps;
+          A[pk(q, r2)] = cQ * b_qr - sQ * b_qs;
+          A[pk(q, s2)] = sQ * b_qr + cQ * b_qs;
+        }
+      }
+      // V <- V J
+      for (int k = tid; k < np * n; k += nt) {
+        int P = k / n, row = k % n;
+        double c = rc[P], s = rs[P];
+        if (s == 0.0) continue;
+        int p = pp[P], q = pq[P];
+        double vp = V[row + (size_t)n * p], vq = V[row + (size_t)n * q];
+        V[row + (size_t)n * p] = c * vp - s * vq;
+        V[row + (size_t)n * q] = s * vp + c * vq;
+      }
+      __syncthreads();
+    }
+    if (*flag == 0) break;
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += nt) e_out[i] = A[pk(i, i)];
+  for (size_t k = tid; k < (size_t)n * n; k += nt) u_out[k] = V[k];
+  if (tid == 0) info[0] = sweep;
+}
+
+// ---------------------------------------------------------------------------
+// WAVES_ORTHO_X iteration as one cluster of CS CTAs.  All matrices are real,
+// column-major n x n, in global memory (L2 resident).  The output tile of every
+// product is split into a TRxTC grid of CTA tiles.
+// ---------------------------------------------------------------------------
+struct OrthoArgs {
+  int n;
+  const double* chichi;
+  const double* psipsi;
+  const double* chipsi;
+  const double* u;
+  const double* e;
+  const double* occ;
+  double* lam;    // in: start, out: result
+  double* lam2;   // second buffer
+  double* haux;
+  double* gamn;
+  double* w;
+  double* maxpart;
+  int* status;    // [0] status, [1] iterations
+  int max_iter;
+  double eps;
+};
+
+// C(tile) = op(A) * op(B); op = transpose when tA / tB
+__device__ void gemm_tile(const double* __restrict__ A, bool tA, const double* __restrict__ B, bool tB, int n,
+                          int i0, int i1, int j0, int j1, double* __restrict__ C, double* smA, double* smB,
+                          int kc) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tm = i1 - i0, tn = j1 - j0;
+  const int tx = tid % 16, ty = tid / 16;  // 16 x (nt/16)
+  const int nty = nt / 16;
+  constexpr int MAXO = 16;
+  double acc[MAXO];
+#pragma unroll
+  for (int o = 0; o < MAXO; ++o) acc[o] = 0.0;
+  for (int k0 = 0; k0 < n; k0 += kc) {
+    const int kk = min(kc, n - k0);
+    for (int t = tid; t < tm * kk; t += nt) {
+      int ii = t % tm, k = t / tm;
+      int gi = i0 + ii, gk = k0 + k;
+      smA[ii + tm * k] = tA ? A[gk + (size_t)n * gi] : A[gi + (size_t)n * gk];
+    }
+    for (int t = tid; t < tn * kk; t += nt) {
+      int k = t % kk, jj = t / kk;
+      int gj = j0 + jj, gk = k0 + k;
+      smB[k + kc * jj] = tB ? B[gj + (size_t)n * gk] : B[gk + (size_t)n * gj];
+    }
+    __syncthreads();
+    int o = 0;
+    for (int ii = ty; ii < tm; ii += nty)
+      for (int jj = tx; jj < tn; jj += 16) {
+        double s = acc[o];
+        for (int k = 0; k < kk; ++k) s += smA[ii + tm * k] * smB[k + kc * jj];
+        acc[o] = s;
+        ++o;
+      }
+    __syncthreads();
+  }
+  int o = 0;
+  for (int ii = ty; ii < tm; ii += nty)
+    for (int jj = tx; jj < tn; jj += 16) {
+      C[(i0 + ii) + (size_t)n * (j0 + jj)] = acc[o];
+      ++o;
+    }
+}
+
+__device__ __forceinline__ void csync() {
+  __threadfence();
+  cg::this_cluster().sync();
+}
+
+__global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
+  extern __shared__ double sm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int cs = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int n = a.n;
+  // CTA tile grid: tr x tc
+  int tr = 1;
+  while (tr * tr < cs) tr *= 2;
+  int tc = cs / tr;
+  if (tr * tc != cs) { tr = cs; tc = 1; }
+  const int ri = rank / tc, ci = rank % tc;
+  const int rs = (n + tr - 1) / tr, csz = (n + tc - 1) / tc;
+  const int i0 = min(n, ri * rs), i1 = min(n, i0 + rs);
+  const int j0 = min(n, ci * csz), j1 = min(n, j0 + csz);
+  const int kc = 32;
+  double* smA = sm;
+  double* smB = sm + (size_t)rs * kc;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double* lam = a.lam;
+  double* lamn = a.lam2;
+  int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
+  for (int iter = 1; iter <= a.max_iter; ++iter) {
+    // HAUX = CHICHI * LAMBDA + 2 CHIPSI
+    gemm_tile(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
+      int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
+      a.haux[i + (size_t)n * j] += 2.0 * a.chipsi[i + (size_t)n * j];
+    }
+    csync();
+    // GAMN = LAMBDA^T * HAUX
+    gemm_tile(lam, true, a.haux, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
+    csync();
+    // W = 0.5 (GAMN + GAMN^T) + PSIPSI - 1 ; tile max
+    double mx = 0.0;
+    for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
+      int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
+      // the reference writes GAMN(J,I)=GAMN(I,J)=0.5*(GAMN(I,J)+GAMN(J,I))+PSIPSI(I,J) for J>=I
+      int lo = min(i, j), hi = max(i, j);
+      double v = 0.5 * (a.gamn[lo + (size_t)n * hi] + a.gamn[hi + (size_t)n * lo]) + a.psipsi[lo + (size_t)n * hi];
+      if (i == j) v -= 1.0;
+      a.w[i + (size_t)n * j] = v;
+      mx = fmax(mx, fabs(v));
+      if (v != v) mx = INFINITY;
+    }
+    // block max
+    __shared__ double red[256];
+    red[tid] = mx;
+    __syncthreads();
+    for (int s = nt / 2; s > 0; s >>= 1) {
+      if (tid < s) red[tid] = fmax(red[tid], red[tid + s]);
+      __syncthreads();
+    }
+    if (tid == 0) a.maxpart[rank] = red[0];
+    csync();
+    double digam = 0.0;
+    for (int r = 0; r < cs; ++r) digam = fmax(digam, a.maxpart[r]);
+    if (digam < a.eps) {
+      status = CUW_OK;
+      iters = iter;
+      break;
+    }
+    if (!(digam <= 1e200)) {
+      status = CUW_ERR_DIVERGED;
+      iters = iter;
+      break;
+    }
+    // HAUX = U^T W
+    gemm_tile(a.u, true, a.w, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    csync();
+    // GAMN = (HAUX U) / (e_i + e_j)
+    gemm_tile(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
+    for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
+      int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
+      a.gamn[i + (size_t)n * j] /= (a.e[i] + a.e[j]);
+    }
+    csync();
+    // HAUX = U GAMN
+    gemm_tile(a.u, false, a.gamn, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    csync();
+    // W = HAUX U^T
+    gemm_tile(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB, kc);
+    csync();
+    // LAMBDA(I,J) -= 2 OCCI/(OCCI+OCCJ) W(I,J); then occupation symmetrisation
+    const double dsmall = 1e-12;
+    for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
+      int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
+      double oi = a.occ[i], oj = a.occ[j];
+      double v;
+      if (oi < oj) {
+        double occj = oj + dsmall, occi = oi + dsmall;
+        double lji = lam[j + (size_t)n * i] - 2.0 * occj / (occj + occi) * a.w[j + (size_t)n * i];
+        v = lji * (oi + dsmall) / (oj + dsmall);
+      } else {
+        double occi = oi + dsmall, occj = oj + dsmall;
+        v = lam[i + (size_t)n * j] - 2.0 * occi / (occi + occj) * a.w[i + (size_t)n * j];
+      }
+      lamn[i + (size_t)n * j] = v;
+    }
+    csync();
+    double* tmp = lam;
+    lam = lamn;
+    lamn = tmp;
+  }
+  // result into a.lam
+  if (lam != a.lam) {
+    for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
+      int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
+      a.lam[i + (size_t)n * j] = lam[i + (size_t)n * j];
+    }
+  }
+  if (rank == 0 && tid == 0) {
+    a.status[0] = status;
+    a.status[1] = iters;
+  }
+  csync();
+}
+
+// LAMBDA1/LAMBDA2 (NBH x NBH complex) from real LAMBDA (NB x NB)
+__global__ void k_lambda12(const double* __restrict__ lam, int nb, int nbh, double2* __restrict__ l1,
+                           double2* __restrict__ l2) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nbh * nbh) return;
+  int ibh1 = idx % nbh, ibh2 = idx / nbh;
+  int a = 2 * ibh1, b = 2 * ibh1 + 1, c = 2 * ibh2, d = 2 * ibh2 + 1;
+  // CSVAR1 = L(a,c) + i L(a,d); CSVAR2 = i L(b,c) - L(b,d)
+  double2 s1 = make_double2(lam[a + (size_t)nb * c], lam[a + (size_t)nb * d]);
+  double2 s2 = make_double2(-lam[b + (size_t)nb * d], lam[b + (size_t)nb * c]);
+  l1[idx] = make_double2(0.5 * (s1.x - s2.x), 0.5 * (s1.y - s2.y));
+  l2[idx] = make_double2(0.5 * (s1.x + s2.x), 0.5 * (s1.y + s2.y));
+}
+
+// X (real NB x NB) -> X1, X2 of WAVES_GRAMSCHMIDT (src/paw_waves2.f90:2109-2128)
+__global__ void k_fold_x(const double* __restrict__ x, int nb, int nbh, double2* __restrict__ x1,
+                         double2* __restrict__ x2) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nbh * nbh) return;
+  int ibh1 = idx % nbh, ibh2 = idx / nbh;
+  int a = 2 * ibh1, b = 2 * ibh1 + 1, c = 2 * ibh2, d = 2 * ibh2 + 1;
+  // CSVAR1 = X11 + i X12 ; CSVAR2 = -i X21 + X22
+  double2 s1 = make_double2(x[a + (size_t)nb * c], x[a + (size_t)nb * d]);
+  double2 s2 = make_double2(x[b + (size_t)nb * d], -x[b + (size_t)nb * c]);
+  x1[idx] = make_double2(0.5 * (s1.x + s2.x), 0.5 * (s1.y + s2.y));
+  x2[idx] = make_double2(0.5 * (s1.x - s2.x), 0.5 * (s1.y - s2.y));
+}
+
+// real LAMBDA -> RLAM0 (complex), and the extrapolation of WAVES$SWITCH
+__global__ void k_store_lambda(const double* __restrict__ lam, int n, double2* __restrict__ rlam0) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < n * n) rlam0[idx] = make_double2(lam[idx], 0.0);
+}
+
+__global__ void k_switch_lambda(double2* __restrict__ rlam0, double2* __restrict__ rlamm, int n, int have_m) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  double2 l0 = rlam0[idx];
+  if (!have_m) {
+    rlamm[idx] = l0;  // NLAMBDA=1: RLAMP = RLAM0, RLAMM = RLAM0
+  } else {
+    double2 lm = rlamm[idx];
+    rlam0[idx] = make_double2(2.0 * l0.x - lm.x, 2.0 * l0.y - lm.y);
+    rlamm[idx] = l0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// WAVES_ORTHO_Y_C with PHIPHI = CHIPHI = CHICHI = S (real) and MAP = identity.
+// One CTA; A, B, C, ALPHA, X, WORK are n x n in global memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, int n, double* A, double* B, double* C,
+                                                  double* AL, double* X, double* W, int* __restrict__ status) {
+  __shared__ double z[1024];
+  __shared__ double zn;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const double r8small = 1e-10;
+  const size_t nn = (size_t)n * n;
+  for (size_t k = tid; k < nn; k += nt) {
+    int i = (int)(k % n), j = (int)(k / n);
+    A[k] = s[k] - (i == j ? 1.0 : 0.0);
+    B[k] = s[k];
+    C[k] = s[k];
+    X[k] = 0.0;
+    AL[k] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  auto I = [n](int i, int j) { return (size_t)i + (size_t)n * j; };
+  for (int nu = 0; nu < n; ++nu) {
+    const int nn0 = nu;
+    if (tid == 0) {
+      double bnn = B[I(nn0, nn0)], ann = A[I(nn0, nn0)], cnn = C[I(nn0, nn0)];
+      double svar = bnn * bnn - ann * cnn;
+      double svar1 = -bnn, zz;
+      if (svar >= 0.0) {
+        double svar2 = sqrt(svar);
+        zz = (svar1 * svar2 >= 0.0) ? svar1 - svar2 : svar1 + svar2;
+      } else {
+        zz = svar1;
+      }
+      zz = zz / (cnn + r8small);
+      if (svar != svar) status[0] = CUW_ERR_NAN;
+      zn = zz;
+    }
+    __syncthreads();
+    const double zz = zn;
+    for (int i = tid; i < n; i += nt) X[I(i, nn0)] += AL[I(i, nn0)] * zz;
+    for (int j = tid; j < n; j += nt) A[I(nn0, j)] += zz * B[I(nn0, j)];
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) A[I(i, nn0)] += B[I(nn0, i)] * zz;
+    __syncthreads();
+    if (tid == 0) A[I(nn0, nn0)] += zz * C[I(nn0, nn0)] * zz;
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) B[I(i, nn0)] += C[I(i, nn0)] * zz;
+    __syncthreads();
+    // orthogonalise higher phis to this phi
+    const double bnn = B[I(nn0, nn0)] + r8small;
+    for (int i = tid; i < n; i += nt) z[i] = (i > nu) ? -(A[I(i, nn0)] / bnn) : 0.0;
+    __syncthreads();
+    const double cnn = C[I(nn0, nn0)];
+    for (size_t k = tid; k < nn; k += nt) {
+      int i = (int)(k % n), j = (int)(k / n);
+      if (j > nu) X[k] += AL[I(i, nn0)] * z[j];
+      double add = 0.0;
+      if (i > nu) add += z[i] * B[I(nn0, j)];
+      if (j > nu) add += B[I(nn0, i)] * z[j];
+      if (i > nu && j > nu) add += z[i] * cnn * z[j];
+      A[k] += add;
+    }
+    __syncthreads();
+    for (size_t k = tid; k < nn; k += nt) {
+      int i = (int)(k % n), j = (int)(k / n);
+      if (j > nu) B[k] += C[I(i, nn0)] * z[j];
+    }
+    __syncthreads();
+    // orthogonalise higher chis to this phi
+    const double bnn2 = B[I(nn0, nn0)] + r8small;
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) z[i] = (i > nu) ? -(B[I(i, nn0)] / bnn2) : 0.0;
+    __syncthreads();
+    for (size_t k = tid; k < nn; k += nt) {
+      int i = (int)(k % n), j = (int)(k / n);
+      if (j > nu) AL[k] += AL[I(i, nn0)] * z[j];
+    }
+    __syncthreads();
+    for (size_t k = tid; k < nn; k += nt) {
+      int i = (int)(k % n), j = (int)(k / n);
+      if (i > nu) B[k] += z[i] * B[I(nn0, j)];
+    }
+    const double cnn2 = C[I(nn0, nn0)];
+    for (size_t k = tid; k < nn; k += nt) {
+      int i = (int)(k % n), j = (int)(k / n);
+      double wv = 0.0;
+      if (i > nu) wv += z[i] * C[I(nn0, j)];
+      if (j > nu) wv += C[I(i, nn0)] * z[j];
+      if (i > nu && j > nu) wv += z[i] * cnn2 * z[j];
+      W[k] = wv;
+    }
+    __syncthreads();
+    for (size_t k = tid; k < nn; k += nt) C[k] += W[k];
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+
+int unravel_run(Handle* h, const double2* pw, const double2* oc, int npair, double* o0, double* o1, double* o2) {
+  const int nbh = h->d.nbh;
+  dim3 grid(ceil_div(nbh * nbh, 256), npair);
+  k_unravel<<<grid, 256, 0, h->stream>>>(pw, oc, npair, nbh, o0, o1, o2);
+  CUW_LAUNCH_CHECK("k_unravel");
+  return CUW_OK;
+}
+
+int lambda12_run(Handle* h, const double* lam_real, double2* l1, double2* l2) {
+  const int nbh = h->d.nbh;
+  k_lambda12<<<ceil_div(nbh * nbh, 256), 256, 0, h->stream>>>(lam_real, h->d.nb, nbh, l1, l2);
+  CUW_LAUNCH_CHECK("k_lambda12");
+  return CUW_OK;
+}
+
+int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
+  const int n = h->d.nb;
+  const size_t packed = (size_t)n * (n + 1) / 2;
+  const size_t base = sizeof(double) * (packed + n) + sizeof(int) * (n + 2) + 16;
+  size_t smem = base + sizeof(double) * (size_t)n * n;
+  int v_in_smem = 1;
+  if (smem > 220 * 1024) {
+    v_in_smem = 0;
+    smem = base;
+  }
+  if (smem > 220 * 1024) return h->fail(CUW_ERR_UNSUPPORTED, "NB too large for the on-chip eigensolver");
+  CUW_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int* info = reinterpret_cast<int*>(h->g.ostatus) + 4;
+  k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, 40, info);
+  CUW_LAUNCH_CHECK("k_jacobi");
+  return CUW_OK;
+}
+
+// Full WAVES_ORTHO_X: matrices mat (PSIPSI), omat (CHIPSI), oomat (CHICHI) and
+// the starting lambda are in h->g.{mat,omat,oomat,lam}.
+int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
+  const int n = h->d.nb;
+  Device& g = h->g;
+  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.gamn);
+  CUW_LAUNCH_CHECK("k_symmetrize");
+  CUW_RET(jacobi_run(h, g.gamn, g.u, g.eig));
+  OrthoArgs a;
+  a.n = n;
+  a.chichi = g.oomat;
+  a.psipsi = g.mat;
+  a.chipsi = g.omat;
+  a.u = g.u;
+  a.e = g.eig;
+  a.occ = g.occ;
+  a.lam = g.lam;
+  a.lam2 = g.lam2;
+  a.haux = g.haux;
+  a.gamn = g.gamn;
+  a.w = g.work;
+  a.maxpart = g.maxpart;
+  a.status = g.ostatus;
+  a.max_iter = max_iter;
+  a.eps = eps;
+  // cluster of 16 CTAs (non-portable size) or 8
+  int cs = 16;
+  int rs_max = (n + 3) / 4;  // tile rows for 16 CTAs (4x4)
+  size_t smem = sizeof(double) * 32 * (size_t)(2 * (rs_max + 8));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  cfg.blockDim = dim3(256);
+  cfg.stream = h->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  cudaError_t e = cudaFuncSetAttribute(k_ortho_x, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) cs = 8;
+  for (; cs >= 1; cs /= 2) {
+    int tr = 1;
+    while (tr * tr < cs) tr *= 2;
+    int tc = cs / tr;
+    if (tr * tc != cs) { tr = cs; tc = 1; }
+    int rs = (n + tr - 1) / tr, csz = (n + tc - 1) / tc;
+    smem = sizeof(double) * 32 * (size_t)(rs + csz);
+    if (smem > 48 * 1024) {
+      if (cudaFuncSetAttribute(k_ortho_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+    }
+    cfg.gridDim = dim3(cs);
+    cfg.dynamicSmemBytes = smem;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    e = cudaLaunchKernelEx(&cfg, k_ortho_x, a);
+    if (e == cudaSuccess) break;
+    cudaGetLastError();
+  }
+  if (cs < 1) return h->fail(CUW_ERR_CUDA, "k_ortho_x: no cluster size could be launched");
+  int st[2] = {0, 0};
+  CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  if (iters) *iters = st[1];
+  if (st[0] == CUW_ERR_NOT_CONVERGED) return h->fail(st[0], "LOOP FOR ORTHOGONALIZATION IS NOT CONVERGED");
+  if (st[0] == CUW_ERR_DIVERGED) return h->fail(st[0], "ITERATION LOOP FOR ORTHOGONALIZATION IS ABOUT TO DIVERGE");
+  if (st[0] != CUW_OK) return h->fail(st[0], "orthogonalisation failed");
+  return CUW_OK;
+}
+
+int lambda_init_run(Handle* h) {
+  const int n = h->d.nb;
+  k_lambda_init<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(h->g.rlam0, h->g.occ, n, h->g.lam);
+  CUW_LAUNCH_CHECK("k_lambda_init");
+  return CUW_OK;
+}
+
+int store_lambda_run(Handle* h) {
+  const int n = h->d.nb;
+  k_store_lambda<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(h->g.lam, n, h->g.rlam0);
+  CUW_LAUNCH_CHECK("k_store_lambda");
+  return CUW_OK;
+}
+
+int switch_lambda_run(Handle* h) {
+  const int n = h->d.nb;
+  k_switch_lambda<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(h->g.rlam0, h->g.rlamm, n, h->have_rlamm ? 1 : 0);
+  CUW_LAUNCH_CHECK("k_switch_lambda");
+  h->have_rlamm = true;
+  return CUW_OK;
+}
+
+int ortho_y_run(Handle* h, const double* s, double* x) {
+  const int n = h->d.nb;
+  Device& g = h->g;
+  CUW_TRY(cudaMemsetAsync(g.ostatus, 0, sizeof(int) * 2, h->stream));
+  k_ortho_y<<<1, 1024, 0, h->stream>>>(s, n, g.haux, g.gamn, g.work, g.lam2, x, g.maxpart, g.ostatus);
+  CUW_LAUNCH_CHECK("k_ortho_y");
+  return CUW_OK;
+}
+
+int fold_x_run(Handle* h, const double* x, double2* x1, double2* x2) {
+  const int nbh = h->d.nbh;
+  k_fold_x<<<ceil_div(nbh * nbh, 256), 256, 0, h->stream>>>(x, h->d.nb, nbh, x1, x2);
+  CUW_LAUNCH_CHECK("k_fold_x");
+  return CUW_OK;
+}
+
+}  // namespace cuw

@@ -1,0 +1,226 @@
+"""Parity of the CUDA engine with the CPU oracle, through the C ABI.
+
+Each test puts the engine and the oracle into the same state (same seeded
+inputs, the same orthonormal PSI0/PSIM, PROJ and RLAM0), runs one WAVES
+operation on both and compares.  Tolerances (FP64 path):
+  H|psi>, PSI after a step       relative 1e-10 / 1e-9 of max|.|
+  energies                       1e-8 Ha absolute
+  forces                         1e-6 Ha/bohr absolute
+  PROJ, overlaps                 relative 1e-10
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import cuwaves  # noqa: E402
+from cuwaves import CUW_HPSI, CUW_OPSI, CUW_PSI0, CUW_PSIM, WavesError, systems  # noqa: E402
+
+CASES = {
+    "Si8-20Ry": lambda: systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry"),
+    "Si8": lambda: systems.named_system("Si8"),
+    "Si2mol": lambda: systems.molecule_box("Si2", box=12.0, epw_psi_ry=15.0, grid=(20, 20, 20)),
+    "H2O2": lambda: systems.water_box(2, box=10.0, lattice=(2, 1, 1), epw_psi_ry=25.0, grid=(32, 32, 32)),
+    "Si6": lambda: systems.si_small(6, epw_psi_ry=15.0, grid=(20, 20, 20)),
+}
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def inputs_cache():
+    return {}
+
+
+def make_pair(name, oracle, cache):
+    if name not in cache:
+        cache[name] = systems.build_inputs(CASES[name]())
+    inp = cache[name]
+    gpu = cuwaves.open_waves(inp).setup().initialize()
+    cpu = oracle.open_oracle(inp).setup()
+    sync_state(gpu, cpu)
+    return inp, gpu, cpu
+
+
+def sync_state(src, dst):
+    """Copy PSI0, PSIM, PROJ and RLAM0 from src to dst."""
+    dst.upload_psi(CUW_PSI0, src.download_psi(CUW_PSI0))
+    dst.upload_psi(CUW_PSIM, src.download_psi(CUW_PSIM))
+    dst.set_proj(src.get_proj())
+    dst.set_rlam0(src.get_rlam0())
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry"])
+def test_roundtrip_bits(name, oracle, inputs_cache):
+    inp, gpu, _ = make_pair(name, oracle, inputs_cache)
+    rng = np.random.default_rng(5)
+    x = rng.normal(size=(inp["nbh"], inp["ngl"])) + 1j * rng.normal(size=(inp["nbh"], inp["ngl"]))
+    for which in (CUW_PSI0, CUW_PSIM, CUW_HPSI, CUW_OPSI):
+        gpu.upload_psi(which, x)
+        assert np.array_equal(gpu.download_psi(which), x)
+    p = rng.normal(size=(gpu.npro, inp["nbh"])) + 1j * rng.normal(size=(gpu.npro, inp["nbh"]))
+    gpu.set_proj(p)
+    assert np.array_equal(gpu.get_proj(), p)
+    r = rng.normal(size=(inp["nb"], inp["nb"])) + 0j
+    gpu.set_rlam0(r)
+    assert np.array_equal(gpu.get_rlam0(), r)
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "H2O2", "Si6"])
+def test_fft_identity(name, oracle, inputs_cache):
+    """With V=1 and DH=0, H|psi> = psi + 1/2 G^2 psi: the FFT pair is an identity."""
+    inp, gpu, _ = make_pair(name, oracle, inputs_cache)
+    gpu.set_potential(np.ones_like(inp["v"]))
+    gpu.set_dh(np.zeros_like(inp["dh"]))
+    gpu.hpsi()
+    psi = gpu.download_psi(CUW_PSI0)
+    want = psi * (1.0 + 0.5 * inp["g2"][None, :])
+    assert rel(gpu.download_psi(CUW_HPSI), want) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "Si8", "H2O2", "Si2mol", "Si6"])
+def test_projections(name, oracle, inputs_cache):
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    gpu.projections()
+    cpu.projections()
+    assert rel(gpu.get_proj(), cpu.get_proj()) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "Si8", "H2O2", "Si2mol", "Si6"])
+def test_hpsi(name, oracle, inputs_cache):
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    gpu.hpsi()
+    cpu.hpsi()
+    assert rel(gpu.download_psi(CUW_HPSI), cpu.download_psi(CUW_HPSI)) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["Si8", "H2O2"])
+def test_energies(name, oracle, inputs_cache):
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    # give PSIM a different value so that the fictitious kinetic energy is nonzero
+    rng = np.random.default_rng(7)
+    pm = gpu.download_psi(CUW_PSI0) * (1 + 1e-3 * rng.normal(size=(inp["nbh"], inp["ngl"])))
+    gpu.upload_psi(CUW_PSIM, pm)
+    cpu.upload_psi(CUW_PSIM, pm)
+    assert abs(gpu.ekin() - cpu.ekin()) < 1e-8
+    eg, vg = gpu.wavekinetic()
+    ec, vc = cpu.wavekinetic()
+    assert abs(eg - ec) < 1e-8 * max(1.0, abs(ec))
+    assert np.abs(vg - vc).max() < 1e-8 * max(1.0, np.abs(vc).max())
+    gpu.hpsi()
+    cpu.hpsi()
+    assert np.abs(gpu.expectation() - cpu.expectation()).max() < 1e-8
+
+
+def test_energies_unequal_occupations(oracle, inputs_cache):
+    """Occupations that differ inside a super wave function exercise the
+    PSI(-G) terms of WAVES_EKIN and WAVES_WAVEKINETIC."""
+    inp, gpu, cpu = make_pair("Si8-20Ry", oracle, inputs_cache)
+    occ = inp["occ"].copy()
+    occ[-3:] = [1.0, 0.5, 0.0]
+    gpu.set_occ(occ)
+    cpu.set_occ(occ)
+    rng = np.random.default_rng(8)
+    pm = gpu.download_psi(CUW_PSI0) * (1 + 1e-3 * rng.normal(size=(inp["nbh"], inp["ngl"])))
+    gpu.upload_psi(CUW_PSIM, pm)
+    cpu.upload_psi(CUW_PSIM, pm)
+    assert abs(gpu.ekin() - cpu.ekin()) < 1e-8
+    assert abs(gpu.wavekinetic()[0] - cpu.wavekinetic()[0]) < 1e-8
+    assert np.abs(gpu.force() - cpu.force()).max() < 1e-6
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "Si8", "H2O2", "Si6"])
+def test_force(name, oracle, inputs_cache):
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    rng = np.random.default_rng(9)
+    lam = rng.normal(size=(inp["nb"], inp["nb"])) * 0.1
+    lam = (lam + lam.T) + 0j
+    gpu.set_rlam0(lam)
+    cpu.set_rlam0(lam)
+    fg, fc = gpu.force(), cpu.force()
+    assert np.abs(fg - fc).max() < 1e-6
+    assert np.abs(fg - fc).max() < 1e-9 * max(1.0, np.abs(fc).max())
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "H2O2"])
+def test_propagate(name, oracle, inputs_cache):
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    gpu.hpsi()
+    cpu.hpsi()
+    gpu.propagate()
+    cpu.propagate()
+    assert rel(gpu.download_psi(CUW_PSIM), cpu.download_psi(CUW_PSIM)) < 1e-10
+    with pytest.raises(WavesError) as e:
+        gpu.propagate()  # HPSI consumed: the reference stops here too
+    assert e.value.code == 3
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "Si8", "H2O2", "Si6"])
+def test_orthogonalize(name, oracle, inputs_cache):
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    for w in (gpu, cpu):
+        w.hpsi()
+        w.propagate()
+    sync_state(gpu, cpu)
+    ig = gpu.orthogonalize()
+    ic = cpu.orthogonalize()
+    assert ig == ic
+    assert rel(gpu.download_psi(CUW_PSIM), cpu.download_psi(CUW_PSIM)) < 1e-9
+    assert rel(gpu.get_proj(), cpu.get_proj()) < 1e-9
+    assert np.abs(gpu.get_rlam0() - cpu.get_rlam0()).max() < 1e-8
+
+
+def test_gramschmidt(oracle, inputs_cache):
+    inp = systems.build_inputs(CASES["Si8-20Ry"]())
+    gpu = cuwaves.open_waves(inp).setup()
+    cpu = oracle.open_oracle(inp).setup()
+    for w in (gpu, cpu):
+        w.gramschmidt(CUW_PSI0, inp["r0"])
+    assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-10
+
+
+@pytest.mark.parametrize("name,nsteps,move", [("Si8-20Ry", 8, False), ("Si8", 5, True), ("H2O2", 5, True)])
+def test_cp_steps(name, nsteps, move, oracle, inputs_cache):
+    """Full CP steps (TIMESTEP order) on both engines, compared step by step."""
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    for step in range(nsteps):
+        og, fg = gpu.cp_step(move_atoms=move)
+        oc, fc = cpu.cp_step(move_atoms=move)
+        assert og[4] == oc[4], f"step {step}: ortho iterations {og[4]} vs {oc[4]}"
+        assert abs(og[0] - oc[0]) < 1e-8, f"step {step}: E {og[0]} vs {oc[0]}"
+        assert abs(og[1] - oc[1]) < 1e-8
+        assert abs(og[2] - oc[2]) < 1e-8
+        assert abs(og[3] - oc[3]) < 1e-8
+        assert np.abs(fg - fc).max() < 1e-6
+    assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-8
+
+
+def test_not_converged_status_and_recovery(oracle, inputs_cache):
+    """A forced non-convergence (max_iter=1) is reported as a status and the
+    handle stays usable (the reference stops the run instead)."""
+    inp, gpu, cpu = make_pair("Si8-20Ry", oracle, inputs_cache)
+    gpu.hpsi()
+    gpu.propagate()
+    with pytest.raises(WavesError) as e:
+        gpu.orthogonalize(max_iter=1, eps=1e-14)
+    assert e.value.code == 4
+    # the context is still usable: a fresh step works
+    gpu2 = cuwaves.open_waves(inp).setup().initialize()
+    out, _ = gpu2.cp_step()
+    assert np.isfinite(out[0])
+
+
+def test_nan_input_detected(oracle, inputs_cache):
+    """A NaN planted in the host input is reported, not propagated silently."""
+    inp = systems.build_inputs(CASES["Si8-20Ry"]())
+    gpu = cuwaves.open_waves(inp).setup()
+    psi = inp["psi"].copy()
+    psi[0, 3] = np.nan
+    gpu.upload_psi(CUW_PSI0, psi)
+    with pytest.raises(WavesError) as e:
+        gpu.gramschmidt(CUW_PSI0, inp["r0"])
+    assert e.value.code == 7
+    gpu2 = cuwaves.open_waves(inp).setup().initialize()
+    assert np.isfinite(gpu2.ekin())

@@ -1,0 +1,184 @@
+"""CPU checks of the oracle and of the host-side index rules (no GPU).
+
+- the MSLNG random-number known answer of the reference
+  (src/paw_generalpurpose.f90:2236-2239: seed 1043618065 after 10000 draws);
+- G-set ordering, MINUSG and grid rules: numpy restatement == C restatement;
+- the oracle's FFT against numpy, its eigensolver against scipy;
+- physical invariants of the oracle's CP dynamics (orthonormality after
+  WAVES$ORTHOGONALIZE, energy conservation of order dt^2);
+- regression against the committed golden fixtures.
+"""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cuwaves import systems
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_mslng_known_answer(oracle):
+    lib = oracle.library()
+    seed = C.c_int(1)
+    for _ in range(10000):
+        lib.orc_mslng(C.byref(seed))
+    assert seed.value == 1043618065
+
+
+@pytest.mark.parametrize("name", ["Si8", "Si64", "H2O32"])
+def test_gset_numpy_equals_oracle(name, oracle):
+    s = systems.named_system(name)
+    gbas, _ = systems.gbass(s.rbas)
+    ig = systems.get_ig(gbas, s.epw_psi)
+    lib = oracle.library()
+    gb = np.asfortranarray(gbas)
+    n = C.c_int()
+    dp = C.POINTER(C.c_double)
+    lib.orc_getig(gb.ctypes.data_as(dp), C.c_double(s.epw_psi), C.byref(n), None)
+    out = np.zeros((n.value, 3), dtype=np.int32)
+    lib.orc_getig(gb.ctypes.data_as(dp), C.c_double(s.epw_psi), C.byref(n), out.ctypes.data_as(C.POINTER(C.c_int)))
+    assert np.array_equal(out, ig)
+    mg = np.zeros(n.value, dtype=np.int32)
+    assert lib.orc_minusg(n.value, out.ctypes.data_as(C.POINTER(C.c_int)), mg.ctypes.data_as(C.POINTER(C.c_int))) == 0
+    assert np.array_equal(mg, systems.minus_g(ig))
+
+
+def test_ngl_and_reference_grids():
+    """NGL and the reference-rule grids of the benchmark systems."""
+    for name, ngl, grid in [("Si8", 2945, (28, 28, 28)), ("Si64", 23847, (56, 56, 56)), ("H2O32", 27633, (56, 56, 56))]:
+        s = systems.named_system(name)
+        gbas, _ = systems.gbass(s.rbas)
+        assert len(systems.get_ig(gbas, s.epw_psi)) == ngl
+        assert systems.reference_grid(s.rbas, 2 * s.epw_psi) == grid
+
+
+def test_fftadjustgrd(oracle):
+    lib = oracle.library()
+    for n in [1, 2, 7, 13, 27, 28, 49, 55, 57, 97, 100, 129]:
+        assert lib.orc_fftadjustgrd(n) == systems.fft_adjust_grid(n)
+
+
+@pytest.mark.parametrize("n", [16, 24, 28, 32, 40, 45, 56, 64, 72, 88, 96])
+def test_fft1d_against_numpy(n, oracle):
+    lib = oracle.library()
+    rng = np.random.default_rng(n)
+    x = rng.normal(size=n) + 1j * rng.normal(size=n)
+    for d in (+1, -1):
+        y = x.copy()
+        lib.orc_fft1d(n, d, y.ctypes.data_as(C.POINTER(C.c_double)))
+        want = np.fft.ifft(x) * n if d > 0 else np.fft.fft(x)
+        assert np.abs(y - want).max() < 1e-12 * np.abs(want).max()
+
+
+def test_eigensolver_against_scipy(oracle):
+    import scipy.linalg
+
+    lib = oracle.library()
+    rng = np.random.default_rng(3)
+    n = 40
+    a = rng.normal(size=(n, n))
+    a = a + a.T
+    e = np.zeros(n)
+    u = np.zeros((n, n))
+    af = np.asfortranarray(a)
+    uf = np.asfortranarray(u)
+    lib.orc_syev(n, af.ctypes.data_as(C.POINTER(C.c_double)), e.ctypes.data_as(C.POINTER(C.c_double)),
+                 uf.ctypes.data_as(C.POINTER(C.c_double)))
+    assert np.abs(np.sort(e) - scipy.linalg.eigvalsh(a)).max() < 1e-12
+    assert np.abs(a @ uf - uf * e[None, :]).max() < 1e-11
+
+
+def test_initializerandom_deterministic(oracle):
+    """WAVES_INITIALIZERANDOM: deterministic stream, envelope exp(-G^2/6)."""
+    lib = oracle.library()
+    s = systems.named_system("Si8")
+    inp = systems.build_inputs(s)
+    g = np.ascontiguousarray(inp["gvec"])
+    out1 = np.zeros((4, inp["ngl"]), dtype=np.complex128)
+    out2 = np.zeros_like(out1)
+    dp = C.POINTER(C.c_double)
+    lib.orc_initializerandom(inp["ngl"], 1, 4, g.ctypes.data_as(dp), out1.ctypes.data_as(dp))
+    lib.orc_initializerandom(inp["ngl"], 1, 4, g.ctypes.data_as(dp), out2.ctypes.data_as(dp))
+    assert np.array_equal(out1, out2)
+    assert np.abs(out1).max() > 0
+    env = np.exp(-0.5 * inp["g2"] / 3.0)
+    assert np.all(np.abs(out1) <= 2 * env[None, :] + 1e-300)
+
+
+def _band_overlap(inp, psi, proj):
+    """Full NB x NB O-overlap of the real bands unravelled from super wave functions."""
+    mg = inp["minusg"] - 1
+    p1 = 0.5 * (psi + np.conj(psi[:, mg]))
+    p2 = -0.5j * (psi - np.conj(psi[:, mg]))
+    bands = np.empty((2 * len(psi), inp["ngl"]), complex)
+    bands[0::2], bands[1::2] = p1, p2
+    s = inp["omega"] * (np.conj(bands) @ bands.T)
+    pr = np.empty((2 * len(psi), proj.shape[0]))
+    pr[0::2], pr[1::2] = proj.real.T, proj.imag.T
+    npro = proj.shape[0]
+    D = np.zeros((npro, npro))
+    ip = 0
+    for a in range(inp["nat"]):
+        sp = inp["isp"][a] - 1
+        lox = inp["lox"][sp]
+        dm = inp["dover"][sp].T
+        offs, o = [], 0
+        for l in lox:
+            offs.append(o)
+            o += 2 * l + 1
+        for i, l1 in enumerate(lox):
+            for j, l2 in enumerate(lox):
+                if l1 == l2:
+                    for m in range(2 * l1 + 1):
+                        D[ip + offs[i] + m, ip + offs[j] + m] = dm[i, j]
+        ip += o
+    return (s + pr @ D @ pr.T).real
+
+
+def test_oracle_orthonormality_and_drift(oracle):
+    s = systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry")
+    inp = systems.build_inputs(s)
+    w = oracle.open_oracle(inp).setup().initialize()
+    ov = _band_overlap(inp, w.download_psi(0), w.get_proj())
+    # ORTHO_Y_C regularises its divisions by R8SMALL=1e-10 (src/paw_waves2.f90:1058)
+    assert np.abs(ov - np.eye(inp["nb"])).max() < 1e-9
+    w.set_dynamics(10.0, 0.3)
+    for _ in range(20):
+        w.cp_step()
+    w.set_dynamics(10.0, 0.0)
+    w.stop()
+    psi0 = w.download_psi(0)
+    proj0 = w.get_proj()
+    drifts = []
+    for dt in (10.0, 5.0):
+        w.upload_psi(0, psi0)
+        w.upload_psi(1, psi0)
+        w.set_proj(proj0)
+        w.set_rlam0(np.zeros((inp["nb"], inp["nb"]), complex))
+        w.stop()
+        w.set_dynamics(dt, 0.0)
+        es = []
+        for _ in range(int(60 / dt)):
+            out, _ = w.cp_step()
+            es.append(out[0] + out[2])
+        drifts.append(np.ptp(es))
+        ov = _band_overlap(inp, w.download_psi(0), w.get_proj())
+        assert np.abs(ov - np.eye(inp["nb"])).max() < 1e-7  # ORTHO_X EPS 1e-8 on max|O-1|
+    assert drifts[1] < drifts[0] / 2.5  # dt^2 scaling of the Verlet error
+
+
+def test_golden_regression(oracle):
+    """The oracle reproduces its committed fixtures (generated by tests/golden/make_golden.py)."""
+    with open(os.path.join(GOLD, "oracle_si8_20ry.json")) as f:
+        gold = json.load(f)
+    from golden.make_golden import run_case  # noqa: E402
+
+    got = run_case(oracle)
+    assert got["ngl"] == gold["ngl"]
+    assert got["igvec_sha256"] == gold["igvec_sha256"]
+    for k in ("etot", "ekin", "ekinpsi", "iters"):
+        assert np.allclose(got[k], gold[k], rtol=0, atol=1e-9), k
+    assert np.allclose(got["force0"], gold["force0"], rtol=0, atol=1e-8)
