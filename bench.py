@@ -1,0 +1,364 @@
+"""Benchmark: Car-Parrinello steps per second of the WAVES hot path.
+
+Workload: Si64 (2x2x2 supercell of cubic diamond Si, a=20.52 bohr, seeded
++-0.05 bohr displacements), Gamma point, 128 bands (64 super wave functions),
+30/60 Ry, 64^3 FFT grid, NVE CP steps with dt=10 a.u. and m=1000 a.u., atoms
+moving.  Synthetic setups, V_loc and DH (no dataset is involved).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--precision fp64]
+
+One JSON line is printed by rank 0.  `value` is whole-job steps/s with every
+array resident in HBM (N independent replicas with --gpus N: the path does
+not shard, one system per GPU); `e2e` is the same metric through the C ABI
+with per-step host buffers (V(r), DH and positions uploaded from pinned host
+memory, energies and forces read back).  --impl reference times the CPU
+restatement of the reference (the reference itself cannot be compiled in this
+image: no Fortran compiler, FFTW, BLAS or LAPACK) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cp-paw_b200"))
+
+METRIC = "CP steps/s Si64"
+WORKLOAD = "Si64 Gamma 128 bands 30/60 Ry 64^3 grid, NVE CP (dt=10, m=1000), moving atoms"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        import statistics
+
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "MEASURED_PEAKS.json"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_peak_tflops(torch):
+    """FP64 tensor throughput measured here: cuBLAS DGEMM via torch.matmul
+    (MEASURED_PEAKS.json has HBM and BF16 only)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def load_ncu_traffic():
+    """Per-launch DRAM traffic of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def make_inputs(name="Si64"):
+    from cuwaves import systems
+
+    return systems.build_inputs(systems.named_system(name))
+
+
+def flops_model(inp):
+    """Algorithmic work per step (real flops / bytes), as used for the roofline."""
+    ngl, nbh, npro = inp["ngl"], inp["nbh"], None
+    npro = sum(sum(2 * l + 1 for l in inp["lox"][s - 1]) for s in inp["isp"].tolist())
+    nr = inp["grid"][0] * inp["grid"][1] * inp["grid"][2]
+    contr = 8.0 * ngl * npro * nbh
+    return {
+        "addpro_propagate_flops": 2 * contr,      # H and O back-projection (one fused kernel)
+        "projections_flops": 2 * contr,           # <p|psibar>, <p|O psi0> at R(+) (one fused kernel)
+        "forces_flops": contr,
+        "gram_flops": 6 * 8.0 * ngl * nbh * nbh,
+        "fft_bytes": 2 * nbh * 2 * nr * 16.0,     # two transforms per band, grid read+write
+        "npro": npro,
+    }
+
+
+def run_cuda(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    import cuwaves
+
+    inp = make_inputs(args.system)
+    w = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_FP64).setup().initialize()
+    stream = torch.cuda.ExternalStream(w.stream())
+    for _ in range(args.warmup):
+        w.cp_step(move_atoms=True)
+    # ---- timed region, device-resident ---------------------------------------
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    w.set_timing(True)
+    _, l0, _ = w.get_timing()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            out, f = w.cp_step(move_atoms=True)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = ev0.elapsed_time(ev1)
+    phases, l1, nsteps = w.get_timing()
+    launches = l1 - l0
+    w.set_timing(False)
+    # ---- e2e: per-step host inputs from pinned memory -------------------------
+    v_h = torch.from_numpy(np.ascontiguousarray(inp["v"])).pin_memory()
+    dh_h = torch.from_numpy(np.ascontiguousarray(inp["dh"]).view(np.float64)).pin_memory()
+    r_h = torch.from_numpy(np.ascontiguousarray(inp["r0"])).pin_memory()
+    out_h = torch.zeros(8, dtype=torch.float64).pin_memory()
+    f_h = torch.zeros((inp["nat"], 3), dtype=torch.float64).pin_memory()
+    m_h = torch.from_numpy(np.ascontiguousarray(inp["masses"])).pin_memory()
+    import ctypes as C
+
+    D = C.POINTER(C.c_double)
+    fns = w._f
+    lmnxx = inp["dh"].shape[-1]
+    torch.cuda.synchronize()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(args.steps):
+        fns["set_potential"](w.h, C.cast(v_h.data_ptr(), D))
+        fns["set_dh"](w.h, lmnxx, C.cast(dh_h.data_ptr(), D))
+        fns["set_atoms"](w.h, C.cast(r_h.data_ptr(), D), None)
+        rc = fns["cp_step"](w.h, 1, C.cast(m_h.data_ptr(), D), 200, 1e-8, C.cast(out_h.data_ptr(), D),
+                            C.cast(f_h.data_ptr(), D))
+        if rc:
+            w._chk(rc, "TIMESTEP")
+    ev3.record(stream)
+    ev3.synchronize()
+    ms_e2e = ev2.elapsed_time(ev3)
+    h2d = v_h.numel() * 8 + dh_h.numel() * 8 + r_h.numel() * 8 + m_h.numel() * 8
+    d2h = out_h.numel() * 8 // 8 * 5 + f_h.numel() * 8
+    # max over ranks
+    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, ms_e2e = float(t[0]), float(t[1])
+    # roofline of the dominant phase
+    fm = flops_model(inp)
+    peaks, peak_src = measured_peaks()
+    result = {"phases_ms_per_step": {k: v / max(1, nsteps) for k, v in phases.items()},
+              "launches": launches, "ms": ms, "ms_e2e": ms_e2e, "h2d": h2d, "d2h": d2h,
+              "clocks": clk.summary(), "fm": fm, "iters_last": float(out[4]), "etot_last": float(out[0])}
+    if rank == 0:
+        p64 = fp64_peak_tflops(torch)
+        result["fp64_peak"] = p64
+        result["peak_src"] = peak_src
+    w.close()
+    return result
+
+
+def emit_cuda(args, res, world):
+    ph = res["phases_ms_per_step"]
+    fm = res["fm"]
+    ms_step = res["ms"] / args.steps
+    value = world * args.steps / (res["ms"] * 1e-3)
+    e2e = world * args.steps / (res["ms_e2e"] * 1e-3)
+    # dominant kernel: the larger of the two fused FP64 contractions
+    cand = {"addpro_propagate": (ph["addpro_propagate"], fm["addpro_propagate_flops"]),
+            "projections": (ph["projections"], fm["projections_flops"])}
+    name = max(cand, key=lambda k: cand[k][0])
+    t_ms, flops = cand[name]
+    achieved = flops / (t_ms * 1e-3) / 1e12 if t_ms > 0 else None
+    peak = res.get("fp64_peak")
+    traffic = load_ncu_traffic().get(name)
+    cpu = cpu_baseline(args) if not args.no_cpu else None
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Si64 cell, synthetic setups, V_loc and DH)",
+        "config": {"workload": WORKLOAD, "system": args.system, "precision": "fp64",
+                   "parallelism": f"replicas{world}", "bands": 128, "grid": "64^3",
+                   "l2": "working set (~0.3 GB: psi0/psim/hpsi/opsi 24 MB each, FFT grid, EIGR) exceeds the 126 MB L2"},
+        "e2e": {"value": round(e2e, 4), "unit": "steps/s", "h2d_bytes_per_step": res["h2d"],
+                "d2h_bytes_per_step": res["d2h"]},
+        "gpu_launches": res["launches"],
+        "roofline": {"bound": "tensor", "kernel": f"k_{'addpro<FUSED>' if name == 'addpro_propagate' else 'proj<DUAL>'}",
+                     "achieved": round(achieved, 3) if achieved else None, "peak": round(peak, 3) if peak else None,
+                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved and peak else None,
+                     "peak_source": "FP64 cuBLAS DGEMM (torch.matmul float64 8192^3) measured in this run; "
+                                    "MEASURED_PEAKS.json has no FP64 figure",
+                     "traffic": traffic, "flops_per_launch": flops},
+        "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()},
+        "clocks": res["clocks"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args):
+    """The oracle (C++ restatement of the reference, OpenMP) on the host cores,
+    over a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import binding
+
+    binding.build()
+    inp = make_inputs(args.system)
+    threads = binding.library().orc_max_threads()
+    w = binding.open_oracle(inp).setup().initialize()
+    w.cp_step(move_atoms=True)  # warm caches
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        w.cp_step(move_atoms=True)
+        n += 1
+        if time.perf_counter() - t0 > args.cpu_seconds or n >= args.cpu_steps:
+            break
+    dt = time.perf_counter() - t0
+    w.close()
+    return {"value": round(n / dt, 5), "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n} CP steps of {args.system} after one warm-up step ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import binding
+
+    binding.build()
+    inp = make_inputs(args.system)
+    threads = binding.library().orc_max_threads()
+    w = binding.open_oracle(inp).setup().initialize()
+    for _ in range(args.warmup):
+        w.cp_step(move_atoms=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        w.cp_step(move_atoms=True)
+    dt = time.perf_counter() - t0
+    w.close()
+    v = args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "steps/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Si64 cell, synthetic setups, V_loc and DH)",
+            "config": {"workload": WORKLOAD, "system": args.system, "precision": "fp64",
+                       "parallelism": "host cores"},
+            "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} CP steps of {args.system} after {args.warmup} warm-up steps; "
+                                       "the CPU restatement of the reference (the Fortran reference cannot be "
+                                       "built here: no Fortran compiler, FFTW, BLAS or LAPACK)"},
+            "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--system", default="Si64")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "cuda" else args.warmup
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch
+
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res = run_cuda(args, rank, world, local)
+    if rank == 0:
+        if world > 1 or args.no_cpu:
+            args.no_cpu = args.no_cpu or rank != 0
+        emit_cuda(args, res, world)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -254,11 +254,15 @@ static int force_dev_run(Handle* h, double* force_dev) {
 }
 
 // the part of WAVES$ORTHOGONALIZE after OPSI is formed (src/paw_waves2.f90:242-490)
+static int mark(Handle* h, int phase);
 static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
   Device& g = h->g;
   // projections of PSIBAR and OPSI at R(+)
+  CUW_RET(mark(h, 1));
   CUW_RET(eigr_compute(h, g.rp));
+  CUW_RET(mark(h, 5));
   CUW_RET(proj_compute(h, g.psim, g.proj, g.opsi, g.oproj));
+  CUW_RET(mark(h, 6));
   // DO*PROJ and DO*OPROJ
   CUW_RET(oproj_compute(h, g.proj, g.hproj));
   CUW_RET(oproj_compute(h, g.oproj, g.pbuf));
@@ -270,16 +274,45 @@ static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
   GramPair pp[3] = {{g.psim, g.psim}, {g.opsi, g.psim}, {g.opsi, g.opsi}};
   CUW_RET(gram_planewave(h, pp, 3, pw));
   CUW_RET(unravel_run(h, pw, oc, 3, g.mat, g.omat, g.oomat));
+  CUW_RET(mark(h, 7));
   CUW_RET(lambda_init_run(h));
   int it = 0;
   int st = ortho_solve(h, max_iter, eps, &it);
   if (iters) *iters = it;
   if (st != CUW_OK) return st;
+  CUW_RET(mark(h, 8));
   CUW_RET(lambda12_run(h, g.lam, g.lam1c, g.lam2c));
   CUW_RET(addopsi_run(h, g.psim, g.opsi, g.lam1c, g.lam2c));
   CUW_RET(addoproj_run(h, g.proj, g.oproj, g.lam1c, g.lam2c));
   CUW_RET(store_lambda_run(h));
   h->have_opsi = false;
+  return CUW_OK;
+}
+
+// phase marks of cuwaves_cp_step (only when timing is enabled)
+enum { PH_RED = 0, PH_EIGR, PH_FORCE, PH_FFT, PH_ADDPRO, PH_PROJ, PH_GRAM, PH_ORTHO, PH_ROTATE, PH_MISC };
+static int mark(Handle* h, int phase) {
+  if (!h->timing) return CUW_OK;
+  if (h->nev >= (int)h->ev.size()) {
+    cudaEvent_t e;
+    CUW_TRY(cudaEventCreate(&e));
+    h->ev.push_back(e);
+    h->ev_phase.push_back(0);
+  }
+  h->ev_phase[h->nev] = phase;  // time from this mark to the next is charged to `phase`
+  CUW_TRY(cudaEventRecord(h->ev[h->nev], h->stream));
+  ++h->nev;
+  return CUW_OK;
+}
+static int collect_marks(Handle* h) {
+  if (!h->timing) return CUW_OK;
+  for (int i = 0; i + 1 < h->nev; ++i) {
+    float ms = 0.f;
+    CUW_TRY(cudaEventElapsedTime(&ms, h->ev[i], h->ev[i + 1]));
+    h->phase_ms[h->ev_phase[i]] += ms;
+  }
+  h->nev = 0;
+  h->phase_calls++;
   return CUW_OK;
 }
 
@@ -433,6 +466,7 @@ extern "C" int cuwaves_destroy(cuw_handle* hp) {
   if (!hp) return CUW_OK;
   H(hp);
   cudaStreamSynchronize(h->stream);
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   free_all(h);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -777,18 +811,26 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   Device& g = h->g;
   double* sc = g.scal;  // [0] ekin [1] etot [2] ekin1 [3] ekin2 [4] eion ; per-band scratch after 8
   double* tmpv = g.scal + 8;
+  h->nev = 0;
+  CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_EKIN, tmpv));
   CUW_TRY(cudaMemcpyAsync(sc + 0, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
   CUW_TRY(cudaMemcpyAsync(sc + 2, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(mark(h, PH_EIGR));
   CUW_RET(eigr_compute(h, g.r0));
+  CUW_RET(mark(h, PH_FORCE));
   CUW_RET(force_dev_run(h, g.force));
+  CUW_RET(mark(h, PH_FFT));
   CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
+  CUW_RET(mark(h, PH_ADDPRO));
   CUW_RET(hproj_compute(h, g.proj, g.hproj));
   CUW_RET(oproj_compute(h, g.proj, g.oproj));
   CUW_RET(addpro_run(h, ADDPRO_FUSED, g.hproj, g.oproj));
+  CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_EXPECT, tmpv));
   CUW_TRY(cudaMemcpyAsync(sc + 1, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
     CUW_TRY(cudaMemcpyAsync(g.mass, mass, sizeof(double) * h->d.nat, cudaMemcpyHostToDevice, h->stream));
     k_atoms_verlet<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(g.r0, g.rm, g.rp, g.force, g.mass, h->d.nat,
@@ -797,8 +839,10 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   }
   int iters = 0;
   CUW_RET(ortho_core(h, max_iter, eps, &iters));
+  CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
   CUW_TRY(cudaMemcpyAsync(sc + 3, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
     k_ion_ekin<<<1, 1, 0, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
     CUW_LAUNCH_CHECK("k_ion_ekin");
@@ -812,10 +856,12 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   std::swap(g.psi0, g.psim);
   CUW_RET(switch_lambda_run(h));
   h->have_hpsi = false;
+  CUW_RET(mark(h, PH_MISC));
   double hs[5];
   CUW_TRY(cudaMemcpyAsync(hs, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
   if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
+  CUW_RET(collect_marks(h));
   if (out) {
     out[0] = hs[1];
     out[1] = hs[0];
@@ -824,5 +870,29 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
     out[4] = iters;
     out[5] = out[6] = out[7] = 0.0;
   }
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_set_timing(cuw_handle* hp, int enable) {
+  H(hp);
+  h->timing = enable != 0;
+  for (int i = 0; i < Handle::kPhases; ++i) h->phase_ms[i] = 0.0;
+  h->phase_calls = 0;
+  h->nev = 0;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_get_timing(cuw_handle* hp, double* ms, int n, long long* launches, long long* steps) {
+  H(hp);
+  for (int i = 0; i < n && i < Handle::kPhases; ++i) ms[i] = h->phase_ms[i];
+  if (launches) *launches = h->launches;
+  if (steps) *steps = h->phase_calls;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_get_stream(cuw_handle* hp, void** stream) {
+  H(hp);
+  if (!stream) return h->fail(CUW_ERR_ARG, "null stream pointer");
+  *stream = reinterpret_cast<void*>(h->stream);
   return CUW_OK;
 }

@@ -30,6 +30,7 @@ struct Status {
 
 #define CUW_LAUNCH_CHECK(name)                                      \
   do {                                                              \
+    ++h->launches;                                                  \
     cudaError_t e__ = cudaGetLastError();                           \
     if (e__ != cudaSuccess)                                         \
       return h->fail(CUW_ERR_CUDA, std::string(name) + ": " +       \
@@ -135,6 +136,15 @@ struct Handle {
   double waveekin1 = 0.0, waveekin2 = 0.0;
   cudaStream_t stream = nullptr;
   int device = 0, nsm = 148;
+  // measurement: kernel launches, and per-phase device time of cuwaves_cp_step
+  long long launches = 0;
+  bool timing = false;
+  static constexpr int kPhases = 10;
+  double phase_ms[kPhases] = {0};
+  long long phase_calls = 0;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ev_phase;
+  int nev = 0;
   Device g;
   std::string err;
 

@@ -652,9 +652,11 @@ int switch_lambda_run(Handle* h) {
 
 int ortho_y_run(Handle* h, const double* s, double* x) {
   const int n = h->d.nb;
+  if (n > 1024) return h->fail(CUW_ERR_UNSUPPORTED, "Gram-Schmidt supports NB <= 1024");
   Device& g = h->g;
   CUW_TRY(cudaMemsetAsync(g.ostatus, 0, sizeof(int) * 2, h->stream));
-  k_ortho_y<<<1, 1024, 0, h->stream>>>(s, n, g.haux, g.gamn, g.work, g.lam2, x, g.maxpart, g.ostatus);
+  // A, B, C, ALPHA, WORK in the NB x NB buffers that are free during start-up
+  k_ortho_y<<<1, 1024, 0, h->stream>>>(s, n, g.haux, g.gamn, g.work, g.lam2, x, g.lam, g.ostatus);
   CUW_LAUNCH_CHECK("k_ortho_y");
   return CUW_OK;
 }

@@ -79,6 +79,9 @@ SIGNATURES = {
 OPTIONAL = {
     "set_async": [_P, C.c_int],
     "synchronize": [_P],
+    "set_timing": [_P, C.c_int],
+    "get_timing": [_P, _D, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "get_stream": [_P, C.POINTER(C.c_void_p)],
     "get_atoms": [_P, _D, _D, _D],
     "set_threads": [_P, C.c_int],
 }
@@ -311,6 +314,23 @@ class Waves:
     def synchronize(self):
         if "synchronize" in self._f:
             self._chk(self._f["synchronize"](self.h), "synchronize")
+
+    PHASES = ("reductions", "structure factors", "forces", "fft_vpsi", "addpro_propagate",
+              "projections", "gram", "ortho_solve", "rotate", "bookkeeping")
+
+    def set_timing(self, on: bool):
+        self._chk(self._f["set_timing"](self.h, int(on)), "set_timing")
+
+    def get_timing(self):
+        ms = np.zeros(len(self.PHASES))
+        nl, ns = C.c_longlong(), C.c_longlong()
+        self._chk(self._f["get_timing"](self.h, _dptr(ms), len(ms), C.byref(nl), C.byref(ns)), "get_timing")
+        return dict(zip(self.PHASES, ms.tolist())), nl.value, ns.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._chk(self._f["get_stream"](self.h, C.byref(s)), "get_stream")
+        return s.value or 0
 
     def initialize(self, gram_schmidt: bool = True):
         """Start-up of WAVES$ETOT at TFIRST (src/paw_waves1.f90:1733-1748):

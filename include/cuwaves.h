@@ -146,6 +146,20 @@ int cuwaves_cp_step(cuw_handle* h, int move_atoms, const double* mass,
 /* Resets the nuclear history so that R(-) = R(0) (start from rest). */
 int cuwaves_reset_atoms(cuw_handle* h, const double* r0);
 
+/* Measurement hooks (no counterpart in the reference, whose TIMING$CLOCKON/OFF
+ * clocks, src/paw_timing.f90:121-192, play this role on the CPU).
+ * cuwaves_set_timing(h, 1) records CUDA events on the handle's stream at the
+ * phase boundaries of cuwaves_cp_step and resets the accumulators;
+ * cuwaves_get_timing returns the accumulated device time per phase in ms
+ * (n <= 10: reductions, structure factors, forces, FFT/V.psi, H and O
+ * back-projection with propagation, projections at R(+), Gram products,
+ * orthogonality solve, rotation by Lambda, bookkeeping), the number of kernels
+ * this handle has launched and the number of timed steps.
+ * cuwaves_get_stream returns the handle's cudaStream_t. */
+int cuwaves_set_timing(cuw_handle* h, int enable);
+int cuwaves_get_timing(cuw_handle* h, double* ms, int n, long long* launches, long long* steps);
+int cuwaves_get_stream(cuw_handle* h, void** stream);
+
 #ifdef __cplusplus
 }
 #endif
