@@ -28,7 +28,8 @@ namespace cuw {
 
 namespace {
 
-constexpr int kMaxV = 16;  // complex values per thread per stage
+constexpr int kMaxV = 8;   // complex values per thread per stage
+constexpr int kPlaneThreads = 256;
 
 // --- radix butterflies: v <- DFT_R(v) with exp(sign*2*pi*i*q*s/R) -----------
 __device__ __forceinline__ double2 mul_i(double2 a, double sgn) {  // a * (sgn*i)
@@ -136,15 +137,16 @@ struct Bfly<7> : BflyGeneric<7> {};
 template <>
 struct Bfly<11> : BflyGeneric<11> {};
 
-// One Stockham stage on `nlines` lines of length n held in shared memory:
-// element e of line L lives at buf[L*ls + e*es].  tw[k] = exp(sgn*2 pi i k/n).
+// One Stockham stage on lines [line0, line0+nl) of length n held in shared
+// memory: element e of line L lives at buf[L*ls + e*es].  tw[k] = exp(sgn*2 pi i k/n).
 // jfast selects the thread mapping (consecutive threads -> consecutive j).
+// The caller guarantees nl*n/R <= blockDim.x * BPT.
 template <int R>
-__device__ __noinline__ void stage(double2* buf, int n, int ns, int nlines, int ls, int es, bool jfast,
-                      const double2* tw, double sgn) {
-  constexpr int BPT = kMaxV / R;
+__device__ __noinline__ void stage(double2* buf, int n, int ns, int line0, int nl, int ls, int es, bool jfast,
+                                      const double2* tw, double sgn) {
+  constexpr int BPT = (kMaxV / R) > 0 ? (kMaxV / R) : 1;
   const int nq = n / R;
-  const int total = nlines * nq;
+  const int total = nl * nq;
   double2 v[BPT][R];
   int line_[BPT], j_[BPT];
 #pragma unroll
@@ -154,7 +156,8 @@ __device__ __noinline__ void stage(double2* buf, int n, int ns, int nlines, int 
     if (bf < total) {
       int line, j;
       if (jfast) { j = bf % nq; line = bf / nq; }
-      else { line = bf % nlines; j = bf / nlines; }
+      else { line = bf % nl; j = bf / nl; }
+      line += line0;
       line_[t] = line;
       j_[t] = j;
       const int k = j % ns;
@@ -183,26 +186,44 @@ __device__ __noinline__ void stage(double2* buf, int n, int ns, int nlines, int 
   __syncthreads();
 }
 
+__host__ __device__ constexpr int bpt_of(int r) { return (kMaxV / r) > 0 ? (kMaxV / r) : 1; }
+
 struct AxisArg {
   int n;
   int nstage;
   int radix[8];
 };
 
+// lines per chunk so that every stage fits one pass of the block
+__device__ __forceinline__ int lines_per_chunk(const AxisArg& ax, int nlines) {
+  int lc = nlines;
+  for (int s = 0; s < ax.nstage; ++s) {
+    int r = ax.radix[s];
+    int cap = (int)(((long)blockDim.x * bpt_of(r) * r) / ax.n);
+    if (cap < 1) cap = 1;
+    lc = min(lc, cap);
+  }
+  return lc;
+}
+
 __device__ void transform(double2* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast,
                           const double2* tw, double sgn) {
-  int ns = 1;
-  for (int s = 0; s < ax.nstage; ++s) {
-    switch (ax.radix[s]) {
-      case 2: stage<2>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
-      case 3: stage<3>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
-      case 4: stage<4>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
-      case 5: stage<5>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
-      case 7: stage<7>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
-      case 8: stage<8>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
-      case 11: stage<11>(buf, ax.n, ns, nlines, ls, es, jfast, tw, sgn); break;
+  const int lc = lines_per_chunk(ax, nlines);
+  for (int l0 = 0; l0 < nlines; l0 += lc) {
+    const int nl = min(lc, nlines - l0);
+    int ns = 1;
+    for (int s = 0; s < ax.nstage; ++s) {
+      switch (ax.radix[s]) {
+        case 2: stage<2>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+        case 3: stage<3>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+        case 4: stage<4>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+        case 5: stage<5>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+        case 7: stage<7>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+        case 8: stage<8>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+        case 11: stage<11>(buf, ax.n, ns, l0, nl, ls, es, jfast, tw, sgn); break;
+      }
+      ns *= ax.radix[s];
     }
-    ns *= ax.radix[s];
   }
 }
 
@@ -215,7 +236,7 @@ __device__ void load_tw(double2* dst, const double2* src, int n, double sgn) {
 }
 
 // ---------------------------------------------------------------------------
-__global__ void k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
                              const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
                              double2* __restrict__ grid, int nzp, AxisArg a1, AxisArg a2,
                              const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
@@ -241,7 +262,7 @@ __global__ void k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, c
 
 constexpr int kTX = 16;  // x columns per z-column block
 
-__global__ void k_zcol_v(double2* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot,
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_zcol_v(double2* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot,
                          int nzp, int nr1, int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
   extern __shared__ double2 sm[];
   const int nr3 = a3.n;
@@ -280,7 +301,7 @@ __global__ void k_zcol_v(double2* __restrict__ grid, const double* __restrict__ 
   }
 }
 
-__global__ void k_rtog_plane(const double2* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
+__global__ void __launch_bounds__(kPlaneThreads, 2) k_rtog_plane(const double2* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
                              const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
                              double2* __restrict__ out, const double2* __restrict__ psi, int ldg, int b0,
                              const double* __restrict__ g2, const double* __restrict__ bucket, int add_kin,
@@ -337,13 +358,6 @@ bool plan_axis(int n, AxisPlan& p) {
   return m == 1;
 }
 
-int plane_threads(int npl) {
-  // values per thread per stage must stay below kMaxV for every radix
-  int t = 128;
-  while (t < 1024 && (npl + t - 1) / t > kMaxV / 2) t *= 2;
-  return t;
-}
-
 }  // namespace
 
 int fft_setup(Handle* h, const int* igvec) {
@@ -354,8 +368,7 @@ int fft_setup(Handle* h, const int* igvec) {
       return h->fail(CUW_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has a prime factor above 11");
   }
   const size_t npl = (size_t)nr1 * nr2;
-  if (npl + nr1 + nr2 > (size_t)(220 * 1024) / sizeof(double2) || npl > (size_t)kMaxV / 2 * 1024 ||
-      (size_t)nr3 * kTX + nr3 > 14000)
+  if (npl + nr1 + nr2 > (size_t)(220 * 1024) / sizeof(double2) || (size_t)nr3 * kTX + nr3 > 14000)
     return h->fail(CUW_ERR_UNSUPPORTED, "FFT plane too large for shared memory");
   // occupied planes and the per-plane G lists
   std::vector<int> cnt(nr3, 0);
@@ -430,8 +443,8 @@ int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
   const size_t npl = (size_t)nr1 * nr2;
   const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(double2));
   const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(double2));
-  const int tp = plane_threads((int)npl);
-  const int tz = plane_threads(nr3 * kTX);
+  const int tp = kPlaneThreads;
+  const int tz = kPlaneThreads;
   AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
   const double scale = 1.0 / ((double)nr1 * nr2 * nr3);
   Device& g = h->g;
