@@ -224,3 +224,22 @@ def test_nan_input_detected(oracle, inputs_cache):
     assert e.value.code == 7
     gpu2 = cuwaves.open_waves(inp).setup().initialize()
     assert np.isfinite(gpu2.ekin())
+
+
+@pytest.mark.parametrize("name", ["Si64", "H2O32"])
+def test_full_size_step(name, oracle):
+    """The benchmark systems at full size (64^3 and 72^3 grids): H|psi> and one
+    complete CP step against the oracle."""
+    inp = systems.build_inputs(systems.named_system(name))
+    gpu = cuwaves.open_waves(inp).setup().initialize()
+    cpu = oracle.open_oracle(inp).setup()
+    sync_state(gpu, cpu)
+    gpu.hpsi()
+    cpu.hpsi()
+    assert rel(gpu.download_psi(CUW_HPSI), cpu.download_psi(CUW_HPSI)) < 1e-10
+    og, fg = gpu.cp_step(move_atoms=True)
+    oc, fc = cpu.cp_step(move_atoms=True)
+    assert og[4] == oc[4]
+    assert abs(og[0] - oc[0]) < 1e-8 * max(1.0, abs(oc[0]) / 100)
+    assert np.abs(fg - fc).max() < 1e-6
+    assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-9
