@@ -97,7 +97,7 @@ struct Device {
   // orthogonalisation (real NB x NB)
   double *mat = nullptr, *omat = nullptr, *oomat = nullptr;
   double *lam = nullptr, *lam2 = nullptr;
-  double *u = nullptr, *eig = nullptr;
+  double *u = nullptr, *u2 = nullptr, *eig = nullptr;
   double *haux = nullptr, *gamn = nullptr, *work = nullptr, *wk2 = nullptr;
   double *maxpart = nullptr;
   int *ostatus = nullptr;        // [0] status, [1] iterations

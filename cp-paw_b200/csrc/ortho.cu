@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int j = tid; j < n; j += nt)
     for (int i = 0; i <= j; ++i) A[pk(i, j)] = s_in[i + (size_t)n * j];
+  __syncthreads();  // V may alias s_in when it lives in global memory
   for (size_t k = tid; k < (size_t)n * n; k += nt) {
     int i = (int)(k % n), j = (int)(k / n);
     V[k] = (i == j) ? 1.0 : 0.0;
@@ -124,7 +125,8 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
         pq[tid] = q;
         double apq = A[pk(p, q)], app = A[pk(p, p)], aqq = A[pk(q, q)];
         double c = 1.0, s = 0.0;
-        if (apq != 0.0 && fabs(apq) > 1e-17 * sqrt(fabs(app * aqq))) {
+        // rotate unless |apq| is at the rounding level of the diagonal (4 ulp)
+        if (apq != 0.0 && fabs(apq) > 8.9e-16 * sqrt(fabs(app * aqq))) {
           double theta = (aqq - app) / (2.0 * apq);
           double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
           c = 1.0 / sqrt(t * t + 1.0);
@@ -209,10 +211,11 @@ struct OrthoArgs {
   double eps;
 };
 
-// C(tile) = op(A) * op(B); op = transpose when tA / tB
-__device__ void gemm_tile(const double* __restrict__ A, bool tA, const double* __restrict__ B, bool tB, int n,
-                          int i0, int i1, int j0, int j1, double* __restrict__ C, double* smA, double* smB,
-                          int kc) {
+// C(tile) = op(A) * op(B); op = transpose when tA / tB.
+// A and B may have been written by other CTAs of the cluster in the previous
+// phase, so they are read through L2 (__ldcg), never through the read-only path.
+__device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, int n, int i0, int i1, int j0, int j1,
+                          double* C, double* smA, double* smB, int kc) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int tm = i1 - i0, tn = j1 - j0;
   const int tx = tid % 16, ty = tid / 16;  // 16 x (nt/16)
@@ -226,12 +229,12 @@ __device__ void gemm_tile(const double* __restrict__ A, bool tA, const double* _
     for (int t = tid; t < tm * kk; t += nt) {
       int ii = t % tm, k = t / tm;
       int gi = i0 + ii, gk = k0 + k;
-      smA[ii + tm * k] = tA ? A[gk + (size_t)n * gi] : A[gi + (size_t)n * gk];
+      smA[ii + tm * k] = __ldcg(tA ? &A[gk + (size_t)n * gi] : &A[gi + (size_t)n * gk]);
     }
     for (int t = tid; t < tn * kk; t += nt) {
       int k = t % kk, jj = t / kk;
       int gj = j0 + jj, gk = k0 + k;
-      smB[k + kc * jj] = tB ? B[gj + (size_t)n * gk] : B[gk + (size_t)n * gj];
+      smB[k + kc * jj] = __ldcg(tB ? &B[gj + (size_t)n * gk] : &B[gk + (size_t)n * gj]);
     }
     __syncthreads();
     int o = 0;
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     gemm_tile(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
-      a.haux[i + (size_t)n * j] += 2.0 * a.chipsi[i + (size_t)n * j];
+      a.haux[i + (size_t)n * j] = __ldcg(&a.haux[i + (size_t)n * j]) + 2.0 * a.chipsi[i + (size_t)n * j];
     }
     csync();
     // GAMN = LAMBDA^T * HAUX
@@ -295,7 +298,8 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
       // the reference writes GAMN(J,I)=GAMN(I,J)=0.5*(GAMN(I,J)+GAMN(J,I))+PSIPSI(I,J) for J>=I
       int lo = min(i, j), hi = max(i, j);
-      double v = 0.5 * (a.gamn[lo + (size_t)n * hi] + a.gamn[hi + (size_t)n * lo]) + a.psipsi[lo + (size_t)n * hi];
+      double v = 0.5 * (__ldcg(&a.gamn[lo + (size_t)n * hi]) + __ldcg(&a.gamn[hi + (size_t)n * lo])) +
+                 a.psipsi[lo + (size_t)n * hi];
       if (i == j) v -= 1.0;
       a.w[i + (size_t)n * j] = v;
       mx = fmax(mx, fabs(v));
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     if (tid == 0) a.maxpart[rank] = red[0];
     csync();
     double digam = 0.0;
-    for (int r = 0; r < cs; ++r) digam = fmax(digam, a.maxpart[r]);
+    for (int r = 0; r < cs; ++r) digam = fmax(digam, __ldcg(&a.maxpart[r]));
     if (digam < a.eps) {
       status = CUW_OK;
       iters = iter;
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     gemm_tile(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
-      a.gamn[i + (size_t)n * j] /= (a.e[i] + a.e[j]);
+      a.gamn[i + (size_t)n * j] = __ldcg(&a.gamn[i + (size_t)n * j]) / (a.e[i] + a.e[j]);
     }
     csync();
     // HAUX = U GAMN
@@ -347,11 +351,11 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
       double v;
       if (oi < oj) {
         double occj = oj + dsmall, occi = oi + dsmall;
-        double lji = lam[j + (size_t)n * i] - 2.0 * occj / (occj + occi) * a.w[j + (size_t)n * i];
+        double lji = __ldcg(&lam[j + (size_t)n * i]) - 2.0 * occj / (occj + occi) * __ldcg(&a.w[j + (size_t)n * i]);
         v = lji * (oi + dsmall) / (oj + dsmall);
       } else {
         double occi = oi + dsmall, occj = oj + dsmall;
-        v = lam[i + (size_t)n * j] - 2.0 * occi / (occi + occj) * a.w[i + (size_t)n * j];
+        v = __ldcg(&lam[i + (size_t)n * j]) - 2.0 * occi / (occi + occj) * __ldcg(&a.w[i + (size_t)n * j]);
       }
       lamn[i + (size_t)n * j] = v;
     }
@@ -364,7 +368,7 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   if (lam != a.lam) {
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
-      a.lam[i + (size_t)n * j] = lam[i + (size_t)n * j];
+      a.lam[i + (size_t)n * j] = __ldcg(&lam[i + (size_t)n * j]);
     }
   }
   if (rank == 0 && tid == 0) {
@@ -372,6 +376,13 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     a.status[1] = iters;
   }
   csync();
+}
+
+// C = op(A) op(B) for n x n matrices, one 32x32 tile per CTA (warm start of the eigensolver)
+__global__ void __launch_bounds__(256) k_small_gemm(const double* A, int tA, const double* B, int tB, int n, double* C) {
+  __shared__ double smA[32 * 32], smB[32 * 32];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  gemm_tile(A, tA != 0, B, tB != 0, n, i0, min(n, i0 + 32), j0, min(n, j0 + 32), C, smA, smB, 32);
 }
 
 // LAMBDA1/LAMBDA2 (NBH x NBH complex) from real LAMBDA (NB x NB)
@@ -564,7 +575,22 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   Device& g = h->g;
   k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.gamn);
   CUW_LAUNCH_CHECK("k_symmetrize");
-  CUW_RET(jacobi_run(h, g.gamn, g.u, g.eig));
+  if (h->have_u) {
+    // warm start: diagonalise U_prev^T S U_prev, then U = U_prev V.  Any
+    // orthogonal eigenbasis of S gives the same Lyapunov operator of ORTHO_X.
+    dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
+    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.gamn, 0, g.u, 0, n, g.haux);
+    CUW_LAUNCH_CHECK("k_small_gemm");
+    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 1, g.haux, 0, n, g.work);
+    CUW_LAUNCH_CHECK("k_small_gemm");
+    CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig));
+    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2);
+    CUW_LAUNCH_CHECK("k_small_gemm");
+    std::swap(g.u, g.u2);
+  } else {
+    CUW_RET(jacobi_run(h, g.gamn, g.u, g.eig));
+    h->have_u = true;
+  }
   OrthoArgs a;
   a.n = n;
   a.chichi = g.oomat;
