@@ -194,6 +194,100 @@ struct AxisArg {
   int radix[8];
 };
 
+// ---------------------------------------------------------------------------
+// Compile-time specialisation for the common grid lengths: every divisor of
+// the index arithmetic is a constant, the stages are inlined and the block
+// size is fixed (kPlaneThreads), so the lines per chunk are constant too.
+// ---------------------------------------------------------------------------
+struct RadixList {
+  int n;
+  int r[8];
+};
+__host__ __device__ constexpr RadixList radices_of(int N) {
+  RadixList L{0, {0, 0, 0, 0, 0, 0, 0, 0}};
+  int m = N;
+  const int order[7] = {8, 4, 2, 3, 5, 7, 11};
+  for (int i = 0; i < 7; ++i)
+    while (m % order[i] == 0 && L.n < 8) {
+      L.r[L.n++] = order[i];
+      m /= order[i];
+    }
+  return L;
+}
+__host__ __device__ constexpr int chunk_lines(int N) {
+  RadixList L = radices_of(N);
+  int lc = 1 << 30;
+  for (int s = 0; s < L.n; ++s) {
+    int cap = (kPlaneThreads * bpt_of(L.r[s]) * L.r[s]) / N;
+    if (cap < 1) cap = 1;
+    lc = lc < cap ? lc : cap;
+  }
+  return lc;
+}
+
+template <int N, int R, int NS, int LC>
+__device__ __forceinline__ void stage_fixed(double2* buf, int line0, int nl, int ls, int es, bool jfast,
+                                            const double2* tw, double sgn) {
+  constexpr int BPT = bpt_of(R);
+  constexpr int NQ = N / R;
+  constexpr int TSTEP = N / (NS * R);
+  const int total = nl * NQ;
+  double2 v[BPT][R];
+  int off_[BPT];
+  bool act[BPT];
+#pragma unroll
+  for (int t = 0; t < BPT; ++t) {
+    const int bf = threadIdx.x + t * kPlaneThreads;
+    int line, j;
+    if (jfast) { j = bf % NQ; line = bf / NQ; }
+    else { line = bf % LC; j = bf / LC; }
+    act[t] = (bf < total) && (line < nl) && (j < NQ);
+    const int k = j % NS;
+    off_[t] = line * N + ((j / NS) * NS * R + k);  // (line, destination index) packed
+    if (act[t]) {
+      double2* base = buf + (size_t)(line0 + line) * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        double2 x = base[(size_t)(j + r * NQ) * es];
+        if (r && k) x = cmul(x, tw[(r * k * TSTEP) % N]);
+        v[t][r] = x;
+      }
+      Bfly<R>::run(v[t], sgn, tw, N);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < BPT; ++t) {
+    if (act[t]) {
+      const int line = off_[t] / N, idxd = off_[t] % N;
+      double2* base = buf + (size_t)(line0 + line) * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[(size_t)(idxd + r * NS) * es] = v[t][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int S, int NS, int LC>
+__device__ __forceinline__ void stages_fixed(double2* buf, int line0, int nl, int ls, int es, bool jfast,
+                                             const double2* tw, double sgn) {
+  constexpr RadixList L = radices_of(N);
+  if constexpr (S < L.n) {
+    constexpr int R = L.r[S];
+    stage_fixed<N, R, NS, LC>(buf, line0, nl, ls, es, jfast, tw, sgn);
+    stages_fixed<N, S + 1, NS * R, LC>(buf, line0, nl, ls, es, jfast, tw, sgn);
+  }
+}
+
+template <int N>
+__device__ void transform_fixed(double2* buf, int nlines, int ls, int es, bool jfast, const double2* tw, double sgn) {
+  constexpr int LC = chunk_lines(N);
+  for (int l0 = 0; l0 < nlines; l0 += LC) {
+    const int nl = min(LC, nlines - l0);
+    stages_fixed<N, 0, 1, LC>(buf, l0, nl, ls, es, jfast, tw, sgn);
+  }
+}
+
 // lines per chunk so that every stage fits one pass of the block
 __device__ __forceinline__ int lines_per_chunk(const AxisArg& ax, int nlines) {
   int lc = nlines;
@@ -208,6 +302,22 @@ __device__ __forceinline__ int lines_per_chunk(const AxisArg& ax, int nlines) {
 
 __device__ void transform(double2* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast,
                           const double2* tw, double sgn) {
+  switch (ax.n) {
+    case 16: transform_fixed<16>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 20: transform_fixed<20>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 24: transform_fixed<24>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 28: transform_fixed<28>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 32: transform_fixed<32>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 36: transform_fixed<36>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 40: transform_fixed<40>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 48: transform_fixed<48>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 56: transform_fixed<56>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 64: transform_fixed<64>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 72: transform_fixed<72>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 80: transform_fixed<80>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    case 96: transform_fixed<96>(buf, nlines, ls, es, jfast, tw, sgn); return;
+    default: break;
+  }
   const int lc = lines_per_chunk(ax, nlines);
   for (int l0 = 0; l0 < nlines; l0 += lc) {
     const int nl = min(lc, nlines - l0);

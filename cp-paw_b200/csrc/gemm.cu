@@ -543,16 +543,26 @@ __global__ void __launch_bounds__(NT) k_force(const double2* __restrict__ psi0, 
   }
 }
 
-// force(c, iat) = 2 * Omega * sum over g tiles and projectors of atom iat
+// force(c, iat) = 2 * Omega * sum over g tiles and projectors of atom iat;
+// one block per (component, atom), fixed-order tree reduction
 __global__ void k_force_final(const double* __restrict__ fpart, int ntile, int npro, const int* __restrict__ ipro0,
                               const int* __restrict__ nlmn, int nat, double gweight, double* __restrict__ force) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 3 * nat) return;
-  int a = i / 3, c = i % 3;
+  const int c = blockIdx.x, a = blockIdx.y;
+  const int p0 = ipro0[a], np = nlmn[a];
+  const int total = ntile * np;
   double s = 0.0;
-  for (int p = ipro0[a]; p < ipro0[a] + nlmn[a]; ++p)
-    for (int t = 0; t < ntile; ++t) s += fpart[((size_t)t * npro + p) * 3 + c];
-  force[i] = gweight * 2.0 * s;
+  for (int k = threadIdx.x; k < total; k += blockDim.x) {
+    int t = k / np, p = p0 + k % np;
+    s += fpart[((size_t)t * npro + p) * 3 + c];
+  }
+  __shared__ double red[128];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) force[3 * a + c] = gweight * 2.0 * red[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -796,8 +806,8 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
                                               h->g.eigr, h->g.gx, h->g.gy, h->g.gz, fpart);
   CUW_LAUNCH_CHECK("k_force");
   TabView t = tables(h);
-  k_force_final<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(fpart, tm, npro, t.ipro0, t.nlmn, h->d.nat,
-                                                                     h->gweight, force_dev);
+  k_force_final<<<dim3(3, h->d.nat), 128, 0, h->stream>>>(fpart, tm, npro, t.ipro0, t.nlmn, h->d.nat, h->gweight,
+                                                          force_dev);
   CUW_LAUNCH_CHECK("k_force_final");
   return CUW_OK;
 }

@@ -209,49 +209,71 @@ struct OrthoArgs {
   int* status;    // [0] status, [1] iterations
   int max_iter;
   double eps;
+  int kc;
 };
 
-// C(tile) = op(A) * op(B); op = transpose when tA / tB.
+// C(tile) = op(A) * op(B); op = transpose when tA / tB.  The tile
+// [i0,i1) x [j0,j1) has at most 16*MR rows and 16*MC columns; thread (ty,tx)
+// of the 16x16 layout owns rows ty+16r and columns tx+16c.  The K extent is
+// staged in chunks of kc into smA[k][row] / smB[k][col] (conflict-free reads).
 // A and B may have been written by other CTAs of the cluster in the previous
 // phase, so they are read through L2 (__ldcg), never through the read-only path.
+template <int MR, int MC>
 __device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, int n, int i0, int i1, int j0, int j1,
                           double* C, double* smA, double* smB, int kc) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int tm = i1 - i0, tn = j1 - j0;
-  const int tx = tid % 16, ty = tid / 16;  // 16 x (nt/16)
-  const int nty = nt / 16;
-  constexpr int MAXO = 16;
-  double acc[MAXO];
+  const int tx = tid % 16, ty = tid / 16;
+  constexpr int RA = 16 * MR, RB = 16 * MC;
+  double acc[MR][MC];
 #pragma unroll
-  for (int o = 0; o < MAXO; ++o) acc[o] = 0.0;
+  for (int r = 0; r < MR; ++r)
+#pragma unroll
+    for (int c = 0; c < MC; ++c) acc[r][c] = 0.0;
   for (int k0 = 0; k0 < n; k0 += kc) {
     const int kk = min(kc, n - k0);
-    for (int t = tid; t < tm * kk; t += nt) {
-      int ii = t % tm, k = t / tm;
-      int gi = i0 + ii, gk = k0 + k;
-      smA[ii + tm * k] = __ldcg(tA ? &A[gk + (size_t)n * gi] : &A[gi + (size_t)n * gk]);
+    if (!tA) {
+      for (int t = tid; t < RA * kk; t += nt) {
+        int ii = t % RA, k = t / RA;
+        smA[k * RA + ii] = ii < tm ? __ldcg(&A[(i0 + ii) + (size_t)n * (k0 + k)]) : 0.0;
+      }
+    } else {
+      for (int t = tid; t < RA * kk; t += nt) {
+        int k = t % kk, ii = t / kk;
+        smA[k * RA + ii] = ii < tm ? __ldcg(&A[(k0 + k) + (size_t)n * (i0 + ii)]) : 0.0;
+      }
     }
-    for (int t = tid; t < tn * kk; t += nt) {
-      int k = t % kk, jj = t / kk;
-      int gj = j0 + jj, gk = k0 + k;
-      smB[k + kc * jj] = __ldcg(tB ? &B[gj + (size_t)n * gk] : &B[gk + (size_t)n * gj]);
+    if (!tB) {
+      for (int t = tid; t < RB * kk; t += nt) {
+        int k = t % kk, jj = t / kk;
+        smB[k * RB + jj] = jj < tn ? __ldcg(&B[(k0 + k) + (size_t)n * (j0 + jj)]) : 0.0;
+      }
+    } else {
+      for (int t = tid; t < RB * kk; t += nt) {
+        int jj = t % RB, k = t / RB;
+        smB[k * RB + jj] = jj < tn ? __ldcg(&B[(j0 + jj) + (size_t)n * (k0 + k)]) : 0.0;
+      }
     }
     __syncthreads();
-    int o = 0;
-    for (int ii = ty; ii < tm; ii += nty)
-      for (int jj = tx; jj < tn; jj += 16) {
-        double s = acc[o];
-        for (int k = 0; k < kk; ++k) s += smA[ii + tm * k] * smB[k + kc * jj];
-        acc[o] = s;
-        ++o;
-      }
+    for (int k = 0; k < kk; ++k) {
+      double av[MR], bv[MC];
+#pragma unroll
+      for (int r = 0; r < MR; ++r) av[r] = smA[k * RA + ty + 16 * r];
+#pragma unroll
+      for (int c = 0; c < MC; ++c) bv[c] = smB[k * RB + tx + 16 * c];
+#pragma unroll
+      for (int r = 0; r < MR; ++r)
+#pragma unroll
+        for (int c = 0; c < MC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+    }
     __syncthreads();
   }
-  int o = 0;
-  for (int ii = ty; ii < tm; ii += nty)
-    for (int jj = tx; jj < tn; jj += 16) {
-      C[(i0 + ii) + (size_t)n * (j0 + jj)] = acc[o];
-      ++o;
+#pragma unroll
+  for (int r = 0; r < MR; ++r)
+#pragma unroll
+    for (int c = 0; c < MC; ++c) {
+      int ii = ty + 16 * r, jj = tx + 16 * c;
+      if (ii < tm && jj < tn) C[(i0 + ii) + (size_t)n * (j0 + jj)] = acc[r][c];
     }
 }
 
@@ -260,6 +282,7 @@ __device__ __forceinline__ void csync() {
   cg::this_cluster().sync();
 }
 
+template <int MR, int MC>
 __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   extern __shared__ double sm[];
   cg::cluster_group cl = cg::this_cluster();
@@ -274,23 +297,23 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   const int rs = (n + tr - 1) / tr, csz = (n + tc - 1) / tc;
   const int i0 = min(n, ri * rs), i1 = min(n, i0 + rs);
   const int j0 = min(n, ci * csz), j1 = min(n, j0 + csz);
-  const int kc = 32;
+  const int kc = a.kc;
   double* smA = sm;
-  double* smB = sm + (size_t)rs * kc;
+  double* smB = sm + (size_t)16 * MR * kc;
   const int tid = threadIdx.x, nt = blockDim.x;
   double* lam = a.lam;
   double* lamn = a.lam2;
   int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
   for (int iter = 1; iter <= a.max_iter; ++iter) {
     // HAUX = CHICHI * LAMBDA + 2 CHIPSI
-    gemm_tile(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    gemm_tile<MR, MC>(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
       a.haux[i + (size_t)n * j] = __ldcg(&a.haux[i + (size_t)n * j]) + 2.0 * a.chipsi[i + (size_t)n * j];
     }
     csync();
     // GAMN = LAMBDA^T * HAUX
-    gemm_tile(lam, true, a.haux, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
+    gemm_tile<MR, MC>(lam, true, a.haux, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
     csync();
     // W = 0.5 (GAMN + GAMN^T) + PSIPSI - 1 ; tile max
     double mx = 0.0;
@@ -328,20 +351,20 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
       break;
     }
     // HAUX = U^T W
-    gemm_tile(a.u, true, a.w, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    gemm_tile<MR, MC>(a.u, true, a.w, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
     csync();
     // GAMN = (HAUX U) / (e_i + e_j)
-    gemm_tile(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
+    gemm_tile<MR, MC>(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
       a.gamn[i + (size_t)n * j] = __ldcg(&a.gamn[i + (size_t)n * j]) / (a.e[i] + a.e[j]);
     }
     csync();
     // HAUX = U GAMN
-    gemm_tile(a.u, false, a.gamn, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    gemm_tile<MR, MC>(a.u, false, a.gamn, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
     csync();
     // W = HAUX U^T
-    gemm_tile(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB, kc);
+    gemm_tile<MR, MC>(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB, kc);
     csync();
     // LAMBDA(I,J) -= 2 OCCI/(OCCI+OCCJ) W(I,J); then occupation symmetrisation
     const double dsmall = 1e-12;
@@ -382,7 +405,7 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
 __global__ void __launch_bounds__(256) k_small_gemm(const double* A, int tA, const double* B, int tB, int n, double* C) {
   __shared__ double smA[32 * 32], smB[32 * 32];
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
-  gemm_tile(A, tA != 0, B, tB != 0, n, i0, min(n, i0 + 32), j0, min(n, j0 + 32), C, smA, smB, 32);
+  gemm_tile<2, 2>(A, tA != 0, B, tB != 0, n, i0, min(n, i0 + 32), j0, min(n, j0 + 32), C, smA, smB, 32);
 }
 
 // LAMBDA1/LAMBDA2 (NBH x NBH complex) from real LAMBDA (NB x NB)
@@ -608,10 +631,8 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   a.status = g.ostatus;
   a.max_iter = max_iter;
   a.eps = eps;
-  // cluster of 16 CTAs (non-portable size) or 8
-  int cs = 16;
-  int rs_max = (n + 3) / 4;  // tile rows for 16 CTAs (4x4)
-  size_t smem = sizeof(double) * 32 * (size_t)(2 * (rs_max + 8));
+  // cluster of 16 CTAs (non-portable size), else 8, 4, ... ; tile rows/cols
+  // per CTA are at most 16*MR x 16*MC with MR, MC in {1,2,4}
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   cfg.blockDim = dim3(256);
@@ -619,31 +640,50 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  cudaError_t e = cudaFuncSetAttribute(k_ortho_x, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  if (e != cudaSuccess) cs = 8;
-  for (; cs >= 1; cs /= 2) {
+  int cs = 16;
+  cudaError_t e = cudaSuccess;
+  bool launched = false;
+  for (; cs >= 1 && !launched; cs /= 2) {
     int tr = 1;
     while (tr * tr < cs) tr *= 2;
     int tc = cs / tr;
     if (tr * tc != cs) { tr = cs; tc = 1; }
-    int rs = (n + tr - 1) / tr, csz = (n + tc - 1) / tc;
-    smem = sizeof(double) * 32 * (size_t)(rs + csz);
-    if (smem > 48 * 1024) {
-      if (cudaFuncSetAttribute(k_ortho_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-        cudaGetLastError();
-        continue;
-      }
+    const int rs = (n + tr - 1) / tr, csz = (n + tc - 1) / tc;
+    const int mr = rs <= 16 ? 1 : (rs <= 32 ? 2 : (rs <= 64 ? 4 : 0));
+    const int mc = csz <= 16 ? 1 : (csz <= 32 ? 2 : (csz <= 64 ? 4 : 0));
+    if (!mr || !mc) continue;
+    a.kc = std::min(n, 128);
+    const size_t smem = sizeof(double) * (size_t)a.kc * 16 * (mr + mc);
+    void (*fn)(OrthoArgs) = nullptr;
+    if (mr == 1 && mc == 1) fn = k_ortho_x<1, 1>;
+    else if (mr == 2 && mc == 2) fn = k_ortho_x<2, 2>;
+    else if (mr == 2 && mc == 4) fn = k_ortho_x<2, 4>;
+    else if (mr == 4 && mc == 2) fn = k_ortho_x<4, 2>;
+    else if (mr == 4 && mc == 4) fn = k_ortho_x<4, 4>;
+    else if (mr == 1 && mc == 2) fn = k_ortho_x<1, 2>;
+    else if (mr == 2 && mc == 1) fn = k_ortho_x<2, 1>;
+    else if (mr == 4 && mc == 1) fn = k_ortho_x<4, 1>;
+    else if (mr == 1 && mc == 4) fn = k_ortho_x<1, 4>;
+    if (!fn) continue;
+    if (cs > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
     }
     cfg.gridDim = dim3(cs);
     cfg.dynamicSmemBytes = smem;
     attr[0].val.clusterDim.x = cs;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    e = cudaLaunchKernelEx(&cfg, k_ortho_x, a);
-    if (e == cudaSuccess) break;
-    cudaGetLastError();
+    e = cudaLaunchKernelEx(&cfg, fn, a);
+    if (e == cudaSuccess) launched = true;
+    else cudaGetLastError();
   }
-  if (cs < 1) return h->fail(CUW_ERR_CUDA, "k_ortho_x: no cluster size could be launched");
+  if (!launched) return h->fail(CUW_ERR_UNSUPPORTED, "k_ortho_x: no cluster configuration fits NB");
+  ++h->launches;
   int st[2] = {0, 0};
   CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
