@@ -344,7 +344,7 @@ static void free_all(Handle* h) {
                   g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_off,
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.u, g.u2, g.eig, g.haux, g.gamn,
-                  g.work, g.wk2, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
+                  g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
                   g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -440,6 +440,8 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     TRYA(g.u2, sizeof(double) * nn);
     TRYA(g.eig, sizeof(double) * d.nb); TRYA(g.haux, sizeof(double) * nn); TRYA(g.gamn, sizeof(double) * nn);
     TRYA(g.work, sizeof(double) * nn); TRYA(g.wk2, sizeof(double) * nn);
+    TRYA(g.smat, sizeof(double) * nn); TRYA(g.emat, sizeof(double) * nn); TRYA(g.gt, sizeof(double) * nn);
+    TRYA(g.xb, sizeof(double) * nn); TRYA(g.tb, sizeof(double) * nn);
     TRYA(g.maxpart, sizeof(double) * 64); TRYA(g.ostatus, sizeof(int) * 16);
     TRYA(g.lam1c, sizeof(double2) * mn); TRYA(g.lam2c, sizeof(double2) * mn);
     TRYA(g.tmat, sizeof(double2) * 12 * mn);
@@ -452,6 +454,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
       break;
     }
     rc = small_tables_setup(h);
+    if (rc == CUW_OK) rc = gemm_setup(h);
   } while (0);
   if (rc != CUW_OK) {
     free_all(h);

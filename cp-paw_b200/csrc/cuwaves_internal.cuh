@@ -99,6 +99,7 @@ struct Device {
   double *lam = nullptr, *lam2 = nullptr;
   double *u = nullptr, *u2 = nullptr, *eig = nullptr;
   double *haux = nullptr, *gamn = nullptr, *work = nullptr, *wk2 = nullptr;
+  double *smat = nullptr, *emat = nullptr, *gt = nullptr, *xb = nullptr, *tb = nullptr;
   double *maxpart = nullptr;
   int *ostatus = nullptr;        // [0] status, [1] iterations
   double2 *lam1c = nullptr, *lam2c = nullptr;  // (NBH, NBH) folded multipliers
@@ -145,6 +146,7 @@ struct Handle {
   std::vector<cudaEvent_t> ev;
   std::vector<int> ev_phase;
   int nev = 0;
+  long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
   Device g;
   std::string err;
 
@@ -210,6 +212,7 @@ int band_reduce(Handle* h, int what, double* out_host, double* eig_host);
 int force_run(Handle* h, double* force_host);
 int force_gemm(Handle* h, const double2* ded, double* force_dev);
 int small_tables_setup(Handle* h);
+int gemm_setup(Handle* h);
 struct GramPair {
   const double2* x;
   const double2* y;

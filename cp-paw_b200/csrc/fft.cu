@@ -231,7 +231,9 @@ __device__ __forceinline__ void stage_fixed(double2* buf, int line0, int nl, int
   constexpr int BPT = bpt_of(R);
   constexpr int NQ = N / R;
   constexpr int TSTEP = N / (NS * R);
-  const int total = nl * NQ;
+  // jfast: index space nl*NQ (line = bf / NQ); otherwise the full chunk LC*NQ
+  // decoded modulo LC, with the lines beyond nl masked
+  const int total = jfast ? nl * NQ : LC * NQ;
   double2 v[BPT][R];
   int off_[BPT];
   bool act[BPT];

@@ -30,13 +30,15 @@ namespace cuw {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 8, LDS = 12, NT = 256;
+constexpr int BM = 64, BN = 64, BK = 16, LDS = 20, NT = 256;
+constexpr int TILE = BM * LDS;  // doubles of one real or imaginary tile part
+constexpr int EPT = BM * BK / NT;  // tile elements per thread and operand (4)
 
 // ---------------------------------------------------------------------------
 // warp-level complex MMA over one BK slice held in shared memory:
-// As[m][k], Bs[n][k] (real and imaginary parts separately).
+// As[m][k], Bs[n][k] (real and imaginary parts separately, row stride LDS,
+// a pattern free of bank conflicts for the m8n8k4 fragments).
 // Warp (wm, wn) in a 2x4 layout owns a 32x16 block: 4 x 2 tiles of 8x8.
-// conjA: use conj(A).
 // ---------------------------------------------------------------------------
 struct Acc {
   double r[4][2][2];
@@ -53,24 +55,25 @@ struct Acc {
 };
 
 template <bool CONJA>
-__device__ __forceinline__ void mma_slice(Acc& acc, const double (*Ar)[LDS], const double (*Ai)[LDS],
-                                          const double (*Br)[LDS], const double (*Bi)[LDS], int wm, int wn,
-                                          int lane) {
+__device__ __forceinline__ void mma_slice(Acc& acc, const double* Ar, const double* Ai, const double* Br,
+                                          const double* Bi, int wm, int wn, int lane) {
   const int r8 = lane >> 2, c4 = lane & 3;
 #pragma unroll
   for (int ks = 0; ks < BK / 4; ++ks) {
     double ar[4], ai[4], nai[4], br[2], bi[2];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
-      ar[mi] = Ar[wm * 32 + mi * 8 + r8][ks * 4 + c4];
-      double t = Ai[wm * 32 + mi * 8 + r8][ks * 4 + c4];
+      const int o = (wm * 32 + mi * 8 + r8) * LDS + ks * 4 + c4;
+      ar[mi] = Ar[o];
+      double t = Ai[o];
       ai[mi] = CONJA ? -t : t;
       nai[mi] = -ai[mi];
     }
 #pragma unroll
     for (int ni = 0; ni < 2; ++ni) {
-      br[ni] = Br[wn * 16 + ni * 8 + r8][ks * 4 + c4];
-      bi[ni] = Bi[wn * 16 + ni * 8 + r8][ks * 4 + c4];
+      const int o = (wn * 16 + ni * 8 + r8) * LDS + ks * 4 + c4;
+      br[ni] = Br[o];
+      bi[ni] = Bi[o];
     }
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
@@ -88,6 +91,95 @@ __device__ __forceinline__ void mma_slice(Acc& acc, const double (*Ar)[LDS], con
 __device__ __forceinline__ void acc_mn(int wm, int wn, int lane, int mi, int ni, int e, int& m, int& n) {
   m = wm * 32 + mi * 8 + (lane >> 2);
   n = wn * 16 + ni * 8 + 2 * (lane & 3) + e;
+}
+
+// element e of a thread's share of a 64 x BK tile -> (row, kk)
+template <bool KFAST>
+__device__ __forceinline__ void tile_rc(int e, int& row, int& kk) {
+  if (KFAST) { kk = e % BK; row = e / BK; }
+  else { row = e % BM; kk = e / BM; }
+}
+
+// Products of the main loop: A0*B0 (+ A1*B0 | + A0*B1 | gram: conj(A0)*B0 and A0*B1)
+enum { MP11 = 0, MP21 = 1, MP12 = 2, MPGRAM = 3 };
+
+// Double-buffered main loop over k in [kbeg, kend): the next slice is read from
+// global memory into registers while the DMMAs run on the current slice, then
+// stored into the other shared-memory stage; one barrier per slice.
+// fa0/fa1(row, k) and fb0/fb1(row, k) return the (bounds-checked) operands.
+template <int MODE, bool AKF, bool BKF, class FA0, class FA1, class FB0, class FB1>
+__device__ __forceinline__ void mainloop(double* sm, int kbeg, int kend, FA0 fa0, FA1 fa1, FB0 fb0, FB1 fb1,
+                                         Acc& acc0, Acc& acc1) {
+  constexpr int NA = (MODE == MP21) ? 2 : 1;
+  constexpr int NBO = (MODE == MP12 || MODE == MPGRAM) ? 2 : 1;
+  constexpr int STAGE = 2 * TILE * (NA + NBO);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  double2 ra[NA][EPT], rb[NBO][EPT];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      int row, kk;
+      tile_rc<AKF>(tid + q * NT, row, kk);
+      ra[0][q] = fa0(row, k0 + kk);
+      if (NA == 2) ra[NA - 1][q] = fa1(row, k0 + kk);
+      tile_rc<BKF>(tid + q * NT, row, kk);
+      rb[0][q] = fb0(row, k0 + kk);
+      if (NBO == 2) rb[NBO - 1][q] = fb1(row, k0 + kk);
+    }
+  };
+  auto store = [&](int st) {
+    double* base = sm + (size_t)st * STAGE;
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      int row, kk;
+      tile_rc<AKF>(tid + q * NT, row, kk);
+#pragma unroll
+      for (int x = 0; x < NA; ++x) {
+        base[(2 * x) * TILE + row * LDS + kk] = ra[x][q].x;
+        base[(2 * x + 1) * TILE + row * LDS + kk] = ra[x][q].y;
+      }
+      tile_rc<BKF>(tid + q * NT, row, kk);
+#pragma unroll
+      for (int x = 0; x < NBO; ++x) {
+        base[(2 * (NA + x)) * TILE + row * LDS + kk] = rb[x][q].x;
+        base[(2 * (NA + x) + 1) * TILE + row * LDS + kk] = rb[x][q].y;
+      }
+    }
+  };
+  if (kbeg >= kend) return;
+  fetch(kbeg);
+  store(0);
+  __syncthreads();
+  int st = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    const bool more = k0 + BK < kend;
+    if (more) fetch(k0 + BK);
+    const double* base = sm + (size_t)st * STAGE;
+    const double* A0r = base;
+    const double* A0i = base + TILE;
+    const double* B0r = base + 2 * NA * TILE;
+    const double* B0i = B0r + TILE;
+    if (MODE == MP11) {
+      mma_slice<false>(acc0, A0r, A0i, B0r, B0i, wm, wn, lane);
+    } else if (MODE == MP21) {
+      mma_slice<false>(acc0, A0r, A0i, B0r, B0i, wm, wn, lane);
+      mma_slice<false>(acc1, A0r + 2 * TILE, A0i + 2 * TILE, B0r, B0i, wm, wn, lane);
+    } else if (MODE == MP12) {
+      mma_slice<false>(acc0, A0r, A0i, B0r, B0i, wm, wn, lane);
+      mma_slice<false>(acc1, A0r, A0i, B0r + 2 * TILE, B0i + 2 * TILE, wm, wn, lane);
+    } else {
+      mma_slice<true>(acc0, A0r, A0i, B0r, B0i, wm, wn, lane);
+      mma_slice<false>(acc1, A0r, A0i, B0r + 2 * TILE, B0i + 2 * TILE, wm, wn, lane);
+    }
+    if (more) store(st ^ 1);
+    __syncthreads();
+    st ^= 1;
+  }
+}
+
+template <int MODE>
+constexpr size_t smem_bytes() {
+  return sizeof(double) * 2 * 2 * TILE * (((MODE == MP21) ? 2 : 1) + ((MODE == MP12 || MODE == MPGRAM) ? 2 : 1));
 }
 
 // PRO(g,p) generated from the tables
@@ -113,19 +205,20 @@ __global__ void k_eigr(const double* __restrict__ gx, const double* __restrict__
   }
 }
 
+__device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
+
 // ---------------------------------------------------------------------------
 // Projections: part[z][b + nbh*p] = sum_{g in split z} conj(PRO(g,p)) X(g,b)
-// for one or two operands X (psiA -> part, psiB -> part + stride).
+// for one or two operands X (psiA -> part, psiB -> part + dual_stride).
 // M = bands (blockIdx.y), N = projectors (blockIdx.x), K = g (blockIdx.z).
 // ---------------------------------------------------------------------------
 template <bool DUAL>
-__global__ void __launch_bounds__(NT) k_proj(const double2* __restrict__ psiA, const double2* __restrict__ psiB,
-                                             int ldg, int ngl, int nbh, int npro, int kchunk,
-                                             const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
-                                             const double* __restrict__ pro, const double2* __restrict__ eigr,
-                                             double2* __restrict__ part, size_t dual_stride) {
-  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS];
-  __shared__ double A2r[DUAL ? BM : 1][LDS], A2i[DUAL ? BM : 1][LDS];
+__global__ void __launch_bounds__(NT, 1) k_proj(const double2* __restrict__ psiA, const double2* __restrict__ psiB,
+                                                int ldg, int ngl, int nbh, int npro, int kchunk,
+                                                const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+                                                const double* __restrict__ pro, const double2* __restrict__ eigr,
+                                                double2* __restrict__ part, size_t dual_stride) {
+  extern __shared__ double sm[];
   __shared__ ProDesc sd[BN];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
   const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
@@ -134,40 +227,25 @@ __global__ void __launch_bounds__(NT) k_proj(const double2* __restrict__ psiA, c
     int p = n0 + tid;
     sd[tid] = p < npro ? pdesc[p] : ProDesc{0, 0, 0, 0};
   }
+  __syncthreads();
   Acc acc, acc2;
   acc.zero();
-  if (DUAL) acc2.zero();
-  for (int k0 = kbeg; k0 < kend; k0 += BK) {
-    __syncthreads();
-    // A tiles: X(g, b) -> As[b][g], coalesced along g
-    for (int i = tid; i < BM * BK; i += NT) {
-      int kk = i % BK, mm = i / BK;
-      int g = k0 + kk, b = m0 + mm;
-      double2 x = make_double2(0.0, 0.0), y = x;
-      if (g < kend && b < nbh) {
-        x = psiA[(size_t)g + (size_t)ldg * b];
-        if (DUAL) y = psiB[(size_t)g + (size_t)ldg * b];
-      }
-      Ar[mm][kk] = x.x;
-      Ai[mm][kk] = x.y;
-      if (DUAL) {
-        A2r[mm][kk] = y.x;
-        A2i[mm][kk] = y.y;
-      }
-    }
-    // B tile: conj(PRO(g, p)) -> Bs[p][g]
-    for (int i = tid; i < BN * BK; i += NT) {
-      int kk = i % BK, nn = i / BK;
-      int g = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (g < kend && n0 + nn < npro) v = gen_pro(g, ngl, sd[nn], ylm, pro, eigr);
-      Br[nn][kk] = v.x;
-      Bi[nn][kk] = -v.y;
-    }
-    __syncthreads();
-    mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
-    if (DUAL) mma_slice<false>(acc2, A2r, A2i, Br, Bi, wm, wn, lane);
-  }
+  acc2.zero();
+  auto fa0 = [&](int row, int g) {
+    int b = m0 + row;
+    return (g < kend && b < nbh) ? psiA[(size_t)g + (size_t)ldg * b] : zero2();
+  };
+  auto fa1 = [&](int row, int g) {
+    int b = m0 + row;
+    return (DUAL && g < kend && b < nbh) ? psiB[(size_t)g + (size_t)ldg * b] : zero2();
+  };
+  auto fb0 = [&](int row, int g) {
+    double2 v = zero2();
+    if (g < kend && n0 + row < npro) v = cconj(gen_pro(g, ngl, sd[row], ylm, pro, eigr));
+    return v;
+  };
+  if (DUAL) mainloop<MP21, true, true>(sm, kbeg, kend, fa0, fa1, fb0, fb0, acc, acc2);
+  else mainloop<MP11, true, true>(sm, kbeg, kend, fa0, fa0, fb0, fb0, acc, acc2);
   double2* out = part + (size_t)blockIdx.z * nbh * npro;
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
@@ -211,54 +289,36 @@ struct StepCoef {
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(NT) k_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi,
-                                               const double2* __restrict__ psi0, double2* __restrict__ psim,
-                                               const double* __restrict__ mpsi, int ldg, int ngl, int nbh,
-                                               int npro, const double2* __restrict__ c1,
-                                               const double2* __restrict__ c2, const ProDesc* __restrict__ pdesc,
-                                               const double* __restrict__ ylm, const double* __restrict__ pro,
-                                               const double2* __restrict__ eigr, StepCoef sc) {
+__global__ void __launch_bounds__(NT, 1) k_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi,
+                                                  const double2* __restrict__ psi0, double2* __restrict__ psim,
+                                                  const double* __restrict__ mpsi, int ldg, int ngl, int nbh,
+                                                  int npro, const double2* __restrict__ c1,
+                                                  const double2* __restrict__ c2, const ProDesc* __restrict__ pdesc,
+                                                  const double* __restrict__ ylm, const double* __restrict__ pro,
+                                                  const double2* __restrict__ eigr, StepCoef sc) {
   constexpr bool USE_H = (MODE != ADDPRO_OPSI);
   constexpr bool USE_O = (MODE != ADDPRO_HPSI);
-  __shared__ double Ar[BM][LDS], Ai[BM][LDS];
-  __shared__ double Br[USE_H ? BN : 1][LDS], Bi[USE_H ? BN : 1][LDS];
-  __shared__ double B2r[USE_O ? BN : 1][LDS], B2i[USE_O ? BN : 1][LDS];
+  extern __shared__ double sm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   Acc acc, acc2;
-  if (USE_H) acc.zero();
-  if (USE_O) acc2.zero();
-  for (int k0 = 0; k0 < npro; k0 += BK) {
-    __syncthreads();
-    // A tile: PRO(g, p) -> As[g][p]
-    for (int i = tid; i < BM * BK; i += NT) {
-      int mm = i % BM, kk = i / BM;
-      int g = m0 + mm, p = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (g < ngl && p < npro) v = gen_pro(g, ngl, pdesc[p], ylm, pro, eigr);
-      Ar[mm][kk] = v.x;
-      Ai[mm][kk] = v.y;
-    }
-    // B tiles: C(p, b) stored C[b + nbh*p] -> Bs[b][p]
-    for (int i = tid; i < BN * BK; i += NT) {
-      int nn = i % BN, kk = i / BN;
-      int b = n0 + nn, p = k0 + kk;
-      bool ok = (b < nbh && p < npro);
-      if (USE_H) {
-        double2 v = ok ? c1[(size_t)b + (size_t)nbh * p] : make_double2(0.0, 0.0);
-        Br[nn][kk] = v.x;
-        Bi[nn][kk] = v.y;
-      }
-      if (USE_O) {
-        double2 v = ok ? c2[(size_t)b + (size_t)nbh * p] : make_double2(0.0, 0.0);
-        B2r[nn][kk] = v.x;
-        B2i[nn][kk] = v.y;
-      }
-    }
-    __syncthreads();
-    if (USE_H) mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
-    if (USE_O) mma_slice<false>(acc2, Ar, Ai, B2r, B2i, wm, wn, lane);
-  }
+  acc.zero();
+  acc2.zero();
+  auto fa = [&](int row, int p) {
+    int g = m0 + row;
+    return (g < ngl && p < npro) ? gen_pro(g, ngl, pdesc[p], ylm, pro, eigr) : zero2();
+  };
+  auto fb1 = [&](int row, int p) {
+    int b = n0 + row;
+    return (b < nbh && p < npro) ? c1[(size_t)b + (size_t)nbh * p] : zero2();
+  };
+  auto fb2 = [&](int row, int p) {
+    int b = n0 + row;
+    return (b < nbh && p < npro) ? c2[(size_t)b + (size_t)nbh * p] : zero2();
+  };
+  if (MODE == ADDPRO_FUSED) mainloop<MP12, false, false>(sm, 0, npro, fa, fa, fb1, fb2, acc, acc2);
+  else if (MODE == ADDPRO_HPSI) mainloop<MP11, false, false>(sm, 0, npro, fa, fa, fb1, fb1, acc, acc2);
+  else mainloop<MP11, false, false>(sm, 0, npro, fa, fa, fb2, fb2, acc2, acc);
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -306,9 +366,10 @@ struct GramArgs {
   int kchunk;
 };
 
-template <bool MINUS>
-__global__ void __launch_bounds__(NT) k_gram(GramArgs a, const int* __restrict__ minusg, double2* __restrict__ part) {
-  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS], B2r[BN][LDS], B2i[BN][LDS];
+template <bool MINUS, bool KFAST>
+__global__ void __launch_bounds__(NT, 1) k_gram(GramArgs a, const int* __restrict__ minusg,
+                                                double2* __restrict__ part) {
+  extern __shared__ double sm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
   const int pair = blockIdx.z % a.npair, split = blockIdx.z / a.npair;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -318,34 +379,21 @@ __global__ void __launch_bounds__(NT) k_gram(GramArgs a, const int* __restrict__
   Acc t1, t2;
   t1.zero();
   t2.zero();
-  const bool kfast = (a.sk == 1);
-  for (int k0 = kbeg; k0 < kend; k0 += BK) {
-    __syncthreads();
-    for (int i = tid; i < BM * BK; i += NT) {
-      int kk, mm;
-      if (kfast) { kk = i % BK; mm = i / BK; }
-      else { mm = i % BM; kk = i / BM; }
-      int k = k0 + kk;
-      bool okk = k < kend;
-      double2 x = make_double2(0.0, 0.0);
-      if (okk && m0 + mm < a.nm) x = X[(size_t)k * a.sk + (size_t)(m0 + mm) * a.sm];
-      Ar[mm][kk] = x.x;
-      Ai[mm][kk] = x.y;
-      double2 y = make_double2(0.0, 0.0), y2 = y;
-      if (okk && n0 + mm < a.nn) {
-        y = Y[(size_t)k * a.sk + (size_t)(n0 + mm) * a.sm];
-        if (MINUS) y2 = Y[(size_t)minusg[k] * a.sk + (size_t)(n0 + mm) * a.sm];
-        else y2 = y;
-      }
-      Br[mm][kk] = y.x;
-      Bi[mm][kk] = y.y;
-      B2r[mm][kk] = y2.x;
-      B2i[mm][kk] = y2.y;
-    }
-    __syncthreads();
-    mma_slice<true>(t1, Ar, Ai, Br, Bi, wm, wn, lane);
-    mma_slice<false>(t2, Ar, Ai, B2r, B2i, wm, wn, lane);
-  }
+  auto fa = [&](int row, int k) {
+    int m = m0 + row;
+    return (k < kend && m < a.nm) ? X[(size_t)k * a.sk + (size_t)m * a.sm] : zero2();
+  };
+  auto fb = [&](int row, int k) {
+    int n = n0 + row;
+    return (k < kend && n < a.nn) ? Y[(size_t)k * a.sk + (size_t)n * a.sm] : zero2();
+  };
+  auto fb2 = [&](int row, int k) {
+    int n = n0 + row;
+    if (!(k < kend && n < a.nn)) return zero2();
+    int kk = MINUS ? minusg[k] : k;
+    return Y[(size_t)kk * a.sk + (size_t)n * a.sm];
+  };
+  mainloop<MPGRAM, KFAST, KFAST>(sm, kbeg, kend, fa, fa, fb, fb2, t1, t2);
   const size_t mn = (size_t)a.nm * a.nn;
   double2* o1 = part + ((size_t)blockIdx.z * 2 + 0) * mn;
   double2* o2 = part + ((size_t)blockIdx.z * 2 + 1) * mn;
@@ -367,7 +415,6 @@ __global__ void __launch_bounds__(NT) k_gram(GramArgs a, const int* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// out(m, n) += sum_k X(k... see below
 //   ADDOPSI form (XMINUS): out(g,n) += sum_k X(g,k) L1(k,n) + conj(X(-g,k)) L2(k,n)
 //   ADDOPROJ form       : out(p,n) += sum_k X(p,k) L1(k,n) + conj(X(p,k)) L2(k,n)
 // X element (m, k) at X[m*sxm + k*sxk]; out element (m, n) at out[m*som + n*son];
@@ -382,48 +429,27 @@ struct AddXArgs {
   size_t sxm, sxk, som, son;
 };
 
-template <bool XMINUS>
-__global__ void __launch_bounds__(NT) k_addx(AddXArgs a, const int* __restrict__ minusg) {
-  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS];
+template <bool XMINUS, bool MFAST>
+__global__ void __launch_bounds__(NT, 1) k_addx(AddXArgs a, const int* __restrict__ minusg) {
+  extern __shared__ double sm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  Acc acc;
+  Acc acc, dummy;
   acc.zero();
   const int ktot = 2 * a.nk;
-  const bool mfast = (a.sxm == 1);
-  for (int k0 = 0; k0 < ktot; k0 += BK) {
-    __syncthreads();
-    for (int i = tid; i < BM * BK; i += NT) {
-      int mm, kk;
-      if (mfast) { mm = i % BM; kk = i / BM; }
-      else { kk = i % BK; mm = i / BK; }
-      int kg = k0 + kk, m = m0 + mm;
-      double2 v = make_double2(0.0, 0.0);
-      if (m < a.nm && kg < ktot) {
-        if (kg < a.nk) v = a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
-        else {
-          int k = kg - a.nk;
-          int mm2 = XMINUS ? minusg[m] : m;
-          v = cconj(a.x[(size_t)mm2 * a.sxm + (size_t)k * a.sxk]);
-        }
-      }
-      Ar[mm][kk] = v.x;
-      Ai[mm][kk] = v.y;
-    }
-    for (int i = tid; i < BN * BK; i += NT) {
-      int kk = i % BK, nn = i / BK;
-      int kg = k0 + kk, n = n0 + nn;
-      double2 v = make_double2(0.0, 0.0);
-      if (n < a.nn && kg < ktot) {
-        if (kg < a.nk) v = a.l1[(size_t)kg + (size_t)a.nk * n];
-        else v = a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
-      }
-      Br[nn][kk] = v.x;
-      Bi[nn][kk] = v.y;
-    }
-    __syncthreads();
-    mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
-  }
+  auto fa = [&](int row, int kg) {
+    int m = m0 + row;
+    if (!(m < a.nm && kg < ktot)) return zero2();
+    if (kg < a.nk) return a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
+    int mm2 = XMINUS ? minusg[m] : m;
+    return cconj(a.x[(size_t)mm2 * a.sxm + (size_t)(kg - a.nk) * a.sxk]);
+  };
+  auto fb = [&](int row, int kg) {
+    int n = n0 + row;
+    if (!(n < a.nn && kg < ktot)) return zero2();
+    return kg < a.nk ? a.l1[(size_t)kg + (size_t)a.nk * n] : a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
+  };
+  mainloop<MP11, !MFAST, true>(sm, 0, ktot, fa, fa, fb, fb, acc, dummy);
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -450,39 +476,27 @@ __global__ void __launch_bounds__(NT) k_addx(AddXArgs a, const int* __restrict__
 // cancels in this sum (c(-G) = -conj(c(G)) for c = i Y P (-i)^l EIGR over the
 // full sphere), so it is not applied.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) k_force(const double2* __restrict__ psi0, int ldg, int ngl, int nbh, int npro,
-                                              const double2* __restrict__ ded, const ProDesc* __restrict__ pdesc,
-                                              const double* __restrict__ ylm, const double* __restrict__ pro,
-                                              const double2* __restrict__ eigr, const double* __restrict__ gx,
-                                              const double* __restrict__ gy, const double* __restrict__ gz,
-                                              double* __restrict__ fpart) {
-  __shared__ double Ar[BM][LDS], Ai[BM][LDS], Br[BN][LDS], Bi[BN][LDS];
-  __shared__ double fred[BN][3][4];  // per projector, per warp row-group (wm) x 2 halves
+__global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi0, int ldg, int ngl, int nbh,
+                                                 int npro, const double2* __restrict__ ded,
+                                                 const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+                                                 const double* __restrict__ pro, const double2* __restrict__ eigr,
+                                                 const double* __restrict__ gx, const double* __restrict__ gy,
+                                                 const double* __restrict__ gz, double* __restrict__ fpart) {
+  extern __shared__ double sm[];
+  __shared__ double fred[BN][3][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  Acc acc;
+  Acc acc, dummy;
   acc.zero();
-  for (int k0 = 0; k0 < nbh; k0 += BK) {
-    __syncthreads();
-    for (int i = tid; i < BM * BK; i += NT) {
-      int mm = i % BM, kk = i / BM;
-      int g = m0 + mm, b = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (g < ngl && b < nbh) v = psi0[(size_t)g + (size_t)ldg * b];
-      Ar[mm][kk] = v.x;
-      Ai[mm][kk] = v.y;
-    }
-    for (int i = tid; i < BN * BK; i += NT) {
-      int kk = i % BK, nn = i / BK;
-      int b = k0 + kk, p = n0 + nn;
-      double2 v = make_double2(0.0, 0.0);
-      if (b < nbh && p < npro) v = ded[(size_t)b + (size_t)nbh * p];
-      Br[nn][kk] = v.x;
-      Bi[nn][kk] = -v.y;
-    }
-    __syncthreads();
-    mma_slice<false>(acc, Ar, Ai, Br, Bi, wm, wn, lane);
-  }
+  auto fa = [&](int row, int b) {
+    int g = m0 + row;
+    return (g < ngl && b < nbh) ? psi0[(size_t)g + (size_t)ldg * b] : zero2();
+  };
+  auto fb = [&](int row, int b) {
+    int p = n0 + row;
+    return (b < nbh && p < npro) ? cconj(ded[(size_t)b + (size_t)nbh * p]) : zero2();
+  };
+  mainloop<MP11, false, true>(sm, 0, nbh, fa, fa, fb, fb, acc, dummy);
   // epilogue: per (g, p) contribution, reduced over g
   double f[2][2][3];
 #pragma unroll
@@ -524,7 +538,6 @@ __global__ void __launch_bounds__(NT) k_force(const double2* __restrict__ psi0, 
         v += __shfl_xor_sync(0xffffffffu, v, 16);
         f[ni][e][c] = v;
       }
-  __syncthreads();
   if (lane < 4) {
 #pragma unroll
     for (int ni = 0; ni < 2; ++ni)
@@ -650,10 +663,10 @@ int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* 
   CUW_RET(ensure_part(h, sizeof(double2) * one * (dual ? 2 : 1)));
   dim3 grid(tn, tm, ks);
   if (dual)
-    k_proj<true><<<grid, NT, 0, h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
+    k_proj<true><<<grid, NT, smem_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
                                              h->g.pro, h->g.eigr, h->g.part, one);
   else
-    k_proj<false><<<grid, NT, 0, h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
+    k_proj<false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
                                               h->g.pro, h->g.eigr, h->g.part, 0);
   CUW_LAUNCH_CHECK("k_proj");
   const size_t n = (size_t)nbh * npro;
@@ -678,15 +691,15 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
   Device& g = h->g;
   switch (mode) {
     case ADDPRO_HPSI:
-      k_addpro<ADDPRO_HPSI><<<grid, NT, 0, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
+      k_addpro<ADDPRO_HPSI><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
                                                          hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
       break;
     case ADDPRO_OPSI:
-      k_addpro<ADDPRO_OPSI><<<grid, NT, 0, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
+      k_addpro<ADDPRO_OPSI><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
                                                          hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
       break;
     default:
-      k_addpro<ADDPRO_FUSED><<<grid, NT, 0, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh,
+      k_addpro<ADDPRO_FUSED><<<grid, NT, smem_bytes<MP12>(), h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh,
                                                           npro, hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
   }
   CUW_LAUNCH_CHECK("k_addpro");
@@ -740,8 +753,8 @@ static int gram_run(Handle* h, const GramPair* pairs, int npair, bool minus, int
   const size_t mn = (size_t)nm * nm;
   CUW_RET(ensure_part(h, sizeof(double2) * mn * 2 * npair * ks));
   dim3 grid(ceil_div(nm, BN), ceil_div(nm, BM), ks * npair);
-  if (minus) k_gram<true><<<grid, NT, 0, h->stream>>>(a, h->g.minusg, h->g.part);
-  else k_gram<false><<<grid, NT, 0, h->stream>>>(a, h->g.minusg, h->g.part);
+  if (minus) k_gram<true, true><<<grid, NT, smem_bytes<MPGRAM>(), h->stream>>>(a, h->g.minusg, h->g.part);
+  else k_gram<false, false><<<grid, NT, smem_bytes<MPGRAM>(), h->stream>>>(a, h->g.minusg, h->g.part);
   CUW_LAUNCH_CHECK("k_gram");
   // reduce over splits: layout part[(split*npair+pair)*2+t] -> dst[(pair*2+t)]
   const size_t n = mn * 2 * npair;
@@ -773,7 +786,7 @@ int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* 
   a.som = 1;
   a.son = (size_t)h->ldg;
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
-  k_addx<true><<<grid, NT, 0, h->stream>>>(a, h->g.minusg);
+  k_addx<true, true><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
   return CUW_OK;
 }
@@ -792,7 +805,7 @@ int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* 
   a.som = (size_t)h->d.nbh;  // out(m=p, n=b) at b + nbh*p
   a.son = 1;
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
-  k_addx<false><<<grid, NT, 0, h->stream>>>(a, h->g.minusg);
+  k_addx<false, false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
   return CUW_OK;
 }
@@ -802,13 +815,35 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
   const int tm = ceil_div(ngl, BM), tn = ceil_div(npro, BN);
   CUW_RET(ensure_part(h, sizeof(double) * 3 * (size_t)tm * npro));
   double* fpart = reinterpret_cast<double*>(h->g.part);
-  k_force<<<dim3(tm, tn), NT, 0, h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro,
+  k_force<<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro,
                                               h->g.eigr, h->g.gx, h->g.gy, h->g.gz, fpart);
   CUW_LAUNCH_CHECK("k_force");
   TabView t = tables(h);
   k_force_final<<<dim3(3, h->d.nat), 128, 0, h->stream>>>(fpart, tm, npro, t.ipro0, t.nlmn, h->d.nat, h->gweight,
                                                           force_dev);
   CUW_LAUNCH_CHECK("k_force_final");
+  return CUW_OK;
+}
+
+// dynamic shared memory above 48 KB for the pipelined contraction kernels
+int gemm_setup(Handle* h) {
+  CUW_TRY(cudaFuncSetAttribute(k_proj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<MP21>()));
+  CUW_TRY(cudaFuncSetAttribute(k_proj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<MP11>()));
+  CUW_TRY(cudaFuncSetAttribute(k_addpro<ADDPRO_HPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MP11>()));
+  CUW_TRY(cudaFuncSetAttribute(k_addpro<ADDPRO_OPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MP11>()));
+  CUW_TRY(cudaFuncSetAttribute(k_addpro<ADDPRO_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MP12>()));
+  CUW_TRY(cudaFuncSetAttribute(k_gram<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MPGRAM>()));
+  CUW_TRY(cudaFuncSetAttribute(k_gram<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MPGRAM>()));
+  CUW_TRY(cudaFuncSetAttribute(k_addx<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MP11>()));
+  CUW_TRY(cudaFuncSetAttribute(k_addx<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<MP11>()));
+  CUW_TRY(cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<MP11>()));
   return CUW_OK;
 }
 

@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
   int* pq = pp + np;                                     // np
   int* flag = pq + np;                                   // 1
   double* V = v_in_smem ? reinterpret_cast<double*>(flag + 2) : vglob;
+  // (P, Q) of every 2x2 block, packed P | Q << 16, after V (or after flag)
+  int* pqtab = v_in_smem ? reinterpret_cast<int*>(V + (size_t)n * n) : (flag + 2);
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int j = tid; j < n; j += nt)
     for (int i = 0; i <= j; ++i) A[pk(i, j)] = s_in[i + (size_t)n * j];
@@ -110,6 +112,8 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
     int i = (int)(k % n), j = (int)(k / n);
     V[k] = (i == j) ? 1.0 : 0.0;
   }
+  for (int Q = tid; Q < np; Q += nt)
+    for (int P = 0; P <= Q; ++P) pqtab[Q * (Q + 1) / 2 + P] = P | (Q << 16);
   __syncthreads();
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
@@ -125,8 +129,9 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
         pq[tid] = q;
         double apq = A[pk(p, q)], app = A[pk(p, p)], aqq = A[pk(q, q)];
         double c = 1.0, s = 0.0;
-        // rotate unless |apq| is at the rounding level of the diagonal (4 ulp)
-        if (apq != 0.0 && fabs(apq) > 8.9e-16 * sqrt(fabs(app * aqq))) {
+        // rotate unless |apq| <= 1e-14 sqrt(|app aqq|): below that the eigenvectors
+        // are exact to ~1e-14, and rounding noise alone keeps |apq| near 1e-16
+        if (apq != 0.0 && fabs(apq) > 1e-14 * sqrt(fabs(app * aqq))) {
           double theta = (aqq - app) / (2.0 * apq);
           double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
           c = 1.0 / sqrt(t * t + 1.0);
@@ -140,11 +145,8 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
       // 2x2 blocks between pair P and pair Q (P <= Q), np*(np+1)/2 of them
       const int nblk = np * (np + 1) / 2;
       for (int k = tid; k < nblk; k += nt) {
-        // decode k -> (P, Q) with P <= Q
-        int Q = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
-        while ((Q + 1) * (Q + 2) / 2 <= k) ++Q;
-        while (Q * (Q + 1) / 2 > k) --Q;
-        int P = k - Q * (Q + 1) / 2;
+        const int pqv = pqtab[k];
+        const int P = pqv & 0xffff, Q = pqv >> 16;
         int p = pp[P], q = pq[P], r2 = pp[Q], s2 = pq[Q];
         double cP = rc[P], sP = rs[P], cQ = rc[Q], sQ = rs[Q];
         if (P == Q) {
@@ -210,6 +212,15 @@ struct OrthoArgs {
   int max_iter;
   double eps;
   int kc;
+  // eigenbasis U of an earlier CHIPSI: U^T sym(CHIPSI) U = diag(e) + emat.
+  // use_e = 0: emat is zero (U diagonalises the current matrix exactly)
+  const double* emat;
+  int use_e;
+  int max_inner;
+  double* gt;     // Gamma in the U basis
+  double* xb;     // second buffer of the Lyapunov fixed point
+  double* tb;     // E X
+  int* inner;     // total inner iterations (diagnostics)
 };
 
 // C(tile) = op(A) * op(B); op = transpose when tA / tB.  The tile
@@ -303,6 +314,7 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   const int tid = threadIdx.x, nt = blockDim.x;
   double* lam = a.lam;
   double* lamn = a.lam2;
+  __shared__ double red[256];
   int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
   for (int iter = 1; iter <= a.max_iter; ++iter) {
     // HAUX = CHICHI * LAMBDA + 2 CHIPSI
@@ -329,7 +341,6 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
       if (v != v) mx = INFINITY;
     }
     // block max
-    __shared__ double red[256];
     red[tid] = mx;
     __syncthreads();
     for (int s = nt / 2; s > 0; s >>= 1) {
@@ -353,15 +364,64 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     // HAUX = U^T W
     gemm_tile<MR, MC>(a.u, true, a.w, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
     csync();
-    // GAMN = (HAUX U) / (e_i + e_j)
-    gemm_tile<MR, MC>(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
+    // GT = HAUX U (Gamma in the U basis);  X = GT / (e_i + e_j)
+    gemm_tile<MR, MC>(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gt, smA, smB, kc);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
-      a.gamn[i + (size_t)n * j] = __ldcg(&a.gamn[i + (size_t)n * j]) / (a.e[i] + a.e[j]);
+      a.gamn[i + (size_t)n * j] = __ldcg(&a.gt[i + (size_t)n * j]) / (a.e[i] + a.e[j]);
     }
     csync();
-    // HAUX = U GAMN
-    gemm_tile<MR, MC>(a.u, false, a.gamn, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    // When U diagonalises an earlier CHIPSI only, D X + X D = GT - E X - X E is
+    // solved by the fixed point X <- (GT - E X - X E)/(e_i + e_j) to rounding
+    // level: the same Lyapunov solution as the eigendecomposition of the
+    // current matrix (E, X symmetric, so X E = (E X)^T).
+    double* xcur = a.gamn;
+    double* xnext = a.xb;
+    if (a.use_e) {
+      for (int it2 = 0; it2 < a.max_inner; ++it2) {
+        gemm_tile<MR, MC>(a.emat, false, xcur, false, n, i0, i1, j0, j1, a.tb, smA, smB, kc);
+        csync();
+        double dx = 0.0, xm = 0.0;
+        for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
+          int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
+          double xn = (__ldcg(&a.gt[i + (size_t)n * j]) - __ldcg(&a.tb[i + (size_t)n * j]) -
+                       __ldcg(&a.tb[j + (size_t)n * i])) / (a.e[i] + a.e[j]);
+          dx = fmax(dx, fabs(xn - __ldcg(&xcur[i + (size_t)n * j])));
+          xm = fmax(xm, fabs(xn));
+          xnext[i + (size_t)n * j] = xn;
+        }
+        red[tid] = dx;
+        __syncthreads();
+        for (int s2 = nt / 2; s2 > 0; s2 >>= 1) {
+          if (tid < s2) red[tid] = fmax(red[tid], red[tid + s2]);
+          __syncthreads();
+        }
+        if (tid == 0) a.maxpart[rank] = red[0];
+        __syncthreads();
+        red[tid] = xm;
+        __syncthreads();
+        for (int s2 = nt / 2; s2 > 0; s2 >>= 1) {
+          if (tid < s2) red[tid] = fmax(red[tid], red[tid + s2]);
+          __syncthreads();
+        }
+        if (tid == 0) a.maxpart[cs + rank] = red[0];
+        csync();
+        double gdx = 0.0, gxm = 0.0;
+        for (int r = 0; r < cs; ++r) {
+          gdx = fmax(gdx, __ldcg(&a.maxpart[r]));
+          gxm = fmax(gxm, __ldcg(&a.maxpart[cs + r]));
+        }
+        double* tmpx = xcur;
+        xcur = xnext;
+        xnext = tmpx;
+        if (rank == 0 && tid == 0) a.inner[0] += 1;
+        if (gdx <= 1e-16 * gxm) break;
+        // the next phase overwrites maxpart and tb only after this barrier
+        csync();
+      }
+    }
+    // HAUX = U X
+    gemm_tile<MR, MC>(a.u, false, xcur, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
     csync();
     // W = HAUX U^T
     gemm_tile<MR, MC>(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB, kc);
@@ -576,7 +636,8 @@ int lambda12_run(Handle* h, const double* lam_real, double2* l1, double2* l2) {
 int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
   const int n = h->d.nb;
   const size_t packed = (size_t)n * (n + 1) / 2;
-  const size_t base = sizeof(double) * (packed + n) + sizeof(int) * (n + 2) + 16;
+  const size_t tab = sizeof(int) * (size_t)(n / 2) * (n / 2 + 1) / 2;
+  const size_t base = sizeof(double) * (packed + n) + sizeof(int) * (n + 2) + 16 + tab;
   size_t smem = base + sizeof(double) * (size_t)n * n;
   int v_in_smem = 1;
   if (smem > 220 * 1024) {
@@ -593,26 +654,73 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
 
 // Full WAVES_ORTHO_X: matrices mat (PSIPSI), omat (CHIPSI), oomat (CHICHI) and
 // the starting lambda are in h->g.{mat,omat,oomat,lam}.
+// diag(B) -> e, B with its diagonal removed -> E; [0] max|E|, [1] min e into out
+__global__ void k_split_diag(const double* __restrict__ b, int n, double* __restrict__ e, double* __restrict__ emat,
+                             double* __restrict__ out) {
+  __shared__ double rmax[256], rmin[256];
+  double mx = 0.0, mn = INFINITY;
+  for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+    int i = k % n, j = k / n;
+    double v = b[k];
+    if (i == j) {
+      e[i] = v;
+      emat[k] = 0.0;
+      mn = fmin(mn, v);
+    } else {
+      emat[k] = v;
+      mx = fmax(mx, fabs(v));
+    }
+  }
+  rmax[threadIdx.x] = mx;
+  rmin[threadIdx.x] = mn;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      rmax[threadIdx.x] = fmax(rmax[threadIdx.x], rmax[threadIdx.x + s]);
+      rmin[threadIdx.x] = fmin(rmin[threadIdx.x], rmin[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = rmax[0];
+    out[1] = rmin[0];
+  }
+}
+
 int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   const int n = h->d.nb;
   Device& g = h->g;
-  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.gamn);
+  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.smat);
   CUW_LAUNCH_CHECK("k_symmetrize");
+  int use_e = 0;
+  const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
   if (h->have_u) {
-    // warm start: diagonalise U_prev^T S U_prev, then U = U_prev V.  Any
-    // orthogonal eigenbasis of S gives the same Lyapunov operator of ORTHO_X.
-    dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
-    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.gamn, 0, g.u, 0, n, g.haux);
+    // B = U^T S U with U from an earlier diagonalisation
+    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.smat, 0, g.u, 0, n, g.haux);
     CUW_LAUNCH_CHECK("k_small_gemm");
     k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 1, g.haux, 0, n, g.work);
     CUW_LAUNCH_CHECK("k_small_gemm");
-    CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig));
-    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2);
-    CUW_LAUNCH_CHECK("k_small_gemm");
-    std::swap(g.u, g.u2);
+    k_split_diag<<<1, 256, 0, h->stream>>>(g.work, n, g.eig, g.emat, g.scal + 2 * n + 8);
+    CUW_LAUNCH_CHECK("k_split_diag");
+    double st2[2];
+    CUW_TRY(cudaMemcpyAsync(st2, g.scal + 2 * n + 8, sizeof(st2), cudaMemcpyDeviceToHost, h->stream));
+    CUW_TRY(cudaStreamSynchronize(h->stream));
+    // contraction bound of the fixed point: n max|E| / min(e)
+    const double rho = st2[1] > 0.0 ? n * st2[0] / st2[1] : 1e300;
+    if (rho < 0.1) {
+      use_e = 1;
+    } else {
+      // rediagonalise: Jacobi on the nearly diagonal B, then U <- U V
+      CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig));
+      k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2);
+      CUW_LAUNCH_CHECK("k_small_gemm");
+      std::swap(g.u, g.u2);
+      ++h->n_rediag;
+    }
   } else {
-    CUW_RET(jacobi_run(h, g.gamn, g.u, g.eig));
+    CUW_RET(jacobi_run(h, g.smat, g.u, g.eig));
     h->have_u = true;
+    ++h->n_rediag;
   }
   OrthoArgs a;
   a.n = n;
@@ -631,6 +739,13 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   a.status = g.ostatus;
   a.max_iter = max_iter;
   a.eps = eps;
+  a.emat = g.emat;
+  a.use_e = use_e;
+  a.max_inner = 60;
+  a.gt = g.gt;
+  a.xb = g.xb;
+  a.tb = g.tb;
+  a.inner = g.ostatus + 8;
   // cluster of 16 CTAs (non-portable size), else 8, 4, ... ; tile rows/cols
   // per CTA are at most 16*MR x 16*MC with MR, MC in {1,2,4}
   cudaLaunchConfig_t cfg = {};
