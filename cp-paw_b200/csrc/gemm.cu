@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "cuwaves_internal.cuh"
 
@@ -888,3 +889,77 @@ int small_tables_setup(Handle* h) {
 }
 
 }  // namespace cuw
+
+// ===========================================================================
+// No-allocation projections.
+//
+// Some callers cannot allocate device memory at all: a host code that hands
+// out device memory only from its own pool, a plug-in running inside another
+// program's CUDA graph capture or under a memory cap, or a process that must
+// not grow its footprint after start-up.  cuwaves_projections_noalloc gives
+// them <p|psi> with no cudaMalloc, cudaFree or allocating library call: the
+// split-K partial sums live in the file-scope array below.  Every GPU that
+// loads this library holds the array (CUW_NOALLOC_SCRATCH_BYTES) until the
+// process exits.
+// ===========================================================================
+
+#define CUW_NOALLOC_SCRATCH_ELEMS (1u << 18) /* complex doubles: 4 MiB */
+static __device__ __align__(256) double2 g_noalloc_scratch[CUW_NOALLOC_SCRATCH_ELEMS];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double2* g_noalloc_ptr[kMaxDevices] = {nullptr};
+}  // namespace
+
+// Device address of the scratch array on the current device; looked up once per
+// device (the host-side name of a __device__ array is not a device address).
+static int noalloc_scratch(double2** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CUW_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return CUW_ERR_CUDA;
+    if (cudaFuncSetAttribute(cuw::k_proj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)cuw::smem_bytes<cuw::MP11>()) != cudaSuccess)
+      return CUW_ERR_CUDA;
+    g_noalloc_ptr[dev] = static_cast<double2*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_projections_noalloc(int ngl, int ldg, int nbh, int nat, int npro, const double* psi,
+                                           const int* pdesc, const double* ylm, const double* pro,
+                                           const double* eigr, double gweight, double* proj, void* stream) {
+  using namespace cuw;
+  if (ngl <= 0 || ldg < ngl || nbh <= 0 || nat <= 0 || npro <= 0 || !psi || !pdesc || !ylm || !pro || !eigr ||
+      !proj)
+    return CUW_ERR_ARG;
+  // one split needs nbh*npro complex partial sums
+  const size_t per_split = (size_t)nbh * npro;
+  if (per_split > CUW_NOALLOC_SCRATCH_ELEMS) return CUW_ERR_ARG;
+  double2* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc != CUW_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int nsm = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int tn = ceil_div(npro, BN), tm = ceil_div(nbh, BM);
+  int ks = std::max(1, std::min(ceil_div(2 * nsm, tn * tm), ceil_div(ngl, 256)));
+  ks = std::min<int>(ks, (int)(CUW_NOALLOC_SCRATCH_ELEMS / per_split));
+  const int kchunk = ceil_div(ceil_div(ngl, ks), BK) * BK;
+  ks = ceil_div(ngl, kchunk);
+  // every partial sum that the reduction reads is written by k_proj in this
+  // call, so nothing in the array has to start at zero
+  k_proj<false><<<dim3(tn, tm, ks), NT, smem_bytes<MP11>(), st>>>(
+      reinterpret_cast<const double2*>(psi), nullptr, ldg, ngl, nbh, npro, kchunk,
+      reinterpret_cast<const ProDesc*>(pdesc), ylm, pro, reinterpret_cast<const double2*>(eigr), scratch, 0);
+  if (cudaGetLastError() != cudaSuccess) return CUW_ERR_CUDA;
+  const int rb = std::min(ceil_div((int)per_split, 256), 4 * nsm);
+  k_reduce_parts<<<rb, 256, 0, st>>>(scratch, ks, per_split, per_split, gweight, reinterpret_cast<double2*>(proj));
+  if (cudaGetLastError() != cudaSuccess) return CUW_ERR_CUDA;
+  return CUW_OK;
+}

@@ -82,6 +82,8 @@ OPTIONAL = {
     "set_timing": [_P, C.c_int],
     "get_timing": [_P, _D, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "get_stream": [_P, C.POINTER(C.c_void_p)],
+    # device-pointer variant without allocation (no handle)
+    "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
     "get_atoms": [_P, _D, _D, _D],
     "set_threads": [_P, C.c_int],
 }

@@ -160,6 +160,26 @@ int cuwaves_set_timing(cuw_handle* h, int enable);
 int cuwaves_get_timing(cuw_handle* h, double* ms, int n, long long* launches, long long* steps);
 int cuwaves_get_stream(cuw_handle* h, void** stream);
 
+/* Projections without any device allocation: PROJ(b,p) = gweight * sum_G
+ * conj(PRO(G,p)) psi(G,b), the contraction of cuwaves_projections, for callers
+ * that cannot call cudaMalloc (memory handed out only by a host pool, code
+ * running under another program's memory cap or inside its stream capture).
+ * There is no counterpart in the reference; WAVES_PROJECTIONS
+ * (src/paw_waves1.f90:5746-5905) computes the same numbers on the host.
+ * Every argument is a device pointer the caller owns:
+ *   psi(ldg,nbh) complex, pdesc(4,npro) int (0-based atom, column of pro, LM, L
+ *   of each projector), ylm(ngl,LMX), pro(ngl,NBAREPRO), eigr(ngl,nat) complex
+ *   exp(-iG.R), proj(nbh,npro) complex output; stream is a cudaStream_t (NULL:
+ *   the default stream).  Work is only enqueued on `stream`.
+ * Its split-K partial sums use one static device array of 4 MiB that every GPU
+ * loading this library holds until exit, so nbh*npro may not exceed 262144
+ * (CUW_ERR_ARG otherwise).  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+int cuwaves_projections_noalloc(int ngl, int ldg, int nbh, int nat, int npro, const double* psi,
+                                const int* pdesc, const double* ylm, const double* pro,
+                                const double* eigr, double gweight, double* proj, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
