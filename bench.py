@@ -223,7 +223,8 @@ def run_cuda(args, rank, world, local):
     peaks, peak_src = measured_peaks()
     result = {"phases_ms_per_step": {k: v / max(1, nsteps) for k, v in phases.items()},
               "launches": launches, "ms": ms, "ms_e2e": ms_e2e, "h2d": h2d, "d2h": d2h,
-              "clocks": clk.summary(), "fm": fm, "iters_last": float(out[4]), "etot_last": float(out[0])}
+              "clocks": clk.summary(), "fm": fm, "iters_last": float(out[4]), "etot_last": float(out[0]),
+              "ortho": w.ortho_stats()}
     if rank == 0:
         p64 = fp64_peak_tflops(torch)
         result["fp64_peak"] = p64
@@ -265,6 +266,7 @@ def emit_cuda(args, res, world):
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "traffic": traffic, "flops_per_launch": flops},
         "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()},
+        "ortho_solve": res.get("ortho"),
         "clocks": res["clocks"],
         "cpu_baseline": cpu,
     }

@@ -343,7 +343,7 @@ static void free_all(Handle* h) {
   void* ptrs[] = {g.psi0, g.psim, g.hpsi, g.opsi, g.proj, g.oproj, g.hproj, g.pbuf, g.rlam0, g.rlamm, g.igvec,
                   g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_off,
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
-                  g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.u, g.u2, g.eig, g.haux, g.gamn,
+                  g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
                   g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
                   g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox};
   for (void* p : ptrs)
@@ -436,7 +436,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     TRYA(g.dover, sizeof(double) * (size_t)h->lnxx * h->lnxx * d.nsp);
     TRYA(g.occ, sizeof(double) * d.nb);
     TRYA(g.mat, sizeof(double) * nn); TRYA(g.omat, sizeof(double) * nn); TRYA(g.oomat, sizeof(double) * nn);
-    TRYA(g.lam, sizeof(double) * nn); TRYA(g.lam2, sizeof(double) * nn); TRYA(g.u, sizeof(double) * nn);
+    TRYA(g.lam, sizeof(double) * nn); TRYA(g.lam2, sizeof(double) * nn); TRYA(g.lam0, sizeof(double) * nn); TRYA(g.u, sizeof(double) * nn);
     TRYA(g.u2, sizeof(double) * nn);
     TRYA(g.eig, sizeof(double) * d.nb); TRYA(g.haux, sizeof(double) * nn); TRYA(g.gamn, sizeof(double) * nn);
     TRYA(g.work, sizeof(double) * nn); TRYA(g.wk2, sizeof(double) * nn);
@@ -898,5 +898,16 @@ extern "C" int cuwaves_get_stream(cuw_handle* hp, void** stream) {
   H(hp);
   if (!stream) return h->fail(CUW_ERR_ARG, "null stream pointer");
   *stream = reinterpret_cast<void*>(h->stream);
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_get_ortho_stats(cuw_handle* hp, double* out, int n) {
+  H(hp);
+  if (!out || n < 1) return h->fail(CUW_ERR_ARG, "bad output buffer");
+  int st[16] = {0};
+  CUW_TRY(cudaMemcpyAsync(st, h->g.ostatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  const double v[5] = {(double)h->n_rediag, (double)st[8], (double)st[4], (double)st[1], (double)h->n_fp_fail};
+  for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
   return CUW_OK;
 }

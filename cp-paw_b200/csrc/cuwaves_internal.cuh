@@ -96,7 +96,7 @@ struct Device {
   double *occ = nullptr;         // (NB)
   // orthogonalisation (real NB x NB)
   double *mat = nullptr, *omat = nullptr, *oomat = nullptr;
-  double *lam = nullptr, *lam2 = nullptr;
+  double *lam = nullptr, *lam2 = nullptr, *lam0 = nullptr;  // lam0: start of a solve that may be redone
   double *u = nullptr, *u2 = nullptr, *eig = nullptr;
   double *haux = nullptr, *gamn = nullptr, *work = nullptr, *wk2 = nullptr;
   double *smat = nullptr, *emat = nullptr, *gt = nullptr, *xb = nullptr, *tb = nullptr;
@@ -147,6 +147,7 @@ struct Handle {
   std::vector<int> ev_phase;
   int nev = 0;
   long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
+  long long n_fp_fail = 0; // Lyapunov fixed-point solves that fell back to a rediagonalisation
   Device g;
   std::string err;
 

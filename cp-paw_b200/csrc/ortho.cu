@@ -221,77 +221,272 @@ struct OrthoArgs {
   double* xb;     // second buffer of the Lyapunov fixed point
   double* tb;     // E X
   int* inner;     // total inner iterations (diagnostics)
+  int fast;       // lyap_fast applies (n <= 128, tiles of at most 32 x 32)
 };
 
 // C(tile) = op(A) * op(B); op = transpose when tA / tB.  The tile
-// [i0,i1) x [j0,j1) has at most 16*MR rows and 16*MC columns; thread (ty,tx)
-// of the 16x16 layout owns rows ty+16r and columns tx+16c.  The K extent is
-// staged in chunks of kc into smA[k][row] / smB[k][col] (conflict-free reads).
+// [i0,i1) x [j0,j1) has at most RA = 16*MR rows and RB = 16*MC columns.  The K
+// extent is staged in chunks of KC (a multiple of 4) into smA[k][row] and
+// smB[k][col] with row strides RA+4 / RB+4 doubles, then multiplied on the
+// FP64 tensor cores (mma m8n8k4): the tile's 8x8 blocks are spread over the
+// warps and the padded strides make the fragment reads free of bank conflicts.
 // A and B may have been written by other CTAs of the cluster in the previous
 // phase, so they are read through L2 (__ldcg), never through the read-only path.
 template <int MR, int MC>
+__host__ __device__ constexpr int tile_lda() { return 16 * MR + 4; }
+template <int MR, int MC>
+__host__ __device__ constexpr int tile_ldb() { return 16 * MC + 4; }
+
+template <int MR, int MC, int KC = 128>
 __device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, int n, int i0, int i1, int j0, int j1,
-                          double* C, double* smA, double* smB, int kc) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+                          double* C, double* smA, double* smB) {
+  static_assert(KC % 4 == 0, "the chunk is a whole number of k=4 MMA steps");
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int tm = i1 - i0, tn = j1 - j0;
-  const int tx = tid % 16, ty = tid / 16;
   constexpr int RA = 16 * MR, RB = 16 * MC;
-  double acc[MR][MC];
+  constexpr int LDA = tile_lda<MR, MC>(), LDB = tile_ldb<MR, MC>();
+  constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC;
+  constexpr int TPW = (NTILE + 7) / 8;  // 8x8 blocks per warp (8 warps)
+  double acc[TPW][2];
 #pragma unroll
-  for (int r = 0; r < MR; ++r)
+  for (int q = 0; q < TPW; ++q) acc[q][0] = acc[q][1] = 0.0;
+  for (int k0 = 0; k0 < n; k0 += KC) {
+    const int kk = min(KC, n - k0);
+    const int kk4 = (kk + 3) & ~3;
+    // stage both operands (the whole chunk, zero past kk) with eight L2 loads in
+    // flight per thread: the tile is tiny and the loop is bound by latency;
+    // every divisor of the index arithmetic is a compile-time constant
+    constexpr int totA = RA * KC, tot = totA + RB * KC;
+    for (int base = 0; base < tot; base += 8 * nt) {
+      double v[8];
 #pragma unroll
-    for (int c = 0; c < MC; ++c) acc[r][c] = 0.0;
-  for (int k0 = 0; k0 < n; k0 += kc) {
-    const int kk = min(kc, n - k0);
-    if (!tA) {
-      for (int t = tid; t < RA * kk; t += nt) {
-        int ii = t % RA, k = t / RA;
-        smA[k * RA + ii] = ii < tm ? __ldcg(&A[(i0 + ii) + (size_t)n * (k0 + k)]) : 0.0;
+      for (int q = 0; q < 8; ++q) {
+        const int t = base + tid + q * nt;
+        v[q] = 0.0;
+        if (t < totA) {
+          int ii, k;
+          if (!tA) { ii = t % RA; k = t / RA; } else { k = t % KC; ii = t / KC; }
+          if (ii < tm && k < kk)
+            v[q] = __ldcg(!tA ? &A[(i0 + ii) + (size_t)n * (k0 + k)] : &A[(k0 + k) + (size_t)n * (i0 + ii)]);
+        } else if (t < tot) {
+          const int u = t - totA;
+          int jj, k;
+          if (!tB) { k = u % KC; jj = u / KC; } else { jj = u % RB; k = u / RB; }
+          if (jj < tn && k < kk)
+            v[q] = __ldcg(!tB ? &B[(k0 + k) + (size_t)n * (j0 + jj)] : &B[(j0 + jj) + (size_t)n * (k0 + k)]);
+        }
       }
-    } else {
-      for (int t = tid; t < RA * kk; t += nt) {
-        int k = t % kk, ii = t / kk;
-        smA[k * RA + ii] = ii < tm ? __ldcg(&A[(k0 + k) + (size_t)n * (i0 + ii)]) : 0.0;
-      }
-    }
-    if (!tB) {
-      for (int t = tid; t < RB * kk; t += nt) {
-        int k = t % kk, jj = t / kk;
-        smB[k * RB + jj] = jj < tn ? __ldcg(&B[(k0 + k) + (size_t)n * (j0 + jj)]) : 0.0;
-      }
-    } else {
-      for (int t = tid; t < RB * kk; t += nt) {
-        int jj = t % RB, k = t / RB;
-        smB[k * RB + jj] = jj < tn ? __ldcg(&B[(j0 + jj) + (size_t)n * (k0 + k)]) : 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int t = base + tid + q * nt;
+        if (t < totA) {
+          int ii, k;
+          if (!tA) { ii = t % RA; k = t / RA; } else { k = t % KC; ii = t / KC; }
+          smA[k * LDA + ii] = v[q];
+        } else if (t < tot) {
+          const int u = t - totA;
+          int jj, k;
+          if (!tB) { k = u % KC; jj = u / KC; } else { jj = u % RB; k = u / RB; }
+          smB[k * LDB + jj] = v[q];
+        }
       }
     }
     __syncthreads();
-    for (int k = 0; k < kk; ++k) {
-      double av[MR], bv[MC];
+    const int fr = lane >> 2, fk = lane & 3;
 #pragma unroll
-      for (int r = 0; r < MR; ++r) av[r] = smA[k * RA + ty + 16 * r];
-#pragma unroll
-      for (int c = 0; c < MC; ++c) bv[c] = smB[k * RB + tx + 16 * c];
-#pragma unroll
-      for (int r = 0; r < MR; ++r)
-#pragma unroll
-        for (int c = 0; c < MC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+    for (int q = 0; q < TPW; ++q) {
+      const int t = warp + q * nw;
+      if (t < NTILE) {
+        const int r0 = (t % TR) * 8, c0 = (t / TR) * 8;
+        for (int k = 0; k < kk4; k += 4) {
+          const double av = smA[(k + fk) * LDA + r0 + fr];
+          const double bv = smB[(k + fk) * LDB + c0 + fr];
+          dmma(acc[q], av, bv);
+        }
+      }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int r = 0; r < MR; ++r)
+  for (int q = 0; q < TPW; ++q) {
+    const int t = warp + q * nw;
+    if (t < NTILE) {
+      const int ii = (t % TR) * 8 + (lane >> 2);
 #pragma unroll
-    for (int c = 0; c < MC; ++c) {
-      int ii = ty + 16 * r, jj = tx + 16 * c;
-      if (ii < tm && jj < tn) C[(i0 + ii) + (size_t)n * (j0 + jj)] = acc[r][c];
+      for (int e = 0; e < 2; ++e) {
+        const int jj = (t / TR) * 8 + 2 * (lane & 3) + e;
+        if (ii < tm && jj < tn) C[(i0 + ii) + (size_t)n * (j0 + jj)] = acc[q][e];
+      }
     }
+  }
+  // callers read the tile back with another thread-to-element map
+  __syncthreads();
+}
+
+// maxima of (a, b) over the CTA: warp shuffles, then one pass over the warps
+// (red holds at least 64 doubles; every thread gets the result)
+__device__ __forceinline__ void block_max2(double& a, double& b, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  }
+  if (lane == 0) {
+    red[warp] = a;
+    red[32 + warp] = b;
+  }
+  __syncthreads();
+  a = red[0];
+  b = red[32];
+  for (int w = 1; w < nw; ++w) {
+    a = fmax(a, red[w]);
+    b = fmax(b, red[32 + w]);
+  }
+  __syncthreads();
 }
 
 __device__ __forceinline__ void csync() {
   __threadfence();
   cg::this_cluster().sync();
 }
+
+// Convergence rule of the Lyapunov fixed point (shared by both loops): true to
+// stop; `failed` when the contraction is too slow (the earlier eigenbasis is
+// too far from the current one) or there is no convergence within the limit.
+__device__ __forceinline__ bool lyap_stop(double gdx, double gxm, double& prev, int it2, int max_inner,
+                                          bool& failed) {
+  const double ratio = gdx / prev;
+  prev = gdx;
+  // converged: change at rounding level, or stalled just above it
+  if (gdx <= 4e-16 * gxm || (gdx <= 1e-13 * gxm && ratio > 0.5)) return true;
+  if ((it2 >= 4 && ratio > 0.6) || it2 == max_inner - 1 || !(gdx <= 1e200)) {
+    failed = true;
+    return true;
+  }
+  return false;
+}
+
+// Lyapunov fixed point X <- (GT - E X - X E) / (e_i + e_j) for n <= 128 and
+// CTA tiles of at most 32 x 32.  The CTA keeps its slices of the constant E
+// in shared memory (rows i0..i1 for E X, columns j0..j1 for X E), stages the
+// X slices it needs once per sweep, forms both products of its tile on the
+// FP64 tensor cores and updates its X tile in registers; one cluster barrier
+// per sweep.  Returns the buffer that holds the last iterate.
+template <int MR, int MC>
+__device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i1, int j0, int j1, double* sm,
+                             double* red, double* xcur, double* xnext, bool& failed) {
+  constexpr int RA = 16 * MR, RB = 16 * MC, LDA = RA + 4, LDB = RB + 4;
+  constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC, TPW = (NTILE + 7) / 8;
+  const int n = a.n, n4 = (n + 3) & ~3;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int fr = lane >> 2, fk = lane & 3;
+  const int tm = i1 - i0, tn = j1 - j0;
+  double* Er = sm;              // Er[k][ii] = E(i0+ii, k)
+  double* Ec = Er + LDA * n4;   // Ec[k][jj] = E(k, j0+jj)
+  double* Xc = Ec + LDB * n4;   // Xc[k][jj] = X(k, j0+jj)
+  double* Xr = Xc + LDB * n4;   // Xr[k][ii] = X(i0+ii, k)
+  for (int t = tid; t < n4 * RA; t += nt) {
+    const int ii = t % RA, k = t / RA;
+    Er[k * LDA + ii] = (ii < tm && k < n) ? __ldcg(&a.emat[(i0 + ii) + (size_t)n * k]) : 0.0;
+  }
+  for (int t = tid; t < n4 * RB; t += nt) {
+    const int k = t % n4, jj = t / n4;
+    Ec[k * LDB + jj] = (jj < tn && k < n) ? __ldcg(&a.emat[k + (size_t)n * (j0 + jj)]) : 0.0;
+  }
+  // this lane's elements of the tile: right-hand side, denominator, iterate
+  double gtv[TPW][2], den[TPW][2], xp[TPW][2];
+  int eidx[TPW][2];
+#pragma unroll
+  for (int q = 0; q < TPW; ++q) {
+    const int t = warp + q * nw;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int ii = (t % TR) * 8 + fr, jj = (t / TR) * 8 + 2 * fk + e;
+      const bool ok = t < NTILE && ii < tm && jj < tn;
+      eidx[q][e] = ok ? (i0 + ii) + n * (j0 + jj) : -1;
+      gtv[q][e] = ok ? __ldcg(&a.gt[eidx[q][e]]) : 0.0;
+      den[q][e] = ok ? a.e[i0 + ii] + a.e[j0 + jj] : 1.0;
+      xp[q][e] = ok ? __ldcg(&xcur[eidx[q][e]]) : 0.0;
+    }
+  }
+  double prev = INFINITY;
+  failed = false;
+  for (int it2 = 0; it2 < a.max_inner; ++it2) {
+    double* mp = a.maxpart + (it2 & 1) * 2 * cs;
+    // stage X(:, j0:j1) and X(i0:i1, :), sixteen loads in flight per thread
+    const int totc = n4 * RB, tot = totc + n4 * RA;
+    for (int base = 0; base < tot; base += 16 * nt) {
+      double v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int t = base + tid + q * nt;
+        v[q] = 0.0;
+        if (t < totc) {
+          const int k = t % n4, jj = t / n4;
+          if (jj < tn && k < n) v[q] = __ldcg(&xcur[k + (size_t)n * (j0 + jj)]);
+        } else if (t < tot) {
+          const int u = t - totc, ii = u % RA, k = u / RA;
+          if (ii < tm && k < n) v[q] = __ldcg(&xcur[(i0 + ii) + (size_t)n * k]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int t = base + tid + q * nt;
+        if (t < totc) {
+          const int k = t % n4, jj = t / n4;
+          Xc[k * LDB + jj] = v[q];
+        } else if (t < tot) {
+          const int u = t - totc, ii = u % RA, k = u / RA;
+          Xr[k * LDA + ii] = v[q];
+        }
+      }
+    }
+    __syncthreads();
+    double dx = 0.0, xm = 0.0;
+#pragma unroll
+    for (int q = 0; q < TPW; ++q) {
+      const int t = warp + q * nw;
+      if (t >= NTILE) continue;
+      const int r0 = (t % TR) * 8, c0 = (t / TR) * 8;
+      double ex[2] = {0.0, 0.0}, xe[2] = {0.0, 0.0};
+      for (int k = 0; k < n4; k += 4) {
+        dmma(ex, Er[(k + fk) * LDA + r0 + fr], Xc[(k + fk) * LDB + c0 + fr]);
+        dmma(xe, Xr[(k + fk) * LDA + r0 + fr], Ec[(k + fk) * LDB + c0 + fr]);
+      }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (eidx[q][e] < 0) continue;
+        const double xn = (gtv[q][e] - ex[e] - xe[e]) / den[q][e];
+        dx = fmax(dx, fabs(xn - xp[q][e]));
+        xm = fmax(xm, fabs(xn));
+        xp[q][e] = xn;
+        xnext[eidx[q][e]] = xn;
+      }
+    }
+    block_max2(dx, xm, red);  // its barriers also end this sweep's reads of Xc / Xr
+    if (tid == 0) {
+      mp[rank] = dx;
+      mp[cs + rank] = xm;
+    }
+    csync();
+    double gdx = 0.0, gxm = 0.0;
+    for (int r = 0; r < cs; ++r) {
+      gdx = fmax(gdx, __ldcg(&mp[r]));
+      gxm = fmax(gxm, __ldcg(&mp[cs + r]));
+    }
+    double* tmpx = xcur;
+    xcur = xnext;
+    xnext = tmpx;
+    if (rank == 0 && tid == 0) a.inner[0] += 1;
+    if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, failed)) break;
+  }
+  return xcur;
+}
+
+// status of k_ortho_x when the Lyapunov fixed point in an earlier eigenbasis
+// does not converge fast enough (internal, never returned to the caller)
+constexpr int kFixedPointFailed = 100;
 
 template <int MR, int MC>
 __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
@@ -308,9 +503,8 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   const int rs = (n + tr - 1) / tr, csz = (n + tc - 1) / tc;
   const int i0 = min(n, ri * rs), i1 = min(n, i0 + rs);
   const int j0 = min(n, ci * csz), j1 = min(n, j0 + csz);
-  const int kc = a.kc;
   double* smA = sm;
-  double* smB = sm + (size_t)16 * MR * kc;
+  double* smB = sm + (size_t)tile_lda<MR, MC>() * a.kc;
   const int tid = threadIdx.x, nt = blockDim.x;
   double* lam = a.lam;
   double* lamn = a.lam2;
@@ -318,14 +512,14 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
   for (int iter = 1; iter <= a.max_iter; ++iter) {
     // HAUX = CHICHI * LAMBDA + 2 CHIPSI
-    gemm_tile<MR, MC>(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    gemm_tile<MR, MC>(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
       a.haux[i + (size_t)n * j] = __ldcg(&a.haux[i + (size_t)n * j]) + 2.0 * a.chipsi[i + (size_t)n * j];
     }
     csync();
     // GAMN = LAMBDA^T * HAUX
-    gemm_tile<MR, MC>(lam, true, a.haux, false, n, i0, i1, j0, j1, a.gamn, smA, smB, kc);
+    gemm_tile<MR, MC>(lam, true, a.haux, false, n, i0, i1, j0, j1, a.gamn, smA, smB);
     csync();
     // W = 0.5 (GAMN + GAMN^T) + PSIPSI - 1 ; tile max
     double mx = 0.0;
@@ -340,14 +534,10 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
       mx = fmax(mx, fabs(v));
       if (v != v) mx = INFINITY;
     }
-    // block max
-    red[tid] = mx;
-    __syncthreads();
-    for (int s = nt / 2; s > 0; s >>= 1) {
-      if (tid < s) red[tid] = fmax(red[tid], red[tid + s]);
-      __syncthreads();
-    }
-    if (tid == 0) a.maxpart[rank] = red[0];
+    // CTA max (NaN propagates as infinity)
+    double unused = 0.0;
+    block_max2(mx, unused, red);
+    if (tid == 0) a.maxpart[rank] = mx;
     csync();
     double digam = 0.0;
     for (int r = 0; r < cs; ++r) digam = fmax(digam, __ldcg(&a.maxpart[r]));
@@ -362,10 +552,10 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
       break;
     }
     // HAUX = U^T W
-    gemm_tile<MR, MC>(a.u, true, a.w, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    gemm_tile<MR, MC>(a.u, true, a.w, false, n, i0, i1, j0, j1, a.haux, smA, smB);
     csync();
     // GT = HAUX U (Gamma in the U basis);  X = GT / (e_i + e_j)
-    gemm_tile<MR, MC>(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gt, smA, smB, kc);
+    gemm_tile<MR, MC>(a.haux, false, a.u, false, n, i0, i1, j0, j1, a.gt, smA, smB);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
       a.gamn[i + (size_t)n * j] = __ldcg(&a.gt[i + (size_t)n * j]) / (a.e[i] + a.e[j]);
@@ -374,57 +564,59 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     // When U diagonalises an earlier CHIPSI only, D X + X D = GT - E X - X E is
     // solved by the fixed point X <- (GT - E X - X E)/(e_i + e_j) to rounding
     // level: the same Lyapunov solution as the eigendecomposition of the
-    // current matrix (E, X symmetric, so X E = (E X)^T).
+    // current matrix.
     double* xcur = a.gamn;
     double* xnext = a.xb;
-    if (a.use_e) {
+    bool fp_failed = false;
+    if (a.use_e && a.fast) {
+      if constexpr (MR <= 2 && MC <= 2)
+        xcur = lyap_fast<MR, MC>(a, cs, rank, i0, i1, j0, j1, sm, red, xcur, xnext, fp_failed);
+    } else if (a.use_e) {
+      double prev = INFINITY;
+      // one cluster barrier per sweep: E X and X E are both formed on this
+      // CTA's tile (X E = (E X)^T would need another CTA's tile), and the
+      // convergence partials alternate between two halves of maxpart
       for (int it2 = 0; it2 < a.max_inner; ++it2) {
-        gemm_tile<MR, MC>(a.emat, false, xcur, false, n, i0, i1, j0, j1, a.tb, smA, smB, kc);
-        csync();
+        double* mp = a.maxpart + (it2 & 1) * 2 * cs;
+        gemm_tile<MR, MC>(a.emat, false, xcur, false, n, i0, i1, j0, j1, a.tb, smA, smB);
+        gemm_tile<MR, MC>(xcur, false, a.emat, false, n, i0, i1, j0, j1, a.haux, smA, smB);
         double dx = 0.0, xm = 0.0;
         for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
           int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
           double xn = (__ldcg(&a.gt[i + (size_t)n * j]) - __ldcg(&a.tb[i + (size_t)n * j]) -
-                       __ldcg(&a.tb[j + (size_t)n * i])) / (a.e[i] + a.e[j]);
+                       __ldcg(&a.haux[i + (size_t)n * j])) / (a.e[i] + a.e[j]);
           dx = fmax(dx, fabs(xn - __ldcg(&xcur[i + (size_t)n * j])));
           xm = fmax(xm, fabs(xn));
           xnext[i + (size_t)n * j] = xn;
         }
-        red[tid] = dx;
-        __syncthreads();
-        for (int s2 = nt / 2; s2 > 0; s2 >>= 1) {
-          if (tid < s2) red[tid] = fmax(red[tid], red[tid + s2]);
-          __syncthreads();
+        block_max2(dx, xm, red);
+        if (tid == 0) {
+          mp[rank] = dx;
+          mp[cs + rank] = xm;
         }
-        if (tid == 0) a.maxpart[rank] = red[0];
-        __syncthreads();
-        red[tid] = xm;
-        __syncthreads();
-        for (int s2 = nt / 2; s2 > 0; s2 >>= 1) {
-          if (tid < s2) red[tid] = fmax(red[tid], red[tid + s2]);
-          __syncthreads();
-        }
-        if (tid == 0) a.maxpart[cs + rank] = red[0];
         csync();
         double gdx = 0.0, gxm = 0.0;
         for (int r = 0; r < cs; ++r) {
-          gdx = fmax(gdx, __ldcg(&a.maxpart[r]));
-          gxm = fmax(gxm, __ldcg(&a.maxpart[cs + r]));
+          gdx = fmax(gdx, __ldcg(&mp[r]));
+          gxm = fmax(gxm, __ldcg(&mp[cs + r]));
         }
         double* tmpx = xcur;
         xcur = xnext;
         xnext = tmpx;
         if (rank == 0 && tid == 0) a.inner[0] += 1;
-        if (gdx <= 1e-16 * gxm) break;
-        // the next phase overwrites maxpart and tb only after this barrier
-        csync();
+        if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, fp_failed)) break;
       }
     }
+    if (fp_failed) {
+      status = kFixedPointFailed;
+      iters = iter;
+      break;
+    }
     // HAUX = U X
-    gemm_tile<MR, MC>(a.u, false, xcur, false, n, i0, i1, j0, j1, a.haux, smA, smB, kc);
+    gemm_tile<MR, MC>(a.u, false, xcur, false, n, i0, i1, j0, j1, a.haux, smA, smB);
     csync();
     // W = HAUX U^T
-    gemm_tile<MR, MC>(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB, kc);
+    gemm_tile<MR, MC>(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB);
     csync();
     // LAMBDA(I,J) -= 2 OCCI/(OCCI+OCCJ) W(I,J); then occupation symmetrisation
     const double dsmall = 1e-12;
@@ -461,11 +653,11 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
   csync();
 }
 
-// C = op(A) op(B) for n x n matrices, one 32x32 tile per CTA (warm start of the eigensolver)
+// C = op(A) op(B) for n x n matrices, one 32x32 tile per CTA
 __global__ void __launch_bounds__(256) k_small_gemm(const double* A, int tA, const double* B, int tB, int n, double* C) {
-  __shared__ double smA[32 * 32], smB[32 * 32];
+  __shared__ double smA[tile_lda<2, 2>() * 32], smB[tile_ldb<2, 2>() * 32];
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
-  gemm_tile<2, 2>(A, tA != 0, B, tB != 0, n, i0, min(n, i0 + 32), j0, min(n, j0 + 32), C, smA, smB, 32);
+  gemm_tile<2, 2, 32>(A, tA != 0, B, tB != 0, n, i0, min(n, i0 + 32), j0, min(n, j0 + 32), C, smA, smB);
 }
 
 // LAMBDA1/LAMBDA2 (NBH x NBH complex) from real LAMBDA (NB x NB)
@@ -652,76 +844,22 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
   return CUW_OK;
 }
 
-// Full WAVES_ORTHO_X: matrices mat (PSIPSI), omat (CHIPSI), oomat (CHICHI) and
-// the starting lambda are in h->g.{mat,omat,oomat,lam}.
-// diag(B) -> e, B with its diagonal removed -> E; [0] max|E|, [1] min e into out
-__global__ void k_split_diag(const double* __restrict__ b, int n, double* __restrict__ e, double* __restrict__ emat,
-                             double* __restrict__ out) {
-  __shared__ double rmax[256], rmin[256];
-  double mx = 0.0, mn = INFINITY;
-  for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
-    int i = k % n, j = k / n;
-    double v = b[k];
-    if (i == j) {
-      e[i] = v;
-      emat[k] = 0.0;
-      mn = fmin(mn, v);
-    } else {
-      emat[k] = v;
-      mx = fmax(mx, fabs(v));
-    }
-  }
-  rmax[threadIdx.x] = mx;
-  rmin[threadIdx.x] = mn;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      rmax[threadIdx.x] = fmax(rmax[threadIdx.x], rmax[threadIdx.x + s]);
-      rmin[threadIdx.x] = fmin(rmin[threadIdx.x], rmin[threadIdx.x + s]);
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    out[0] = rmax[0];
-    out[1] = rmin[0];
+// diag(B) -> e, B with its diagonal removed -> E
+__global__ void k_split_diag(const double* __restrict__ b, int n, double* __restrict__ e, double* __restrict__ emat) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n * n; k += gridDim.x * blockDim.x) {
+    const int i = k % n, j = k / n;
+    const double v = b[k];
+    if (i == j) e[i] = v;
+    emat[k] = (i == j) ? 0.0 : v;
   }
 }
 
-int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
+// One launch of the ORTHO_X iteration (k_ortho_x) with the eigenbasis in
+// g.u / g.eig; use_e: g.u diagonalises an earlier CHIPSI only and g.emat holds
+// the off-diagonal rest.  st = {status, iterations}.
+static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st[2]) {
   const int n = h->d.nb;
   Device& g = h->g;
-  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.smat);
-  CUW_LAUNCH_CHECK("k_symmetrize");
-  int use_e = 0;
-  const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
-  if (h->have_u) {
-    // B = U^T S U with U from an earlier diagonalisation
-    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.smat, 0, g.u, 0, n, g.haux);
-    CUW_LAUNCH_CHECK("k_small_gemm");
-    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 1, g.haux, 0, n, g.work);
-    CUW_LAUNCH_CHECK("k_small_gemm");
-    k_split_diag<<<1, 256, 0, h->stream>>>(g.work, n, g.eig, g.emat, g.scal + 2 * n + 8);
-    CUW_LAUNCH_CHECK("k_split_diag");
-    double st2[2];
-    CUW_TRY(cudaMemcpyAsync(st2, g.scal + 2 * n + 8, sizeof(st2), cudaMemcpyDeviceToHost, h->stream));
-    CUW_TRY(cudaStreamSynchronize(h->stream));
-    // contraction bound of the fixed point: n max|E| / min(e)
-    const double rho = st2[1] > 0.0 ? n * st2[0] / st2[1] : 1e300;
-    if (rho < 0.1) {
-      use_e = 1;
-    } else {
-      // rediagonalise: Jacobi on the nearly diagonal B, then U <- U V
-      CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig));
-      k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2);
-      CUW_LAUNCH_CHECK("k_small_gemm");
-      std::swap(g.u, g.u2);
-      ++h->n_rediag;
-    }
-  } else {
-    CUW_RET(jacobi_run(h, g.smat, g.u, g.eig));
-    h->have_u = true;
-    ++h->n_rediag;
-  }
   OrthoArgs a;
   a.n = n;
   a.chichi = g.oomat;
@@ -741,7 +879,7 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   a.eps = eps;
   a.emat = g.emat;
   a.use_e = use_e;
-  a.max_inner = 60;
+  a.max_inner = 64;
   a.gt = g.gt;
   a.xb = g.xb;
   a.tb = g.tb;
@@ -767,8 +905,10 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
     const int mr = rs <= 16 ? 1 : (rs <= 32 ? 2 : (rs <= 64 ? 4 : 0));
     const int mc = csz <= 16 ? 1 : (csz <= 32 ? 2 : (csz <= 64 ? 4 : 0));
     if (!mr || !mc) continue;
-    a.kc = std::min(n, 128);
-    const size_t smem = sizeof(double) * (size_t)a.kc * 16 * (mr + mc);
+    a.kc = 128;  // staging chunk of gemm_tile (its default KC)
+    const int n4 = (n + 3) & ~3;
+    a.fast = (n <= 128 && mr <= 2 && mc <= 2) ? 1 : 0;
+    const size_t smem = sizeof(double) * (16 * (mr + mc) + 8) * (size_t)std::max(a.kc, a.fast ? 2 * n4 : 0);
     void (*fn)(OrthoArgs) = nullptr;
     if (mr == 1 && mc == 1) fn = k_ortho_x<1, 1>;
     else if (mr == 2 && mc == 2) fn = k_ortho_x<2, 2>;
@@ -799,13 +939,65 @@ int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
   }
   if (!launched) return h->fail(CUW_ERR_UNSUPPORTED, "k_ortho_x: no cluster configuration fits NB");
   ++h->launches;
-  int st[2] = {0, 0};
   CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
+  return CUW_OK;
+}
+
+// B = U^T S U -> g.work, its diagonal -> g.eig and off-diagonal rest -> g.emat
+static int rotate_to_basis(Handle* h) {
+  const int n = h->d.nb;
+  Device& g = h->g;
+  const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
+  k_small_gemm<<<tg, 256, 0, h->stream>>>(g.smat, 0, g.u, 0, n, g.haux);
+  CUW_LAUNCH_CHECK("k_small_gemm");
+  k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 1, g.haux, 0, n, g.work);
+  CUW_LAUNCH_CHECK("k_small_gemm");
+  k_split_diag<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.work, n, g.eig, g.emat);
+  CUW_LAUNCH_CHECK("k_split_diag");
+  return CUW_OK;
+}
+
+// WAVES_ORTHO_X with S = sym(CHIPSI).  The reference diagonalises S in every
+// call (src/paw_waves2.f90:1905-1915) to solve S X + X S = Gamma.  Here the
+// eigenbasis of an earlier call is kept: X is the fixed point of
+// X <- (GT - E X - X E) / (e_i + e_j) in that basis (U^T S U = diag(e) + E),
+// the same unique Lyapunov solution to rounding.  When the fixed point
+// contracts too slowly the kernel reports it, S is rediagonalised (Jacobi on
+// U^T S U, U <- U V) and the iteration restarts from the saved Lambda.
+int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
+  const int n = h->d.nb;
+  Device& g = h->g;
+  const size_t nn = (size_t)n * n;
+  const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
+  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.smat);
+  CUW_LAUNCH_CHECK("k_symmetrize");
+  int st[2] = {0, 0};
+  if (h->have_u) {
+    CUW_RET(rotate_to_basis(h));
+    CUW_TRY(cudaMemcpyAsync(g.lam0, g.lam, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->stream));
+    CUW_RET(ortho_x_launch(h, 1, max_iter, eps, st));
+    if (st[0] == kFixedPointFailed) {
+      ++h->n_fp_fail;
+      CUW_RET(rotate_to_basis(h));  // g.work was overwritten by the iteration
+      CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig));
+      k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2);
+      CUW_LAUNCH_CHECK("k_small_gemm");
+      std::swap(g.u, g.u2);
+      ++h->n_rediag;
+      CUW_TRY(cudaMemcpyAsync(g.lam, g.lam0, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->stream));
+      CUW_RET(ortho_x_launch(h, 0, max_iter, eps, st));
+    }
+  } else {
+    CUW_RET(jacobi_run(h, g.smat, g.u, g.eig));
+    h->have_u = true;
+    ++h->n_rediag;
+    CUW_RET(ortho_x_launch(h, 0, max_iter, eps, st));
+  }
   if (iters) *iters = st[1];
   if (st[0] == CUW_ERR_NOT_CONVERGED) return h->fail(st[0], "LOOP FOR ORTHOGONALIZATION IS NOT CONVERGED");
   if (st[0] == CUW_ERR_DIVERGED) return h->fail(st[0], "ITERATION LOOP FOR ORTHOGONALIZATION IS ABOUT TO DIVERGE");
-  if (st[0] != CUW_OK) return h->fail(st[0], "orthogonalisation failed");
+  if (st[0] != CUW_OK) return h->fail(CUW_ERR_STATE, "orthogonalisation failed");
   return CUW_OK;
 }
 

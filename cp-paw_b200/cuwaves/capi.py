@@ -82,6 +82,7 @@ OPTIONAL = {
     "set_timing": [_P, C.c_int],
     "get_timing": [_P, _D, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "get_stream": [_P, C.POINTER(C.c_void_p)],
+    "get_ortho_stats": [_P, _D, C.c_int],
     # device-pointer variant without allocation (no handle)
     "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
     "get_atoms": [_P, _D, _D, _D],
@@ -328,6 +329,14 @@ class Waves:
         nl, ns = C.c_longlong(), C.c_longlong()
         self._chk(self._f["get_timing"](self.h, _dptr(ms), len(ms), C.byref(nl), C.byref(ns)), "get_timing")
         return dict(zip(self.PHASES, ms.tolist())), nl.value, ns.value
+
+    ORTHO_STATS = ("eigendecompositions", "fixed_point_sweeps", "last_jacobi_sweeps", "last_ortho_iterations",
+                   "fixed_point_fallbacks")
+
+    def ortho_stats(self) -> dict:
+        out = np.zeros(len(self.ORTHO_STATS))
+        self._chk(self._f["get_ortho_stats"](self.h, _dptr(out), len(out)), "get_ortho_stats")
+        return dict(zip(self.ORTHO_STATS, out.tolist()))
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -159,6 +159,13 @@ int cuwaves_reset_atoms(cuw_handle* h, const double* r0);
 int cuwaves_set_timing(cuw_handle* h, int enable);
 int cuwaves_get_timing(cuw_handle* h, double* ms, int n, long long* launches, long long* steps);
 int cuwaves_get_stream(cuw_handle* h, void** stream);
+/* Diagnostics of the orthonormality solve (no reference counterpart): out[0]
+ * eigendecompositions of sym(CHIPSI) so far, out[1] Lyapunov fixed-point sweeps
+ * so far, out[2] Jacobi sweeps of the last eigendecomposition, out[3] ORTHO_X
+ * iterations of the last solve, out[4] solves whose fixed point in the earlier
+ * eigenbasis converged too slowly and were redone after a rediagonalisation.
+ * n values are written. */
+int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
 
 /* Projections without any device allocation: PROJ(b,p) = gweight * sum_G
  * conj(PRO(G,p)) psi(G,b), the contraction of cuwaves_projections, for callers
