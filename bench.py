@@ -233,6 +233,55 @@ def run_cuda(args, rank, world, local):
     return result
 
 
+def run_mixed(args, local):
+    """The same workload on the mixed-precision path (FP32 FFTs, tf32x3
+    tensor-core contractions, FP64 constraint solve and sums): device-timed
+    steps/s and phase split, and the largest deviation of energy and forces
+    from the FP64 path over the first steps from an identical state.  (CP
+    trajectories from random wave functions separate chaotically over tens of
+    steps, so later differences measure the dynamics, not the precision.)"""
+    import numpy as np
+    import torch
+    import cuwaves
+
+    inp = make_inputs(args.system)
+    ref = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_FP64).setup().initialize()
+    w = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup()
+    for which in (cuwaves.CUW_PSI0, cuwaves.CUW_PSIM):
+        w.upload_psi(which, ref.download_psi(which))
+    w.set_proj(ref.get_proj())
+    w.set_rlam0(ref.get_rlam0())
+    de = df = 0.0
+    nacc = 5
+    for _ in range(nacc):
+        o_r, f_r = ref.cp_step(move_atoms=True)
+        o_m, f_m = w.cp_step(move_atoms=True)
+        de = max(de, abs(float(o_m[0]) - float(o_r[0])) / inp["nat"])
+        df = max(df, float(np.abs(f_m - f_r).max()))
+    ref.close()
+    stream = torch.cuda.ExternalStream(w.stream())
+    for _ in range(args.warmup):
+        w.cp_step(move_atoms=True)
+    torch.cuda.synchronize()
+    w.set_timing(True)
+    _, l0, _ = w.get_timing()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        w.cp_step(move_atoms=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    phases, l1, nsteps = w.get_timing()
+    w.set_timing(False)
+    w.close()
+    return {"value": round(args.steps / (ms * 1e-3), 4), "unit": "steps/s", "ms_per_step": round(ms / args.steps, 4),
+            "dtype": "f32 FFT / tf32x3 tensor cores / f64 solve and sums",
+            f"max_dE_per_atom_vs_fp64_{nacc}_steps": de, f"max_dF_vs_fp64_{nacc}_steps": df,
+            "gpu_launches": l1 - l0,
+            "phase_ms_per_step": {k: round(v / max(1, nsteps), 4) for k, v in phases.items()}}
+
+
 def emit_cuda(args, res, world):
     ph = res["phases_ms_per_step"]
     fm = res["fm"]
@@ -267,6 +316,7 @@ def emit_cuda(args, res, world):
                      "traffic": traffic, "flops_per_launch": flops},
         "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()},
         "ortho_solve": res.get("ortho"),
+        "mixed": res.get("mixed"),
         "clocks": res["clocks"],
         "cpu_baseline": cpu,
     }
@@ -340,6 +390,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "cuda" else args.warmup
     if args.impl == "reference":
@@ -351,6 +402,8 @@ def main():
 
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     res = run_cuda(args, rank, world, local)
+    if not args.no_mixed:
+        res["mixed"] = run_mixed(args, local)
     if rank == 0:
         if world > 1 or args.no_cpu:
             args.no_cpu = args.no_cpu or rank != 0

@@ -4,7 +4,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["capi.cu", "fft.cu", "gemm.cu", "ortho.cu"]
+SRC = ["capi.cu", "fft.cu", "gemm.cu", "ortho.cu", "tc.cu"]
 OUT = os.path.join(HERE, "lib", "libcuwaves.so")
 
 
@@ -17,7 +17,8 @@ def nvcc() -> str:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
-    deps = srcs + [os.path.join(HERE, "csrc", "cuwaves_internal.cuh"),
+    deps = srcs + [os.path.join(HERE, "csrc", "cuwaves_internal.cuh"), os.path.join(HERE, "csrc", "tc_sm100.cuh"),
+                   os.path.join(HERE, "csrc", "tc_pipe.cuh"),
                    os.path.join(os.path.dirname(HERE), "include", "cuwaves.h")]
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(d) for d in deps):
         return OUT

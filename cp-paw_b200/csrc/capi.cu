@@ -455,6 +455,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     }
     rc = small_tables_setup(h);
     if (rc == CUW_OK) rc = gemm_setup(h);
+    if (rc == CUW_OK && h->mixed()) rc = tc_setup(h);
   } while (0);
   if (rc != CUW_OK) {
     free_all(h);
@@ -865,6 +866,7 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   CUW_TRY(cudaMemcpyAsync(hs, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
   if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
+  CUW_RET(h->tc_status());
   CUW_RET(collect_marks(h));
   if (out) {
     out[0] = hs[1];

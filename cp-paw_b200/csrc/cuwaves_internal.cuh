@@ -84,7 +84,7 @@ struct Device {
   int *plane_pos = nullptr;      // (NGL) ix + NR1*iy of that G
   int *zslot = nullptr;          // (NR3) compact plane index or -1
   double *v = nullptr;           // (NR1*NR2*NR3) local potential
-  double2 *grid = nullptr;       // (batch, nzp, NR2, NR1) work grid
+  void *grid = nullptr;          // (batch, nzp, NR2, NR1) work grid, double2 or float2 (mixed)
   double2 *tw1 = nullptr, *tw2 = nullptr, *tw3 = nullptr;  // twiddles exp(+2 pi i k/n)
   // atoms and one-centre data
   double *r0 = nullptr, *rp = nullptr, *rm = nullptr;  // (3, NAT)
@@ -146,6 +146,7 @@ struct Handle {
   std::vector<cudaEvent_t> ev;
   std::vector<int> ev_phase;
   int nev = 0;
+  bool mixed() const { return d.precision == CUW_PREC_MIXED; }
   long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
   long long n_fp_fail = 0; // Lyapunov fixed-point solves that fell back to a rediagonalisation
   Device g;
@@ -159,6 +160,15 @@ struct Handle {
     if (async) return CUW_OK;
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(CUW_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+    return tc_status();
+  }
+  // error flag of the tensor-core pipelines (a bounded wait that ran out)
+  int tc_status() {
+    if (!mixed()) return CUW_OK;
+    int f = 0;
+    cudaError_t e = cudaMemcpy(&f, g.ostatus + 12, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(CUW_ERR_CUDA, std::string("status: ") + cudaGetErrorString(e));
+    if (f) return fail(CUW_ERR_CUDA, "tensor-core pipeline: a bounded wait ran out");
     return CUW_OK;
   }
 };
@@ -176,6 +186,13 @@ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// the same for float2 (FP32 transforms of the mixed-precision path)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
 // (-i)^l
 __device__ __forceinline__ double2 mipow(int l) {
@@ -186,6 +203,20 @@ __device__ __forceinline__ double2 mipow(int l) {
     default: return make_double2(0.0, 1.0);
   }
 }
+
+// PRO(g,p) = Y_lm(g) P_ln(|g|) (-i)^l EIGR(g,a) generated from the tables
+// (WAVES_EXPANDPRO, src/paw_waves1.f90:6070-6109)
+__device__ __forceinline__ double2 pro_value(int g, int ngl, const ProDesc& d, const double* __restrict__ ylm,
+                                             const double* __restrict__ pro, const double2* __restrict__ eigr) {
+  double s = ylm[(size_t)g + (size_t)ngl * d.lm] * pro[(size_t)g + (size_t)ngl * d.ibare];
+  double2 e = cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]);
+  return make_double2(s * e.x, s * e.y);
+}
+
+// coefficients of the fused ADDPRO epilogues (see k_addpro)
+struct StepCoef {
+  double a1, a2, a3, oscale;
+};
 
 // FP64 tensor-core MMA, m8n8k4, A row-major / B column-major fragments:
 //   a = A[lane>>2][lane&3], b = B[lane&3][lane>>2],
@@ -220,6 +251,17 @@ struct GramPair {
 };
 int gram_planewave(Handle* h, const GramPair* pairs, int npair, double2* dst);
 int gram_projections(Handle* h, const GramPair* pairs, int npair, double2* dst);
+int ensure_part(Handle* h, size_t bytes);  // split-K scratch h->g.part of at least `bytes`
+// split-precision (tf32 x3) tensor-core versions, used when precision is
+// CUW_PREC_MIXED; same arguments and results as the FP64 functions above
+int tc_setup(Handle* h);
+int tc_proj(Handle* h, const double2* psi, double2* proj);
+int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const StepCoef& sc);
+int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
+            double scale, double2* dst);
+int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double2* l1, const double2* l2, int nm,
+            int nn, int nk, size_t sxm, size_t sxk, size_t som, size_t son);
+int tc_force(Handle* h, const double2* ded, double* fpart, int* ntile);
 int propagate_run(Handle* h);
 int opsi_scale_run(Handle* h);
 int switch_lambda_run(Handle* h);

@@ -31,9 +31,25 @@ namespace {
 constexpr int kMaxV = 8;   // complex values per thread per stage
 constexpr int kPlaneThreads = 256;
 
+// The transforms are written once for double2 (FP64 path) and float2 (the FP32
+// FFT of the mixed-precision path).
+template <class C>
+struct CT;
+template <>
+struct CT<double2> {
+  using R = double;
+  __device__ __forceinline__ static double2 mk(double x, double y) { return make_double2(x, y); }
+};
+template <>
+struct CT<float2> {
+  using R = float;
+  __device__ __forceinline__ static float2 mk(float x, float y) { return make_float2(x, y); }
+};
+
 // --- radix butterflies: v <- DFT_R(v) with exp(sign*2*pi*i*q*s/R) -----------
-__device__ __forceinline__ double2 mul_i(double2 a, double sgn) {  // a * (sgn*i)
-  return make_double2(-sgn * a.y, sgn * a.x);
+template <class C>
+__device__ __forceinline__ C mul_i(C a, typename CT<C>::R sgn) {  // a * (sgn*i)
+  return CT<C>::mk(-sgn * a.y, sgn * a.x);
 }
 
 template <int R>
@@ -41,8 +57,9 @@ struct Bfly;
 
 template <>
 struct Bfly<2> {
-  __device__ __forceinline__ static void run(double2 (&v)[2], double, const double2*, int) {
-    double2 a = v[0], b = v[1];
+  template <class C>
+  __device__ __forceinline__ static void run(C (&v)[2], typename CT<C>::R, const C*, int) {
+    C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   }
@@ -50,11 +67,13 @@ struct Bfly<2> {
 
 template <>
 struct Bfly<3> {
-  __device__ __forceinline__ static void run(double2 (&v)[3], double sgn, const double2*, int) {
-    const double h = 0.86602540378443864676;  // sqrt(3)/2
-    double2 a = v[0], t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    double2 u = mul_i(cscale(d, h), sgn);
-    double2 m = make_double2(a.x - 0.5 * t.x, a.y - 0.5 * t.y);
+  template <class C>
+  __device__ __forceinline__ static void run(C (&v)[3], typename CT<C>::R sgn, const C*, int) {
+    using T = typename CT<C>::R;
+    const T h = (T)0.86602540378443864676;  // sqrt(3)/2
+    C a = v[0], t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    C u = mul_i(cscale(d, h), sgn);
+    C m = CT<C>::mk(a.x - (T)0.5 * t.x, a.y - (T)0.5 * t.y);
     v[0] = cadd(a, t);
     v[1] = cadd(m, u);
     v[2] = csub(m, u);
@@ -63,9 +82,10 @@ struct Bfly<3> {
 
 template <>
 struct Bfly<4> {
-  __device__ __forceinline__ static void run(double2 (&v)[4], double sgn, const double2*, int) {
-    double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-    double2 t2 = cadd(v[1], v[3]), t3 = mul_i(csub(v[1], v[3]), sgn);
+  template <class C>
+  __device__ __forceinline__ static void run(C (&v)[4], typename CT<C>::R sgn, const C*, int) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), t3 = mul_i(csub(v[1], v[3]), sgn);
     v[0] = cadd(t0, t2);
     v[2] = csub(t0, t2);
     v[1] = cadd(t1, t3);
@@ -75,17 +95,19 @@ struct Bfly<4> {
 
 template <>
 struct Bfly<5> {
-  __device__ __forceinline__ static void run(double2 (&v)[5], double sgn, const double2*, int) {
-    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-    double2 a = v[0];
-    double2 p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
-    double2 p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
-    double2 r1 = make_double2(a.x + c1 * p1.x + c2 * p2.x, a.y + c1 * p1.y + c2 * p2.y);
-    double2 r2 = make_double2(a.x + c2 * p1.x + c1 * p2.x, a.y + c2 * p1.y + c1 * p2.y);
-    double2 i1 = mul_i(make_double2(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y), sgn);
-    double2 i2 = mul_i(make_double2(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y), sgn);
-    v[0] = make_double2(a.x + p1.x + p2.x, a.y + p1.y + p2.y);
+  template <class C>
+  __device__ __forceinline__ static void run(C (&v)[5], typename CT<C>::R sgn, const C*, int) {
+    using T = typename CT<C>::R;
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    C a = v[0];
+    C p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
+    C p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
+    C r1 = CT<C>::mk(a.x + c1 * p1.x + c2 * p2.x, a.y + c1 * p1.y + c2 * p2.y);
+    C r2 = CT<C>::mk(a.x + c2 * p1.x + c1 * p2.x, a.y + c2 * p1.y + c1 * p2.y);
+    C i1 = mul_i(CT<C>::mk(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y), sgn);
+    C i2 = mul_i(CT<C>::mk(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y), sgn);
+    v[0] = CT<C>::mk(a.x + p1.x + p2.x, a.y + p1.y + p2.y);
     v[1] = cadd(r1, i1);
     v[4] = csub(r1, i1);
     v[2] = cadd(r2, i2);
@@ -95,15 +117,17 @@ struct Bfly<5> {
 
 template <>
 struct Bfly<8> {
-  __device__ __forceinline__ static void run(double2 (&v)[8], double sgn, const double2*, int) {
-    const double q = 0.70710678118654752440;
-    double2 e[4] = {v[0], v[2], v[4], v[6]};
-    double2 o[4] = {v[1], v[3], v[5], v[7]};
-    Bfly<4>::run(e, sgn, nullptr, 0);
-    Bfly<4>::run(o, sgn, nullptr, 0);
+  template <class C>
+  __device__ __forceinline__ static void run(C (&v)[8], typename CT<C>::R sgn, const C*, int) {
+    using T = typename CT<C>::R;
+    const T q = (T)0.70710678118654752440;
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
+    Bfly<4>::run(e, sgn, (const C*)nullptr, 0);
+    Bfly<4>::run(o, sgn, (const C*)nullptr, 0);
     // twiddles W8^k = exp(sgn*i*pi*k/4)
-    double2 w1 = make_double2(q, sgn * q), w3 = make_double2(-q, sgn * q);
-    double2 o1 = cmul(o[1], w1), o2 = mul_i(o[2], sgn), o3 = cmul(o[3], w3);
+    C w1 = CT<C>::mk(q, sgn * q), w3 = CT<C>::mk(-q, sgn * q);
+    C o1 = cmul(o[1], w1), o2 = mul_i(o[2], sgn), o3 = cmul(o[3], w3);
     v[0] = cadd(e[0], o[0]);
     v[4] = csub(e[0], o[0]);
     v[1] = cadd(e[1], o1);
@@ -118,12 +142,13 @@ struct Bfly<8> {
 // generic prime radix through the twiddle table of the axis (tw[k] = W_N^k)
 template <int R>
 struct BflyGeneric {
-  __device__ __forceinline__ static void run(double2 (&v)[R], double, const double2* tw, int n) {
-    double2 out[R];
+  template <class C>
+  __device__ __forceinline__ static void run(C (&v)[R], typename CT<C>::R, const C* tw, int n) {
+    C out[R];
     const int step = n / R;
 #pragma unroll
     for (int s = 0; s < R; ++s) {
-      double2 acc = v[0];
+      C acc = v[0];
 #pragma unroll
       for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], tw[((q * s) % R) * step]));
       out[s] = acc;
@@ -141,13 +166,13 @@ struct Bfly<11> : BflyGeneric<11> {};
 // memory: element e of line L lives at buf[L*ls + e*es].  tw[k] = exp(sgn*2 pi i k/n).
 // jfast selects the thread mapping (consecutive threads -> consecutive j).
 // The caller guarantees nl*n/R <= blockDim.x * BPT.
-template <int R>
-__device__ __noinline__ void stage(double2* buf, int n, int ns, int line0, int nl, int ls, int es, bool jfast,
-                                      const double2* tw, double sgn) {
+template <int R, class C>
+__device__ __noinline__ void stage(C* buf, int n, int ns, int line0, int nl, int ls, int es, bool jfast,
+                                      const C* tw, typename CT<C>::R sgn) {
   constexpr int BPT = (kMaxV / R) > 0 ? (kMaxV / R) : 1;
   const int nq = n / R;
   const int total = nl * nq;
-  double2 v[BPT][R];
+  C v[BPT][R];
   int line_[BPT], j_[BPT];
 #pragma unroll
   for (int t = 0; t < BPT; ++t) {
@@ -162,10 +187,10 @@ __device__ __noinline__ void stage(double2* buf, int n, int ns, int line0, int n
       j_[t] = j;
       const int k = j % ns;
       const int tstep = n / (ns * R);
-      double2* base = buf + (size_t)line * ls;
+      C* base = buf + (size_t)line * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        double2 x = base[(size_t)(j + r * nq) * es];
+        C x = base[(size_t)(j + r * nq) * es];
         if (r && k) x = cmul(x, tw[(r * k * tstep) % n]);
         v[t][r] = x;
       }
@@ -178,7 +203,7 @@ __device__ __noinline__ void stage(double2* buf, int n, int ns, int line0, int n
     if (line_[t] >= 0) {
       const int j = j_[t], k = j % ns;
       const int idxd = (j / ns) * ns * R + k;
-      double2* base = buf + (size_t)line_[t] * ls;
+      C* base = buf + (size_t)line_[t] * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) base[(size_t)(idxd + r * ns) * es] = v[t][r];
     }
@@ -225,16 +250,16 @@ __host__ __device__ constexpr int chunk_lines(int N) {
   return lc;
 }
 
-template <int N, int R, int NS, int LC>
-__device__ __forceinline__ void stage_fixed(double2* buf, int line0, int nl, int ls, int es, bool jfast,
-                                            const double2* tw, double sgn) {
+template <int N, int R, int NS, int LC, class C>
+__device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, int es, bool jfast, const C* tw,
+                                            typename CT<C>::R sgn) {
   constexpr int BPT = bpt_of(R);
   constexpr int NQ = N / R;
   constexpr int TSTEP = N / (NS * R);
   // jfast: index space nl*NQ (line = bf / NQ); otherwise the full chunk LC*NQ
   // decoded modulo LC, with the lines beyond nl masked
   const int total = jfast ? nl * NQ : LC * NQ;
-  double2 v[BPT][R];
+  C v[BPT][R];
   int off_[BPT];
   bool act[BPT];
 #pragma unroll
@@ -247,10 +272,10 @@ __device__ __forceinline__ void stage_fixed(double2* buf, int line0, int nl, int
     const int k = j % NS;
     off_[t] = line * N + ((j / NS) * NS * R + k);  // (line, destination index) packed
     if (act[t]) {
-      double2* base = buf + (size_t)(line0 + line) * ls;
+      C* base = buf + (size_t)(line0 + line) * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        double2 x = base[(size_t)(j + r * NQ) * es];
+        C x = base[(size_t)(j + r * NQ) * es];
         if (r && k) x = cmul(x, tw[(r * k * TSTEP) % N]);
         v[t][r] = x;
       }
@@ -262,7 +287,7 @@ __device__ __forceinline__ void stage_fixed(double2* buf, int line0, int nl, int
   for (int t = 0; t < BPT; ++t) {
     if (act[t]) {
       const int line = off_[t] / N, idxd = off_[t] % N;
-      double2* base = buf + (size_t)(line0 + line) * ls;
+      C* base = buf + (size_t)(line0 + line) * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) base[(size_t)(idxd + r * NS) * es] = v[t][r];
     }
@@ -270,9 +295,9 @@ __device__ __forceinline__ void stage_fixed(double2* buf, int line0, int nl, int
   __syncthreads();
 }
 
-template <int N, int S, int NS, int LC>
-__device__ __forceinline__ void stages_fixed(double2* buf, int line0, int nl, int ls, int es, bool jfast,
-                                             const double2* tw, double sgn) {
+template <int N, int S, int NS, int LC, class C>
+__device__ __forceinline__ void stages_fixed(C* buf, int line0, int nl, int ls, int es, bool jfast, const C* tw,
+                                             typename CT<C>::R sgn) {
   constexpr RadixList L = radices_of(N);
   if constexpr (S < L.n) {
     constexpr int R = L.r[S];
@@ -281,8 +306,8 @@ __device__ __forceinline__ void stages_fixed(double2* buf, int line0, int nl, in
   }
 }
 
-template <int N>
-__device__ void transform_fixed(double2* buf, int nlines, int ls, int es, bool jfast, const double2* tw, double sgn) {
+template <int N, class C>
+__device__ void transform_fixed(C* buf, int nlines, int ls, int es, bool jfast, const C* tw, typename CT<C>::R sgn) {
   constexpr int LC = chunk_lines(N);
   for (int l0 = 0; l0 < nlines; l0 += LC) {
     const int nl = min(LC, nlines - l0);
@@ -302,8 +327,9 @@ __device__ __forceinline__ int lines_per_chunk(const AxisArg& ax, int nlines) {
   return lc;
 }
 
-__device__ void transform(double2* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast,
-                          const double2* tw, double sgn) {
+template <class C>
+__device__ void transform(C* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast, const C* tw,
+                          typename CT<C>::R sgn) {
   switch (ax.n) {
     case 16: transform_fixed<16>(buf, nlines, ls, es, jfast, tw, sgn); return;
     case 20: transform_fixed<20>(buf, nlines, ls, es, jfast, tw, sgn); return;
@@ -339,73 +365,91 @@ __device__ void transform(double2* buf, const AxisArg& ax, int nlines, int ls, i
   }
 }
 
-// load twiddles exp(sgn*2 pi i k/n) from the table exp(+2 pi i k/n)
-__device__ void load_tw(double2* dst, const double2* src, int n, double sgn) {
+// load twiddles exp(sgn*2 pi i k/n) from the FP64 table exp(+2 pi i k/n)
+template <class C>
+__device__ void load_tw(C* dst, const double2* src, int n, double sgn) {
+  using T = typename CT<C>::R;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     double2 w = src[k];
-    dst[k] = make_double2(w.x, sgn * w.y);
+    dst[k] = CT<C>::mk((T)w.x, (T)(sgn * w.y));
   }
 }
 
+template <class C>
+__device__ __forceinline__ C from_d2(double2 a) {
+  using T = typename CT<C>::R;
+  return CT<C>::mk((T)a.x, (T)a.y);
+}
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2((double)a.x, (double)a.y); }
+
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPlaneThreads, 2) k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
-                             const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
-                             double2* __restrict__ grid, int nzp, AxisArg a1, AxisArg a2,
-                             const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
-  extern __shared__ double2 sm[];
+// The kernels take the work-grid type C (double2 or float2); the sphere
+// coefficients psi/out stay FP64 and are converted at the gather/scatter.
+template <class C>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
+                 const int* __restrict__ plane_g, const int* __restrict__ plane_pos, C* __restrict__ grid, int nzp,
+                 AxisArg a1, AxisArg a2, const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
   const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2;
-  double2* plane = sm;
-  double2* tw1 = sm + npl;
-  double2* tw2 = tw1 + nr1;
+  C* plane = sm;
+  C* tw1 = sm + npl;
+  C* tw2 = tw1 + nr1;
   const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
-  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = CT<C>::mk(0, 0);
   load_tw(tw1, tw1g, nr1, +1.0);
   load_tw(tw2, tw2g, nr2, +1.0);
   __syncthreads();
   const double2* src = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x)
-    plane[plane_pos[k]] = src[plane_g[k]];
+    plane[plane_pos[k]] = from_d2<C>(src[plane_g[k]]);
   __syncthreads();
-  transform(plane, a1, nr2, nr1, 1, true, tw1, +1.0);   // x lines
-  transform(plane, a2, nr1, 1, nr1, false, tw2, +1.0);  // y lines
-  double2* dst = grid + ((size_t)bl * nzp + p) * npl;
+  transform(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)1);   // x lines
+  transform(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)1);  // y lines
+  C* dst = grid + ((size_t)bl * nzp + p) * npl;
   for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i];
 }
 
 constexpr int kTX = 16;  // x columns per z-column block
 
-__global__ void __launch_bounds__(kPlaneThreads, 2) k_zcol_v(double2* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot,
-                         int nzp, int nr1, int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
-  extern __shared__ double2 sm[];
+template <class C>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_zcol_v(C* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot, int nzp, int nr1,
+             int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
+  using T = typename CT<C>::R;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
   const int nr3 = a3.n;
-  double2* tile = sm;             // [nr3][kTX]
-  double2* tw = sm + nr3 * kTX;
+  C* tile = sm;             // [nr3][kTX]
+  C* tw = sm + nr3 * kTX;
   const int nxb = (nr1 + kTX - 1) / kTX;
   const int iy = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * kTX;
   const int bl = blockIdx.y;
   const size_t npl = (size_t)nr1 * nr2;
-  double2* gb = grid + (size_t)bl * nzp * npl;
+  C* gb = grid + (size_t)bl * nzp * npl;
   load_tw(tw, tw3g, nr3, +1.0);
   for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
     int iz = i / kTX, x = i % kTX;
     int s = zslot[iz];
-    double2 val = make_double2(0.0, 0.0);
+    C val = CT<C>::mk(0, 0);
     if (s >= 0 && x0 + x < nr1) val = gb[(size_t)s * npl + (size_t)iy * nr1 + x0 + x];
     tile[i] = val;
   }
   __syncthreads();
-  transform(tile, a3, kTX, 1, kTX, false, tw, +1.0);
+  transform(tile, a3, kTX, 1, kTX, false, tw, (T)1);
   for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
     int iz = i / kTX, x = i % kTX;
     double vv = 0.0;
     if (x0 + x < nr1) vv = v[(size_t)x0 + x + (size_t)nr1 * (iy + (size_t)nr2 * iz)] * scale;
-    tile[i] = cscale(tile[i], vv);
+    tile[i] = cscale(tile[i], (T)vv);
   }
   __syncthreads();
   // forward transform: conjugated twiddles
   for (int k = threadIdx.x; k < nr3; k += blockDim.x) tw[k].y = -tw[k].y;
   __syncthreads();
-  transform(tile, a3, kTX, 1, kTX, false, tw, -1.0);
+  transform(tile, a3, kTX, 1, kTX, false, tw, (T)-1);
   for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
     int iz = i / kTX, x = i % kTX;
     int s = zslot[iz];
@@ -413,30 +457,32 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) k_zcol_v(double2* __restrict
   }
 }
 
-__global__ void __launch_bounds__(kPlaneThreads, 2) k_rtog_plane(const double2* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
-                             const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
-                             double2* __restrict__ out, const double2* __restrict__ psi, int ldg, int b0,
-                             const double* __restrict__ g2, const double* __restrict__ bucket, int add_kin,
-                             AxisArg a1, AxisArg a2, const double2* __restrict__ tw1g,
-                             const double2* __restrict__ tw2g) {
-  extern __shared__ double2 sm[];
+template <class C>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_rtog_plane(const C* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
+                 const int* __restrict__ plane_g, const int* __restrict__ plane_pos, double2* __restrict__ out,
+                 const double2* __restrict__ psi, int ldg, int b0, const double* __restrict__ g2,
+                 const double* __restrict__ bucket, int add_kin, AxisArg a1, AxisArg a2,
+                 const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
   const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2;
-  double2* plane = sm;
-  double2* tw1 = sm + npl;
-  double2* tw2 = tw1 + nr1;
+  C* plane = sm;
+  C* tw1 = sm + npl;
+  C* tw2 = tw1 + nr1;
   const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
-  const double2* srcp = grid + ((size_t)bl * nzp + p) * npl;
+  const C* srcp = grid + ((size_t)bl * nzp + p) * npl;
   for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = srcp[i];
   load_tw(tw1, tw1g, nr1, -1.0);
   load_tw(tw2, tw2g, nr2, -1.0);
   __syncthreads();
-  transform(plane, a2, nr1, 1, nr1, false, tw2, -1.0);  // y lines
-  transform(plane, a1, nr2, nr1, 1, true, tw1, -1.0);   // x lines
+  transform(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)-1);  // y lines
+  transform(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)-1);   // x lines
   double2* dst = out + (size_t)ldg * b;
   const double2* ps = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
     int g = plane_g[k];
-    double2 val = plane[plane_pos[k]];
+    double2 val = to_d2(plane[plane_pos[k]]);
     if (add_kin) {
       double kin = 0.5 * g2[g] + (bucket ? bucket[g] : 0.0);
       double2 c = ps[g];
@@ -480,7 +526,9 @@ int fft_setup(Handle* h, const int* igvec) {
       return h->fail(CUW_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has a prime factor above 11");
   }
   const size_t npl = (size_t)nr1 * nr2;
-  if (npl + nr1 + nr2 > (size_t)(220 * 1024) / sizeof(double2) || (size_t)nr3 * kTX + nr3 > 14000)
+  // work-grid element: FP64 complex, or FP32 complex on the mixed path
+  const size_t es = h->mixed() ? sizeof(float2) : sizeof(double2);
+  if ((npl + nr1 + nr2) * es > (size_t)(220 * 1024) || ((size_t)nr3 * kTX + nr3) * es > 14000 * sizeof(double2))
     return h->fail(CUW_ERR_UNSUPPORTED, "FFT plane too large for shared memory");
   // occupied planes and the per-plane G lists
   std::vector<int> cnt(nr3, 0);
@@ -510,7 +558,7 @@ int fft_setup(Handle* h, const int* igvec) {
   }
   h->nzp = nzp;
   // band batch: keep the work grid near 48 MB so that it stays in L2
-  const size_t per_band = (size_t)nzp * npl * sizeof(double2);
+  const size_t per_band = (size_t)nzp * npl * es;
   int batch = (int)std::max<size_t>(1, (48u << 20) / per_band);
   batch = std::min(batch, h->d.nbh);
   h->batch = batch;
@@ -541,42 +589,56 @@ int fft_setup(Handle* h, const int* igvec) {
     CUW_TRY(cudaMalloc(tws[a], sizeof(double2) * n));
     CUW_TRY(cudaMemcpy(*tws[a], t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   }
-  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(double2));
-  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(double2));
-  CUW_TRY(cudaFuncSetAttribute(k_gtor_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-  CUW_TRY(cudaFuncSetAttribute(k_rtog_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-  CUW_TRY(cudaFuncSetAttribute(k_zcol_v, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  const int smem_plane = (int)((npl + nr1 + nr2) * es);
+  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * es);
+  if (h->mixed()) {
+    CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+    CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+    CUW_TRY(cudaFuncSetAttribute(k_zcol_v<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  } else {
+    CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+    CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+    CUW_TRY(cudaFuncSetAttribute(k_zcol_v<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  }
   return CUW_OK;
 }
 
 // out = FFT_RTOG[ V * FFT_GTOR[psi] ] (+ 1/2 G^2 psi + bucket psi when add_kinetic)
-int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
+template <class C>
+static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   const size_t npl = (size_t)nr1 * nr2;
-  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(double2));
-  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(double2));
+  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
+  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(C));
   const int tp = kPlaneThreads;
   const int tz = kPlaneThreads;
   AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
   const double scale = 1.0 / ((double)nr1 * nr2 * nr3);
   Device& g = h->g;
+  C* grid = reinterpret_cast<C*>(g.grid);
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
-    k_gtor_plane<<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
-                                                                   g.plane_pos, g.grid, h->nzp, a1, a2, g.tw1,
-                                                                   g.tw2);
+    k_gtor_plane<C><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
+                                                                      g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
+                                                                      g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
     const int nxb = (nr1 + kTX - 1) / kTX;
-    k_zcol_v<<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(g.grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
-                                                             scale);
+    k_zcol_v<C><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
+                                                                scale);
     CUW_LAUNCH_CHECK("k_zcol_v");
-    k_rtog_plane<<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(g.grid, h->nzp, g.plane_off, g.plane_g,
-                                                                   g.plane_pos, out, psi, h->ldg, b0, g.g2,
-                                                                   g.bucket, add_kinetic ? 1 : 0, a1, a2,
-                                                                   g.tw1, g.tw2);
+    k_rtog_plane<C><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
+                                                                      g.plane_pos, out, psi, h->ldg, b0, g.g2,
+                                                                      g.bucket, add_kinetic ? 1 : 0, a1, a2,
+                                                                      g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_rtog_plane");
   }
   return CUW_OK;
+}
+
+// FP64 transforms, or FP32 transforms and V(r) product on the mixed path
+int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
+  if (h->mixed()) return fft_vpsi_t<float2>(h, psi, out, add_kinetic);
+  return fft_vpsi_t<double2>(h, psi, out, add_kinetic);
 }
 
 }  // namespace cuw

@@ -183,12 +183,9 @@ constexpr size_t smem_bytes() {
   return sizeof(double) * 2 * 2 * TILE * (((MODE == MP21) ? 2 : 1) + ((MODE == MP12 || MODE == MPGRAM) ? 2 : 1));
 }
 
-// PRO(g,p) generated from the tables
 __device__ __forceinline__ double2 gen_pro(int g, int ngl, const ProDesc& d, const double* __restrict__ ylm,
                                            const double* __restrict__ pro, const double2* __restrict__ eigr) {
-  double s = ylm[(size_t)g + (size_t)ngl * d.lm] * pro[(size_t)g + (size_t)ngl * d.ibare];
-  double2 e = cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]);
-  return make_double2(s * e.x, s * e.y);
+  return pro_value(g, ngl, d, ylm, pro, eigr);
 }
 
 // ---------------------------------------------------------------------------
@@ -285,10 +282,6 @@ __global__ void k_reduce_parts(const double2* __restrict__ part, int nz, size_t 
 // mode ADDPRO_OPSI : opsi  = (psi0 + PRO*C2) * dt^2/((1+annee) m_G)
 // mode ADDPRO_FUSED: both, then psim = a1 psi0 + a2 psim + a3/m_G hpsi
 // ---------------------------------------------------------------------------
-struct StepCoef {
-  double a1, a2, a3, oscale;
-};
-
 template <int MODE>
 __global__ void __launch_bounds__(NT, 1) k_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi,
                                                   const double2* __restrict__ psi0, double2* __restrict__ psim,
@@ -629,7 +622,7 @@ __global__ void k_oproj(const double2* __restrict__ proj, const double* __restri
 // host side
 // ---------------------------------------------------------------------------
 
-static int ensure_part(Handle* h, size_t bytes) {
+int ensure_part(Handle* h, size_t bytes) {
   if (bytes <= h->g.part_bytes) return CUW_OK;
   if (h->g.part) cudaFree(h->g.part);
   h->g.part = nullptr;
@@ -654,6 +647,10 @@ int eigr_compute(Handle* h, const double* r_dev) {
 
 // projA = Omega <p|psiA>, projB likewise when psiB != null; uses h->g.eigr
 int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* psiB, double2* projB) {
+  if (h->mixed()) {
+    CUW_RET(tc_proj(h, psiA, projA));
+    return psiB ? tc_proj(h, psiB, projB) : CUW_OK;
+  }
   const int nbh = h->d.nbh, npro = h->npro, ngl = h->d.ngl;
   const int tn = ceil_div(npro, BN), tm = ceil_div(nbh, BM);
   int ks = choose_split(h, tn * tm, ngl, 256);
@@ -689,6 +686,7 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
   sc.a2 = 1.0 - sc.a1;
   sc.a3 = -h->delt * h->delt / (1.0 + h->annee);
   sc.oscale = h->delt * h->delt / (1.0 + h->annee);  // src/paw_waves2.f90:148-156
+  if (h->mixed()) return tc_addpro(h, mode, hpc, opc, sc);
   Device& g = h->g;
   switch (mode) {
     case ADDPRO_HPSI:
@@ -739,6 +737,7 @@ int oproj_compute(Handle* h, const double2* proj, double2* out) {
 // offset `dst` (complex), scaled by `scale`.
 static int gram_run(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
                     double scale, double2* dst) {
+  if (h->mixed()) return tc_gram(h, pairs, npair, minus, nk, nm, sk, sm, scale, dst);
   GramArgs a;
   for (int i = 0; i < npair; ++i) a.pair[i] = pairs[i];
   a.npair = npair;
@@ -786,6 +785,7 @@ int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* 
   a.sxk = (size_t)h->ldg;
   a.som = 1;
   a.son = (size_t)h->ldg;
+  if (h->mixed()) return tc_addx(h, true, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
   k_addx<true, true><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
@@ -805,6 +805,7 @@ int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* 
   a.sxk = 1;
   a.som = (size_t)h->d.nbh;  // out(m=p, n=b) at b + nbh*p
   a.son = 1;
+  if (h->mixed()) return tc_addx(h, false, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
   k_addx<false, false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
@@ -813,12 +814,18 @@ int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* 
 
 int force_gemm(Handle* h, const double2* ded, double* force_dev) {
   const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
-  const int tm = ceil_div(ngl, BM), tn = ceil_div(npro, BN);
-  CUW_RET(ensure_part(h, sizeof(double) * 3 * (size_t)tm * npro));
+  int tm = ceil_div(ngl, BM);
+  const int tn = ceil_div(npro, BN);
+  CUW_RET(ensure_part(h, sizeof(double) * 3 * (size_t)std::max(tm, ceil_div(ngl, 128)) * npro));
   double* fpart = reinterpret_cast<double*>(h->g.part);
-  k_force<<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro,
-                                              h->g.eigr, h->g.gx, h->g.gy, h->g.gz, fpart);
-  CUW_LAUNCH_CHECK("k_force");
+  if (h->mixed()) {
+    CUW_RET(tc_force(h, ded, fpart, &tm));
+  } else {
+    k_force<<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc,
+                                                                 h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
+                                                                 h->g.gz, fpart);
+    CUW_LAUNCH_CHECK("k_force");
+  }
   TabView t = tables(h);
   k_force_final<<<dim3(3, h->d.nat), 128, 0, h->stream>>>(fpart, tm, npro, t.ipro0, t.nlmn, h->d.nat, h->gweight,
                                                           force_dev);

@@ -1,0 +1,527 @@
+// Mixed-precision contractions on the 5th-generation tensor cores (tcgen05).
+//
+// Every product is a real GEMM C = A * B^T whose FP64 operands are split on the
+// fly into tf32 pairs (hi + lo) and multiplied as hi*hi + hi*lo + lo*hi with
+// fp32 accumulation in tensor memory (three-term split precision), drained
+// after every K = 8 step into register sums (tc_pipe.cuh).  Complex products
+// use the real form of tc_pipe.cuh.  Every wait is bounded; a wait that runs
+// out sets an error flag and the kernel leaves through its cleanup path (TMEM
+// released) instead of hanging.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "cuwaves_internal.cuh"
+#include "tc_pipe.cuh"
+
+namespace cuw {
+namespace {
+
+// Real K values per shared-memory stage (four MMA steps of K = 8).  The
+// accumulation run stays one MMA step: the tensor core's truncating fp32
+// accumulation was measured on B200 at a signed mean error of -3.7e-8 /
+// -8.7e-8 / -1.8e-7 of |C| for runs of 8 / 16 / 32 real K, and one step keeps
+// the energy bias below 1e-6 Ha/atom.
+constexpr int kBK = 32, kCK = kBK / 2, kStages = 3, kNPW = 4;
+using MPipe = tc::Pipe<kBK, kStages, kNPW>;
+constexpr int kProd = MPipe::kProducers;
+// k_tc_force reuses the stage buffers for a 128 x 64 FP64 tile
+static_assert(sizeof(float) * kStages * MPipe::kStage >= sizeof(double) * 128 * 64, "stage area too small");
+
+__device__ __forceinline__ double2 dz() { return make_double2(0.0, 0.0); }
+
+// ---------------------------------------------------------------------------
+// Plain real GEMM C(M,N) = A(M,K) * B(N,K)^T, FP64 in and out, row-major with
+// K contiguous: the reference product of the split-precision machinery.
+// One CTA computes a 128 x 128 tile over the whole K range.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(MPipe::kThreads, 1)
+    k_tf32x3_gemm(int M, int N, int K, const double* __restrict__ A, const double* __restrict__ B,
+                  double* __restrict__ C, int* __restrict__ err) {
+  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 128;
+  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
+    const int k0 = c * kBK;
+    for (int it = t; it < 128 * (kBK / 4); it += kProd) {
+      const int r = it % 128, g = it / 128, k = k0 + 4 * g;
+      double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (m0 + r < M && k + q < K) a[q] = A[(size_t)(m0 + r) * K + k + q];
+        if (n0 + r < N && k + q < K) b[q] = B[(size_t)(n0 + r) * K + k + q];
+      }
+      tc::store_split4(ahi, alo, tc::tile_f4(r, g), a[0], a[1], a[2], a[3]);
+      tc::store_split4(bhi, blo, tc::tile_f4(r, g), b[0], b[1], b[2], b[3]);
+    }
+  };
+  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+    if (m0 + row >= M) return;
+    double* out = C + (size_t)(m0 + row) * N + n0 + col0;
+    const int nc = min(MPipe::kCols, N - n0 - col0);
+#pragma unroll
+    for (int j = 0; j < MPipe::kCols; ++j)
+      if (j < nc) out[j] = (double)acc[j];
+  };
+  tc::pipe_run<kBK, kStages, kNPW>((K + kBK - 1) / kBK, produce, finish, err);
+}
+
+// out[i] = scale * sum_z part[z*n + i], summed in FP64 in a fixed order
+__global__ void k_tc_reduce(const float2* __restrict__ part, int nz, size_t n, double scale,
+                            double2* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double sx = 0.0, sy = 0.0;
+    for (int z = 0; z < nz; ++z) {
+      const float2 v = part[(size_t)z * n + i];
+      sx += (double)v.x;
+      sy += (double)v.y;
+    }
+    out[i] = make_double2(sx * scale, sy * scale);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// <p|psi> partial sums (WAVES_PROJECTIONS, src/paw_waves1.f90:5746-5905):
+// part[z][p][b] = sum_{g in split z} conj(PRO(g,p)) psi(g,b)   (float2)
+// M = projectors (blockIdx.x), N = 64 bands (blockIdx.y), K = g (blockIdx.z)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(MPipe::kThreads, 1)
+    k_tc_proj(const double2* __restrict__ psi, int ldg, int ngl, int nbh, int npro, int kchunk,
+              const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm, const double* __restrict__ pro,
+              const double2* __restrict__ eigr, float2* __restrict__ part, int* __restrict__ err) {
+  __shared__ ProDesc sd[128];
+  const int m0 = blockIdx.x * 128, b0 = blockIdx.y * 64;
+  const int gbeg = blockIdx.z * kchunk, gend = min(ngl, gbeg + kchunk);
+  for (int t = threadIdx.x; t < 128; t += blockDim.x) sd[t] = m0 + t < npro ? pdesc[m0 + t] : ProDesc{0, 0, 0, -1};
+  __syncthreads();
+  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
+    const int g0 = gbeg + c * kCK;
+    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
+      const int r = it % 128, gi = it / 128, g = g0 + 2 * gi;
+      const ProDesc d = sd[r];
+      double2 a0 = dz(), a1 = dz();
+      if (d.l >= 0) {
+        if (g < gend) a0 = cconj(pro_value(g, ngl, d, ylm, pro, eigr));
+        if (g + 1 < gend) a1 = cconj(pro_value(g + 1, ngl, d, ylm, pro, eigr));
+      }
+      tc::put_a(ahi, alo, r, gi, a0, a1);
+    }
+    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
+      const int j = it % 64, gi = it / 64, g = g0 + 2 * gi, b = b0 + j;
+      double2 c0 = dz(), c1 = dz();
+      if (b < nbh) {
+        if (g < gend) c0 = psi[(size_t)g + (size_t)ldg * b];
+        if (g + 1 < gend) c1 = psi[(size_t)g + 1 + (size_t)ldg * b];
+      }
+      tc::put_b(bhi, blo, j, gi, c0, c1);
+    }
+  };
+  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+    const int p = m0 + row;
+    if (p >= npro) return;
+    float2* out = part + ((size_t)blockIdx.z * npro + p) * nbh;
+    const int bb = b0 + col0 / 2;
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (bb + j < nbh) out[bb + j] = make_float2(acc[2 * j], acc[2 * j + 1]);
+  };
+  const int nchunk = gend > gbeg ? (gend - gbeg + kCK - 1) / kCK : 0;
+  tc::pipe_run<kBK, kStages, kNPW>(nchunk, produce, finish, err);
+}
+
+// ---------------------------------------------------------------------------
+// ADDPRO with the step epilogues (WAVES_ADDPRO, src/paw_waves1.f90:5908-6067,
+// and the epilogues of the FP64 k_addpro): 128 g x 32 bands per CTA, the tile
+// columns hold C1 (hproj) products for the bands, then C2 (oproj) products.
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(MPipe::kThreads, 1)
+    k_tc_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi, const double2* __restrict__ psi0,
+                double2* __restrict__ psim, const double* __restrict__ mpsi, int ldg, int ngl, int nbh, int npro,
+                const double2* __restrict__ c1, const double2* __restrict__ c2, const ProDesc* __restrict__ pdesc,
+                const double* __restrict__ ylm, const double* __restrict__ pro, const double2* __restrict__ eigr,
+                StepCoef sc, int* __restrict__ err) {
+  constexpr bool USE_H = (MODE != ADDPRO_OPSI);
+  constexpr bool USE_O = (MODE != ADDPRO_HPSI);
+  const int g0 = blockIdx.x * 128, b0 = blockIdx.y * 32;
+  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
+    const int p0 = c * kCK;
+    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
+      const int r = it % 128, pi = it / 128, g = g0 + r, p = p0 + 2 * pi;
+      double2 a0 = dz(), a1 = dz();
+      if (g < ngl) {
+        if (p < npro) a0 = pro_value(g, ngl, pdesc[p], ylm, pro, eigr);
+        if (p + 1 < npro) a1 = pro_value(g, ngl, pdesc[p + 1], ylm, pro, eigr);
+      }
+      tc::put_a(ahi, alo, r, pi, a0, a1);
+    }
+    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
+      const int j = it % 64, pi = it / 64, mt = j / 32, b = b0 + (j % 32), p = p0 + 2 * pi;
+      const double2* cm = mt == 0 ? c1 : c2;
+      const bool use = mt == 0 ? USE_H : USE_O;
+      double2 x0 = dz(), x1 = dz();
+      if (use && b < nbh) {
+        if (p < npro) x0 = cm[(size_t)b + (size_t)nbh * p];
+        if (p + 1 < npro) x1 = cm[(size_t)b + (size_t)nbh * (p + 1)];
+      }
+      tc::put_b(bhi, blo, j, pi, x0, x1);
+    }
+  };
+  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+    const int g = g0 + row;
+    if (g >= ngl) return;
+    const double rm = 1.0 / mpsi[g];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int b = b0 + j;
+      if (b >= nbh) continue;
+      const size_t k = (size_t)g + (size_t)ldg * b;
+      const double2 v = make_double2((double)acc[2 * j], (double)acc[2 * j + 1]);
+      if (col0 == 0 && USE_H) {
+        const double2 hv = cadd(hpsi[k], v);
+        hpsi[k] = hv;
+        if (MODE == ADDPRO_FUSED) {
+          const double2 p0v = psi0[k], pm = psim[k];
+          const double a3 = sc.a3 * rm;
+          psim[k] = make_double2(sc.a1 * p0v.x + sc.a2 * pm.x + a3 * hv.x, sc.a1 * p0v.y + sc.a2 * pm.y + a3 * hv.y);
+        }
+      } else if (col0 != 0 && USE_O) {
+        const double2 p0v = psi0[k];
+        const double s = sc.oscale * rm;
+        opsi[k] = make_double2((p0v.x + v.x) * s, (p0v.y + v.y) * s);
+      }
+    }
+  };
+  tc::pipe_run<kBK, kStages, kNPW>((npro + kCK - 1) / kCK, produce, finish, err);
+}
+
+// ---------------------------------------------------------------------------
+// Gram products (PLANEWAVE$SCALARPRODUCT, src/paw_fft.f90:2344-2422, for
+// WAVES_OVERLAP and WAVES_1COVERLAP): for pair (X, Y)
+//   T1(m,n) = sum_k conj(X(k,m)) Y(k,n)
+//   T2(m,n) = sum_k X(k,m) Y(-k,n) = sum_k X(-k,m) Y(k,n)   (MINUS; the sphere
+//             is closed under k -> -k), else sum_k X(k,m) Y(k,n)
+// Tile rows 0..63: conj(X) for T1, rows 64..127: X(-k) for T2, sharing the
+// Y columns.  Partials part[z][t][m + nm n] (float2), z = split*npair + pair.
+// ---------------------------------------------------------------------------
+struct TcGramArgs {
+  GramPair pair[3];
+  int npair, nk, nm;
+  size_t sk, sm;
+  int kchunk;
+};
+
+template <bool MINUS>
+__global__ void __launch_bounds__(MPipe::kThreads, 1)
+    k_tc_gram(TcGramArgs a, const int* __restrict__ minusg, float2* __restrict__ part, int* __restrict__ err) {
+  const int pair = blockIdx.z % a.npair, split = blockIdx.z / a.npair;
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  const double2* X = a.pair[pair].x;
+  const double2* Y = a.pair[pair].y;
+  const int kbeg = split * a.kchunk, kend = min(a.nk, kbeg + a.kchunk);
+  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
+    const int k0 = kbeg + c * kCK;
+    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
+      const int r = it % 128, ki = it / 128, k = k0 + 2 * ki, m = m0 + (r & 63);
+      double2 v[2] = {dz(), dz()};
+      if (m < a.nm) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (k + q >= kend) continue;
+          if (r < 64) {
+            v[q] = cconj(X[(size_t)(k + q) * a.sk + (size_t)m * a.sm]);
+          } else {
+            const int kk = MINUS ? minusg[k + q] : k + q;
+            v[q] = X[(size_t)kk * a.sk + (size_t)m * a.sm];
+          }
+        }
+      }
+      tc::put_a(ahi, alo, r, ki, v[0], v[1]);
+    }
+    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
+      const int j = it % 64, ki = it / 64, k = k0 + 2 * ki, n = n0 + j;
+      double2 y0 = dz(), y1 = dz();
+      if (n < a.nm) {
+        if (k < kend) y0 = Y[(size_t)k * a.sk + (size_t)n * a.sm];
+        if (k + 1 < kend) y1 = Y[(size_t)(k + 1) * a.sk + (size_t)n * a.sm];
+      }
+      tc::put_b(bhi, blo, j, ki, y0, y1);
+    }
+  };
+  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+    const int t = row >> 6, m = m0 + (row & 63);
+    if (m >= a.nm) return;
+    const size_t mn = (size_t)a.nm * a.nm;
+    float2* out = part + ((size_t)blockIdx.z * 2 + t) * mn;
+    const int nb = n0 + col0 / 2;
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (nb + j < a.nm) out[(size_t)m + (size_t)a.nm * (nb + j)] = make_float2(acc[2 * j], acc[2 * j + 1]);
+  };
+  const int nchunk = kend > kbeg ? (kend - kbeg + kCK - 1) / kCK : 0;
+  tc::pipe_run<kBK, kStages, kNPW>(nchunk, produce, finish, err);
+}
+
+// ---------------------------------------------------------------------------
+// ADDOPSI / ADDOPROJ (src/paw_waves2.f90:547-615, 687-758):
+//   out(m,n) += sum_k X(m,k) L1(k,n) + conj(X(m',k)) L2(k,n),
+//   m' = minusg[m] (XMINUS) or m.  K runs over both halves (2 nk).
+// ---------------------------------------------------------------------------
+struct TcAddXArgs {
+  double2* out;
+  const double2* x;
+  const double2* l1;
+  const double2* l2;
+  int nm, nn, nk;
+  size_t sxm, sxk, som, son;
+};
+
+template <bool XMINUS>
+__global__ void __launch_bounds__(MPipe::kThreads, 1)
+    k_tc_addx(TcAddXArgs a, const int* __restrict__ minusg, int* __restrict__ err) {
+  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 64;
+  const int ktot = 2 * a.nk;
+  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
+    const int kg0 = c * kCK;
+    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
+      const int r = it % 128, ki = it / 128, m = m0 + r;
+      double2 v[2] = {dz(), dz()};
+      if (m < a.nm) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int kg = kg0 + 2 * ki + q;
+          if (kg >= ktot) continue;
+          if (kg < a.nk) {
+            v[q] = a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
+          } else {
+            const int mm = XMINUS ? minusg[m] : m;
+            v[q] = cconj(a.x[(size_t)mm * a.sxm + (size_t)(kg - a.nk) * a.sxk]);
+          }
+        }
+      }
+      tc::put_a(ahi, alo, r, ki, v[0], v[1]);
+    }
+    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
+      const int j = it % 64, ki = it / 64, n = n0 + j;
+      double2 w[2] = {dz(), dz()};
+      if (n < a.nn) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int kg = kg0 + 2 * ki + q;
+          if (kg >= ktot) continue;
+          w[q] = kg < a.nk ? a.l1[(size_t)kg + (size_t)a.nk * n] : a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
+        }
+      }
+      tc::put_b(bhi, blo, j, ki, w[0], w[1]);
+    }
+  };
+  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+    const int m = m0 + row;
+    if (m >= a.nm) return;
+    const int nb = n0 + col0 / 2;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (nb + j >= a.nn) continue;
+      const size_t k = (size_t)m * a.som + (size_t)(nb + j) * a.son;
+      const double2 o = a.out[k];
+      a.out[k] = make_double2(o.x + (double)acc[2 * j], o.y + (double)acc[2 * j + 1]);
+    }
+  };
+  tc::pipe_run<kBK, kStages, kNPW>((ktot + kCK - 1) / kCK, produce, finish, err);
+}
+
+// ---------------------------------------------------------------------------
+// Forces (WAVES_DEDPRO + WAVES_PROFORCE, src/paw_waves1.f90:5694-5743,
+// 6112-6234): D(g,p) = sum_b psi0(g,b) conj(E(b,p)) on the tensor cores for
+// 128 g x 64 projectors, then sv(g,p) = Re[i P (-i)^l EIGR conj(D)] Y_lm in the
+// drain warps (into the freed stage buffers) and fpart[tile][p][c] =
+// sum_g sv(g,p) G_c(g) by the whole CTA.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(MPipe::kThreads, 1)
+    k_tc_force(const double2* __restrict__ psi0, int ldg, int ngl, int nbh, int npro,
+               const double2* __restrict__ ded, const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+               const double* __restrict__ pro, const double2* __restrict__ eigr, const double* __restrict__ gx,
+               const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ fpart,
+               int* __restrict__ err) {
+  const int g0 = blockIdx.x * 128, p0 = blockIdx.y * 64;
+  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
+    const int bb = c * kCK;
+    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
+      const int r = it % 128, bi = it / 128, g = g0 + r, b = bb + 2 * bi;
+      double2 a0 = dz(), a1 = dz();
+      if (g < ngl) {
+        if (b < nbh) a0 = psi0[(size_t)g + (size_t)ldg * b];
+        if (b + 1 < nbh) a1 = psi0[(size_t)g + (size_t)ldg * (b + 1)];
+      }
+      tc::put_a(ahi, alo, r, bi, a0, a1);
+    }
+    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
+      const int j = it % 64, bi = it / 64, p = p0 + j, b = bb + 2 * bi;
+      double2 e0 = dz(), e1 = dz();
+      if (p < npro) {
+        if (b < nbh) e0 = cconj(ded[(size_t)b + (size_t)nbh * p]);
+        if (b + 1 < nbh) e1 = cconj(ded[(size_t)b + 1 + (size_t)nbh * p]);
+      }
+      tc::put_b(bhi, blo, j, bi, e0, e1);
+    }
+  };
+  double* sv = reinterpret_cast<double*>(tc::pipe_stage_base());  // [128][64]
+  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+    const int g = g0 + row, pb = col0 / 2;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int p = p0 + pb + j;
+      double v = 0.0;
+      if (g < ngl && p < npro) {
+        const ProDesc d = pdesc[p];
+        const double pr = pro[(size_t)g + (size_t)ngl * d.ibare];
+        const double y = ylm[(size_t)g + (size_t)ngl * d.lm];
+        const double2 cw = cmul(make_double2(0.0, pr), cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]));
+        v = (cw.x * (double)acc[2 * j] + cw.y * (double)acc[2 * j + 1]) * y;
+      }
+      sv[row * 64 + pb + j] = v;
+    }
+  };
+  tc::pipe_run<kBK, kStages, kNPW>((nbh + kCK - 1) / kCK, produce, finish, err);
+  // pipe_run ended with a CTA barrier: sv is complete (if a wait ran out the
+  // error flag is set and the caller discards the result)
+  for (int i = threadIdx.x; i < 64 * 3; i += blockDim.x) {
+    const int pl = i / 3, c = i % 3, p = p0 + pl;
+    if (p >= npro) continue;
+    const double* gc = c == 0 ? gx : (c == 1 ? gy : gz);
+    double s = 0.0;
+    for (int r = 0; r < 128 && g0 + r < ngl; ++r) s += sv[r * 64 + pl] * gc[g0 + r];
+    fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = s;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side of the split-precision contractions
+// ---------------------------------------------------------------------------
+static int* tc_err(Handle* h) { return h->g.ostatus + 12; }
+
+// number of K splits so that tiles * splits fills the GPU once (one CTA per SM)
+static int tc_splits(Handle* h, int tiles, int nk) {
+  const int want = std::max(1, ceil_div(h->nsm, std::max(1, tiles)));
+  return std::max(1, std::min(want, ceil_div(nk, 4 * kCK)));
+}
+
+int tc_setup(Handle* h) {
+  const int sm = (int)MPipe::kSmem;
+  CUW_TRY(cudaFuncSetAttribute(k_tc_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_addpro<ADDPRO_HPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_addpro<ADDPRO_OPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_addpro<ADDPRO_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_gram<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_gram<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_addx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_addx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(cudaFuncSetAttribute(k_tc_force, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  return CUW_OK;
+}
+
+static int tc_reduce(Handle* h, const float2* part, int nz, size_t n, double scale, double2* out) {
+  const int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)4 * h->nsm);
+  k_tc_reduce<<<rb, 256, 0, h->stream>>>(part, nz, n, scale, out);
+  CUW_LAUNCH_CHECK("k_tc_reduce");
+  return CUW_OK;
+}
+
+int tc_proj(Handle* h, const double2* psi, double2* proj) {
+  const int nbh = h->d.nbh, npro = h->npro, ngl = h->d.ngl;
+  const int tn = ceil_div(npro, 128), tb = ceil_div(nbh, 64);
+  int ks = tc_splits(h, tn * tb, ngl);
+  const int kchunk = ceil_div(ceil_div(ngl, ks), kCK) * kCK;
+  ks = ceil_div(ngl, kchunk);
+  const size_t n = (size_t)nbh * npro;
+  CUW_RET(ensure_part(h, sizeof(float2) * n * ks));
+  float2* part = reinterpret_cast<float2*>(h->g.part);
+  k_tc_proj<<<dim3(tn, tb, ks), MPipe::kThreads, MPipe::kSmem, h->stream>>>(
+      psi, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, part, tc_err(h));
+  CUW_LAUNCH_CHECK("k_tc_proj");
+  return tc_reduce(h, part, ks, n, h->gweight, proj);
+}
+
+int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const StepCoef& sc) {
+  const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
+  const dim3 grid(ceil_div(ngl, 128), ceil_div(nbh, 32));
+  Device& g = h->g;
+#define TC_ADDPRO(M)                                                                                         \
+  k_tc_addpro<M><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, \
+                                                                     h->ldg, ngl, nbh, npro, hpc, opc,       \
+                                                                     g.pdesc, g.ylm, g.pro, g.eigr, sc,      \
+                                                                     tc_err(h))
+  if (mode == ADDPRO_HPSI) TC_ADDPRO(ADDPRO_HPSI);
+  else if (mode == ADDPRO_OPSI) TC_ADDPRO(ADDPRO_OPSI);
+  else TC_ADDPRO(ADDPRO_FUSED);
+#undef TC_ADDPRO
+  CUW_LAUNCH_CHECK("k_tc_addpro");
+  return CUW_OK;
+}
+
+int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
+            double scale, double2* dst) {
+  TcGramArgs a;
+  for (int i = 0; i < npair; ++i) a.pair[i] = pairs[i];
+  a.npair = npair;
+  a.nk = nk;
+  a.nm = nm;
+  a.sk = sk;
+  a.sm = sm;
+  const int tiles = ceil_div(nm, 64) * ceil_div(nm, 64) * npair;
+  int ks = tc_splits(h, tiles, nk);
+  a.kchunk = ceil_div(ceil_div(nk, ks), kCK) * kCK;
+  ks = ceil_div(nk, a.kchunk);
+  const size_t mn = (size_t)nm * nm;
+  CUW_RET(ensure_part(h, sizeof(float2) * mn * 2 * npair * ks));
+  float2* part = reinterpret_cast<float2*>(h->g.part);
+  const dim3 grid(ceil_div(nm, 64), ceil_div(nm, 64), ks * npair);
+  if (minus)
+    k_tc_gram<true><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, part, tc_err(h));
+  else
+    k_tc_gram<false><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, part, tc_err(h));
+  CUW_LAUNCH_CHECK("k_tc_gram");
+  return tc_reduce(h, part, ks, mn * 2 * npair, scale, dst);
+}
+
+int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double2* l1, const double2* l2, int nm,
+            int nn, int nk, size_t sxm, size_t sxk, size_t som, size_t son) {
+  TcAddXArgs a{out, x, l1, l2, nm, nn, nk, sxm, sxk, som, son};
+  const dim3 grid(ceil_div(nm, 128), ceil_div(nn, 64));
+  if (xminus) k_tc_addx<true><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, tc_err(h));
+  else k_tc_addx<false><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, tc_err(h));
+  CUW_LAUNCH_CHECK("k_tc_addx");
+  return CUW_OK;
+}
+
+int tc_force(Handle* h, const double2* ded, double* fpart, int* ntile) {
+  const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
+  const int tm = ceil_div(ngl, 128), tn = ceil_div(npro, 64);
+  k_tc_force<<<dim3(tm, tn), MPipe::kThreads, MPipe::kSmem, h->stream>>>(
+      h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy, h->g.gz,
+      fpart, tc_err(h));
+  CUW_LAUNCH_CHECK("k_tc_force");
+  *ntile = tm;
+  return CUW_OK;
+}
+
+}  // namespace cuw
+
+// Check of the split-precision tensor-core path (no reference counterpart):
+// C(M,N) = A(M,K) B(N,K)^T on device buffers, FP64 row-major with K
+// contiguous, computed as three tf32 products with fp32 accumulation.
+// err (device int) is set to 1 if a bounded wait ran out.
+extern "C" int cuwaves_tc_gemm_check(int M, int N, int K, const double* A, const double* B, double* C, int* err,
+                                     void* stream) {
+  using namespace cuw;
+  if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C || !err) return CUW_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t smem = MPipe::kSmem;
+  if (cudaFuncSetAttribute(k_tf32x3_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return CUW_ERR_CUDA;
+  dim3 grid((M + 127) / 128, (N + 127) / 128);
+  k_tf32x3_gemm<<<grid, MPipe::kThreads, smem, st>>>(M, N, K, A, B, C, err);
+  if (cudaGetLastError() != cudaSuccess) return CUW_ERR_CUDA;
+  return CUW_OK;
+}

@@ -83,6 +83,7 @@ OPTIONAL = {
     "get_timing": [_P, _D, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "get_stream": [_P, C.POINTER(C.c_void_p)],
     "get_ortho_stats": [_P, _D, C.c_int],
+    "tc_gemm_check": [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P],
     # device-pointer variant without allocation (no handle)
     "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
     "get_atoms": [_P, _D, _D, _D],

@@ -166,6 +166,13 @@ int cuwaves_get_stream(cuw_handle* h, void** stream);
  * eigenbasis converged too slowly and were redone after a rediagonalisation.
  * n values are written. */
 int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
+/* Check of the split-precision tensor-core product (no reference
+ * counterpart): C(M,N) = A(M,K) * B(N,K)^T on device buffers, FP64 row-major
+ * with K contiguous, computed as three tf32 tcgen05 products (hi*hi + hi*lo +
+ * lo*hi) with fp32 accumulation.  *err (device int) becomes 1 if a bounded wait
+ * inside the kernel ran out.  Work is enqueued on `stream`. */
+int cuwaves_tc_gemm_check(int M, int N, int K, const double* A, const double* B, double* C, int* err,
+                          void* stream);
 
 /* Projections without any device allocation: PROJ(b,p) = gweight * sum_G
  * conj(PRO(G,p)) psi(G,b), the contraction of cuwaves_projections, for callers
