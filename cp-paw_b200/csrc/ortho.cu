@@ -346,10 +346,24 @@ __device__ __forceinline__ void block_max2(double& a, double& b, double* red) {
   __syncthreads();
 }
 
-__device__ __forceinline__ void csync() {
-  __threadfence();
-  cg::this_cluster().sync();
+// Maxima over the cluster's partials mp[0..cs) and mp[cs..2cs) (cs <= 32):
+// one L2 read per lane, then a warp reduction, instead of a chain of reads.
+__device__ __forceinline__ void cluster_max2(const double* mp, int cs, double& a, double& b) {
+  const int lane = threadIdx.x & 31;
+  a = lane < cs ? __ldcg(&mp[lane]) : 0.0;
+  b = lane < cs ? __ldcg(&mp[cs + lane]) : 0.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  }
 }
+
+// Barrier of the cluster.  Its arrive/wait pair has release/acquire semantics
+// at cluster scope, which orders the global-memory writes of every CTA before
+// the other CTAs' later reads (all done through L2, __ldcg); no GPU-scope
+// fence is needed because every reader is in the cluster.
+__device__ __forceinline__ void csync() { cg::this_cluster().sync(); }
 
 // Convergence rule of the Lyapunov fixed point (shared by both loops): true to
 // stop; `failed` when the contraction is too slow (the earlier eigenbasis is
@@ -378,24 +392,32 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
                              double* red, double* xcur, double* xnext, bool& failed) {
   constexpr int RA = 16 * MR, RB = 16 * MC, LDA = RA + 4, LDB = RB + 4;
   constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC, TPW = (NTILE + 7) / 8;
+  // the slices always hold KN = 128 rows of k (zero past n), so that every
+  // divisor of the staging index arithmetic is a compile-time constant
+  constexpr int KN = 128;
   const int n = a.n, n4 = (n + 3) & ~3;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int fr = lane >> 2, fk = lane & 3;
   const int tm = i1 - i0, tn = j1 - j0;
+  // Column slices are held column by column ([jj][k], stride LDK = KN + 4):
+  // the staging stores run along k and stay free of bank conflicts, and so do
+  // the B-fragment reads (LDK = 4 mod 16 doubles).  Row slices are [k][ii].
+  constexpr int LDK = KN + 4;
   double* Er = sm;              // Er[k][ii] = E(i0+ii, k)
-  double* Ec = Er + LDA * n4;   // Ec[k][jj] = E(k, j0+jj)
-  double* Xc = Ec + LDB * n4;   // Xc[k][jj] = X(k, j0+jj)
-  double* Xr = Xc + LDB * n4;   // Xr[k][ii] = X(i0+ii, k)
-  for (int t = tid; t < n4 * RA; t += nt) {
+  double* Ec = Er + LDA * KN;   // Ec[jj][k] = E(k, j0+jj)
+  double* Xc = Ec + RB * LDK;   // Xc[jj][k] = X(k, j0+jj)
+  double* Xr = Xc + RB * LDK;   // Xr[k][ii] = X(i0+ii, k)
+  for (int t = tid; t < KN * RA; t += nt) {
     const int ii = t % RA, k = t / RA;
     Er[k * LDA + ii] = (ii < tm && k < n) ? __ldcg(&a.emat[(i0 + ii) + (size_t)n * k]) : 0.0;
   }
-  for (int t = tid; t < n4 * RB; t += nt) {
-    const int k = t % n4, jj = t / n4;
-    Ec[k * LDB + jj] = (jj < tn && k < n) ? __ldcg(&a.emat[k + (size_t)n * (j0 + jj)]) : 0.0;
+  for (int t = tid; t < KN * RB; t += nt) {
+    const int k = t % KN, jj = t / KN;
+    Ec[jj * LDK + k] = (jj < tn && k < n) ? __ldcg(&a.emat[k + (size_t)n * (j0 + jj)]) : 0.0;
   }
   // this lane's elements of the tile: right-hand side, denominator, iterate
-  double gtv[TPW][2], den[TPW][2], xp[TPW][2];
+  // and the iterate before it (Chebyshev recurrence)
+  double gtv[TPW][2], den[TPW][2], xp[TPW][2], xq[TPW][2];
   int eidx[TPW][2];
 #pragma unroll
   for (int q = 0; q < TPW; ++q) {
@@ -408,14 +430,20 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
       gtv[q][e] = ok ? __ldcg(&a.gt[eidx[q][e]]) : 0.0;
       den[q][e] = ok ? a.e[i0 + ii] + a.e[j0 + jj] : 1.0;
       xp[q][e] = ok ? __ldcg(&xcur[eidx[q][e]]) : 0.0;
+      xq[q][e] = xp[q][e];
     }
   }
-  double prev = INFINITY;
+  // Chebyshev acceleration: the map X -> -(E X + X E)/(e_i + e_j) is self-adjoint
+  // in the inner product weighted by e_i + e_j, so its spectrum is real, in
+  // [-rho, rho].  Three plain sweeps estimate rho from the ratio of successive
+  // changes (with a margin; an estimate below the true rho still contracts),
+  // then x_{k+1} = w (F(x_k) - x_{k-1}) + x_{k-1} with the Chebyshev weights.
+  double prev = INFINITY, rho = 0.0, omega = 1.0;
   failed = false;
   for (int it2 = 0; it2 < a.max_inner; ++it2) {
     double* mp = a.maxpart + (it2 & 1) * 2 * cs;
     // stage X(:, j0:j1) and X(i0:i1, :), sixteen loads in flight per thread
-    const int totc = n4 * RB, tot = totc + n4 * RA;
+    constexpr int totc = KN * RB, tot = totc + KN * RA;
     for (int base = 0; base < tot; base += 16 * nt) {
       double v[16];
 #pragma unroll
@@ -423,7 +451,7 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
         const int t = base + tid + q * nt;
         v[q] = 0.0;
         if (t < totc) {
-          const int k = t % n4, jj = t / n4;
+          const int k = t % KN, jj = t / KN;
           if (jj < tn && k < n) v[q] = __ldcg(&xcur[k + (size_t)n * (j0 + jj)]);
         } else if (t < tot) {
           const int u = t - totc, ii = u % RA, k = u / RA;
@@ -434,8 +462,8 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
       for (int q = 0; q < 16; ++q) {
         const int t = base + tid + q * nt;
         if (t < totc) {
-          const int k = t % n4, jj = t / n4;
-          Xc[k * LDB + jj] = v[q];
+          const int k = t % KN, jj = t / KN;
+          Xc[jj * LDK + k] = v[q];
         } else if (t < tot) {
           const int u = t - totc, ii = u % RA, k = u / RA;
           Xr[k * LDA + ii] = v[q];
@@ -449,17 +477,29 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
       const int t = warp + q * nw;
       if (t >= NTILE) continue;
       const int r0 = (t % TR) * 8, c0 = (t / TR) * 8;
-      double ex[2] = {0.0, 0.0}, xe[2] = {0.0, 0.0};
-      for (int k = 0; k < n4; k += 4) {
-        dmma(ex, Er[(k + fk) * LDA + r0 + fr], Xc[(k + fk) * LDB + c0 + fr]);
-        dmma(xe, Xr[(k + fk) * LDA + r0 + fr], Ec[(k + fk) * LDB + c0 + fr]);
+      // four independent accumulation chains (two per product, even and odd
+      // k steps) to hide the MMA latency
+      double ex[2] = {0.0, 0.0}, xe[2] = {0.0, 0.0}, ex1[2] = {0.0, 0.0}, xe1[2] = {0.0, 0.0};
+      for (int k = 0; k < n4; k += 8) {
+        dmma(ex, Er[(k + fk) * LDA + r0 + fr], Xc[(c0 + fr) * LDK + k + fk]);
+        dmma(xe, Xr[(k + fk) * LDA + r0 + fr], Ec[(c0 + fr) * LDK + k + fk]);
+        if (k + 4 < n4) {
+          dmma(ex1, Er[(k + 4 + fk) * LDA + r0 + fr], Xc[(c0 + fr) * LDK + k + 4 + fk]);
+          dmma(xe1, Xr[(k + 4 + fk) * LDA + r0 + fr], Ec[(c0 + fr) * LDK + k + 4 + fk]);
+        }
       }
+      ex[0] += ex1[0];
+      ex[1] += ex1[1];
+      xe[0] += xe1[0];
+      xe[1] += xe1[1];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         if (eidx[q][e] < 0) continue;
-        const double xn = (gtv[q][e] - ex[e] - xe[e]) / den[q][e];
+        const double fx = (gtv[q][e] - ex[e] - xe[e]) / den[q][e];
+        const double xn = omega * (fx - xq[q][e]) + xq[q][e];
         dx = fmax(dx, fabs(xn - xp[q][e]));
         xm = fmax(xm, fabs(xn));
+        xq[q][e] = xp[q][e];
         xp[q][e] = xn;
         xnext[eidx[q][e]] = xn;
       }
@@ -470,16 +510,20 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
       mp[cs + rank] = xm;
     }
     csync();
-    double gdx = 0.0, gxm = 0.0;
-    for (int r = 0; r < cs; ++r) {
-      gdx = fmax(gdx, __ldcg(&mp[r]));
-      gxm = fmax(gxm, __ldcg(&mp[cs + r]));
-    }
+    double gdx, gxm;
+    cluster_max2(mp, cs, gdx, gxm);
     double* tmpx = xcur;
     xcur = xnext;
     xnext = tmpx;
     if (rank == 0 && tid == 0) a.inner[0] += 1;
+    const double ratio = gdx / prev;
     if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, failed)) break;
+    if (it2 == 2) {
+      rho = fmin(0.9, fmax(0.05, 1.1 * ratio));
+      omega = 1.0 / (1.0 - 0.5 * rho * rho);
+    } else if (it2 > 2) {
+      omega = 1.0 / (1.0 - 0.25 * rho * rho * omega);
+    }
   }
   return xcur;
 }
@@ -489,7 +533,7 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
 constexpr int kFixedPointFailed = 100;
 
 template <int MR, int MC>
-__global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
+__global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
   extern __shared__ double sm[];
   cg::cluster_group cl = cg::this_cluster();
   const int cs = (int)cl.num_blocks(), rank = (int)cl.block_rank();
@@ -539,8 +583,8 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
     block_max2(mx, unused, red);
     if (tid == 0) a.maxpart[rank] = mx;
     csync();
-    double digam = 0.0;
-    for (int r = 0; r < cs; ++r) digam = fmax(digam, __ldcg(&a.maxpart[r]));
+    double digam, unused2;
+    cluster_max2(a.maxpart, cs, digam, unused2);
     if (digam < a.eps) {
       status = CUW_OK;
       iters = iter;
@@ -595,11 +639,8 @@ __global__ void __launch_bounds__(256) k_ortho_x(OrthoArgs a) {
           mp[cs + rank] = xm;
         }
         csync();
-        double gdx = 0.0, gxm = 0.0;
-        for (int r = 0; r < cs; ++r) {
-          gdx = fmax(gdx, __ldcg(&mp[r]));
-          gxm = fmax(gxm, __ldcg(&mp[cs + r]));
-        }
+        double gdx, gxm;
+        cluster_max2(mp, cs, gdx, gxm);
         double* tmpx = xcur;
         xcur = xnext;
         xnext = tmpx;
@@ -888,7 +929,7 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
   // per CTA are at most 16*MR x 16*MC with MR, MC in {1,2,4}
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
-  cfg.blockDim = dim3(256);
+  cfg.blockDim = dim3(512);  // 16 warps: one 8x8 block of a 32x32 tile each
   cfg.stream = h->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
@@ -906,9 +947,8 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
     const int mc = csz <= 16 ? 1 : (csz <= 32 ? 2 : (csz <= 64 ? 4 : 0));
     if (!mr || !mc) continue;
     a.kc = 128;  // staging chunk of gemm_tile (its default KC)
-    const int n4 = (n + 3) & ~3;
     a.fast = (n <= 128 && mr <= 2 && mc <= 2) ? 1 : 0;
-    const size_t smem = sizeof(double) * (16 * (mr + mc) + 8) * (size_t)std::max(a.kc, a.fast ? 2 * n4 : 0);
+    const size_t smem = sizeof(double) * (16 * (mr + mc) + 8) * (size_t)std::max(a.kc, a.fast ? 2 * 128 : 0);
     void (*fn)(OrthoArgs) = nullptr;
     if (mr == 1 && mc == 1) fn = k_ortho_x<1, 1>;
     else if (mr == 2 && mc == 2) fn = k_ortho_x<2, 2>;

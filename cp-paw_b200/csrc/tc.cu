@@ -31,6 +31,14 @@ static_assert(sizeof(float) * kStages * MPipe::kStage >= sizeof(double) * 128 * 
 
 __device__ __forceinline__ double2 dz() { return make_double2(0.0, 0.0); }
 
+// Producer items per thread and stage: 128 A rows and 64 complex B columns,
+// each item covering two complex K values.  Every producer first issues all
+// global loads of its items (held in registers), then converts and stores: the
+// shared-memory stores would otherwise keep later loads from being hoisted.
+constexpr int kItemsA = 128 * (kCK / 2) / kProd;
+constexpr int kItemsB = 64 * (kCK / 2) / kProd;
+static_assert(128 * (kCK / 2) % kProd == 0 && 64 * (kCK / 2) % kProd == 0, "items must divide evenly");
+
 // ---------------------------------------------------------------------------
 // Plain real GEMM C(M,N) = A(M,K) * B(N,K)^T, FP64 in and out, row-major with
 // K contiguous: the reference product of the split-precision machinery.
@@ -95,24 +103,32 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
   __syncthreads();
   auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
     const int g0 = gbeg + c * kCK;
-    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
-      const int r = it % 128, gi = it / 128, g = g0 + 2 * gi;
+    double2 av[kItemsA][2], bv[kItemsB][2];
+    // eight consecutive lanes cover the stage's 16 g of one row: the table and
+    // coefficient reads are contiguous in g
+    constexpr int NG = kCK / 2;
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd, r = it / NG, g = g0 + 2 * (it % NG);
       const ProDesc d = sd[r];
-      double2 a0 = dz(), a1 = dz();
-      if (d.l >= 0) {
-        if (g < gend) a0 = cconj(pro_value(g, ngl, d, ylm, pro, eigr));
-        if (g + 1 < gend) a1 = cconj(pro_value(g + 1, ngl, d, ylm, pro, eigr));
-      }
-      tc::put_a(ahi, alo, r, gi, a0, a1);
+      av[q][0] = (d.l >= 0 && g < gend) ? pro_value(g, ngl, d, ylm, pro, eigr) : dz();
+      av[q][1] = (d.l >= 0 && g + 1 < gend) ? pro_value(g + 1, ngl, d, ylm, pro, eigr) : dz();
     }
-    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
-      const int j = it % 64, gi = it / 64, g = g0 + 2 * gi, b = b0 + j;
-      double2 c0 = dz(), c1 = dz();
-      if (b < nbh) {
-        if (g < gend) c0 = psi[(size_t)g + (size_t)ldg * b];
-        if (g + 1 < gend) c1 = psi[(size_t)g + 1 + (size_t)ldg * b];
-      }
-      tc::put_b(bhi, blo, j, gi, c0, c1);
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd, b = b0 + it / NG, g = g0 + 2 * (it % NG);
+      bv[q][0] = (b < nbh && g < gend) ? psi[(size_t)g + (size_t)ldg * b] : dz();
+      bv[q][1] = (b < nbh && g + 1 < gend) ? psi[(size_t)g + 1 + (size_t)ldg * b] : dz();
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd;
+      tc::put_a(ahi, alo, it / NG, it % NG, cconj(av[q][0]), cconj(av[q][1]));
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd;
+      tc::put_b(bhi, blo, it / NG, it % NG, bv[q][0], bv[q][1]);
     }
   };
   auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
@@ -145,25 +161,30 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
   const int g0 = blockIdx.x * 128, b0 = blockIdx.y * 32;
   auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
     const int p0 = c * kCK;
-    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
-      const int r = it % 128, pi = it / 128, g = g0 + r, p = p0 + 2 * pi;
-      double2 a0 = dz(), a1 = dz();
-      if (g < ngl) {
-        if (p < npro) a0 = pro_value(g, ngl, pdesc[p], ylm, pro, eigr);
-        if (p + 1 < npro) a1 = pro_value(g, ngl, pdesc[p + 1], ylm, pro, eigr);
-      }
-      tc::put_a(ahi, alo, r, pi, a0, a1);
+    double2 av[kItemsA][2], bv[kItemsB][2];
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd, g = g0 + it % 128, p = p0 + 2 * (it / 128);
+      av[q][0] = (g < ngl && p < npro) ? pro_value(g, ngl, pdesc[p], ylm, pro, eigr) : dz();
+      av[q][1] = (g < ngl && p + 1 < npro) ? pro_value(g, ngl, pdesc[p + 1], ylm, pro, eigr) : dz();
     }
-    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
-      const int j = it % 64, pi = it / 64, mt = j / 32, b = b0 + (j % 32), p = p0 + 2 * pi;
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd, j = it % 64, mt = j / 32, b = b0 + (j % 32), p = p0 + 2 * (it / 64);
       const double2* cm = mt == 0 ? c1 : c2;
-      const bool use = mt == 0 ? USE_H : USE_O;
-      double2 x0 = dz(), x1 = dz();
-      if (use && b < nbh) {
-        if (p < npro) x0 = cm[(size_t)b + (size_t)nbh * p];
-        if (p + 1 < npro) x1 = cm[(size_t)b + (size_t)nbh * (p + 1)];
-      }
-      tc::put_b(bhi, blo, j, pi, x0, x1);
+      const bool use = (mt == 0 ? USE_H : USE_O) && b < nbh;
+      bv[q][0] = (use && p < npro) ? cm[(size_t)b + (size_t)nbh * p] : dz();
+      bv[q][1] = (use && p + 1 < npro) ? cm[(size_t)b + (size_t)nbh * (p + 1)] : dz();
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd;
+      tc::put_a(ahi, alo, it % 128, it / 128, av[q][0], av[q][1]);
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd;
+      tc::put_b(bhi, blo, it % 64, it / 64, bv[q][0], bv[q][1]);
     }
   };
   auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
@@ -220,31 +241,46 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
   const int kbeg = split * a.kchunk, kend = min(a.nk, kbeg + a.kchunk);
   auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
     const int k0 = kbeg + c * kCK;
-    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
-      const int r = it % 128, ki = it / 128, k = k0 + 2 * ki, m = m0 + (r & 63);
-      double2 v[2] = {dz(), dz()};
-      if (m < a.nm) {
+    // lanes run along the contiguous index: k when sk == 1 (plane waves), the
+    // band otherwise (projections)
+    constexpr int NK = kCK / 2;
+    const bool kfast = a.sk == 1;
+    double2 av[kItemsA][2], bv[kItemsB][2];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          if (k + q >= kend) continue;
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd;
+      const int r = kfast ? it / NK : it % 128, ki = kfast ? it % NK : it / 128;
+      const int k = k0 + 2 * ki, m = m0 + (r & 63);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        av[q][e] = dz();
+        if (m < a.nm && k + e < kend) {
           if (r < 64) {
-            v[q] = cconj(X[(size_t)(k + q) * a.sk + (size_t)m * a.sm]);
+            av[q][e] = cconj(X[(size_t)(k + e) * a.sk + (size_t)m * a.sm]);
           } else {
-            const int kk = MINUS ? minusg[k + q] : k + q;
-            v[q] = X[(size_t)kk * a.sk + (size_t)m * a.sm];
+            const int kk = MINUS ? minusg[k + e] : k + e;
+            av[q][e] = X[(size_t)kk * a.sk + (size_t)m * a.sm];
           }
         }
       }
-      tc::put_a(ahi, alo, r, ki, v[0], v[1]);
     }
-    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
-      const int j = it % 64, ki = it / 64, k = k0 + 2 * ki, n = n0 + j;
-      double2 y0 = dz(), y1 = dz();
-      if (n < a.nm) {
-        if (k < kend) y0 = Y[(size_t)k * a.sk + (size_t)n * a.sm];
-        if (k + 1 < kend) y1 = Y[(size_t)(k + 1) * a.sk + (size_t)n * a.sm];
-      }
-      tc::put_b(bhi, blo, j, ki, y0, y1);
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd;
+      const int j = kfast ? it / NK : it % 64, ki = kfast ? it % NK : it / 64;
+      const int n = n0 + j, k = k0 + 2 * ki;
+      bv[q][0] = (n < a.nm && k < kend) ? Y[(size_t)k * a.sk + (size_t)n * a.sm] : dz();
+      bv[q][1] = (n < a.nm && k + 1 < kend) ? Y[(size_t)(k + 1) * a.sk + (size_t)n * a.sm] : dz();
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd;
+      tc::put_a(ahi, alo, kfast ? it / NK : it % 128, kfast ? it % NK : it / 128, av[q][0], av[q][1]);
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd;
+      tc::put_b(bhi, blo, kfast ? it / NK : it % 64, kfast ? it % NK : it / 64, bv[q][0], bv[q][1]);
     }
   };
   auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
@@ -282,36 +318,44 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
   const int ktot = 2 * a.nk;
   auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
     const int kg0 = c * kCK;
-    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
-      const int r = it % 128, ki = it / 128, m = m0 + r;
-      double2 v[2] = {dz(), dz()};
-      if (m < a.nm) {
+    double2 av[kItemsA][2], bv[kItemsB][2];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int kg = kg0 + 2 * ki + q;
-          if (kg >= ktot) continue;
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd, m = m0 + it % 128;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int kg = kg0 + 2 * (it / 128) + e;
+        av[q][e] = dz();
+        if (m < a.nm && kg < ktot) {
           if (kg < a.nk) {
-            v[q] = a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
+            av[q][e] = a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
           } else {
             const int mm = XMINUS ? minusg[m] : m;
-            v[q] = cconj(a.x[(size_t)mm * a.sxm + (size_t)(kg - a.nk) * a.sxk]);
+            av[q][e] = cconj(a.x[(size_t)mm * a.sxm + (size_t)(kg - a.nk) * a.sxk]);
           }
         }
       }
-      tc::put_a(ahi, alo, r, ki, v[0], v[1]);
     }
-    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
-      const int j = it % 64, ki = it / 64, n = n0 + j;
-      double2 w[2] = {dz(), dz()};
-      if (n < a.nn) {
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int kg = kg0 + 2 * ki + q;
-          if (kg >= ktot) continue;
-          w[q] = kg < a.nk ? a.l1[(size_t)kg + (size_t)a.nk * n] : a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
-        }
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd, n = n0 + it % 64;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int kg = kg0 + 2 * (it / 64) + e;
+        bv[q][e] = dz();
+        if (n < a.nn && kg < ktot)
+          bv[q][e] = kg < a.nk ? a.l1[(size_t)kg + (size_t)a.nk * n] : a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
       }
-      tc::put_b(bhi, blo, j, ki, w[0], w[1]);
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd;
+      tc::put_a(ahi, alo, it % 128, it / 128, av[q][0], av[q][1]);
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd;
+      tc::put_b(bhi, blo, it % 64, it / 64, bv[q][0], bv[q][1]);
     }
   };
   auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
@@ -345,23 +389,28 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
   const int g0 = blockIdx.x * 128, p0 = blockIdx.y * 64;
   auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
     const int bb = c * kCK;
-    for (int it = t; it < 128 * (kCK / 2); it += kProd) {
-      const int r = it % 128, bi = it / 128, g = g0 + r, b = bb + 2 * bi;
-      double2 a0 = dz(), a1 = dz();
-      if (g < ngl) {
-        if (b < nbh) a0 = psi0[(size_t)g + (size_t)ldg * b];
-        if (b + 1 < nbh) a1 = psi0[(size_t)g + (size_t)ldg * (b + 1)];
-      }
-      tc::put_a(ahi, alo, r, bi, a0, a1);
+    double2 av[kItemsA][2], bv[kItemsB][2];
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd, g = g0 + it % 128, b = bb + 2 * (it / 128);
+      av[q][0] = (g < ngl && b < nbh) ? psi0[(size_t)g + (size_t)ldg * b] : dz();
+      av[q][1] = (g < ngl && b + 1 < nbh) ? psi0[(size_t)g + (size_t)ldg * (b + 1)] : dz();
     }
-    for (int it = t; it < 64 * (kCK / 2); it += kProd) {
-      const int j = it % 64, bi = it / 64, p = p0 + j, b = bb + 2 * bi;
-      double2 e0 = dz(), e1 = dz();
-      if (p < npro) {
-        if (b < nbh) e0 = cconj(ded[(size_t)b + (size_t)nbh * p]);
-        if (b + 1 < nbh) e1 = cconj(ded[(size_t)b + 1 + (size_t)nbh * p]);
-      }
-      tc::put_b(bhi, blo, j, bi, e0, e1);
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd, p = p0 + it % 64, b = bb + 2 * (it / 64);
+      bv[q][0] = (p < npro && b < nbh) ? cconj(ded[(size_t)b + (size_t)nbh * p]) : dz();
+      bv[q][1] = (p < npro && b + 1 < nbh) ? cconj(ded[(size_t)b + 1 + (size_t)nbh * p]) : dz();
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsA; ++q) {
+      const int it = t + q * kProd;
+      tc::put_a(ahi, alo, it % 128, it / 128, av[q][0], av[q][1]);
+    }
+#pragma unroll
+    for (int q = 0; q < kItemsB; ++q) {
+      const int it = t + q * kProd;
+      tc::put_b(bhi, blo, it % 64, it / 64, bv[q][0], bv[q][1]);
     }
   };
   double* sv = reinterpret_cast<double*>(tc::pipe_stage_base());  // [128][64]

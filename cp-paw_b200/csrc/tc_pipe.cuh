@@ -10,11 +10,12 @@
 //
 // A stage holds BKR real K values (BKR/8 MMA steps of K = 8).  Each MMA step
 // (its three products hi*hi + hi*lo + lo*hi) is accumulated in a fresh TMEM
-// region, two regions of 128 columns alternating, and drained on its own: the
+// region (four regions of 128 columns in rotation, all of TMEM) and drained on
+// its own: the
 // tensor core's fp32 accumulation truncates, with a bias that grows with the
 // number of products summed into one accumulator, while the register sums of
-// the drain warps round to nearest.  The drain of one step overlaps the MMAs
-// of the next, and the producers fill later stages meanwhile.
+// the drain warps round to nearest.  The MMAs run up to three steps ahead of
+// the drain, and the producers fill later stages meanwhile.
 //
 // Synchronisation: smem_free[s] (MMA commit -> producers), acc_full[r] (MMA
 // commit -> drain), acc_empty[r] (drain arrivals -> MMA thread).  Every wait is
@@ -42,7 +43,8 @@ struct Pipe {
   static constexpr int kDrain = 8;                  // drain warps
   static constexpr int kCols = 128 / (kDrain / 4);  // columns per drain thread
   static constexpr int kThreads = 32 * (NPW + kDrain);
-  static constexpr size_t kSmem = sizeof(float) * NSTAGE * kStage + 1024 + 256;
+  static constexpr int kRegions = 4;                // TMEM accumulators of 128 columns
+  static constexpr size_t kSmem = sizeof(float) * NSTAGE * kStage + 1024 + 512;
 };
 
 // Element (row, k) of a split operand tile (see tc_sm100.cuh): float4 index of
@@ -91,22 +93,23 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
   using P = Pipe<BKR, NSTAGE, NPW>;
   float* st = pipe_stage_base();
   uint64_t* bfree = reinterpret_cast<uint64_t*>(st + NSTAGE * P::kStage);
+  constexpr int NR = P::kRegions;
   uint64_t* bfull = bfree + NSTAGE;
-  uint64_t* bempty = bfull + 2;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bempty + 2);
+  uint64_t* bempty = bfull + NR;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bempty + NR);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) mbar_init(&bfree[s], 1);
-    mbar_init(&bfull[0], 1);
-    mbar_init(&bfull[1], 1);
-    mbar_init(&bempty[0], 32 * P::kDrain);
-    mbar_init(&bempty[1], 32 * P::kDrain);
+    for (int r = 0; r < NR; ++r) {
+      mbar_init(&bfull[r], 1);
+      mbar_init(&bempty[r], 32 * P::kDrain);
+    }
     *abort_flag = 0;
     fence_mbar_init();
   }
   if (warp == 0) {
-    tmem_alloc(tslot, 256);
+    tmem_alloc(tslot, 128 * NR);
     tmem_relinquish();
   }
   fence_before_sync();
@@ -141,8 +144,8 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
         bool ok = true;
 #pragma unroll
         for (int ks = 0; ks < P::kSteps; ++ks) {
-          const int t = c * P::kSteps + ks, r = t & 1;
-          if (t >= 2 && !mbar_wait(&bempty[r], ((t >> 1) - 1) & 1, kWaitCycles)) {
+          const int t = c * P::kSteps + ks, r = t % NR;
+          if (t >= NR && !mbar_wait(&bempty[r], ((t / NR) - 1) & 1, kWaitCycles)) {
             ok = false;
             break;
           }
@@ -165,7 +168,7 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
     }
     if (tid == 0 && *abort_flag && last >= 0) {
       // let the MMAs in flight finish before TMEM is released
-      mbar_wait(&bfull[last & 1], (last >> 1) & 1, kWaitCycles);
+      mbar_wait(&bfull[last % NR], (last / NR) & 1, kWaitCycles);
     }
   } else {
     const int q = warp & 3, dw = warp - NPW, col0 = P::kCols * (dw / 4);
@@ -175,8 +178,8 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
     for (int j = 0; j < P::kCols; ++j) acc[j] = 0.f;
     bool aborted = false;
     for (int t = 0; t < nrun; ++t) {
-      const int r = t & 1;
-      const bool ok = mbar_wait(&bfull[r], (t >> 1) & 1, kWaitCycles);
+      const int r = t % NR;
+      const bool ok = mbar_wait(&bfull[r], (t / NR) & 1, kWaitCycles);
       if (bar_or(2, 32 * P::kDrain, !ok || *abort_flag != 0)) {
         aborted = true;
         if (warp == NPW && lane == 0) {
@@ -186,14 +189,15 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
         break;
       }
       fence_after_sync();
+      // all loads of the run in flight, one wait
+      uint32_t v[P::kCols / 16][16];
 #pragma unroll
-      for (int j = 0; j < P::kCols / 16; ++j) {
-        uint32_t v[16];
-        tmem_ld16(tmem + lane_base + (uint32_t)(r * 128 + 16 * j), v);
-        tmem_wait_ld();
+      for (int j = 0; j < P::kCols / 16; ++j) tmem_ld16(tmem + lane_base + (uint32_t)(r * 128 + 16 * j), v[j]);
+      tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[16 * j + i] += __uint_as_float(v[i]);
-      }
+      for (int j = 0; j < P::kCols / 16; ++j)
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[16 * j + i] += __uint_as_float(v[j][i]);
       fence_before_sync();
       mbar_arrive(&bempty[r]);
     }
@@ -202,7 +206,7 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, 128 * NR);
 }
 
 }  // namespace tc

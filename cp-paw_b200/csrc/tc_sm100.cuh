@@ -134,13 +134,15 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 // ---- split precision ------------------------------------------------------------------------
 // x = hi + lo with hi a tf32 value (10 explicit mantissa bits, rounded to
-// nearest) and lo the fp32 remainder; the tensor core reads lo as tf32 too, so
-// hi*hi + hi*lo + lo*hi carries about 21 significant bits.
+// nearest) and lo = fp32(x) - hi, exact in fp32; the tensor core reads lo as
+// tf32 too, so hi*hi + hi*lo + lo*hi carries about 21 significant bits (the
+// bits of x beyond fp32 lie far below lo's tf32 precision).  One conversion
+// per value: float/double conversions are a low-throughput operation.
 __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   const float xf = (float)x;
   const uint32_t u = (__float_as_uint(xf) + 0x1000u) & 0xFFFFE000u;
   hi = __uint_as_float(u);
-  lo = (float)(x - (double)hi);
+  lo = xf - hi;
 }
 
 }  // namespace tc
