@@ -23,7 +23,9 @@ namespace {
 // accumulation was measured on B200 at a signed mean error of -3.7e-8 /
 // -8.7e-8 / -1.8e-7 of |C| for runs of 8 / 16 / 32 real K, and one step keeps
 // the energy bias below 1e-6 Ha/atom.
-constexpr int kBK = 32, kCK = kBK / 2, kStages = 3, kNPW = 4;
+// Eight producer warps (two per SM sub-partition): the producers' dependent
+// table and coefficient loads need more than one warp per scheduler in flight.
+constexpr int kBK = 32, kCK = kBK / 2, kStages = 3, kNPW = 8;
 using MPipe = tc::Pipe<kBK, kStages, kNPW>;
 constexpr int kProd = MPipe::kProducers;
 // k_tc_force reuses the stage buffers for a 128 x 64 FP64 tile

@@ -189,15 +189,19 @@ __device__ __forceinline__ void pipe_run(int nchunk, Produce& produce, Finish& f
         break;
       }
       fence_after_sync();
-      // all loads of the run in flight, one wait
-      uint32_t v[P::kCols / 16][16];
+      // two loads in flight per wait (register budget of the drain threads)
 #pragma unroll
-      for (int j = 0; j < P::kCols / 16; ++j) tmem_ld16(tmem + lane_base + (uint32_t)(r * 128 + 16 * j), v[j]);
-      tmem_wait_ld();
+      for (int j = 0; j < P::kCols / 16; j += 2) {
+        uint32_t v[2][16];
+        tmem_ld16(tmem + lane_base + (uint32_t)(r * 128 + 16 * j), v[0]);
+        tmem_ld16(tmem + lane_base + (uint32_t)(r * 128 + 16 * j + 16), v[1]);
+        tmem_wait_ld();
 #pragma unroll
-      for (int j = 0; j < P::kCols / 16; ++j)
-#pragma unroll
-        for (int i = 0; i < 16; ++i) acc[16 * j + i] += __uint_as_float(v[j][i]);
+        for (int i = 0; i < 16; ++i) {
+          acc[16 * j + i] += __uint_as_float(v[0][i]);
+          acc[16 * j + 16 + i] += __uint_as_float(v[1][i]);
+        }
+      }
       fence_before_sync();
       mbar_arrive(&bempty[r]);
     }
