@@ -122,13 +122,25 @@ def fp64_peak_tflops(torch):
 
 
 def load_ncu_traffic():
-    """Per-launch DRAM traffic of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    """Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum,
+    bytes) of the dominant FP64 kernels, from the committed ncu summaries: a
+    line `traffic_bytes_per_launch: <phase> <bytes>` in profiles/*.md."""
+    out = {}
+    d = os.path.join(ROOT, "profiles")
     try:
-        with open(p) as f:
-            return json.load(f)
-    except (OSError, ValueError):
-        return {}
+        names = sorted(os.listdir(d))
+    except OSError:
+        return out
+    for n in names:
+        if not n.endswith(".md"):
+            continue
+        with open(os.path.join(d, n)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    parts = line.split()
+                    if len(parts) == 3:
+                        out[parts[1]] = float(parts[2])
+    return out
 
 
 def make_inputs(name="Si64"):
