@@ -132,6 +132,7 @@ struct Handle {
   int nzp = 0;                   // occupied z planes
   int batch = 0;                 // bands per FFT batch
   AxisPlan ax[3];
+  int (*fft_run)(Handle*, const double2*, double2*, bool) = nullptr;  // chosen by fft_setup
   size_t nr = 0;
   std::vector<double> occ_h;
   double waveekin1 = 0.0, waveekin2 = 0.0;

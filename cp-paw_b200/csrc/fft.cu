@@ -365,6 +365,15 @@ __device__ void transform(C* buf, const AxisArg& ax, int nlines, int ls, int es,
   }
 }
 
+// N > 0: the transform of compile-time length N, inlined alone into the
+// kernel (its registers then fit without spills); N == 0: run-time dispatch.
+template <int N, class C>
+__device__ __forceinline__ void xform(C* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast,
+                                      const C* tw, typename CT<C>::R sgn) {
+  if constexpr (N > 0) transform_fixed<N>(buf, nlines, ls, es, jfast, tw, sgn);
+  else transform(buf, ax, nlines, ls, es, jfast, tw, sgn);
+}
+
 // load twiddles exp(sgn*2 pi i k/n) from the FP64 table exp(+2 pi i k/n)
 template <class C>
 __device__ void load_tw(C* dst, const double2* src, int n, double sgn) {
@@ -386,7 +395,7 @@ __device__ __forceinline__ double2 to_d2(float2 a) { return make_double2((double
 // ---------------------------------------------------------------------------
 // The kernels take the work-grid type C (double2 or float2); the sphere
 // coefficients psi/out stay FP64 and are converted at the gather/scatter.
-template <class C>
+template <class C, int N>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
                  const int* __restrict__ plane_g, const int* __restrict__ plane_pos, C* __restrict__ grid, int nzp,
@@ -406,15 +415,15 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x)
     plane[plane_pos[k]] = from_d2<C>(src[plane_g[k]]);
   __syncthreads();
-  transform(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)1);   // x lines
-  transform(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)1);  // y lines
+  xform<N>(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)1);   // x lines
+  xform<N>(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)1);  // y lines
   C* dst = grid + ((size_t)bl * nzp + p) * npl;
   for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i];
 }
 
 constexpr int kTX = 16;  // x columns per z-column block
 
-template <class C>
+template <class C, int N>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_zcol_v(C* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot, int nzp, int nr1,
              int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
@@ -438,7 +447,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
     tile[i] = val;
   }
   __syncthreads();
-  transform(tile, a3, kTX, 1, kTX, false, tw, (T)1);
+  xform<N>(tile, a3, kTX, 1, kTX, false, tw, (T)1);
   for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
     int iz = i / kTX, x = i % kTX;
     double vv = 0.0;
@@ -449,7 +458,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   // forward transform: conjugated twiddles
   for (int k = threadIdx.x; k < nr3; k += blockDim.x) tw[k].y = -tw[k].y;
   __syncthreads();
-  transform(tile, a3, kTX, 1, kTX, false, tw, (T)-1);
+  xform<N>(tile, a3, kTX, 1, kTX, false, tw, (T)-1);
   for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
     int iz = i / kTX, x = i % kTX;
     int s = zslot[iz];
@@ -457,7 +466,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   }
 }
 
-template <class C>
+template <class C, int N>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_rtog_plane(const C* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
                  const int* __restrict__ plane_g, const int* __restrict__ plane_pos, double2* __restrict__ out,
@@ -476,8 +485,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   load_tw(tw1, tw1g, nr1, -1.0);
   load_tw(tw2, tw2g, nr2, -1.0);
   __syncthreads();
-  transform(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)-1);  // y lines
-  transform(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)-1);   // x lines
+  xform<N>(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)-1);  // y lines
+  xform<N>(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)-1);   // x lines
   double2* dst = out + (size_t)ldg * b;
   const double2* ps = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
@@ -517,6 +526,50 @@ bool plan_axis(int n, AxisPlan& p) {
 }
 
 }  // namespace
+
+// out = FFT_RTOG[ V * FFT_GTOR[psi] ] (+ 1/2 G^2 psi + bucket psi when add_kinetic)
+template <class C, int N>
+static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
+  const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
+  const size_t npl = (size_t)nr1 * nr2;
+  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
+  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(C));
+  const int tp = kPlaneThreads;
+  const int tz = kPlaneThreads;
+  AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
+  const double scale = 1.0 / ((double)nr1 * nr2 * nr3);
+  Device& g = h->g;
+  C* grid = reinterpret_cast<C*>(g.grid);
+  for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
+    const int nb = std::min(h->batch, h->d.nbh - b0);
+    k_gtor_plane<C, N><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
+                                                                      g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
+                                                                      g.tw2);
+    CUW_LAUNCH_CHECK("k_gtor_plane");
+    const int nxb = (nr1 + kTX - 1) / kTX;
+    k_zcol_v<C, N><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
+                                                                scale);
+    CUW_LAUNCH_CHECK("k_zcol_v");
+    k_rtog_plane<C, N><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
+                                                                      g.plane_pos, out, psi, h->ldg, b0, g.g2,
+                                                                      g.bucket, add_kinetic ? 1 : 0, a1, a2,
+                                                                      g.tw1, g.tw2);
+    CUW_LAUNCH_CHECK("k_rtog_plane");
+  }
+  return CUW_OK;
+}
+
+
+// kernels of work-grid type C and length N (0: any length): shared-memory
+// limits and the launcher
+template <class C, int N>
+static int fft_select(Handle* h, int smem_plane, int smem_z) {
+  CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+  CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
+  CUW_TRY(cudaFuncSetAttribute(k_zcol_v<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  h->fft_run = &fft_vpsi_t<C, N>;
+  return CUW_OK;
+}
 
 int fft_setup(Handle* h, const int* igvec) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3, ngl = h->d.ngl;
@@ -591,54 +644,32 @@ int fft_setup(Handle* h, const int* igvec) {
   }
   const int smem_plane = (int)((npl + nr1 + nr2) * es);
   const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * es);
-  if (h->mixed()) {
-    CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-    CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-    CUW_TRY(cudaFuncSetAttribute(k_zcol_v<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
-  } else {
-    CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-    CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-    CUW_TRY(cudaFuncSetAttribute(k_zcol_v<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  // cubic grids of a specialised length get kernels compiled for that length
+  const int nc = (nr1 == nr2 && nr2 == nr3) ? nr1 : 0;
+  int rc = CUW_OK;
+  switch (h->mixed() ? -nc - 1 : nc + 1) {
+#define CUW_FFT_CASE(LEN)                                                                  \
+  case LEN + 1: rc = fft_select<double2, LEN>(h, smem_plane, smem_z); break;               \
+  case -LEN - 1: rc = fft_select<float2, LEN>(h, smem_plane, smem_z); break;
+    CUW_FFT_CASE(24)
+    CUW_FFT_CASE(32)
+    CUW_FFT_CASE(48)
+    CUW_FFT_CASE(64)
+    CUW_FFT_CASE(72)
+    CUW_FFT_CASE(96)
+#undef CUW_FFT_CASE
+    default:
+      rc = h->mixed() ? fft_select<float2, 0>(h, smem_plane, smem_z) : fft_select<double2, 0>(h, smem_plane, smem_z);
   }
+  if (rc != CUW_OK) return rc;
   return CUW_OK;
 }
 
-// out = FFT_RTOG[ V * FFT_GTOR[psi] ] (+ 1/2 G^2 psi + bucket psi when add_kinetic)
-template <class C>
-static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
-  const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
-  const size_t npl = (size_t)nr1 * nr2;
-  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
-  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(C));
-  const int tp = kPlaneThreads;
-  const int tz = kPlaneThreads;
-  AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
-  const double scale = 1.0 / ((double)nr1 * nr2 * nr3);
-  Device& g = h->g;
-  C* grid = reinterpret_cast<C*>(g.grid);
-  for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
-    const int nb = std::min(h->batch, h->d.nbh - b0);
-    k_gtor_plane<C><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
-                                                                      g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
-                                                                      g.tw2);
-    CUW_LAUNCH_CHECK("k_gtor_plane");
-    const int nxb = (nr1 + kTX - 1) / kTX;
-    k_zcol_v<C><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
-                                                                scale);
-    CUW_LAUNCH_CHECK("k_zcol_v");
-    k_rtog_plane<C><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
-                                                                      g.plane_pos, out, psi, h->ldg, b0, g.g2,
-                                                                      g.bucket, add_kinetic ? 1 : 0, a1, a2,
-                                                                      g.tw1, g.tw2);
-    CUW_LAUNCH_CHECK("k_rtog_plane");
-  }
-  return CUW_OK;
-}
-
-// FP64 transforms, or FP32 transforms and V(r) product on the mixed path
+// FP64 transforms, or FP32 transforms and V(r) product on the mixed path, with
+// the kernels chosen by fft_setup for the grid
 int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
-  if (h->mixed()) return fft_vpsi_t<float2>(h, psi, out, add_kinetic);
-  return fft_vpsi_t<double2>(h, psi, out, add_kinetic);
+  if (!h->fft_run) return h->fail(CUW_ERR_STATE, "FFT not set up");
+  return h->fft_run(h, psi, out, add_kinetic);
 }
 
 }  // namespace cuw
