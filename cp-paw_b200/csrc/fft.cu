@@ -421,35 +421,41 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i];
 }
 
-constexpr int kTX = 16;  // x columns per z-column block
+constexpr int kTX = 16;  // x columns per z-column block, generic kernels
+// x columns per z-column block for transforms of compile-time length N: a
+// whole x row up to 64, which amortises the block's fixed work (twiddles,
+// plane map, barriers) over 4x more columns
+template <int N>
+__host__ __device__ constexpr int tx_of() { return N == 0 ? kTX : (N < 64 ? N : 64); }
 
 template <class C, int N>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_zcol_v(C* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot, int nzp, int nr1,
              int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
   using T = typename CT<C>::R;
+  constexpr int TX = tx_of<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int nr3 = a3.n;
-  C* tile = sm;             // [nr3][kTX]
-  C* tw = sm + nr3 * kTX;
-  const int nxb = (nr1 + kTX - 1) / kTX;
-  const int iy = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * kTX;
+  C* tile = sm;             // [nr3][TX]
+  C* tw = sm + nr3 * TX;
+  const int nxb = (nr1 + TX - 1) / TX;
+  const int iy = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * TX;
   const int bl = blockIdx.y;
   const size_t npl = (size_t)nr1 * nr2;
   C* gb = grid + (size_t)bl * nzp * npl;
   load_tw(tw, tw3g, nr3, +1.0);
-  for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
-    int iz = i / kTX, x = i % kTX;
+  for (int i = threadIdx.x; i < nr3 * TX; i += blockDim.x) {
+    int iz = i / TX, x = i % TX;
     int s = zslot[iz];
     C val = CT<C>::mk(0, 0);
     if (s >= 0 && x0 + x < nr1) val = gb[(size_t)s * npl + (size_t)iy * nr1 + x0 + x];
     tile[i] = val;
   }
   __syncthreads();
-  xform<N>(tile, a3, kTX, 1, kTX, false, tw, (T)1);
-  for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
-    int iz = i / kTX, x = i % kTX;
+  xform<N>(tile, a3, TX, 1, TX, false, tw, (T)1);
+  for (int i = threadIdx.x; i < nr3 * TX; i += blockDim.x) {
+    int iz = i / TX, x = i % TX;
     double vv = 0.0;
     if (x0 + x < nr1) vv = v[(size_t)x0 + x + (size_t)nr1 * (iy + (size_t)nr2 * iz)] * scale;
     tile[i] = cscale(tile[i], (T)vv);
@@ -458,9 +464,9 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   // forward transform: conjugated twiddles
   for (int k = threadIdx.x; k < nr3; k += blockDim.x) tw[k].y = -tw[k].y;
   __syncthreads();
-  xform<N>(tile, a3, kTX, 1, kTX, false, tw, (T)-1);
-  for (int i = threadIdx.x; i < nr3 * kTX; i += blockDim.x) {
-    int iz = i / kTX, x = i % kTX;
+  xform<N>(tile, a3, TX, 1, TX, false, tw, (T)-1);
+  for (int i = threadIdx.x; i < nr3 * TX; i += blockDim.x) {
+    int iz = i / TX, x = i % TX;
     int s = zslot[iz];
     if (s >= 0 && x0 + x < nr1) gb[(size_t)s * npl + (size_t)iy * nr1 + x0 + x] = tile[i];
   }
@@ -533,7 +539,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   const size_t npl = (size_t)nr1 * nr2;
   const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
-  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * sizeof(C));
+  const int smem_z = (int)(((size_t)nr3 * tx_of<N>() + nr3) * sizeof(C));
   const int tp = kPlaneThreads;
   const int tz = kPlaneThreads;
   AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
@@ -546,7 +552,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
                                                                       g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
                                                                       g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
-    const int nxb = (nr1 + kTX - 1) / kTX;
+    const int nxb = (nr1 + tx_of<N>() - 1) / tx_of<N>();
     k_zcol_v<C, N><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
                                                                 scale);
     CUW_LAUNCH_CHECK("k_zcol_v");
@@ -563,7 +569,8 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
 // kernels of work-grid type C and length N (0: any length): shared-memory
 // limits and the launcher
 template <class C, int N>
-static int fft_select(Handle* h, int smem_plane, int smem_z) {
+static int fft_select(Handle* h, int smem_plane, int /*smem_z of the generic kernel*/) {
+  const int smem_z = (int)(((size_t)h->d.nr3 * tx_of<N>() + h->d.nr3) * sizeof(C));
   CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
   CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
   CUW_TRY(cudaFuncSetAttribute(k_zcol_v<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
