@@ -808,6 +808,38 @@ extern "C" int cuwaves_gramschmidt(cuw_handle* hp, int which, const double* r) {
 //   EKIN, WAVEKINETIC(1) | EIGR(R0) | forces | FFT V.psi | DH.PROJ, DO.PROJ |
 //   fused ADDPRO (HPSI, OPSI, PROPAGATE) | <psi|H|psi> | atoms |
 //   ORTHOGONALIZE at R(+) | WAVEKINETIC(2) | SWITCH
+// Single-point evaluation at the current wave functions and positions, the
+// energy part of WAVES$ETOT (src/paw_waves1.f90:2094-2123 with EKIN and FORCE):
+// out[0] = sum_n f_n <psi_n|H|psi_n>, out[1] = kinetic energy; force (3*NAT)
+// at R(0).  Leaves H|psi> in HPSI; nothing is propagated.
+extern "C" int cuwaves_etot(cuw_handle* hp, double* out, double* force) {
+  H(hp);
+  NEED(h->have_gset && h->have_v && h->have_dh && h->have_do, CUW_ERR_STATE, "inputs not loaded");
+  NEED(out != nullptr, CUW_ERR_ARG, "null output");
+  Device& g = h->g;
+  double* sc = g.scal;
+  double* tmpv = g.scal + 8;
+  h->nev = 0;
+  CUW_RET(energy_run(h, RED_EKIN, tmpv));
+  CUW_TRY(cudaMemcpyAsync(sc + 0, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(eigr_compute(h, g.r0));
+  if (force) CUW_RET(force_dev_run(h, g.force));
+  CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
+  CUW_RET(hproj_compute(h, g.proj, g.hproj));
+  CUW_RET(addpro_run(h, ADDPRO_HPSI, g.hproj, g.oproj));
+  h->have_hpsi = true;
+  CUW_RET(energy_run(h, RED_EXPECT, tmpv));
+  CUW_TRY(cudaMemcpyAsync(sc + 1, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  double hs[2];
+  CUW_TRY(cudaMemcpyAsync(hs, sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
+  if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  CUW_RET(h->tc_status());
+  out[0] = hs[1];
+  out[1] = hs[0];
+  return CUW_OK;
+}
+
 extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mass, int max_iter, double eps,
                                double* out, double* force) {
   H(hp);

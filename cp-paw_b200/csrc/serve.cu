@@ -1,0 +1,369 @@
+// Serving runtime: a request loop with continuous batching over wave-function
+// sets kept on the GPU (host code only; the device work is the engine's).
+//
+// A request carries the complete input set of one system (what the Fortran host
+// would load into a WVSET) and either a single-point solve (energy and forces,
+// nsteps = 0) or nsteps CP steps.  Requests queue in arrival order and are
+// admitted while the estimated device memory of all admitted systems stays
+// within the HBM budget.  Worker threads each take one unit of work at a time
+// from the admitted systems in round-robin order (set-up, one CP step, or the
+// single point), each system on its own CUDA stream, so the steps of different
+// systems overlap on the device and a request that arrives while others run
+// starts as soon as memory allows.  The wave functions stay on the device from
+// admission to completion; the handle is released when the request finishes.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/cuwaves.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  long long id = 0;
+  cuw_dims dims{};
+  std::vector<int> isp, igvec, minusg;
+  std::vector<double> gbas, gvec, g2, pro, ylm, mpsi, v, dh, dover, r0, occ, psi, mass;
+  double gweight = 0.0, delt = 0.0, annee = 0.0;
+  int lmnxx = 0, lnxx = 0, nsteps = 0, done_steps = 0;
+  cuw_handle* h = nullptr;
+  size_t bytes = 0;
+  bool busy = false, finished = false;
+  int status = CUW_OK;
+  std::string err;
+  double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<double> force;
+  Clock::time_point t_submit, t_done;
+};
+
+// projectors of the set (sum over atoms of 2l+1 per radial function)
+int count_projectors(const cuw_dims& d, const std::vector<int>& isp) {
+  int n = 0;
+  for (int a = 0; a < d.nat; ++a) {
+    const int s = isp[a] - 1;
+    for (int ln = 0; ln < d.lnx[s]; ++ln) n += 2 * d.lox[s][ln] + 1;
+  }
+  return n;
+}
+
+// Upper estimate of the device memory of one handle (the allocations of
+// cuwaves_create and the FFT set-up, plus the split-K scratch).
+size_t estimate_bytes(const cuw_dims& d, const std::vector<int>& isp) {
+  const size_t ldg = (size_t)((d.ngl + 31) / 32) * 32, nbh = d.nbh, nb = d.nb, ngl = d.ngl;
+  const size_t npro = count_projectors(d, isp);
+  size_t nbare = 0;
+  for (int s = 0; s < d.nsp; ++s) nbare += d.lnx[s];
+  const size_t nr = (size_t)d.nr1 * d.nr2 * d.nr3;
+  size_t b = 4 * ldg * nbh * 16;                       // psi0, psim, hpsi, opsi
+  b += 4 * nbh * npro * 16;                            // proj, oproj, hproj, pbuf
+  b += 2 * nb * nb * 16 + 24 * nb * nb * 8;            // Lagrange and solve matrices
+  b += ngl * (3 * 4 + 7 * 8) + ngl * (nbare + d.lmx) * 8;  // G set and tables
+  b += ngl * (size_t)d.nat * 16;                       // EIGR
+  b += nr * 8;                                         // V(r)
+  b += std::min(nbh * nr * 16, ((size_t)48 << 20) + nr * 16);  // FFT work grid
+  b += (size_t)20 << 20;                               // split-K partials and small tables
+  return b;
+}
+
+}  // namespace
+
+struct cuw_server {
+  size_t budget = 0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::map<long long, std::unique_ptr<Job>> jobs;
+  std::deque<Job*> queue;    // submitted, not admitted
+  std::vector<Job*> active;  // admitted, unfinished
+  size_t rr = 0;             // round-robin position in active
+  size_t in_use = 0, peak = 0;
+  long long next_id = 1, completed = 0, failed = 0;
+  std::vector<double> latencies_ms;
+  Clock::time_point t_first, t_last;
+  bool have_first = false, stop = false;
+  double busy_integral = 0.0;  // time-weighted number of admitted systems
+  Clock::time_point t_mark;
+  std::vector<std::thread> workers;
+
+  void account(Clock::time_point now) {
+    busy_integral += std::chrono::duration<double>(now - t_mark).count() * (double)active.size();
+    t_mark = now;
+  }
+
+  // admission in arrival order while the budget allows
+  void admit() {
+    while (!queue.empty()) {
+      Job* j = queue.front();
+      if (in_use + j->bytes > budget) break;
+      queue.pop_front();
+      account(Clock::now());
+      in_use += j->bytes;
+      peak = std::max(peak, in_use);
+      active.push_back(j);
+    }
+  }
+
+  Job* pick() {
+    const size_t n = active.size();
+    for (size_t k = 0; k < n; ++k) {
+      Job* j = active[(rr + k) % n];
+      if (!j->busy) {
+        rr = (rr + k + 1) % n;
+        return j;
+      }
+    }
+    return nullptr;
+  }
+
+  static void fail(Job* j, int rc, const char* what) {
+    j->status = rc;
+    char buf[256] = {0};
+    if (j->h) cuwaves_last_error(j->h, buf, sizeof(buf));
+    j->err = std::string(what) + ": " + buf;
+  }
+
+  // one unit of work of job j, outside the lock
+  static bool run_unit(Job* j) {
+    int rc;
+    if (!j->h) {
+      j->dims.isp = j->isp.data();
+      if ((rc = cuwaves_create(&j->dims, &j->h)) != CUW_OK) {
+        j->h = nullptr;
+        fail(j, rc, "create");
+        return true;
+      }
+      if ((rc = cuwaves_set_gset(j->h, j->igvec.data(), j->minusg.data(), j->gbas.data(), j->gvec.data(),
+                                 j->g2.data(), j->pro.data(), j->ylm.data(), j->mpsi.data(), nullptr, j->gweight)) ||
+          (rc = cuwaves_set_potential(j->h, j->v.data())) || (rc = cuwaves_set_dh(j->h, j->lmnxx, j->dh.data())) ||
+          (rc = cuwaves_set_do(j->h, j->lnxx, j->dover.data())) || (rc = cuwaves_reset_atoms(j->h, j->r0.data())) ||
+          (rc = cuwaves_set_occ(j->h, j->occ.data())) || (rc = cuwaves_set_dynamics(j->h, j->delt, j->annee)) ||
+          (rc = cuwaves_upload_psi(j->h, CUW_PSI0, j->psi.data())) ||
+          (rc = cuwaves_upload_psi(j->h, CUW_PSIM, j->psi.data())) ||
+          (rc = cuwaves_gramschmidt(j->h, CUW_PSI0, j->r0.data())) ||
+          (rc = cuwaves_gramschmidt(j->h, CUW_PSIM, j->r0.data())) || (rc = cuwaves_projections(j->h))) {
+        fail(j, rc, "set-up");
+        return true;
+      }
+      return false;
+    }
+    j->force.assign(3 * (size_t)j->dims.nat, 0.0);
+    if (j->nsteps == 0) {
+      if ((rc = cuwaves_etot(j->h, j->out, j->force.data())) != CUW_OK) fail(j, rc, "single point");
+      return true;
+    }
+    const bool move = !j->mass.empty();
+    if ((rc = cuwaves_cp_step(j->h, move ? 1 : 0, move ? j->mass.data() : nullptr, 200, 1e-8, j->out,
+                              j->force.data())) != CUW_OK) {
+      fail(j, rc, "CP step");
+      return true;
+    }
+    return ++j->done_steps >= j->nsteps;
+  }
+
+  void worker() {
+    std::unique_lock<std::mutex> lk(mu);
+    while (!stop) {
+      admit();
+      Job* j = pick();
+      if (!j) {
+        cv.wait(lk);
+        continue;
+      }
+      j->busy = true;
+      lk.unlock();
+      const bool done = run_unit(j);
+      if (done && j->h) {
+        cuwaves_destroy(j->h);
+        j->h = nullptr;
+      }
+      lk.lock();
+      j->busy = false;
+      if (done) {
+        const Clock::time_point now = Clock::now();
+        account(now);
+        j->finished = true;
+        j->t_done = now;
+        t_last = now;
+        active.erase(std::find(active.begin(), active.end(), j));
+        if (rr > 0 && rr >= active.size()) rr = 0;
+        in_use -= j->bytes;
+        if (j->status == CUW_OK) {
+          ++completed;
+          latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - j->t_submit).count());
+        } else {
+          ++failed;
+        }
+      }
+      cv.notify_all();
+    }
+  }
+};
+
+namespace {
+
+template <class T>
+bool copy_in(std::vector<T>& dst, const T* src, size_t n, bool required) {
+  if (!src) {
+    dst.clear();
+    return !required;
+  }
+  dst.assign(src, src + n);
+  return true;
+}
+
+double percentile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (double)(v.size() - 1);
+  const size_t i = (size_t)pos;
+  const double f = pos - (double)i;
+  return i + 1 < v.size() ? v[i] * (1.0 - f) + v[i + 1] * f : v[i];
+}
+
+}  // namespace
+
+extern "C" int cuwaves_server_create(size_t hbm_budget, int nworkers, cuw_server** out) {
+  if (!out || nworkers < 1 || nworkers > 64 || hbm_budget == 0) return CUW_ERR_ARG;
+  cuw_server* s = new (std::nothrow) cuw_server;
+  if (!s) return CUW_ERR_NOMEM;
+  s->budget = hbm_budget;
+  s->t_mark = Clock::now();
+  for (int w = 0; w < nworkers; ++w) s->workers.emplace_back([s] { s->worker(); });
+  *out = s;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_submit(cuw_server* s, const cuw_request* r, long long* id) {
+  if (!s || !r || !id) return CUW_ERR_ARG;
+  const cuw_dims& d = r->dims;
+  if (d.ngl <= 0 || d.nb <= 0 || d.nbh <= 0 || d.nat <= 0 || d.nsp <= 0 || d.nsp > CUW_MAXSP || d.lmx <= 0 ||
+      d.nr1 <= 0 || d.nr2 <= 0 || d.nr3 <= 0 || !d.isp || r->nsteps < 0 || r->lmnxx <= 0 || r->lnxx <= 0)
+    return CUW_ERR_ARG;
+  for (int a = 0; a < d.nat; ++a)
+    if (d.isp[a] < 1 || d.isp[a] > d.nsp) return CUW_ERR_ARG;
+  for (int sp = 0; sp < d.nsp; ++sp)
+    if (d.lnx[sp] < 0 || d.lnx[sp] > CUW_MAXLN) return CUW_ERR_ARG;
+  std::unique_ptr<Job> j(new (std::nothrow) Job);
+  if (!j) return CUW_ERR_NOMEM;
+  j->dims = d;
+  const size_t ngl = d.ngl, nat = d.nat, nr = (size_t)d.nr1 * d.nr2 * d.nr3;
+  size_t nbare = 0;
+  for (int sp = 0; sp < d.nsp; ++sp) nbare += d.lnx[sp];
+  bool ok = copy_in(j->isp, d.isp, nat, true) && copy_in(j->igvec, r->igvec, 3 * ngl, true) &&
+            copy_in(j->minusg, r->minusg, ngl, true) && copy_in(j->gbas, r->gbas, 9, true) &&
+            copy_in(j->gvec, r->gvec, 3 * ngl, true) && copy_in(j->g2, r->g2, ngl, true) &&
+            copy_in(j->pro, r->pro, ngl * nbare, true) && copy_in(j->ylm, r->ylm, ngl * (size_t)d.lmx, true) &&
+            copy_in(j->mpsi, r->mpsi, ngl, true) && copy_in(j->v, r->v, nr, true) &&
+            copy_in(j->dh, r->dh, 2 * (size_t)r->lmnxx * r->lmnxx * nat, true) &&
+            copy_in(j->dover, r->dover, (size_t)r->lnxx * r->lnxx * d.nsp, true) &&
+            copy_in(j->r0, r->r0, 3 * nat, true) && copy_in(j->occ, r->occ, (size_t)d.nb, true) &&
+            copy_in(j->psi, r->psi, 2 * ngl * (size_t)d.nbh, true) && copy_in(j->mass, r->mass, nat, false);
+  if (!ok) return CUW_ERR_ARG;
+  j->dims.isp = nullptr;
+  j->gweight = r->gweight;
+  j->delt = r->delt;
+  j->annee = r->annee;
+  j->lmnxx = r->lmnxx;
+  j->lnxx = r->lnxx;
+  j->nsteps = r->nsteps;
+  j->bytes = estimate_bytes(d, j->isp);
+  if (j->bytes > s->budget) return CUW_ERR_NOMEM;  // could never be admitted
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return CUW_ERR_STATE;
+  j->id = s->next_id++;
+  j->t_submit = Clock::now();
+  if (!s->have_first) {
+    s->have_first = true;
+    s->t_first = j->t_submit;
+  }
+  *id = j->id;
+  s->queue.push_back(j.get());
+  s->jobs[j->id] = std::move(j);
+  s->cv.notify_all();
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_poll(cuw_server* s, long long id, int* done, int* status, double* out,
+                                   double* force, double* latency_ms) {
+  if (!s || !done) return CUW_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return CUW_ERR_ARG;
+  Job* j = it->second.get();
+  *done = j->finished ? 1 : 0;
+  if (!j->finished) return CUW_OK;
+  if (status) *status = j->status;
+  if (out) std::memcpy(out, j->out, sizeof(j->out));
+  if (force && !j->force.empty()) std::memcpy(force, j->force.data(), sizeof(double) * j->force.size());
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_error(cuw_server* s, long long id, char* buf, int len) {
+  if (!s || !buf || len <= 0) return CUW_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return CUW_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", it->second->err.c_str());
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_release(cuw_server* s, long long id) {
+  if (!s) return CUW_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end() || !it->second->finished) return CUW_ERR_ARG;
+  s->jobs.erase(it);
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_wait_all(cuw_server* s) {
+  if (!s) return CUW_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  s->cv.wait(lk, [s] { return s->queue.empty() && s->active.empty(); });
+  return s->failed ? CUW_ERR_STATE : CUW_OK;
+}
+
+extern "C" int cuwaves_server_stats(cuw_server* s, double* out, int n) {
+  if (!s || !out || n < 0) return CUW_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->account(Clock::now());
+  const double span = s->have_first ? std::chrono::duration<double>(s->t_last - s->t_first).count() : 0.0;
+  const double v[10] = {(double)s->completed,
+                        (double)s->failed,
+                        percentile(s->latencies_ms, 0.50),
+                        percentile(s->latencies_ms, 0.99),
+                        span > 0 ? (double)s->completed / span : 0.0,
+                        (double)s->peak,
+                        (double)s->in_use,
+                        (double)(s->queue.size() + s->active.size()),
+                        span > 0 ? s->busy_integral / span : 0.0,
+                        s->latencies_ms.empty() ? 0.0 : *std::max_element(s->latencies_ms.begin(), s->latencies_ms.end())};
+  for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_destroy(cuw_server* s) {
+  if (!s) return CUW_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;  // workers finish the unit they hold, then leave
+    s->cv.notify_all();
+  }
+  for (auto& t : s->workers) t.join();
+  for (Job* j : s->active)
+    if (j->h) cuwaves_destroy(j->h);
+  delete s;
+  return CUW_OK;
+}

@@ -75,6 +75,7 @@ SIGNATURES = {
     "switch": [_P],
     "stop": [_P],
     "cp_step": [_P, C.c_int, _D, C.c_int, C.c_double, _D, _D],
+    "etot": [_P, _D, _D],
 }
 OPTIONAL = {
     "set_async": [_P, C.c_int],
@@ -309,6 +310,14 @@ class Waves:
         m = np.ascontiguousarray(self.inp["masses"], dtype=np.float64)
         self._chk(self._f["cp_step"](self.h, int(move_atoms), _dptr(m), max_iter, eps, _dptr(out), _dptr(f)),
                   "TIMESTEP")
+        return out, f
+
+    def etot(self, want_force=True):
+        """Single-point energy (sum_n f_n <psi_n|H|psi_n>, kinetic energy) and forces
+        at PSI0 and R(0), without propagation (WAVES$ETOT energy part)."""
+        out = np.zeros(2)
+        f = np.zeros((self.nat, 3)) if want_force else None
+        self._chk(self._f["etot"](self.h, _dptr(out), _dptr(f)), "ETOT")
         return out, f
 
     def set_async(self, flag: bool):

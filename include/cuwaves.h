@@ -44,7 +44,7 @@ extern "C" {
 #define CUW_OPSI 3   /* THIS%OPSI (mass-scaled O|psi0>, valid inside a step) */
 
 #define CUW_PREC_FP64  0  /* every product in FP64 */
-#define CUW_PREC_MIXED 1  /* FP32 FFT/V.psi, split-BF16 tensor-core contractions, FP64 solves */
+#define CUW_PREC_MIXED 1  /* FP32 FFT/V.psi, split-tf32 tensor-core contractions, FP64 solves */
 
 #define CUW_MAXSP 16
 #define CUW_MAXLN 8
@@ -145,6 +145,72 @@ int cuwaves_cp_step(cuw_handle* h, int move_atoms, const double* mass,
                     int max_iter, double eps, double* out, double* force);
 /* Resets the nuclear history so that R(-) = R(0) (start from rest). */
 int cuwaves_reset_atoms(cuw_handle* h, const double* r0);
+/* Single-point evaluation at PSI0 and R(0), the energy part of WAVES$ETOT
+ * (src/paw_waves1.f90:2094-2123) with EKIN (:2790-2954) and FORCE
+ * (:4570-4739): out[0] = sum_n f_n <psi_n|H|psi_n>, out[1] = kinetic energy,
+ * force (3*NAT, may be NULL).  Nothing is propagated. */
+int cuwaves_etot(cuw_handle* h, double* out, double* force);
+
+/* Serving runtime (no counterpart in the reference, which runs one system per
+ * program: PAW_DRIVER's time loop, src/paw_driver.f90:280-561).  A request
+ * carries the complete input of one wave-function set, with the meanings and
+ * layouts of cuwaves_set_gset, _set_potential, _set_dh, _set_do, _set_occ,
+ * _set_dynamics and _upload_psi; the server copies every array at submission.
+ * nsteps = 0 asks for a single point (cuwaves_etot after Gram-Schmidt of psi at
+ * r0); nsteps > 0 for that many cuwaves_cp_step calls starting from rest
+ * (PSIM = PSI0), with the nuclei moving when mass (NAT) is given.  Requests are
+ * admitted in submission order while the estimated device memory of all
+ * admitted sets stays within hbm_budget bytes; nworkers host threads advance
+ * the admitted sets one step at a time in round-robin order, each set on its
+ * own CUDA stream, so that sets of different sizes share the GPU and a new
+ * request starts as soon as memory is free.  A set's result does not depend on
+ * what else the server runs (every reduction has a fixed order). */
+typedef struct cuw_server cuw_server;
+typedef struct cuw_request {
+  cuw_dims dims;  /* dims.isp is copied */
+  const int* igvec;
+  const int* minusg;
+  const double* gbas;
+  const double* gvec;
+  const double* g2;
+  const double* pro;
+  const double* ylm;
+  const double* mpsi;
+  double gweight;
+  const double* v;
+  int lmnxx;
+  const double* dh;
+  int lnxx;
+  const double* dover;
+  const double* r0;
+  const double* occ;
+  const double* psi;   /* starting PSI0 (complex NGL x NBH) */
+  double delt, annee;
+  int nsteps;
+  const double* mass;  /* (NAT) electron masses, or NULL: fixed nuclei */
+} cuw_request;
+
+int cuwaves_server_create(size_t hbm_budget, int nworkers, cuw_server** out);
+/* CUW_ERR_NOMEM when the request alone exceeds the budget. */
+int cuwaves_server_submit(cuw_server* s, const cuw_request* r, long long* id);
+/* *done = 1 once the request has finished; then *status is its own CUW_* code,
+ * out[8] the last cuwaves_cp_step (or cuwaves_etot: out[0..1]) output, force
+ * (3,NAT) the forces of the last step and *latency_ms the time from submission
+ * to completion.  Any output pointer may be NULL. */
+int cuwaves_server_poll(cuw_server* s, long long id, int* done, int* status, double* out,
+                        double* force, double* latency_ms);
+int cuwaves_server_error(cuw_server* s, long long id, char* buf, int len);
+/* Forgets a finished request. */
+int cuwaves_server_release(cuw_server* s, long long id);
+/* Blocks until every submitted request has finished; CUW_ERR_STATE if any failed. */
+int cuwaves_server_wait_all(cuw_server* s);
+/* out[0] completed, [1] failed, [2] p50 and [3] p99 latency in ms, [4] requests
+ * completed per second between the first submission and the last completion,
+ * [5] peak and [6] current admitted device bytes, [7] requests in the system,
+ * [8] mean number of admitted sets, [9] maximum latency in ms.  n values. */
+int cuwaves_server_stats(cuw_server* s, double* out, int n);
+/* Finishes the steps in flight, releases every set and stops the workers. */
+int cuwaves_server_destroy(cuw_server* s);
 
 /* Measurement hooks (no counterpart in the reference, whose TIMING$CLOCKON/OFF
  * clocks, src/paw_timing.f90:121-192, play this role on the CPU).

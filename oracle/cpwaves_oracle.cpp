@@ -1378,6 +1378,30 @@ int orc_force(orc_handle* h, double* force) {
 
 // One CP step in the order of TIMESTEP (src/paw_driver.f90:280-561) for a fixed
 // potential; see cuwaves_cp_step in the C ABI for the meaning of out[].
+// Single-point energy and forces at PSI0, R(0): the energy part of WAVES$ETOT
+// (src/paw_waves1.f90:2094-2123) with EKIN and FORCE; nothing is propagated.
+int orc_etot(orc_handle* h, double* out, double* force) {
+  const int nb = h->d.nb, nat = h->d.nat;
+  double ekin = 0.0;
+  int st = orc_ekin(h, &ekin);
+  if (st) return st;
+  if (force) {
+    std::vector<double> f(3 * nat);
+    st = orc_force(h, f.data());
+    if (st) return st;
+    std::copy(f.begin(), f.end(), force);
+  }
+  st = orc_hpsi(h);
+  if (st) return st;
+  std::vector<double> eig(nb);
+  orc_expectation(h, eig.data());
+  double etot = 0.0;
+  for (int i = 0; i < nb; ++i) etot += h->occ[i] * eig[i];
+  out[0] = etot;
+  out[1] = ekin;
+  return CUW_OK;
+}
+
 int orc_cp_step(orc_handle* h, int move_atoms, const double* mass, int maxit, double eps,
                 double* out, double* force) {
   const int nb = h->d.nb, nat = h->d.nat;

@@ -29,14 +29,18 @@ def test_library_exports_every_declared_symbol(engine_lib):
 
 def test_binding_covers_the_abi(engine_lib):
     from cuwaves.capi import OPTIONAL, SIGNATURES
+    from cuwaves.serve import _bind
 
     bound = {"cuwaves_" + n for n in list(SIGNATURES) + list(OPTIONAL)}
+    bound |= {"cuwaves_server_" + n for n in _bind()}
     assert set(declared_symbols()) <= bound | {"cuwaves_get_atoms"}
 
 
 def test_oracle_exports_the_same_abi(oracle):
     lib = oracle.library()
     for n in declared_symbols():
+        if n.startswith("cuwaves_server_"):  # runtime over the ABI, not part of the path
+            continue
         if n in ("cuwaves_set_async", "cuwaves_synchronize", "cuwaves_set_timing", "cuwaves_get_timing",
                  "cuwaves_get_stream", "cuwaves_get_ortho_stats", "cuwaves_projections_noalloc",
                  "cuwaves_tc_gemm_check"):  # device-only entry points
@@ -72,3 +76,28 @@ def test_invalid_dims_rejected_without_device(engine_lib):
         assert rc == 0
         lib.cuwaves_destroy.argtypes = [C.c_void_p]
         lib.cuwaves_destroy(h)
+
+
+def test_server_admission_rules_without_device(engine_lib):
+    """Submission validates and copies on the host; a request whose estimated
+    device memory exceeds the whole budget is refused (CUW_ERR_NOMEM), and an
+    idle server shuts down cleanly."""
+    from cuwaves import systems
+    from cuwaves.capi import WavesError
+    from cuwaves.serve import Server
+
+    inp = systems.build_inputs(systems.molecule_box("Si2", box=12.0))
+    srv = Server(hbm_budget=1 << 20, workers=2)  # 1 MiB: nothing fits
+    with pytest.raises(WavesError) as e:
+        srv.submit(inp, nsteps=0)
+    assert e.value.code == 8
+    bad = dict(inp)
+    bad["isp"] = np.full_like(np.asarray(inp["isp"]), 7)  # species index out of range
+    with pytest.raises(WavesError) as e:
+        srv.submit(bad, nsteps=0)
+    assert e.value.code == 1
+    st = srv.stats()
+    assert st["completed"] == 0 and st["in_system"] == 0 and st["peak_bytes"] == 0
+    srv.close()
+    with pytest.raises(WavesError):
+        Server(hbm_budget=0)
