@@ -294,6 +294,147 @@ def run_mixed(args, local):
             "phase_ms_per_step": {k: round(v / max(1, nsteps), 4) for k, v in phases.items()}}
 
 
+def run_serving(args):
+    """Serving workload: a seeded Poisson stream of single-point solves and
+    20-step CP runs of perturbed bulk Si_n and water clusters, submitted in
+    real time to the device-resident server (HBM-budget admission, continuous
+    batching).  Latency is submission to completion, measured by the server."""
+    import numpy as np
+    import cuwaves
+    from cuwaves import systems
+    from cuwaves.serve import Server
+
+    rng = np.random.default_rng(7)
+    kinds = [("Si", n) for n in sorted(systems.SERVING_SI)] + [("W", n) for n in systems.SERVING_WATER]
+    pool = {}
+    for kind, n in kinds:
+        for seed in (1, 2):
+            inp = systems.build_inputs(systems.serving_system(kind, n, seed))
+            inp["annee"] = 0.05  # friction on the wave functions: a damped (relaxing) run
+            pool[(kind, n, seed)] = inp
+    nreq, rate = args.serve_requests, args.serve_rate
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+    plan = []
+    for i in range(nreq):
+        kind, n = kinds[int(rng.integers(0, len(kinds)))]
+        plan.append(((kind, n, int(rng.integers(1, 3))), 0 if rng.random() < 0.5 else 20))
+    srv = Server(hbm_budget=args.serve_budget_gb << 30, workers=args.serve_workers)
+    # warm-up outside the stream: one request of every kind
+    for kind, n in kinds:
+        srv.submit(pool[(kind, n, 1)], nsteps=1, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
+    srv.wait_all()
+    srv.close()
+    srv = Server(hbm_budget=args.serve_budget_gb << 30, workers=args.serve_workers)
+    ids = []
+    t0 = time.perf_counter()
+    for (key, nsteps), ta in zip(plan, arrivals):
+        dt = ta - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append((srv.submit(pool[key], nsteps=nsteps, move_atoms=nsteps > 0, precision=cuwaves.CUW_PREC_MIXED,
+                               borrow=True), nsteps))
+    srv.wait_all()
+    st = srv.stats()
+    lat = {0: [], 20: []}
+    failed = 0
+    for rid, nsteps in ids:
+        r = srv.poll(rid)
+        if r[0]:
+            failed += 1
+        else:
+            lat[nsteps].append(r[3])
+    srv.close()
+    pct = lambda v, q: round(float(np.percentile(v, q)), 3) if v else None  # noqa: E731
+    return {"requests": nreq, "offered_rate_per_s": rate, "completed": int(st["completed"]), "failed": failed,
+            "solves_per_s": round(st["throughput_per_s"], 3), "p50_ms": round(st["p50_ms"], 3),
+            "p99_ms": round(st["p99_ms"], 3), "max_ms": round(st["max_ms"], 3),
+            "single_point_p50_ms": pct(lat[0], 50), "single_point_p99_ms": pct(lat[0], 99),
+            "cp20_p50_ms": pct(lat[20], 50), "cp20_p99_ms": pct(lat[20], 99),
+            "hbm_budget_gb": args.serve_budget_gb, "peak_admitted_gb": round(st["peak_bytes"] / 2 ** 30, 3),
+            "mean_admitted_sets": round(st["mean_admitted"], 2), "workers": args.serve_workers,
+            "precision": "mixed",
+            "workload": "Poisson stream, 50% single points (energy+forces) and 50% 20-step damped CP runs with "
+                        "moving nuclei; Si8/16/32/64/128 (+-0.05 bohr, 30 Ry) and (H2O)1/2/4/8/16 clusters (40 Ry, "
+                        "8 bohr vacuum), two seeds each; latency from submission to completion"}
+
+
+def run_batched(args):
+    """Batched workloads, mixed precision.
+    (1) Si64: `batched_si64` independent Si64 cells (different seeded
+        displacements), resident together, each stepped by its own host thread
+        on its own stream; aggregate CP steps/s after set-up and warm-up
+        (device-resident steady state).
+    (2) 64 independent small systems of uneven size (bulk Si2-Si16, Si2 and
+        H2O molecules in 20-bohr boxes) through the server, all admitted at
+        once, set-up included, against the same systems one at a time."""
+    import threading
+
+    import torch
+    import cuwaves
+    from cuwaves import systems
+    from cuwaves.serve import Server
+
+    res = {}
+    for prec, tag in ((cuwaves.CUW_PREC_MIXED, "mixed"), (cuwaves.CUW_PREC_FP64, "fp64")):
+        ws = []
+        for i in range(args.batched_si64):
+            inp = systems.build_inputs(systems.si_cell(2, a=10.26, disp=0.05, seed=1 + i, grid=(64, 64, 64),
+                                                       name="Si64"))
+            ws.append(cuwaves.open_waves(inp, precision=prec).setup().initialize())
+        for w in ws:
+            for _ in range(args.warmup):
+                w.cp_step(move_atoms=True)
+        bar = threading.Barrier(len(ws) + 1)
+
+        def body(w):
+            bar.wait()
+            for _ in range(args.steps):
+                w.cp_step(move_atoms=True)
+
+        th = [threading.Thread(target=body, args=(w,)) for w in ws]
+        for t in th:
+            t.start()
+        torch.cuda.synchronize()
+        bar.wait()
+        t0 = time.perf_counter()
+        for t in th:
+            t.join()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        for w in ws:
+            w.close()
+        res[tag] = len(ws) * args.steps / dt
+    inps = [systems.build_inputs(s) for s in systems.batched_mix(64)]
+    k = args.batched_steps
+    small = {}
+    for workers in (1, args.batched_workers):
+        srv = Server(hbm_budget=64 << 30, workers=workers)
+        for inp in inps[:4]:  # warm-up
+            srv.submit(inp, nsteps=1, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
+        srv.wait_all()
+        srv.close()
+        srv = Server(hbm_budget=64 << 30, workers=workers)
+        t0 = time.perf_counter()
+        for inp in inps:
+            srv.submit(inp, nsteps=k, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
+        srv.wait_all()
+        dt = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        small[workers] = (len(inps) * k / dt, st)
+    vb, stb = small[args.batched_workers]
+    return {"value": round(res["mixed"], 2), "unit": "CP steps/s (all Si64 cells)", "precision": "mixed",
+            "si64_cells": args.batched_si64, "fp64_same_batch": round(res["fp64"], 2),
+            "timing": "wall clock between a host barrier and the last thread's last step, with device "
+                      "synchronisation on both sides; every step ends in a host read of its energies",
+            "small_systems": {"value": round(vb, 2), "unit": "CP steps/s (all systems, set-up included)",
+                              "systems": len(inps), "steps_per_system": k, "workers": args.batched_workers,
+                              "one_at_a_time_value": round(small[1][0], 2),
+                              "mean_admitted_sets": round(stb["mean_admitted"], 2), "failed": int(stb["failed"]),
+                              "sizes": "Si2-Si16 bulk (4-32 bands, 28^3 / 28x28x56 grids), Si2 and H2O molecules "
+                                       "in 20-bohr boxes (56^3)"}}
+
+
 def emit_cuda(args, res, world):
     ph = res["phases_ms_per_step"]
     fm = res["fm"]
@@ -329,6 +470,8 @@ def emit_cuda(args, res, world):
         "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()},
         "ortho_solve": res.get("ortho"),
         "mixed": res.get("mixed"),
+        "serving": res.get("serving"),
+        "batched": res.get("batched"),
         "clocks": res["clocks"],
         "cpu_baseline": cpu,
     }
@@ -403,6 +546,14 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving and batched runs")
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-workers", type=int, default=8)
+    ap.add_argument("--serve-budget-gb", type=int, default=48)
+    ap.add_argument("--batched-steps", type=int, default=10)
+    ap.add_argument("--batched-workers", type=int, default=16)
+    ap.add_argument("--batched-si64", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "cuda" else args.warmup
     if args.impl == "reference":
@@ -416,6 +567,9 @@ def main():
     res = run_cuda(args, rank, world, local)
     if not args.no_mixed:
         res["mixed"] = run_mixed(args, local)
+    if not args.no_serving and world == 1:
+        res["serving"] = run_serving(args)
+        res["batched"] = run_batched(args)
     if rank == 0:
         if world > 1 or args.no_cpu:
             args.no_cpu = args.no_cpu or rank != 0

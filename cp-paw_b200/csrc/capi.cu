@@ -8,7 +8,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cuwaves_internal.cuh"
@@ -215,6 +218,20 @@ static int energy_run(Handle* h, int mode, double* out_dev) {
                                          h->gweight, h->delt * h->delt, h->tbucket ? 1 : 0, out_dev);
   CUW_LAUNCH_CHECK("k_energy_final");
   return CUW_OK;
+}
+
+cudaError_t smem_allow(const void* fn, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> limit;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  int& cur = limit[std::make_pair(dev, fn)];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
 }
 
 int band_reduce(Handle* h, int what, double* out_host, double* eig_host) {

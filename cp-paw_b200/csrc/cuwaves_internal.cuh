@@ -253,6 +253,11 @@ struct GramPair {
 int gram_planewave(Handle* h, const GramPair* pairs, int npair, double2* dst);
 int gram_projections(Handle* h, const GramPair* pairs, int npair, double2* dst);
 int ensure_part(Handle* h, size_t bytes);  // split-K scratch h->g.part of at least `bytes`
+// Raises (never lowers) the dynamic shared-memory limit of kernel fn on the
+// current device.  The limit belongs to the function, so it is shared by all
+// handles of the process: a handle of a smaller system must not lower the
+// limit that a larger one launches with.
+cudaError_t smem_allow(const void* fn, int bytes);
 // split-precision (tf32 x3) tensor-core versions, used when precision is
 // CUW_PREC_MIXED; same arguments and results as the FP64 functions above
 int tc_setup(Handle* h);

@@ -571,9 +571,9 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
 template <class C, int N>
 static int fft_select(Handle* h, int smem_plane, int /*smem_z of the generic kernel*/) {
   const int smem_z = (int)(((size_t)h->d.nr3 * tx_of<N>() + h->d.nr3) * sizeof(C));
-  CUW_TRY(cudaFuncSetAttribute(k_gtor_plane<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-  CUW_TRY(cudaFuncSetAttribute(k_rtog_plane<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plane));
-  CUW_TRY(cudaFuncSetAttribute(k_zcol_v<C, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_z));
+  CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N>, smem_plane));
+  CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N>, smem_plane));
+  CUW_TRY(smem_allow((const void*)k_zcol_v<C, N>, smem_z));
   h->fft_run = &fft_vpsi_t<C, N>;
   return CUW_OK;
 }

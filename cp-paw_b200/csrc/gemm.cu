@@ -835,23 +835,16 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
 
 // dynamic shared memory above 48 KB for the pipelined contraction kernels
 int gemm_setup(Handle* h) {
-  CUW_TRY(cudaFuncSetAttribute(k_proj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<MP21>()));
-  CUW_TRY(cudaFuncSetAttribute(k_proj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<MP11>()));
-  CUW_TRY(cudaFuncSetAttribute(k_addpro<ADDPRO_HPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MP11>()));
-  CUW_TRY(cudaFuncSetAttribute(k_addpro<ADDPRO_OPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MP11>()));
-  CUW_TRY(cudaFuncSetAttribute(k_addpro<ADDPRO_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MP12>()));
-  CUW_TRY(cudaFuncSetAttribute(k_gram<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MPGRAM>()));
-  CUW_TRY(cudaFuncSetAttribute(k_gram<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MPGRAM>()));
-  CUW_TRY(cudaFuncSetAttribute(k_addx<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MP11>()));
-  CUW_TRY(cudaFuncSetAttribute(k_addx<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<MP11>()));
-  CUW_TRY(cudaFuncSetAttribute(k_force, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_proj<true>, (int)smem_bytes<MP21>()));
+  CUW_TRY(smem_allow((const void*)k_proj<false>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED>, (int)smem_bytes<MP12>()));
+  CUW_TRY(smem_allow((const void*)k_gram<true, true>, (int)smem_bytes<MPGRAM>()));
+  CUW_TRY(smem_allow((const void*)k_gram<false, false>, (int)smem_bytes<MPGRAM>()));
+  CUW_TRY(smem_allow((const void*)k_addx<true, true>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addx<false, false>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_force, (int)smem_bytes<MP11>()));
   return CUW_OK;
 }
 
@@ -928,8 +921,7 @@ static int noalloc_scratch(double2** out) {
   if (!g_noalloc_ptr[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return CUW_ERR_CUDA;
-    if (cudaFuncSetAttribute(cuw::k_proj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)cuw::smem_bytes<cuw::MP11>()) != cudaSuccess)
+    if (cuw::smem_allow((const void*)cuw::k_proj<false>, (int)cuw::smem_bytes<cuw::MP11>()) != cudaSuccess)
       return CUW_ERR_CUDA;
     g_noalloc_ptr[dev] = static_cast<double2*>(p);
   }

@@ -878,7 +878,7 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
     smem = base;
   }
   if (smem > 220 * 1024) return h->fail(CUW_ERR_UNSUPPORTED, "NB too large for the on-chip eigensolver");
-  CUW_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUW_TRY(smem_allow((const void*)k_jacobi, (int)smem));
   int* info = reinterpret_cast<int*>(h->g.ostatus) + 4;
   k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, 40, info);
   CUW_LAUNCH_CHECK("k_jacobi");
@@ -964,7 +964,7 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
       cudaGetLastError();
       continue;
     }
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (smem_allow((const void*)fn, (int)smem) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }

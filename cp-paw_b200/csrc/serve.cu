@@ -31,11 +31,21 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Input arrays of one request: either views of the caller's arrays
+// (CUW_REQ_BORROW) or of the copies the job owns.
+struct Inputs {
+  const int *isp = nullptr, *igvec = nullptr, *minusg = nullptr;
+  const double *gbas = nullptr, *gvec = nullptr, *g2 = nullptr, *pro = nullptr, *ylm = nullptr, *mpsi = nullptr,
+               *v = nullptr, *dh = nullptr, *dover = nullptr, *r0 = nullptr, *occ = nullptr, *psi = nullptr,
+               *mass = nullptr;
+};
+
 struct Job {
   long long id = 0;
   cuw_dims dims{};
-  std::vector<int> isp, igvec, minusg;
-  std::vector<double> gbas, gvec, g2, pro, ylm, mpsi, v, dh, dover, r0, occ, psi, mass;
+  Inputs in;
+  std::vector<int> own_i;     // owned copies (isp, igvec, minusg)
+  std::vector<double> own_d;  // owned copies of the double arrays
   double gweight = 0.0, delt = 0.0, annee = 0.0;
   int lmnxx = 0, lnxx = 0, nsteps = 0, done_steps = 0;
   cuw_handle* h = nullptr;
@@ -49,7 +59,7 @@ struct Job {
 };
 
 // projectors of the set (sum over atoms of 2l+1 per radial function)
-int count_projectors(const cuw_dims& d, const std::vector<int>& isp) {
+int count_projectors(const cuw_dims& d, const int* isp) {
   int n = 0;
   for (int a = 0; a < d.nat; ++a) {
     const int s = isp[a] - 1;
@@ -60,7 +70,7 @@ int count_projectors(const cuw_dims& d, const std::vector<int>& isp) {
 
 // Upper estimate of the device memory of one handle (the allocations of
 // cuwaves_create and the FFT set-up, plus the split-K scratch).
-size_t estimate_bytes(const cuw_dims& d, const std::vector<int>& isp) {
+size_t estimate_bytes(const cuw_dims& d, const int* isp) {
   const size_t ldg = (size_t)((d.ngl + 31) / 32) * 32, nbh = d.nbh, nb = d.nb, ngl = d.ngl;
   const size_t npro = count_projectors(d, isp);
   size_t nbare = 0;
@@ -137,21 +147,21 @@ struct cuw_server {
   static bool run_unit(Job* j) {
     int rc;
     if (!j->h) {
-      j->dims.isp = j->isp.data();
+      const Inputs& in = j->in;
+      j->dims.isp = in.isp;
       if ((rc = cuwaves_create(&j->dims, &j->h)) != CUW_OK) {
         j->h = nullptr;
         fail(j, rc, "create");
         return true;
       }
-      if ((rc = cuwaves_set_gset(j->h, j->igvec.data(), j->minusg.data(), j->gbas.data(), j->gvec.data(),
-                                 j->g2.data(), j->pro.data(), j->ylm.data(), j->mpsi.data(), nullptr, j->gweight)) ||
-          (rc = cuwaves_set_potential(j->h, j->v.data())) || (rc = cuwaves_set_dh(j->h, j->lmnxx, j->dh.data())) ||
-          (rc = cuwaves_set_do(j->h, j->lnxx, j->dover.data())) || (rc = cuwaves_reset_atoms(j->h, j->r0.data())) ||
-          (rc = cuwaves_set_occ(j->h, j->occ.data())) || (rc = cuwaves_set_dynamics(j->h, j->delt, j->annee)) ||
-          (rc = cuwaves_upload_psi(j->h, CUW_PSI0, j->psi.data())) ||
-          (rc = cuwaves_upload_psi(j->h, CUW_PSIM, j->psi.data())) ||
-          (rc = cuwaves_gramschmidt(j->h, CUW_PSI0, j->r0.data())) ||
-          (rc = cuwaves_gramschmidt(j->h, CUW_PSIM, j->r0.data())) || (rc = cuwaves_projections(j->h))) {
+      if ((rc = cuwaves_set_gset(j->h, in.igvec, in.minusg, in.gbas, in.gvec, in.g2, in.pro, in.ylm, in.mpsi, nullptr,
+                                 j->gweight)) ||
+          (rc = cuwaves_set_potential(j->h, in.v)) || (rc = cuwaves_set_dh(j->h, j->lmnxx, in.dh)) ||
+          (rc = cuwaves_set_do(j->h, j->lnxx, in.dover)) || (rc = cuwaves_reset_atoms(j->h, in.r0)) ||
+          (rc = cuwaves_set_occ(j->h, in.occ)) || (rc = cuwaves_set_dynamics(j->h, j->delt, j->annee)) ||
+          (rc = cuwaves_upload_psi(j->h, CUW_PSI0, in.psi)) || (rc = cuwaves_upload_psi(j->h, CUW_PSIM, in.psi)) ||
+          (rc = cuwaves_gramschmidt(j->h, CUW_PSI0, in.r0)) || (rc = cuwaves_gramschmidt(j->h, CUW_PSIM, in.r0)) ||
+          (rc = cuwaves_projections(j->h))) {
         fail(j, rc, "set-up");
         return true;
       }
@@ -162,8 +172,8 @@ struct cuw_server {
       if ((rc = cuwaves_etot(j->h, j->out, j->force.data())) != CUW_OK) fail(j, rc, "single point");
       return true;
     }
-    const bool move = !j->mass.empty();
-    if ((rc = cuwaves_cp_step(j->h, move ? 1 : 0, move ? j->mass.data() : nullptr, 200, 1e-8, j->out,
+    const bool move = j->in.mass != nullptr;
+    if ((rc = cuwaves_cp_step(j->h, move ? 1 : 0, j->in.mass, 200, 1e-8, j->out,
                               j->force.data())) != CUW_OK) {
       fail(j, rc, "CP step");
       return true;
@@ -212,16 +222,6 @@ struct cuw_server {
 
 namespace {
 
-template <class T>
-bool copy_in(std::vector<T>& dst, const T* src, size_t n, bool required) {
-  if (!src) {
-    dst.clear();
-    return !required;
-  }
-  dst.assign(src, src + n);
-  return true;
-}
-
 double percentile(std::vector<double> v, double q) {
   if (v.empty()) return 0.0;
   std::sort(v.begin(), v.end());
@@ -260,16 +260,51 @@ extern "C" int cuwaves_server_submit(cuw_server* s, const cuw_request* r, long l
   const size_t ngl = d.ngl, nat = d.nat, nr = (size_t)d.nr1 * d.nr2 * d.nr3;
   size_t nbare = 0;
   for (int sp = 0; sp < d.nsp; ++sp) nbare += d.lnx[sp];
-  bool ok = copy_in(j->isp, d.isp, nat, true) && copy_in(j->igvec, r->igvec, 3 * ngl, true) &&
-            copy_in(j->minusg, r->minusg, ngl, true) && copy_in(j->gbas, r->gbas, 9, true) &&
-            copy_in(j->gvec, r->gvec, 3 * ngl, true) && copy_in(j->g2, r->g2, ngl, true) &&
-            copy_in(j->pro, r->pro, ngl * nbare, true) && copy_in(j->ylm, r->ylm, ngl * (size_t)d.lmx, true) &&
-            copy_in(j->mpsi, r->mpsi, ngl, true) && copy_in(j->v, r->v, nr, true) &&
-            copy_in(j->dh, r->dh, 2 * (size_t)r->lmnxx * r->lmnxx * nat, true) &&
-            copy_in(j->dover, r->dover, (size_t)r->lnxx * r->lnxx * d.nsp, true) &&
-            copy_in(j->r0, r->r0, 3 * nat, true) && copy_in(j->occ, r->occ, (size_t)d.nb, true) &&
-            copy_in(j->psi, r->psi, 2 * ngl * (size_t)d.nbh, true) && copy_in(j->mass, r->mass, nat, false);
-  if (!ok) return CUW_ERR_ARG;
+  // (source, element count) of every array, in the order of Inputs
+  const int* isrc[3] = {d.isp, r->igvec, r->minusg};
+  const size_t icnt[3] = {nat, 3 * ngl, ngl};
+  const double* dsrc[13] = {r->gbas, r->gvec, r->g2, r->pro, r->ylm, r->mpsi, r->v,
+                            r->dh, r->dover, r->r0, r->occ, r->psi, r->mass};
+  const size_t dcnt[13] = {9, 3 * ngl, ngl, ngl * nbare, ngl * (size_t)d.lmx, ngl, nr,
+                           2 * (size_t)r->lmnxx * r->lmnxx * nat, (size_t)r->lnxx * r->lnxx * d.nsp, 3 * nat,
+                           (size_t)d.nb, 2 * ngl * (size_t)d.nbh, nat};
+  for (int k = 0; k < 3; ++k)
+    if (!isrc[k]) return CUW_ERR_ARG;
+  for (int k = 0; k < 12; ++k)  // mass (the last) is optional
+    if (!dsrc[k]) return CUW_ERR_ARG;
+  const int* ip[3];
+  const double* dp[13];
+  if (r->flags & CUW_REQ_BORROW) {
+    for (int k = 0; k < 3; ++k) ip[k] = isrc[k];
+    for (int k = 0; k < 13; ++k) dp[k] = dsrc[k];
+  } else {
+    size_t ni = 0, nd = 0;
+    for (int k = 0; k < 3; ++k) ni += icnt[k];
+    for (int k = 0; k < 13; ++k) nd += dsrc[k] ? dcnt[k] : 0;
+    try {
+      j->own_i.resize(ni);
+      j->own_d.resize(nd);
+    } catch (const std::bad_alloc&) {
+      return CUW_ERR_NOMEM;
+    }
+    size_t oi = 0, od = 0;
+    for (int k = 0; k < 3; ++k) {
+      std::memcpy(j->own_i.data() + oi, isrc[k], sizeof(int) * icnt[k]);
+      ip[k] = j->own_i.data() + oi;
+      oi += icnt[k];
+    }
+    for (int k = 0; k < 13; ++k) {
+      dp[k] = nullptr;
+      if (!dsrc[k]) continue;
+      std::memcpy(j->own_d.data() + od, dsrc[k], sizeof(double) * dcnt[k]);
+      dp[k] = j->own_d.data() + od;
+      od += dcnt[k];
+    }
+  }
+  Inputs& in = j->in;
+  in.isp = ip[0], in.igvec = ip[1], in.minusg = ip[2];
+  in.gbas = dp[0], in.gvec = dp[1], in.g2 = dp[2], in.pro = dp[3], in.ylm = dp[4], in.mpsi = dp[5], in.v = dp[6];
+  in.dh = dp[7], in.dover = dp[8], in.r0 = dp[9], in.occ = dp[10], in.psi = dp[11], in.mass = dp[12];
   j->dims.isp = nullptr;
   j->gweight = r->gweight;
   j->delt = r->delt;
@@ -277,7 +312,7 @@ extern "C" int cuwaves_server_submit(cuw_server* s, const cuw_request* r, long l
   j->lmnxx = r->lmnxx;
   j->lnxx = r->lnxx;
   j->nsteps = r->nsteps;
-  j->bytes = estimate_bytes(d, j->isp);
+  j->bytes = estimate_bytes(d, in.isp);
   if (j->bytes > s->budget) return CUW_ERR_NOMEM;  // could never be admitted
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return CUW_ERR_STATE;

@@ -460,15 +460,15 @@ static int tc_splits(Handle* h, int tiles, int nk) {
 
 int tc_setup(Handle* h) {
   const int sm = (int)MPipe::kSmem;
-  CUW_TRY(cudaFuncSetAttribute(k_tc_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_addpro<ADDPRO_HPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_addpro<ADDPRO_OPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_addpro<ADDPRO_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_gram<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_gram<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_addx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_addx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CUW_TRY(cudaFuncSetAttribute(k_tc_force, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_proj, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_HPSI>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_OPSI>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_FUSED>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_gram<true>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_gram<false>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_addx<true>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_addx<false>, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_force, sm));
   return CUW_OK;
 }
 
@@ -569,7 +569,7 @@ extern "C" int cuwaves_tc_gemm_check(int M, int N, int K, const double* A, const
   if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C || !err) return CUW_ERR_ARG;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t smem = MPipe::kSmem;
-  if (cudaFuncSetAttribute(k_tf32x3_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (smem_allow((const void*)k_tf32x3_gemm, (int)smem) != cudaSuccess)
     return CUW_ERR_CUDA;
   dim3 grid((M + 127) / 128, (N + 127) / 128);
   k_tf32x3_gemm<<<grid, MPipe::kThreads, smem, st>>>(M, N, K, A, B, C, err);

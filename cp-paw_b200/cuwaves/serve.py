@@ -23,8 +23,11 @@ class Request(C.Structure):
         ("igvec", _I), ("minusg", _I), ("gbas", _D), ("gvec", _D), ("g2", _D), ("pro", _D), ("ylm", _D),
         ("mpsi", _D), ("gweight", C.c_double), ("v", _D), ("lmnxx", C.c_int), ("dh", _D), ("lnxx", C.c_int),
         ("dover", _D), ("r0", _D), ("occ", _D), ("psi", _D), ("delt", C.c_double), ("annee", C.c_double),
-        ("nsteps", C.c_int), ("mass", _D),
+        ("nsteps", C.c_int), ("mass", _D), ("flags", C.c_int),
     ]
+
+
+CUW_REQ_BORROW = 1
 
 
 STATS = ("completed", "failed", "p50_ms", "p99_ms", "throughput_per_s", "peak_bytes", "bytes_in_use",
@@ -76,7 +79,9 @@ class Server:
         self._nat = {}
 
     def submit(self, inputs: dict, nsteps: int = 0, move_atoms: bool = False,
-               precision: int = CUW_PREC_FP64, psi: Optional[np.ndarray] = None) -> int:
+               precision: int = CUW_PREC_FP64, psi: Optional[np.ndarray] = None, borrow: bool = False) -> int:
+        """Queues one set; with borrow the server reads the arrays in place and
+        this object keeps them alive until the request is released."""
         i = inputs
         d = Dims()
         d.ngl, d.ndim, d.nb, d.nbh, d.tinv = i["ngl"], 1, i["nb"], i["nbh"], 1
@@ -117,11 +122,14 @@ class Server:
         r.delt, r.annee = float(i["delt"]), float(i["annee"])
         r.nsteps = int(nsteps)
         r.mass = _ptr(k["mass"], _D) if move_atoms else None
+        r.flags = CUW_REQ_BORROW if borrow else 0
         rid = C.c_longlong()
         rc = self._f["submit"](self.h, C.byref(r), C.byref(rid))
         if rc:
             raise WavesError(rc, "server_submit", "request rejected")
         self._nat[rid.value] = int(i["nat"])
+        if borrow:
+            self._keep[rid.value] = k
         return rid.value
 
     def poll(self, rid: int):
@@ -156,6 +164,7 @@ class Server:
     def release(self, rid: int):
         self._f["release"](self.h, rid)
         self._nat.pop(rid, None)
+        self._keep.pop(rid, None)
 
     def wait_all(self) -> int:
         return self._f["wait_all"](self.h)
@@ -169,6 +178,7 @@ class Server:
         if getattr(self, "h", None):
             self._f["destroy"](self.h)
             self.h = None
+        self._keep = {}
 
     def __del__(self):
         try:

@@ -412,6 +412,64 @@ def molecule_box(kind: str, box: float = 20.0, seed: int = 3, epw_psi_ry: float 
     raise ValueError(kind)
 
 
+def si_supercell(n1: int, n2: int, n3: int, a: float = 10.26, disp: float = 0.05, seed: int = 1,
+                 epw_psi_ry: float = 30.0, grid=None) -> System:
+    """n1 x n2 x n3 cubic cells of diamond Si (8 n1 n2 n3 atoms) with seeded
+    uniform [-disp, disp] bohr displacements; doubly occupied valence bands."""
+    rng = np.random.default_rng(seed)
+    frac = []
+    for i in range(n1):
+        for j in range(n2):
+            for k in range(n3):
+                for f in DIAMOND:
+                    frac.append(f + np.array([i, j, k]))
+    pos = np.array(frac, dtype=np.float64) * a
+    pos = pos + rng.uniform(-disp, disp, size=pos.shape)
+    nat = len(pos)
+    return System(f"Si{nat}", np.diag([n1 * a, n2 * a, n3 * a]), pos, [SI], np.ones(nat, dtype=np.int32), 2 * nat,
+                  0.5 * epw_psi_ry, grid or (0, 0, 0), seed=seed)
+
+
+def water_cluster(nmol: int, seed: int = 5, epw_psi_ry: float = 40.0, spacing: float = 5.6,
+                  vacuum: float = 8.0) -> System:
+    """A cluster of nmol water molecules (seeded orientations, on a cubic
+    lattice of the given spacing) centred in a cubic box with `vacuum` bohr of
+    space on every side."""
+    side = int(math.ceil(nmol ** (1.0 / 3.0) - 1e-9))
+    box = side * spacing + 2.0 * vacuum
+    s = water_box(nmol, box=side * spacing, lattice=(side, side, side), seed=seed, epw_psi_ry=epw_psi_ry)
+    s.pos = s.pos + vacuum
+    s.rbas = np.eye(3) * box
+    s.name = f"(H2O){nmol}"
+    return s
+
+
+# Batched workload: 64 independent small systems of uneven size (bulk Si2-Si16
+# cells and isolated molecules in 20-bohr boxes, 4-32 bands, 30 Ry).
+def batched_mix(count: int = 64, seed: int = 11) -> List[System]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        k = int(rng.integers(0, 10))
+        if k < 8:
+            out.append(si_small(int(2 * (k + 1)), seed=100 + i))  # Si2..Si16
+        else:
+            out.append(molecule_box("Si2" if k == 8 else "H2O", box=20.0, seed=100 + i))
+    return out
+
+
+# Serving workload: perturbed bulk Si_n (n in 8..128) and water clusters of
+# 1-16 molecules, 30-40 Ry.
+SERVING_SI = {8: (1, 1, 1), 16: (1, 1, 2), 32: (1, 2, 2), 64: (2, 2, 2), 128: (2, 2, 4)}
+SERVING_WATER = (1, 2, 4, 8, 16)
+
+
+def serving_system(kind: str, n: int, seed: int) -> System:
+    if kind == "Si":
+        return si_supercell(*SERVING_SI[n], disp=0.05, seed=seed, epw_psi_ry=30.0)
+    return water_cluster(n, seed=seed, epw_psi_ry=40.0)
+
+
 # ----------------------------------------------------------------------------
 # arrays for the engine
 # ----------------------------------------------------------------------------

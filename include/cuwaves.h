@@ -155,7 +155,8 @@ int cuwaves_etot(cuw_handle* h, double* out, double* force);
  * program: PAW_DRIVER's time loop, src/paw_driver.f90:280-561).  A request
  * carries the complete input of one wave-function set, with the meanings and
  * layouts of cuwaves_set_gset, _set_potential, _set_dh, _set_do, _set_occ,
- * _set_dynamics and _upload_psi; the server copies every array at submission.
+ * _set_dynamics and _upload_psi; the server copies every array at submission
+ * unless the request is flagged CUW_REQ_BORROW.
  * nsteps = 0 asks for a single point (cuwaves_etot after Gram-Schmidt of psi at
  * r0); nsteps > 0 for that many cuwaves_cp_step calls starting from rest
  * (PSIM = PSI0), with the nuclei moving when mass (NAT) is given.  Requests are
@@ -188,7 +189,11 @@ typedef struct cuw_request {
   double delt, annee;
   int nsteps;
   const double* mass;  /* (NAT) electron masses, or NULL: fixed nuclei */
+  int flags;           /* CUW_REQ_* */
 } cuw_request;
+/* The server reads the request's arrays in place instead of copying them at
+ * submission; the caller keeps them unchanged until the request has finished. */
+#define CUW_REQ_BORROW 1
 
 int cuwaves_server_create(size_t hbm_budget, int nworkers, cuw_server** out);
 /* CUW_ERR_NOMEM when the request alone exceeds the budget. */

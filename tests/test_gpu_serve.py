@@ -126,3 +126,21 @@ def test_estimate_bounds_the_allocation(inputs):
     free1 = torch.cuda.mem_get_info()[0]
     w.close()
     assert free0 - free1 <= est, (free0 - free1, est)
+
+
+def test_handles_of_different_grids_interleave():
+    """Kernel launch limits are per function and shared by every handle: a set
+    created after a larger one must not break the larger one's next step."""
+    big = systems.build_inputs(systems.molecule_box("H2O", box=20.0))         # 56^3 grid
+    small = systems.build_inputs(systems.si_small(2))                        # 28^3 grid
+    tall = systems.build_inputs(systems.si_small(12))                        # 28 x 28 x 56
+    for prec in (CUW_PREC_FP64, CUW_PREC_MIXED):
+        a = cuwaves.open_waves(big, precision=prec).setup().initialize()
+        a.cp_step(move_atoms=True)
+        b = cuwaves.open_waves(small, precision=prec).setup().initialize()
+        c = cuwaves.open_waves(tall, precision=prec).setup().initialize()
+        for _ in range(2):
+            for w in (a, b, c):
+                w.cp_step(move_atoms=True)
+        for w in (a, b, c):
+            w.close()
