@@ -362,7 +362,7 @@ static void free_all(Handle* h) {
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
                   g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
-                  g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox};
+                  g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   h->g = Device();

@@ -91,6 +91,8 @@ struct Device {
   double *force = nullptr;       // (3, NAT)
   double *mass = nullptr;        // (NAT)
   double2 *eigr = nullptr;       // (NGL, NAT) structure factors of the last position set
+  float2 *pf = nullptr;          // (LDG, NPRO) mixed path: PRO(g,p) of the last position set in fp32, 0 for g >= NGL
+  double2 *xminus[2] = {nullptr, nullptr};  // (LDG, NBH) mixed path: X(-G) copies of wave-function arrays
   double2 *dh = nullptr;         // (LMNXX, LMNXX, NAT)
   double *dover = nullptr;       // (LNXX, LNXX, NSP)
   double *occ = nullptr;         // (NB)
@@ -261,6 +263,7 @@ cudaError_t smem_allow(const void* fn, int bytes);
 // split-precision (tf32 x3) tensor-core versions, used when precision is
 // CUW_PREC_MIXED; same arguments and results as the FP64 functions above
 int tc_setup(Handle* h);
+int tc_pro_table(Handle* h);  // h->g.pf from h->g.eigr (mixed path)
 int tc_proj(Handle* h, const double2* psi, double2* proj);
 int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const StepCoef& sc);
 int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,

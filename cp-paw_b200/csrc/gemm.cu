@@ -642,7 +642,7 @@ int eigr_compute(Handle* h, const double* r_dev) {
   dim3 grid(std::min(ceil_div(h->d.ngl, 256), 64), h->d.nat);
   k_eigr<<<grid, 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz, r_dev, h->d.ngl, h->d.nat, h->g.eigr);
   CUW_LAUNCH_CHECK("k_eigr");
-  return CUW_OK;
+  return h->mixed() ? tc_pro_table(h) : CUW_OK;
 }
 
 // projA = Omega <p|psiA>, projB likewise when psiB != null; uses h->g.eigr

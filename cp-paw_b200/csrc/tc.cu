@@ -1,16 +1,20 @@
 // Mixed-precision contractions on the 5th-generation tensor cores (tcgen05).
 //
-// Every product is a real GEMM C = A * B^T whose FP64 operands are split on the
-// fly into tf32 pairs (hi + lo) and multiplied as hi*hi + hi*lo + lo*hi with
-// fp32 accumulation in tensor memory (three-term split precision), drained
-// after every K = 8 step into register sums (tc_pipe.cuh).  Complex products
-// use the real form of tc_pipe.cuh.  Every wait is bounded; a wait that runs
-// out sets an error flag and the kernel leaves through its cleanup path (TMEM
-// released) instead of hanging.
+// Every product is a real GEMM C = A * B^T whose operands are split into tf32
+// pairs (hi + lo) and multiplied as lo*hi + hi*lo + hi*hi with fp32
+// accumulation in tensor memory (three-term split precision), drained after
+// every K = 8 step into register sums (tc_pipe.cuh).  Complex products use the
+// real form of tc_pipe.cuh.  Operand data is staged raw (FP64 wave functions
+// and matrices, the fp32 projector table) with cp.async several chunks ahead,
+// then split in shared memory by the converter warps.  Every wait is bounded;
+// a wait that runs out sets an error flag and the kernel leaves through its
+// cleanup path (TMEM released) instead of hanging.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
+#include <string>
 
 #include "cuwaves_internal.cuh"
 #include "tc_pipe.cuh"
@@ -18,61 +22,110 @@
 namespace cuw {
 namespace {
 
-// Real K values per shared-memory stage (four MMA steps of K = 8).  The
-// accumulation run stays one MMA step: the tensor core's truncating fp32
+// Real K values per chunk: 16 (two MMA steps of K = 8), i.e. eight complex K.
+// The accumulation run stays one MMA step: the tensor core's truncating fp32
 // accumulation was measured on B200 at a signed mean error of -3.7e-8 /
 // -8.7e-8 / -1.8e-7 of |C| for runs of 8 / 16 / 32 real K, and one step keeps
 // the energy bias below 1e-6 Ha/atom.
-// Eight producer warps (two per SM sub-partition): the producers' dependent
-// table and coefficient loads need more than one warp per scheduler in flight.
-constexpr int kBK = 32, kCK = kBK / 2, kStages = 3, kNPW = 8;
-using MPipe = tc::Pipe<kBK, kStages, kNPW>;
-constexpr int kProd = MPipe::kProducers;
-// k_tc_force reuses the stage buffers for a 128 x 64 FP64 tile
-static_assert(sizeof(float) * kStages * MPipe::kStage >= sizeof(double) * 128 * 64, "stage area too small");
+constexpr int kCK = 8, kNSplit = 2;
 
+// Raw slot layouts (bytes).  TMA boxes land row-major; boxes whose rows are
+// read down a column by the converters use the 64- or 128-byte swizzle, so
+// that eight consecutive rows hit distinct banks.
+constexpr int kRawProj = 16384;   // Pf 128 p x 8 g (64-byte rows, 64B swizzle) + psi 64 b x 8 g (128B swizzle)
+constexpr int kRawAddpro = 16384; // Pf 8 p x 128 g (1 KB rows) + C1, C2 8 p x 32 b (512-byte rows)
+constexpr int kRawGram = 24576;   // X, X(-k), Y: 64 rows of 8 k (128B swizzle), or 8 rows of 64 (1 KB)
+constexpr int kRawAddx = 49152;   // X, second-half X: 8 k x 128 m (2 KB rows) or 128 m x 8 k (128B swizzle); L1, L2
+constexpr int kRawForce = 24576;  // psi0 8 b x 128 g (2 KB rows) + E 64 p x 8 b (128B swizzle)
+constexpr int kRawGemm = 36864;   // A, B 128 rows x 16 doubles (144-byte rows, element copies)
+using ProjPipe = tc::Pipe<kNSplit, 8, kRawProj>;
+using AddproPipe = tc::Pipe<kNSplit, 8, kRawAddpro>;
+using GramPipe = tc::Pipe<kNSplit, 6, kRawGram>;
+using AddxPipe = tc::Pipe<kNSplit, 3, kRawAddx>;
+using ForcePipe = tc::Pipe<kNSplit, 6, kRawForce>;
+using GemmPipe = tc::Pipe<kNSplit, 3, kRawGemm>;
+constexpr int kThreads = ProjPipe::kThreads;
+constexpr int kConv = ProjPipe::kConv;
+constexpr int kNC = ProjPipe::kCols / 2;  // complex output columns per drain thread
+static_assert(ProjPipe::kSmem <= 232448 && GramPipe::kSmem <= 232448 && AddxPipe::kSmem <= 232448 &&
+                  GemmPipe::kSmem <= 232448 && ForcePipe::kSmem <= 232448,
+              "shared memory");
+// k_tc_force reuses the stage and raw buffers for a 128 x 64 FP64 tile
+static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * 128 * 64, "stage area too small");
+
+// offset of 16-byte chunk e of row r in a box with 128-byte (64-byte) rows
+// under the TMA 128-byte (64-byte) swizzle: chunk bits 4-6 (4-5) of the
+// address are XORed with bits 7-9 (7-8)
+__device__ __forceinline__ int sw128(int r, int e) { return r * 128 + ((e ^ (r & 7)) << 4); }
+__device__ __forceinline__ int sw64(int r, int e) { return r * 64 + ((e ^ ((r >> 1) & 3)) << 4); }
+
+template <class T>
+__device__ __forceinline__ T at(const unsigned char* raw, int byte) {
+  return *reinterpret_cast<const T*>(raw + byte);
+}
 __device__ __forceinline__ double2 dz() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double2 cj(double2 a) { return make_double2(a.x, -a.y); }
 
-// Producer items per thread and stage: 128 A rows and 64 complex B columns,
-// each item covering two complex K values.  Every producer first issues all
-// global loads of its items (held in registers), then converts and stores: the
-// shared-memory stores would otherwise keep later loads from being hoisted.
-constexpr int kItemsA = 128 * (kCK / 2) / kProd;
-constexpr int kItemsB = 64 * (kCK / 2) / kProd;
-static_assert(128 * (kCK / 2) % kProd == 0 && 64 * (kCK / 2) % kProd == 0, "items must divide evenly");
+// The real-form B rows 2j (R even) / 2j+1 (R odd) of two complex values c0, c1
+// (complex K pair hp): four real K values split into the hi/lo tiles
+__device__ __forceinline__ void put_b_pair(float* bhi, float* blo, int R, int hp, double2 c0, double2 c1) {
+  if ((R & 1) == 0) tc::store_split4(bhi, blo, tc::tile_f4(R, hp), c0.x, -c0.y, c1.x, -c1.y);
+  else tc::store_split4(bhi, blo, tc::tile_f4(R, hp), c0.y, c0.x, c1.y, c1.x);
+}
+// complex value i of an A row as real K values 2i, 2i+1 (conj: -Im)
+template <bool CONJ, class C2>
+__device__ __forceinline__ void a_put(float (&v)[8], int i, C2 a) {
+  v[2 * i] = (float)a.x;
+  v[2 * i + 1] = CONJ ? -(float)a.y : (float)a.y;
+}
 
 // ---------------------------------------------------------------------------
 // Plain real GEMM C(M,N) = A(M,K) * B(N,K)^T, FP64 in and out, row-major with
 // K contiguous: the reference product of the split-precision machinery.
 // One CTA computes a 128 x 128 tile over the whole K range.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(MPipe::kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     k_tf32x3_gemm(int M, int N, int K, const double* __restrict__ A, const double* __restrict__ B,
                   double* __restrict__ C, int* __restrict__ err) {
   const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 128;
-  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
-    const int k0 = c * kBK;
-    for (int it = t; it < 128 * (kBK / 4); it += kProd) {
-      const int r = it % 128, g = it / 128, k = k0 + 4 * g;
-      double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (m0 + r < M && k + q < K) a[q] = A[(size_t)(m0 + r) * K + k + q];
-        if (n0 + r < N && k + q < K) b[q] = B[(size_t)(n0 + r) * K + k + q];
-      }
-      tc::store_split4(ahi, alo, tc::tile_f4(r, g), a[0], a[1], a[2], a[3]);
-      tc::store_split4(bhi, blo, tc::tile_f4(r, g), b[0], b[1], b[2], b[3]);
+  constexpr int RS = 144;  // raw row stride (16 doubles + 16 bytes)
+  auto load = [&](int c, int lane, tc::Copier& cp) {
+    const int k0 = c * 16;
+    for (int it = lane; it < 2 * 128 * 16; it += 32) {
+      const int op = it / (128 * 16), r = (it / 16) % 128, kk = it % 16;
+      const int row = (op == 0 ? m0 : n0) + r, lim = op == 0 ? M : N;
+      if (row < lim && k0 + kk < K) cp.el8(op * 128 * RS + r * RS + kk * 8, (op == 0 ? A : B) + (size_t)row * K + k0 + kk);
     }
   };
-  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+  auto a_row = [&](int c, const unsigned char* raw, int row, int kh, float (&v)[8]) {
+    const bool rok = m0 + row < M;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int k = c * 16 + 8 * kh + i;
+      v[i] = (rok && k < K) ? (float)at<double>(raw, row * RS + (8 * kh + i) * 8) : 0.f;
+    }
+  };
+  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {
+    for (int it = ct; it < 128 * 4; it += kConv) {
+      const int r = it % 128, g = it / 128;
+      double x[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = c * 16 + 4 * g + i;
+        x[i] = (n0 + r < N && k < K) ? at<double>(raw, 128 * RS + r * RS + (4 * g + i) * 8) : 0.0;
+      }
+      tc::store_split4(bhi, blo, tc::tile_f4(r, g), x[0], x[1], x[2], x[3]);
+    }
+  };
+  auto finish = [&](const float (&acc)[GemmPipe::kCols], int row, int col0) {
     if (m0 + row >= M) return;
     double* out = C + (size_t)(m0 + row) * N + n0 + col0;
-    const int nc = min(MPipe::kCols, N - n0 - col0);
+    const int nc = min(GemmPipe::kCols, N - n0 - col0);
 #pragma unroll
-    for (int j = 0; j < MPipe::kCols; ++j)
+    for (int j = 0; j < GemmPipe::kCols; ++j)
       if (j < nc) out[j] = (double)acc[j];
   };
-  tc::pipe_run<kBK, kStages, kNPW>((K + kBK - 1) / kBK, produce, finish, err);
+  tc::pipe_run<kNSplit, 3, kRawGemm>((K + 15) / 16, load, a_row, convert_b, finish, err);
 }
 
 // out[i] = scale * sum_z part[z*n + i], summed in FP64 in a fixed order
@@ -89,61 +142,68 @@ __global__ void k_tc_reduce(const float2* __restrict__ part, int nz, size_t n, d
   }
 }
 
+// Projector table of the mixed path: pf[p*ldg + g] = fp32(PRO(g,p)) with
+// PRO(g,p) = Y_lm(g) P_ln(|g|) (-i)^l EIGR(g,a) (WAVES_EXPANDPRO,
+// src/paw_waves1.f90:6070-6109) evaluated in FP64, zero for g >= NGL.  The
+// single rounding to fp32 is the one the split into tf32 pairs starts from.
+__global__ void k_pro_f32(int ngl, int ldg, const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+                          const double* __restrict__ pro, const double2* __restrict__ eigr, float2* __restrict__ pf) {
+  const int p = blockIdx.y;
+  const ProDesc d = pdesc[p];
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ldg; g += gridDim.x * blockDim.x) {
+    float2 v = make_float2(0.f, 0.f);
+    if (g < ngl) {
+      const double2 x = pro_value(g, ngl, d, ylm, pro, eigr);
+      v = make_float2((float)x.x, (float)x.y);
+    }
+    pf[(size_t)p * ldg + g] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // <p|psi> partial sums (WAVES_PROJECTIONS, src/paw_waves1.f90:5746-5905):
 // part[z][p][b] = sum_{g in split z} conj(PRO(g,p)) psi(g,b)   (float2)
-// M = projectors (blockIdx.x), N = 64 bands (blockIdx.y), K = g (blockIdx.z)
+// M = 128 projectors (blockIdx.x), N = 64 bands (blockIdx.y), K = g (blockIdx.z)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(MPipe::kThreads, 1)
-    k_tc_proj(const double2* __restrict__ psi, int ldg, int ngl, int nbh, int npro, int kchunk,
-              const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm, const double* __restrict__ pro,
-              const double2* __restrict__ eigr, float2* __restrict__ part, int* __restrict__ err) {
-  __shared__ ProDesc sd[128];
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_proj(const __grid_constant__ CUtensorMap tm_pf, const __grid_constant__ CUtensorMap tm_psi, int ngl, int nbh,
+              int npro, int kchunk, float2* __restrict__ part, int* __restrict__ err) {
   const int m0 = blockIdx.x * 128, b0 = blockIdx.y * 64;
   const int gbeg = blockIdx.z * kchunk, gend = min(ngl, gbeg + kchunk);
-  for (int t = threadIdx.x; t < 128; t += blockDim.x) sd[t] = m0 + t < npro ? pdesc[m0 + t] : ProDesc{0, 0, 0, -1};
-  __syncthreads();
-  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
-    const int g0 = gbeg + c * kCK;
-    double2 av[kItemsA][2], bv[kItemsB][2];
-    // eight consecutive lanes cover the stage's 16 g of one row: the table and
-    // coefficient reads are contiguous in g
-    constexpr int NG = kCK / 2;
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd, r = it / NG, g = g0 + 2 * (it % NG);
-      const ProDesc d = sd[r];
-      av[q][0] = (d.l >= 0 && g < gend) ? pro_value(g, ngl, d, ylm, pro, eigr) : dz();
-      av[q][1] = (d.l >= 0 && g + 1 < gend) ? pro_value(g + 1, ngl, d, ylm, pro, eigr) : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd, b = b0 + it / NG, g = g0 + 2 * (it % NG);
-      bv[q][0] = (b < nbh && g < gend) ? psi[(size_t)g + (size_t)ldg * b] : dz();
-      bv[q][1] = (b < nbh && g + 1 < gend) ? psi[(size_t)g + 1 + (size_t)ldg * b] : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd;
-      tc::put_a(ahi, alo, it / NG, it % NG, cconj(av[q][0]), cconj(av[q][1]));
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd;
-      tc::put_b(bhi, blo, it / NG, it % NG, bv[q][0], bv[q][1]);
+  // raw slot: [0, 8K) Pf box 128 p x 8 g (64-byte rows, 64B swizzle);
+  // [8K, 16K) psi box 64 b x 8 g (128-byte rows, 128B swizzle).  Chunks never
+  // straddle a split boundary (kchunk is a multiple of 8) and read zeros past NGL.
+  auto load = [&](int c, int lane, tc::Copier& cp) {
+    if (lane == 0) {
+      const int g0 = gbeg + c * kCK;
+      cp.tensor(0, &tm_pf, 2 * g0, m0, 8192);
+      cp.tensor(8192, &tm_psi, 2 * g0, b0, 8192);
     }
   };
-  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+  auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // conj(Pf) row p
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float4 x = at<float4>(raw, sw64(r, 2 * kh + i));
+      v[4 * i] = x.x, v[4 * i + 1] = -x.y, v[4 * i + 2] = x.z, v[4 * i + 3] = -x.w;
+    }
+  };
+  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // psi, real form
+    for (int it = ct; it < 512; it += kConv) {
+      const int R = it & 127, hp = it >> 7, j = R >> 1;
+      put_b_pair(bhi, blo, R, hp, at<double2>(raw, 8192 + sw128(j, 2 * hp)), at<double2>(raw, 8192 + sw128(j, 2 * hp + 1)));
+    }
+  };
+  auto finish = [&](const float (&acc)[ProjPipe::kCols], int row, int col0) {
     const int p = m0 + row;
     if (p >= npro) return;
     float2* out = part + ((size_t)blockIdx.z * npro + p) * nbh;
     const int bb = b0 + col0 / 2;
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
+    for (int j = 0; j < kNC; ++j)
       if (bb + j < nbh) out[bb + j] = make_float2(acc[2 * j], acc[2 * j + 1]);
   };
   const int nchunk = gend > gbeg ? (gend - gbeg + kCK - 1) / kCK : 0;
-  tc::pipe_run<kBK, kStages, kNPW>(nchunk, produce, finish, err);
+  tc::pipe_run<kNSplit, 8, kRawProj>(nchunk, load, a_row, convert_b, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -152,54 +212,50 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
 // columns hold C1 (hproj) products for the bands, then C2 (oproj) products.
 // ---------------------------------------------------------------------------
 template <int MODE>
-__global__ void __launch_bounds__(MPipe::kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     k_tc_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi, const double2* __restrict__ psi0,
                 double2* __restrict__ psim, const double* __restrict__ mpsi, int ldg, int ngl, int nbh, int npro,
-                const double2* __restrict__ c1, const double2* __restrict__ c2, const ProDesc* __restrict__ pdesc,
-                const double* __restrict__ ylm, const double* __restrict__ pro, const double2* __restrict__ eigr,
-                StepCoef sc, int* __restrict__ err) {
+                const __grid_constant__ CUtensorMap tm_pf, const __grid_constant__ CUtensorMap tm_c1,
+                const __grid_constant__ CUtensorMap tm_c2, StepCoef sc, int* __restrict__ err) {
   constexpr bool USE_H = (MODE != ADDPRO_OPSI);
   constexpr bool USE_O = (MODE != ADDPRO_HPSI);
   const int g0 = blockIdx.x * 128, b0 = blockIdx.y * 32;
-  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
-    const int p0 = c * kCK;
-    double2 av[kItemsA][2], bv[kItemsB][2];
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd, g = g0 + it % 128, p = p0 + 2 * (it / 128);
-      av[q][0] = (g < ngl && p < npro) ? pro_value(g, ngl, pdesc[p], ylm, pro, eigr) : dz();
-      av[q][1] = (g < ngl && p + 1 < npro) ? pro_value(g, ngl, pdesc[p + 1], ylm, pro, eigr) : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd, j = it % 64, mt = j / 32, b = b0 + (j % 32), p = p0 + 2 * (it / 64);
-      const double2* cm = mt == 0 ? c1 : c2;
-      const bool use = (mt == 0 ? USE_H : USE_O) && b < nbh;
-      bv[q][0] = (use && p < npro) ? cm[(size_t)b + (size_t)nbh * p] : dz();
-      bv[q][1] = (use && p + 1 < npro) ? cm[(size_t)b + (size_t)nbh * (p + 1)] : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd;
-      tc::put_a(ahi, alo, it % 128, it / 128, av[q][0], av[q][1]);
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd;
-      tc::put_b(bhi, blo, it % 64, it / 64, bv[q][0], bv[q][1]);
+  // raw slot: [0, 8K) Pf box 8 p x 128 g (1 KB rows); [8K, 12K) C1 box and
+  // [12K, 16K) C2 box, 8 p x 32 b (512-byte rows); zeros past NGL, NPRO, NBH
+  auto load = [&](int c, int lane, tc::Copier& cp) {
+    if (lane == 0) {
+      const int p0 = c * kCK;
+      cp.tensor(0, &tm_pf, 2 * g0, p0, 8192);
+      if (USE_H) cp.tensor(8192, &tm_c1, 2 * b0, p0, 4096);
+      if (USE_O) cp.tensor(12288, &tm_c2, 2 * b0, p0, 4096);
     }
   };
-  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+  auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // Pf(g, p), K = p
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a_put<false>(v, i, at<float2>(raw, (4 * kh + i) * 1024 + r * 8));
+  };
+  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // [C1 | C2], real form
+    for (int it = ct; it < 512; it += kConv) {
+      const int R = it & 127, hp = it >> 7, j = R >> 1, mt = j >> 5, bl = j & 31;
+      const bool ok = mt == 0 ? USE_H : USE_O;  // a box left out holds stale data
+      const int o = 8192 + mt * 4096 + bl * 16;
+      put_b_pair(bhi, blo, R, hp, ok ? at<double2>(raw, o + (2 * hp) * 512) : dz(),
+                 ok ? at<double2>(raw, o + (2 * hp + 1) * 512) : dz());
+    }
+  };
+  auto finish = [&](const float (&acc)[AddproPipe::kCols], int row, int col0) {
     const int g = g0 + row;
     if (g >= ngl) return;
     const double rm = 1.0 / mpsi[g];
+    const bool hcol = col0 < 64;  // columns 0..63: C1 (H) products, 64..127: C2 (O)
+    const int bl0 = (col0 & 63) / 2;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const int b = b0 + j;
+    for (int j = 0; j < kNC; ++j) {
+      const int b = b0 + bl0 + j;
       if (b >= nbh) continue;
       const size_t k = (size_t)g + (size_t)ldg * b;
       const double2 v = make_double2((double)acc[2 * j], (double)acc[2 * j + 1]);
-      if (col0 == 0 && USE_H) {
+      if (hcol && USE_H) {
         const double2 hv = cadd(hpsi[k], v);
         hpsi[k] = hv;
         if (MODE == ADDPRO_FUSED) {
@@ -207,14 +263,14 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
           const double a3 = sc.a3 * rm;
           psim[k] = make_double2(sc.a1 * p0v.x + sc.a2 * pm.x + a3 * hv.x, sc.a1 * p0v.y + sc.a2 * pm.y + a3 * hv.y);
         }
-      } else if (col0 != 0 && USE_O) {
+      } else if (!hcol && USE_O) {
         const double2 p0v = psi0[k];
         const double s = sc.oscale * rm;
         opsi[k] = make_double2((p0v.x + v.x) * s, (p0v.y + v.y) * s);
       }
     }
   };
-  tc::pipe_run<kBK, kStages, kNPW>((npro + kCK - 1) / kCK, produce, finish, err);
+  tc::pipe_run<kNSplit, 8, kRawAddpro>((npro + kCK - 1) / kCK, load, a_row, convert_b, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -227,76 +283,68 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
 // Y columns.  Partials part[z][t][m + nm n] (float2), z = split*npair + pair.
 // ---------------------------------------------------------------------------
 struct TcGramArgs {
-  GramPair pair[3];
-  int npair, nk, nm;
-  size_t sk, sm;
-  int kchunk;
+  int npair, nk, nm, kchunk;
+  bool kfast;  // X(k, m) contiguous in k (plane waves); else in m (projections)
+};
+// TMA maps of the pairs: X, X(-k) (plane waves with MINUS) and Y
+struct TcGramMaps {
+  CUtensorMap x[3], xm[3], y[3];
 };
 
 template <bool MINUS>
-__global__ void __launch_bounds__(MPipe::kThreads, 1)
-    k_tc_gram(TcGramArgs a, const int* __restrict__ minusg, float2* __restrict__ part, int* __restrict__ err) {
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_gram(TcGramArgs a, const __grid_constant__ TcGramMaps tm, float2* __restrict__ part, int* __restrict__ err) {
   const int pair = blockIdx.z % a.npair, split = blockIdx.z / a.npair;
   const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-  const double2* X = a.pair[pair].x;
-  const double2* Y = a.pair[pair].y;
   const int kbeg = split * a.kchunk, kend = min(a.nk, kbeg + a.kchunk);
-  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
-    const int k0 = kbeg + c * kCK;
-    // lanes run along the contiguous index: k when sk == 1 (plane waves), the
-    // band otherwise (projections)
-    constexpr int NK = kCK / 2;
-    const bool kfast = a.sk == 1;
-    double2 av[kItemsA][2], bv[kItemsB][2];
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd;
-      const int r = kfast ? it / NK : it % 128, ki = kfast ? it % NK : it / 128;
-      const int k = k0 + 2 * ki, m = m0 + (r & 63);
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        av[q][e] = dz();
-        if (m < a.nm && k + e < kend) {
-          if (r < 64) {
-            av[q][e] = cconj(X[(size_t)(k + e) * a.sk + (size_t)m * a.sm]);
-          } else {
-            const int kk = MINUS ? minusg[k + e] : k + e;
-            av[q][e] = X[(size_t)kk * a.sk + (size_t)m * a.sm];
-          }
-        }
+  const bool kfast = a.kfast;
+  // raw slot: X at 0, X(-k) at 8K (MINUS), Y at 16K.  kfast: boxes of 64
+  // rows (m or n) of eight k (128-byte rows, 128B swizzle); otherwise 8 rows
+  // (k) of 64 m or n (1 KB rows).  Zeros past NK and NM.
+  constexpr int XM = 8192, YO = 16384;
+  auto load = [&](int c, int lane, tc::Copier& cp) {
+    if (lane == 0) {
+      const int k0 = kbeg + c * kCK;
+      if (kfast) {
+        cp.tensor(0, &tm.x[pair], 2 * k0, m0, 8192);
+        if (MINUS) cp.tensor(XM, &tm.xm[pair], 2 * k0, m0, 8192);
+        cp.tensor(YO, &tm.y[pair], 2 * k0, n0, 8192);
+      } else {
+        cp.tensor(0, &tm.x[pair], 2 * m0, k0, 8192);
+        cp.tensor(YO, &tm.y[pair], 2 * n0, k0, 8192);
       }
     }
+  };
+  auto xoff = [&](int r, int e) { return kfast ? sw128(r, e) : e * 1024 + r * 16; };
+  auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {
+    // rows 0..63 conj X(k), rows 64..127 X(-k) (MINUS) or X(k)
+    const int ml = r & 63;
+    const int base = (MINUS && r >= 64) ? XM : 0;
 #pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd;
-      const int j = kfast ? it / NK : it % 64, ki = kfast ? it % NK : it / 64;
-      const int n = n0 + j, k = k0 + 2 * ki;
-      bv[q][0] = (n < a.nm && k < kend) ? Y[(size_t)k * a.sk + (size_t)n * a.sm] : dz();
-      bv[q][1] = (n < a.nm && k + 1 < kend) ? Y[(size_t)(k + 1) * a.sk + (size_t)n * a.sm] : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd;
-      tc::put_a(ahi, alo, kfast ? it / NK : it % 128, kfast ? it % NK : it / 128, av[q][0], av[q][1]);
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd;
-      tc::put_b(bhi, blo, kfast ? it / NK : it % 64, kfast ? it % NK : it / 64, bv[q][0], bv[q][1]);
+    for (int i = 0; i < 4; ++i) {
+      const double2 x = at<double2>(raw, base + xoff(ml, 4 * kh + i));
+      if (r < 64) a_put<true>(v, i, x);
+      else a_put<false>(v, i, x);
     }
   };
-  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // Y, real form
+    for (int it = ct; it < 512; it += kConv) {
+      const int R = it & 127, hp = it >> 7, j = R >> 1;
+      put_b_pair(bhi, blo, R, hp, at<double2>(raw, YO + xoff(j, 2 * hp)), at<double2>(raw, YO + xoff(j, 2 * hp + 1)));
+    }
+  };
+  auto finish = [&](const float (&acc)[GramPipe::kCols], int row, int col0) {
     const int t = row >> 6, m = m0 + (row & 63);
     if (m >= a.nm) return;
     const size_t mn = (size_t)a.nm * a.nm;
     float2* out = part + ((size_t)blockIdx.z * 2 + t) * mn;
     const int nb = n0 + col0 / 2;
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
+    for (int j = 0; j < kNC; ++j)
       if (nb + j < a.nm) out[(size_t)m + (size_t)a.nm * (nb + j)] = make_float2(acc[2 * j], acc[2 * j + 1]);
   };
   const int nchunk = kend > kbeg ? (kend - kbeg + kCK - 1) / kCK : 0;
-  tc::pipe_run<kBK, kStages, kNPW>(nchunk, produce, finish, err);
+  tc::pipe_run<kNSplit, 6, kRawGram>(nchunk, load, a_row, convert_b, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -306,73 +354,78 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
 // ---------------------------------------------------------------------------
 struct TcAddXArgs {
   double2* out;
-  const double2* x;
-  const double2* l1;
-  const double2* l2;
   int nm, nn, nk;
-  size_t sxm, sxk, som, son;
+  size_t som, son;
+  bool mfast;  // X(m, k) contiguous in m (plane waves); else in k (projections)
+};
+// TMA maps: X for K < NK, the second-half X (conj X(m') for K >= NK), L1, L2
+struct TcAddXMaps {
+  CUtensorMap x, x2, l1, l2;
 };
 
-template <bool XMINUS>
-__global__ void __launch_bounds__(MPipe::kThreads, 1)
-    k_tc_addx(TcAddXArgs a, const int* __restrict__ minusg, int* __restrict__ err) {
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_addx(TcAddXArgs a, const __grid_constant__ TcAddXMaps tm, int* __restrict__ err) {
   const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 64;
   const int ktot = 2 * a.nk;
-  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
-    const int kg0 = c * kCK;
-    double2 av[kItemsA][2], bv[kItemsB][2];
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd, m = m0 + it % 128;
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int kg = kg0 + 2 * (it / 128) + e;
-        av[q][e] = dz();
-        if (m < a.nm && kg < ktot) {
-          if (kg < a.nk) {
-            av[q][e] = a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
-          } else {
-            const int mm = XMINUS ? minusg[m] : m;
-            av[q][e] = cconj(a.x[(size_t)mm * a.sxm + (size_t)(kg - a.nk) * a.sxk]);
-          }
-        }
+  const bool mfast = a.mfast;
+  // raw slot: X at 0 and the second-half X at 16K: mfast boxes of 8 rows (k)
+  // of 128 m (2 KB rows), else 128 rows (m) of eight k (128B swizzle); L1 at
+  // 32K, L2 at 40K: 64 rows (n) of eight k (128B swizzle).  Second-half boxes
+  // start at k = kg0 - NK, negative for a chunk that straddles NK: rows or
+  // columns outside the arrays read as zero.
+  constexpr int X2 = 16384, L1O = 32768, L2O = 40960;
+  auto load = [&](int c, int lane, tc::Copier& cp) {
+    if (lane == 0) {
+      const int kg0 = c * kCK, k2 = kg0 - a.nk;
+      if (kg0 < a.nk) {
+        if (mfast) cp.tensor(0, &tm.x, 2 * m0, kg0, 16384);
+        else cp.tensor(0, &tm.x, 2 * kg0, m0, 16384);
+        cp.tensor(L1O, &tm.l1, 2 * kg0, n0, 8192);
       }
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd, n = n0 + it % 64;
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int kg = kg0 + 2 * (it / 64) + e;
-        bv[q][e] = dz();
-        if (n < a.nn && kg < ktot)
-          bv[q][e] = kg < a.nk ? a.l1[(size_t)kg + (size_t)a.nk * n] : a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
+      if (kg0 + kCK > a.nk) {
+        if (mfast) cp.tensor(X2, &tm.x2, 2 * m0, k2, 16384);
+        else cp.tensor(X2, &tm.x2, 2 * k2, m0, 16384);
+        cp.tensor(L2O, &tm.l2, 2 * k2, n0, 8192);
       }
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd;
-      tc::put_a(ahi, alo, it % 128, it / 128, av[q][0], av[q][1]);
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd;
-      tc::put_b(bhi, blo, it % 64, it / 64, bv[q][0], bv[q][1]);
     }
   };
-  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+  auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // X(m,k) | conj X(m',k)
+    const int kg0 = c * kCK + 4 * kh;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int e = 4 * kh + i;
+      const bool first = kg0 + i < a.nk;
+      const double2 x = (kg0 + i < ktot) ? at<double2>(raw, (first ? 0 : X2) + (mfast ? e * 2048 + r * 16 : sw128(r, e))) : dz();
+      if (first) a_put<false>(v, i, x);
+      else a_put<true>(v, i, x);
+    }
+  };
+  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // [L1; L2], real form
+    const int kg0 = c * kCK;
+    for (int it = ct; it < 512; it += kConv) {
+      const int R = it & 127, hp = it >> 7, j = R >> 1;
+      double2 cv[2];
+#pragma unroll
+      for (int e2 = 0; e2 < 2; ++e2) {
+        const int e = 2 * hp + e2, kg = kg0 + e;
+        cv[e2] = kg < ktot ? at<double2>(raw, (kg < a.nk ? L1O : L2O) + sw128(j, e)) : dz();
+      }
+      put_b_pair(bhi, blo, R, hp, cv[0], cv[1]);
+    }
+  };
+  auto finish = [&](const float (&acc)[AddxPipe::kCols], int row, int col0) {
     const int m = m0 + row;
     if (m >= a.nm) return;
     const int nb = n0 + col0 / 2;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
+    for (int j = 0; j < kNC; ++j) {
       if (nb + j >= a.nn) continue;
       const size_t k = (size_t)m * a.som + (size_t)(nb + j) * a.son;
       const double2 o = a.out[k];
       a.out[k] = make_double2(o.x + (double)acc[2 * j], o.y + (double)acc[2 * j + 1]);
     }
   };
-  tc::pipe_run<kBK, kStages, kNPW>((ktot + kCK - 1) / kCK, produce, finish, err);
+  tc::pipe_run<kNSplit, 3, kRawAddx>((ktot + kCK - 1) / kCK, load, a_row, convert_b, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -382,44 +435,40 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
 // drain warps (into the freed stage buffers) and fpart[tile][p][c] =
 // sum_g sv(g,p) G_c(g) by the whole CTA.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(MPipe::kThreads, 1)
-    k_tc_force(const double2* __restrict__ psi0, int ldg, int ngl, int nbh, int npro,
-               const double2* __restrict__ ded, const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_force(const __grid_constant__ CUtensorMap tm_psi, const __grid_constant__ CUtensorMap tm_e, int ngl, int nbh,
+               int npro, const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
                const double* __restrict__ pro, const double2* __restrict__ eigr, const double* __restrict__ gx,
                const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ fpart,
                int* __restrict__ err) {
   const int g0 = blockIdx.x * 128, p0 = blockIdx.y * 64;
-  auto produce = [&](int c, int t, float* ahi, float* alo, float* bhi, float* blo) {
-    const int bb = c * kCK;
-    double2 av[kItemsA][2], bv[kItemsB][2];
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd, g = g0 + it % 128, b = bb + 2 * (it / 128);
-      av[q][0] = (g < ngl && b < nbh) ? psi0[(size_t)g + (size_t)ldg * b] : dz();
-      av[q][1] = (g < ngl && b + 1 < nbh) ? psi0[(size_t)g + (size_t)ldg * (b + 1)] : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd, p = p0 + it % 64, b = bb + 2 * (it / 64);
-      bv[q][0] = (p < npro && b < nbh) ? cconj(ded[(size_t)b + (size_t)nbh * p]) : dz();
-      bv[q][1] = (p < npro && b + 1 < nbh) ? cconj(ded[(size_t)b + 1 + (size_t)nbh * p]) : dz();
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsA; ++q) {
-      const int it = t + q * kProd;
-      tc::put_a(ahi, alo, it % 128, it / 128, av[q][0], av[q][1]);
-    }
-#pragma unroll
-    for (int q = 0; q < kItemsB; ++q) {
-      const int it = t + q * kProd;
-      tc::put_b(bhi, blo, it % 64, it / 64, bv[q][0], bv[q][1]);
+  // raw slot: [0, 16K) psi0 box 8 b x 128 g (2 KB rows); [16K, 24K) E box
+  // 64 p x 8 b (128B swizzle); zeros past NGL, NBH, NPRO
+  constexpr int EO = 16384;
+  auto load = [&](int c, int lane, tc::Copier& cp) {
+    if (lane == 0) {
+      const int bb = c * kCK;
+      cp.tensor(0, &tm_psi, 2 * g0, bb, 16384);
+      cp.tensor(EO, &tm_e, 2 * bb, p0, 8192);
     }
   };
-  double* sv = reinterpret_cast<double*>(tc::pipe_stage_base());  // [128][64]
-  auto finish = [&](const float (&acc)[MPipe::kCols], int row, int col0) {
+  auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // psi0(g, b), K = b
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a_put<false>(v, i, at<double2>(raw, (4 * kh + i) * 2048 + r * 16));
+  };
+  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // conj(E), real form
+    for (int it = ct; it < 512; it += kConv) {
+      const int R = it & 127, hp = it >> 7, j = R >> 1;
+      put_b_pair(bhi, blo, R, hp, cj(at<double2>(raw, EO + sw128(j, 2 * hp))), cj(at<double2>(raw, EO + sw128(j, 2 * hp + 1))));
+    }
+  };
+  // [128][64], over the stage and raw buffers: when a drain thread finishes,
+  // every chunk has been converted and multiplied and no copy is in flight
+  double* sv = reinterpret_cast<double*>(tc::pipe_stage_base());
+  auto finish = [&](const float (&acc)[ForcePipe::kCols], int row, int col0) {
     const int g = g0 + row, pb = col0 / 2;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
+    for (int j = 0; j < kNC; ++j) {
       const int p = p0 + pb + j;
       double v = 0.0;
       if (g < ngl && p < npro) {
@@ -432,7 +481,7 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
       sv[row * 64 + pb + j] = v;
     }
   };
-  tc::pipe_run<kBK, kStages, kNPW>((nbh + kCK - 1) / kCK, produce, finish, err);
+  tc::pipe_run<kNSplit, 6, kRawForce>((nbh + kCK - 1) / kCK, load, a_row, convert_b, finish, err);
   // pipe_run ended with a CTA barrier: sv is complete (if a wait ran out the
   // error flag is set and the caller discards the result)
   for (int i = threadIdx.x; i < 64 * 3; i += blockDim.x) {
@@ -442,6 +491,16 @@ __global__ void __launch_bounds__(MPipe::kThreads, 1)
     double s = 0.0;
     for (int r = 0; r < 128 && g0 + r < ngl; ++r) s += sv[r * 64 + pl] * gc[g0 + r];
     fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = s;
+  }
+}
+
+// dst(g, b) = src(-g, b) for g < NGL, 0 in the padding (ld = ldg)
+__global__ void k_minus_copy(const double2* __restrict__ src, double2* __restrict__ dst,
+                             const int* __restrict__ minusg, int ngl, int ldg, int nbh) {
+  const size_t n = (size_t)ldg * nbh;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int g = (int)(i % ldg);
+    dst[i] = g < ngl ? src[(size_t)minusg[g] + (i - g)] : dz();
   }
 }
 
@@ -458,17 +517,89 @@ static int tc_splits(Handle* h, int tiles, int nk) {
   return std::max(1, std::min(want, ceil_div(nk, 4 * kCK)));
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the runtime only)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled encode_tiled() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// 2-D map of `rows` rows of `inner` real elements (FP64 or fp32), rows `ld`
+// elements apart, box bx x by; elements outside read as zero
+static int make_map(Handle* h, CUtensorMap* m, const void* base, bool f64, long long inner, long long rows,
+                    long long ld, int bx, int by, CUtensorMapSwizzle sw) {
+  const EncodeTiled fn = encode_tiled();
+  if (!fn) return h->fail(CUW_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const long long es = f64 ? 8 : 4;
+  const cuuint64_t dims[2] = {(cuuint64_t)std::max(1ll, inner), (cuuint64_t)std::max(1ll, rows)};
+  const cuuint64_t strides[1] = {(cuuint64_t)(ld * es)};
+  const cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return h->fail(CUW_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return CUW_OK;
+}
+// complex (ld, cols) array of FP64 pairs: rows = columns of the array
+static int map_c(Handle* h, CUtensorMap* m, const double2* base, long long n, long long cols, long long ld, int bx,
+                 int by, CUtensorMapSwizzle sw) {
+  return make_map(h, m, base, true, 2 * n, cols, 2 * ld, bx, by, sw);
+}
+
 int tc_setup(Handle* h) {
-  const int sm = (int)MPipe::kSmem;
-  CUW_TRY(smem_allow((const void*)k_tc_proj, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_HPSI>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_OPSI>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_FUSED>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_gram<true>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_gram<false>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_addx<true>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_addx<false>, sm));
-  CUW_TRY(smem_allow((const void*)k_tc_force, sm));
+  CUW_TRY(smem_allow((const void*)k_tc_proj, (int)ProjPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_HPSI>, (int)AddproPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_OPSI>, (int)AddproPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_addpro<ADDPRO_FUSED>, (int)AddproPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_gram<true>, (int)GramPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_gram<false>, (int)GramPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_addx, (int)AddxPipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_force, (int)ForcePipe::kSmem));
+  if (!encode_tiled()) return h->fail(CUW_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  auto alloc = [&](void** p, size_t bytes) -> int {
+    if (*p) return CUW_OK;
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      *p = nullptr;
+      return h->fail(CUW_ERR_NOMEM, "cudaMalloc of mixed-path scratch failed");
+    }
+    CUW_TRY(cudaMemsetAsync(*p, 0, bytes, h->stream));
+    return CUW_OK;
+  };
+  CUW_RET(alloc(reinterpret_cast<void**>(&h->g.pf), sizeof(float2) * (size_t)h->ldg * std::max(1, h->npro)));
+  for (int i = 0; i < 2; ++i)
+    CUW_RET(alloc(reinterpret_cast<void**>(&h->g.xminus[i]), sizeof(double2) * (size_t)h->ldg * h->d.nbh));
+  return CUW_OK;
+}
+
+int tc_pro_table(Handle* h) {
+  if (h->npro == 0) return CUW_OK;
+  const dim3 grid(std::min(ceil_div(h->ldg, 256), 64), h->npro);
+  k_pro_f32<<<grid, 256, 0, h->stream>>>(h->d.ngl, h->ldg, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.pf);
+  CUW_LAUNCH_CHECK("k_pro_f32");
+  return CUW_OK;
+}
+
+// X(-G) copy of a wave-function array into scratch slot i
+static int tc_minus(Handle* h, const double2* x, int i, const double2** out) {
+  const size_t n = (size_t)h->ldg * h->d.nbh;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)8 * h->nsm);
+  k_minus_copy<<<blocks, 256, 0, h->stream>>>(x, h->g.xminus[i], h->g.minusg, h->d.ngl, h->ldg, h->d.nbh);
+  CUW_LAUNCH_CHECK("k_minus_copy");
+  *out = h->g.xminus[i];
   return CUW_OK;
 }
 
@@ -488,8 +619,11 @@ int tc_proj(Handle* h, const double2* psi, double2* proj) {
   const size_t n = (size_t)nbh * npro;
   CUW_RET(ensure_part(h, sizeof(float2) * n * ks));
   float2* part = reinterpret_cast<float2*>(h->g.part);
-  k_tc_proj<<<dim3(tn, tb, ks), MPipe::kThreads, MPipe::kSmem, h->stream>>>(
-      psi, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, part, tc_err(h));
+  CUtensorMap tpf, tps;
+  CUW_RET(make_map(h, &tpf, h->g.pf, false, 2ll * ngl, npro, 2ll * h->ldg, 16, 128, CU_TENSOR_MAP_SWIZZLE_64B));
+  CUW_RET(map_c(h, &tps, psi, ngl, nbh, h->ldg, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+  k_tc_proj<<<dim3(tn, tb, ks), kThreads, ProjPipe::kSmem, h->stream>>>(tpf, tps, ngl, nbh, npro, kchunk, part,
+                                                                         tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_proj");
   return tc_reduce(h, part, ks, n, h->gweight, proj);
 }
@@ -498,11 +632,15 @@ int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const
   const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
   const dim3 grid(ceil_div(ngl, 128), ceil_div(nbh, 32));
   Device& g = h->g;
-#define TC_ADDPRO(M)                                                                                         \
-  k_tc_addpro<M><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, \
-                                                                     h->ldg, ngl, nbh, npro, hpc, opc,       \
-                                                                     g.pdesc, g.ylm, g.pro, g.eigr, sc,      \
-                                                                     tc_err(h))
+  CUtensorMap tpf, tc1, tc2;
+  CUW_RET(make_map(h, &tpf, g.pf, false, 2ll * ngl, npro, 2ll * h->ldg, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+  const double2* c1 = hpc ? hpc : opc;
+  const double2* c2 = opc ? opc : hpc;
+  CUW_RET(map_c(h, &tc1, c1, nbh, npro, nbh, 64, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+  CUW_RET(map_c(h, &tc2, c2, nbh, npro, nbh, 64, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+#define TC_ADDPRO(M)                                                                                            \
+  k_tc_addpro<M><<<grid, kThreads, AddproPipe::kSmem, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, \
+                                                                   ngl, nbh, npro, tpf, tc1, tc2, sc, tc_err(h))
   if (mode == ADDPRO_HPSI) TC_ADDPRO(ADDPRO_HPSI);
   else if (mode == ADDPRO_OPSI) TC_ADDPRO(ADDPRO_OPSI);
   else TC_ADDPRO(ADDPRO_FUSED);
@@ -514,12 +652,42 @@ int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const
 int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
             double scale, double2* dst) {
   TcGramArgs a;
-  for (int i = 0; i < npair; ++i) a.pair[i] = pairs[i];
   a.npair = npair;
   a.nk = nk;
   a.nm = nm;
-  a.sk = sk;
-  a.sm = sm;
+  a.kfast = sk == 1;
+  if (!a.kfast && sm != 1) return h->fail(CUW_ERR_UNSUPPORTED, "Gram product with neither index contiguous");
+  if (minus && !a.kfast) return h->fail(CUW_ERR_UNSUPPORTED, "X(-k) Gram product of projections");
+  TcGramMaps tm;
+  // X(-k) copies of the distinct X arrays (at most two: PSIBAR and OPSI)
+  const double2* src[2] = {nullptr, nullptr};
+  const double2* mcopy[2] = {nullptr, nullptr};
+  for (int i = 0; i < npair; ++i) {
+    const double2 *x = pairs[i].x, *y = pairs[i].y;
+    if (a.kfast) {
+      CUW_RET(map_c(h, &tm.x[i], x, nk, nm, (long long)sm, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+      CUW_RET(map_c(h, &tm.y[i], y, nk, nm, (long long)sm, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+    } else {
+      CUW_RET(map_c(h, &tm.x[i], x, nm, nk, (long long)sk, 128, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+      CUW_RET(map_c(h, &tm.y[i], y, nm, nk, (long long)sk, 128, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+    }
+    tm.xm[i] = tm.x[i];
+    if (minus) {
+      if (sm != (size_t)h->ldg || nk != h->d.ngl || nm != h->d.nbh)
+        return h->fail(CUW_ERR_UNSUPPORTED, "X(-k) Gram product of a non wave-function array");
+      int slot = -1;
+      for (int j = 0; j < 2; ++j)
+        if (src[j] == x) slot = j;
+      if (slot < 0) {
+        slot = src[0] ? 1 : 0;
+        if (src[slot]) return h->fail(CUW_ERR_UNSUPPORTED, "more than two X arrays in one Gram call");
+        src[slot] = x;
+        CUW_RET(tc_minus(h, x, slot, &mcopy[slot]));
+      }
+      CUW_RET(map_c(h, &tm.xm[i], mcopy[slot], nk, nm, (long long)sm, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+    }
+  }
+  for (int i = npair; i < 3; ++i) tm.x[i] = tm.xm[i] = tm.y[i] = tm.x[0];
   const int tiles = ceil_div(nm, 64) * ceil_div(nm, 64) * npair;
   int ks = tc_splits(h, tiles, nk);
   a.kchunk = ceil_div(ceil_div(nk, ks), kCK) * kCK;
@@ -528,20 +696,34 @@ int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int
   CUW_RET(ensure_part(h, sizeof(float2) * mn * 2 * npair * ks));
   float2* part = reinterpret_cast<float2*>(h->g.part);
   const dim3 grid(ceil_div(nm, 64), ceil_div(nm, 64), ks * npair);
-  if (minus)
-    k_tc_gram<true><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, part, tc_err(h));
-  else
-    k_tc_gram<false><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, part, tc_err(h));
+  if (minus) k_tc_gram<true><<<grid, kThreads, GramPipe::kSmem, h->stream>>>(a, tm, part, tc_err(h));
+  else k_tc_gram<false><<<grid, kThreads, GramPipe::kSmem, h->stream>>>(a, tm, part, tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_gram");
   return tc_reduce(h, part, ks, mn * 2 * npair, scale, dst);
 }
 
 int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double2* l1, const double2* l2, int nm,
             int nn, int nk, size_t sxm, size_t sxk, size_t som, size_t son) {
-  TcAddXArgs a{out, x, l1, l2, nm, nn, nk, sxm, sxk, som, son};
+  TcAddXArgs a{out, nm, nn, nk, som, son, sxm == 1};
+  TcAddXMaps tm;
+  if (a.mfast) {
+    const double2* x2 = x;
+    if (xminus) {
+      if (sxk != (size_t)h->ldg || nm != h->d.ngl || nk != h->d.nbh)
+        return h->fail(CUW_ERR_UNSUPPORTED, "X(-G) update of a non wave-function array");
+      CUW_RET(tc_minus(h, x, 0, &x2));
+    }
+    CUW_RET(map_c(h, &tm.x, x, nm, nk, (long long)sxk, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+    CUW_RET(map_c(h, &tm.x2, x2, nm, nk, (long long)sxk, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+  } else {
+    if (sxk != 1 || xminus) return h->fail(CUW_ERR_UNSUPPORTED, "projection update with gathered rows");
+    CUW_RET(map_c(h, &tm.x, x, nk, nm, (long long)sxm, 16, 128, CU_TENSOR_MAP_SWIZZLE_128B));
+    tm.x2 = tm.x;
+  }
+  CUW_RET(map_c(h, &tm.l1, l1, nk, nn, nk, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+  CUW_RET(map_c(h, &tm.l2, l2, nk, nn, nk, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
   const dim3 grid(ceil_div(nm, 128), ceil_div(nn, 64));
-  if (xminus) k_tc_addx<true><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, tc_err(h));
-  else k_tc_addx<false><<<grid, MPipe::kThreads, MPipe::kSmem, h->stream>>>(a, h->g.minusg, tc_err(h));
+  k_tc_addx<<<grid, kThreads, AddxPipe::kSmem, h->stream>>>(a, tm, tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_addx");
   return CUW_OK;
 }
@@ -549,9 +731,12 @@ int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double
 int tc_force(Handle* h, const double2* ded, double* fpart, int* ntile) {
   const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
   const int tm = ceil_div(ngl, 128), tn = ceil_div(npro, 64);
-  k_tc_force<<<dim3(tm, tn), MPipe::kThreads, MPipe::kSmem, h->stream>>>(
-      h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy, h->g.gz,
-      fpart, tc_err(h));
+  CUtensorMap tps, te;
+  CUW_RET(map_c(h, &tps, h->g.psi0, ngl, nbh, h->ldg, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+  CUW_RET(map_c(h, &te, ded, nbh, npro, nbh, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+  k_tc_force<<<dim3(tm, tn), kThreads, ForcePipe::kSmem, h->stream>>>(tps, te, ngl, nbh, npro, h->g.pdesc, h->g.ylm,
+                                                                      h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
+                                                                      h->g.gz, fpart, tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_force");
   *ntile = tm;
   return CUW_OK;
@@ -568,11 +753,10 @@ extern "C" int cuwaves_tc_gemm_check(int M, int N, int K, const double* A, const
   using namespace cuw;
   if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C || !err) return CUW_ERR_ARG;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const size_t smem = MPipe::kSmem;
-  if (smem_allow((const void*)k_tf32x3_gemm, (int)smem) != cudaSuccess)
-    return CUW_ERR_CUDA;
+  const size_t smem = GemmPipe::kSmem;
+  if (smem_allow((const void*)k_tf32x3_gemm, (int)smem) != cudaSuccess) return CUW_ERR_CUDA;
   dim3 grid((M + 127) / 128, (N + 127) / 128);
-  k_tf32x3_gemm<<<grid, MPipe::kThreads, smem, st>>>(M, N, K, A, B, C, err);
+  k_tf32x3_gemm<<<grid, kThreads, smem, st>>>(M, N, K, A, B, C, err);
   if (cudaGetLastError() != cudaSuccess) return CUW_ERR_CUDA;
   return CUW_OK;
 }

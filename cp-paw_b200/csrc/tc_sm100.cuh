@@ -12,6 +12,7 @@
 // kind::tf32 consumes K = 8, i.e. two such groups.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -112,6 +113,17 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// D[tmem] (+)= A[tmem] * B[smem]^T: A held in tensor memory (lane = row,
+// one 32-bit column per K value), issued by one thread
+__device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // arrives once on *bar when every MMA issued so far by this thread has completed
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -131,6 +143,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
       : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// registers -> TMEM: lane t of warp w (w % 4 = q) writes row 32q+t, columns
+// [col, col+8) of the 32-bit TMEM address taddr
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr), "r"(r[0]),
+               "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // ---- split precision ------------------------------------------------------------------------
 // x = hi + lo with hi a tf32 value (10 explicit mantissa bits, rounded to
@@ -138,11 +158,70 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // tf32 too, so hi*hi + hi*lo + lo*hi carries about 21 significant bits (the
 // bits of x beyond fp32 lie far below lo's tf32 precision).  One conversion
 // per value: float/double conversions are a low-throughput operation.
-__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
-  const float xf = (float)x;
+__device__ __forceinline__ void split_tf32f(float xf, float& hi, float& lo) {
   const uint32_t u = (__float_as_uint(xf) + 0x1000u) & 0xFFFFE000u;
   hi = __uint_as_float(u);
   lo = xf - hi;
+}
+__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) { split_tf32f((float)x, hi, lo); }
+
+// ---- asynchronous global -> shared copies (cp.async) -------------------------------------
+// 16 bytes from gmem to smem; bytes beyond src_bytes (0..16) are zero-filled
+// and not read.  Both addresses are 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem)), "l"(gmem), "r"(src_bytes)
+               : "memory");
+}
+// 8 bytes (8-byte aligned addresses), zero-filled beyond src_bytes (0 or 8)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(smem)), "l"(gmem), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// the mbarrier receives one arrival (counted in addition to the ones it was
+// initialised for) once every prior cp.async of this thread has completed
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from
+// global to this CTA's shared memory, completing `bytes` transactions on *bar
+__device__ __forceinline__ void bulk_g2s(void* smem, const void* gmem, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(smem)),
+               "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// 2-D tiled TMA load (no multicast): the box of tensor map *tm at element
+// coordinates (x, y) into this CTA's shared memory, completing its bytes on
+// *bar.  x times the element size is a multiple of 16 bytes; elements outside
+// the tensor read as zero.
+__device__ __forceinline__ void tma_load_2d(void* smem, const CUtensorMap* tm, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(smem)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// one arrival on *bar that also announces `tx` bytes of copies to complete
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t tx) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(tx) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// ---- packed fp32 ------------------------------------------------------------------------
+// (a0, a1) += (b0, b1) with one add.rn.f32x2 (round to nearest)
+__device__ __forceinline__ void add2(float& a0, float& a1, uint32_t b0, uint32_t b1) {
+  asm("{\n\t.reg .b64 p, q;\n\t"
+      "mov.b64 p, {%0, %1};\n\t"
+      "mov.b64 q, {%2, %3};\n\t"
+      "add.rn.f32x2 p, p, q;\n\t"
+      "mov.b64 {%0, %1}, p;\n\t}"
+      : "+f"(a0), "+f"(a1)
+      : "r"(b0), "r"(b1));
 }
 
 }  // namespace tc
