@@ -83,40 +83,41 @@ __global__ void k_band_sums(int mode, const double2* __restrict__ x, const doubl
   if (threadIdx.x < 4) part[((size_t)b * nblk + blk) * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
-// final: res[b*4+k] = sum over blocks
-__global__ void k_band_final(const double* __restrict__ part, int nbh, int nblk, double* __restrict__ res) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nbh * 4) return;
-  int b = i / 4, k = i % 4;
-  double s = 0.0;
-  for (int t = 0; t < nblk; ++t) s += part[((size_t)b * nblk + t) * 4 + k];
-  res[i] = s;
-}
-
-// scalar results from band sums and occupations (one thread)
+// scalar results from band sums and occupations: the block sums the block
+// partials of every band (the order of the former two-kernel form), forms the
+// per-band terms in parallel, and thread 0 adds them in band order
 //   out[0] EKIN or WAVEKINETIC energy; out[1 + i] per-band values
-__global__ void k_energy_final(int mode, const double* __restrict__ res, const double* __restrict__ occ, int nbh,
-                               double gweight, double dt2, int tbucket, double* __restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double e = 0.0;
-  for (int b = 0; b < nbh; ++b) {
-    double f1 = occ[2 * b], f2 = occ[2 * b + 1];
+__global__ void k_energy_final(int mode, const double* __restrict__ part, int nblk, const double* __restrict__ occ,
+                               int nbh, double gweight, double dt2, int tbucket, double* __restrict__ out) {
+  extern __shared__ double sh[];
+  double* res = sh;            // [4 nbh]
+  double* term = sh + 4 * nbh;  // [nbh]
+  for (int i = threadIdx.x; i < 4 * nbh; i += blockDim.x) {
+    const int b = i / 4, k = i % 4;
+    double s = 0.0;
+    for (int t = 0; t < nblk; ++t) s += part[((size_t)b * nblk + t) * 4 + k];
+    res[i] = s;
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbh; b += blockDim.x) {
+    const double f1 = occ[2 * b], f2 = occ[2 * b + 1];
     const double* q = res + 4 * b;
+    double e = 0.0;
     if (mode == 0) {
-      double fp = 0.5 * (f1 + f2), fm = 0.5 * (f1 - f2);
-      if (fp == 0.0 && fm == 0.0) continue;
-      double t = 0.5 * fp * q[0] + (tbucket ? fp * q[2] : 0.0);
-      if (fabs(fm) >= 1e-12) t += 0.5 * fm * q[1] + (tbucket ? fm * q[3] : 0.0);
-      e += t;
+      const double fp = 0.5 * (f1 + f2), fm = 0.5 * (f1 - f2);
+      if (!(fp == 0.0 && fm == 0.0)) {
+        e = 0.5 * fp * q[0] + (tbucket ? fp * q[2] : 0.0);
+        if (fabs(fm) >= 1e-12) e += 0.5 * fm * q[1] + (tbucket ? fm * q[3] : 0.0);
+      }
     } else if (mode == 1) {
       double ev1 = 0.0, ev2 = 0.0;
       if (!(f1 == 0.0 && f2 == 0.0)) {
-        double sum = q[0] / dt2;
+        const double sum = q[0] / dt2;
         ev1 = 0.5 * sum;
         ev2 = 0.5 * sum;
-        e += sum * 0.5 * (f1 + f2);
+        e = sum * 0.5 * (f1 + f2);
         if (f1 - f2 != 0.0) {
-          double s2 = q[1] / dt2;
+          const double s2 = q[1] / dt2;
           ev1 += 0.5 * s2;
           ev2 -= 0.5 * s2;
           e += s2 * 0.5 * (f1 - f2);
@@ -125,13 +126,19 @@ __global__ void k_energy_final(int mode, const double* __restrict__ res, const d
       out[1 + 2 * b] = ev1;
       out[2 + 2 * b] = ev2;
     } else {
-      double tp = q[0] * gweight, tm = q[2] * gweight;
+      const double tp = q[0] * gweight, tm = q[2] * gweight;
       out[1 + 2 * b] = 0.5 * tp + 0.5 * tm;
       out[2 + 2 * b] = 0.5 * tp - 0.5 * tm;
-      e += f1 * out[1 + 2 * b] + f2 * out[2 + 2 * b];
+      e = f1 * out[1 + 2 * b] + f2 * out[2 + 2 * b];
     }
+    term[b] = e;
   }
-  out[0] = (mode == 2) ? e : e * gweight;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0;
+    for (int b = 0; b < nbh; ++b) e += term[b];
+    out[0] = (mode == 2) ? e : e * gweight;
+  }
 }
 
 // WAVES$PROPAGATE (src/paw_waves1.f90:6575-6583)
@@ -177,13 +184,17 @@ __global__ void k_atoms_verlet(const double* __restrict__ r0, const double* __re
 
 __global__ void k_ion_ekin(const double* __restrict__ rp, const double* __restrict__ rm,
                            const double* __restrict__ mass, int nat, double dt, double* __restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double e = 0.0;
-  for (int i = 0; i < 3 * nat; ++i) {
-    double v = (rp[i] - rm[i]) / (2.0 * dt);
-    e += 0.5 * mass[i / 3] * v * v;
+  extern __shared__ double term[];  // [3 nat]; summed by thread 0 in index order
+  for (int i = threadIdx.x; i < 3 * nat; i += blockDim.x) {
+    const double v = (rp[i] - rm[i]) / (2.0 * dt);
+    term[i] = 0.5 * mass[i / 3] * v * v;
   }
-  out[0] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0;
+    for (int i = 0; i < 3 * nat; ++i) e += term[i];
+    out[0] = e;
+  }
 }
 
 __global__ void k_copy_psi(const double2* __restrict__ src, double2* __restrict__ dst, size_t n) {
@@ -196,26 +207,25 @@ __global__ void k_copy_psi(const double2* __restrict__ src, double2* __restrict_
 // ---------------------------------------------------------------------------
 // band reductions: results in h->g.scal (device): [0] energy, [1..nb] per band
 // ---------------------------------------------------------------------------
-static int band_sums_run(Handle* h, int mode, const double2* x, const double2* y, const double* w1, const double* w2,
-                         double* res_dev) {
+static int band_sums_run(Handle* h, int mode, const double2* x, const double2* y, const double* w1, const double* w2) {
   const int nblk = ceil_div(h->d.ngl, RG);
   k_band_sums<<<dim3(nblk, h->d.nbh), RB, 0, h->stream>>>(mode, x, y, h->ldg, h->d.ngl, w1, w2, h->g.minusg,
                                                           h->g.red, nblk);
   CUW_LAUNCH_CHECK("k_band_sums");
-  k_band_final<<<ceil_div(4 * h->d.nbh, 128), 128, 0, h->stream>>>(h->g.red, h->d.nbh, nblk, res_dev);
-  CUW_LAUNCH_CHECK("k_band_final");
   return CUW_OK;
 }
 
 // mode: RED_EKIN / RED_WAVEKIN / RED_EXPECT; result vector at out_dev
 static int energy_run(Handle* h, int mode, double* out_dev) {
   Device& g = h->g;
-  double* res = g.red + (size_t)4 * h->d.nbh * ceil_div(h->d.ngl, RG);
-  if (mode == RED_EKIN) CUW_RET(band_sums_run(h, 0, g.psi0, nullptr, g.g2, h->tbucket ? g.bucket : nullptr, res));
-  else if (mode == RED_WAVEKIN) CUW_RET(band_sums_run(h, 1, g.psi0, g.psim, g.mpsi, nullptr, res));
-  else CUW_RET(band_sums_run(h, 2, g.psi0, g.hpsi, nullptr, nullptr, res));
-  k_energy_final<<<1, 1, 0, h->stream>>>(mode == RED_EKIN ? 0 : (mode == RED_WAVEKIN ? 1 : 2), res, g.occ, h->d.nbh,
-                                         h->gweight, h->delt * h->delt, h->tbucket ? 1 : 0, out_dev);
+  if (mode == RED_EKIN) CUW_RET(band_sums_run(h, 0, g.psi0, nullptr, g.g2, h->tbucket ? g.bucket : nullptr));
+  else if (mode == RED_WAVEKIN) CUW_RET(band_sums_run(h, 1, g.psi0, g.psim, g.mpsi, nullptr));
+  else CUW_RET(band_sums_run(h, 2, g.psi0, g.hpsi, nullptr, nullptr));
+  const size_t sm = sizeof(double) * 5 * (size_t)h->d.nbh;
+  if (sm > 48 * 1024) CUW_TRY(smem_allow((const void*)k_energy_final, (int)sm));
+  k_energy_final<<<1, 256, sm, h->stream>>>(mode == RED_EKIN ? 0 : (mode == RED_WAVEKIN ? 1 : 2), g.red,
+                                            ceil_div(h->d.ngl, RG), g.occ, h->d.nbh, h->gweight, h->delt * h->delt,
+                                            h->tbucket ? 1 : 0, out_dev);
   CUW_LAUNCH_CHECK("k_energy_final");
   return CUW_OK;
 }
@@ -278,6 +288,15 @@ static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
   CUW_RET(mark(h, 1));
   CUW_RET(eigr_compute(h, g.rp));
   CUW_RET(mark(h, 5));
+  // PSIBAR and OPSI stay fixed through the Gram products: their split forms
+  // are reused (the guard closes the scope on every way out)
+  struct ScopeGuard {
+    Handle* h;
+    ~ScopeGuard() {
+      if (h) tc_scope(h, false);
+    }
+  } guard{h->mixed() ? h : nullptr};
+  if (h->mixed()) tc_scope(h, true);
   CUW_RET(proj_compute(h, g.psim, g.proj, g.opsi, g.oproj));
   CUW_RET(mark(h, 6));
   // DO*PROJ and DO*OPROJ
@@ -290,6 +309,8 @@ static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
   CUW_RET(gram_projections(h, pc, 3, oc));
   GramPair pp[3] = {{g.psim, g.psim}, {g.opsi, g.psim}, {g.opsi, g.opsi}};
   CUW_RET(gram_planewave(h, pp, 3, pw));
+  if (h->mixed()) tc_scope(h, false);
+  guard.h = nullptr;
   CUW_RET(unravel_run(h, pw, oc, 3, g.mat, g.omat, g.oomat));
   CUW_RET(mark(h, 7));
   CUW_RET(lambda_init_run(h));
@@ -362,7 +383,8 @@ static void free_all(Handle* h) {
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
                   g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
-                  g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1]};
+                  g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1], g.bpre[0],
+                  g.bpre[1], g.bsmall};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   h->g = Device();
@@ -518,6 +540,7 @@ extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* min
                                 const double* gvec, const double* g2, const double* pro, const double* ylm,
                                 const double* mpsi, const double* bucket, double gweight) {
   H(hp);
+  h->eigr_src = nullptr;
   NEED(igvec && minusg && gbas && gvec && g2 && pro && ylm && mpsi, CUW_ERR_ARG, "null argument");
   NEED(gweight > 0.0, CUW_ERR_ARG, "gweight must be the positive cell volume");
   const int ngl = h->d.ngl;
@@ -597,6 +620,7 @@ extern "C" int cuwaves_set_do(cuw_handle* hp, int lnxx, const double* dover) {
 extern "C" int cuwaves_set_atoms(cuw_handle* hp, const double* r0, const double* rp) {
   H(hp);
   const size_t n = sizeof(double) * 3 * h->d.nat;
+  h->eigr_src = nullptr;
   if (r0) CUW_TRY(cudaMemcpy(h->g.r0, r0, n, cudaMemcpyHostToDevice));
   if (rp) CUW_TRY(cudaMemcpy(h->g.rp, rp, n, cudaMemcpyHostToDevice));
   return CUW_OK;
@@ -606,6 +630,7 @@ extern "C" int cuwaves_reset_atoms(cuw_handle* hp, const double* r0) {
   H(hp);
   NEED(r0, CUW_ERR_ARG, "null positions");
   const size_t n = sizeof(double) * 3 * h->d.nat;
+  h->eigr_src = nullptr;
   CUW_TRY(cudaMemcpy(h->g.r0, r0, n, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(h->g.rp, r0, n, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(h->g.rm, r0, n, cudaMemcpyHostToDevice));
@@ -887,6 +912,7 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
     CUW_TRY(cudaMemcpyAsync(g.mass, mass, sizeof(double) * h->d.nat, cudaMemcpyHostToDevice, h->stream));
+    if (h->eigr_src == g.rp) h->eigr_src = nullptr;  // R(+) is rewritten
     k_atoms_verlet<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(g.r0, g.rm, g.rp, g.force, g.mass, h->d.nat,
                                                                        h->delt * h->delt);
     CUW_LAUNCH_CHECK("k_atoms_verlet");
@@ -898,11 +924,12 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   CUW_TRY(cudaMemcpyAsync(sc + 3, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
-    k_ion_ekin<<<1, 1, 0, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
+    k_ion_ekin<<<1, 128, sizeof(double) * 3 * h->d.nat, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
     CUW_LAUNCH_CHECK("k_ion_ekin");
     // ATOMS$SWITCH: R(-) <- R(0), R(0) <- R(+)
     std::swap(g.rm, g.r0);
     std::swap(g.r0, g.rp);
+    if (h->eigr_src == g.rp) h->eigr_src = nullptr;
     CUW_TRY(cudaMemcpyAsync(g.rp, g.r0, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToDevice, h->stream));
   } else {
     CUW_TRY(cudaMemsetAsync(sc + 4, 0, sizeof(double), h->stream));

@@ -93,6 +93,10 @@ struct Device {
   double2 *eigr = nullptr;       // (NGL, NAT) structure factors of the last position set
   float2 *pf = nullptr;          // (LDG, NPRO) mixed path: PRO(g,p) of the last position set in fp32, 0 for g >= NGL
   double2 *xminus[2] = {nullptr, nullptr};  // (LDG, NBH) mixed path: X(-G) copies of wave-function arrays
+  float *bpre[2] = {nullptr, nullptr};       // mixed path: wave-function arrays split into tf32 B tiles
+  const double2 *bpre_src[2] = {nullptr, nullptr};  // arrays they hold (valid inside a solve scope)
+  float *bsmall = nullptr;                   // mixed path: small matrices split into tf32 B tiles (3 slots)
+  size_t bsmall_slot = 0;                    // floats per slot
   double2 *dh = nullptr;         // (LMNXX, LMNXX, NAT)
   double *dover = nullptr;       // (LNXX, LNXX, NSP)
   double *occ = nullptr;         // (NB)
@@ -152,6 +156,8 @@ struct Handle {
   bool mixed() const { return d.precision == CUW_PREC_MIXED; }
   long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
   long long n_fp_fail = 0; // Lyapunov fixed-point solves that fell back to a rediagonalisation
+  bool tc_scope_open = false;
+  const double* eigr_src = nullptr;  // position buffer (r0, rp or rm) that EIGR (and the fp32 table) was built from
   Device g;
   std::string err;
 
@@ -264,6 +270,9 @@ cudaError_t smem_allow(const void* fn, int bytes);
 // CUW_PREC_MIXED; same arguments and results as the FP64 functions above
 int tc_setup(Handle* h);
 int tc_pro_table(Handle* h);  // h->g.pf from h->g.eigr (mixed path)
+// Split wave-function operands computed inside a scope are reused by later
+// contractions of the same scope (the arrays do not change inside it).
+void tc_scope(Handle* h, bool open);
 int tc_proj(Handle* h, const double2* psi, double2* proj);
 int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const StepCoef& sc);
 int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,

@@ -639,10 +639,18 @@ static int choose_split(Handle* h, int tiles, int nk, int minchunk) {
 }
 
 int eigr_compute(Handle* h, const double* r_dev) {
+  // EIGR (and the fp32 projector table) of the positions in a position buffer
+  // stay current until that buffer is written: R(+) of one step is R(0) of the
+  // next
+  const bool pos = r_dev == h->g.r0 || r_dev == h->g.rp || r_dev == h->g.rm;
+  if (pos && r_dev == h->eigr_src) return CUW_OK;
+  h->eigr_src = nullptr;
   dim3 grid(std::min(ceil_div(h->d.ngl, 256), 64), h->d.nat);
   k_eigr<<<grid, 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz, r_dev, h->d.ngl, h->d.nat, h->g.eigr);
   CUW_LAUNCH_CHECK("k_eigr");
-  return h->mixed() ? tc_pro_table(h) : CUW_OK;
+  if (h->mixed()) CUW_RET(tc_pro_table(h));
+  if (pos) h->eigr_src = r_dev;
+  return CUW_OK;
 }
 
 // projA = Omega <p|psiA>, projB likewise when psiB != null; uses h->g.eigr

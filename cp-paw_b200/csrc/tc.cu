@@ -27,28 +27,29 @@ namespace {
 // accumulation was measured on B200 at a signed mean error of -3.7e-8 /
 // -8.7e-8 / -1.8e-7 of |C| for runs of 8 / 16 / 32 real K, and one step keeps
 // the energy bias below 1e-6 Ha/atom.
-constexpr int kCK = 8, kNSplit = 2;
+constexpr int kCK = 8, kNSplit = 4;
 
-// Raw slot layouts (bytes).  TMA boxes land row-major; boxes whose rows are
-// read down a column by the converters use the 64- or 128-byte swizzle, so
-// that eight consecutive rows hit distinct banks.
-constexpr int kRawProj = 16384;   // Pf 128 p x 8 g (64-byte rows, 64B swizzle) + psi 64 b x 8 g (128B swizzle)
-constexpr int kRawAddpro = 16384; // Pf 8 p x 128 g (1 KB rows) + C1, C2 8 p x 32 b (512-byte rows)
-constexpr int kRawGram = 24576;   // X, X(-k), Y: 64 rows of 8 k (128B swizzle), or 8 rows of 64 (1 KB)
-constexpr int kRawAddx = 49152;   // X, second-half X: 8 k x 128 m (2 KB rows) or 128 m x 8 k (128B swizzle); L1, L2
-constexpr int kRawForce = 24576;  // psi0 8 b x 128 g (2 KB rows) + E 64 p x 8 b (128B swizzle)
+// Raw slot layouts (bytes) of the A operands.  TMA boxes land row-major; boxes
+// whose rows are read down a column by the converters use the 64- or 128-byte
+// swizzle, so that eight consecutive rows hit distinct banks.  The B operands
+// arrive already split (k_bsplit) as one bulk copy per chunk.
+constexpr int kRawProj = 8192;    // Pf 128 p x 8 g (64-byte rows, 64B swizzle)
+constexpr int kRawAddpro = 8192;  // Pf 8 p x 128 g (1 KB rows)
+constexpr int kRawGram = 16384;   // X, X(-k): 64 rows of 8 k (128B swizzle), or X: 8 rows of 64 (1 KB)
+constexpr int kRawAddx = 32768;   // X, second-half X: 8 k x 128 m (2 KB rows) or 128 m x 8 k (128B swizzle)
+constexpr int kRawForce = 16384;  // psi0 8 b x 128 g (2 KB rows)
 constexpr int kRawGemm = 36864;   // A, B 128 rows x 16 doubles (144-byte rows, element copies)
 using ProjPipe = tc::Pipe<kNSplit, 8, kRawProj>;
 using AddproPipe = tc::Pipe<kNSplit, 8, kRawAddpro>;
 using GramPipe = tc::Pipe<kNSplit, 6, kRawGram>;
-using AddxPipe = tc::Pipe<kNSplit, 3, kRawAddx>;
+using AddxPipe = tc::Pipe<kNSplit, 4, kRawAddx>;
 using ForcePipe = tc::Pipe<kNSplit, 6, kRawForce>;
-using GemmPipe = tc::Pipe<kNSplit, 3, kRawGemm>;
+using GemmPipe = tc::Pipe<kNSplit, 3, kRawGemm, false>;
 constexpr int kThreads = ProjPipe::kThreads;
-constexpr int kConv = ProjPipe::kConv;
 constexpr int kNC = ProjPipe::kCols / 2;  // complex output columns per drain thread
+constexpr int kBTile = 4096;              // floats of one split B chunk (hi and lo tiles)
 static_assert(ProjPipe::kSmem <= 232448 && GramPipe::kSmem <= 232448 && AddxPipe::kSmem <= 232448 &&
-                  GemmPipe::kSmem <= 232448 && ForcePipe::kSmem <= 232448,
+                  GemmPipe::kSmem <= 232448 && ForcePipe::kSmem <= 232448 && AddproPipe::kSmem <= 232448,
               "shared memory");
 // k_tc_force reuses the stage and raw buffers for a 128 x 64 FP64 tile
 static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * 128 * 64, "stage area too small");
@@ -66,12 +67,18 @@ __device__ __forceinline__ T at(const unsigned char* raw, int byte) {
 __device__ __forceinline__ double2 dz() { return make_double2(0.0, 0.0); }
 __device__ __forceinline__ double2 cj(double2 a) { return make_double2(a.x, -a.y); }
 
-// The real-form B rows 2j (R even) / 2j+1 (R odd) of two complex values c0, c1
-// (complex K pair hp): four real K values split into the hi/lo tiles
-__device__ __forceinline__ void put_b_pair(float* bhi, float* blo, int R, int hp, double2 c0, double2 c1) {
-  if ((R & 1) == 0) tc::store_split4(bhi, blo, tc::tile_f4(R, hp), c0.x, -c0.y, c1.x, -c1.y);
-  else tc::store_split4(bhi, blo, tc::tile_f4(R, hp), c0.y, c0.x, c1.y, c1.x);
+// B functors of the pipelines that do not use them
+struct NoLoadB {
+  __device__ void operator()(int, int, tc::Copier&) const {}
+};
+struct NoConvertB {
+  __device__ void operator()(int, const unsigned char*, int, float*, float*) const {}
+};
+// bulk copy of the pre-split B chunk (tile, chunk) of a k_bsplit array
+__device__ __forceinline__ void load_bsplit(tc::Copier& cp, int lane, const float* bs, int nchk, int tile, int chunk) {
+  if (lane == 0) cp.bulk(0, bs + ((size_t)tile * nchk + chunk) * kBTile, 4 * kBTile);
 }
+
 // complex value i of an A row as real K values 2i, 2i+1 (conj: -Im)
 template <bool CONJ, class C2>
 __device__ __forceinline__ void a_put(float (&v)[8], int i, C2 a) {
@@ -106,7 +113,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   };
   auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {
-    for (int it = ct; it < 128 * 4; it += kConv) {
+    for (int it = ct; it < 128 * 4; it += GemmPipe::kGroup) {
       const int r = it % 128, g = it / 128;
       double x[4];
 #pragma unroll
@@ -125,7 +132,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int j = 0; j < GemmPipe::kCols; ++j)
       if (j < nc) out[j] = (double)acc[j];
   };
-  tc::pipe_run<kNSplit, 3, kRawGemm>((K + 15) / 16, load, a_row, convert_b, finish, err);
+  NoLoadB no_b;
+  tc::pipe_run<GemmPipe>((K + 15) / 16, load, no_b, a_row, convert_b, finish, err);
 }
 
 // out[i] = scale * sum_z part[z*n + i], summed in FP64 in a fixed order
@@ -146,17 +154,23 @@ __global__ void k_tc_reduce(const float2* __restrict__ part, int nz, size_t n, d
 // PRO(g,p) = Y_lm(g) P_ln(|g|) (-i)^l EIGR(g,a) (WAVES_EXPANDPRO,
 // src/paw_waves1.f90:6070-6109) evaluated in FP64, zero for g >= NGL.  The
 // single rounding to fp32 is the one the split into tf32 pairs starts from.
-__global__ void k_pro_f32(int ngl, int ldg, const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+__global__ void k_pro_f32(int ngl, int ldg, const int* __restrict__ ipro0, const int* __restrict__ nlmn,
+                          const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
                           const double* __restrict__ pro, const double2* __restrict__ eigr, float2* __restrict__ pf) {
-  const int p = blockIdx.y;
-  const ProDesc d = pdesc[p];
+  // one thread per (g, atom): EIGR(g, a) read once for all projectors of the atom
+  const int a = blockIdx.y, p0 = ipro0[a], np = nlmn[a];
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ldg; g += gridDim.x * blockDim.x) {
-    float2 v = make_float2(0.f, 0.f);
-    if (g < ngl) {
-      const double2 x = pro_value(g, ngl, d, ylm, pro, eigr);
-      v = make_float2((float)x.x, (float)x.y);
+    if (g >= ngl) {
+      for (int k = 0; k < np; ++k) pf[(size_t)(p0 + k) * ldg + g] = make_float2(0.f, 0.f);
+      continue;
     }
-    pf[(size_t)p * ldg + g] = v;
+    const double2 e = eigr[(size_t)g + (size_t)ngl * a];
+    for (int k = 0; k < np; ++k) {
+      const ProDesc d = pdesc[p0 + k];
+      const double s = ylm[(size_t)g + (size_t)ngl * d.lm] * pro[(size_t)g + (size_t)ngl * d.ibare];
+      const double2 em = cmul(mipow(d.l), e);
+      pf[(size_t)(p0 + k) * ldg + g] = make_float2((float)(s * em.x), (float)(s * em.y));
+    }
   }
 }
 
@@ -166,31 +180,21 @@ __global__ void k_pro_f32(int ngl, int ldg, const ProDesc* __restrict__ pdesc, c
 // M = 128 projectors (blockIdx.x), N = 64 bands (blockIdx.y), K = g (blockIdx.z)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads, 1)
-    k_tc_proj(const __grid_constant__ CUtensorMap tm_pf, const __grid_constant__ CUtensorMap tm_psi, int ngl, int nbh,
+    k_tc_proj(const __grid_constant__ CUtensorMap tm_pf, const float* __restrict__ bpsi, int nchk, int ngl, int nbh,
               int npro, int kchunk, float2* __restrict__ part, int* __restrict__ err) {
   const int m0 = blockIdx.x * 128, b0 = blockIdx.y * 64;
   const int gbeg = blockIdx.z * kchunk, gend = min(ngl, gbeg + kchunk);
-  // raw slot: [0, 8K) Pf box 128 p x 8 g (64-byte rows, 64B swizzle);
-  // [8K, 16K) psi box 64 b x 8 g (128-byte rows, 128B swizzle).  Chunks never
-  // straddle a split boundary (kchunk is a multiple of 8) and read zeros past NGL.
+  // raw slot: Pf box 128 p x 8 g (64-byte rows, 64B swizzle); zeros past NGL
+  // and NPRO.  Chunks never straddle a split boundary (kchunk is a multiple of 8).
   auto load = [&](int c, int lane, tc::Copier& cp) {
-    if (lane == 0) {
-      const int g0 = gbeg + c * kCK;
-      cp.tensor(0, &tm_pf, 2 * g0, m0, 8192);
-      cp.tensor(8192, &tm_psi, 2 * g0, b0, 8192);
-    }
+    if (lane == 0) cp.tensor(0, &tm_pf, 2 * (gbeg + c * kCK), m0, 8192);
   };
+  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, bpsi, nchk, blockIdx.y, gbeg / kCK + c); };
   auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // conj(Pf) row p
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       const float4 x = at<float4>(raw, sw64(r, 2 * kh + i));
       v[4 * i] = x.x, v[4 * i + 1] = -x.y, v[4 * i + 2] = x.z, v[4 * i + 3] = -x.w;
-    }
-  };
-  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // psi, real form
-    for (int it = ct; it < 512; it += kConv) {
-      const int R = it & 127, hp = it >> 7, j = R >> 1;
-      put_b_pair(bhi, blo, R, hp, at<double2>(raw, 8192 + sw128(j, 2 * hp)), at<double2>(raw, 8192 + sw128(j, 2 * hp + 1)));
     }
   };
   auto finish = [&](const float (&acc)[ProjPipe::kCols], int row, int col0) {
@@ -202,8 +206,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int j = 0; j < kNC; ++j)
       if (bb + j < nbh) out[bb + j] = make_float2(acc[2 * j], acc[2 * j + 1]);
   };
+  NoConvertB no_cb;
   const int nchunk = gend > gbeg ? (gend - gbeg + kCK - 1) / kCK : 0;
-  tc::pipe_run<kNSplit, 8, kRawProj>(nchunk, load, a_row, convert_b, finish, err);
+  tc::pipe_run<ProjPipe>(nchunk, load, load_b, a_row, no_cb, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -215,33 +220,20 @@ template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tc_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi, const double2* __restrict__ psi0,
                 double2* __restrict__ psim, const double* __restrict__ mpsi, int ldg, int ngl, int nbh, int npro,
-                const __grid_constant__ CUtensorMap tm_pf, const __grid_constant__ CUtensorMap tm_c1,
-                const __grid_constant__ CUtensorMap tm_c2, StepCoef sc, int* __restrict__ err) {
+                const __grid_constant__ CUtensorMap tm_pf, const float* __restrict__ bc, int nchk, StepCoef sc,
+                int* __restrict__ err) {
   constexpr bool USE_H = (MODE != ADDPRO_OPSI);
   constexpr bool USE_O = (MODE != ADDPRO_HPSI);
   const int g0 = blockIdx.x * 128, b0 = blockIdx.y * 32;
-  // raw slot: [0, 8K) Pf box 8 p x 128 g (1 KB rows); [8K, 12K) C1 box and
-  // [12K, 16K) C2 box, 8 p x 32 b (512-byte rows); zeros past NGL, NPRO, NBH
+  // raw slot: Pf box 8 p x 128 g (1 KB rows); zeros past NGL and NPRO.  B:
+  // [C1 | C2] of bands b0..b0+31, split (k_bsplit, zero where unused)
   auto load = [&](int c, int lane, tc::Copier& cp) {
-    if (lane == 0) {
-      const int p0 = c * kCK;
-      cp.tensor(0, &tm_pf, 2 * g0, p0, 8192);
-      if (USE_H) cp.tensor(8192, &tm_c1, 2 * b0, p0, 4096);
-      if (USE_O) cp.tensor(12288, &tm_c2, 2 * b0, p0, 4096);
-    }
+    if (lane == 0) cp.tensor(0, &tm_pf, 2 * g0, c * kCK, 8192);
   };
+  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, bc, nchk, blockIdx.y, c); };
   auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // Pf(g, p), K = p
 #pragma unroll
     for (int i = 0; i < 4; ++i) a_put<false>(v, i, at<float2>(raw, (4 * kh + i) * 1024 + r * 8));
-  };
-  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // [C1 | C2], real form
-    for (int it = ct; it < 512; it += kConv) {
-      const int R = it & 127, hp = it >> 7, j = R >> 1, mt = j >> 5, bl = j & 31;
-      const bool ok = mt == 0 ? USE_H : USE_O;  // a box left out holds stale data
-      const int o = 8192 + mt * 4096 + bl * 16;
-      put_b_pair(bhi, blo, R, hp, ok ? at<double2>(raw, o + (2 * hp) * 512) : dz(),
-                 ok ? at<double2>(raw, o + (2 * hp + 1) * 512) : dz());
-    }
   };
   auto finish = [&](const float (&acc)[AddproPipe::kCols], int row, int col0) {
     const int g = g0 + row;
@@ -270,7 +262,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   };
-  tc::pipe_run<kNSplit, 8, kRawAddpro>((npro + kCK - 1) / kCK, load, a_row, convert_b, finish, err);
+  NoConvertB no_cb;
+  tc::pipe_run<AddproPipe>((npro + kCK - 1) / kCK, load, load_b, a_row, no_cb, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -283,12 +276,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Y columns.  Partials part[z][t][m + nm n] (float2), z = split*npair + pair.
 // ---------------------------------------------------------------------------
 struct TcGramArgs {
-  int npair, nk, nm, kchunk;
-  bool kfast;  // X(k, m) contiguous in k (plane waves); else in m (projections)
+  int npair, nk, nm, kchunk, nchk;
+  bool kfast;            // X(k, m) contiguous in k (plane waves); else in m (projections)
+  const float* ybs[3];   // Y of each pair, split (k_bsplit)
 };
-// TMA maps of the pairs: X, X(-k) (plane waves with MINUS) and Y
+// TMA maps of the pairs: X and X(-k) (plane waves with MINUS)
 struct TcGramMaps {
-  CUtensorMap x[3], xm[3], y[3];
+  CUtensorMap x[3], xm[3];
 };
 
 template <bool MINUS>
@@ -298,23 +292,23 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
   const int kbeg = split * a.kchunk, kend = min(a.nk, kbeg + a.kchunk);
   const bool kfast = a.kfast;
-  // raw slot: X at 0, X(-k) at 8K (MINUS), Y at 16K.  kfast: boxes of 64
-  // rows (m or n) of eight k (128-byte rows, 128B swizzle); otherwise 8 rows
-  // (k) of 64 m or n (1 KB rows).  Zeros past NK and NM.
-  constexpr int XM = 8192, YO = 16384;
+  // raw slot: X at 0, X(-k) at 8K (MINUS).  kfast: boxes of 64 rows (m) of
+  // eight k (128-byte rows, 128B swizzle); otherwise 8 rows (k) of 64 m (1 KB
+  // rows).  Zeros past NK and NM.
+  constexpr int XM = 8192;
+  const float* ybs = a.ybs[pair];
   auto load = [&](int c, int lane, tc::Copier& cp) {
     if (lane == 0) {
       const int k0 = kbeg + c * kCK;
       if (kfast) {
         cp.tensor(0, &tm.x[pair], 2 * k0, m0, 8192);
         if (MINUS) cp.tensor(XM, &tm.xm[pair], 2 * k0, m0, 8192);
-        cp.tensor(YO, &tm.y[pair], 2 * k0, n0, 8192);
       } else {
         cp.tensor(0, &tm.x[pair], 2 * m0, k0, 8192);
-        cp.tensor(YO, &tm.y[pair], 2 * n0, k0, 8192);
       }
     }
   };
+  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, ybs, a.nchk, blockIdx.x, kbeg / kCK + c); };
   auto xoff = [&](int r, int e) { return kfast ? sw128(r, e) : e * 1024 + r * 16; };
   auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {
     // rows 0..63 conj X(k), rows 64..127 X(-k) (MINUS) or X(k)
@@ -327,12 +321,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       else a_put<false>(v, i, x);
     }
   };
-  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // Y, real form
-    for (int it = ct; it < 512; it += kConv) {
-      const int R = it & 127, hp = it >> 7, j = R >> 1;
-      put_b_pair(bhi, blo, R, hp, at<double2>(raw, YO + xoff(j, 2 * hp)), at<double2>(raw, YO + xoff(j, 2 * hp + 1)));
-    }
-  };
   auto finish = [&](const float (&acc)[GramPipe::kCols], int row, int col0) {
     const int t = row >> 6, m = m0 + (row & 63);
     if (m >= a.nm) return;
@@ -343,8 +331,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int j = 0; j < kNC; ++j)
       if (nb + j < a.nm) out[(size_t)m + (size_t)a.nm * (nb + j)] = make_float2(acc[2 * j], acc[2 * j + 1]);
   };
+  NoConvertB no_cb;
   const int nchunk = kend > kbeg ? (kend - kbeg + kCK - 1) / kCK : 0;
-  tc::pipe_run<kNSplit, 6, kRawGram>(nchunk, load, a_row, convert_b, finish, err);
+  tc::pipe_run<GramPipe>(nchunk, load, load_b, a_row, no_cb, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -354,13 +343,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------------------
 struct TcAddXArgs {
   double2* out;
-  int nm, nn, nk;
+  int nm, nn, nk, nchk;
   size_t som, son;
-  bool mfast;  // X(m, k) contiguous in m (plane waves); else in k (projections)
+  bool mfast;       // X(m, k) contiguous in m (plane waves); else in k (projections)
+  const float* lbs; // [L1; L2], split (k_bsplit)
 };
-// TMA maps: X for K < NK, the second-half X (conj X(m') for K >= NK), L1, L2
+// TMA maps: X for K < NK, the second-half X (conj X(m') for K >= NK)
 struct TcAddXMaps {
-  CUtensorMap x, x2, l1, l2;
+  CUtensorMap x, x2;
 };
 
 __global__ void __launch_bounds__(kThreads, 1)
@@ -368,27 +358,26 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 64;
   const int ktot = 2 * a.nk;
   const bool mfast = a.mfast;
+  (void)n0;
   // raw slot: X at 0 and the second-half X at 16K: mfast boxes of 8 rows (k)
-  // of 128 m (2 KB rows), else 128 rows (m) of eight k (128B swizzle); L1 at
-  // 32K, L2 at 40K: 64 rows (n) of eight k (128B swizzle).  Second-half boxes
-  // start at k = kg0 - NK, negative for a chunk that straddles NK: rows or
-  // columns outside the arrays read as zero.
-  constexpr int X2 = 16384, L1O = 32768, L2O = 40960;
+  // of 128 m (2 KB rows), else 128 rows (m) of eight k (128B swizzle).
+  // Second-half boxes start at k = kg0 - NK, negative for a chunk that
+  // straddles NK: rows or columns outside the arrays read as zero.
+  constexpr int X2 = 16384;
   auto load = [&](int c, int lane, tc::Copier& cp) {
     if (lane == 0) {
       const int kg0 = c * kCK, k2 = kg0 - a.nk;
       if (kg0 < a.nk) {
         if (mfast) cp.tensor(0, &tm.x, 2 * m0, kg0, 16384);
         else cp.tensor(0, &tm.x, 2 * kg0, m0, 16384);
-        cp.tensor(L1O, &tm.l1, 2 * kg0, n0, 8192);
       }
       if (kg0 + kCK > a.nk) {
         if (mfast) cp.tensor(X2, &tm.x2, 2 * m0, k2, 16384);
         else cp.tensor(X2, &tm.x2, 2 * k2, m0, 16384);
-        cp.tensor(L2O, &tm.l2, 2 * k2, n0, 8192);
       }
     }
   };
+  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, a.lbs, a.nchk, blockIdx.y, c); };
   auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // X(m,k) | conj X(m',k)
     const int kg0 = c * kCK + 4 * kh;
 #pragma unroll
@@ -400,23 +389,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       else a_put<true>(v, i, x);
     }
   };
-  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // [L1; L2], real form
-    const int kg0 = c * kCK;
-    for (int it = ct; it < 512; it += kConv) {
-      const int R = it & 127, hp = it >> 7, j = R >> 1;
-      double2 cv[2];
-#pragma unroll
-      for (int e2 = 0; e2 < 2; ++e2) {
-        const int e = 2 * hp + e2, kg = kg0 + e;
-        cv[e2] = kg < ktot ? at<double2>(raw, (kg < a.nk ? L1O : L2O) + sw128(j, e)) : dz();
-      }
-      put_b_pair(bhi, blo, R, hp, cv[0], cv[1]);
-    }
-  };
   auto finish = [&](const float (&acc)[AddxPipe::kCols], int row, int col0) {
     const int m = m0 + row;
     if (m >= a.nm) return;
-    const int nb = n0 + col0 / 2;
+    const int nb = blockIdx.y * 64 + col0 / 2;
 #pragma unroll
     for (int j = 0; j < kNC; ++j) {
       if (nb + j >= a.nn) continue;
@@ -425,7 +401,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       a.out[k] = make_double2(o.x + (double)acc[2 * j], o.y + (double)acc[2 * j + 1]);
     }
   };
-  tc::pipe_run<kNSplit, 3, kRawAddx>((ktot + kCK - 1) / kCK, load, a_row, convert_b, finish, err);
+  NoConvertB no_cb;
+  tc::pipe_run<AddxPipe>((ktot + kCK - 1) / kCK, load, load_b, a_row, no_cb, finish, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -436,31 +413,21 @@ __global__ void __launch_bounds__(kThreads, 1)
 // sum_g sv(g,p) G_c(g) by the whole CTA.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads, 1)
-    k_tc_force(const __grid_constant__ CUtensorMap tm_psi, const __grid_constant__ CUtensorMap tm_e, int ngl, int nbh,
+    k_tc_force(const __grid_constant__ CUtensorMap tm_psi, const float* __restrict__ be, int nchk, int ngl, int nbh,
                int npro, const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
                const double* __restrict__ pro, const double2* __restrict__ eigr, const double* __restrict__ gx,
                const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ fpart,
                int* __restrict__ err) {
   const int g0 = blockIdx.x * 128, p0 = blockIdx.y * 64;
-  // raw slot: [0, 16K) psi0 box 8 b x 128 g (2 KB rows); [16K, 24K) E box
-  // 64 p x 8 b (128B swizzle); zeros past NGL, NBH, NPRO
-  constexpr int EO = 16384;
+  // raw slot: psi0 box 8 b x 128 g (2 KB rows); zeros past NGL and NBH.  B:
+  // conj(E) of projectors p0..p0+63, split (k_bsplit)
   auto load = [&](int c, int lane, tc::Copier& cp) {
-    if (lane == 0) {
-      const int bb = c * kCK;
-      cp.tensor(0, &tm_psi, 2 * g0, bb, 16384);
-      cp.tensor(EO, &tm_e, 2 * bb, p0, 8192);
-    }
+    if (lane == 0) cp.tensor(0, &tm_psi, 2 * g0, c * kCK, 16384);
   };
+  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, be, nchk, blockIdx.y, c); };
   auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // psi0(g, b), K = b
 #pragma unroll
     for (int i = 0; i < 4; ++i) a_put<false>(v, i, at<double2>(raw, (4 * kh + i) * 2048 + r * 16));
-  };
-  auto convert_b = [&](int c, const unsigned char* raw, int ct, float* bhi, float* blo) {  // conj(E), real form
-    for (int it = ct; it < 512; it += kConv) {
-      const int R = it & 127, hp = it >> 7, j = R >> 1;
-      put_b_pair(bhi, blo, R, hp, cj(at<double2>(raw, EO + sw128(j, 2 * hp))), cj(at<double2>(raw, EO + sw128(j, 2 * hp + 1))));
-    }
   };
   // [128][64], over the stage and raw buffers: when a drain thread finishes,
   // every chunk has been converted and multiplied and no copy is in flight
@@ -481,7 +448,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       sv[row * 64 + pb + j] = v;
     }
   };
-  tc::pipe_run<kNSplit, 6, kRawForce>((nbh + kCK - 1) / kCK, load, a_row, convert_b, finish, err);
+  NoConvertB no_cb;
+  tc::pipe_run<ForcePipe>((nbh + kCK - 1) / kCK, load, load_b, a_row, no_cb, finish, err);
   // pipe_run ended with a CTA barrier: sv is complete (if a wait ran out the
   // error flag is set and the caller discards the result)
   for (int i = threadIdx.x; i < 64 * 3; i += blockDim.x) {
@@ -491,6 +459,55 @@ __global__ void __launch_bounds__(kThreads, 1)
     double s = 0.0;
     for (int r = 0; r < 128 && g0 + r < ngl; ++r) s += sv[r * 64 + pl] * gc[g0 + r];
     fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = s;
+  }
+}
+
+// Source of a split B operand: value(row, h) of complex output column `row`
+// at complex K index h
+//   kind 0: x[h + ld*row]            kind 1: x[row + ld*h]
+//   kind 2: conj x[h + ld*row]       kind 3: h < nk1 ? x[h + ld*row] : x2[h - nk1 + ld*row]
+//   kind 4: tile of 32 rows of x then 32 rows of x2, each as kind 1 (null: zero)
+struct BSplitSrc {
+  int kind;
+  const double2* x;
+  const double2* x2;
+  long long ld;
+  int nrow, nk, nk1;
+};
+
+// B operand in real form, split into tf32 hi/lo tiles in the shared-memory
+// layout of the pipeline (tc_pipe.cuh): block (tile, chunk) of 4096 floats =
+// hi then lo, element (R, k) of 128 real rows x 16 real K at
+// (k/4)*512 + R*4 + k%4; real rows 2j / 2j+1 of complex column j are
+// (Re c, -Im c) / (Im c, Re c).  Zero outside the source.
+__global__ void k_bsplit(BSplitSrc b, int nchk, float* __restrict__ out) {
+  const int tile = blockIdx.y, c = blockIdx.x;
+  float* o = out + ((size_t)tile * nchk + c) * kBTile;
+  for (int it = threadIdx.x; it < 512; it += blockDim.x) {
+    const int R = it & 127, kg = it >> 7, j = R >> 1;
+    double2 v[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int h = c * kCK + 2 * kg + e;
+      v[e] = dz();
+      if (h >= b.nk) continue;
+      if (b.kind == 4) {
+        const double2* src = j < 32 ? b.x : b.x2;
+        const int row = 32 * tile + (j & 31);
+        if (src && row < b.nrow) v[e] = src[(size_t)row + (size_t)b.ld * h];
+      } else {
+        const int row = 64 * tile + j;
+        if (row >= b.nrow) continue;
+        if (b.kind == 0) v[e] = b.x[(size_t)h + (size_t)b.ld * row];
+        else if (b.kind == 1) v[e] = b.x[(size_t)row + (size_t)b.ld * h];
+        else if (b.kind == 2) v[e] = cj(b.x[(size_t)h + (size_t)b.ld * row]);
+        else v[e] = h < b.nk1 ? b.x[(size_t)h + (size_t)b.ld * row] : b.x2[(size_t)(h - b.nk1) + (size_t)b.ld * row];
+      }
+    }
+    double w[4];
+    if ((R & 1) == 0) w[0] = v[0].x, w[1] = -v[0].y, w[2] = v[1].x, w[3] = -v[1].y;
+    else w[0] = v[0].y, w[1] = v[0].x, w[2] = v[1].y, w[3] = v[1].x;
+    tc::store_split4(o, o + 2048, kg * 128 + R, w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -582,14 +599,59 @@ int tc_setup(Handle* h) {
   CUW_RET(alloc(reinterpret_cast<void**>(&h->g.pf), sizeof(float2) * (size_t)h->ldg * std::max(1, h->npro)));
   for (int i = 0; i < 2; ++i)
     CUW_RET(alloc(reinterpret_cast<void**>(&h->g.xminus[i]), sizeof(double2) * (size_t)h->ldg * h->d.nbh));
+  const size_t psi_split = (size_t)kBTile * ceil_div(h->d.nbh, 64) * ceil_div(h->d.ngl, kCK);
+  for (int i = 0; i < 2; ++i) CUW_RET(alloc(reinterpret_cast<void**>(&h->g.bpre[i]), sizeof(float) * psi_split));
+  // largest small-matrix operand: [C1 | C2] of ADDPRO, tiles of 32 bands
+  const int np = std::max(1, h->npro), nb = h->d.nbh;
+  size_t slot = (size_t)ceil_div(nb, 32) * ceil_div(np, kCK);
+  slot = std::max(slot, (size_t)ceil_div(np, 64) * ceil_div(nb, kCK));
+  slot = std::max(slot, (size_t)ceil_div(nb, 64) * ceil_div(np, kCK));
+  slot = std::max(slot, (size_t)ceil_div(nb, 64) * ceil_div(2 * nb, kCK));
+  h->g.bsmall_slot = slot * kBTile;
+  CUW_RET(alloc(reinterpret_cast<void**>(&h->g.bsmall), sizeof(float) * 3 * h->g.bsmall_slot));
   return CUW_OK;
 }
 
 int tc_pro_table(Handle* h) {
   if (h->npro == 0) return CUW_OK;
-  const dim3 grid(std::min(ceil_div(h->ldg, 256), 64), h->npro);
-  k_pro_f32<<<grid, 256, 0, h->stream>>>(h->d.ngl, h->ldg, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.pf);
+  const dim3 grid(std::min(ceil_div(h->ldg, 256), 64), h->d.nat);
+  k_pro_f32<<<grid, 256, 0, h->stream>>>(h->d.ngl, h->ldg, h->g.t_ipro0, h->g.t_nlmn, h->g.pdesc, h->g.ylm, h->g.pro,
+                                         h->g.eigr, h->g.pf);
   CUW_LAUNCH_CHECK("k_pro_f32");
+  return CUW_OK;
+}
+
+void tc_scope(Handle* h, bool open) {
+  h->tc_scope_open = open;
+  h->g.bpre_src[0] = h->g.bpre_src[1] = nullptr;
+}
+
+static int tc_bsplit(Handle* h, const BSplitSrc& b, int ntile, int nchk, float* out) {
+  k_bsplit<<<dim3(nchk, ntile), 256, 0, h->stream>>>(b, nchk, out);
+  CUW_LAUNCH_CHECK("k_bsplit");
+  return CUW_OK;
+}
+// split form of wave-function array psi (B operand, rows = bands, K = g)
+static int tc_bsplit_psi(Handle* h, const double2* psi, const float** out) {
+  Device& g = h->g;
+  for (int i = 0; i < 2; ++i)
+    if (h->tc_scope_open && g.bpre_src[i] == psi) {
+      *out = g.bpre[i];
+      return CUW_OK;
+    }
+  const int i = g.bpre_src[0] ? 1 : 0;
+  BSplitSrc b{0, psi, nullptr, (long long)h->ldg, h->d.nbh, h->d.ngl, 0};
+  CUW_RET(tc_bsplit(h, b, ceil_div(h->d.nbh, 64), ceil_div(h->d.ngl, kCK), g.bpre[i]));
+  if (h->tc_scope_open) g.bpre_src[i] = psi;
+  *out = g.bpre[i];
+  return CUW_OK;
+}
+// split form of a small matrix into slot `slot` of h->g.bsmall
+static int tc_bsplit_small(Handle* h, const BSplitSrc& b, int ntile, int nchk, int slot, const float** out) {
+  if ((size_t)ntile * nchk * kBTile > h->g.bsmall_slot) return h->fail(CUW_ERR_STATE, "split operand scratch too small");
+  float* dst = h->g.bsmall + (size_t)slot * h->g.bsmall_slot;
+  CUW_RET(tc_bsplit(h, b, ntile, nchk, dst));
+  *out = dst;
   return CUW_OK;
 }
 
@@ -619,11 +681,12 @@ int tc_proj(Handle* h, const double2* psi, double2* proj) {
   const size_t n = (size_t)nbh * npro;
   CUW_RET(ensure_part(h, sizeof(float2) * n * ks));
   float2* part = reinterpret_cast<float2*>(h->g.part);
-  CUtensorMap tpf, tps;
+  CUtensorMap tpf;
   CUW_RET(make_map(h, &tpf, h->g.pf, false, 2ll * ngl, npro, 2ll * h->ldg, 16, 128, CU_TENSOR_MAP_SWIZZLE_64B));
-  CUW_RET(map_c(h, &tps, psi, ngl, nbh, h->ldg, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
-  k_tc_proj<<<dim3(tn, tb, ks), kThreads, ProjPipe::kSmem, h->stream>>>(tpf, tps, ngl, nbh, npro, kchunk, part,
-                                                                         tc_err(h));
+  const float* bpsi = nullptr;
+  CUW_RET(tc_bsplit_psi(h, psi, &bpsi));
+  k_tc_proj<<<dim3(tn, tb, ks), kThreads, ProjPipe::kSmem, h->stream>>>(tpf, bpsi, ceil_div(ngl, kCK), ngl, nbh, npro,
+                                                                         kchunk, part, tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_proj");
   return tc_reduce(h, part, ks, n, h->gweight, proj);
 }
@@ -632,15 +695,15 @@ int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const
   const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
   const dim3 grid(ceil_div(ngl, 128), ceil_div(nbh, 32));
   Device& g = h->g;
-  CUtensorMap tpf, tc1, tc2;
+  CUtensorMap tpf;
   CUW_RET(make_map(h, &tpf, g.pf, false, 2ll * ngl, npro, 2ll * h->ldg, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
-  const double2* c1 = hpc ? hpc : opc;
-  const double2* c2 = opc ? opc : hpc;
-  CUW_RET(map_c(h, &tc1, c1, nbh, npro, nbh, 64, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
-  CUW_RET(map_c(h, &tc2, c2, nbh, npro, nbh, 64, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+  const int nchk = ceil_div(npro, kCK);
+  const float* bc = nullptr;
+  BSplitSrc b{4, mode == ADDPRO_OPSI ? nullptr : hpc, mode == ADDPRO_HPSI ? nullptr : opc, (long long)nbh, nbh, npro, 0};
+  CUW_RET(tc_bsplit_small(h, b, ceil_div(nbh, 32), nchk, 0, &bc));
 #define TC_ADDPRO(M)                                                                                            \
   k_tc_addpro<M><<<grid, kThreads, AddproPipe::kSmem, h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, \
-                                                                   ngl, nbh, npro, tpf, tc1, tc2, sc, tc_err(h))
+                                                                   ngl, nbh, npro, tpf, bc, nchk, sc, tc_err(h))
   if (mode == ADDPRO_HPSI) TC_ADDPRO(ADDPRO_HPSI);
   else if (mode == ADDPRO_OPSI) TC_ADDPRO(ADDPRO_OPSI);
   else TC_ADDPRO(ADDPRO_FUSED);
@@ -656,20 +719,32 @@ int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int
   a.nk = nk;
   a.nm = nm;
   a.kfast = sk == 1;
+  a.nchk = ceil_div(nk, kCK);
   if (!a.kfast && sm != 1) return h->fail(CUW_ERR_UNSUPPORTED, "Gram product with neither index contiguous");
   if (minus && !a.kfast) return h->fail(CUW_ERR_UNSUPPORTED, "X(-k) Gram product of projections");
   TcGramMaps tm;
   // X(-k) copies of the distinct X arrays (at most two: PSIBAR and OPSI)
   const double2* src[2] = {nullptr, nullptr};
   const double2* mcopy[2] = {nullptr, nullptr};
+  const double2* ydone[3] = {nullptr, nullptr, nullptr};
+  int nsmall = 0;
   for (int i = 0; i < npair; ++i) {
     const double2 *x = pairs[i].x, *y = pairs[i].y;
     if (a.kfast) {
       CUW_RET(map_c(h, &tm.x[i], x, nk, nm, (long long)sm, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
-      CUW_RET(map_c(h, &tm.y[i], y, nk, nm, (long long)sm, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+      CUW_RET(tc_bsplit_psi(h, y, &a.ybs[i]));
     } else {
       CUW_RET(map_c(h, &tm.x[i], x, nm, nk, (long long)sk, 128, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
-      CUW_RET(map_c(h, &tm.y[i], y, nm, nk, (long long)sk, 128, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
+      int same = -1;
+      for (int j = 0; j < i; ++j)
+        if (ydone[j] == y) same = j;
+      if (same >= 0) {
+        a.ybs[i] = a.ybs[same];
+      } else {
+        BSplitSrc b{1, y, nullptr, (long long)sk, nm, nk, 0};
+        CUW_RET(tc_bsplit_small(h, b, ceil_div(nm, 64), a.nchk, nsmall++, &a.ybs[i]));
+      }
+      ydone[i] = y;
     }
     tm.xm[i] = tm.x[i];
     if (minus) {
@@ -687,7 +762,10 @@ int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int
       CUW_RET(map_c(h, &tm.xm[i], mcopy[slot], nk, nm, (long long)sm, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
     }
   }
-  for (int i = npair; i < 3; ++i) tm.x[i] = tm.xm[i] = tm.y[i] = tm.x[0];
+  for (int i = npair; i < 3; ++i) {
+    tm.x[i] = tm.xm[i] = tm.x[0];
+    a.ybs[i] = a.ybs[0];
+  }
   const int tiles = ceil_div(nm, 64) * ceil_div(nm, 64) * npair;
   int ks = tc_splits(h, tiles, nk);
   a.kchunk = ceil_div(ceil_div(nk, ks), kCK) * kCK;
@@ -704,7 +782,15 @@ int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int
 
 int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double2* l1, const double2* l2, int nm,
             int nn, int nk, size_t sxm, size_t sxk, size_t som, size_t son) {
-  TcAddXArgs a{out, nm, nn, nk, som, son, sxm == 1};
+  TcAddXArgs a;
+  a.out = out;
+  a.nm = nm;
+  a.nn = nn;
+  a.nk = nk;
+  a.som = som;
+  a.son = son;
+  a.mfast = sxm == 1;
+  a.nchk = ceil_div(2 * nk, kCK);
   TcAddXMaps tm;
   if (a.mfast) {
     const double2* x2 = x;
@@ -720,8 +806,8 @@ int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double
     CUW_RET(map_c(h, &tm.x, x, nk, nm, (long long)sxm, 16, 128, CU_TENSOR_MAP_SWIZZLE_128B));
     tm.x2 = tm.x;
   }
-  CUW_RET(map_c(h, &tm.l1, l1, nk, nn, nk, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
-  CUW_RET(map_c(h, &tm.l2, l2, nk, nn, nk, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
+  BSplitSrc b{3, l1, l2, (long long)nk, nn, 2 * nk, nk};
+  CUW_RET(tc_bsplit_small(h, b, ceil_div(nn, 64), a.nchk, 0, &a.lbs));
   const dim3 grid(ceil_div(nm, 128), ceil_div(nn, 64));
   k_tc_addx<<<grid, kThreads, AddxPipe::kSmem, h->stream>>>(a, tm, tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_addx");
@@ -731,12 +817,15 @@ int tc_addx(Handle* h, bool xminus, double2* out, const double2* x, const double
 int tc_force(Handle* h, const double2* ded, double* fpart, int* ntile) {
   const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
   const int tm = ceil_div(ngl, 128), tn = ceil_div(npro, 64);
-  CUtensorMap tps, te;
+  CUtensorMap tps;
   CUW_RET(map_c(h, &tps, h->g.psi0, ngl, nbh, h->ldg, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
-  CUW_RET(map_c(h, &te, ded, nbh, npro, nbh, 16, 64, CU_TENSOR_MAP_SWIZZLE_128B));
-  k_tc_force<<<dim3(tm, tn), kThreads, ForcePipe::kSmem, h->stream>>>(tps, te, ngl, nbh, npro, h->g.pdesc, h->g.ylm,
-                                                                      h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
-                                                                      h->g.gz, fpart, tc_err(h));
+  const int nchk = ceil_div(nbh, kCK);
+  const float* be = nullptr;
+  BSplitSrc b{2, ded, nullptr, (long long)nbh, npro, nbh, 0};
+  CUW_RET(tc_bsplit_small(h, b, tn, nchk, 0, &be));
+  k_tc_force<<<dim3(tm, tn), kThreads, ForcePipe::kSmem, h->stream>>>(tps, be, nchk, ngl, nbh, npro, h->g.pdesc,
+                                                                      h->g.ylm, h->g.pro, h->g.eigr, h->g.gx,
+                                                                      h->g.gy, h->g.gz, fpart, tc_err(h));
   CUW_LAUNCH_CHECK("k_tc_force");
   *ntile = tm;
   return CUW_OK;
