@@ -384,7 +384,7 @@ static void free_all(Handle* h) {
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
                   g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
                   g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1], g.bpre[0],
-                  g.bpre[1], g.bsmall};
+                  g.bpre[1], g.bsmall, g.jac_a};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   h->g = Device();
@@ -818,6 +818,13 @@ extern "C" int cuwaves_gramschmidt(cuw_handle* hp, int which, const double* r) {
   NEED(r, CUW_ERR_ARG, "null positions");
   Device& g = h->g;
   double2* psi = psi_ptr(h, which);
+  // The overlap of arbitrary start vectors can be nearly singular: its
+  // contractions run in FP64 on every path (restored on every way out)
+  struct Fp64Guard {
+    Handle* h;
+    ~Fp64Guard() { h->fp64_only = false; }
+  } fp64_guard{h};
+  h->fp64_only = true;
   // atom positions r -> rm slot is not touched: use force buffer as scratch for r
   double* rd = g.force;
   CUW_TRY(cudaMemcpyAsync(rd, r, sizeof(double) * 3 * h->d.nat, cudaMemcpyHostToDevice, h->stream));

@@ -96,6 +96,7 @@ struct Device {
   float *bpre[2] = {nullptr, nullptr};       // mixed path: wave-function arrays split into tf32 B tiles
   const double2 *bpre_src[2] = {nullptr, nullptr};  // arrays they hold (valid inside a solve scope)
   float *bsmall = nullptr;                   // mixed path: small matrices split into tf32 B tiles (3 slots)
+  double *jac_a = nullptr;                   // packed matrix of the eigensolver when NB is too large for shared memory
   size_t bsmall_slot = 0;                    // floats per slot
   double2 *dh = nullptr;         // (LMNXX, LMNXX, NAT)
   double *dover = nullptr;       // (LNXX, LNXX, NSP)
@@ -154,6 +155,8 @@ struct Handle {
   std::vector<int> ev_phase;
   int nev = 0;
   bool mixed() const { return d.precision == CUW_PREC_MIXED; }
+  bool fp64_only = false;  // contractions in FP64 even on the mixed path (start-up orthonormalisation)
+  bool tc_on() const { return mixed() && !fp64_only; }
   long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
   long long n_fp_fail = 0; // Lyapunov fixed-point solves that fell back to a rediagonalisation
   bool tc_scope_open = false;

@@ -655,7 +655,7 @@ int eigr_compute(Handle* h, const double* r_dev) {
 
 // projA = Omega <p|psiA>, projB likewise when psiB != null; uses h->g.eigr
 int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* psiB, double2* projB) {
-  if (h->mixed()) {
+  if (h->tc_on()) {
     CUW_RET(tc_proj(h, psiA, projA));
     return psiB ? tc_proj(h, psiB, projB) : CUW_OK;
   }
@@ -694,7 +694,7 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
   sc.a2 = 1.0 - sc.a1;
   sc.a3 = -h->delt * h->delt / (1.0 + h->annee);
   sc.oscale = h->delt * h->delt / (1.0 + h->annee);  // src/paw_waves2.f90:148-156
-  if (h->mixed()) return tc_addpro(h, mode, hpc, opc, sc);
+  if (h->tc_on()) return tc_addpro(h, mode, hpc, opc, sc);
   Device& g = h->g;
   switch (mode) {
     case ADDPRO_HPSI:
@@ -745,7 +745,7 @@ int oproj_compute(Handle* h, const double2* proj, double2* out) {
 // offset `dst` (complex), scaled by `scale`.
 static int gram_run(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
                     double scale, double2* dst) {
-  if (h->mixed()) return tc_gram(h, pairs, npair, minus, nk, nm, sk, sm, scale, dst);
+  if (h->tc_on()) return tc_gram(h, pairs, npair, minus, nk, nm, sk, sm, scale, dst);
   GramArgs a;
   for (int i = 0; i < npair; ++i) a.pair[i] = pairs[i];
   a.npair = npair;
@@ -793,7 +793,7 @@ int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* 
   a.sxk = (size_t)h->ldg;
   a.som = 1;
   a.son = (size_t)h->ldg;
-  if (h->mixed()) return tc_addx(h, true, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
+  if (h->tc_on()) return tc_addx(h, true, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
   k_addx<true, true><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
@@ -813,7 +813,7 @@ int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* 
   a.sxk = 1;
   a.som = (size_t)h->d.nbh;  // out(m=p, n=b) at b + nbh*p
   a.son = 1;
-  if (h->mixed()) return tc_addx(h, false, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
+  if (h->tc_on()) return tc_addx(h, false, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
   k_addx<false, false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
@@ -826,7 +826,7 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
   const int tn = ceil_div(npro, BN);
   CUW_RET(ensure_part(h, sizeof(double) * 3 * (size_t)std::max(tm, ceil_div(ngl, 128)) * npro));
   double* fpart = reinterpret_cast<double*>(h->g.part);
-  if (h->mixed()) {
+  if (h->tc_on()) {
     CUW_RET(tc_force(h, ded, fpart, &tm));
   } else {
     k_force<<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc,

@@ -92,11 +92,15 @@ __device__ __forceinline__ int pk(int i, int j) { return i <= j ? (j * (j + 1)) 
 
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in, int n, double* __restrict__ u_out,
                                                  double* __restrict__ e_out, double* __restrict__ vglob,
-                                                 int v_in_smem, int max_sweeps, int* __restrict__ info) {
+                                                 int v_in_smem, double* __restrict__ aglob, int max_sweeps,
+                                                 int* __restrict__ info) {
   extern __shared__ double sm[];
   const int np = n / 2;
-  double* A = sm;                                        // packed n(n+1)/2
-  double* rc = A + (size_t)n * (n + 1) / 2;              // np cosines
+  // packed n(n+1)/2 matrix in shared memory, or in global memory (aglob) when
+  // it does not fit (NB above about 200; through L2, slower, used only for
+  // the occasional rediagonalisation)
+  double* A = aglob ? aglob : sm;
+  double* rc = aglob ? sm : A + (size_t)n * (n + 1) / 2;  // np cosines
   double* rs = rc + np;                                  // np sines
   int* pp = reinterpret_cast<int*>(rs + np);             // np
   int* pq = pp + np;                                     // np
@@ -873,14 +877,21 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
   const size_t base = sizeof(double) * (packed + n) + sizeof(int) * (n + 2) + 16 + tab;
   size_t smem = base + sizeof(double) * (size_t)n * n;
   int v_in_smem = 1;
+  double* aglob = nullptr;
   if (smem > 220 * 1024) {
     v_in_smem = 0;
     smem = base;
   }
-  if (smem > 220 * 1024) return h->fail(CUW_ERR_UNSUPPORTED, "NB too large for the on-chip eigensolver");
+  if (smem > 220 * 1024) {
+    // the packed matrix goes to global memory too
+    smem = base - sizeof(double) * packed;
+    if (smem > 220 * 1024) return h->fail(CUW_ERR_UNSUPPORTED, "NB too large for the eigensolver");
+    if (!h->g.jac_a) CUW_TRY(cudaMalloc(&h->g.jac_a, sizeof(double) * packed));
+    aglob = h->g.jac_a;
+  }
   CUW_TRY(smem_allow((const void*)k_jacobi, (int)smem));
   int* info = reinterpret_cast<int*>(h->g.ostatus) + 4;
-  k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, 40, info);
+  k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, aglob, 40, info);
   CUW_LAUNCH_CHECK("k_jacobi");
   return CUW_OK;
 }
