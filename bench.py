@@ -294,37 +294,20 @@ def run_mixed(args, local):
             "phase_ms_per_step": {k: round(v / max(1, nsteps), 4) for k, v in phases.items()}}
 
 
-def run_serving(args):
-    """Serving workload: a seeded Poisson stream of single-point solves and
-    20-step CP runs of perturbed bulk Si_n and water clusters, submitted in
-    real time to the device-resident server (HBM-budget admission, continuous
-    batching).  Latency is submission to completion, measured by the server."""
+def _serve_stream(pool, kinds, rate, nreq, workers, budget_gb, seed):
+    """One seeded Poisson stream through a fresh server; per-request latency is
+    measured by the server from submission to completion."""
     import numpy as np
     import cuwaves
-    from cuwaves import systems
     from cuwaves.serve import Server
 
-    rng = np.random.default_rng(7)
-    kinds = [("Si", n) for n in sorted(systems.SERVING_SI)] + [("W", n) for n in systems.SERVING_WATER]
-    pool = {}
-    for kind, n in kinds:
-        for seed in (1, 2):
-            inp = systems.build_inputs(systems.serving_system(kind, n, seed))
-            inp["annee"] = 0.05  # friction on the wave functions: a damped (relaxing) run
-            pool[(kind, n, seed)] = inp
-    nreq, rate = args.serve_requests, args.serve_rate
+    rng = np.random.default_rng(seed)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
     plan = []
-    for i in range(nreq):
+    for _ in range(nreq):
         kind, n = kinds[int(rng.integers(0, len(kinds)))]
         plan.append(((kind, n, int(rng.integers(1, 3))), 0 if rng.random() < 0.5 else 20))
-    srv = Server(hbm_budget=args.serve_budget_gb << 30, workers=args.serve_workers)
-    # warm-up outside the stream: one request of every kind
-    for kind, n in kinds:
-        srv.submit(pool[(kind, n, 1)], nsteps=1, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
-    srv.wait_all()
-    srv.close()
-    srv = Server(hbm_budget=args.serve_budget_gb << 30, workers=args.serve_workers)
+    srv = Server(hbm_budget=budget_gb << 30, workers=workers)
     ids = []
     t0 = time.perf_counter()
     for (key, nsteps), ta in zip(plan, arrivals):
@@ -345,17 +328,50 @@ def run_serving(args):
             lat[nsteps].append(r[3])
     srv.close()
     pct = lambda v, q: round(float(np.percentile(v, q)), 3) if v else None  # noqa: E731
-    return {"requests": nreq, "offered_rate_per_s": rate, "completed": int(st["completed"]), "failed": failed,
-            "solves_per_s": round(st["throughput_per_s"], 3), "p50_ms": round(st["p50_ms"], 3),
+    return {"requests": nreq, "offered_rate_per_s": round(rate, 3), "completed": int(st["completed"]),
+            "failed": failed, "solves_per_s": round(st["throughput_per_s"], 3), "p50_ms": round(st["p50_ms"], 3),
             "p99_ms": round(st["p99_ms"], 3), "max_ms": round(st["max_ms"], 3),
             "single_point_p50_ms": pct(lat[0], 50), "single_point_p99_ms": pct(lat[0], 99),
             "cp20_p50_ms": pct(lat[20], 50), "cp20_p99_ms": pct(lat[20], 99),
-            "hbm_budget_gb": args.serve_budget_gb, "peak_admitted_gb": round(st["peak_bytes"] / 2 ** 30, 3),
-            "mean_admitted_sets": round(st["mean_admitted"], 2), "workers": args.serve_workers,
-            "precision": "mixed",
-            "workload": "Poisson stream, 50% single points (energy+forces) and 50% 20-step damped CP runs with "
+            "peak_admitted_gb": round(st["peak_bytes"] / 2 ** 30, 3), "mean_admitted_sets": round(st["mean_admitted"], 2)}
+
+
+def run_serving(args):
+    """Serving workload: seeded Poisson streams of single-point solves and
+    20-step CP runs of perturbed bulk Si_n and water clusters, submitted in
+    real time to the device-resident server (HBM-budget admission, continuous
+    batching).  The stream at the nominal rate (200 requests/s) overloads one
+    GPU, so it measures the capacity (solves/s); a second stream offered at
+    60% of that capacity gives the latency at sustained throughput."""
+    import cuwaves
+    from cuwaves import systems
+    from cuwaves.serve import Server
+
+    kinds = [("Si", n) for n in sorted(systems.SERVING_SI)] + [("W", n) for n in systems.SERVING_WATER]
+    pool = {}
+    for kind, n in kinds:
+        for seed in (1, 2):
+            inp = systems.build_inputs(systems.serving_system(kind, n, seed))
+            inp["annee"] = 0.05  # friction on the wave functions: a damped (relaxing) run
+            pool[(kind, n, seed)] = inp
+    # warm-up outside the streams: one request of every kind
+    srv = Server(hbm_budget=args.serve_budget_gb << 30, workers=args.serve_workers)
+    for kind, n in kinds:
+        srv.submit(pool[(kind, n, 1)], nsteps=1, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
+    srv.wait_all()
+    srv.close()
+    peak = _serve_stream(pool, kinds, args.serve_rate, args.serve_requests, args.serve_workers, args.serve_budget_gb, 7)
+    cap = max(peak["solves_per_s"], 0.1)
+    rate = 0.6 * cap
+    nreq = max(10, min(args.serve_requests, int(rate * args.serve_seconds)))
+    sustained = _serve_stream(pool, kinds, rate, nreq, args.serve_workers, args.serve_budget_gb, 8)
+    return {"at_nominal_rate": peak, "sustained_at_60pct_capacity": sustained,
+            "p50_ms": sustained["p50_ms"], "p99_ms": sustained["p99_ms"], "solves_per_s": peak["solves_per_s"],
+            "hbm_budget_gb": args.serve_budget_gb, "workers": args.serve_workers, "precision": "mixed",
+            "workload": "Poisson streams, 50% single points (energy+forces) and 50% 20-step damped CP runs with "
                         "moving nuclei; Si8/16/32/64/128 (+-0.05 bohr, 30 Ry) and (H2O)1/2/4/8/16 clusters (40 Ry, "
-                        "8 bohr vacuum), two seeds each; latency from submission to completion"}
+                        "8 bohr vacuum), two seeds each; latency from submission to completion; solves_per_s is the "
+                        "capacity measured under the nominal 200 requests/s stream, p50/p99 are at 60% of it"}
 
 
 def run_batched(args):
@@ -551,6 +567,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=int, default=48)
+    ap.add_argument("--serve-seconds", type=float, default=25.0, help="arrival window of the sustained stream")
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--batched-workers", type=int, default=16)
     ap.add_argument("--batched-si64", type=int, default=8)

@@ -92,6 +92,7 @@ size_t estimate_bytes(const cuw_dims& d, const int* isp) {
 
 struct cuw_server {
   size_t budget = 0;
+  int max_active = 0;         // admitted sets at most (sets beyond wait in the queue)
   std::mutex mu;
   std::condition_variable cv;
   std::map<long long, std::unique_ptr<Job>> jobs;
@@ -116,7 +117,7 @@ struct cuw_server {
   void admit() {
     while (!queue.empty()) {
       Job* j = queue.front();
-      if (in_use + j->bytes > budget) break;
+      if (in_use + j->bytes > budget || (int)active.size() >= max_active) break;
       queue.pop_front();
       account(Clock::now());
       in_use += j->bytes;
@@ -239,9 +240,18 @@ extern "C" int cuwaves_server_create(size_t hbm_budget, int nworkers, cuw_server
   cuw_server* s = new (std::nothrow) cuw_server;
   if (!s) return CUW_ERR_NOMEM;
   s->budget = hbm_budget;
+  s->max_active = 4 * nworkers;
   s->t_mark = Clock::now();
   for (int w = 0; w < nworkers; ++w) s->workers.emplace_back([s] { s->worker(); });
   *out = s;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_server_set_max_active(cuw_server* s, int max_active) {
+  if (!s || max_active < 1) return CUW_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->max_active = max_active;
+  s->cv.notify_all();
   return CUW_OK;
 }
 

@@ -27,7 +27,7 @@ namespace {
 // accumulation was measured on B200 at a signed mean error of -3.7e-8 /
 // -8.7e-8 / -1.8e-7 of |C| for runs of 8 / 16 / 32 real K, and one step keeps
 // the energy bias below 1e-6 Ha/atom.
-constexpr int kCK = 8, kNSplit = 4;
+constexpr int kCK = 8, kNSplit = 8;
 
 // Raw slot layouts (bytes) of the A operands.  TMA boxes land row-major; boxes
 // whose rows are read down a column by the converters use the 64- or 128-byte
@@ -42,9 +42,9 @@ constexpr int kRawGemm = 36864;   // A, B 128 rows x 16 doubles (144-byte rows, 
 using ProjPipe = tc::Pipe<kNSplit, 8, kRawProj>;
 using AddproPipe = tc::Pipe<kNSplit, 8, kRawAddpro>;
 using GramPipe = tc::Pipe<kNSplit, 6, kRawGram>;
-using AddxPipe = tc::Pipe<kNSplit, 4, kRawAddx>;
+using AddxPipe = tc::Pipe<kNSplit, 3, kRawAddx>;
 using ForcePipe = tc::Pipe<kNSplit, 6, kRawForce>;
-using GemmPipe = tc::Pipe<kNSplit, 3, kRawGemm, false>;
+using GemmPipe = tc::Pipe<kNSplit, 2, kRawGemm, false>;
 constexpr int kThreads = ProjPipe::kThreads;
 constexpr int kNC = ProjPipe::kCols / 2;  // complex output columns per drain thread
 constexpr int kBTile = 4096;              // floats of one split B chunk (hi and lo tiles)
@@ -52,7 +52,8 @@ static_assert(ProjPipe::kSmem <= 232448 && GramPipe::kSmem <= 232448 && AddxPipe
                   GemmPipe::kSmem <= 232448 && ForcePipe::kSmem <= 232448 && AddproPipe::kSmem <= 232448,
               "shared memory");
 // k_tc_force reuses the stage and raw buffers for a 128 x 64 FP64 tile
-static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * 128 * 64, "stage area too small");
+static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * (128 * 64 + 3 * 128 + 4 * 192),
+              "stage area too small");
 
 // offset of 16-byte chunk e of row r in a box with 128-byte (64-byte) rows
 // under the TMA 128-byte (64-byte) swizzle: chunk bits 4-6 (4-5) of the
@@ -451,14 +452,27 @@ __global__ void __launch_bounds__(kThreads, 1)
   NoConvertB no_cb;
   tc::pipe_run<ForcePipe>((nbh + kCK - 1) / kCK, load, load_b, a_row, no_cb, finish, err);
   // pipe_run ended with a CTA barrier: sv is complete (if a wait ran out the
-  // error flag is set and the caller discards the result)
-  for (int i = threadIdx.x; i < 64 * 3; i += blockDim.x) {
-    const int pl = i / 3, c = i % 3, p = p0 + pl;
-    if (p >= npro) continue;
-    const double* gc = c == 0 ? gx : (c == 1 ? gy : gz);
+  // error flag is set and the caller discards the result).  G components of the
+  // tile, then fpart = sum_g sv(g,p) G_c(g) in four row quarters combined in a
+  // fixed order
+  double* gsh = sv + 128 * 64;  // [3][128]
+  double* qsum = gsh + 3 * 128; // [4][192]
+  for (int i = threadIdx.x; i < 3 * 128; i += blockDim.x) {
+    const int c = i / 128, r = i % 128, g = g0 + r;
+    gsh[i] = g < ngl ? (c == 0 ? gx : (c == 1 ? gy : gz))[g] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * 192; i += blockDim.x) {
+    const int qr = i / 192, k = i % 192, pl = k / 3, c = k % 3;
     double s = 0.0;
-    for (int r = 0; r < 128 && g0 + r < ngl; ++r) s += sv[r * 64 + pl] * gc[g0 + r];
-    fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = s;
+#pragma unroll 8
+    for (int r = 32 * qr; r < 32 * qr + 32; ++r) s += sv[r * 64 + pl] * gsh[c * 128 + r];
+    qsum[i] = s;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 192; k += blockDim.x) {
+    const int pl = k / 3, c = k % 3, p = p0 + pl;
+    if (p < npro) fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = ((qsum[k] + qsum[192 + k]) + qsum[384 + k]) + qsum[576 + k];
   }
 }
 

@@ -14,7 +14,7 @@
 //                         lanes 32*(w%4).. (tile rows) and 32 of the 128 columns
 //
 // A chunk holds 16 real K values (two MMA steps of K = 8).  The products of
-// CPR consecutive chunks accumulate in one TMEM region (three regions of 128
+// CPR consecutive chunks accumulate in one TMEM region (regions of 128
 // columns in rotation), which the drain warps then add into fp32 registers
 // (round to nearest).  The tensor core's fp32 accumulation truncates toward
 // zero: every add into an accumulator loses on average half a unit in the
@@ -26,8 +26,10 @@
 // keeps the tensor core's shared-memory reads to the B tiles:
 // shared-memory bandwidth bounds a tf32 product of this shape.
 //
-// TMEM columns: [0, 384) accumulator regions, [384 + 32 s, +32) A of stage s
-// (hi: 16 columns, lo: 16 columns; at most four stages).  The copies run up to NRAW chunks ahead of
+// TMEM columns: [0, 128 NREG) accumulator regions, [128 NREG + 32 s, +32) A of
+// stage s (hi: 16 columns, lo: 16 columns).  Two regions and eight stages keep
+// four regions' worth of chunks in flight: the hand-overs between converters,
+// MMA thread and drain each take several hundred cycles.  The copies run up to NRAW chunks ahead of
 // the conversion; converted operands sit in NSPLIT stages, so copies,
 // conversion, MMAs and drains of different chunks overlap.  Every hand-over is
 // an mbarrier: rawfull[slot] (copies landed), rawempty[slot] (converters done
@@ -48,9 +50,10 @@ constexpr long long kWaitCycles = 1ll << 31;  // about one second at 2 GHz
 // 2^-23 relative to the binade of the accumulated value
 constexpr float kLossPerStep = 0.25f * 1.1920928955078125e-7f;
 
-template <int NSPLIT, int NRAW, int RAWB, bool BPRE = true, int CPR = 2>
+template <int NSPLIT, int NRAW, int RAWB, bool BPRE = true, int CPR = 2, int NREG = 2>
 struct Pipe {
-  static_assert(NRAW >= 2 && NSPLIT >= 2 * CPR && NSPLIT <= 4, "stage counts");
+  static_assert(NRAW >= 2 && NSPLIT >= 2 * CPR, "stage counts");
+  static_assert(128 * NREG + 32 * NSPLIT <= 512, "TMEM: accumulator regions and A stages");
   static_assert(RAWB % 1024 == 0, "raw slots keep the 1024-byte alignment of swizzled TMA boxes");
   static constexpr int kRows = 128;                 // A rows = TMEM lanes = B rows (N)
   static constexpr int kBK = 16;                    // real K values per chunk
@@ -65,7 +68,7 @@ struct Pipe {
   static constexpr int kDrain = 16;                 // drain warps
   static constexpr int kCols = 128 / (kDrain / 4);  // columns per drain thread
   static constexpr int kThreads = 32 * (3 + kConvWarps + kDrain);
-  static constexpr int kRegions = 3;                // TMEM accumulators of 128 columns
+  static constexpr int kRegions = NREG;             // TMEM accumulators of 128 columns
   static constexpr int kCPR = CPR;                  // chunks per accumulation region
   static constexpr int kACol = 128 * kRegions;      // first TMEM column of the A stages
   static constexpr int kRawBytes = RAWB;
@@ -82,14 +85,21 @@ struct Copier {
   unsigned char* raw;
   uint64_t* bar;
   uint32_t bytes;
+  bool async = false;  // element copies issued (their completion is tracked on bar)
   __device__ __forceinline__ void bulk(int off, const void* src, uint32_t n) {
     if (n) {
       bulk_g2s(raw + off, src, n, bar);
       bytes += n;
     }
   }
-  __device__ __forceinline__ void el16(int off, const void* src) { cp_async16(raw + off, src, 16); }
-  __device__ __forceinline__ void el8(int off, const void* src) { cp_async8(raw + off, src, 8); }
+  __device__ __forceinline__ void el16(int off, const void* src) {
+    cp_async16(raw + off, src, 16);
+    async = true;
+  }
+  __device__ __forceinline__ void el8(int off, const void* src) {
+    cp_async8(raw + off, src, 8);
+    async = true;
+  }
   // one TMA box of `box_bytes` (issued by one lane)
   __device__ __forceinline__ void tensor(int off, const CUtensorMap* tm, int x, int y, uint32_t box_bytes) {
     tma_load_2d(raw + off, tm, x, y, bar);
@@ -200,6 +210,14 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_tf32(128, 128);
       constexpr uint32_t lbo = 128 * 16;  // next group of four K values
+      // The issuing warp shares its scheduler with converter and drain warps:
+      // every MMA costs only a few instructions (descriptors differ in their
+      // start-address field, address / 16, alone).
+      const uint64_t dsc0 = sdesc(0, lbo, 128);
+      const uint32_t st0 = smem_u32(st) >> 4;
+      constexpr uint32_t kStageU = (uint32_t)(sizeof(float) * P::kStage) >> 4;
+      constexpr uint32_t kLoU = (uint32_t)(sizeof(float) * P::kTile) >> 4;
+      constexpr uint32_t kOffU = (2 * lbo) >> 4;
       int last = -1;  // last region issued
       for (int u = 0; u < nreg && !*abort_flag; ++u) {
         const int r = u % NR, c0 = u * CPR, nc = min(CPR, nchunk - c0);
@@ -212,19 +230,23 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
         fence_after_sync();
         const uint32_t d = tmem + (uint32_t)(r * 128);
         // cross products of every MMA step of the region, then the hi*hi products
+#pragma unroll
         for (int pass = 0; pass < 2; ++pass)
-          for (int i = 0; i < nc; ++i) {
+#pragma unroll
+          for (int i = 0; i < CPR; ++i) {
+            if (i >= nc) continue;
             const int s = (c0 + i) % NSPLIT;
-            const uint32_t sb = smem_u32(st + s * P::kStage), sbl = sb + 4 * P::kTile;
+            const uint32_t bu = st0 + (uint32_t)s * kStageU;
             const uint32_t ta = tmem + (uint32_t)(P::kACol + 32 * s);
 #pragma unroll
             for (int ks = 0; ks < P::kSteps; ++ks) {
-              const uint32_t off = ks * 2 * lbo, ahi = ta + 8 * ks, alo = ahi + 16;
+              const uint64_t bhi = dsc0 | (uint64_t)(bu + ks * kOffU), blo = dsc0 | (uint64_t)(bu + kLoU + ks * kOffU);
+              const uint32_t ahi = ta + 8 * ks, alo = ahi + 16;
               if (pass == 0) {
-                mma_tf32_ta(d, alo, sdesc(sb + off, lbo, 128), idesc, (i | ks) ? 1u : 0u);
-                mma_tf32_ta(d, ahi, sdesc(sbl + off, lbo, 128), idesc, 1u);
+                mma_tf32_ta(d, alo, bhi, idesc, (i | ks) ? 1u : 0u);
+                mma_tf32_ta(d, ahi, blo, idesc, 1u);
               } else {
-                mma_tf32_ta(d, ahi, sdesc(sb + off, lbo, 128), idesc, 1u);
+                mma_tf32_ta(d, ahi, bhi, idesc, 1u);
               }
             }
           }
@@ -252,7 +274,9 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
       }
       Copier cp{raw0 + (size_t)slot * RAWB, &rawfull[slot], 0u};
       load(c, lane, cp);
-      cp_async_mbar_arrive(&rawfull[slot]);
+      // (an arrival per lane with element copies: many arrivals on one
+      // mbarrier serialise, so lanes without any skip it)
+      if (cp.async) cp_async_mbar_arrive(&rawfull[slot]);
       __syncwarp();
       const uint32_t total = __reduce_add_sync(0xffffffffu, cp.bytes);
       if (lane == 0) mbar_arrive_expect_tx(&rawfull[slot], total);

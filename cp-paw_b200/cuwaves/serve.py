@@ -43,6 +43,7 @@ def _bind():
         P, LL = C.c_void_p, C.c_longlong
         sig = {
             "create": [C.c_size_t, C.c_int, C.POINTER(P)],
+            "set_max_active": [P, C.c_int],
             "submit": [P, C.POINTER(Request), C.POINTER(LL)],
             "poll": [P, LL, _I, _I, _D, _D, _D],
             "error": [P, LL, C.c_char_p, C.c_int],
@@ -68,13 +69,15 @@ def _ptr(a, t):
 class Server:
     """Continuous-batching request loop over wave-function sets on one GPU."""
 
-    def __init__(self, hbm_budget: int, workers: int = 4):
+    def __init__(self, hbm_budget: int, workers: int = 4, max_active: Optional[int] = None):
         self._f = _bind()
         h = C.c_void_p()
         rc = self._f["create"](C.c_size_t(int(hbm_budget)), int(workers), C.byref(h))
         if rc:
             raise WavesError(rc, "server_create", "invalid budget or worker count")
         self.h = h
+        if max_active is not None:
+            self._f["set_max_active"](h, int(max_active))
         self._keep = {}
         self._nat = {}
 

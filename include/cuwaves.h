@@ -196,6 +196,10 @@ typedef struct cuw_request {
 #define CUW_REQ_BORROW 1
 
 int cuwaves_server_create(size_t hbm_budget, int nworkers, cuw_server** out);
+/* At most max_active sets are admitted at a time (default 4 * nworkers): the
+ * admitted sets share the workers in turn, so the cap trades throughput
+ * (overlap on the device) against the latency of the sets already running. */
+int cuwaves_server_set_max_active(cuw_server* s, int max_active);
 /* CUW_ERR_NOMEM when the request alone exceeds the budget. */
 int cuwaves_server_submit(cuw_server* s, const cuw_request* r, long long* id);
 /* *done = 1 once the request has finished; then *status is its own CUW_* code,
