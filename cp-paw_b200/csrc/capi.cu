@@ -390,19 +390,27 @@ static void free_all(Handle* h) {
   h->g = Device();
 }
 
+// message of the calling thread's last failed cuwaves_create (its handle is gone)
+static thread_local std::string t_create_err;
+
 extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
-  if (!dims || !out) return CUW_ERR_ARG;
+  auto bad = [](int code, const char* m) {
+    t_create_err = m;
+    return code;
+  };
+  if (!dims || !out) return bad(CUW_ERR_ARG, "null argument");
   *out = nullptr;
   const cuw_dims& d = *dims;
   if (d.ngl <= 0 || d.nb <= 0 || d.nat < 0 || d.nsp <= 0 || d.nsp > CUW_MAXSP || d.nr1 <= 0 || d.nr2 <= 0 ||
       d.nr3 <= 0 || d.lmx <= 0 || (d.nat > 0 && !d.isp))
-    return CUW_ERR_ARG;
-  if (d.ndim != 1 || !d.tinv || (d.nb % 2) || d.nbh != d.nb / 2) return CUW_ERR_UNSUPPORTED;
-  if (d.precision != CUW_PREC_FP64 && d.precision != CUW_PREC_MIXED) return CUW_ERR_ARG;
+    return bad(CUW_ERR_ARG, "invalid dimensions");
+  if (d.ndim != 1 || !d.tinv || (d.nb % 2) || d.nbh != d.nb / 2)
+    return bad(CUW_ERR_UNSUPPORTED, "only scalar Gamma-point super wave functions with an even band count");
+  if (d.precision != CUW_PREC_FP64 && d.precision != CUW_PREC_MIXED) return bad(CUW_ERR_ARG, "unknown precision");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
-    return CUW_ERR_CUDA;
+    return bad(CUW_ERR_CUDA, "no CUDA device");
   }
   Handle* h = new Handle();
   h->d = d;
@@ -414,18 +422,18 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     h->isp[a] = dims->isp[a] - 1;
     if (h->isp[a] < 0 || h->isp[a] >= d.nsp) {
       delete h;
-      return CUW_ERR_ARG;
+      return bad(CUW_ERR_ARG, "atom species index out of range");
     }
   }
   h->lmnx.resize(d.nsp);
   h->ibpro.resize(d.nsp);
   int nbare = 0;
   for (int s = 0; s < d.nsp; ++s) {
-    if (d.lnx[s] <= 0 || d.lnx[s] > CUW_MAXLN) { delete h; return CUW_ERR_ARG; }
+    if (d.lnx[s] <= 0 || d.lnx[s] > CUW_MAXLN) { delete h; return bad(CUW_ERR_ARG, "projector count out of range"); }
     int n = 0;
     for (int ln = 0; ln < d.lnx[s]; ++ln) {
       int l = d.lox[s][ln];
-      if (l < 0 || (l + 1) * (l + 1) > d.lmx) { delete h; return CUW_ERR_ARG; }
+      if (l < 0 || (l + 1) * (l + 1) > d.lmx) { delete h; return bad(CUW_ERR_ARG, "angular momentum above lmx"); }
       n += 2 * l + 1;
     }
     h->lmnx[s] = n;
@@ -450,7 +458,10 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
   h->occ_h.assign(d.nb, 0.0);
   int rc = CUW_OK;
   do {
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = CUW_ERR_CUDA; break; }
+    if (cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking); e != cudaSuccess) {
+      rc = h->fail(CUW_ERR_CUDA, std::string("cudaStreamCreateWithFlags: ") + cudaGetErrorString(e));
+      break;
+    }
     Device& g = h->g;
     const size_t nps = (size_t)h->ldg * d.nbh * sizeof(double2);
     const size_t npj = (size_t)d.nbh * std::max(1, h->npro) * sizeof(double2);
@@ -488,8 +499,9 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     TRYA(g.scal, sizeof(double) * (size_t)(2 * d.nb + 16));
 #undef TRYA
     if (rc != CUW_OK) break;
-    if (cudaMemcpy(g.pdesc, h->pdesc.data(), sizeof(ProDesc) * h->npro, cudaMemcpyHostToDevice) != cudaSuccess) {
-      rc = CUW_ERR_CUDA;
+    if (cudaError_t e = cudaMemcpy(g.pdesc, h->pdesc.data(), sizeof(ProDesc) * h->npro, cudaMemcpyHostToDevice);
+        e != cudaSuccess) {
+      rc = h->fail(CUW_ERR_CUDA, std::string("cudaMemcpy of the projector table: ") + cudaGetErrorString(e));
       break;
     }
     rc = small_tables_setup(h);
@@ -497,6 +509,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     if (rc == CUW_OK && h->mixed()) rc = tc_setup(h);
   } while (0);
   if (rc != CUW_OK) {
+    t_create_err = h->err.empty() ? "handle set-up failed" : h->err;
     free_all(h);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -520,7 +533,8 @@ extern "C" int cuwaves_destroy(cuw_handle* hp) {
 extern "C" int cuwaves_last_error(const cuw_handle* hp, char* buf, int len) {
   if (!buf || len <= 0) return CUW_ERR_ARG;
   const Handle* h = reinterpret_cast<const Handle*>(hp);
-  std::snprintf(buf, (size_t)len, "%s", h ? h->err.c_str() : "null handle");
+  // without a handle: the calling thread's last failed cuwaves_create
+  std::snprintf(buf, (size_t)len, "%s", h ? h->err.c_str() : t_create_err.c_str());
   return CUW_OK;
 }
 

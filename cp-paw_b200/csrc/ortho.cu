@@ -988,7 +988,12 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
     if (e == cudaSuccess) launched = true;
     else cudaGetLastError();
   }
-  if (!launched) return h->fail(CUW_ERR_UNSUPPORTED, "k_ortho_x: no cluster configuration fits NB");
+  if (!launched) {
+    if (e != cudaSuccess && e != cudaErrorInvalidValue && e != cudaErrorInvalidConfiguration &&
+        e != cudaErrorInvalidClusterSize && e != cudaErrorLaunchOutOfResources)
+      return h->fail(CUW_ERR_CUDA, std::string("k_ortho_x: ") + cudaGetErrorString(e));
+    return h->fail(CUW_ERR_UNSUPPORTED, "k_ortho_x: no cluster configuration fits NB");
+  }
   ++h->launches;
   CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));

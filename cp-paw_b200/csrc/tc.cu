@@ -42,7 +42,7 @@ constexpr int kRawGemm = 36864;   // A, B 128 rows x 16 doubles (144-byte rows, 
 using ProjPipe = tc::Pipe<kNSplit, 8, kRawProj>;
 using AddproPipe = tc::Pipe<kNSplit, 8, kRawAddpro>;
 using GramPipe = tc::Pipe<kNSplit, 6, kRawGram>;
-using AddxPipe = tc::Pipe<kNSplit, 3, kRawAddx>;
+using AddxPipe = tc::Pipe<6, 4, kRawAddx>;
 using ForcePipe = tc::Pipe<kNSplit, 6, kRawForce>;
 using GemmPipe = tc::Pipe<kNSplit, 2, kRawGemm, false>;
 constexpr int kThreads = ProjPipe::kThreads;

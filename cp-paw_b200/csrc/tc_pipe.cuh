@@ -53,6 +53,14 @@ constexpr float kLossPerStep = 0.25f * 1.1920928955078125e-7f;
 template <int NSPLIT, int NRAW, int RAWB, bool BPRE = true, int CPR = 2, int NREG = 2>
 struct Pipe {
   static_assert(NRAW >= 2 && NSPLIT >= 2 * CPR, "stage counts");
+  // The two converter groups take alternate chunks.  With an even slot count
+  // every raw slot belongs to one group, whose waits on it are never more than
+  // one phase ahead of the barrier.  With an odd count a group can wait on
+  // phase k+2 of a slot while phase k+1 (the other group's chunk, whose copies
+  // may land after later ones) is still open, and the parity wait then passes
+  // on phase k.  (Stages need no such rule: the MMAs that free them complete
+  // in issue order.)
+  static_assert(NRAW % 2 == 0, "raw slot count must be even");
   static_assert(128 * NREG + 32 * NSPLIT <= 512, "TMEM: accumulator regions and A stages");
   static_assert(RAWB % 1024 == 0, "raw slots keep the 1024-byte alignment of swizzled TMA boxes");
   static constexpr int kRows = 128;                 // A rows = TMEM lanes = B rows (N)

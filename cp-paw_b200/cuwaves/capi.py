@@ -146,7 +146,9 @@ class Waves:
         h = C.c_void_p()
         rc = fns["create"](C.byref(d), C.byref(h))
         if rc:
-            raise WavesError(rc, "create", "invalid dimensions")
+            buf = C.create_string_buffer(512)
+            fns["last_error"](None, buf, 512)
+            raise WavesError(rc, "create", buf.value.decode(errors="replace"))
         self.h = h
         self.ngl, self.nb, self.nbh, self.nat = d.ngl, d.nb, d.nbh, d.nat
         self.npro = sum(sum(2 * l + 1 for l in inputs["lox"][s - 1]) for s in self._isp.tolist())

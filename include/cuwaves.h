@@ -71,7 +71,8 @@ typedef struct cuw_dims {
 /* Replaces the WVSET allocation of WAVES$INITIALIZE (src/paw_waves1.f90:1187-1450). */
 int cuwaves_create(const cuw_dims* dims, cuw_handle** out);
 int cuwaves_destroy(cuw_handle* h);
-/* Copies the last error message (NUL-terminated, truncated to len). */
+/* Copies the last error message (NUL-terminated, truncated to len); with
+ * h == NULL, the message of the calling thread's last failed cuwaves_create. */
 int cuwaves_last_error(const cuw_handle* h, char* buf, int len);
 /* 0: every call waits for its work (default); 1: calls only enqueue. */
 int cuwaves_set_async(cuw_handle* h, int async);

@@ -144,3 +144,39 @@ def test_handles_of_different_grids_interleave():
                 w.cp_step(move_atoms=True)
         for w in (a, b, c):
             w.close()
+
+
+def test_concurrent_sets_match_alone():
+    """Mixed-precision sets of serving size stepped at the same time from
+    several host threads (each on its own stream, so that the kernels of
+    different sets share the SMs) give bit for bit the results of the same
+    sets run one at a time."""
+    import threading
+
+    specs = [("Si", 32, 1), ("W", 8, 1), ("Si", 64, 1), ("W", 4, 2), ("Si", 16, 1), ("Si", 32, 2), ("W", 16, 1)]
+    inps = [systems.build_inputs(systems.serving_system(k, n, s)) for k, n, s in specs]
+    nsteps = 4
+
+    def run(inp, out, i):
+        w = cuwaves.open_waves(inp, precision=CUW_PREC_MIXED).setup().initialize()
+        res = []
+        for _ in range(nsteps):
+            o, f = w.cp_step(move_atoms=True)
+            res.append((o.copy(), f.copy()))
+        w.close()
+        out[i] = res
+
+    alone = [None] * len(inps)
+    for i, inp in enumerate(inps):
+        run(inp, alone, i)
+    for _ in range(2):
+        mixed = [None] * len(inps)
+        th = [threading.Thread(target=run, args=(inp, mixed, i)) for i, inp in enumerate(inps)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        for i, spec in enumerate(specs):
+            assert mixed[i] is not None, spec
+            for step, ((oa, fa), (om, fm)) in enumerate(zip(alone[i], mixed[i])):
+                assert np.array_equal(oa, om) and np.array_equal(fa, fm), (spec, step)
