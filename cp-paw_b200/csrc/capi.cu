@@ -454,6 +454,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     h->npro += h->lmnx[s];
   }
   h->ldg = ceil_div(d.ngl, 32) * 32;
+  h->lyap_tol = d.precision == CUW_PREC_MIXED ? 1e-3 : 1e-6;
   h->nr = (size_t)d.nr1 * d.nr2 * d.nr3;
   h->occ_h.assign(d.nb, 0.0);
   int rc = CUW_OK;
@@ -1009,4 +1010,16 @@ extern "C" int cuwaves_get_ortho_stats(cuw_handle* hp, double* out, int n) {
   const double v[5] = {(double)h->n_rediag, (double)st[8], (double)st[4], (double)st[1], (double)h->n_fp_fail};
   for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
   return CUW_OK;
+}
+
+extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
+  H(hp);
+  switch (option) {
+    case CUW_OPT_LYAP_TOL:
+      if (!(value >= 0.0 && value < 0.1)) return h->fail(CUW_ERR_ARG, "LYAP_TOL must be in [0, 0.1)");
+      h->lyap_tol = value;
+      return CUW_OK;
+    default:
+      return h->fail(CUW_ERR_ARG, "unknown option");
+  }
 }

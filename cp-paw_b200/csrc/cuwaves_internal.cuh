@@ -159,6 +159,12 @@ struct Handle {
   bool tc_on() const { return mixed() && !fp64_only; }
   long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
   long long n_fp_fail = 0; // Lyapunov fixed-point solves that fell back to a rediagonalisation
+  // relative accuracy to which each ORTHO_X iteration solves its Lyapunov
+  // equation (0: to rounding).  Measured on Si64 over 40 CP steps against the
+  // solve to rounding: 1e-6 moves the FP64 total energy by 3e-12 Ha and the
+  // forces by 1e-13 Ha/bohr with 40% of the sweeps; 1e-3 moves it by 1e-8 Ha,
+  // far inside the mixed path's own error.
+  double lyap_tol = 0.0;
   bool tc_scope_open = false;
   const double* eigr_src = nullptr;  // position buffer (r0, rp or rm) that EIGR (and the fp32 table) was built from
   Device g;

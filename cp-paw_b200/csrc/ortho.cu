@@ -226,6 +226,7 @@ struct OrthoArgs {
   double* tb;     // E X
   int* inner;     // total inner iterations (diagnostics)
   int fast;       // lyap_fast applies (n <= 128, tiles of at most 32 x 32)
+  double lyap_tol;  // relative accuracy of the Lyapunov solve (0: rounding)
 };
 
 // C(tile) = op(A) * op(B); op = transpose when tA / tB.  The tile
@@ -372,10 +373,13 @@ __device__ __forceinline__ void csync() { cg::this_cluster().sync(); }
 // Convergence rule of the Lyapunov fixed point (shared by both loops): true to
 // stop; `failed` when the contraction is too slow (the earlier eigenbasis is
 // too far from the current one) or there is no convergence within the limit.
-__device__ __forceinline__ bool lyap_stop(double gdx, double gxm, double& prev, int it2, int max_inner,
+__device__ __forceinline__ bool lyap_stop(double gdx, double gxm, double& prev, int it2, int max_inner, double tol,
                                           bool& failed) {
   const double ratio = gdx / prev;
   prev = gdx;
+  // requested accuracy reached (the sweep's change bounds the error of a
+  // contraction well below one)
+  if (gdx <= tol * gxm) return true;
   // converged: change at rounding level, or stalled just above it
   if (gdx <= 4e-16 * gxm || (gdx <= 1e-13 * gxm && ratio > 0.5)) return true;
   if ((it2 >= 4 && ratio > 0.6) || it2 == max_inner - 1 || !(gdx <= 1e200)) {
@@ -521,7 +525,7 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
     xnext = tmpx;
     if (rank == 0 && tid == 0) a.inner[0] += 1;
     const double ratio = gdx / prev;
-    if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, failed)) break;
+    if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, a.lyap_tol, failed)) break;
     if (it2 == 2) {
       rho = fmin(0.9, fmax(0.05, 1.1 * ratio));
       omega = 1.0 / (1.0 - 0.5 * rho * rho);
@@ -649,7 +653,7 @@ __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
         xcur = xnext;
         xnext = tmpx;
         if (rank == 0 && tid == 0) a.inner[0] += 1;
-        if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, fp_failed)) break;
+        if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, a.lyap_tol, fp_failed)) break;
       }
     }
     if (fp_failed) {
@@ -936,6 +940,7 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
   a.xb = g.xb;
   a.tb = g.tb;
   a.inner = g.ostatus + 8;
+  a.lyap_tol = h->lyap_tol;
   // cluster of 16 CTAs (non-portable size), else 8, 4, ... ; tile rows/cols
   // per CTA are at most 16*MR x 16*MC with MR, MC in {1,2,4}
   cudaLaunchConfig_t cfg = {};

@@ -19,6 +19,7 @@ CUW_MAXSP = 16
 CUW_MAXLN = 8
 CUW_PSI0, CUW_PSIM, CUW_HPSI, CUW_OPSI = 0, 1, 2, 3
 CUW_PREC_FP64, CUW_PREC_MIXED = 0, 1
+CUW_OPT_LYAP_TOL = 1
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
@@ -84,6 +85,7 @@ OPTIONAL = {
     "get_timing": [_P, _D, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "get_stream": [_P, C.POINTER(C.c_void_p)],
     "get_ortho_stats": [_P, _D, C.c_int],
+    "set_option": [_P, C.c_int, C.c_double],
     "tc_gemm_check": [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P],
     # device-pointer variant without allocation (no handle)
     "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
@@ -332,6 +334,9 @@ class Waves:
 
     PHASES = ("reductions", "structure factors", "forces", "fft_vpsi", "addpro_propagate",
               "projections", "gram", "ortho_solve", "rotate", "bookkeeping")
+
+    def set_option(self, option: int, value: float):
+        self._chk(self._f["set_option"](self.h, int(option), float(value)), "set_option")
 
     def set_timing(self, on: bool):
         self._chk(self._f["set_timing"](self.h, int(on)), "set_timing")

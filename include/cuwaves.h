@@ -240,8 +240,17 @@ int cuwaves_get_stream(cuw_handle* h, void** stream);
  * so far, out[2] Jacobi sweeps of the last eigendecomposition, out[3] ORTHO_X
  * iterations of the last solve, out[4] solves whose fixed point in the earlier
  * eigenbasis converged too slowly and were redone after a rediagonalisation.
- * n values are written. */
+ * n values (at most 5) are written. */
 int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
+/* Tuning options (no reference counterpart).
+ * CUW_OPT_LYAP_TOL: relative accuracy to which every ORTHO_X iteration solves
+ * its Lyapunov equation S X + X S = Gamma (the reference solves it exactly by
+ * diagonalising S).  0 = to rounding; default 1e-6 (FP64) and 1e-3 (mixed
+ * precision).  The ORTHO_X loop itself still stops on
+ * max|<psi|O|psi> - 1| < eps, so a looser inner solve changes the iteration
+ * path, not the constraint that the result satisfies. */
+#define CUW_OPT_LYAP_TOL 1
+int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Check of the split-precision tensor-core product (no reference
  * counterpart): C(M,N) = A(M,K) * B(N,K)^T on device buffers, FP64 row-major
  * with K contiguous, computed as three tf32 tcgen05 products (hi*hi + hi*lo +
