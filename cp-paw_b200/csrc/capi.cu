@@ -19,7 +19,7 @@
 namespace cuw {
 
 int unravel_run(Handle* h, const double2* pw, const double2* oc, int npair, double* o0, double* o1, double* o2);
-int jacobi_run(Handle* h, const double* s_dev, double* u, double* e);
+int jacobi_run(Handle* h, const double* s_dev, double* u, double* e, const int* gate);
 int lambda_init_run(Handle* h);
 int store_lambda_run(Handle* h);
 int ortho_y_run(Handle* h, const double* s, double* x);
@@ -282,7 +282,8 @@ static int force_dev_run(Handle* h, double* force_dev) {
 
 // the part of WAVES$ORTHOGONALIZE after OPSI is formed (src/paw_waves2.f90:242-490)
 static int mark(Handle* h, int phase);
-static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
+// (enqueues only: the solve's status is read with the step's results)
+static int ortho_core(Handle* h, int max_iter, double eps) {
   Device& g = h->g;
   // projections of PSIBAR and OPSI at R(+)
   CUW_RET(mark(h, 1));
@@ -314,10 +315,7 @@ static int ortho_core(Handle* h, int max_iter, double eps, int* iters) {
   CUW_RET(unravel_run(h, pw, oc, 3, g.mat, g.omat, g.oomat));
   CUW_RET(mark(h, 7));
   CUW_RET(lambda_init_run(h));
-  int it = 0;
-  int st = ortho_solve(h, max_iter, eps, &it);
-  if (iters) *iters = it;
-  if (st != CUW_OK) return st;
+  CUW_RET(ortho_solve(h, max_iter, eps));
   CUW_RET(mark(h, 8));
   CUW_RET(lambda12_run(h, g.lam, g.lam1c, g.lam2c));
   CUW_RET(addopsi_run(h, g.psim, g.opsi, g.lam1c, g.lam2c));
@@ -525,6 +523,7 @@ extern "C" int cuwaves_destroy(cuw_handle* hp) {
   H(hp);
   cudaStreamSynchronize(h->stream);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  h->drop_graphs();
   free_all(h);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -555,6 +554,7 @@ extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* min
                                 const double* gvec, const double* g2, const double* pro, const double* ylm,
                                 const double* mpsi, const double* bucket, double gweight) {
   H(hp);
+  h->touch();
   h->eigr_src = nullptr;
   NEED(igvec && minusg && gbas && gvec && g2 && pro && ylm && mpsi, CUW_ERR_ARG, "null argument");
   NEED(gweight > 0.0, CUW_ERR_ARG, "gweight must be the positive cell volume");
@@ -621,6 +621,7 @@ extern "C" int cuwaves_set_dh(cuw_handle* hp, int lmnxx, const double* dh) {
 
 extern "C" int cuwaves_set_do(cuw_handle* hp, int lnxx, const double* dover) {
   H(hp);
+  h->touch();
   NEED(dover && lnxx >= h->lnxx, CUW_ERR_ARG, "DO: lnxx smaller than the largest LNX");
   const int L = h->lnxx, nsp = h->d.nsp;
   std::vector<double> t((size_t)L * L * nsp);
@@ -643,6 +644,7 @@ extern "C" int cuwaves_set_atoms(cuw_handle* hp, const double* r0, const double*
 
 extern "C" int cuwaves_reset_atoms(cuw_handle* hp, const double* r0) {
   H(hp);
+  h->touch();
   NEED(r0, CUW_ERR_ARG, "null positions");
   const size_t n = sizeof(double) * 3 * h->d.nat;
   h->eigr_src = nullptr;
@@ -664,6 +666,7 @@ extern "C" int cuwaves_get_atoms(cuw_handle* hp, double* rm, double* r0, double*
 
 extern "C" int cuwaves_set_occ(cuw_handle* hp, const double* occ) {
   H(hp);
+  h->touch();
   NEED(occ, CUW_ERR_ARG, "null occupations");
   h->occ_h.assign(occ, occ + h->d.nb);
   CUW_TRY(cudaMemcpy(h->g.occ, occ, sizeof(double) * h->d.nb, cudaMemcpyHostToDevice));
@@ -672,6 +675,7 @@ extern "C" int cuwaves_set_occ(cuw_handle* hp, const double* occ) {
 
 extern "C" int cuwaves_set_dynamics(cuw_handle* hp, double delt, double annee) {
   H(hp);
+  h->touch();
   NEED(delt > 0.0 && annee > -1.0, CUW_ERR_ARG, "DELT must be positive and ANNEE > -1");
   h->delt = delt;
   h->annee = annee;
@@ -690,6 +694,7 @@ static double2* psi_ptr(Handle* h, int which) {
 
 extern "C" int cuwaves_upload_psi(cuw_handle* hp, int which, const double* psi) {
   H(hp);
+  h->touch();
   double2* d = psi_ptr(h, which);
   NEED(d && psi, CUW_ERR_ARG, "bad wave-function selector or null pointer");
   CUW_TRY(cudaMemcpy2DAsync(d, sizeof(double2) * h->ldg, psi, sizeof(double2) * h->d.ngl,
@@ -717,6 +722,7 @@ extern "C" int cuwaves_get_proj(cuw_handle* hp, double* proj) {
 
 extern "C" int cuwaves_set_proj(cuw_handle* hp, const double* proj) {
   H(hp);
+  h->touch();
   CUW_TRY(cudaMemcpyAsync(h->g.proj, proj, sizeof(double2) * h->d.nbh * h->npro, cudaMemcpyHostToDevice, h->stream));
   return h->sync();
 }
@@ -730,12 +736,14 @@ extern "C" int cuwaves_get_rlam0(cuw_handle* hp, double* r) {
 
 extern "C" int cuwaves_set_rlam0(cuw_handle* hp, const double* r) {
   H(hp);
+  h->touch();
   CUW_TRY(cudaMemcpyAsync(h->g.rlam0, r, sizeof(double2) * h->d.nb * h->d.nb, cudaMemcpyHostToDevice, h->stream));
   return h->sync();
 }
 
 extern "C" int cuwaves_projections(cuw_handle* hp) {
   H(hp);
+  h->touch();
   NEED(h->have_gset, CUW_ERR_STATE, "G set not loaded");
   CUW_RET(eigr_compute(h, h->g.r0));
   CUW_RET(proj_compute(h, h->g.psi0, h->g.proj, nullptr, nullptr));
@@ -744,6 +752,7 @@ extern "C" int cuwaves_projections(cuw_handle* hp) {
 
 extern "C" int cuwaves_hpsi(cuw_handle* hp) {
   H(hp);
+  h->touch();
   NEED(h->have_gset && h->have_v && h->have_dh, CUW_ERR_STATE, "G set, potential or DH not loaded");
   CUW_RET(fft_vpsi(h, h->g.psi0, h->g.hpsi, true));
   CUW_RET(hproj_compute(h, h->g.proj, h->g.hproj));
@@ -788,6 +797,7 @@ extern "C" int cuwaves_force(cuw_handle* hp, double* force) {
 
 extern "C" int cuwaves_propagate(cuw_handle* hp) {
   H(hp);
+  h->touch();
   NEED(h->have_hpsi, CUW_ERR_STATE, "HPSI NOT AVAILABLE: EITHER WAVES$ETOT HAS NOT BEEN CALLED OR WAVES$PROPAGATE HAS BEEN CALLED PREVIOUSLY");
   CUW_RET(propagate_run(h));
   h->have_hpsi = false;
@@ -796,13 +806,18 @@ extern "C" int cuwaves_propagate(cuw_handle* hp) {
 
 extern "C" int cuwaves_orthogonalize(cuw_handle* hp, int max_iter, double eps, int* iters) {
   H(hp);
+  h->touch();
   NEED(h->have_gset && h->have_do, CUW_ERR_STATE, "G set or DO not loaded");
   NEED(max_iter > 0 && eps > 0.0, CUW_ERR_ARG, "max_iter and eps must be positive");
   // OPSI = (PSI0 + |p>DO<p|PSI0>) * dt^2/((1+annee) m_G) with PROJ at R(0)
   CUW_RET(oproj_compute(h, h->g.proj, h->g.oproj));
   CUW_RET(eigr_compute(h, h->g.r0));
   CUW_RET(addpro_run(h, ADDPRO_OPSI, nullptr, h->g.oproj));
-  CUW_RET(ortho_core(h, max_iter, eps, iters));
+  CUW_RET(ortho_core(h, max_iter, eps));
+  int st[2];
+  CUW_TRY(cudaMemcpyAsync(st, h->g.ostatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  CUW_RET(ortho_result(h, st, iters));
   // second part of the fictitious kinetic energy (src/paw_waves2.f90:490)
   double e2 = 0.0;
   CUW_RET(band_reduce(h, RED_WAVEKIN, &e2, nullptr));
@@ -812,6 +827,7 @@ extern "C" int cuwaves_orthogonalize(cuw_handle* hp, int max_iter, double eps, i
 
 extern "C" int cuwaves_switch(cuw_handle* hp) {
   H(hp);
+  h->touch();
   std::swap(h->g.psi0, h->g.psim);
   CUW_RET(switch_lambda_run(h));
   h->waveekin1 = h->waveekin2 = 0.0;
@@ -820,6 +836,7 @@ extern "C" int cuwaves_switch(cuw_handle* hp) {
 
 extern "C" int cuwaves_stop(cuw_handle* hp) {
   H(hp);
+  h->touch();
   CUW_TRY(cudaMemcpyAsync(h->g.psim, h->g.psi0, sizeof(double2) * h->ldg * h->d.nbh, cudaMemcpyDeviceToDevice,
                           h->stream));
   h->have_rlamm = false;
@@ -828,6 +845,7 @@ extern "C" int cuwaves_stop(cuw_handle* hp) {
 
 extern "C" int cuwaves_gramschmidt(cuw_handle* hp, int which, const double* r) {
   H(hp);
+  h->touch();
   NEED(h->have_gset && h->have_do, CUW_ERR_STATE, "G set or DO not loaded");
   NEED(which == CUW_PSI0 || which == CUW_PSIM, CUW_ERR_ARG, "Gram-Schmidt acts on PSI0 or PSIM");
   NEED(r, CUW_ERR_ARG, "null positions");
@@ -878,6 +896,7 @@ extern "C" int cuwaves_gramschmidt(cuw_handle* hp, int which, const double* r) {
 // at R(0).  Leaves H|psi> in HPSI; nothing is propagated.
 extern "C" int cuwaves_etot(cuw_handle* hp, double* out, double* force) {
   H(hp);
+  h->touch();
   NEED(h->have_gset && h->have_v && h->have_dh && h->have_do, CUW_ERR_STATE, "inputs not loaded");
   NEED(out != nullptr, CUW_ERR_ARG, "null output");
   Device& g = h->g;
@@ -904,15 +923,12 @@ extern "C" int cuwaves_etot(cuw_handle* hp, double* out, double* force) {
   return CUW_OK;
 }
 
-extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mass, int max_iter, double eps,
-                               double* out, double* force) {
-  H(hp);
-  NEED(h->have_gset && h->have_v && h->have_dh && h->have_do, CUW_ERR_STATE, "inputs not loaded");
-  NEED(!move_atoms || mass, CUW_ERR_ARG, "masses required to move atoms");
+// The launches of one CP step (everything between the host inputs and the
+// results), in the order of TIMESTEP; also the host-side buffer rotation.
+static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   Device& g = h->g;
   double* sc = g.scal;  // [0] ekin [1] etot [2] ekin1 [3] ekin2 [4] eion ; per-band scratch after 8
   double* tmpv = g.scal + 8;
-  h->nev = 0;
   CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_EKIN, tmpv));
   CUW_TRY(cudaMemcpyAsync(sc + 0, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -933,14 +949,12 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   CUW_TRY(cudaMemcpyAsync(sc + 1, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
-    CUW_TRY(cudaMemcpyAsync(g.mass, mass, sizeof(double) * h->d.nat, cudaMemcpyHostToDevice, h->stream));
     if (h->eigr_src == g.rp) h->eigr_src = nullptr;  // R(+) is rewritten
     k_atoms_verlet<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(g.r0, g.rm, g.rp, g.force, g.mass, h->d.nat,
                                                                        h->delt * h->delt);
     CUW_LAUNCH_CHECK("k_atoms_verlet");
   }
-  int iters = 0;
-  CUW_RET(ortho_core(h, max_iter, eps, &iters));
+  CUW_RET(ortho_core(h, max_iter, eps));
   CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
   CUW_TRY(cudaMemcpyAsync(sc + 3, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -948,23 +962,128 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
   if (move_atoms) {
     k_ion_ekin<<<1, 128, sizeof(double) * 3 * h->d.nat, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
     CUW_LAUNCH_CHECK("k_ion_ekin");
-    // ATOMS$SWITCH: R(-) <- R(0), R(0) <- R(+)
-    std::swap(g.rm, g.r0);
-    std::swap(g.r0, g.rp);
-    if (h->eigr_src == g.rp) h->eigr_src = nullptr;
-    CUW_TRY(cudaMemcpyAsync(g.rp, g.r0, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToDevice, h->stream));
+    // ATOMS$SWITCH: R(-) <- R(0), R(0) <- R(+) by copies (the buffers keep
+    // their roles, so a step's launches see the same pointers every time);
+    // R(+) keeps R(0) until the next Verlet step, and EIGR of R(+) is now
+    // EIGR of R(0)
+    const size_t nb3 = sizeof(double) * 3 * h->d.nat;
+    CUW_TRY(cudaMemcpyAsync(g.rm, g.r0, nb3, cudaMemcpyDeviceToDevice, h->stream));
+    CUW_TRY(cudaMemcpyAsync(g.r0, g.rp, nb3, cudaMemcpyDeviceToDevice, h->stream));
+    h->eigr_src = h->eigr_src == g.rp ? g.r0 : nullptr;
   } else {
     CUW_TRY(cudaMemsetAsync(sc + 4, 0, sizeof(double), h->stream));
   }
   std::swap(g.psi0, g.psim);
   CUW_RET(switch_lambda_run(h));
   h->have_hpsi = false;
-  CUW_RET(mark(h, PH_MISC));
+  return mark(h, PH_MISC);
+}
+
+// The step as a CUDA graph when one was captured for the present host-side
+// state (Handle::StepGraph), else captured now; returns false (with nothing
+// enqueued and the host state untouched) when the step must run uncaptured.
+static bool step_graph(Handle* h, int move_atoms, int max_iter, double eps, int* rc) {
+  Device& g = h->g;
+  const void* key[6] = {g.psi0, g.psim, g.r0, g.rm, g.rp, h->eigr_src};
+  const int rlamm = h->have_rlamm ? 1 : 0;
+  for (auto it = h->graphs.begin(); it != h->graphs.end();)  // retire graphs of an earlier epoch
+    if (it->epoch != h->epoch) {
+      cudaGraphExecDestroy(it->exec);
+      it = h->graphs.erase(it);
+    } else {
+      ++it;
+    }
+  for (Handle::StepGraph& sg : h->graphs) {
+    if (std::memcmp(sg.key, key, sizeof(key)) || sg.move != move_atoms || sg.max_iter != max_iter || sg.eps != eps ||
+        sg.rlamm != rlamm)
+      continue;
+    cudaError_t e = cudaGraphLaunch(sg.exec, h->stream);
+    if (e != cudaSuccess) {
+      *rc = h->fail(CUW_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+      return true;
+    }
+    // the host side of the captured step
+    std::swap(g.psi0, g.psim);
+    h->eigr_src = sg.eigr_after;
+    h->have_hpsi = false;
+    h->have_opsi = false;
+    h->have_rlamm = true;
+    h->launches += sg.launches;
+    ++h->graph_replays;
+    *rc = CUW_OK;
+    return true;
+  }
+  // capture; on any failure restore the host state and run uncaptured
+  Device saved = g;
+  const double* eigr_saved = h->eigr_src;
+  const bool hp = h->have_hpsi, ho = h->have_opsi, hr = h->have_rlamm;
+  const long long l0 = h->launches, ep = h->epoch;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  h->capturing = true;
+  const int brc = step_body(h, move_atoms, max_iter, eps);
+  h->capturing = false;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (brc == CUW_OK && e == cudaSuccess && graph && h->epoch == ep)
+    e = cudaGraphInstantiate(&exec, graph, 0);
+  else if (e == cudaSuccess)
+    e = cudaErrorUnknown;
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess || !exec) {
+    cudaGetLastError();
+    g = saved;
+    h->eigr_src = eigr_saved;
+    h->have_hpsi = hp;
+    h->have_opsi = ho;
+    h->have_rlamm = hr;
+    h->launches = l0;
+    h->err.clear();
+    return false;
+  }
+  Handle::StepGraph sg;
+  std::memcpy(sg.key, key, sizeof(key));
+  sg.move = move_atoms;
+  sg.max_iter = max_iter;
+  sg.eps = eps;
+  sg.rlamm = rlamm;
+  sg.epoch = h->epoch;
+  sg.eigr_after = h->eigr_src;
+  sg.launches = h->launches - l0;
+  sg.exec = exec;
+  if (h->graphs.size() >= 12) h->drop_graphs();
+  h->graphs.push_back(sg);
+  e = cudaGraphLaunch(exec, h->stream);
+  *rc = e == cudaSuccess ? CUW_OK : h->fail(CUW_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+  return true;
+}
+
+extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mass, int max_iter, double eps,
+                               double* out, double* force) {
+  H(hp);
+  NEED(h->have_gset && h->have_v && h->have_dh && h->have_do, CUW_ERR_STATE, "inputs not loaded");
+  NEED(!move_atoms || mass, CUW_ERR_ARG, "masses required to move atoms");
+  Device& g = h->g;
+  h->nev = 0;
+  if (move_atoms) CUW_TRY(cudaMemcpyAsync(g.mass, mass, sizeof(double) * h->d.nat, cudaMemcpyHostToDevice, h->stream));
+  // graphs once the eigenbasis exists and every step enqueues the same launches
+  int rc = CUW_OK;
+  const bool graphed = h->use_graphs && !h->timing && h->have_u && h->have_rlamm &&
+                       step_graph(h, move_atoms, max_iter, eps, &rc);
+  if (!graphed) rc = step_body(h, move_atoms, max_iter, eps);
+  if (rc != CUW_OK) return rc;
   double hs[5];
-  CUW_TRY(cudaMemcpyAsync(hs, sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+  int st[2];
+  CUW_TRY(cudaMemcpyAsync(hs, g.scal, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
   CUW_RET(h->tc_status());
+  int iters = 0;
+  CUW_RET(ortho_result(h, st, &iters));
   CUW_RET(collect_marks(h));
   if (out) {
     out[0] = hs[1];
@@ -1007,17 +1126,33 @@ extern "C" int cuwaves_get_ortho_stats(cuw_handle* hp, double* out, int n) {
   int st[16] = {0};
   CUW_TRY(cudaMemcpyAsync(st, h->g.ostatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
-  const double v[5] = {(double)h->n_rediag, (double)st[8], (double)st[4], (double)st[1], (double)h->n_fp_fail};
+  const double v[5] = {(double)st[10], (double)st[8], (double)st[4], (double)st[1], (double)st[9]};
   for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_get_graph_stats(cuw_handle* hp, long long* graphs, long long* replays) {
+  H(hp);
+  if (graphs) *graphs = (long long)h->graphs.size();
+  if (replays) *replays = h->graph_replays;
   return CUW_OK;
 }
 
 extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
   H(hp);
+  h->touch();
   switch (option) {
     case CUW_OPT_LYAP_TOL:
       if (!(value >= 0.0 && value < 0.1)) return h->fail(CUW_ERR_ARG, "LYAP_TOL must be in [0, 0.1)");
       h->lyap_tol = value;
+      return CUW_OK;
+    case CUW_OPT_LYAP_MAX_SWEEPS:
+      if (!(value >= 1.0 && value <= 1000.0)) return h->fail(CUW_ERR_ARG, "LYAP_MAX_SWEEPS must be in [1, 1000]");
+      h->lyap_max_sweeps = (int)value;
+      return CUW_OK;
+    case CUW_OPT_GRAPHS:
+      h->use_graphs = value != 0.0;
+      if (!h->use_graphs) h->drop_graphs();
       return CUW_OK;
     default:
       return h->fail(CUW_ERR_ARG, "unknown option");

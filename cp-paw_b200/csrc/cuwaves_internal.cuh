@@ -145,6 +145,32 @@ struct Handle {
   double waveekin1 = 0.0, waveekin2 = 0.0;
   cudaStream_t stream = nullptr;
   int device = 0, nsm = 148;
+  // CUDA graphs of cuwaves_cp_step.  A step's launches depend on host-side
+  // state only through the PSI0/PSIM swap, the buffer EIGR was built from,
+  // the Lagrange history flag and the arguments; one graph is kept per such
+  // state (two in a run of steps).  `epoch` changes with every call that
+  // could change what a step enqueues otherwise (inputs by value, scratch
+  // reallocation, set-up routines), which retires the graphs.
+  struct StepGraph {
+    const void* key[6];
+    int move = 0, max_iter = 0, rlamm = 0;
+    double eps = 0.0;
+    long long epoch = -1;
+    const double* eigr_after = nullptr;  // EIGR's source buffer after the step
+    long long launches = 0;              // kernels in the graph
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<StepGraph> graphs;
+  long long epoch = 0;
+  bool use_graphs = true;
+  bool capturing = false;
+  long long graph_replays = 0;
+  void touch() { ++epoch; }
+  void drop_graphs() {
+    for (StepGraph& sg : graphs)
+      if (sg.exec) cudaGraphExecDestroy(sg.exec);
+    graphs.clear();
+  }
   // measurement: kernel launches, and per-phase device time of cuwaves_cp_step
   long long launches = 0;
   bool timing = false;
@@ -157,14 +183,13 @@ struct Handle {
   bool mixed() const { return d.precision == CUW_PREC_MIXED; }
   bool fp64_only = false;  // contractions in FP64 even on the mixed path (start-up orthonormalisation)
   bool tc_on() const { return mixed() && !fp64_only; }
-  long long n_rediag = 0;  // full eigendecompositions of CHIPSI so far
-  long long n_fp_fail = 0; // Lyapunov fixed-point solves that fell back to a rediagonalisation
   // relative accuracy to which each ORTHO_X iteration solves its Lyapunov
   // equation (0: to rounding).  Measured on Si64 over 40 CP steps against the
   // solve to rounding: 1e-6 moves the FP64 total energy by 3e-12 Ha and the
   // forces by 1e-13 Ha/bohr with 40% of the sweeps; 1e-3 moves it by 1e-8 Ha,
   // far inside the mixed path's own error.
   double lyap_tol = 0.0;
+  int lyap_max_sweeps = 64;  // sweeps per Lyapunov solve before the fixed point counts as failed
   bool tc_scope_open = false;
   const double* eigr_src = nullptr;  // position buffer (r0, rp or rm) that EIGR (and the fp32 table) was built from
   Device g;
@@ -254,7 +279,8 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc);
 int hproj_compute(Handle* h, const double2* proj, double2* out);
 int oproj_compute(Handle* h, const double2* proj, double2* out);
 int gram_overlaps(Handle* h, double2* projP, double2* projO);
-int ortho_solve(Handle* h, int max_iter, double eps, int* iters);
+int ortho_solve(Handle* h, int max_iter, double eps);
+int ortho_result(Handle* h, const int* st, int* iters);
 int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* l1, const double2* l2);
 int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* l1, const double2* l2);
 int lambda12_run(Handle* h, const double* lam_real, double2* l1, double2* l2);

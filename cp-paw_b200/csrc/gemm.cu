@@ -624,6 +624,9 @@ __global__ void k_oproj(const double2* __restrict__ proj, const double* __restri
 
 int ensure_part(Handle* h, size_t bytes) {
   if (bytes <= h->g.part_bytes) return CUW_OK;
+  // (a step being captured into a graph runs again uncaptured instead)
+  if (h->capturing) return h->fail(CUW_ERR_STATE, "scratch grows during graph capture");
+  h->touch();  // graphs hold the old buffer
   if (h->g.part) cudaFree(h->g.part);
   h->g.part = nullptr;
   h->g.part_bytes = 0;

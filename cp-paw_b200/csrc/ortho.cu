@@ -28,6 +28,21 @@ namespace cuw {
 
 namespace {
 
+// status of k_ortho_x when the Lyapunov fixed point in an earlier eigenbasis
+// does not converge fast enough (internal, never returned to the caller)
+constexpr int kFixedPointFailed = 100;
+// Slots of Device::ostatus used here: [0] status and [1] iterations of the
+// last ORTHO_X solve, [4] Jacobi sweeps of the last eigendecomposition, [8]
+// Lyapunov sweeps so far, [9] solves redone after a rediagonalisation, [10]
+// eigendecompositions so far.
+constexpr int kStFallbacks = 9, kStRediag = 10;
+
+// The rediagonalisation after a failed fixed point is enqueued every step and
+// decided on the device, so that a step holds no host round trip (and can be
+// replayed as a CUDA graph): a gated kernel does nothing unless the ORTHO_X
+// status it is given says that the fixed point failed.
+__device__ __forceinline__ bool gate_closed(const int* gate) { return gate && *gate != kFixedPointFailed; }
+
 // ---------------------------------------------------------------------------
 // T[pair][t] (NBH x NBH complex) -> real (NB x NB) matrices
 //   pw : plane-wave part, t=0 <X|Y>, t=1 sum X(G) Y(-G)     (both times Omega)
@@ -93,8 +108,14 @@ __device__ __forceinline__ int pk(int i, int j) { return i <= j ? (j * (j + 1)) 
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in, int n, double* __restrict__ u_out,
                                                  double* __restrict__ e_out, double* __restrict__ vglob,
                                                  int v_in_smem, double* __restrict__ aglob, int max_sweeps,
-                                                 int* __restrict__ info) {
+                                                 int* __restrict__ ost, const int* __restrict__ gate) {
   extern __shared__ double sm[];
+  if (gate_closed(gate)) return;
+  if (threadIdx.x == 0) {
+    ++ost[kStRediag];
+    if (gate) ++ost[kStFallbacks];
+  }
+  int* info = ost + 4;
   const int np = n / 2;
   // packed n(n+1)/2 matrix in shared memory, or in global memory (aglob) when
   // it does not fit (NB above about 200; through L2, slower, used only for
@@ -227,6 +248,7 @@ struct OrthoArgs {
   int* inner;     // total inner iterations (diagnostics)
   int fast;       // lyap_fast applies (n <= 128, tiles of at most 32 x 32)
   double lyap_tol;  // relative accuracy of the Lyapunov solve (0: rounding)
+  const int* gate;  // gated launch (see gate_closed) or nullptr
 };
 
 // C(tile) = op(A) * op(B); op = transpose when tA / tB.  The tile
@@ -536,12 +558,11 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
   return xcur;
 }
 
-// status of k_ortho_x when the Lyapunov fixed point in an earlier eigenbasis
-// does not converge fast enough (internal, never returned to the caller)
-constexpr int kFixedPointFailed = 100;
-
 template <int MR, int MC>
 __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
+  // (a gated launch reads the gate before any CTA of the cluster can reach
+  // the status write at the end: every CTA leaves together or none does)
+  if (gate_closed(a.gate)) return;
   extern __shared__ double sm[];
   cg::cluster_group cl = cg::this_cluster();
   const int cs = (int)cl.num_blocks(), rank = (int)cl.block_rank();
@@ -703,8 +724,10 @@ __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
 }
 
 // C = op(A) op(B) for n x n matrices, one 32x32 tile per CTA
-__global__ void __launch_bounds__(256) k_small_gemm(const double* A, int tA, const double* B, int tB, int n, double* C) {
+__global__ void __launch_bounds__(256) k_small_gemm(const double* A, int tA, const double* B, int tB, int n, double* C,
+                                                    const int* gate) {
   __shared__ double smA[tile_lda<2, 2>() * 32], smB[tile_ldb<2, 2>() * 32];
+  if (gate_closed(gate)) return;
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
   gemm_tile<2, 2, 32>(A, tA != 0, B, tB != 0, n, i0, min(n, i0 + 32), j0, min(n, j0 + 32), C, smA, smB);
 }
@@ -874,7 +897,7 @@ int lambda12_run(Handle* h, const double* lam_real, double2* l1, double2* l2) {
   return CUW_OK;
 }
 
-int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
+int jacobi_run(Handle* h, const double* s_dev, double* u, double* e, const int* gate) {
   const int n = h->d.nb;
   const size_t packed = (size_t)n * (n + 1) / 2;
   const size_t tab = sizeof(int) * (size_t)(n / 2) * (n / 2 + 1) / 2;
@@ -894,14 +917,15 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e) {
     aglob = h->g.jac_a;
   }
   CUW_TRY(smem_allow((const void*)k_jacobi, (int)smem));
-  int* info = reinterpret_cast<int*>(h->g.ostatus) + 4;
-  k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, aglob, 40, info);
+  k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, aglob, 40, h->g.ostatus, gate);
   CUW_LAUNCH_CHECK("k_jacobi");
   return CUW_OK;
 }
 
 // diag(B) -> e, B with its diagonal removed -> E
-__global__ void k_split_diag(const double* __restrict__ b, int n, double* __restrict__ e, double* __restrict__ emat) {
+__global__ void k_split_diag(const double* __restrict__ b, int n, double* __restrict__ e, double* __restrict__ emat,
+                             const int* gate) {
+  if (gate_closed(gate)) return;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n * n; k += gridDim.x * blockDim.x) {
     const int i = k % n, j = k / n;
     const double v = b[k];
@@ -910,10 +934,16 @@ __global__ void k_split_diag(const double* __restrict__ b, int n, double* __rest
   }
 }
 
+__global__ void k_copy_gated(const double* __restrict__ src, double* __restrict__ dst, int n, const int* gate) {
+  if (gate_closed(gate)) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) dst[k] = src[k];
+}
+
 // One launch of the ORTHO_X iteration (k_ortho_x) with the eigenbasis in
 // g.u / g.eig; use_e: g.u diagonalises an earlier CHIPSI only and g.emat holds
-// the off-diagonal rest.  st = {status, iterations}.
-static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st[2]) {
+// the off-diagonal rest.  Status and iteration count go to g.ostatus[0..1];
+// gate: launch gated on the status of an earlier launch (gate_closed).
+static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, const int* gate) {
   const int n = h->d.nb;
   Device& g = h->g;
   OrthoArgs a;
@@ -935,12 +965,13 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
   a.eps = eps;
   a.emat = g.emat;
   a.use_e = use_e;
-  a.max_inner = 64;
+  a.max_inner = h->lyap_max_sweeps;
   a.gt = g.gt;
   a.xb = g.xb;
   a.tb = g.tb;
   a.inner = g.ostatus + 8;
   a.lyap_tol = h->lyap_tol;
+  a.gate = gate;
   // cluster of 16 CTAs (non-portable size), else 8, 4, ... ; tile rows/cols
   // per CTA are at most 16*MR x 16*MC with MR, MC in {1,2,4}
   cudaLaunchConfig_t cfg = {};
@@ -976,7 +1007,10 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
     else if (mr == 4 && mc == 1) fn = k_ortho_x<4, 1>;
     else if (mr == 1 && mc == 4) fn = k_ortho_x<1, 4>;
     if (!fn) continue;
-    if (cs > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    // (set once per kernel, outside any graph capture: a captured step follows
+    // an uncaptured one)
+    if (cs > 8 && !h->capturing &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
@@ -1000,21 +1034,19 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, int st
     return h->fail(CUW_ERR_UNSUPPORTED, "k_ortho_x: no cluster configuration fits NB");
   }
   ++h->launches;
-  CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
-  CUW_TRY(cudaStreamSynchronize(h->stream));
   return CUW_OK;
 }
 
 // B = U^T S U -> g.work, its diagonal -> g.eig and off-diagonal rest -> g.emat
-static int rotate_to_basis(Handle* h) {
+static int rotate_to_basis(Handle* h, const int* gate) {
   const int n = h->d.nb;
   Device& g = h->g;
   const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
-  k_small_gemm<<<tg, 256, 0, h->stream>>>(g.smat, 0, g.u, 0, n, g.haux);
+  k_small_gemm<<<tg, 256, 0, h->stream>>>(g.smat, 0, g.u, 0, n, g.haux, gate);
   CUW_LAUNCH_CHECK("k_small_gemm");
-  k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 1, g.haux, 0, n, g.work);
+  k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 1, g.haux, 0, n, g.work, gate);
   CUW_LAUNCH_CHECK("k_small_gemm");
-  k_split_diag<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.work, n, g.eig, g.emat);
+  k_split_diag<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.work, n, g.eig, g.emat, gate);
   CUW_LAUNCH_CHECK("k_split_diag");
   return CUW_OK;
 }
@@ -1023,38 +1055,45 @@ static int rotate_to_basis(Handle* h) {
 // call (src/paw_waves2.f90:1905-1915) to solve S X + X S = Gamma.  Here the
 // eigenbasis of an earlier call is kept: X is the fixed point of
 // X <- (GT - E X - X E) / (e_i + e_j) in that basis (U^T S U = diag(e) + E),
-// the same unique Lyapunov solution to rounding.  When the fixed point
-// contracts too slowly the kernel reports it, S is rediagonalised (Jacobi on
-// U^T S U, U <- U V) and the iteration restarts from the saved Lambda.
-int ortho_solve(Handle* h, int max_iter, double eps, int* iters) {
+// the same Lyapunov solution to the requested accuracy.  When the fixed point
+// contracts too slowly the kernel reports it, and the gated launches after it
+// rediagonalise S (Jacobi on U^T S U, U <- U V) and restart the iteration from
+// the saved Lambda; they do nothing otherwise.  Only enqueues: ortho_result
+// reads the outcome.
+int ortho_solve(Handle* h, int max_iter, double eps) {
   const int n = h->d.nb;
   Device& g = h->g;
-  const size_t nn = (size_t)n * n;
+  const int nn = n * n;
   const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
   k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.smat);
   CUW_LAUNCH_CHECK("k_symmetrize");
-  int st[2] = {0, 0};
   if (h->have_u) {
-    CUW_RET(rotate_to_basis(h));
+    const int* gate = g.ostatus;  // status of the first launch
+    const int cb = std::min(ceil_div(nn, 256), 2 * h->nsm);
+    CUW_RET(rotate_to_basis(h, nullptr));
     CUW_TRY(cudaMemcpyAsync(g.lam0, g.lam, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->stream));
-    CUW_RET(ortho_x_launch(h, 1, max_iter, eps, st));
-    if (st[0] == kFixedPointFailed) {
-      ++h->n_fp_fail;
-      CUW_RET(rotate_to_basis(h));  // g.work was overwritten by the iteration
-      CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig));
-      k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2);
-      CUW_LAUNCH_CHECK("k_small_gemm");
-      std::swap(g.u, g.u2);
-      ++h->n_rediag;
-      CUW_TRY(cudaMemcpyAsync(g.lam, g.lam0, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->stream));
-      CUW_RET(ortho_x_launch(h, 0, max_iter, eps, st));
-    }
+    CUW_RET(ortho_x_launch(h, 1, max_iter, eps, nullptr));
+    CUW_RET(rotate_to_basis(h, gate));  // g.work was overwritten by the iteration
+    CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig, gate));
+    k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2, gate);
+    CUW_LAUNCH_CHECK("k_small_gemm");
+    k_copy_gated<<<cb, 256, 0, h->stream>>>(g.u2, g.u, nn, gate);
+    CUW_LAUNCH_CHECK("k_copy_gated");
+    k_copy_gated<<<cb, 256, 0, h->stream>>>(g.lam0, g.lam, nn, gate);
+    CUW_LAUNCH_CHECK("k_copy_gated");
+    CUW_RET(ortho_x_launch(h, 0, max_iter, eps, gate));
   } else {
-    CUW_RET(jacobi_run(h, g.smat, g.u, g.eig));
+    CUW_RET(jacobi_run(h, g.smat, g.u, g.eig, nullptr));
     h->have_u = true;
-    ++h->n_rediag;
-    CUW_RET(ortho_x_launch(h, 0, max_iter, eps, st));
+    CUW_RET(ortho_x_launch(h, 0, max_iter, eps, nullptr));
   }
+  return CUW_OK;
+}
+
+// Outcome of the last ortho_solve from its device status st = ostatus[0..1]
+// (copied to the host by the caller); the error messages are the reference's
+// (src/paw_waves2.f90:1929-1935, 2007-2014).
+int ortho_result(Handle* h, const int* st, int* iters) {
   if (iters) *iters = st[1];
   if (st[0] == CUW_ERR_NOT_CONVERGED) return h->fail(st[0], "LOOP FOR ORTHOGONALIZATION IS NOT CONVERGED");
   if (st[0] == CUW_ERR_DIVERGED) return h->fail(st[0], "ITERATION LOOP FOR ORTHOGONALIZATION IS ABOUT TO DIVERGE");

@@ -20,6 +20,8 @@ CUW_MAXLN = 8
 CUW_PSI0, CUW_PSIM, CUW_HPSI, CUW_OPSI = 0, 1, 2, 3
 CUW_PREC_FP64, CUW_PREC_MIXED = 0, 1
 CUW_OPT_LYAP_TOL = 1
+CUW_OPT_GRAPHS = 2
+CUW_OPT_LYAP_MAX_SWEEPS = 3
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
@@ -56,6 +58,7 @@ SIGNATURES = {
     "set_do": [_P, C.c_int, _D],
     "set_atoms": [_P, _D, _D],
     "reset_atoms": [_P, _D],
+    "get_atoms": [_P, _D, _D, _D],
     "set_occ": [_P, _D],
     "set_dynamics": [_P, C.c_double, C.c_double],
     "upload_psi": [_P, C.c_int, _D],
@@ -86,6 +89,7 @@ OPTIONAL = {
     "get_stream": [_P, C.POINTER(C.c_void_p)],
     "get_ortho_stats": [_P, _D, C.c_int],
     "set_option": [_P, C.c_int, C.c_double],
+    "get_graph_stats": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "tc_gemm_check": [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P],
     # device-pointer variant without allocation (no handle)
     "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
@@ -220,6 +224,12 @@ class Waves:
         b = None if rp is None else np.ascontiguousarray(rp, dtype=np.float64)
         self._chk(self._f["set_atoms"](self.h, _dptr(a), _dptr(b)), "set_atoms")
 
+    def get_atoms(self):
+        """(R(-), R(0), R(+)) as (NAT, 3) arrays."""
+        rs = [np.zeros((self.nat, 3)) for _ in range(3)]
+        self._chk(self._f["get_atoms"](self.h, _dptr(rs[0]), _dptr(rs[1]), _dptr(rs[2])), "get_atoms")
+        return tuple(rs)
+
     def reset_atoms(self, r0):
         a = np.ascontiguousarray(r0, dtype=np.float64)
         self._chk(self._f["reset_atoms"](self.h, _dptr(a)), "reset_atoms")
@@ -337,6 +347,11 @@ class Waves:
 
     def set_option(self, option: int, value: float):
         self._chk(self._f["set_option"](self.h, int(option), float(value)), "set_option")
+
+    def graph_stats(self) -> tuple:
+        n, r = C.c_longlong(), C.c_longlong()
+        self._chk(self._f["get_graph_stats"](self.h, C.byref(n), C.byref(r)), "get_graph_stats")
+        return n.value, r.value
 
     def set_timing(self, on: bool):
         self._chk(self._f["set_timing"](self.h, int(on)), "set_timing")

@@ -96,6 +96,9 @@ int cuwaves_set_dh(cuw_handle* h, int lmnxx, const double* dh);
 int cuwaves_set_do(cuw_handle* h, int lnxx, const double* dover);
 /* Atomic positions R(0) and R(+) (ATOMLIST 'R(0)', 'R(+)'), each (3,NAT). */
 int cuwaves_set_atoms(cuw_handle* h, const double* r0, const double* rp);
+/* Positions R(-), R(0), R(+) (each (3,NAT), any may be NULL) as ATOMLIST$GETR8A
+ * 'R(-)', 'R(0)', 'R(+)' after the steps this handle has taken. */
+int cuwaves_get_atoms(cuw_handle* h, double* rm, double* r0, double* rp);
 /* Occupations OCC(NB) of this (k,spin) as WAVES_DYNOCCGETR8A('OCC'). */
 int cuwaves_set_occ(cuw_handle* h, const double* occ);
 /* DELT and ANNEE (friction) of WAVES_MODULE (src/paw_waves1.f90:216-218). */
@@ -250,7 +253,17 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * max|<psi|O|psi> - 1| < eps, so a looser inner solve changes the iteration
  * path, not the constraint that the result satisfies. */
 #define CUW_OPT_LYAP_TOL 1
+/* CUW_OPT_GRAPHS: 1 (default) replays cuwaves_cp_step as CUDA graphs, one for
+ * each of the two PSI0/PSIM buffer states of a run of steps, captured on first use and
+ * retired by any other call that changes what a step enqueues; 0 launches
+ * every kernel from the host.  Results are bit-identical either way. */
+#define CUW_OPT_GRAPHS 2
+/* CUW_OPT_LYAP_MAX_SWEEPS: sweeps of the Lyapunov fixed point before it counts
+ * as failed and the solve is redone after a rediagonalisation (default 64). */
+#define CUW_OPT_LYAP_MAX_SWEEPS 3
 int cuwaves_set_option(cuw_handle* h, int option, double value);
+/* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
+int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);
 /* Check of the split-precision tensor-core product (no reference
  * counterpart): C(M,N) = A(M,K) * B(N,K)^T on device buffers, FP64 row-major
  * with K contiguous, computed as three tf32 tcgen05 products (hi*hi + hi*lo +
