@@ -138,6 +138,10 @@ struct Handle {
   bool async = false;
   int nzp = 0;                   // occupied z planes
   int batch = 0;                 // bands per FFT batch
+  int grid_bands = 0;            // bands the FFT work grid has room for
+  // split-K factors of the projections and Gram products, as multiples of the
+  // default (about two waves of CTAs); set by cuwaves_autotune
+  double split_proj = 1.0, split_gram = 1.0;
   AxisPlan ax[3];
   int (*fft_run)(Handle*, const double2*, double2*, bool) = nullptr;  // chosen by fft_setup
   size_t nr = 0;

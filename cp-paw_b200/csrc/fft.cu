@@ -633,6 +633,7 @@ int fft_setup(Handle* h, const int* igvec) {
   CUW_TRY(cudaMalloc(&g.zslot, sizeof(int) * nr3));
   CUW_TRY(cudaMalloc(&g.plane_iz, sizeof(int) * nzp));
   CUW_TRY(cudaMalloc(&g.grid, per_band * batch));
+  h->grid_bands = batch;
   CUW_TRY(cudaMemcpy(g.plane_off, off.data(), sizeof(int) * (nzp + 1), cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(g.plane_g, pg.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(g.plane_pos, pp.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));

@@ -635,8 +635,8 @@ int ensure_part(Handle* h, size_t bytes) {
   return CUW_OK;
 }
 
-static int choose_split(Handle* h, int tiles, int nk, int minchunk) {
-  int want = std::max(1, ceil_div(2 * h->nsm, std::max(1, tiles)));
+static int choose_split(Handle* h, int tiles, int nk, int minchunk, double mul) {
+  int want = std::max(1, (int)std::ceil(2.0 * h->nsm * mul / std::max(1, tiles)));
   int maxs = std::max(1, ceil_div(nk, minchunk));
   return std::min(want, maxs);
 }
@@ -664,7 +664,7 @@ int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* 
   }
   const int nbh = h->d.nbh, npro = h->npro, ngl = h->d.ngl;
   const int tn = ceil_div(npro, BN), tm = ceil_div(nbh, BM);
-  int ks = choose_split(h, tn * tm, ngl, 256);
+  int ks = choose_split(h, tn * tm, ngl, 256, h->split_proj);
   int kchunk = ceil_div(ceil_div(ngl, ks), BK) * BK;
   ks = ceil_div(ngl, kchunk);
   const size_t one = (size_t)ks * nbh * npro;
@@ -758,7 +758,7 @@ static int gram_run(Handle* h, const GramPair* pairs, int npair, bool minus, int
   a.sk = sk;
   a.sm = sm;
   const int tiles = ceil_div(nm, BM) * ceil_div(nm, BN) * npair;
-  int ks = choose_split(h, tiles, nk, 128);
+  int ks = choose_split(h, tiles, nk, 128, h->split_gram);
   a.kchunk = ceil_div(ceil_div(nk, ks), BK) * BK;
   ks = ceil_div(nk, a.kchunk);
   const size_t mn = (size_t)nm * nm;

@@ -90,6 +90,9 @@ size_t estimate_bytes(const cuw_dims& d, const int* isp) {
 
 }  // namespace
 
+// requests with at least this many CP steps replay their steps as CUDA graphs
+constexpr int kGraphSteps = 64;
+
 struct cuw_server {
   size_t budget = 0;
   int max_active = 0;         // admitted sets at most (sets beyond wait in the queue)
@@ -156,6 +159,10 @@ struct cuw_server {
         fail(j, rc, "create");
         return true;
       }
+      // Step graphs pay for their capture and instantiation (two per set)
+      // only over long runs; measured on the serving mix of 20-step requests
+      // they cost a third of the capacity.
+      if (j->nsteps < kGraphSteps) cuwaves_set_option(j->h, CUW_OPT_GRAPHS, 0.0);
       if ((rc = cuwaves_set_gset(j->h, in.igvec, in.minusg, in.gbas, in.gvec, in.g2, in.pro, in.ylm, in.mpsi, nullptr,
                                  j->gweight)) ||
           (rc = cuwaves_set_potential(j->h, in.v)) || (rc = cuwaves_set_dh(j->h, j->lmnxx, in.dh)) ||

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -543,8 +544,8 @@ __global__ void k_minus_copy(const double2* __restrict__ src, double2* __restric
 static int* tc_err(Handle* h) { return h->g.ostatus + 12; }
 
 // number of K splits so that tiles * splits fills the GPU once (one CTA per SM)
-static int tc_splits(Handle* h, int tiles, int nk) {
-  const int want = std::max(1, ceil_div(h->nsm, std::max(1, tiles)));
+static int tc_splits(Handle* h, int tiles, int nk, double mul) {
+  const int want = std::max(1, (int)std::ceil(h->nsm * mul / std::max(1, tiles)));
   return std::max(1, std::min(want, ceil_div(nk, 4 * kCK)));
 }
 
@@ -689,7 +690,7 @@ static int tc_reduce(Handle* h, const float2* part, int nz, size_t n, double sca
 int tc_proj(Handle* h, const double2* psi, double2* proj) {
   const int nbh = h->d.nbh, npro = h->npro, ngl = h->d.ngl;
   const int tn = ceil_div(npro, 128), tb = ceil_div(nbh, 64);
-  int ks = tc_splits(h, tn * tb, ngl);
+  int ks = tc_splits(h, tn * tb, ngl, h->split_proj);
   const int kchunk = ceil_div(ceil_div(ngl, ks), kCK) * kCK;
   ks = ceil_div(ngl, kchunk);
   const size_t n = (size_t)nbh * npro;
@@ -781,7 +782,7 @@ int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int
     a.ybs[i] = a.ybs[0];
   }
   const int tiles = ceil_div(nm, 64) * ceil_div(nm, 64) * npair;
-  int ks = tc_splits(h, tiles, nk);
+  int ks = tc_splits(h, tiles, nk, h->split_gram);
   a.kchunk = ceil_div(ceil_div(nk, ks), kCK) * kCK;
   ks = ceil_div(nk, a.kchunk);
   const size_t mn = (size_t)nm * nm;

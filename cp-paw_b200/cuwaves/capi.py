@@ -90,6 +90,7 @@ OPTIONAL = {
     "get_ortho_stats": [_P, _D, C.c_int],
     "set_option": [_P, C.c_int, C.c_double],
     "get_graph_stats": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "autotune": [_P, _D, C.c_int],
     "tc_gemm_check": [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P],
     # device-pointer variant without allocation (no handle)
     "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
@@ -347,6 +348,13 @@ class Waves:
 
     def set_option(self, option: int, value: float):
         self._chk(self._f["set_option"](self.h, int(option), float(value)), "set_option")
+
+    def autotune(self) -> dict:
+        """Times and fixes the FFT band batch and the split-K factors."""
+        out = np.zeros(7)
+        self._chk(self._f["autotune"](self.h, _dptr(out), len(out)), "autotune")
+        keys = ("fft_batch", "split_proj", "split_gram", "fft_ms", "proj_ms", "gram_ms", "cached")
+        return dict(zip(keys, out.tolist()))
 
     def graph_stats(self) -> tuple:
         n, r = C.c_longlong(), C.c_longlong()

@@ -264,6 +264,15 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);
+/* Autotuner (no reference counterpart; FFTW's planner picks the reference's
+ * FFT plans): times the FFT band batch and the split-K factors of the
+ * projections and plane-wave Gram products on this handle's data (G set, V,
+ * DH, DO and PSI0/PSIM loaded) and keeps the fastest, in a process-wide table
+ * keyed by the shape so that later handles of the same shape reuse it.
+ * out[0..6] (n values): batch, projection split factor, Gram split factor,
+ * their best times in ms, 1 if the choice came from the table.  Results move
+ * at rounding level (another summation order). */
+int cuwaves_autotune(cuw_handle* h, double* out, int n);
 /* Check of the split-precision tensor-core product (no reference
  * counterpart): C(M,N) = A(M,K) * B(N,K)^T on device buffers, FP64 row-major
  * with K contiguous, computed as three tf32 tcgen05 products (hi*hi + hi*lo +

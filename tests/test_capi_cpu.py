@@ -43,7 +43,8 @@ def test_oracle_exports_the_same_abi(oracle):
             continue
         if n in ("cuwaves_set_async", "cuwaves_synchronize", "cuwaves_set_timing", "cuwaves_get_timing",
                  "cuwaves_get_stream", "cuwaves_get_ortho_stats", "cuwaves_projections_noalloc",
-                 "cuwaves_tc_gemm_check", "cuwaves_set_option", "cuwaves_get_graph_stats"):  # device-only entry points
+                 "cuwaves_tc_gemm_check", "cuwaves_set_option", "cuwaves_get_graph_stats",
+                 "cuwaves_autotune"):  # device-only entry points
             continue
         assert hasattr(lib, n.replace("cuwaves_", "orc_")), n
 
