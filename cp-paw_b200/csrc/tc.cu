@@ -52,8 +52,11 @@ constexpr int kBTile = 4096;              // floats of one split B chunk (hi and
 static_assert(ProjPipe::kSmem <= 232448 && GramPipe::kSmem <= 232448 && AddxPipe::kSmem <= 232448 &&
                   GemmPipe::kSmem <= 232448 && ForcePipe::kSmem <= 232448 && AddproPipe::kSmem <= 232448,
               "shared memory");
-// k_tc_force reuses the stage and raw buffers for a 128 x 64 FP64 tile
-static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * (128 * 64 + 3 * 128 + 4 * 192),
+// k_tc_force reuses the stage and raw buffers for a 128 x 64 FP64 tile, rows
+// padded to an odd number of doubles so that the column stores of a warp (one
+// row per lane) spread over the banks
+constexpr int kSvLd = 65;
+static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * (128 * kSvLd + 4 * 128 + 4 * 192),
               "stage area too small");
 
 // offset of 16-byte chunk e of row r in a box with 128-byte (64-byte) rows
@@ -431,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
     for (int i = 0; i < 4; ++i) a_put<false>(v, i, at<double2>(raw, (4 * kh + i) * 2048 + r * 16));
   };
-  // [128][64], over the stage and raw buffers: when a drain thread finishes,
+  // [128][kSvLd], over the stage and raw buffers: when a drain thread finishes,
   // every chunk has been converted and multiplied and no copy is in flight
   double* sv = reinterpret_cast<double*>(tc::pipe_stage_base());
   auto finish = [&](const float (&acc)[ForcePipe::kCols], int row, int col0) {
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const double2 cw = cmul(make_double2(0.0, pr), cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]));
         v = (cw.x * (double)acc[2 * j] + cw.y * (double)acc[2 * j + 1]) * y;
       }
-      sv[row * 64 + pb + j] = v;
+      sv[row * kSvLd + pb + j] = v;
     }
   };
   NoConvertB no_cb;
@@ -456,24 +459,332 @@ __global__ void __launch_bounds__(kThreads, 1)
   // error flag is set and the caller discards the result).  G components of the
   // tile, then fpart = sum_g sv(g,p) G_c(g) in four row quarters combined in a
   // fixed order
-  double* gsh = sv + 128 * 64;  // [3][128]
-  double* qsum = gsh + 3 * 128; // [4][192]
+  double* gsh = sv + 128 * kSvLd;  // [128][4]
+  double* qsum = gsh + 4 * 128;    // [4][192]
   for (int i = threadIdx.x; i < 3 * 128; i += blockDim.x) {
     const int c = i / 128, r = i % 128, g = g0 + r;
-    gsh[i] = g < ngl ? (c == 0 ? gx : (c == 1 ? gy : gz))[g] : 0.0;
+    gsh[4 * r + c] = g < ngl ? (c == 0 ? gx : (c == 1 ? gy : gz))[g] : 0.0;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 4 * 192; i += blockDim.x) {
     const int qr = i / 192, k = i % 192, pl = k / 3, c = k % 3;
     double s = 0.0;
 #pragma unroll 8
-    for (int r = 32 * qr; r < 32 * qr + 32; ++r) s += sv[r * 64 + pl] * gsh[c * 128 + r];
+    for (int r = 32 * qr; r < 32 * qr + 32; ++r) s += sv[r * kSvLd + pl] * gsh[4 * r + c];
     qsum[i] = s;
   }
   __syncthreads();
   for (int k = threadIdx.x; k < 192; k += blockDim.x) {
     const int pl = k / 3, c = k % 3, p = p0 + pl;
     if (p < npro) fpart[((size_t)blockIdx.x * npro + p) * 3 + c] = ((qsum[k] + qsum[192 + k]) + qsum[384 + k]) + qsum[576 + k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forces, persistent form for NBH <= 64 (an even number of K chunks, at most
+// eight): the same D(g,p) = sum_b psi0(g,b) conj(E(b,p)) and force sums as
+// k_tc_force, but one CTA per SM walks a contiguous run of (g tile, projector
+// tile) items.  The split psi0 rows of a g tile (all of K: 8 chunks x 32 TMEM
+// columns) stay in tensor memory for every projector tile of that g tile, so
+// only the pre-split conj(E) chunks stream.  Each item accumulates in one of
+// two TMEM regions (two chunks at a time: cross terms, then hi*hi); the drain
+// warps copy the region to registers and release it at once, so the MMAs of
+// the next items run while the drains form sv(g,p) = Re[i pf(g,p) conj(D)]
+// from the FP32 projector table and the G-weighted column sums of this item.
+//   warp 0   TMEM allocation, MMA issue (one thread)
+//   warp 1   TMA copies of raw psi0 chunks (two raw slots, one per converter group)
+//   warp 2   bulk copies of the split conj(E) chunks into kFNS stages
+//   3..10    converters (two groups of four warps, alternate chunks of a g tile)
+//   11..26   drains and the per-item force epilogue
+// Barriers: rawfull/rawempty (raw psi0 slots), afull[c] (A chunk c of the
+// current g tile in TMEM), afree (MMAs of the last item of a g tile done),
+// sfull/sfree (B stages), bfull/bempty (accumulation regions, one item each).
+// Every wait is bounded; the drain group decides to leave by one vote per item
+// (a reduction barrier all 16 drain warps reach), so none of them is left at a
+// barrier.  The hand-over protocol is model-checked on the CPU
+// (tests/test_pipe_protocol.py).
+// ---------------------------------------------------------------------------
+constexpr int kFNS = 6;        // B stages (16 KB each)
+constexpr int kFMaxChunks = 8; // K chunks of a resident A tile (TMEM columns 256..511)
+constexpr size_t kForcePSmem = (size_t)kFNS * 16384 + 2 * 16384 +
+                               sizeof(double) * (128 * kSvLd + 4 * 128 + 4 * 192) + 1024 + 512;
+static_assert(kForcePSmem <= 232448, "shared memory");
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_force_p(const __grid_constant__ CUtensorMap tm_psi, const float* __restrict__ be, int nchk, int ngl, int npro,
+                 int ldg, int tn, int nitems, const float2* __restrict__ pf, const double* __restrict__ gx,
+                 const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ fpart,
+                 int* __restrict__ err) {
+  using namespace tc;
+  float* st = pipe_stage_base();
+  unsigned char* raw0 = reinterpret_cast<unsigned char*>(st) + (size_t)kFNS * 16384;
+  double* sv = reinterpret_cast<double*>(raw0 + 2 * 16384);  // [128][kSvLd]
+  double* gsh = sv + 128 * kSvLd;                            // [128][4]
+  double* qsum = gsh + 4 * 128;                              // [4][192]
+  uint64_t* rawfull = reinterpret_cast<uint64_t*>(qsum + 4 * 192);
+  uint64_t* rawempty = rawfull + 2;
+  uint64_t* sfull = rawempty + 2;
+  uint64_t* sfree = sfull + kFNS;
+  uint64_t* bfull = sfree + kFNS;
+  uint64_t* bempty = bfull + 2;
+  uint64_t* afull = bempty + 2;
+  uint64_t* afree = afull + kFMaxChunks;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(afree + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long G = gridDim.x;
+  const int w0 = (int)((long long)blockIdx.x * nitems / G), w1 = (int)((long long)(blockIdx.x + 1) * nitems / G);
+  const int m_first = w0 / tn;
+  const int nm = w1 > w0 ? (w1 - 1) / tn - m_first + 1 : 0;  // g tiles of this CTA
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&rawfull[i], 1);
+      mbar_init(&rawempty[i], 128);
+      mbar_init(&bfull[i], 1);
+      mbar_init(&bempty[i], 512);
+    }
+    for (int i = 0; i < kFNS; ++i) {
+      mbar_init(&sfull[i], 1);
+      mbar_init(&sfree[i], 1);
+    }
+    for (int c = 0; c < kFMaxChunks; ++c) mbar_init(&afull[c], 128);
+    mbar_init(afree, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tslot, 512);
+    tmem_relinquish();
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = *tslot;
+  auto raise = [&]() {
+    *abort_flag = 1;
+    atomicExch(err, 1);
+  };
+  if (warp == 0) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_tf32(128, 128);
+      constexpr uint32_t lbo = 128 * 16;
+      const uint64_t dsc0 = sdesc(0, lbo, 128);
+      const uint32_t st0 = smem_u32(st) >> 4;
+      constexpr uint32_t kStageU = 16384u >> 4, kLoU = 8192u >> 4, kOffU = (2 * lbo) >> 4;
+      int it = 0, j = 0;
+      bool ok = true, pending = false;  // pending: MMAs issued since the last bfull commit
+      for (int w = w0; w < w1 && ok && !*abort_flag; ++w, ++it) {
+        const int im = w / tn - m_first, r = it & 1;
+        const bool first_of_m = (w == w0) || (w % tn == 0), last_of_m = (w == w1 - 1) || ((w + 1) % tn == 0);
+        if (it >= 2) ok = mbar_wait(&bempty[r], ((it >> 1) - 1) & 1, kWaitCycles);
+        const uint32_t d = tmem + (uint32_t)(r * 128);
+        for (int rr = 0; rr < nchk / 2 && ok; ++rr, j += 2) {
+          for (int i = 0; i < 2 && ok; ++i) {
+            if (first_of_m) ok = mbar_wait(&afull[2 * rr + i], im & 1, kWaitCycles);
+            if (ok) ok = mbar_wait(&sfull[(j + i) % kFNS], ((j + i) / kFNS) & 1, kWaitCycles);
+          }
+          if (!ok) break;
+          fence_after_sync();
+#pragma unroll
+          for (int pass = 0; pass < 2; ++pass)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int c = 2 * rr + i, s = (j + i) % kFNS;
+              const uint32_t bu = st0 + (uint32_t)s * kStageU;
+              const uint32_t ta = tmem + (uint32_t)(256 + 32 * c);
+#pragma unroll
+              for (int ks = 0; ks < 2; ++ks) {
+                const uint64_t bhi = dsc0 | (uint64_t)(bu + ks * kOffU), blo = dsc0 | (uint64_t)(bu + kLoU + ks * kOffU);
+                const uint32_t ahi = ta + 8 * ks, alo = ahi + 16;
+                if (pass == 0) {
+                  mma_tf32_ta(d, alo, bhi, idesc, (rr | i | ks) ? 1u : 0u);
+                  mma_tf32_ta(d, ahi, blo, idesc, 1u);
+                } else {
+                  mma_tf32_ta(d, ahi, bhi, idesc, 1u);
+                }
+              }
+            }
+          mma_commit(&sfree[j % kFNS]);
+          mma_commit(&sfree[(j + 1) % kFNS]);
+          pending = true;
+        }
+        if (!ok) break;
+        mma_commit(&bfull[r]);
+        pending = false;
+        if (last_of_m) mma_commit(afree);
+      }
+      if (!ok) raise();
+      // the MMAs in flight finish before TMEM is released (after an abort in
+      // the middle of an item, through one more commit on its region)
+      if (pending) {
+        mma_commit(&bfull[it & 1]);
+        mbar_wait(&bfull[it & 1], (it >> 1) & 1, kWaitCycles);
+      } else if (it > 0) {
+        mbar_wait(&bfull[(it - 1) & 1], ((it - 1) >> 1) & 1, kWaitCycles);
+      }
+    }
+  } else if (warp == 1) {
+    // raw psi0 chunks: chunk c of the im-th g tile goes to slot c % 2 (the slot
+    // of converter group c % 2)
+    int issued = 0;
+    const int total = nm * nchk;
+    for (int q = 0; q < total; ++q) {
+      const int slot = q & 1, m = m_first + q / nchk, c = q % nchk;
+      bool ok = true;
+      if (lane == 0) {
+        if (q >= 2) ok = mbar_wait(&rawempty[slot], ((q >> 1) - 1) & 1, kWaitCycles);
+        ok = ok && !*abort_flag;
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) raise();
+        break;
+      }
+      if (lane == 0) {
+        tma_load_2d(raw0 + slot * 16384, &tm_psi, 2 * 128 * m, c * kCK, &rawfull[slot]);
+        mbar_arrive_expect_tx(&rawfull[slot], 16384);
+      }
+      issued = q + 1;
+    }
+    if (*abort_flag && lane == 0)
+      for (int q = max(0, issued - 2); q < issued; ++q) mbar_wait(&rawfull[q & 1], (q >> 1) & 1, kWaitCycles);
+  } else if (warp == 2) {
+    int issued = 0;
+    int j = 0;
+    for (int w = w0; w < w1; ++w) {
+      const int n = w % tn;
+      bool ok = true;
+      for (int c = 0; c < nchk; ++c, ++j) {
+        const int s = j % kFNS;
+        if (lane == 0) {
+          if (j >= kFNS) ok = mbar_wait(&sfree[s], ((j / kFNS) - 1) & 1, kWaitCycles);
+          ok = ok && !*abort_flag;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        if (lane == 0) {
+          bulk_g2s(st + (size_t)s * 4096, be + ((size_t)n * nchk + c) * kBTile, 16384, &sfull[s]);
+          mbar_arrive_expect_tx(&sfull[s], 16384);
+        }
+        issued = j + 1;
+      }
+      if (!ok) {
+        if (lane == 0) raise();
+        break;
+      }
+    }
+    if (*abort_flag && lane == 0)
+      for (int q = max(0, issued - kFNS); q < issued; ++q) mbar_wait(&sfull[q % kFNS], (q / kFNS) & 1, kWaitCycles);
+  } else if (warp < 11) {
+    // converters: group grp owns chunks grp, grp + 2, ... of every g tile
+    const int grp = (warp - 3) >> 2;
+    const int arow = 32 * (warp & 3) + lane;
+    const uint32_t tlane = (uint32_t)(32 * (warp & 3)) << 16;
+    bool ok = true;
+    for (int im = 0; im < nm && ok; ++im) {
+      for (int c = grp; c < nchk; c += 2) {
+        const int q = im * nchk + c, slot = q & 1;
+        bool got = mbar_wait(&rawfull[slot], (q >> 1) & 1, kWaitCycles);
+        if (got && c == grp && im >= 1) got = mbar_wait(afree, (im - 1) & 1, kWaitCycles);
+        ok = __all_sync(0xffffffffu, got && !*abort_flag);
+        if (!ok) {
+          if (lane == 0) raise();
+          break;
+        }
+        const unsigned char* raw = raw0 + slot * 16384;
+#pragma unroll
+        for (int kh = 0; kh < 2; ++kh) {
+          uint32_t hi[8], lo[8];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const double2 x = at<double2>(raw, (4 * kh + i) * 2048 + arow * 16);
+            float h0, l0, h1, l1;
+            split_tf32f((float)x.x, h0, l0);
+            split_tf32f((float)x.y, h1, l1);
+            hi[2 * i] = __float_as_uint(h0), lo[2 * i] = __float_as_uint(l0);
+            hi[2 * i + 1] = __float_as_uint(h1), lo[2 * i + 1] = __float_as_uint(l1);
+          }
+          const uint32_t ta = tmem + tlane + (uint32_t)(256 + 32 * c + 8 * kh);
+          tmem_st8(ta, hi);
+          tmem_st8(ta + 16, lo);
+        }
+        tmem_wait_st();
+        fence_before_sync();
+        mbar_arrive(&afull[c]);
+        mbar_arrive(&rawempty[slot]);
+      }
+    }
+  } else {
+    const int q = warp & 3, dw = warp - 11, col0 = 32 * (dw / 4), dt = tid - 11 * 32;
+    const uint32_t lane_base = ((uint32_t)(32 * q) << 16) + (uint32_t)col0;
+    const int row = 32 * q + lane, pb = col0 / 2;
+    // expected truncation loss: a quarter unit in the last place per K=8 step
+    const float half_ulps = kLossPerStep * (float)(2 * nchk);
+    int it = 0;
+    for (int w = w0; w < w1; ++w, ++it) {
+      const int m = w / tn, n = w % tn, g = m * 128 + row, r = it & 1;
+      bool got = mbar_wait(&bfull[r], (it >> 1) & 1, kWaitCycles);
+      got = __all_sync(0xffffffffu, got && !*abort_flag);
+      float acc[32];
+      if (got) {
+        fence_after_sync();
+        uint32_t v[2][16];
+        tmem_ld16(tmem + lane_base + (uint32_t)(r * 128), v[0]);
+        tmem_ld16(tmem + lane_base + (uint32_t)(r * 128 + 16), v[1]);
+        tmem_wait_ld();
+        fence_before_sync();
+        mbar_arrive(&bempty[r]);  // the region is free for the item after next
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc[k] = untruncate(__uint_as_float(v[k >> 4][k & 15]), half_ulps);
+      }
+      // one decision for the whole drain group, reached by all 16 warps
+      if (bar_or(1, 512, !got)) {
+        if (dt == 0) raise();
+        break;
+      }
+      // G components of the item's g tile ([row][4]: the three components of
+      // a row in different banks); sv(g,p) = Re[i pf(g,p) conj(D)], with the
+      // sixteen table loads of a thread in flight together
+      if (dt < 128) {
+        const int gg = m * 128 + dt;
+        const bool in = gg < ngl;
+        gsh[4 * dt] = in ? gx[gg] : 0.0;
+        gsh[4 * dt + 1] = in ? gy[gg] : 0.0;
+        gsh[4 * dt + 2] = in ? gz[gg] : 0.0;
+      }
+      float2 pfv[16];
+#pragma unroll
+      for (int jx = 0; jx < 16; ++jx) {
+        const int p = n * 64 + pb + jx;
+        pfv[jx] = (g < ngl && p < npro) ? __ldg(&pf[(size_t)p * ldg + g]) : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int jx = 0; jx < 16; ++jx)
+        sv[row * kSvLd + pb + jx] = -(double)pfv[jx].y * (double)acc[2 * jx] + (double)pfv[jx].x * (double)acc[2 * jx + 1];
+      bar_sync(1, 512);
+      // fpart[m][p][c] = sum_g sv(g,p) G_c(g): four row quarters, fixed order
+      for (int t = dt; t < 4 * 192; t += 512) {
+        const int qr = t / 192, k = t % 192, pl = k / 3, c = k % 3;
+        double sum = 0.0;
+#pragma unroll 8
+        for (int rw = 32 * qr; rw < 32 * qr + 32; ++rw) sum += sv[rw * kSvLd + pl] * gsh[4 * rw + c];
+        qsum[t] = sum;
+      }
+      bar_sync(1, 512);
+      if (dt < 192) {
+        const int pl = dt / 3, c = dt % 3, p = n * 64 + pl;
+        if (p < npro)
+          fpart[((size_t)m * npro + p) * 3 + c] = ((qsum[dt] + qsum[192 + dt]) + qsum[384 + dt]) + qsum[576 + dt];
+      }
+      bar_sync(1, 512);
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == 0) {
+    __syncwarp();
+    tmem_dealloc(tmem, 512);
   }
 }
 
@@ -600,6 +911,7 @@ int tc_setup(Handle* h) {
   CUW_TRY(smem_allow((const void*)k_tc_gram<false>, (int)GramPipe::kSmem));
   CUW_TRY(smem_allow((const void*)k_tc_addx, (int)AddxPipe::kSmem));
   CUW_TRY(smem_allow((const void*)k_tc_force, (int)ForcePipe::kSmem));
+  CUW_TRY(smem_allow((const void*)k_tc_force_p, (int)kForcePSmem));
   if (!encode_tiled()) return h->fail(CUW_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   auto alloc = [&](void** p, size_t bytes) -> int {
     if (*p) return CUW_OK;
@@ -838,6 +1150,15 @@ int tc_force(Handle* h, const double2* ded, double* fpart, int* ntile) {
   const float* be = nullptr;
   BSplitSrc b{2, ded, nullptr, (long long)nbh, npro, nbh, 0};
   CUW_RET(tc_bsplit_small(h, b, tn, nchk, 0, &be));
+  if (nchk % 2 == 0 && nchk <= kFMaxChunks) {
+    // persistent form: the psi0 tile stays in tensor memory across projector tiles
+    const int nitems = tm * tn;
+    k_tc_force_p<<<std::min(nitems, h->nsm), kThreads, kForcePSmem, h->stream>>>(
+        tps, be, nchk, ngl, npro, h->ldg, tn, nitems, h->g.pf, h->g.gx, h->g.gy, h->g.gz, fpart, tc_err(h));
+    CUW_LAUNCH_CHECK("k_tc_force_p");
+    *ntile = tm;
+    return CUW_OK;
+  }
   k_tc_force<<<dim3(tm, tn), kThreads, ForcePipe::kSmem, h->stream>>>(tps, be, nchk, ngl, nbh, npro, h->g.pdesc,
                                                                       h->g.ylm, h->g.pro, h->g.eigr, h->g.gx,
                                                                       h->g.gy, h->g.gz, fpart, tc_err(h));

@@ -22,6 +22,7 @@ CASES = {
     "Si8-20Ry": lambda: systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry"),
     "H2O2": lambda: systems.water_box(2, box=10.0, lattice=(2, 1, 1), epw_psi_ry=25.0, grid=(32, 32, 32)),
     "Si64": lambda: systems.named_system("Si64"),
+    "Si32": lambda: systems.serving_system("Si", 32, 1),
 }
 
 
@@ -53,6 +54,18 @@ def test_mixed_projections_and_hpsi(name):
     e = rel(mix.download_psi(CUW_HPSI), ref.download_psi(CUW_HPSI))
     print(f"{name}: H|psi> mixed vs FP64 {e:.2e}")
     assert e < 2e-6
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "Si32", "Si64"])
+def test_mixed_forces_same_state(name):
+    """Forces of one state: the FP64 contraction against the tcgen05 one
+    (Si8: one K chunk, per-tile kernel; Si32 and Si64: 4 and 8 chunks, the
+    persistent kernel with the psi0 tile resident in tensor memory)."""
+    inp, ref, mix = pair(name)
+    fr, fm = ref.force(), mix.force()
+    d = float(np.abs(fm - fr).max())
+    print(f"{name}: forces mixed vs FP64 max |dF| {d:.2e} Ha/bohr (max |F| {np.abs(fr).max():.2e})")
+    assert d < 2e-6
 
 
 @pytest.mark.parametrize("name,nsteps", [("Si8-20Ry", 5), ("H2O2", 5), ("Si64", 3)])

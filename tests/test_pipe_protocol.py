@@ -235,3 +235,174 @@ def test_model_finds_an_odd_raw_slot_count():
             found = True
             break
     assert found
+
+
+def simulate_force(nchk, w0, w1, tn, nstage, seed, conv_warps=2, drain_warps=2, plant=None):
+    """Protocol of the persistent force kernel (k_tc_force_p): items
+    (g tile m, projector tile n) = divmod(w, tn) for w in [w0, w1); the A tile
+    (all nchk chunks) stays resident while the items of one m run; two raw
+    slots, per-chunk afull barriers, one afree barrier, nstage B stages, two
+    accumulation regions holding one item each."""
+    rng = random.Random(seed)
+    m_first = w0 // tn
+    nm = (w1 - 1) // tn - m_first + 1
+    rpi = nchk // 2
+    rawfull = [Bar(1) for _ in range(2)]
+    rawempty = [Bar(conv_warps) for _ in range(2)]
+    afull = [Bar(conv_warps) for _ in range(nchk)]
+    afree = Bar(1)
+    sfull = [Bar(1) for _ in range(nstage)]
+    sfree = [Bar(1) for _ in range(nstage)]
+    bfull = [Bar(1) for _ in range(2)]
+    bempty = [Bar(drain_warps) for _ in range(2)]
+    raw = [None, None]
+    atile = [None] * nchk
+    stage = [None] * nstage
+    region = [None, None]
+    copies, mmas = [], []
+
+    def land(kind, idx, val):
+        if kind == "raw":
+            raw[idx] = val
+            rawfull[idx].complete_tx(1)
+        else:
+            stage[idx] = val
+            sfull[idx].complete_tx(1)
+
+    def copy_a():
+        for q in range(nm * nchk):
+            slot = q & 1
+            if q >= 2:
+                yield rawempty[slot], ((q >> 1) - 1) & 1
+            copies.append(("raw", slot, q))
+            yield None
+            rawfull[slot].arrive(expect_tx=1)
+
+    def copy_b():
+        j = 0
+        for w in range(w0, w1):
+            for c in range(nchk):
+                s = j % nstage
+                if j >= nstage:
+                    yield sfree[s], ((j // nstage) - 1) & 1
+                copies.append(("stage", s, (w, c)))
+                yield None
+                sfull[s].arrive(expect_tx=1)
+                j += 1
+
+    def converter(grp):
+        for im in range(nm):
+            for c in range(grp, nchk, 2):
+                q = im * nchk + c
+                slot = q & 1
+                yield rawfull[slot], (q >> 1) & 1
+                if c == grp and im >= 1 and plant != "no_afree":
+                    yield afree, (im - 1) & 1
+                check(raw[slot] == q, f"converter of A chunk {q} reads slot holding {raw[slot]}")
+                yield None
+                atile[c] = im
+                check(raw[slot] == q, f"raw slot {slot} overwritten during conversion of {q}")
+                afull[c].arrive()
+                rawempty[slot].arrive()
+
+    drained = [-1] * drain_warps
+
+    def mma():
+        it = j = 0
+        for w in range(w0, w1):
+            im = w // tn - m_first
+            first = w == w0 or w % tn == 0
+            last = w == w1 - 1 or (w + 1) % tn == 0
+            r = it & 1
+            if it >= 2:
+                yield bempty[r], ((it >> 1) - 1) & 1
+            check(all(d >= it - 2 for d in drained), f"item {it} written before item {it - 2} was drained")
+            for rr in range(rpi):
+                for i in range(2):
+                    if first:
+                        yield afull[2 * rr + i], im & 1
+                    yield sfull[(j + i) % nstage], ((j + i) // nstage) & 1
+                for i in range(2):
+                    c = 2 * rr + i
+                    check(atile[c] == im, f"MMA of item {w} chunk {c}: A holds tile {atile[c]}")
+                    check(stage[(j + i) % nstage] == (w, c), f"MMA of item {w} chunk {c}: stage holds wrong chunk")
+                mmas.append(("pair", w, rr, j, im))
+                yield None
+                j += 2
+            mmas.append(("item", it, last))
+            it += 1
+
+    def mma_done(kind, *a):
+        if kind == "pair":
+            w, rr, j, im = a
+            for i in range(2):
+                c = 2 * rr + i
+                check(atile[c] == im, f"A chunk {c} overwritten before the MMA of item {w} completed")
+                check(stage[(j + i) % nstage] == (w, c), f"stage overwritten before the MMA of item {w} completed")
+            sfree[j % nstage].arrive()
+            sfree[(j + 1) % nstage].arrive()
+        else:
+            it, last = a
+            region[it & 1] = it
+            bfull[it & 1].arrive()
+            if last:
+                afree.arrive()
+
+    def drain(k):
+        for it in range(w1 - w0):
+            r = it & 1
+            yield bfull[r], (it >> 1) & 1
+            check(region[r] == it, f"drain of item {it} reads {region[r]}")
+            yield None
+            check(region[r] == it, f"region of item {it} overwritten while read")
+            drained[k] = it
+            bempty[r].arrive()
+
+    actors = [copy_a(), copy_b(), mma()]
+    for _ in range(conv_warps):
+        actors += [converter(0), converter(1)]
+    actors += [drain(k) for k in range(drain_warps)]
+    state = {a: next(a, "done") for a in actors}
+    while True:
+        live = [a for a, w in state.items() if w != "done"]
+        ready = [a for a in live if state[a] is None or state[a][0].passes(state[a][1])]
+        choices = [("actor", a) for a in ready] + [("copy", i) for i in range(len(copies))]
+        if mmas:
+            choices.append(("mma", 0))
+        if not choices:
+            check(not live, f"deadlock with {len(live)} roles waiting")
+            break
+        kind, x = rng.choice(choices)
+        if kind == "actor":
+            state[x] = next(x, "done")
+        elif kind == "copy":
+            land(*copies.pop(x))
+        else:
+            mma_done(*mmas.pop(0))
+
+
+def force_stages():
+    m = re.search(r"constexpr int kFNS = (\d+);", TC.read_text())
+    assert m
+    return int(m.group(1))
+
+
+@pytest.mark.parametrize("nchk", [2, 4, 8])
+def test_force_protocol_holds_under_random_interleavings(nchk):
+    ns = force_stages()
+    for (w0, w1, tn) in [(0, 10, 8), (5, 17, 8), (3, 4, 2), (0, 9, 1), (7, 30, 4)]:
+        for seed in range(25):
+            simulate_force(nchk, w0, w1, tn, ns, seed)
+
+
+def test_force_model_finds_a_missing_afree_wait():
+    """Planted mistake in the model: converters that do not wait for the MMAs
+    of the previous g tile overwrite its resident A operand."""
+    found = False
+    for seed in range(300):
+        try:
+            simulate_force(4, 0, 12, 2, force_stages(), seed, plant="no_afree")
+        except Violation:
+            found = True
+            break
+    assert found
