@@ -246,24 +246,48 @@ __global__ void __launch_bounds__(kThreads, 1)
     const double rm = 1.0 / mpsi[g];
     const bool hcol = col0 < 64;  // columns 0..63: C1 (H) products, 64..127: C2 (O)
     const int bl0 = (col0 & 63) / 2;
+    // columns in groups of kB whose loads are all issued before any store of
+    // the group (the arrays may alias as far as the compiler knows, so a load
+    // after a store would wait for it: one memory round trip per group, not
+    // two per column)
+    constexpr int kB = 2;
 #pragma unroll
-    for (int j = 0; j < kNC; ++j) {
-      const int b = b0 + bl0 + j;
-      if (b >= nbh) continue;
-      const size_t k = (size_t)g + (size_t)ldg * b;
-      const double2 v = make_double2((double)acc[2 * j], (double)acc[2 * j + 1]);
-      if (hcol && USE_H) {
-        const double2 hv = cadd(hpsi[k], v);
-        hpsi[k] = hv;
-        if (MODE == ADDPRO_FUSED) {
-          const double2 p0v = psi0[k], pm = psim[k];
-          const double a3 = sc.a3 * rm;
-          psim[k] = make_double2(sc.a1 * p0v.x + sc.a2 * pm.x + a3 * hv.x, sc.a1 * p0v.y + sc.a2 * pm.y + a3 * hv.y);
+    for (int j0 = 0; j0 < kNC; j0 += kB) {
+      double2 hv[kB], p0v[kB], pm[kB];
+      size_t k[kB];
+      bool ok[kB];
+#pragma unroll
+      for (int q = 0; q < kB; ++q) {
+        const int b = b0 + bl0 + j0 + q;
+        ok[q] = b < nbh;
+        k[q] = (size_t)g + (size_t)ldg * (ok[q] ? b : 0);
+        if (hcol && USE_H) {
+          hv[q] = ok[q] ? hpsi[k[q]] : dz();
+          if (MODE == ADDPRO_FUSED) {
+            p0v[q] = ok[q] ? psi0[k[q]] : dz();
+            pm[q] = ok[q] ? psim[k[q]] : dz();
+          }
+        } else if (!hcol && USE_O) {
+          p0v[q] = ok[q] ? psi0[k[q]] : dz();
         }
-      } else if (!hcol && USE_O) {
-        const double2 p0v = psi0[k];
-        const double s = sc.oscale * rm;
-        opsi[k] = make_double2((p0v.x + v.x) * s, (p0v.y + v.y) * s);
+      }
+#pragma unroll
+      for (int q = 0; q < kB; ++q) {
+        if (!ok[q]) continue;
+        const int j = j0 + q;
+        const double2 v = make_double2((double)acc[2 * j], (double)acc[2 * j + 1]);
+        if (hcol && USE_H) {
+          const double2 h2 = cadd(hv[q], v);
+          hpsi[k[q]] = h2;
+          if (MODE == ADDPRO_FUSED) {
+            const double a3 = sc.a3 * rm;
+            psim[k[q]] = make_double2(sc.a1 * p0v[q].x + sc.a2 * pm[q].x + a3 * h2.x,
+                                      sc.a1 * p0v[q].y + sc.a2 * pm[q].y + a3 * h2.y);
+          }
+        } else if (!hcol && USE_O) {
+          const double s = sc.oscale * rm;
+          opsi[k[q]] = make_double2((p0v[q].x + v.x) * s, (p0v[q].y + v.y) * s);
+        }
       }
     }
   };
@@ -398,12 +422,22 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int m = m0 + row;
     if (m >= a.nm) return;
     const int nb = blockIdx.y * 64 + col0 / 2;
+    // four columns' loads before their stores (one memory round trip per group)
 #pragma unroll
-    for (int j = 0; j < kNC; ++j) {
-      if (nb + j >= a.nn) continue;
-      const size_t k = (size_t)m * a.som + (size_t)(nb + j) * a.son;
-      const double2 o = a.out[k];
-      a.out[k] = make_double2(o.x + (double)acc[2 * j], o.y + (double)acc[2 * j + 1]);
+    for (int j0 = 0; j0 < kNC; j0 += 4) {
+      double2 o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = j0 + q;
+        o[q] = nb + j < a.nn ? a.out[(size_t)m * a.som + (size_t)(nb + j) * a.son] : dz();
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = j0 + q;
+        if (nb + j < a.nn)
+          a.out[(size_t)m * a.som + (size_t)(nb + j) * a.son] =
+              make_double2(o[q].x + (double)acc[2 * j], o[q].y + (double)acc[2 * j + 1]);
+      }
     }
   };
   NoConvertB no_cb;
