@@ -462,6 +462,26 @@ __global__ void __launch_bounds__(NT, 1) k_addx(AddXArgs a, const int* __restric
       }
 }
 
+// out(b,p) += sum_k x(k,p) l1(k,b) + conj(x(k,p)) l2(k,b) for (NBH, NPRO)
+// arrays with the band index fastest; thread t = b + NBH p
+__global__ void k_addoproj(double2* __restrict__ out, const double2* __restrict__ x, const double2* __restrict__ l1,
+                           const double2* __restrict__ l2, int npro, int nbh) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npro * nbh) return;
+  const int b = t % nbh, p = t / nbh;
+  const double2* xp = x + (size_t)p * nbh;
+  const double2* a = l1 + (size_t)nbh * b;
+  const double2* c = l2 + (size_t)nbh * b;
+  double sr = 0.0, si = 0.0;
+  for (int k = 0; k < nbh; ++k) {
+    const double2 xv = xp[k], av = a[k], cv = c[k];
+    sr += xv.x * av.x - xv.y * av.y + xv.x * cv.x + xv.y * cv.y;
+    si += xv.x * av.y + xv.y * av.x + xv.x * cv.y - xv.y * cv.x;
+  }
+  const double2 o = out[t];
+  out[t] = make_double2(o.x + sr, o.y + si);
+}
+
 // ---------------------------------------------------------------------------
 // Forces: D(g,p) = sum_b psi0(g,b) conj(E(b,p)); then per projector
 //   f_p += Re[ i P(g) (-i)^l EIGR(g) conj(D(g,p)) ] Y_lm(g) G(g)
@@ -803,23 +823,16 @@ int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* 
   return CUW_OK;
 }
 
+// ADDOPROJ for the (NBH, NPRO) projection arrays (src/paw_waves2.f90:687-758):
+// PROJ(b,p) += sum_k OPROJ(k,p) L1(k,b) + conj(OPROJ(k,p)) L2(k,b), in FP64 on
+// both paths.  The product is small (NPRO x NBH outputs, K = NBH), so one
+// thread per output with K in order beats a tiled GEMM, whose few CTAs
+// mostly fill and drain their pipeline.
 int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* l1, const double2* l2) {
-  AddXArgs a;
-  a.out = proj;
-  a.x = oproj;
-  a.l1 = l1;
-  a.l2 = l2;
-  a.nm = h->npro;
-  a.nn = h->d.nbh;
-  a.nk = h->d.nbh;
-  a.sxm = (size_t)h->d.nbh;  // X(m=p, k=b) at b + nbh*p
-  a.sxk = 1;
-  a.som = (size_t)h->d.nbh;  // out(m=p, n=b) at b + nbh*p
-  a.son = 1;
-  if (h->tc_on()) return tc_addx(h, false, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
-  dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
-  k_addx<false, false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
-  CUW_LAUNCH_CHECK("k_addx");
+  const int n = h->npro * h->d.nbh;
+  if (n == 0) return CUW_OK;
+  k_addoproj<<<ceil_div(n, 128), 128, 0, h->stream>>>(proj, oproj, l1, l2, h->npro, h->d.nbh);
+  CUW_LAUNCH_CHECK("k_addoproj");
   return CUW_OK;
 }
 
@@ -854,7 +867,6 @@ int gemm_setup(Handle* h) {
   CUW_TRY(smem_allow((const void*)k_gram<true, true>, (int)smem_bytes<MPGRAM>()));
   CUW_TRY(smem_allow((const void*)k_gram<false, false>, (int)smem_bytes<MPGRAM>()));
   CUW_TRY(smem_allow((const void*)k_addx<true, true>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_addx<false, false>, (int)smem_bytes<MP11>()));
   CUW_TRY(smem_allow((const void*)k_force, (int)smem_bytes<MP11>()));
   return CUW_OK;
 }
