@@ -190,8 +190,9 @@ struct Handle {
   // relative accuracy to which each ORTHO_X iteration solves its Lyapunov
   // equation (0: to rounding).  Measured on Si64 over 40 CP steps against the
   // solve to rounding: 1e-6 moves the FP64 total energy by 3e-12 Ha and the
-  // forces by 1e-13 Ha/bohr with 40% of the sweeps; 1e-3 moves it by 1e-8 Ha,
-  // far inside the mixed path's own error.
+  // forces by 1e-13 Ha/bohr with 40% of the sweeps; 1e-2 moves it by 6e-7 Ha
+  // (1e-8 Ha/atom) and the forces by 1e-8 Ha/bohr with 16% of the sweeps, far
+  // inside the mixed path's own error.
   double lyap_tol = 0.0;
   int lyap_max_sweeps = 64;  // sweeps per Lyapunov solve before the fixed point counts as failed
   bool tc_scope_open = false;

@@ -249,6 +249,7 @@ struct OrthoArgs {
   int fast;       // lyap_fast applies (n <= 128, tiles of at most 32 x 32)
   double lyap_tol;  // relative accuracy of the Lyapunov solve (0: rounding)
   const int* gate;  // gated launch (see gate_closed) or nullptr
+  int occ_equal;    // all occupations equal: the Lambda update needs no transpose
 };
 
 // C(tile) = op(A) * op(B); op = transpose when tA / tB.  The tile
@@ -264,9 +265,16 @@ __host__ __device__ constexpr int tile_lda() { return 16 * MR + 4; }
 template <int MR, int MC>
 __host__ __device__ constexpr int tile_ldb() { return 16 * MC + 4; }
 
+// Number of 8x8 output blocks a warp holds in gemm_acc (8 warps' worth of
+// blocks spread over the CTA's warps)
+template <int MR, int MC>
+__host__ __device__ constexpr int tile_tpw() { return ((16 * MR / 8) * (16 * MC / 8) + 7) / 8; }
+
+// acc += op(A) * op(B) on the tile (see gemm_tile); acc holds this thread's
+// elements of its warps' 8x8 blocks
 template <int MR, int MC, int KC = 128>
-__device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, int n, int i0, int i1, int j0, int j1,
-                          double* C, double* smA, double* smB) {
+__device__ void gemm_acc(const double* A, bool tA, const double* B, bool tB, int n, int i0, int i1, int j0, int j1,
+                         double (&acc)[tile_tpw<MR, MC>()][2], double* smA, double* smB) {
   static_assert(KC % 4 == 0, "the chunk is a whole number of k=4 MMA steps");
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int tm = i1 - i0, tn = j1 - j0;
@@ -274,9 +282,6 @@ __device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, in
   constexpr int LDA = tile_lda<MR, MC>(), LDB = tile_ldb<MR, MC>();
   constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC;
   constexpr int TPW = (NTILE + 7) / 8;  // 8x8 blocks per warp (8 warps)
-  double acc[TPW][2];
-#pragma unroll
-  for (int q = 0; q < TPW; ++q) acc[q][0] = acc[q][1] = 0.0;
   for (int k0 = 0; k0 < n; k0 += KC) {
     const int kk = min(KC, n - k0);
     const int kk4 = (kk + 3) & ~3;
@@ -325,15 +330,27 @@ __device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, in
       const int t = warp + q * nw;
       if (t < NTILE) {
         const int r0 = (t % TR) * 8, c0 = (t / TR) * 8;
-        for (int k = 0; k < kk4; k += 4) {
-          const double av = smA[(k + fk) * LDA + r0 + fr];
-          const double bv = smB[(k + fk) * LDB + c0 + fr];
-          dmma(acc[q], av, bv);
+        // two independent MMA chains (even and odd k steps) to hide the MMA latency
+        double a2[2] = {0.0, 0.0};
+        for (int k = 0; k < kk4; k += 8) {
+          dmma(acc[q], smA[(k + fk) * LDA + r0 + fr], smB[(k + fk) * LDB + c0 + fr]);
+          if (k + 4 < kk4) dmma(a2, smA[(k + 4 + fk) * LDA + r0 + fr], smB[(k + 4 + fk) * LDB + c0 + fr]);
         }
+        acc[q][0] += a2[0];
+        acc[q][1] += a2[1];
       }
     }
     __syncthreads();
   }
+}
+
+// calls f(i, j, value) for this thread's elements of the tile
+template <int MR, int MC, class F>
+__device__ __forceinline__ void tile_each(const double (&acc)[tile_tpw<MR, MC>()][2], int i0, int i1, int j0, int j1,
+                                          F&& f) {
+  constexpr int TR = 16 * MR / 8, TC = 16 * MC / 8, NTILE = TR * TC, TPW = tile_tpw<MR, MC>();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int tm = i1 - i0, tn = j1 - j0;
 #pragma unroll
   for (int q = 0; q < TPW; ++q) {
     const int t = warp + q * nw;
@@ -342,10 +359,20 @@ __device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, in
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int jj = (t / TR) * 8 + 2 * (lane & 3) + e;
-        if (ii < tm && jj < tn) C[(i0 + ii) + (size_t)n * (j0 + jj)] = acc[q][e];
+        if (ii < tm && jj < tn) f(i0 + ii, j0 + jj, acc[q][e]);
       }
     }
   }
+}
+
+template <int MR, int MC, int KC = 128>
+__device__ void gemm_tile(const double* A, bool tA, const double* B, bool tB, int n, int i0, int i1, int j0, int j1,
+                          double* C, double* smA, double* smB) {
+  double acc[tile_tpw<MR, MC>()][2];
+#pragma unroll
+  for (int q = 0; q < tile_tpw<MR, MC>(); ++q) acc[q][0] = acc[q][1] = 0.0;
+  gemm_acc<MR, MC, KC>(A, tA, B, tB, n, i0, i1, j0, j1, acc, smA, smB);
+  tile_each<MR, MC>(acc, i0, i1, j0, j1, [&](int i, int j, double v) { C[i + (size_t)n * j] = v; });
   // callers read the tile back with another thread-to-element map
   __syncthreads();
 }
@@ -419,7 +446,7 @@ __device__ __forceinline__ bool lyap_stop(double gdx, double gxm, double& prev, 
 // per sweep.  Returns the buffer that holds the last iterate.
 template <int MR, int MC>
 __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i1, int j0, int j1, double* sm,
-                             double* red, double* xcur, double* xnext, bool& failed) {
+                             double* red, double* xcur, double* xnext, bool& failed, double& rho_io) {
   constexpr int RA = 16 * MR, RB = 16 * MC, LDA = RA + 4, LDB = RB + 4;
   constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC, TPW = (NTILE + 7) / 8;
   // the slices always hold KN = 128 rows of k (zero past n), so that every
@@ -468,7 +495,10 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
   // [-rho, rho].  Three plain sweeps estimate rho from the ratio of successive
   // changes (with a margin; an estimate below the true rho still contracts),
   // then x_{k+1} = w (F(x_k) - x_{k-1}) + x_{k-1} with the Chebyshev weights.
-  double prev = INFINITY, rho = 0.0, omega = 1.0;
+  // E and e are the same in every ORTHO_X iteration of a launch, and so is
+  // rho: a later solve (rho_io > 0) starts the weights after one plain sweep.
+  double prev = INFINITY, rho = rho_io, omega = 1.0;
+  const int cheb0 = rho > 0.0 ? 0 : 2;  // sweep after which the weights start
   failed = false;
   for (int it2 = 0; it2 < a.max_inner; ++it2) {
     double* mp = a.maxpart + (it2 & 1) * 2 * cs;
@@ -548,10 +578,10 @@ __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i
     if (rank == 0 && tid == 0) a.inner[0] += 1;
     const double ratio = gdx / prev;
     if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, a.lyap_tol, failed)) break;
-    if (it2 == 2) {
-      rho = fmin(0.9, fmax(0.05, 1.1 * ratio));
+    if (it2 == cheb0) {
+      if (cheb0 == 2) rho_io = rho = fmin(0.9, fmax(0.05, 1.1 * ratio));
       omega = 1.0 / (1.0 - 0.5 * rho * rho);
-    } else if (it2 > 2) {
+    } else if (it2 > cheb0) {
       omega = 1.0 / (1.0 - 0.25 * rho * rho * omega);
     }
   }
@@ -583,29 +613,36 @@ __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
   double* lamn = a.lam2;
   __shared__ double red[256];
   int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
+  double rho_known = 0.0;  // contraction of the Lyapunov map, once estimated (lyap_fast)
   for (int iter = 1; iter <= a.max_iter; ++iter) {
-    // HAUX = CHICHI * LAMBDA + 2 CHIPSI
+    // The reference forms GAMN = LAMBDA^T (CHICHI LAMBDA + 2 CHIPSI) and then
+    // W = 0.5 (GAMN + GAMN^T) + PSIPSI - 1 (PSIPSI of the upper triangle).
+    // With CHICHI symmetric that is
+    //   W = LAMBDA^T (CHICHI LAMBDA + CHIPSI) + CHIPSI^T LAMBDA + PSIPSI - 1,
+    // whose tile needs no transposed tile: one product phase and one barrier
+    // fewer per iteration (the same matrix to rounding).
+    // HAUX = CHICHI * LAMBDA + CHIPSI
     gemm_tile<MR, MC>(a.chichi, false, lam, false, n, i0, i1, j0, j1, a.haux, smA, smB);
     for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
       int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
-      a.haux[i + (size_t)n * j] = __ldcg(&a.haux[i + (size_t)n * j]) + 2.0 * a.chipsi[i + (size_t)n * j];
+      a.haux[i + (size_t)n * j] = __ldcg(&a.haux[i + (size_t)n * j]) + a.chipsi[i + (size_t)n * j];
     }
     csync();
-    // GAMN = LAMBDA^T * HAUX
-    gemm_tile<MR, MC>(lam, true, a.haux, false, n, i0, i1, j0, j1, a.gamn, smA, smB);
-    csync();
-    // W = 0.5 (GAMN + GAMN^T) + PSIPSI - 1 ; tile max
+    // W = LAMBDA^T HAUX + CHIPSI^T LAMBDA + PSIPSI - 1 ; tile max
     double mx = 0.0;
-    for (int t = tid; t < (i1 - i0) * (j1 - j0); t += nt) {
-      int i = i0 + t % (i1 - i0), j = j0 + t / (i1 - i0);
-      // the reference writes GAMN(J,I)=GAMN(I,J)=0.5*(GAMN(I,J)+GAMN(J,I))+PSIPSI(I,J) for J>=I
-      int lo = min(i, j), hi = max(i, j);
-      double v = 0.5 * (__ldcg(&a.gamn[lo + (size_t)n * hi]) + __ldcg(&a.gamn[hi + (size_t)n * lo])) +
-                 a.psipsi[lo + (size_t)n * hi];
-      if (i == j) v -= 1.0;
-      a.w[i + (size_t)n * j] = v;
-      mx = fmax(mx, fabs(v));
-      if (v != v) mx = INFINITY;
+    {
+      double acc[tile_tpw<MR, MC>()][2];
+#pragma unroll
+      for (int q = 0; q < tile_tpw<MR, MC>(); ++q) acc[q][0] = acc[q][1] = 0.0;
+      gemm_acc<MR, MC>(lam, true, a.haux, false, n, i0, i1, j0, j1, acc, smA, smB);
+      gemm_acc<MR, MC>(a.chipsi, true, lam, false, n, i0, i1, j0, j1, acc, smA, smB);
+      tile_each<MR, MC>(acc, i0, i1, j0, j1, [&](int i, int j, double g) {
+        double v = g + a.psipsi[min(i, j) + (size_t)n * max(i, j)];
+        if (i == j) v -= 1.0;
+        a.w[i + (size_t)n * j] = v;
+        mx = fmax(mx, fabs(v));
+        if (v != v) mx = INFINITY;
+      });
     }
     // CTA max (NaN propagates as infinity)
     double unused = 0.0;
@@ -643,7 +680,7 @@ __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
     bool fp_failed = false;
     if (a.use_e && a.fast) {
       if constexpr (MR <= 2 && MC <= 2)
-        xcur = lyap_fast<MR, MC>(a, cs, rank, i0, i1, j0, j1, sm, red, xcur, xnext, fp_failed);
+        xcur = lyap_fast<MR, MC>(a, cs, rank, i0, i1, j0, j1, sm, red, xcur, xnext, fp_failed, rho_known);
     } else if (a.use_e) {
       double prev = INFINITY;
       // one cluster barrier per sweep: E X and X E are both formed on this
@@ -685,6 +722,23 @@ __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
     // HAUX = U X
     gemm_tile<MR, MC>(a.u, false, xcur, false, n, i0, i1, j0, j1, a.haux, smA, smB);
     csync();
+    if (a.occ_equal) {
+      // equal occupations: LAMBDA(I,J) -= W(I,J) (the weight 2 OCCI/(OCCI+OCCJ)
+      // is 1 and the symmetrisation rule never applies), straight from the
+      // product tile W = HAUX U^T
+      double acc[tile_tpw<MR, MC>()][2];
+#pragma unroll
+      for (int q = 0; q < tile_tpw<MR, MC>(); ++q) acc[q][0] = acc[q][1] = 0.0;
+      gemm_acc<MR, MC>(a.haux, false, a.u, true, n, i0, i1, j0, j1, acc, smA, smB);
+      tile_each<MR, MC>(acc, i0, i1, j0, j1, [&](int i, int j, double wv) {
+        lamn[i + (size_t)n * j] = __ldcg(&lam[i + (size_t)n * j]) - wv;
+      });
+      csync();
+      double* tmp = lam;
+      lam = lamn;
+      lamn = tmp;
+      continue;
+    }
     // W = HAUX U^T
     gemm_tile<MR, MC>(a.haux, false, a.u, true, n, i0, i1, j0, j1, a.w, smA, smB);
     csync();
@@ -972,6 +1026,9 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, const 
   a.inner = g.ostatus + 8;
   a.lyap_tol = h->lyap_tol;
   a.gate = gate;
+  a.occ_equal = 1;
+  for (int i = 1; i < n; ++i)
+    if (h->occ_h[i] != h->occ_h[0]) a.occ_equal = 0;
   // cluster of 16 CTAs (non-portable size), else 8, 4, ... ; tile rows/cols
   // per CTA are at most 16*MR x 16*MC with MR, MC in {1,2,4}
   cudaLaunchConfig_t cfg = {};
