@@ -282,6 +282,8 @@ __device__ void gemm_acc(const double* A, bool tA, const double* B, bool tB, int
   constexpr int LDA = tile_lda<MR, MC>(), LDB = tile_ldb<MR, MC>();
   constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC;
   constexpr int TPW = (NTILE + 7) / 8;  // 8x8 blocks per warp (8 warps)
+  // 16-byte staging needs even offsets of the tile and an even leading dimension
+  const bool vec = (n % 2 == 0) && (i0 % 2 == 0) && (j0 % 2 == 0);
   for (int k0 = 0; k0 < n; k0 += KC) {
     const int kk = min(KC, n - k0);
     const int kk4 = (kk + 3) & ~3;
@@ -289,7 +291,71 @@ __device__ void gemm_acc(const double* A, bool tA, const double* B, bool tB, int
     // flight per thread: the tile is tiny and the loop is bound by latency;
     // every divisor of the index arithmetic is a compile-time constant
     constexpr int totA = RA * KC, tot = totA + RB * KC;
-    for (int base = 0; base < tot; base += 8 * nt) {
+    if (vec) {
+      // pairs of neighbouring elements of the contiguous index (16-byte loads),
+      // four pairs in flight per thread; a pair half past the tile or the chunk
+      // is loaded alone
+      constexpr int totA2 = totA / 2, tot2 = tot / 2;
+      for (int base = 0; base < tot2; base += 4 * nt) {
+        double2 v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int t = base + tid + q * nt;
+          v[q] = make_double2(0.0, 0.0);
+          if (t < totA2) {
+            if (!tA) {
+              const int ii = 2 * (t % (RA / 2)), k = t / (RA / 2);
+              const double* src = &A[(i0 + ii) + (size_t)n * (k0 + k)];
+              if (k < kk && ii + 1 < tm) v[q] = __ldcg(reinterpret_cast<const double2*>(src));
+              else if (k < kk && ii < tm) v[q].x = __ldcg(src);
+            } else {
+              const int k = 2 * (t % (KC / 2)), ii = t / (KC / 2);
+              const double* src = &A[(k0 + k) + (size_t)n * (i0 + ii)];
+              if (ii < tm && k + 1 < kk) v[q] = __ldcg(reinterpret_cast<const double2*>(src));
+              else if (ii < tm && k < kk) v[q].x = __ldcg(src);
+            }
+          } else if (t < tot2) {
+            const int u = t - totA2;
+            if (!tB) {
+              const int k = 2 * (u % (KC / 2)), jj = u / (KC / 2);
+              const double* src = &B[(k0 + k) + (size_t)n * (j0 + jj)];
+              if (jj < tn && k + 1 < kk) v[q] = __ldcg(reinterpret_cast<const double2*>(src));
+              else if (jj < tn && k < kk) v[q].x = __ldcg(src);
+            } else {
+              const int jj = 2 * (u % (RB / 2)), k = u / (RB / 2);
+              const double* src = &B[(j0 + jj) + (size_t)n * (k0 + k)];
+              if (k < kk && jj + 1 < tn) v[q] = __ldcg(reinterpret_cast<const double2*>(src));
+              else if (k < kk && jj < tn) v[q].x = __ldcg(src);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int t = base + tid + q * nt;
+          if (t < totA2) {
+            if (!tA) {
+              const int ii = 2 * (t % (RA / 2)), k = t / (RA / 2);
+              *reinterpret_cast<double2*>(&smA[k * LDA + ii]) = v[q];
+            } else {
+              const int k = 2 * (t % (KC / 2)), ii = t / (KC / 2);
+              smA[k * LDA + ii] = v[q].x;
+              smA[(k + 1) * LDA + ii] = v[q].y;
+            }
+          } else if (t < tot2) {
+            const int u = t - totA2;
+            if (!tB) {
+              const int k = 2 * (u % (KC / 2)), jj = u / (KC / 2);
+              smB[k * LDB + jj] = v[q].x;
+              smB[(k + 1) * LDB + jj] = v[q].y;
+            } else {
+              const int jj = 2 * (u % (RB / 2)), k = u / (RB / 2);
+              *reinterpret_cast<double2*>(&smB[k * LDB + jj]) = v[q];
+            }
+          }
+        }
+      }
+    }
+    for (int base = vec ? tot : 0; base < tot; base += 8 * nt) {
       double v[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
