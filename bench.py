@@ -41,14 +41,44 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and clock-event (throttle) reasons during the timed region:
+    NVML read every 10 ms from a thread (read-only queries), else
+    nvidia-smi every 200 ms."""
+
+    NAMES = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+             ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+             ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+             ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, [reasons])
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:  # noqa: BLE001 (fall back to the index)
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.nvml = (nv, h)
+            self.thread = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:  # noqa: BLE001
+            self.nvml = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -56,17 +86,41 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
         return self
 
-    def _read(self):
+    def _poll_nvml(self):
+        nv, h = self.nvml
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                rs = [n for n, c in self.NAMES if bits & getattr(nv, c, 0)]
+                self.samples.append((float(sm), float(mx), rs))
+            except Exception:  # noqa: BLE001
+                break
+            self.stop.wait(0.01)
+
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            s = [x.strip() for x in line.split(",")]
+            if len(s) < 9 or not s[1].replace(".", "").isdigit():
+                continue
+            rs = [n for k, (n, _) in enumerate(self.NAMES) if s[5 + k].lower().startswith("active")]
+            self.samples.append((float(s[1]), float(s[2]), rs))
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml:
+            self.thread.join(timeout=2)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:  # noqa: BLE001
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -79,16 +133,10 @@ class ClockSampler:
 
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for k, n in enumerate(names):
-                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+        reasons = sorted({r for _, _, rs in self.samples for r in rs})
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples), "sm_max_mhz": max(x[1] for x in self.samples),
+                "reasons": reasons, "samples": len(self.samples),
+                "source": "nvml (10 ms)" if self.nvml else "nvidia-smi (200 ms)"}
 
 
 def measured_peaks():
