@@ -56,8 +56,16 @@ def test_invalid_dims_rejected_without_device(engine_lib):
     f = lib.cuwaves_create
     f.argtypes = [C.POINTER(Dims), C.POINTER(C.c_void_p)]
     h = C.c_void_p()
+    lib.cuwaves_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+    buf = C.create_string_buffer(256)
+
+    def why():
+        lib.cuwaves_last_error(None, buf, 256)  # the thread's last failed create
+        return buf.value.decode()
+
     d = Dims()  # all zero: invalid
     assert f(C.byref(d), C.byref(h)) == 1  # CUW_ERR_ARG
+    assert why() == "invalid dimensions"
     d.ngl, d.ndim, d.nb, d.nbh, d.tinv = 100, 1, 3, 2, 1  # odd NB with super wave functions
     d.nr1 = d.nr2 = d.nr3 = 8
     d.nsp, d.lmx = 1, 1
@@ -66,6 +74,7 @@ def test_invalid_dims_rejected_without_device(engine_lib):
     d.nat = 1
     d.isp = C.cast(isp, C.POINTER(C.c_int))
     assert f(C.byref(d), C.byref(h)) == 6  # CUW_ERR_UNSUPPORTED
+    assert "even band count" in why()
     d.nb, d.nbh = 4, 2
     rc = f(C.byref(d), C.byref(h))
     # valid dims: without a CUDA device the engine refuses (no host fallback)
@@ -73,6 +82,7 @@ def test_invalid_dims_rejected_without_device(engine_lib):
 
     if not torch.cuda.is_available():
         assert rc == 2  # CUW_ERR_CUDA
+        assert why() == "no CUDA device"
     else:
         assert rc == 0
         lib.cuwaves_destroy.argtypes = [C.c_void_p]
