@@ -376,7 +376,7 @@ static int dev_alloc(Handle* h, void** p, size_t bytes) {
 
 static void free_all(Handle* h) {
   Device& g = h->g;
-  void* ptrs[] = {g.psi0, g.psim, g.hpsi, g.opsi, g.proj, g.oproj, g.hproj, g.pbuf, g.rlam0, g.rlamm, g.igvec,
+  void* ptrs[] = {g.rho, g.psi0, g.psim, g.hpsi, g.opsi, g.proj, g.oproj, g.hproj, g.pbuf, g.rlam0, g.rlamm, g.igvec,
                   g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_off,
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
@@ -793,6 +793,41 @@ extern "C" int cuwaves_force(cuw_handle* hp, double* force) {
   CUW_TRY(cudaMemcpyAsync(force, h->g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
   return CUW_OK;
+}
+
+// WAVES_DENSITY (src/paw_waves1.f90:5377-5500) of this wave-function set, the
+// term WAVES$RHO (:4068-4144) adds per (k-point, spin): rho(NR1*NR2*NR3) on
+// the host, x fastest.  PSI0 and the occupations of the handle.
+extern "C" int cuwaves_density(cuw_handle* hp, double* rho) {
+  H(hp);
+  NEED(h->have_gset, CUW_ERR_STATE, "G set not loaded");
+  NEED(rho, CUW_ERR_ARG, "null rho");
+  if (!h->g.rho) CUW_RET(dev_alloc(h, reinterpret_cast<void**>(&h->g.rho), sizeof(double) * h->nr));
+  CUW_RET(fft_density(h, h->g.psi0, h->g.rho));
+  CUW_TRY(cudaMemcpyAsync(rho, h->g.rho, sizeof(double) * h->nr, cudaMemcpyDeviceToHost, h->stream));
+  return h->sync();
+}
+
+// WAVES$DENMAT (src/paw_waves1.f90:2957-3134) of this wave-function set:
+// denmat and edenmat (LMNXX,LMNXX,NAT) complex as the reference's DENMAT and
+// EDENMAT for one spin (edenmat may be NULL), from PROJ, RLAM0 and the
+// occupations.
+extern "C" int cuwaves_denmat(cuw_handle* hp, int lmnxx, double* denmat, double* edenmat) {
+  H(hp);
+  NEED(denmat, CUW_ERR_ARG, "null denmat");
+  NEED(lmnxx >= h->lmnxx, CUW_ERR_ARG, "lmnxx smaller than the largest LMNX");
+  const size_t n = (size_t)lmnxx * lmnxx * std::max(1, h->d.nat);
+  double2 *dd = nullptr, *de = nullptr;
+  CUW_TRY(cudaMallocAsync(reinterpret_cast<void**>(&dd), sizeof(double2) * n * 2, h->stream));
+  de = dd + n;
+  int rc = denmat_run(h, lmnxx, dd, edenmat ? de : nullptr);
+  if (rc == CUW_OK) {
+    cudaMemcpyAsync(denmat, dd, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->stream);
+    if (edenmat) cudaMemcpyAsync(edenmat, de, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->stream);
+  }
+  cudaFreeAsync(dd, h->stream);
+  if (rc != CUW_OK) return rc;
+  return h->sync();
 }
 
 extern "C" int cuwaves_propagate(cuw_handle* hp) {

@@ -85,6 +85,7 @@ struct Device {
   int *zslot = nullptr;          // (NR3) compact plane index or -1
   double *v = nullptr;           // (NR1*NR2*NR3) local potential
   void *grid = nullptr;          // (batch, nzp, NR2, NR1) work grid, double2 or float2 (mixed)
+  double* rho = nullptr;         // (NR) pseudo density of cuwaves_density (allocated on first use)
   double2 *tw1 = nullptr, *tw2 = nullptr, *tw3 = nullptr;  // twiddles exp(+2 pi i k/n)
   // atoms and one-centre data
   double *r0 = nullptr, *rp = nullptr, *rm = nullptr;  // (3, NAT)
@@ -144,6 +145,7 @@ struct Handle {
   double split_proj = 1.0, split_gram = 1.0;
   AxisPlan ax[3];
   int (*fft_run)(Handle*, const double2*, double2*, bool) = nullptr;  // chosen by fft_setup
+  int (*fft_rho)(Handle*, const double2*, double*) = nullptr;          // density, chosen by fft_setup
   size_t nr = 0;
   std::vector<double> occ_h;
   double waveekin1 = 0.0, waveekin2 = 0.0;
@@ -278,6 +280,8 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
 // host helpers implemented in the .cu files
 int fft_setup(Handle* h, const int* igvec_host);
 int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic);
+int fft_density(Handle* h, const double2* psi, double* rho);
+int denmat_run(Handle* h, int lmnxx, double2* denmat, double2* edenmat);
 int eigr_compute(Handle* h, const double* r_dev);
 int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* psiB, double2* projB);
 int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc);

@@ -472,6 +472,67 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   }
 }
 
+// Pseudo density of WAVES_DENSITY (src/paw_waves1.f90:5377-5500) for super
+// wave functions at the Gamma point: after the x/y passes of k_gtor_plane, the
+// G->R z transform of kRhoTX x columns of every band of the batch in turn, and
+// rho(r) += f1 Re(psi)^2 + f2 Im(psi)^2 (= Re[psi (s1 conj psi + s2 psi)] with
+// s1,2 = (f1 +- f2)/2, :5474-5496) in FP64, bands in order, so that the sum is
+// deterministic; `first` starts rho from zero, else the batch adds to it.
+constexpr int kRhoTX = 16;
+template <class C, int N>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_zcol_rho(const C* __restrict__ grid, const int* __restrict__ zslot, int nzp, int nr1, int nr2, AxisArg a3,
+               const double2* __restrict__ tw3g, const double* __restrict__ occ, int nb, int b0, int nbatch,
+               double* __restrict__ rho, int first) {
+  using T = typename CT<C>::R;
+  constexpr int TX = kRhoTX;
+  constexpr int EPT = 8;  // tile elements per thread (nr3 * TX <= EPT * blockDim)
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int nr3 = a3.n;
+  C* tile = sm;  // [nr3][TX]
+  C* tw = sm + nr3 * TX;
+  const int nxb = (nr1 + TX - 1) / TX;
+  const int iy = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * TX;
+  const size_t npl = (size_t)nr1 * nr2;
+  load_tw(tw, tw3g, nr3, +1.0);
+  double acc[EPT];
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x, iz = i / TX, x = i % TX;
+    const bool in = i < nr3 * TX && x0 + x < nr1;
+    acc[e] = (!first && in) ? rho[(size_t)x0 + x + (size_t)nr1 * (iy + (size_t)nr2 * iz)] : 0.0;
+  }
+  for (int bl = 0; bl < nbatch; ++bl) {
+    const int b = b0 + bl;
+    const double f1 = occ[2 * b], f2 = 2 * b + 1 < nb ? occ[2 * b + 1] : 0.0;
+    if (f1 == 0.0 && f2 == 0.0) continue;  // the same for the whole block
+    const C* gb = grid + (size_t)bl * nzp * npl;
+    __syncthreads();  // the previous band's reads of the tile are done
+    for (int i = threadIdx.x; i < nr3 * TX; i += blockDim.x) {
+      const int iz = i / TX, x = i % TX, s = zslot[iz];
+      C val = CT<C>::mk(0, 0);
+      if (s >= 0 && x0 + x < nr1) val = gb[(size_t)s * npl + (size_t)iy * nr1 + x0 + x];
+      tile[i] = val;
+    }
+    __syncthreads();
+    xform<N>(tile, a3, TX, 1, TX, false, tw, (T)1);
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const int i = threadIdx.x + e * blockDim.x;
+      if (i < nr3 * TX) {
+        const double re = (double)tile[i].x, im = (double)tile[i].y;
+        acc[e] += f1 * re * re + f2 * im * im;
+      }
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x, iz = i / TX, x = i % TX;
+    if (i < nr3 * TX && x0 + x < nr1) rho[(size_t)x0 + x + (size_t)nr1 * (iy + (size_t)nr2 * iz)] = acc[e];
+  }
+}
+
 template <class C, int N>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_rtog_plane(const C* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
@@ -566,6 +627,31 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
 }
 
 
+// rho = sum over the bands of this set of f |psi(r)|^2 terms (WAVES_DENSITY
+// for TINV at Gamma), batch by batch through the work grid
+template <class C, int N>
+static int fft_density_t(Handle* h, const double2* psi, double* rho) {
+  const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
+  if (nr3 * kRhoTX > 8 * kPlaneThreads) return h->fail(CUW_ERR_UNSUPPORTED, "density: NR3 above 128");
+  const size_t npl = (size_t)nr1 * nr2;
+  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
+  const int smem_rho = (int)(((size_t)nr3 * kRhoTX + nr3) * sizeof(C));
+  AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
+  Device& g = h->g;
+  C* grid = reinterpret_cast<C*>(g.grid);
+  const int nxb = (nr1 + kRhoTX - 1) / kRhoTX;
+  for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
+    const int nb = std::min(h->batch, h->d.nbh - b0);
+    k_gtor_plane<C, N><<<dim3(h->nzp, nb), kPlaneThreads, smem_plane, h->stream>>>(
+        psi, h->ldg, b0, g.plane_off, g.plane_g, g.plane_pos, grid, h->nzp, a1, a2, g.tw1, g.tw2);
+    CUW_LAUNCH_CHECK("k_gtor_plane");
+    k_zcol_rho<C, N><<<nr2 * nxb, kPlaneThreads, smem_rho, h->stream>>>(grid, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
+                                                                       g.occ, h->d.nb, b0, nb, rho, b0 == 0);
+    CUW_LAUNCH_CHECK("k_zcol_rho");
+  }
+  return CUW_OK;
+}
+
 // kernels of work-grid type C and length N (0: any length): shared-memory
 // limits and the launcher
 template <class C, int N>
@@ -574,7 +660,9 @@ static int fft_select(Handle* h, int smem_plane, int /*smem_z of the generic ker
   CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_zcol_v<C, N>, smem_z));
+  CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
   h->fft_run = &fft_vpsi_t<C, N>;
+  h->fft_rho = &fft_density_t<C, N>;
   return CUW_OK;
 }
 
@@ -678,6 +766,11 @@ int fft_setup(Handle* h, const int* igvec) {
 int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
   if (!h->fft_run) return h->fail(CUW_ERR_STATE, "FFT not set up");
   return h->fft_run(h, psi, out, add_kinetic);
+}
+
+int fft_density(Handle* h, const double2* psi, double* rho) {
+  if (!h->fft_rho) return h->fail(CUW_ERR_STATE, "FFT not set up");
+  return h->fft_rho(h, psi, rho);
 }
 
 }  // namespace cuw

@@ -745,6 +745,83 @@ static TabView tables(Handle* h) {
   return TabView{g.t_ipro0, g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox};
 }
 
+// WAVES_DENMAT (src/paw_waves1.f90:3331-3572) for super wave functions (TINV,
+// NDIM=1), one block per atom: the one-centre density matrix
+//   D(l1,l2) = Re sum_ib P(ib,l1) (s1 conj P(ib,l2) + s2 P(ib,l2)),
+//   s1,2 = (f(2ib-1) +- f(2ib))/2                                   (:3384-3412)
+// and the energy-weighted E(l1,l2) = Re sum_ib1 conj P(ib1,l1) FUNC_ib1(l2) with
+// FUNC_ib1 = sum_ib2 c1 P(ib2,.) + c2 conj P(ib2,.) from LAGR = RLAM0 * OCC
+// (:3416-3449); both then Hermitian (:3525-3540, a symmetric average of real
+// matrices) and real.  P(ib,l) = PROJ(ib, ipro0 + l).  Sums in band order.
+__global__ void k_denmat(const double2* __restrict__ proj, const double2* __restrict__ rlam0,
+                         const double* __restrict__ occ, const int* __restrict__ ipro0, const int* __restrict__ nlmn,
+                         int nb, int nbh, int lmnxx, double2* __restrict__ denmat, double2* __restrict__ edenmat) {
+  extern __shared__ double dsm[];
+  const int a = blockIdx.x, lmnx = nlmn[a], p0 = ipro0[a];
+  double* d1 = dsm;                   // [lmnx][lmnx]
+  double* e1 = dsm + lmnx * lmnx;     // [lmnx][lmnx]
+  auto P = [&](int ib, int l) { return proj[(size_t)ib + (size_t)nbh * (p0 + l)]; };
+  auto L = [&](int i, int j) {  // LAGR(i,j) = LAMBDA(i,j) OCC(j), 1-based
+    const double2 v = rlam0[(size_t)(i - 1) + (size_t)nb * (j - 1)];
+    return make_double2(v.x * occ[j - 1], v.y * occ[j - 1]);
+  };
+  for (int t = threadIdx.x; t < lmnx * lmnx; t += blockDim.x) {
+    const int l1 = t % lmnx, l2 = t / lmnx;
+    double d = 0.0;
+    for (int ib = 0; ib < nbh; ++ib) {
+      const double f1 = occ[2 * ib], f2 = 2 * ib + 1 < nb ? occ[2 * ib + 1] : 0.0;
+      const double s1 = 0.5 * (f1 + f2), s2 = 0.5 * (f1 - f2);
+      const double2 a1 = P(ib, l1), a2 = P(ib, l2);
+      // Re[a1 (s1 conj a2 + s2 a2)]
+      d += s1 * (a1.x * a2.x + a1.y * a2.y) + s2 * (a1.x * a2.x - a1.y * a2.y);
+    }
+    double e = 0.0;
+    if (edenmat) {
+      for (int ib1 = 1; ib1 <= nbh; ++ib1) {
+        double2 fu = make_double2(0.0, 0.0);
+        for (int ib2 = 1; ib2 <= nbh; ++ib2) {
+          const double2 r1 = L(2 * ib1 - 1, 2 * ib2 - 1), r2 = L(2 * ib1, 2 * ib2 - 1);
+          const double2 i1 = L(2 * ib1 - 1, 2 * ib2), i2 = L(2 * ib1, 2 * ib2);
+          const double2 cr = make_double2(r1.x - r2.y, r1.y + r2.x);  // r1 + i r2
+          const double2 ci = make_double2(i1.x - i2.y, i1.y + i2.x);  // i1 + i i2
+          // c1 = (cr - i ci)/2, c2 = (cr + i ci)/2
+          const double2 c1 = make_double2(0.5 * (cr.x + ci.y), 0.5 * (cr.y - ci.x));
+          const double2 c2 = make_double2(0.5 * (cr.x - ci.y), 0.5 * (cr.y + ci.x));
+          const double2 p = P(ib2 - 1, l2);
+          fu.x += c1.x * p.x - c1.y * p.y + c2.x * p.x + c2.y * p.y;
+          fu.y += c1.x * p.y + c1.y * p.x - c2.x * p.y + c2.y * p.x;
+        }
+        const double2 q = P(ib1 - 1, l1);
+        e += q.x * fu.x + q.y * fu.y;  // Re[conj q fu]
+      }
+    }
+    d1[l1 + lmnx * l2] = d;
+    e1[l1 + lmnx * l2] = e;
+  }
+  __syncthreads();
+  const size_t per = (size_t)lmnxx * lmnxx;
+  for (int t = threadIdx.x; t < lmnxx * lmnxx; t += blockDim.x) {
+    const int l1 = t % lmnxx, l2 = t / lmnxx;
+    double dv = 0.0, ev = 0.0;
+    if (l1 < lmnx && l2 < lmnx) {
+      dv = l1 == l2 ? d1[l1 + lmnx * l2] : 0.5 * (d1[l1 + lmnx * l2] + d1[l2 + lmnx * l1]);
+      ev = l1 == l2 ? e1[l1 + lmnx * l2] : 0.5 * (e1[l1 + lmnx * l2] + e1[l2 + lmnx * l1]);
+    }
+    denmat[per * a + t] = make_double2(dv, 0.0);
+    if (edenmat) edenmat[per * a + t] = make_double2(ev, 0.0);
+  }
+}
+
+int denmat_run(Handle* h, int lmnxx, double2* denmat, double2* edenmat) {
+  if (h->d.nat == 0) return CUW_OK;
+  TabView t = tables(h);
+  const size_t smem = sizeof(double) * 2 * (size_t)h->lmnxx * h->lmnxx;
+  k_denmat<<<h->d.nat, 128, smem, h->stream>>>(h->g.proj, h->g.rlam0, h->g.occ, t.ipro0, t.nlmn, h->d.nb, h->d.nbh,
+                                                lmnxx, denmat, edenmat);
+  CUW_LAUNCH_CHECK("k_denmat");
+  return CUW_OK;
+}
+
 int hproj_compute(Handle* h, const double2* proj, double2* out) {
   TabView t = tables(h);
   size_t n = (size_t)h->d.nbh * h->npro;

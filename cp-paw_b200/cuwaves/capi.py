@@ -74,6 +74,8 @@ SIGNATURES = {
     "expectation": [_P, _D],
     "wavekinetic": [_P, _D, _D],
     "force": [_P, _D],
+    "density": [_P, _D],
+    "denmat": [_P, C.c_int, _D, _D],
     "propagate": [_P],
     "orthogonalize": [_P, C.c_int, C.c_double, _I],
     "switch": [_P],
@@ -304,6 +306,24 @@ class Waves:
         a = np.empty((self.nat, 3))
         self._chk(self._f["force"](self.h, _dptr(a)), "WAVES$FORCE")
         return a
+
+    def density(self) -> np.ndarray:
+        """WAVES_DENSITY of this set: rho as an (NR3, NR2, NR1) array."""
+        d = self.dims
+        rho = np.empty(d.nr1 * d.nr2 * d.nr3)
+        self._chk(self._f["density"](self.h, _dptr(rho)), "WAVES$RHO")
+        return rho.reshape(d.nr3, d.nr2, d.nr1)
+
+    def denmat(self, lmnxx=None):
+        """WAVES$DENMAT of this set: (denmat, edenmat), each (NAT, LMNXX, LMNXX)
+        complex with [a, lmn2, lmn1] = DENMAT(lmn1, lmn2, a)."""
+        if lmnxx is None:
+            lmnxx = max(sum(2 * l + 1 for l in self.inp["lox"][s - 1]) for s in self._isp.tolist())
+        n = lmnxx * lmnxx * max(1, self.nat)
+        dm = np.zeros(n, dtype=np.complex128)
+        em = np.zeros(n, dtype=np.complex128)
+        self._chk(self._f["denmat"](self.h, lmnxx, dm.ctypes.data_as(_D), em.ctypes.data_as(_D)), "WAVES$DENMAT")
+        return dm.reshape(max(1, self.nat), lmnxx, lmnxx), em.reshape(max(1, self.nat), lmnxx, lmnxx)
 
     def propagate(self):
         self._chk(self._f["propagate"](self.h), "WAVES$PROPAGATE")

@@ -24,6 +24,8 @@
 #ifndef CUWAVES_H
 #define CUWAVES_H
 
+#include <stddef.h> /* size_t */
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -125,6 +127,16 @@ int cuwaves_expectation(cuw_handle* h, double* eig);
 int cuwaves_wavekinetic(cuw_handle* h, double* ekin, double* eig);
 /* WAVES$FORCE without stress (src/paw_waves1.f90:4570-4739), force(3,NAT). */
 int cuwaves_force(cuw_handle* h, double* force);
+/* WAVES_DENSITY (src/paw_waves1.f90:5377-5500) of this set at the Gamma point,
+ * the term WAVES$RHO (:4068-4144) adds per (k-point, spin): the pseudo density
+ * rho(NR1*NR2*NR3), x fastest, from PSI0 and the occupations.  No kinetic-energy
+ * density (TRHOKIN). */
+int cuwaves_density(cuw_handle* h, double* rho);
+/* WAVES$DENMAT (src/paw_waves1.f90:2957-3134) of this set with WAVES_DENMAT
+ * (:3331-3572): one-centre density matrix denmat and energy-weighted density
+ * matrix edenmat (may be NULL), each (LMNXX,LMNXX,NAT) complex for one spin,
+ * from PROJ, RLAM0 and the occupations. */
+int cuwaves_denmat(cuw_handle* h, int lmnxx, double* denmat, double* edenmat);
 /* WAVES$PROPAGATE without cell dynamics (src/paw_waves1.f90:6479-6592). */
 int cuwaves_propagate(cuw_handle* h);
 /* WAVES$ORTHOGONALIZE with SAFEORTHO=T at the Gamma point (src/paw_waves2.f90:11-494,

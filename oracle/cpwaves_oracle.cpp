@@ -1458,6 +1458,97 @@ int orc_cp_step(orc_handle* h, int move_atoms, const double* mass, int maxit, do
   return CUW_OK;
 }
 
+// WAVES_DENSITY (src/paw_waves1.f90:5377-5500) for super wave functions
+// (TINV, NDIM=1) at the Gamma point, where EI2KR = 1 (:5466-5470): the pseudo
+// density of one wave-function set, rho(r) = sum_ibh Re[psi(r) (s1 conj psi(r)
+// + s2 psi(r))] with s1,s2 = (f(2ibh-1) +- f(2ibh))/2 (:5474-5496); the
+// G->R transforms of PLANEWAVE$FFT('GTOR') (:5441).  RHOKIN is not formed.
+int orc_density(orc_handle* h, double* rho) {
+  OCHECK(h->have_gset, CUW_ERR_STATE, "gset not set");
+  OCHECK(rho, CUW_ERR_ARG, "null rho");
+  const int nb = h->d.nb, nbh = h->d.nbh;
+  const size_t nr = (size_t)h->d.nr1 * h->d.nr2 * h->d.nr3;
+  std::vector<cplx> psir(nr * nbh);
+#pragma omp parallel for schedule(dynamic)
+  for (int ib = 0; ib < nbh; ++ib) fft_gtor(h, &h->psi0[PS(h, 0, ib)], &psir[nr * ib]);
+  for (size_t ir = 0; ir < nr; ++ir) rho[ir] = 0.0;
+  for (int ib = 0; ib < nbh; ++ib) {
+    const double f1 = h->occ[2 * ib], f2 = 2 * ib + 1 < nb ? h->occ[2 * ib + 1] : 0.0;
+    const double s1 = 0.5 * (f1 + f2), s2 = 0.5 * (f1 - f2);
+    if (s1 == 0.0 && s2 == 0.0) continue;
+    const cplx* pr = &psir[nr * ib];
+#pragma omp parallel for
+    for (long long ir = 0; ir < (long long)nr; ++ir) {
+      cplx p1 = s1 * std::conj(pr[ir]);
+      if (s2 != 0.0) p1 += s2 * pr[ir];
+      rho[ir] += std::real(pr[ir] * p1);
+    }
+  }
+  return CUW_OK;
+}
+
+// WAVES$DENMAT (src/paw_waves1.f90:2957-3134) for one wave-function set with
+// WAVES_DENMAT (:3331-3572) per atom, TINV and NDIM=1: the one-centre density
+// matrix D(lmn1,lmn2) = Re sum_ib PROJ(ib,lmn1) (s1 conj PROJ(ib,lmn2) + s2
+// PROJ(ib,lmn2)) and the energy-weighted EDENMAT from RLAM0 and the
+// occupations (:3438-3472), both made Hermitian (:3525-3540) and real
+// (:3551-3554).  denmat, edenmat: (LMNXX,LMNXX,NAT) complex, zero past LMNX.
+int orc_denmat(orc_handle* h, int lmnxx, double* denmat, double* edenmat) {
+  OCHECK(lmnxx >= h->lmnxx, CUW_ERR_ARG, "lmnxx smaller than the largest LMNX");
+  const int nb = h->d.nb, nbh = h->d.nbh, nat = h->d.nat;
+  const cplx ci(0.0, 1.0);
+  cplx* D = reinterpret_cast<cplx*>(denmat);
+  cplx* E = reinterpret_cast<cplx*>(edenmat);
+  const size_t per = (size_t)lmnxx * lmnxx;
+  if (D) std::fill(D, D + per * nat, cplx(0.0));
+  if (E) std::fill(E, E + per * nat, cplx(0.0));
+  // LAGR(:,IB2) = LAMBDA(:,IB2) OCC(IB2)
+  std::vector<cplx> lagr((size_t)nb * nb);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) lagr[i + (size_t)nb * j] = h->rlam0[i + (size_t)nb * j] * h->occ[j];
+  auto L = [&](int i, int j) { return lagr[(size_t)(i - 1) + (size_t)nb * (j - 1)]; };  // 1-based
+  for (int a = 0; a < nat; ++a) {
+    const int lmnx = h->lmnx[h->isp[a]], p0 = h->p_ipro0[a];
+    auto P = [&](int ib, int lmn) { return h->proj[PJ(h, ib, p0 + lmn)]; };
+    std::vector<cplx> d1((size_t)lmnx * lmnx, 0.0), e1((size_t)lmnx * lmnx, 0.0), func(lmnx);
+    for (int ib = 0; ib < nbh; ++ib) {
+      const double f1 = h->occ[2 * ib], f2 = 2 * ib + 1 < nb ? h->occ[2 * ib + 1] : 0.0;
+      const double s1 = 0.5 * (f1 + f2), s2 = 0.5 * (f1 - f2);
+      for (int l = 0; l < lmnx; ++l) func[l] = s1 * std::conj(P(ib, l)) + s2 * P(ib, l);
+      for (int l2 = 0; l2 < lmnx; ++l2)
+        for (int l1 = 0; l1 < lmnx; ++l1) d1[l1 + (size_t)lmnx * l2] += P(ib, l1) * func[l2];
+    }
+    for (auto& x : d1) x = std::real(x);
+    for (int ib1 = 1; ib1 <= nbh; ++ib1) {
+      std::fill(func.begin(), func.end(), cplx(0.0));
+      for (int ib2 = 1; ib2 <= nbh; ++ib2) {
+        const cplx cr = L(2 * ib1 - 1, 2 * ib2 - 1) + ci * L(2 * ib1, 2 * ib2 - 1);
+        const cplx cim = L(2 * ib1 - 1, 2 * ib2) + ci * L(2 * ib1, 2 * ib2);
+        const cplx c1 = 0.5 * (cr - ci * cim), c2 = 0.5 * (cr + ci * cim);
+        for (int l = 0; l < lmnx; ++l) func[l] += c1 * P(ib2 - 1, l) + c2 * std::conj(P(ib2 - 1, l));
+      }
+      for (int l2 = 0; l2 < lmnx; ++l2)
+        for (int l1 = 0; l1 < lmnx; ++l1) e1[l1 + (size_t)lmnx * l2] += std::conj(P(ib1 - 1, l1)) * func[l2];
+    }
+    for (auto& x : e1) x = std::real(x);
+    for (int l1 = 0; l1 < lmnx; ++l1)
+      for (int l2 = l1 + 1; l2 < lmnx; ++l2) {
+        cplx c = 0.5 * (d1[l1 + (size_t)lmnx * l2] + std::conj(d1[l2 + (size_t)lmnx * l1]));
+        d1[l1 + (size_t)lmnx * l2] = c;
+        d1[l2 + (size_t)lmnx * l1] = std::conj(c);
+        c = 0.5 * (e1[l1 + (size_t)lmnx * l2] + std::conj(e1[l2 + (size_t)lmnx * l1]));
+        e1[l1 + (size_t)lmnx * l2] = c;
+        e1[l2 + (size_t)lmnx * l1] = std::conj(c);
+      }
+    for (int l2 = 0; l2 < lmnx; ++l2)
+      for (int l1 = 0; l1 < lmnx; ++l1) {
+        if (D) D[per * a + l1 + (size_t)lmnxx * l2] = std::real(d1[l1 + (size_t)lmnx * l2]);
+        if (E) E[per * a + l1 + (size_t)lmnxx * l2] = std::real(e1[l1 + (size_t)lmnx * l2]);
+      }
+  }
+  return CUW_OK;
+}
+
 int orc_get_atoms(orc_handle* h, double* rm, double* r0, double* rp) {
   if (rm) std::memcpy(rm, h->rm.data(), sizeof(double) * 3 * h->d.nat);
   if (r0) std::memcpy(r0, h->r0.data(), sizeof(double) * 3 * h->d.nat);

@@ -144,6 +144,42 @@ def test_force(name, oracle, inputs_cache):
     assert np.abs(fg - fc).max() < 1e-9 * max(1.0, np.abs(fc).max())
 
 
+@pytest.mark.parametrize("name", ["Si8-20Ry", "Si8", "H2O2", "Si6", "Si2mol"])
+def test_density_and_denmat(name, oracle, inputs_cache):
+    """WAVES_DENSITY (pseudo density on the grid) and WAVES$DENMAT (one-centre
+    and energy-weighted density matrices) against the oracle, FP64 path, with a
+    nonzero Lagrange history so that EDENMAT is not trivial; unequal
+    occupations exercise the s2 terms of the super wave functions."""
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    rng = np.random.default_rng(11)
+    nb = inp["nb"]
+    lam = rng.normal(size=(nb, nb)) * 0.1 + 1j * rng.normal(size=(nb, nb)) * 0.01
+    occ = np.array(inp["occ"], dtype=np.float64)
+    occ[-1] = 0.5
+    for w in (gpu, cpu):
+        w.set_rlam0(lam)
+        w.set_occ(occ)
+    rg, rc = gpu.density(), cpu.density()
+    assert rel(rg, rc) < 1e-12
+    (dg, eg), (dc, ec) = gpu.denmat(), cpu.denmat()
+    assert rel(dg, dc) < 1e-12 and rel(eg, ec) < 1e-12
+    assert np.abs(dg.imag).max() == 0.0
+
+
+def test_density_mixed_path(oracle, inputs_cache):
+    """The density on the mixed path (FP32 G->R transforms, FP64 sums)."""
+    name = "Si8-20Ry"
+    if name not in inputs_cache:
+        inputs_cache[name] = systems.build_inputs(CASES[name]())
+    inp = inputs_cache[name]
+    mix = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup().initialize()
+    cpu = oracle.open_oracle(inp).setup()
+    sync_state(mix, cpu)
+    assert rel(mix.density(), cpu.density()) < 2e-6
+    (dg, _), (dc, _) = mix.denmat(), cpu.denmat()
+    assert rel(dg, dc) < 1e-12  # PROJ is the same state; the sums are FP64 on both paths
+
+
 @pytest.mark.parametrize("name", ["Si8-20Ry", "H2O2"])
 def test_propagate(name, oracle, inputs_cache):
     inp, gpu, cpu = make_pair(name, oracle, inputs_cache)

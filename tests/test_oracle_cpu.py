@@ -182,3 +182,47 @@ def test_golden_regression(oracle):
     for k in ("etot", "ekin", "ekinpsi", "iters"):
         assert np.allclose(got[k], gold[k], rtol=0, atol=1e-9), k
     assert np.allclose(got["force0"], gold["force0"], rtol=0, atol=1e-8)
+
+
+def _numpy_density(inp, psi, occ):
+    """WAVES_DENSITY at Gamma by numpy: psi(r) = sum_G psi(G) exp(iGr) on the
+    grid (x fastest), rho = sum f1 Re(psi)^2 + f2 Im(psi)^2."""
+    nr1, nr2, nr3 = inp["grid"]
+    ig = inp["igvec"]
+    rho = np.zeros((nr3, nr2, nr1))
+    for b in range(psi.shape[0]):
+        grid = np.zeros((nr3, nr2, nr1), complex)
+        grid[ig[:, 2] % nr3, ig[:, 1] % nr2, ig[:, 0] % nr1] = psi[b]
+        r = np.fft.ifftn(grid) * grid.size
+        f1 = occ[2 * b]
+        f2 = occ[2 * b + 1] if 2 * b + 1 < len(occ) else 0.0
+        rho += f1 * r.real ** 2 + f2 * r.imag ** 2
+    return rho
+
+
+def test_oracle_density_and_denmat(oracle):
+    """WAVES_DENSITY against numpy's FFT; WAVES_DENMAT against a numpy
+    restatement of its TINV sums; both matrices real and symmetric."""
+    s = systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry")
+    inp = systems.build_inputs(s)
+    w = oracle.open_oracle(inp).setup().initialize()
+    for _ in range(2):
+        w.cp_step()
+    rho = w.density()
+    want = _numpy_density(inp, w.download_psi(0), inp["occ"])
+    assert np.abs(rho - want).max() < 1e-12 * np.abs(want).max()
+    d, e = w.denmat()
+    proj = w.get_proj().T  # (nbh, npro) complex
+    occ = inp["occ"]
+    s1 = 0.5 * (occ[0::2] + occ[1::2])
+    s2 = 0.5 * (occ[0::2] - occ[1::2])
+    p0 = 0
+    for a, isp in enumerate(inp["isp"].tolist()):
+        lmnx = sum(2 * l + 1 for l in inp["lox"][isp - 1])
+        p = proj[:, p0:p0 + lmnx]
+        dm = np.einsum("bi,bj->ij", p, s1[:, None] * p.conj() + s2[:, None] * p).real
+        dm = 0.5 * (dm + dm.T)
+        assert np.abs(d[a][:lmnx, :lmnx].T - dm).max() < 1e-12 * max(1.0, np.abs(dm).max())
+        assert np.abs(d[a].imag).max() == 0.0 and np.abs(e[a].imag).max() == 0.0
+        assert np.abs(e[a] - e[a].T).max() < 1e-13 * max(1.0, np.abs(e[a]).max())
+        p0 += lmnx
