@@ -4,7 +4,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["capi.cu", "fft.cu", "gemm.cu", "ortho.cu", "tc.cu", "serve.cu", "tune.cu"]
+SRC = ["capi.cu", "fft.cu", "gemm.cu", "ortho.cu", "tc.cu", "serve.cu", "tune.cu", "restart.cu"]
 OUT = os.path.join(HERE, "lib", "libcuwaves.so")
 
 

@@ -574,6 +574,7 @@ extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* min
   }
   std::memcpy(h->gbas, gbas, sizeof(h->gbas));
   h->gweight = gweight;
+  h->igvec_h.assign(igvec, igvec + 3 * (size_t)ngl);
   CUW_TRY(cudaMemcpy(g.igvec, igvec, sizeof(int) * 3 * ngl, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(g.minusg, mg.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(g.gx, x.data(), sizeof(double) * ngl, cudaMemcpyHostToDevice));

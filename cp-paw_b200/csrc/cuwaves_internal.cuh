@@ -132,6 +132,7 @@ struct Handle {
   int ldg = 0;                   // leading dimension of wave-function arrays
   double gweight = 0.0;
   double gbas[9] = {0};
+  std::vector<int> igvec_h;      // IGVEC(3,NGL) of the G set (restart records)
   double delt = 0.0, annee = 0.0;
   bool have_gset = false, have_v = false, have_dh = false, have_do = false;
   bool have_hpsi = false, have_rlamm = false, have_opsi = false, have_u = false;

@@ -75,6 +75,8 @@ SIGNATURES = {
     "wavekinetic": [_P, _D, _D],
     "force": [_P, _D],
     "density": [_P, _D],
+    "write_restart": [_P, C.c_char_p, _D],
+    "read_restart": [_P, C.c_char_p],
     "denmat": [_P, C.c_int, _D, _D],
     "propagate": [_P],
     "orthogonalize": [_P, C.c_int, C.c_double, _I],
@@ -306,6 +308,15 @@ class Waves:
         a = np.empty((self.nat, 3))
         self._chk(self._f["force"](self.h, _dptr(a)), "WAVES$FORCE")
         return a
+
+    def write_restart(self, path, rbas=None):
+        """WAVES$WRITE: the WAVES section of a restart file for this set."""
+        r = None if rbas is None else np.asfortranarray(rbas, dtype=np.float64)
+        self._chk(self._f["write_restart"](self.h, str(path).encode(), _dptr(r)), "WAVES$WRITE")
+
+    def read_restart(self, path):
+        """WAVES$READ of a section written for the same bands."""
+        self._chk(self._f["read_restart"](self.h, str(path).encode()), "WAVES$READ")
 
     def density(self) -> np.ndarray:
         """WAVES_DENSITY of this set: rho as an (NR3, NR2, NR1) array."""

@@ -137,6 +137,18 @@ int cuwaves_density(cuw_handle* h, double* rho);
  * matrix edenmat (may be NULL), each (LMNXX,LMNXX,NAT) complex for one spin,
  * from PROJ, RLAM0 and the occupations. */
 int cuwaves_denmat(cuw_handle* h, int lmnxx, double* denmat, double* edenmat);
+/* The WAVES section of the restart file for this set, as WAVES$WRITE
+ * (src/paw_waves2.f90:3058-3088) with WAVES_WRITEPSI (:3168-3357) and
+ * WAVES_WRITELAMBDA (:3920-4040) write it for one k-point and spin: the
+ * separator record, then NKPT/NSPIN/RBAS/NWAVE, the PSI header, XK and IGVEC,
+ * PSI0 and PSIM of every super wave function, the LAMBDA header and RLAM0 (and
+ * RLAMM once the handle holds it), as sequential unformatted Fortran records
+ * (4-byte length markers).  rbas(3,3) = CELL T(0), or NULL to derive it from
+ * the G set's GBAS.  cuwaves_read_restart reads such a section back as
+ * WAVES_READPSI (:5147-5513) does for the same bands: G vectors are matched by
+ * IGVEC in any order; NWAVE = 1 sets PSIM = PSI0. */
+int cuwaves_write_restart(cuw_handle* h, const char* path, const double* rbas);
+int cuwaves_read_restart(cuw_handle* h, const char* path);
 /* WAVES$PROPAGATE without cell dynamics (src/paw_waves1.f90:6479-6592). */
 int cuwaves_propagate(cuw_handle* h);
 /* WAVES$ORTHOGONALIZE with SAFEORTHO=T at the Gamma point (src/paw_waves2.f90:11-494,

@@ -28,6 +28,7 @@
 #include "../include/cuwaves.h"
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -1546,6 +1547,153 @@ int orc_denmat(orc_handle* h, int lmnxx, double* denmat, double* edenmat) {
         if (E) E[per * a + l1 + (size_t)lmnxx * l2] = std::real(e1[l1 + (size_t)lmnx * l2]);
       }
   }
+  return CUW_OK;
+}
+
+// WAVES$WRITE (src/paw_waves2.f90:3058-3088) for one set: the separator
+// (SEPARATOR_TYPE, src/paw_report.f90:108-115) and the records of
+// WAVES_WRITEPSI (src/paw_waves2.f90:3216-3326) and WAVES_WRITELAMBDA
+// (:3974-4025) for NKPT = NSPIN = NDIM = 1 and a dynamic restart, as
+// sequential unformatted Fortran records (4-byte length markers).
+}  // extern "C"
+static void orc_rec(FILE* f, const std::string& b) {
+  const int32_t n = (int32_t)b.size();
+  std::fwrite(&n, 4, 1, f);
+  std::fwrite(b.data(), 1, b.size(), f);
+  std::fwrite(&n, 4, 1, f);
+}
+template <class T>
+static void orc_put(std::string& b, const T* p, size_t n) {
+  b.append(reinterpret_cast<const char*>(p), sizeof(T) * n);
+}
+static void orc_chars(std::string& b, const char* s, size_t w) {
+  std::string t(s);
+  t.resize(w, ' ');
+  b += t;
+}
+
+extern "C" {
+int orc_write_restart(orc_handle* h, const char* path, const double* rbas_in) {
+  OCHECK(h->have_gset && path, CUW_ERR_ARG, "G set or path missing");
+  const int ngl = h->d.ngl, nb = h->d.nb, nbh = h->d.nbh;
+  double rbas[9];
+  if (rbas_in) {
+    std::memcpy(rbas, rbas_in, sizeof(rbas));
+  } else {  // RBAS = 2 pi GBAS^-T: RBAS(i,j) = 2 pi cofactor(i,j) / det
+    auto G = [&](int r, int c) { return h->gbas[r + 3 * c]; };
+    auto cof = [&](int i, int j) {
+      int r[2], c[2], nr = 0, nc = 0;
+      for (int k = 0; k < 3; ++k) {
+        if (k != i) r[nr++] = k;
+        if (k != j) c[nc++] = k;
+      }
+      const double m = G(r[0], c[0]) * G(r[1], c[1]) - G(r[0], c[1]) * G(r[1], c[0]);
+      return ((i + j) % 2 ? -m : m);
+    };
+    const double det = G(0, 0) * cof(0, 0) + G(0, 1) * cof(0, 1) + G(0, 2) * cof(0, 2);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) rbas[i + 3 * j] = 2.0 * M_PI * cof(i, j) / det;
+  }
+  const int32_t nwave = 2, nlambda = h->have_rlamm ? 2 : 1;
+  const int32_t nrec = 1 + 2 + nwave * nbh + 1 + nlambda;
+  FILE* f = std::fopen(path, "wb");
+  OCHECK(f, CUW_ERR_ARG, "cannot open the restart file");
+  std::string b;
+  orc_put(b, &nrec, 1);
+  orc_chars(b, "WAVES", 32); orc_chars(b, "NONE", 32); orc_chars(b, "AUG1996", 64); orc_chars(b, "NONE", 256);
+  orc_rec(f, b);
+  b.clear();
+  const int32_t one = 1;
+  orc_put(b, &one, 1); orc_put(b, &one, 1); orc_put(b, rbas, 9); orc_put(b, &nwave, 1);
+  orc_rec(f, b);
+  b.clear();
+  const int32_t hdr[4] = {ngl, 1, nb, 1};
+  orc_chars(b, "PSI", 8); orc_put(b, hdr, 4);
+  orc_rec(f, b);
+  b.clear();
+  const double xk[3] = {0, 0, 0};
+  orc_put(b, xk, 3); orc_put(b, h->igvec.data(), h->igvec.size());
+  orc_rec(f, b);
+  for (int w = 0; w < nwave; ++w)
+    for (int ib = 0; ib < nbh; ++ib) {
+      b.clear();
+      orc_put(b, &(w ? h->psim : h->psi0)[PS(h, 0, ib)], (size_t)ngl);
+      orc_rec(f, b);
+    }
+  b.clear();
+  const int32_t lh[4] = {nb, 1, 1, nlambda};
+  orc_chars(b, "LAMBDA", 8); orc_put(b, lh, 4);
+  orc_rec(f, b);
+  for (int l = 0; l < nlambda; ++l) {
+    b.clear();
+    orc_put(b, (l ? h->rlamm : h->rlam0).data(), (size_t)nb * nb);
+    orc_rec(f, b);
+  }
+  std::fclose(f);
+  return CUW_OK;
+}
+
+// WAVES_READPSI (src/paw_waves2.f90:5147-5513) of a section written for the
+// same bands, with the G vectors matched by IGVEC
+int orc_read_restart(orc_handle* h, const char* path) {
+  OCHECK(h->have_gset && path, CUW_ERR_ARG, "G set or path missing");
+  FILE* f = std::fopen(path, "rb");
+  OCHECK(f, CUW_ERR_ARG, "cannot open the restart file");
+  auto rd = [&](std::string& b) {
+    int32_t n = 0, m = 0;
+    if (std::fread(&n, 4, 1, f) != 1 || n < 0) return false;
+    b.resize(n);
+    if (n && std::fread(&b[0], 1, n, f) != (size_t)n) return false;
+    return std::fread(&m, 4, 1, f) == 1 && m == n;
+  };
+  const int ngl = h->d.ngl, nb = h->d.nb, nbh = h->d.nbh;
+  std::string b;
+  bool ok = rd(b) && b.size() == 388 && b.compare(4, 5, "WAVES") == 0;
+  int32_t v4[4];
+  ok = ok && rd(b) && b.size() == 84;
+  int32_t nwave = 0;
+  if (ok) std::memcpy(&nwave, b.data() + 80, 4);
+  ok = ok && rd(b) && b.size() == 24 && b.compare(0, 3, "PSI") == 0;
+  if (ok) std::memcpy(v4, b.data() + 8, 16);
+  const int ngg = ok ? v4[0] : 0;
+  ok = ok && v4[2] == nb && rd(b) && b.size() == 24 + (size_t)12 * ngg;
+  std::vector<int> map(ngg, -1);
+  if (ok) {
+    std::map<std::vector<int>, int> pos;
+    for (int i = 0; i < ngl; ++i) pos[{h->igvec[3 * i], h->igvec[3 * i + 1], h->igvec[3 * i + 2]}] = i;
+    for (int i = 0; i < ngg; ++i) {
+      int v[3];
+      std::memcpy(v, b.data() + 24 + 12 * (size_t)i, 12);
+      auto it = pos.find({v[0], v[1], v[2]});
+      if (it != pos.end()) map[i] = it->second;
+    }
+  }
+  // G vectors that the file lacks become zero (MAPG(IG)=0, src/paw_waves2.f90:5395-5403)
+  if (ok) {
+    std::fill(h->psi0.begin(), h->psi0.end(), cplx(0.0, 0.0));
+    std::fill(h->psim.begin(), h->psim.end(), cplx(0.0, 0.0));
+  }
+  for (int w = 0; w < nwave && ok; ++w)
+    for (int ib = 0; ib < nbh && ok; ++ib) {
+      ok = rd(b) && b.size() == 16 * (size_t)ngg;
+      for (int i = 0; i < ngg && ok; ++i)
+        if (map[i] >= 0) std::memcpy(&(w ? h->psim : h->psi0)[PS(h, map[i], ib)], b.data() + 16 * (size_t)i, 16);
+    }
+  if (ok && nwave == 1) h->psim = h->psi0;
+  ok = ok && rd(b) && b.size() == 24 && b.compare(0, 6, "LAMBDA") == 0;
+  int nlambda = 0;
+  if (ok) {
+    std::memcpy(v4, b.data() + 8, 16);
+    nlambda = v4[3];
+  }
+  for (int l = 0; l < nlambda && ok; ++l) {
+    ok = rd(b) && b.size() == 16 * (size_t)nb * nb;
+    if (ok && l < 2) std::memcpy((l ? h->rlamm : h->rlam0).data(), b.data(), b.size());
+  }
+  std::fclose(f);
+  OCHECK(ok, CUW_ERR_ARG, "restart file does not hold a WAVES section of this set");
+  h->have_rlamm = nlambda >= 2;
+  h->have_hpsi = false;
   return CUW_OK;
 }
 

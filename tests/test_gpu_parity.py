@@ -279,3 +279,63 @@ def test_full_size_step(name, oracle):
     assert abs(og[0] - oc[0]) < 1e-8 * max(1.0, abs(oc[0]) / 100)
     assert np.abs(fg - fc).max() < 1e-6
     assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-9
+
+
+@pytest.mark.parametrize("precision", [cuwaves.CUW_PREC_FP64, cuwaves.CUW_PREC_MIXED])
+def test_restart_records(precision, oracle, inputs_cache, tmp_path):
+    """WAVES$WRITE / WAVES$READ on the device: the engine reads the oracle's
+    file bit for bit, writes back the same bytes, maps a file whose G vectors
+    are permuted and partly missing, and continues the run like the oracle."""
+    import restart_file as rf
+
+    name = "Si8-20Ry"
+    if name not in inputs_cache:
+        inputs_cache[name] = systems.build_inputs(CASES[name]())
+    inp = inputs_cache[name]
+    cpu = oracle.open_oracle(inp).setup().initialize()
+    for _ in range(3):
+        cpu.cp_step()
+    a = tmp_path / "cpu.rst"
+    cpu.write_restart(a, inp["rbas"])
+    gpu = cuwaves.open_waves(inp, precision=precision).setup()
+    gpu.read_restart(a)
+    assert np.array_equal(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0))
+    assert np.array_equal(gpu.download_psi(CUW_PSIM), cpu.download_psi(CUW_PSIM))
+    assert np.array_equal(gpu.get_rlam0(), cpu.get_rlam0())
+    b = tmp_path / "gpu.rst"
+    gpu.write_restart(b, inp["rbas"])
+    assert b.read_bytes() == a.read_bytes()
+    # RBAS from the handle's GBAS
+    gpu.write_restart(tmp_path / "g2.rst")
+    r = rf.parse_waves(rf.read_records(tmp_path / "g2.rst"))["rbas"]
+    assert np.abs(r - np.asarray(inp["rbas"])).max() < 1e-12 * np.abs(inp["rbas"]).max()
+
+    # the run continues from the file (PROJ formed from PSI0 on both sides)
+    gpu.projections()
+    cpu.projections()
+    for _ in range(2):
+        (og, fg), (oc, fc) = gpu.cp_step(), cpu.cp_step()
+    tol_e = 1e-8 if precision == cuwaves.CUW_PREC_FP64 else 1e-6 * inp["nat"]
+    tol_f = 1e-6 if precision == cuwaves.CUW_PREC_FP64 else 1e-4
+    assert abs(og[0] - oc[0]) < tol_e
+    assert np.abs(fg - fc).max() < tol_f
+
+    # permuted and truncated G vectors: mapped by G vector, the rest zero
+    d = rf.parse_waves(rf.read_records(a))
+    perm = np.random.default_rng(3).permutation(d["ngg"])
+    keep = d["ngg"] - 40
+    c = tmp_path / "perm.rst"
+    rf.write_records(c, rf.permuted(rf.read_records(a), perm, keep))
+    gpu.read_restart(c)
+    want = d["psi"][0].copy()
+    want[:, perm[keep:]] = 0.0
+    assert np.array_equal(gpu.download_psi(CUW_PSI0), want)
+    # a file for another band count is refused and leaves the handle usable
+    import struct
+    bad = rf.read_records(a)
+    bad[2] = bad[2][:16] + struct.pack("<i", inp["nb"] + 2) + bad[2][20:]
+    rf.write_records(tmp_path / "bad.rst", bad)
+    with pytest.raises(WavesError):
+        gpu.read_restart(tmp_path / "bad.rst")
+    gpu.read_restart(a)
+    assert np.array_equal(gpu.download_psi(CUW_PSI0), d["psi"][0])

@@ -226,3 +226,65 @@ def test_oracle_density_and_denmat(oracle):
         assert np.abs(d[a].imag).max() == 0.0 and np.abs(e[a].imag).max() == 0.0
         assert np.abs(e[a] - e[a].T).max() < 1e-13 * max(1.0, np.abs(e[a]).max())
         p0 += lmnx
+
+
+def test_oracle_restart_records(oracle, tmp_path):
+    """WAVES$WRITE record layout, read back into a fresh set: the next steps
+    are bit-identical; a file with its G vectors permuted and a part of them
+    missing maps by G vector and zero-fills the rest (WAVES_READPSI)."""
+    import restart_file as rf
+
+    s = systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry")
+    inp = systems.build_inputs(s)
+    w = oracle.open_oracle(inp).setup().initialize()
+    for _ in range(3):
+        w.cp_step()
+    p = tmp_path / "a.rst"
+    w.write_restart(p, inp["rbas"])
+    d = rf.parse_waves(rf.read_records(p))
+    assert (d["id"], d["name"], d["version"], d["notes"]) == ("WAVES", "NONE", "AUG1996", "NONE")
+    assert (d["nkpt"], d["nspin"], d["nwave"], d["ndim"], d["tsuper"]) == (1, 1, 2, 1, 1)
+    assert d["ngg"] == w.ngl and d["nb"] == w.nb and d["nlambda"] == 2
+    assert np.array_equal(d["rbas"], np.asarray(inp["rbas"], dtype=np.float64))
+    assert np.array_equal(d["igvec"], np.asarray(inp["igvec"]).reshape(-1, 3))
+    assert np.array_equal(d["psi"][0], w.download_psi(0))
+    assert np.array_equal(d["psi"][1], w.download_psi(1))
+    assert np.array_equal(d["lambda"][0], w.get_rlam0())
+    # RBAS from the handle's GBAS when none is given
+    q = tmp_path / "b.rst"
+    w.write_restart(q)
+    r2 = rf.parse_waves(rf.read_records(q))["rbas"]
+    assert np.abs(r2 - np.asarray(inp["rbas"])).max() < 1e-12 * np.abs(inp["rbas"]).max()
+
+    v = oracle.open_oracle(inp).setup()
+    v.read_restart(p)
+    assert np.array_equal(v.download_psi(0), w.download_psi(0))
+    assert np.array_equal(v.download_psi(1), w.download_psi(1))
+    # PROJ is not in the file: both form it from PSI0, as a run does at its
+    # first step (WAVES$ETOT at TFIRST)
+    w.projections()
+    v.projections()
+    for _ in range(2):
+        ea, eb = w.cp_step(), v.cp_step()
+    assert np.array_equal(w.download_psi(0), v.download_psi(0))
+    assert np.array_equal(ea[0], eb[0]) and np.array_equal(ea[1], eb[1])
+
+    # permuted and truncated G set
+    rng = np.random.default_rng(7)
+    perm = rng.permutation(d["ngg"])
+    keep = d["ngg"] - 50
+    rf.write_records(tmp_path / "c.rst", rf.permuted(rf.read_records(p), perm, keep))
+    u = oracle.open_oracle(inp).setup()
+    u.read_restart(tmp_path / "c.rst")
+    want0, want1 = d["psi"][0].copy(), d["psi"][1].copy()
+    want0[:, perm[keep:]] = 0.0
+    want1[:, perm[keep:]] = 0.0
+    assert np.array_equal(u.download_psi(0), want0)
+    assert np.array_equal(u.download_psi(1), want1)
+    # a file of another band count is refused
+    bad = rf.read_records(p)
+    import struct
+    bad[2] = bad[2][:16] + struct.pack("<i", w.nb + 2) + bad[2][20:]
+    rf.write_records(tmp_path / "d.rst", bad)
+    with pytest.raises(Exception):
+        oracle.open_oracle(inp).setup().read_restart(tmp_path / "d.rst")
