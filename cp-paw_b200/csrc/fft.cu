@@ -392,6 +392,22 @@ __device__ __forceinline__ C from_d2(double2 a) {
 __device__ __forceinline__ double2 to_d2(double2 a) { return a; }
 __device__ __forceinline__ double2 to_d2(float2 a) { return make_double2((double)a.x, (double)a.y); }
 
+// Shared-memory layout of an xy plane: rows of NR1 elements at a stride of
+// NR1+1, and the x lines transformed with consecutive threads on consecutive
+// rows.  With the odd stride, the eight (FP64) or sixteen (FP32) threads that
+// share a shared-memory wavefront touch eight/sixteen different 16/8-byte bank
+// groups in every Stockham stage; with the dense stride NR1 = 2^k, the
+// scattered writes of the first radix-8 stage of the x lines (stride 8
+// elements) hit one bank group eight times.
+__host__ __device__ constexpr int plane_stride(int nr1) { return nr1 + 1; }
+// row index of the dense plane offset i (i / NR1, with a constant divisor when
+// the kernel is specialised for one length)
+template <int N>
+__device__ __forceinline__ int row_of(int i, int nr1) {
+  if constexpr (N > 0) return i / N;
+  else return i / nr1;
+}
+
 // ---------------------------------------------------------------------------
 // The kernels take the work-grid type C (double2 or float2); the sphere
 // coefficients psi/out stay FP64 and are converted at the gather/scatter.
@@ -402,12 +418,12 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
                  AxisArg a1, AxisArg a2, const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2;
-  C* plane = sm;
-  C* tw1 = sm + npl;
+  const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2, ps = plane_stride(nr1);
+  C* plane = sm;  // [nr2][ps]
+  C* tw1 = sm + nr2 * ps;
   C* tw2 = tw1 + nr1;
   const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
-  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = CT<C>::mk(0, 0);
+  for (int i = threadIdx.x; i < nr2 * ps; i += blockDim.x) plane[i] = CT<C>::mk(0, 0);
   load_tw(tw1, tw1g, nr1, +1.0);
   load_tw(tw2, tw2g, nr2, +1.0);
   __syncthreads();
@@ -415,10 +431,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x)
     plane[plane_pos[k]] = from_d2<C>(src[plane_g[k]]);
   __syncthreads();
-  xform<N>(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)1);   // x lines
-  xform<N>(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)1);  // y lines
+  xform<N>(plane, a1, nr2, ps, 1, false, tw1, (typename CT<C>::R)1);  // x lines
+  xform<N>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);  // y lines
   C* dst = grid + ((size_t)bl * nzp + p) * npl;
-  for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i];
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i + row_of<N>(i, nr1)];
 }
 
 constexpr int kTX = 16;  // x columns per z-column block, generic kernels
@@ -542,18 +558,18 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
                  const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2;
-  C* plane = sm;
-  C* tw1 = sm + npl;
+  const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2, pst = plane_stride(nr1);
+  C* plane = sm;  // [nr2][pst]
+  C* tw1 = sm + nr2 * pst;
   C* tw2 = tw1 + nr1;
   const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
   const C* srcp = grid + ((size_t)bl * nzp + p) * npl;
-  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i] = srcp[i];
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i + row_of<N>(i, nr1)] = srcp[i];
   load_tw(tw1, tw1g, nr1, -1.0);
   load_tw(tw2, tw2g, nr2, -1.0);
   __syncthreads();
-  xform<N>(plane, a2, nr1, 1, nr1, false, tw2, (typename CT<C>::R)-1);  // y lines
-  xform<N>(plane, a1, nr2, nr1, 1, true, tw1, (typename CT<C>::R)-1);   // x lines
+  xform<N>(plane, a2, nr1, 1, pst, false, tw2, (typename CT<C>::R)-1);  // y lines
+  xform<N>(plane, a1, nr2, pst, 1, false, tw1, (typename CT<C>::R)-1);  // x lines
   double2* dst = out + (size_t)ldg * b;
   const double2* ps = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
@@ -599,7 +615,7 @@ template <class C, int N>
 static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   const size_t npl = (size_t)nr1 * nr2;
-  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
+  const int smem_plane = (int)(((size_t)nr2 * plane_stride(nr1) + nr1 + nr2) * sizeof(C));
   const int smem_z = (int)(((size_t)nr3 * tx_of<N>() + nr3) * sizeof(C));
   const int tp = kPlaneThreads;
   const int tz = kPlaneThreads;
@@ -633,8 +649,7 @@ template <class C, int N>
 static int fft_density_t(Handle* h, const double2* psi, double* rho) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   if (nr3 * kRhoTX > 8 * kPlaneThreads) return h->fail(CUW_ERR_UNSUPPORTED, "density: NR3 above 128");
-  const size_t npl = (size_t)nr1 * nr2;
-  const int smem_plane = (int)((npl + nr1 + nr2) * sizeof(C));
+  const int smem_plane = (int)(((size_t)nr2 * plane_stride(nr1) + nr1 + nr2) * sizeof(C));
   const int smem_rho = (int)(((size_t)nr3 * kRhoTX + nr3) * sizeof(C));
   AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
   Device& g = h->g;
@@ -676,7 +691,8 @@ int fft_setup(Handle* h, const int* igvec) {
   const size_t npl = (size_t)nr1 * nr2;
   // work-grid element: FP64 complex, or FP32 complex on the mixed path
   const size_t es = h->mixed() ? sizeof(float2) : sizeof(double2);
-  if ((npl + nr1 + nr2) * es > (size_t)(220 * 1024) || ((size_t)nr3 * kTX + nr3) * es > 14000 * sizeof(double2))
+  const size_t plane_elems = (size_t)nr2 * plane_stride(nr1) + nr1 + nr2;
+  if (plane_elems * es > (size_t)(220 * 1024) || ((size_t)nr3 * kTX + nr3) * es > 14000 * sizeof(double2))
     return h->fail(CUW_ERR_UNSUPPORTED, "FFT plane too large for shared memory");
   // occupied planes and the per-plane G lists
   std::vector<int> cnt(nr3, 0);
@@ -686,7 +702,7 @@ int fft_setup(Handle* h, const int* igvec) {
     int i2 = ((igvec[3 * g + 1] % nr2) + nr2) % nr2;
     int i3 = ((igvec[3 * g + 2] % nr3) + nr3) % nr3;
     iz_of[g] = i3;
-    pos_of[g] = i1 + nr1 * i2;
+    pos_of[g] = i1 + plane_stride(nr1) * i2;  // padded shared-memory plane
     cnt[i3]++;
   }
   std::vector<int> zslot(nr3, -1), plane_iz, off(1, 0);
@@ -738,7 +754,7 @@ int fft_setup(Handle* h, const int* igvec) {
     CUW_TRY(cudaMalloc(tws[a], sizeof(double2) * n));
     CUW_TRY(cudaMemcpy(*tws[a], t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   }
-  const int smem_plane = (int)((npl + nr1 + nr2) * es);
+  const int smem_plane = (int)(plane_elems * es);
   const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * es);
   // cubic grids of a specialised length get kernels compiled for that length
   const int nc = (nr1 == nr2 && nr2 == nr3) ? nr1 : 0;
