@@ -93,3 +93,13 @@ def permuted(recs, perm, keep):
             out[k] = np.ascontiguousarray(band[sel]).tobytes()
             k += 1
     return out
+
+
+def static(recs):
+    """The section as a static restart writes it (NWAVE = 1: PSI0 only, no PSIM
+    records), with NREC of the separator adjusted."""
+    d = parse_waves(recs)
+    nbh = len(d["psi"][0])
+    out = [recs[0], recs[1][:80] + struct.pack("<i", 1)] + list(recs[2:4 + nbh]) + list(recs[4 + 2 * nbh:])
+    out[0] = struct.pack("<i", len(out) - 1) + recs[0][4:]
+    return out

@@ -330,6 +330,11 @@ def test_restart_records(precision, oracle, inputs_cache, tmp_path):
     want = d["psi"][0].copy()
     want[:, perm[keep:]] = 0.0
     assert np.array_equal(gpu.download_psi(CUW_PSI0), want)
+    # a static restart (NWAVE = 1) starts PSIM from PSI0
+    rf.write_records(tmp_path / "static.rst", rf.static(rf.read_records(a)))
+    gpu.read_restart(tmp_path / "static.rst")
+    assert np.array_equal(gpu.download_psi(CUW_PSI0), d["psi"][0])
+    assert np.array_equal(gpu.download_psi(CUW_PSIM), d["psi"][0])
     # a file for another band count is refused and leaves the handle usable
     import struct
     bad = rf.read_records(a)

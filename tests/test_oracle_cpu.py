@@ -281,6 +281,12 @@ def test_oracle_restart_records(oracle, tmp_path):
     want1[:, perm[keep:]] = 0.0
     assert np.array_equal(u.download_psi(0), want0)
     assert np.array_equal(u.download_psi(1), want1)
+    # a static restart (NWAVE = 1) starts PSIM from PSI0
+    rf.write_records(tmp_path / "s.rst", rf.static(rf.read_records(p)))
+    t = oracle.open_oracle(inp).setup()
+    t.read_restart(tmp_path / "s.rst")
+    assert np.array_equal(t.download_psi(0), d["psi"][0])
+    assert np.array_equal(t.download_psi(1), d["psi"][0])
     # a file of another band count is refused
     bad = rf.read_records(p)
     import struct
