@@ -488,6 +488,84 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   }
 }
 
+// z transforms of one y row for a 64^3 grid without block-wide barriers.
+// Each x column is transformed by the 8 lanes t = 0..7 of a warp quarter-group
+// as 64 = 8 x 8 (Cooley-Tukey): a radix-8 DFT over the lane's strided elements
+// x[t + 8r], the twiddles exp(sgn 2 pi i t k1/64), a transpose through the
+// column's own 64 shared-memory slots, and a radix-8 DFT across the lanes, which
+// leaves X[t + 8 k2] in lane t, the same distribution as the input.  V(r) is
+// applied in registers between the G->R and the R->G transforms, so the only
+// block barriers are around the coalesced load and store of the tile.
+//
+// Shared-memory banks: the tile's row stride kZ64Ld = 68 and the rotated slot
+// order of the transpose ((t + k1) mod 8) put the lanes of one wavefront
+// (8 lanes of 16 bytes, or 16 lanes of 8 bytes) on different bank groups in
+// every access.
+constexpr int kZ64Ld = 68;
+constexpr int kZ64Smem = 64 * kZ64Ld + 2 * 64;  // elements: tile and two twiddle tables
+
+// on entry a[r] = x[t + 8r]; on exit a[k] = X[t + 8k], X[k] = sum_n x[n] tw[nk mod 64]
+// with tw[k] = exp(sgn 2 pi i k/64); col[q * kZ64Ld] are the column's slots
+template <class C>
+__device__ __forceinline__ void z64(C (&a)[8], C* col, int t, const C* tw, typename CT<C>::R sgn) {
+  Bfly<8>::run(a, sgn, tw, 64);
+#pragma unroll
+  for (int k1 = 1; k1 < 8; ++k1) a[k1] = cmul(a[k1], tw[t * k1]);
+  __syncwarp();  // the lanes' earlier reads of the slots are done
+#pragma unroll
+  for (int k1 = 0; k1 < 8; ++k1) col[(k1 * 8 + ((t + k1) & 7)) * kZ64Ld] = a[k1];
+  __syncwarp();
+#pragma unroll
+  for (int n1 = 0; n1 < 8; ++n1) a[n1] = col[(t * 8 + ((n1 + t) & 7)) * kZ64Ld];
+  Bfly<8>::run(a, sgn, tw, 64);
+}
+
+template <class C>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_zcol_v64(C* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot, int nzp, int nr2,
+               const double2* __restrict__ tw3g, double scale) {
+  using T = typename CT<C>::R;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  C* tile = sm;               // [64 z][kZ64Ld], x columns 0..63
+  C* twp = sm + 64 * kZ64Ld;  // exp(+2 pi i k/64)
+  C* twm = twp + 64;          // exp(-2 pi i k/64)
+  const int iy = blockIdx.x, bl = blockIdx.y;
+  const size_t npl = (size_t)64 * nr2;
+  C* gb = grid + (size_t)bl * nzp * npl;
+  load_tw(twp, tw3g, 64, +1.0);
+  load_tw(twm, tw3g, 64, -1.0);
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+    const int iz = i >> 6, x = i & 63, s = zslot[iz];
+    tile[iz * kZ64Ld + x] = s >= 0 ? gb[(size_t)s * npl + (size_t)iy * 64 + x] : CT<C>::mk(0, 0);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = lane >> 2, l = lane & 3;
+  for (int round = 0; round < 2; ++round) {  // 8 warps x 2 rounds x 4 columns
+    const int x = warp * 8 + round * 4 + l;
+    C* col = tile + x;
+    C a[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) a[r] = col[(t + 8 * r) * kZ64Ld];
+    z64(a, col, t, twp, (T)1);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int iz = t + 8 * k;
+      a[k] = cscale(a[k], (T)(v[(size_t)x + 64 * ((size_t)iy + (size_t)nr2 * iz)] * scale));
+    }
+    z64(a, col, t, twm, (T)-1);
+    __syncwarp();  // the transpose reads are done before the slots take the result
+#pragma unroll
+    for (int k = 0; k < 8; ++k) col[(t + 8 * k) * kZ64Ld] = a[k];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+    const int iz = i >> 6, x = i & 63, s = zslot[iz];
+    if (s >= 0) gb[(size_t)s * npl + (size_t)iy * 64 + x] = tile[iz * kZ64Ld + x];
+  }
+}
+
 // Pseudo density of WAVES_DENSITY (src/paw_waves1.f90:5377-5500) for super
 // wave functions at the Gamma point: after the x/y passes of k_gtor_plane, the
 // G->R z transform of kRhoTX x columns of every band of the batch in turn, and
@@ -629,10 +707,16 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
                                                                       g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
                                                                       g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
-    const int nxb = (nr1 + tx_of<N>() - 1) / tx_of<N>();
-    k_zcol_v<C, N><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
-                                                                scale);
-    CUW_LAUNCH_CHECK("k_zcol_v");
+    if constexpr (N == 64) {
+      k_zcol_v64<C><<<dim3(nr2, nb), tz, kZ64Smem * (int)sizeof(C), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
+                                                                                 g.tw3, scale);
+      CUW_LAUNCH_CHECK("k_zcol_v64");
+    } else {
+      const int nxb = (nr1 + tx_of<N>() - 1) / tx_of<N>();
+      k_zcol_v<C, N><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3,
+                                                                  g.tw3, scale);
+      CUW_LAUNCH_CHECK("k_zcol_v");
+    }
     k_rtog_plane<C, N><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
                                                                       g.plane_pos, out, psi, h->ldg, b0, g.g2,
                                                                       g.bucket, add_kinetic ? 1 : 0, a1, a2,
@@ -675,6 +759,7 @@ static int fft_select(Handle* h, int smem_plane, int /*smem_z of the generic ker
   CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_zcol_v<C, N>, smem_z));
+  if constexpr (N == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, kZ64Smem * (int)sizeof(C)));
   CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
   h->fft_run = &fft_vpsi_t<C, N>;
   h->fft_rho = &fft_density_t<C, N>;
