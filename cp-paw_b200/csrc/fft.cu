@@ -503,6 +503,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
 // every access.
 constexpr int kZ64Ld = 68;
 constexpr int kZ64Smem = 64 * kZ64Ld + 2 * 64;  // elements: tile and two twiddle tables
+// bytes of shared memory of k_zcol_v64<C>: the elements above and the y row of
+// V(r) * scale as [64 z][kZ64Ld] real numbers of the work-grid precision
+template <class C>
+constexpr int z64_smem_bytes() { return kZ64Smem * (int)sizeof(C) + 64 * kZ64Ld * (int)sizeof(typename CT<C>::R); }
 
 // on entry a[r] = x[t + 8r]; on exit a[k] = X[t + 8k], X[k] = sum_n x[n] tw[nk mod 64]
 // with tw[k] = exp(sgn 2 pi i k/64); col[q * kZ64Ld] are the column's slots
@@ -530,6 +534,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   C* tile = sm;               // [64 z][kZ64Ld], x columns 0..63
   C* twp = sm + 64 * kZ64Ld;  // exp(+2 pi i k/64)
   C* twm = twp + 64;          // exp(-2 pi i k/64)
+  T* vrow = reinterpret_cast<T*>(twm + 64);  // [64 z][kZ64Ld]: V(x, iy, z) * scale
   const int iy = blockIdx.x, bl = blockIdx.y;
   const size_t npl = (size_t)64 * nr2;
   C* gb = grid + (size_t)bl * nzp * npl;
@@ -538,6 +543,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
     const int iz = i >> 6, x = i & 63, s = zslot[iz];
     tile[iz * kZ64Ld + x] = s >= 0 ? gb[(size_t)s * npl + (size_t)iy * 64 + x] : CT<C>::mk(0, 0);
+    vrow[iz * kZ64Ld + x] = (T)(v[(size_t)x + 64 * ((size_t)iy + (size_t)nr2 * iz)] * scale);
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -550,10 +556,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
     for (int r = 0; r < 8; ++r) a[r] = col[(t + 8 * r) * kZ64Ld];
     z64(a, col, t, twp, (T)1);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int iz = t + 8 * k;
-      a[k] = cscale(a[k], (T)(v[(size_t)x + 64 * ((size_t)iy + (size_t)nr2 * iz)] * scale));
-    }
+    for (int k = 0; k < 8; ++k) a[k] = cscale(a[k], vrow[(t + 8 * k) * kZ64Ld + x]);
     z64(a, col, t, twm, (T)-1);
     __syncwarp();  // the transpose reads are done before the slots take the result
 #pragma unroll
@@ -708,7 +711,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
                                                                       g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
     if constexpr (N == 64) {
-      k_zcol_v64<C><<<dim3(nr2, nb), tz, kZ64Smem * (int)sizeof(C), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
+      k_zcol_v64<C><<<dim3(nr2, nb), tz, z64_smem_bytes<C>(), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
                                                                                  g.tw3, scale);
       CUW_LAUNCH_CHECK("k_zcol_v64");
     } else {
@@ -759,7 +762,7 @@ static int fft_select(Handle* h, int smem_plane, int /*smem_z of the generic ker
   CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_zcol_v<C, N>, smem_z));
-  if constexpr (N == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, kZ64Smem * (int)sizeof(C)));
+  if constexpr (N == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, z64_smem_bytes<C>()));
   CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
   h->fft_run = &fft_vpsi_t<C, N>;
   h->fft_rho = &fft_density_t<C, N>;
