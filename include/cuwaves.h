@@ -146,7 +146,10 @@ int cuwaves_denmat(cuw_handle* h, int lmnxx, double* denmat, double* edenmat);
  * (4-byte length markers).  rbas(3,3) = CELL T(0), or NULL to derive it from
  * the G set's GBAS.  cuwaves_read_restart reads such a section back as
  * WAVES_READPSI (:5147-5513) does for the same bands: G vectors are matched by
- * IGVEC in any order; NWAVE = 1 sets PSIM = PSI0. */
+ * IGVEC in any order, those the file lacks start at zero; NWAVE = 1 sets
+ * PSIM = PSI0.  PROJ is not in the file: call cuwaves_projections after
+ * reading, as a run does at its first step.  A file of another band count or
+ * layout is refused (CUW_ERR_ARG) before anything on the device changes. */
 int cuwaves_write_restart(cuw_handle* h, const char* path, const double* rbas);
 int cuwaves_read_restart(cuw_handle* h, const char* path);
 /* WAVES$PROPAGATE without cell dynamics (src/paw_waves1.f90:6479-6592). */
