@@ -287,6 +287,11 @@ def test_oracle_restart_records(oracle, tmp_path):
     t.read_restart(tmp_path / "s.rst")
     assert np.array_equal(t.download_psi(0), d["psi"][0])
     assert np.array_equal(t.download_psi(1), d["psi"][0])
+    # a file cut inside a wave-function record is refused
+    raw = p.read_bytes()
+    (tmp_path / "cut.rst").write_bytes(raw[: len(raw) // 2])
+    with pytest.raises(Exception):
+        oracle.open_oracle(inp).setup().read_restart(tmp_path / "cut.rst")
     # a file of another band count is refused
     bad = rf.read_records(p)
     import struct
