@@ -1669,17 +1669,16 @@ int orc_read_restart(orc_handle* h, const char* path) {
     }
   }
   // G vectors that the file lacks become zero (MAPG(IG)=0, src/paw_waves2.f90:5395-5403)
-  if (ok) {
-    std::fill(h->psi0.begin(), h->psi0.end(), cplx(0.0, 0.0));
-    std::fill(h->psim.begin(), h->psim.end(), cplx(0.0, 0.0));
-  }
+  // read into copies; the handle changes only once the whole section is valid
+  std::vector<cplx> psi0(h->psi0.size(), cplx(0.0, 0.0)), psim(h->psim.size(), cplx(0.0, 0.0));
+  std::vector<cplx> rlam0(h->rlam0.size(), cplx(0.0, 0.0)), rlamm(h->rlamm.size(), cplx(0.0, 0.0));
   for (int w = 0; w < nwave && ok; ++w)
     for (int ib = 0; ib < nbh && ok; ++ib) {
       ok = rd(b) && b.size() == 16 * (size_t)ngg;
       for (int i = 0; i < ngg && ok; ++i)
-        if (map[i] >= 0) std::memcpy(&(w ? h->psim : h->psi0)[PS(h, map[i], ib)], b.data() + 16 * (size_t)i, 16);
+        if (map[i] >= 0) std::memcpy(&(w ? psim : psi0)[PS(h, map[i], ib)], b.data() + 16 * (size_t)i, 16);
     }
-  if (ok && nwave == 1) h->psim = h->psi0;
+  if (ok && nwave == 1) psim = psi0;
   ok = ok && rd(b) && b.size() == 24 && b.compare(0, 6, "LAMBDA") == 0;
   int nlambda = 0;
   if (ok) {
@@ -1688,10 +1687,14 @@ int orc_read_restart(orc_handle* h, const char* path) {
   }
   for (int l = 0; l < nlambda && ok; ++l) {
     ok = rd(b) && b.size() == 16 * (size_t)nb * nb;
-    if (ok && l < 2) std::memcpy((l ? h->rlamm : h->rlam0).data(), b.data(), b.size());
+    if (ok && l < 2) std::memcpy((l ? rlamm : rlam0).data(), b.data(), b.size());
   }
   std::fclose(f);
   OCHECK(ok, CUW_ERR_ARG, "restart file does not hold a WAVES section of this set");
+  h->psi0.swap(psi0);
+  h->psim.swap(psim);
+  h->rlam0.swap(rlam0);
+  if (nlambda >= 2) h->rlamm.swap(rlamm);
   h->have_rlamm = nlambda >= 2;
   h->have_hpsi = false;
   return CUW_OK;
