@@ -1043,6 +1043,9 @@ extern "C" int cuwaves_projections_noalloc(int ngl, int ldg, int nbh, int nat, i
   int rc = noalloc_scratch(&scratch);
   if (rc != CUW_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // an error the caller left pending belongs to the caller: it is reported as a
+  // failure of this call but left in place, and nothing is launched
+  if (cudaPeekAtLastError() != cudaSuccess) return CUW_ERR_CUDA;
   int nsm = 148, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1052,7 +1055,8 @@ extern "C" int cuwaves_projections_noalloc(int ngl, int ldg, int nbh, int nat, i
   const int kchunk = ceil_div(ceil_div(ngl, ks), BK) * BK;
   ks = ceil_div(ngl, kchunk);
   // every partial sum that the reduction reads is written by k_proj in this
-  // call, so nothing in the array has to start at zero
+  // call, so nothing in the array has to start at zero; with no error pending
+  // before the launches, cudaGetLastError reports only their own failures
   k_proj<false><<<dim3(tn, tm, ks), NT, smem_bytes<MP11>(), st>>>(
       reinterpret_cast<const double2*>(psi), nullptr, ldg, ngl, nbh, npro, kchunk,
       reinterpret_cast<const ProDesc*>(pdesc), ylm, pro, reinterpret_cast<const double2*>(eigr), scratch, 0);

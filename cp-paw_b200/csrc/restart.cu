@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <string>
 #include <tuple>
@@ -56,9 +57,11 @@ bool write_rec(FILE* f, const Rec& r) {
          std::fwrite(&n, 4, 1, f) == 1;
 }
 
-bool read_rec(FILE* f, std::vector<unsigned char>& out) {
+// Reads one record whose length must be `expect` bytes; a record of another
+// length is refused before any buffer is sized from the file's marker.
+bool read_rec(FILE* f, std::vector<unsigned char>& out, size_t expect) {
   int32_t n = 0, m = 0;
-  if (std::fread(&n, 4, 1, f) != 1 || n < 0) return false;
+  if (std::fread(&n, 4, 1, f) != 1 || n < 0 || (size_t)n != expect) return false;
   out.resize((size_t)n);
   if (n && std::fread(out.data(), 1, (size_t)n, f) != (size_t)n) return false;
   return std::fread(&m, 4, 1, f) == 1 && m == n;
@@ -195,23 +198,25 @@ int restart_read(Handle* h, const char* path) {
     return h->fail(CUW_ERR_ARG, "restart file " + std::string(path) + ": " + m);
   };
   size_t off = 0;
-  if (!read_rec(f, b) || b.size() != 4 + 32 + 32 + 64 + 256) return bad("no WAVES separator");
+  if (!read_rec(f, b, 4 + 32 + 32 + 64 + 256)) return bad("no WAVES separator");
   const int32_t nrec = get<int32_t>(b, off);
   if (get_chars(b, off, 32) != "WAVES") return bad("separator is not WAVES");
-  if (!read_rec(f, b) || b.size() != 4 + 4 + 72 + 4) return bad("record 1");
+  if (!read_rec(f, b, 4 + 4 + 72 + 4)) return bad("record 1");
   off = 0;
   const int nkpt = get<int32_t>(b, off), nspin = get<int32_t>(b, off);
   off += 72;
   const int nwave = get<int32_t>(b, off);
   if (nkpt != 1 || nspin != 1) return bad("one k-point and one spin are supported");
   if (nwave != 1 && nwave != 2) return bad("NWAVE");
-  if (!read_rec(f, b) || b.size() != 8 + 16) return bad("PSI header");
+  if (!read_rec(f, b, 8 + 16)) return bad("PSI header");
   off = 0;
   if (get_chars(b, off, 8) != "PSI") return bad("PSI key");
   const int ngg = get<int32_t>(b, off), ndim = get<int32_t>(b, off), nbf = get<int32_t>(b, off),
             tsuper = get<int32_t>(b, off);
   if (ndim != 1 || tsuper != 1 || nbf != nb) return bad("NDIM, NB or TSUPER differ from the handle");
-  if (!read_rec(f, b) || b.size() != 24 + (size_t)12 * ngg) return bad("G vectors");
+  // a G-vector count that no record length can hold is refused before anything is sized from it
+  if (ngg <= 0 || (size_t)ngg > ((size_t)INT32_MAX - 24) / 12) return bad("NGG");
+  if (!read_rec(f, b, 24 + (size_t)12 * ngg)) return bad("G vectors");
   // the file's G vectors onto this G set (WAVES_READPSI maps by G vector)
   std::map<std::tuple<int, int, int>, int> pos;
   for (int i = 0; i < ngl; ++i) pos[{h->igvec_h[3 * i], h->igvec_h[3 * i + 1], h->igvec_h[3 * i + 2]}] = i;
@@ -227,13 +232,13 @@ int restart_read(Handle* h, const char* path) {
   std::vector<double2> psi((size_t)ngl * nbh * 2, make_double2(0.0, 0.0));
   for (int w = 0; w < nwave; ++w)
     for (int ib = 0; ib < nbh; ++ib) {
-      if (!read_rec(f, b) || b.size() != sizeof(double2) * ngg) return bad("wave-function record");
+      if (!read_rec(f, b, sizeof(double2) * ngg)) return bad("wave-function record");
       double2* dst = psi.data() + ((size_t)w * nbh + ib) * ngl;
       for (int i = 0; i < ngg; ++i)
         if (map[i] >= 0) std::memcpy(&dst[map[i]], b.data() + sizeof(double2) * i, sizeof(double2));
     }
   if (nwave == 1) std::memcpy(psi.data() + (size_t)ngl * nbh, psi.data(), sizeof(double2) * ngl * nbh);
-  if (!read_rec(f, b) || b.size() != 8 + 16) return bad("LAMBDA header");
+  if (!read_rec(f, b, 8 + 16)) return bad("LAMBDA header");
   off = 0;
   if (get_chars(b, off, 8) != "LAMBDA") return bad("LAMBDA key");
   const int nbl = get<int32_t>(b, off);
@@ -242,7 +247,7 @@ int restart_read(Handle* h, const char* path) {
   if (nbl != nb || nlambda < 0 || nlambda > 4) return bad("LAMBDA sizes");
   std::vector<double2> lam((size_t)nb * nb * 2, make_double2(0.0, 0.0));
   for (int l = 0; l < nlambda; ++l) {
-    if (!read_rec(f, b) || b.size() != sizeof(double2) * nb * nb) return bad("LAMBDA record");
+    if (!read_rec(f, b, sizeof(double2) * nb * nb)) return bad("LAMBDA record");
     if (l < 2) std::memcpy(lam.data() + (size_t)l * nb * nb, b.data(), b.size());
   }
   std::fclose(f);
@@ -272,5 +277,11 @@ extern "C" int cuwaves_read_restart(cuw_handle* hp, const char* path) {
   if (!hp) return CUW_ERR_ARG;
   cuw::Handle* h = reinterpret_cast<cuw::Handle*>(hp);
   h->touch();
-  return cuw::restart_read(h, path);
+  // no C++ exception may cross the C ABI: a host allocation that fails while a
+  // damaged file is parsed becomes an argument error of this call
+  try {
+    return cuw::restart_read(h, path);
+  } catch (const std::exception& e) {
+    return h->fail(CUW_ERR_ARG, std::string("restart file ") + path + ": " + e.what());
+  }
 }

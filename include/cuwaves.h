@@ -319,11 +319,14 @@ int cuwaves_tc_gemm_check(int M, int N, int K, const double* A, const double* B,
  *   of each projector), ylm(ngl,LMX), pro(ngl,NBAREPRO), eigr(ngl,nat) complex
  *   exp(-iG.R), proj(nbh,npro) complex output; stream is a cudaStream_t (NULL:
  *   the default stream).  Work is only enqueued on `stream`.
- * Its split-K partial sums use one static device array of 4 MiB that every GPU
- * loading this library holds until exit, so nbh*npro may not exceed 262144
- * (CUW_ERR_ARG otherwise).  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * Its split-K partial sums use one static device array of 4 MiB, so nbh*npro
+ * may not exceed 262144 (CUW_ERR_ARG otherwise).  The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress), which loads this
+ * library's device code there and commits the 4 MiB on that device, where it
+ * stays until the process exits: it must fit the caller's memory cap, and that
+ * first call should come before any stream capture.  An error already pending
+ * on the calling thread is reported (CUW_ERR_CUDA) and left in place.  All
+ * calls share the array: calls that overlap on the GPU race. */
 int cuwaves_projections_noalloc(int ngl, int ldg, int nbh, int nat, int npro, const double* psi,
                                 const int* pdesc, const double* ylm, const double* pro,
                                 const double* eigr, double gweight, double* proj, void* stream);

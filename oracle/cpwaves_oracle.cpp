@@ -1639,24 +1639,29 @@ int orc_read_restart(orc_handle* h, const char* path) {
   OCHECK(h->have_gset && path, CUW_ERR_ARG, "G set or path missing");
   FILE* f = std::fopen(path, "rb");
   OCHECK(f, CUW_ERR_ARG, "cannot open the restart file");
-  auto rd = [&](std::string& b) {
+  // one record of exactly `expect` bytes; another length is refused before
+  // anything is sized from the file's marker
+  auto rd = [&](std::string& b, size_t expect) {
     int32_t n = 0, m = 0;
-    if (std::fread(&n, 4, 1, f) != 1 || n < 0) return false;
+    if (std::fread(&n, 4, 1, f) != 1 || n < 0 || (size_t)n != expect) return false;
     b.resize(n);
     if (n && std::fread(&b[0], 1, n, f) != (size_t)n) return false;
     return std::fread(&m, 4, 1, f) == 1 && m == n;
   };
   const int ngl = h->d.ngl, nb = h->d.nb, nbh = h->d.nbh;
   std::string b;
-  bool ok = rd(b) && b.size() == 388 && b.compare(4, 5, "WAVES") == 0;
+  bool ok = rd(b, 388) && b.compare(4, 5, "WAVES") == 0;
   int32_t v4[4];
-  ok = ok && rd(b) && b.size() == 84;
+  ok = ok && rd(b, 84);
   int32_t nwave = 0;
   if (ok) std::memcpy(&nwave, b.data() + 80, 4);
-  ok = ok && rd(b) && b.size() == 24 && b.compare(0, 3, "PSI") == 0;
+  ok = ok && (nwave == 1 || nwave == 2);
+  ok = ok && rd(b, 24) && b.compare(0, 3, "PSI") == 0;
   if (ok) std::memcpy(v4, b.data() + 8, 16);
+  // a G-vector count that no record can hold is refused before anything is sized from it
+  ok = ok && v4[0] > 0 && (size_t)v4[0] <= ((size_t)INT32_MAX - 24) / 12;
   const int ngg = ok ? v4[0] : 0;
-  ok = ok && v4[2] == nb && rd(b) && b.size() == 24 + (size_t)12 * ngg;
+  ok = ok && v4[2] == nb && rd(b, 24 + (size_t)12 * ngg);
   std::vector<int> map(ngg, -1);
   if (ok) {
     std::map<std::vector<int>, int> pos;
@@ -1674,19 +1679,20 @@ int orc_read_restart(orc_handle* h, const char* path) {
   std::vector<cplx> rlam0(h->rlam0.size(), cplx(0.0, 0.0)), rlamm(h->rlamm.size(), cplx(0.0, 0.0));
   for (int w = 0; w < nwave && ok; ++w)
     for (int ib = 0; ib < nbh && ok; ++ib) {
-      ok = rd(b) && b.size() == 16 * (size_t)ngg;
+      ok = rd(b, 16 * (size_t)ngg);
       for (int i = 0; i < ngg && ok; ++i)
         if (map[i] >= 0) std::memcpy(&(w ? psim : psi0)[PS(h, map[i], ib)], b.data() + 16 * (size_t)i, 16);
     }
   if (ok && nwave == 1) psim = psi0;
-  ok = ok && rd(b) && b.size() == 24 && b.compare(0, 6, "LAMBDA") == 0;
+  ok = ok && rd(b, 24) && b.compare(0, 6, "LAMBDA") == 0;
   int nlambda = 0;
   if (ok) {
     std::memcpy(v4, b.data() + 8, 16);
     nlambda = v4[3];
+    ok = v4[0] == nb && nlambda >= 0 && nlambda <= 4;
   }
   for (int l = 0; l < nlambda && ok; ++l) {
-    ok = rd(b) && b.size() == 16 * (size_t)nb * nb;
+    ok = rd(b, 16 * (size_t)nb * nb);
     if (ok && l < 2) std::memcpy((l ? rlamm : rlam0).data(), b.data(), b.size());
   }
   std::fclose(f);

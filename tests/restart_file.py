@@ -103,3 +103,17 @@ def static(recs):
     out = [recs[0], recs[1][:80] + struct.pack("<i", 1)] + list(recs[2:4 + nbh]) + list(recs[4 + 2 * nbh:])
     out[0] = struct.pack("<i", len(out) - 1) + recs[0][4:]
     return out
+
+
+def damaged(path):
+    """(name, bytes) of two corrupt copies of a restart section: NGG = -5 in the
+    PSI header, and a G-vector record whose leading length marker claims
+    2**31 - 1 bytes."""
+    recs = read_records(path)
+    neg = list(recs)
+    neg[2] = recs[2][:8] + struct.pack("<i", -5) + recs[2][12:]
+    raw_neg = b"".join(struct.pack("<i", len(r)) + r + struct.pack("<i", len(r)) for r in neg)
+    raw = bytearray(open(path, "rb").read())
+    off = sum(8 + len(r) for r in recs[:3])
+    struct.pack_into("<i", raw, off, 2**31 - 1)
+    return [("neg_ngg.rst", raw_neg), ("huge_rec.rst", bytes(raw))]

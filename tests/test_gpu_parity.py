@@ -344,3 +344,10 @@ def test_restart_records(precision, oracle, inputs_cache, tmp_path):
         gpu.read_restart(tmp_path / "bad.rst")
     gpu.read_restart(a)
     assert np.array_equal(gpu.download_psi(CUW_PSI0), d["psi"][0])
+    # a negative G-vector count or a 2 GB record marker is an argument error
+    # of the call, and the handle keeps its state
+    for fname, raw in rf.damaged(a):
+        (tmp_path / fname).write_bytes(raw)
+        with pytest.raises(WavesError):
+            gpu.read_restart(tmp_path / fname)
+        assert np.array_equal(gpu.download_psi(CUW_PSI0), d["psi"][0])

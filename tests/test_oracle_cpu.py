@@ -302,3 +302,11 @@ def test_oracle_restart_records(oracle, tmp_path):
     rf.write_records(tmp_path / "d.rst", bad)
     with pytest.raises(Exception):
         oracle.open_oracle(inp).setup().read_restart(tmp_path / "d.rst")
+    # a negative G-vector count and a record marker of 2 GB are refused as
+    # argument errors, before anything is sized from them
+    for name, raw in rf.damaged(p):
+        (tmp_path / name).write_bytes(raw)
+        with pytest.raises(Exception):
+            u2.read_restart(tmp_path / name)
+        assert np.array_equal(u2.download_psi(0), d["psi"][0])
+
