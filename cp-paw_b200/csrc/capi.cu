@@ -927,6 +927,46 @@ extern "C" int cuwaves_gramschmidt(cuw_handle* hp, int which, const double* r) {
 //   fused ADDPRO (HPSI, OPSI, PROPAGATE) | <psi|H|psi> | atoms |
 //   ORTHOGONALIZE at R(+) | WAVEKINETIC(2) | SWITCH
 // Single-point evaluation at the current wave functions and positions, the
+// The orthonormality test of WAVES$ORTHOGONALIZE (TTEST block,
+// src/paw_waves2.f90:421-460): MAT = <psi_i|O|psi_j> of PSI0, plane-wave part
+// (WAVES_OVERLAP) plus one-centre part (WAVES_1COVERLAP) of projections formed
+// afresh at R(0), as the real NB x NB matrix of the Gamma point.  Always FP64,
+// whatever the handle's precision, so that it measures the state itself.
+// Uses only scratch of the step (PBUF, HPROJ, TMAT, WK2); PROJ is untouched.
+extern "C" int cuwaves_overlap_check(cuw_handle* hp, double* mat, double* maxdev) {
+  H(hp);
+  NEED(h->have_gset && h->have_do, CUW_ERR_STATE, "inputs not loaded");
+  NEED(mat || maxdev, CUW_ERR_ARG, "no output");
+  Device& g = h->g;
+  struct Fp64 {
+    Handle* h;
+    bool old;
+    ~Fp64() { h->fp64_only = old; }
+  } fp64{h, h->fp64_only};
+  h->fp64_only = true;
+  const int nb = h->d.nb, nbh = h->d.nbh;
+  const size_t mn = (size_t)nbh * nbh;
+  CUW_RET(eigr_compute(h, g.r0));
+  CUW_RET(proj_compute(h, g.psi0, g.pbuf, nullptr, nullptr));
+  CUW_RET(oproj_compute(h, g.pbuf, g.hproj));
+  double2* pw = g.tmat;
+  double2* oc = g.tmat + 2 * mn;
+  GramPair pc[1] = {{g.pbuf, g.hproj}};
+  CUW_RET(gram_projections(h, pc, 1, oc));
+  GramPair pp[1] = {{g.psi0, g.psi0}};
+  CUW_RET(gram_planewave(h, pp, 1, pw));
+  CUW_RET(unravel_run(h, pw, oc, 1, g.wk2, nullptr, nullptr));
+  std::vector<double> m((size_t)nb * nb);
+  CUW_TRY(cudaMemcpyAsync(m.data(), g.wk2, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  double dev = 0.0;
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) dev = std::max(dev, std::fabs(m[i + (size_t)nb * j] - (i == j ? 1.0 : 0.0)));
+  if (mat) std::memcpy(mat, m.data(), sizeof(double) * m.size());
+  if (maxdev) *maxdev = dev;
+  return CUW_OK;
+}
+
 // energy part of WAVES$ETOT (src/paw_waves1.f90:2094-2123 with EKIN and FORCE):
 // out[0] = sum_n f_n <psi_n|H|psi_n>, out[1] = kinetic energy; force (3*NAT)
 // at R(0).  Leaves H|psi> in HPSI; nothing is propagated.

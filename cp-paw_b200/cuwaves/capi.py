@@ -84,6 +84,7 @@ SIGNATURES = {
     "stop": [_P],
     "cp_step": [_P, C.c_int, _D, C.c_int, C.c_double, _D, _D],
     "etot": [_P, _D, _D],
+    "overlap_check": [_P, _D, _D],
 }
 OPTIONAL = {
     "set_async": [_P, C.c_int],
@@ -365,6 +366,15 @@ class Waves:
         f = np.zeros((self.nat, 3)) if want_force else None
         self._chk(self._f["etot"](self.h, _dptr(out), _dptr(f)), "ETOT")
         return out, f
+
+    def overlap_check(self):
+        """(MAT, max|MAT - 1|): <psi_i|O|psi_j> of PSI0 with projections formed
+        afresh at R(0), the orthonormality test of WAVES$ORTHOGONALIZE.  MAT is
+        returned as an (NB, NB) array indexed [j, i]."""
+        m = np.empty((self.nb, self.nb))
+        x = C.c_double()
+        self._chk(self._f["overlap_check"](self.h, _dptr(m), C.byref(x)), "overlap_check")
+        return m, x.value
 
     def set_async(self, flag: bool):
         if "set_async" in self._f:

@@ -182,6 +182,16 @@ int cuwaves_reset_atoms(cuw_handle* h, const double* r0);
  * force (3*NAT, may be NULL).  Nothing is propagated. */
 int cuwaves_etot(cuw_handle* h, double* out, double* force);
 
+/* Orthonormality test of WAVES$ORTHOGONALIZE (its TTEST block,
+ * src/paw_waves2.f90:421-460) for PSI0 at R(0), e.g. after cuwaves_cp_step:
+ * projections of PSI0 formed afresh, mat(NB,NB) = <psi_i|O|psi_j> (plane-wave
+ * plus one-centre overlap, real at the Gamma point; may be NULL) and
+ * *maxdev = max_ij |mat(i,j) - delta_ij| (may be NULL).  The reference
+ * diagonalises the matrix and stops when an eigenvalue is off 1 by more than
+ * 1e-4; the caller applies its own bound.  Computed in FP64 on both precision
+ * paths; PROJ and the step state are not changed. */
+int cuwaves_overlap_check(cuw_handle* h, double* mat, double* maxdev);
+
 /* Serving runtime (no counterpart in the reference, which runs one system per
  * program: PAW_DRIVER's time loop, src/paw_driver.f90:280-561).  A request
  * carries the complete input of one wave-function set, with the meanings and

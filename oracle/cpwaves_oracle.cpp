@@ -1171,6 +1171,30 @@ int orc_orthogonalize(orc_handle* h, int maxit, double eps, int* iters) {
   return CUW_OK;
 }
 
+// TTEST block of WAVES$ORTHOGONALIZE (src/paw_waves2.f90:421-460) for PSI0:
+// projections at R(0) (waves2:424), WAVES_1COVERLAP (:427) plus WAVES_OVERLAP
+// (:438), real part at the Gamma point, and max|MAT - 1|
+int orc_overlap_check(orc_handle* h, double* mat, double* maxdev) {
+  OCHECK(h->have_gset && h->have_do, CUW_ERR_STATE, "gset/do not set");
+  const int nbh = h->d.nbh, nb = h->d.nb, npro = h->npro;
+  std::vector<cplx> proj((size_t)nbh * npro);
+  projections(h, h->r0.data(), h->psi0.data(), proj.data());
+  const size_t nn = (size_t)nb * nb;
+  std::vector<cplx> m(nn), aux(nn);
+  onecoverlap(h, proj.data(), proj.data(), m.data());
+  overlap(h, true, h->psi0.data(), h->psi0.data(), aux.data());
+  double dev = 0.0;
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) {
+      const size_t k = i + (size_t)nb * j;
+      const double v = (m[k] + aux[k]).real();
+      if (mat) mat[k] = v;
+      dev = std::max(dev, std::fabs(v - (i == j ? 1.0 : 0.0)));
+    }
+  if (maxdev) *maxdev = dev;
+  return CUW_OK;
+}
+
 // WAVES$SWITCH (src/paw_waves2.f90:2180-2317), NLAMBDAX=2, no stress
 int orc_switch(orc_handle* h) {
   std::swap(h->psi0, h->psim);
