@@ -320,10 +320,7 @@ def run_mixed(args, local):
     inp = make_inputs(args.system)
     ref = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_FP64).setup().initialize()
     w = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup()
-    for which in (cuwaves.CUW_PSI0, cuwaves.CUW_PSIM):
-        w.upload_psi(which, ref.download_psi(which))
-    w.set_proj(ref.get_proj())
-    w.set_rlam0(ref.get_rlam0())
+    copy_state(ref, w)
     tuned = w.autotune() if not args.no_autotune else None
     de = df = 0.0
     nacc = 5
@@ -353,6 +350,91 @@ def run_mixed(args, local):
             f"max_dE_per_atom_vs_fp64_{nacc}_steps": de, f"max_dF_vs_fp64_{nacc}_steps": df,
             "gpu_launches": l1 - l0, "autotune": tuned,
             "phase_ms_per_step": {k: round(v / max(1, nsteps), 4) for k, v in phases.items()}}
+
+
+def copy_state(src, dst):
+    """PSI0, PSIM, PROJ and RLAM0 of one handle into another."""
+    import cuwaves
+
+    for which in (cuwaves.CUW_PSI0, cuwaves.CUW_PSIM):
+        dst.upload_psi(which, src.download_psi(which))
+    dst.set_proj(src.get_proj())
+    dst.set_rlam0(src.get_rlam0())
+
+
+AU_TIME_PS = 2.4188843265857e-5  # one atomic unit of time in ps
+
+
+def run_precision(args):
+    """Errors of the mixed path against the FP64 path, per system (Si64 at
+    64^3, 30/60 Ry, and 32 H2O at 72^3, 40/80 Ry):
+    - energy per atom and forces over the first 5 CP steps (moving nuclei) from
+      one state;
+    - orthonormality residual max|<psi_i|O|psi_j> - delta_ij| of PSI0 after every
+      step, formed in FP64 with projections computed afresh (the test of
+      WAVES$ORTHOGONALIZE, src/paw_waves2.f90:421-460, whose bound is 1e-4);
+    - NVE drift: the wave functions are first relaxed with friction (ANNEE)
+      at fixed nuclei, then both paths run `drift_steps` frictionless CP steps
+      with moving nuclei from rest; the conserved energy is assembled as the
+      reference's 'CONSTANT ENERGY' (src/paw_driver.f90:481-535): total energy
+      + wave-function (fictitious) kinetic energy + ionic kinetic energy.  The
+      drift is the least-squares slope of that energy per atom in Ha/atom/ps,
+      with its largest excursion from the start."""
+    import numpy as np
+    import cuwaves
+
+    out = {}
+    for name in args.precision_systems.split(","):
+        inp = make_inputs(name)
+        nat = inp["nat"]
+        ref = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_FP64).setup().initialize()
+        mix = cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup()
+        copy_state(ref, mix)
+        de = df = 0.0
+        ores = {"fp64": 0.0, "mixed": 0.0}
+        for _ in range(5):
+            o_r, f_r = ref.cp_step(move_atoms=True)
+            o_m, f_m = mix.cp_step(move_atoms=True)
+            de = max(de, abs(float(o_m[0]) - float(o_r[0])) / nat)
+            df = max(df, float(np.abs(f_m - f_r).max()))
+            ores["fp64"] = max(ores["fp64"], ref.overlap_check()[1])
+            ores["mixed"] = max(ores["mixed"], mix.overlap_check()[1])
+        # relax the wave functions at fixed nuclei (damped CP), FP64
+        ref.reset_atoms(inp["r0"])
+        ref.set_dynamics(inp["delt"], args.quench_friction)
+        for _ in range(args.quench_steps):
+            ref.cp_step(move_atoms=False)
+        ref.set_dynamics(inp["delt"], 0.0)
+        ref.reset_atoms(inp["r0"])
+        mix.set_dynamics(inp["delt"], 0.0)
+        mix.reset_atoms(inp["r0"])
+        copy_state(ref, mix)
+        drift = {}
+        for tag, w in (("fp64", ref), ("mixed", mix)):
+            econs = []
+            worst = 0.0
+            for k in range(args.drift_steps):
+                o, _ = w.cp_step(move_atoms=True, want_force=False)
+                econs.append(float(o[0] + o[2] + o[3]))
+                if k % 50 == 49:
+                    worst = max(worst, w.overlap_check()[1])
+            e = np.asarray(econs) / nat
+            t_ps = np.arange(len(e)) * inp["delt"] * AU_TIME_PS
+            slope = float(np.polyfit(t_ps, e, 1)[0])
+            drift[tag] = {"slope_ha_per_atom_per_ps": slope,
+                          "max_excursion_ha_per_atom": float(np.abs(e - e[0]).max()),
+                          "orthonormality_residual_max": worst,
+                          "econs_start_ha": float(econs[0]), "econs_end_ha": float(econs[-1])}
+        ref.close()
+        mix.close()
+        out[name] = {
+            "grid": "x".join(map(str, inp["grid"])), "bands": inp["nb"], "atoms": nat,
+            "max_dE_per_atom_vs_fp64_5_steps": de, "max_dF_vs_fp64_5_steps": df,
+            "orthonormality_residual_5_steps": ores,
+            "nve": {"steps": args.drift_steps, "dt_au": inp["delt"], "quench_steps": args.quench_steps,
+                    "quench_friction": args.quench_friction, **drift},
+        }
+    return out
 
 
 def _serve_stream(pool, kinds, rate, nreq, workers, budget_gb, seed):
@@ -551,6 +633,7 @@ def emit_cuda(args, res, world):
         "step_graphs": res.get("graphs"),
         "autotune": res.get("autotune"),
         "mixed": res.get("mixed"),
+        "precision": res.get("precision"),
         "serving": res.get("serving"),
         "batched": res.get("batched"),
         "clocks": res["clocks"],
@@ -628,6 +711,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision (error and drift) runs")
+    ap.add_argument("--precision-systems", default="Si64,H2O32")
+    ap.add_argument("--drift-steps", type=int, default=500)
+    ap.add_argument("--quench-steps", type=int, default=300)
+    ap.add_argument("--quench-friction", type=float, default=0.1)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving and batched runs")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)
@@ -650,6 +738,8 @@ def main():
     res = run_cuda(args, rank, world, local)
     if not args.no_mixed:
         res["mixed"] = run_mixed(args, local)
+        if world == 1 and not args.no_precision:
+            res["precision"] = run_precision(args)
     if not args.no_serving and world == 1:
         res["serving"] = run_serving(args)
         res["batched"] = run_batched(args)

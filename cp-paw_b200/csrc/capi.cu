@@ -197,6 +197,11 @@ __global__ void k_ion_ekin(const double* __restrict__ rp, const double* __restri
   }
 }
 
+__global__ void k_add_vec(double* __restrict__ a, const double* __restrict__ b, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] += b[i];
+}
+
 __global__ void k_copy_psi(const double2* __restrict__ src, double2* __restrict__ dst, size_t n) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
     dst[k] = src[k];
@@ -326,7 +331,7 @@ static int ortho_core(Handle* h, int max_iter, double eps) {
 }
 
 // phase marks of cuwaves_cp_step (only when timing is enabled)
-enum { PH_RED = 0, PH_EIGR, PH_FORCE, PH_FFT, PH_ADDPRO, PH_PROJ, PH_GRAM, PH_ORTHO, PH_ROTATE, PH_MISC };
+enum { PH_RED = 0, PH_EIGR, PH_FORCE, PH_FFT, PH_ADDPRO, PH_PROJ, PH_GRAM, PH_ORTHO, PH_ROTATE, PH_MISC, PH_POT };
 static int mark(Handle* h, int phase) {
   if (!h->timing) return CUW_OK;
   if (h->nev >= (int)h->ev.size()) {
@@ -382,7 +387,9 @@ static void free_all(Handle* h) {
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
                   g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
                   g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1], g.bpre[0],
-                  g.bpre[1], g.bsmall, g.jac_a};
+                  g.bpre[1], g.bsmall, g.jac_a, g.r_plus, g.r_minus, g.r_gx, g.r_gy, g.r_gz, g.r_g2, g.r_ylm,
+                  g.r_g0, g.r_v0, g.r_pscore, g.r_vbar, g.r_lmrx, g.qlm, g.r_rhog, g.r_vg, g.r_pot, g.r_vtot,
+                  g.r_grid, g.r_part, g.fpot, g.vqlm, g.r_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   h->g = Device();
@@ -1012,8 +1019,19 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   CUW_TRY(cudaMemcpyAsync(sc + 2, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   CUW_RET(mark(h, PH_EIGR));
   CUW_RET(eigr_compute(h, g.r0));
+  if (h->scf) {
+    // self-consistent step: the density of PSI0 and POTENTIAL$VOFRHO give the
+    // potential of this step (EHARTREE, EXC, int V rho into sc[5..7])
+    CUW_RET(mark(h, PH_POT));
+    CUW_RET(fft_density(h, g.psi0, g.rho));
+    CUW_RET(vofrho_run(h, g.rho));
+  }
   CUW_RET(mark(h, PH_FORCE));
   CUW_RET(force_dev_run(h, g.force));
+  if (h->scf) {
+    k_add_vec<<<ceil_div(3 * h->d.nat, 128), 128, 0, h->stream>>>(g.force, g.fpot, 3 * h->d.nat);
+    CUW_LAUNCH_CHECK("k_add_vec");
+  }
   CUW_RET(mark(h, PH_FFT));
   CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
   CUW_RET(mark(h, PH_ADDPRO));
@@ -1151,9 +1169,9 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
                        step_graph(h, move_atoms, max_iter, eps, &rc);
   if (!graphed) rc = step_body(h, move_atoms, max_iter, eps);
   if (rc != CUW_OK) return rc;
-  double hs[5];
+  double hs[8];
   int st[2];
-  CUW_TRY(cudaMemcpyAsync(hs, g.scal, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaMemcpyAsync(hs, g.scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
@@ -1168,6 +1186,14 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
     out[3] = hs[4];
     out[4] = iters;
     out[5] = out[6] = out[7] = 0.0;
+    if (h->scf) {
+      // total energy of the self-consistent step: the band energy without
+      // int V rho, plus EHARTREE and EXC
+      out[0] = hs[1] - hs[7] + hs[5] + hs[6];
+      out[5] = hs[5];
+      out[6] = hs[6];
+      out[7] = hs[7];
+    }
   }
   return CUW_OK;
 }
@@ -1229,6 +1255,11 @@ extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
     case CUW_OPT_GRAPHS:
       h->use_graphs = value != 0.0;
       if (!h->use_graphs) h->drop_graphs();
+      return CUW_OK;
+    case CUW_OPT_SELFCONSISTENT:
+      if (value != 0.0 && !(h->have_rhoset && h->have_qlm))
+        return h->fail(CUW_ERR_STATE, "self-consistent steps need cuwaves_set_rhoset and cuwaves_set_qlm");
+      h->scf = value != 0.0;
       return CUW_OK;
     default:
       return h->fail(CUW_ERR_ARG, "unknown option");

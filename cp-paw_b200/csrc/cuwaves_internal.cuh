@@ -117,6 +117,20 @@ struct Device {
   size_t part_bytes = 0;
   double *red = nullptr;         // reductions
   double *scal = nullptr;        // small scalar results
+  // potential (POTENTIAL$VOFRHO): the density G set (one G of each +-G pair),
+  // its tables and work arrays
+  int *r_plus = nullptr, *r_minus = nullptr;   // (NGLH) grid offsets of +G and -G
+  double *r_gx = nullptr, *r_gy = nullptr, *r_gz = nullptr, *r_g2 = nullptr;  // (NGLH)
+  double *r_ylm = nullptr;                     // (LMRXX, NGLH) Y_lm(G) |G|^l
+  double *r_g0 = nullptr, *r_v0 = nullptr, *r_pscore = nullptr, *r_vbar = nullptr;  // (NGLH, NSP)
+  int *r_lmrx = nullptr;                       // (NSP)
+  double *qlm = nullptr;                       // (LMRXX, NAT)
+  double2 *r_rhog = nullptr, *r_vg = nullptr, *r_pot = nullptr, *r_vtot = nullptr;  // (NGLH)
+  double2 *r_grid = nullptr;                   // (NR1*NR2*NR3) full complex grid
+  double *r_part = nullptr;                    // block partial sums
+  double *fpot = nullptr;                      // (3, NAT) Hartree and pseudo-core forces
+  double *vqlm = nullptr;                      // (LMRXX, NAT)
+  double *r_out = nullptr;                     // [0] EHARTREE [1] EXC [2] RHOB of the last cuwaves_vofrho
   // projector-map tables: first IPRO and #LMN per atom, species per atom,
   // (LN, M) of each IPRO, first LMN of each (species, LN), LOX (-1 = none)
   int *t_ipro0 = nullptr, *t_nlmn = nullptr, *t_isp = nullptr, *t_lnofp = nullptr, *t_mofp = nullptr,
@@ -181,7 +195,7 @@ struct Handle {
   // measurement: kernel launches, and per-phase device time of cuwaves_cp_step
   long long launches = 0;
   bool timing = false;
-  static constexpr int kPhases = 10;
+  static constexpr int kPhases = 11;
   double phase_ms[kPhases] = {0};
   long long phase_calls = 0;
   std::vector<cudaEvent_t> ev;
@@ -200,6 +214,10 @@ struct Handle {
   int lyap_max_sweeps = 64;  // sweeps per Lyapunov solve before the fixed point counts as failed
   bool tc_scope_open = false;
   const double* eigr_src = nullptr;  // position buffer (r0, rp or rm) that EIGR (and the fp32 table) was built from
+  // potential: density G set size, LMRXX, index of G = 0 (-1: none), and
+  // whether cuwaves_cp_step forms V(r) from the density first
+  int nglh = 0, lmrxx = 0, ngamma = -1;
+  bool have_rhoset = false, have_qlm = false, scf = false;
   Device g;
   std::string err;
 
@@ -282,6 +300,8 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
 int fft_setup(Handle* h, const int* igvec_host);
 int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic);
 int fft_density(Handle* h, const double2* psi, double* rho);
+int grid_fft(Handle* h, double2* grid, int dir);  // full-grid FP64 transform, unscaled
+int vofrho_run(Handle* h, const double* rho_dev);  // POTENTIAL$VOFRHO on the device
 int denmat_run(Handle* h, int lmnxx, double2* denmat, double2* edenmat);
 int eigr_compute(Handle* h, const double* r_dev);
 int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* psiB, double2* projB);

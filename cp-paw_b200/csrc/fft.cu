@@ -666,6 +666,54 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   }
 }
 
+// One pass of a 3-D transform of a full FP64 complex grid (x fastest), for
+// the single real functions of the potential (PLANEWAVE$SUPFFT of
+// POTENTIAL$VOFRHO): every block transforms kGridTX lines of one axis in
+// shared memory.  x lines are rows (tile [line][x] at a row stride n + 1);
+// y and z lines are taken as kGridTX consecutive x columns of one z plane
+// (axis 1) or one y row (axis 2), loaded and stored coalesced along x.
+constexpr int kGridTX = 16;
+__global__ void __launch_bounds__(kPlaneThreads)
+    k_grid_lines(double2* __restrict__ grid, int nr1, int nr2, int nr3, int axis, AxisArg ax,
+                 const double2* __restrict__ twg, double sgn) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* tile = reinterpret_cast<double2*>(smraw);
+  const int n = ax.n;
+  const int TX = kGridTX;
+  double2* tw = tile + (size_t)TX * (n + 1);
+  load_tw(tw, twg, n, sgn);
+  if (axis == 0) {
+    const int nrows = nr2 * nr3, row0 = blockIdx.x * TX, nl = min(TX, nrows - row0);
+    for (int i = threadIdx.x; i < nl * n; i += blockDim.x) {
+      const int r = i / n, x = i % n;
+      tile[r * (n + 1) + x] = grid[(size_t)(row0 + r) * nr1 + x];
+    }
+    __syncthreads();
+    xform<0>(tile, ax, nl, n + 1, 1, false, tw, sgn);
+    for (int i = threadIdx.x; i < nl * n; i += blockDim.x) {
+      const int r = i / n, x = i % n;
+      grid[(size_t)(row0 + r) * nr1 + x] = tile[r * (n + 1) + x];
+    }
+    return;
+  }
+  // axis 1: lines along y at fixed z; axis 2: lines along z at fixed y
+  const int nxb = (nr1 + TX - 1) / TX;
+  const int x0 = (blockIdx.x % nxb) * TX, other = blockIdx.x / nxb;
+  const size_t es = axis == 1 ? (size_t)nr1 : (size_t)nr1 * nr2;
+  const size_t base = axis == 1 ? (size_t)nr1 * nr2 * other : (size_t)nr1 * other;
+  const int nl = min(TX, nr1 - x0);
+  for (int i = threadIdx.x; i < n * TX; i += blockDim.x) {
+    const int e = i / TX, x = i % TX;
+    tile[i] = x < nl ? grid[base + (size_t)e * es + x0 + x] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  xform<0>(tile, ax, TX, 1, TX, false, tw, sgn);
+  for (int i = threadIdx.x; i < n * TX; i += blockDim.x) {
+    const int e = i / TX, x = i % TX;
+    if (x < nl) grid[base + (size_t)e * es + x0 + x] = tile[i];
+  }
+}
+
 AxisArg make_axis(const AxisPlan& p) {
   AxisArg a;
   a.n = p.n;
@@ -862,6 +910,24 @@ int fft_setup(Handle* h, const int* igvec) {
       rc = h->mixed() ? fft_select<float2, 0>(h, smem_plane, smem_z) : fft_select<double2, 0>(h, smem_plane, smem_z);
   }
   if (rc != CUW_OK) return rc;
+  return CUW_OK;
+}
+
+// 3-D transform of a full FP64 complex grid (x fastest), in place and
+// unscaled: dir = +1 is G->R (exp(+iGr)), dir = -1 is R->G (exp(-iGr)); the
+// caller applies the 1/N of the reference's R->G transform.
+int grid_fft(Handle* h, double2* grid, int dir) {
+  const int n[3] = {h->d.nr1, h->d.nr2, h->d.nr3};
+  const double2* tw[3] = {h->g.tw1, h->g.tw2, h->g.tw3};
+  for (int a = 0; a < 3; ++a) {
+    const AxisArg ax = make_axis(h->ax[a]);
+    const int smem = (int)(((size_t)kGridTX * (n[a] + 1) + n[a]) * sizeof(double2));
+    CUW_TRY(smem_allow((const void*)k_grid_lines, smem));
+    const int nxb = (n[0] + kGridTX - 1) / kGridTX;
+    const int blocks = a == 0 ? ceil_div(n[1] * n[2], kGridTX) : nxb * (a == 1 ? n[2] : n[1]);
+    k_grid_lines<<<blocks, kPlaneThreads, smem, h->stream>>>(grid, n[0], n[1], n[2], a, ax, tw[a], (double)dir);
+    CUW_LAUNCH_CHECK("k_grid_lines");
+  }
   return CUW_OK;
 }
 

@@ -22,6 +22,7 @@ CUW_PREC_FP64, CUW_PREC_MIXED = 0, 1
 CUW_OPT_LYAP_TOL = 1
 CUW_OPT_GRAPHS = 2
 CUW_OPT_LYAP_MAX_SWEEPS = 3
+CUW_OPT_SELFCONSISTENT = 4
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
@@ -85,6 +86,9 @@ SIGNATURES = {
     "cp_step": [_P, C.c_int, _D, C.c_int, C.c_double, _D, _D],
     "etot": [_P, _D, _D],
     "overlap_check": [_P, _D, _D],
+    "set_rhoset": [_P, C.c_int, _I, _D, _D, C.c_int, _I, _D, _D, _D, _D, _D],
+    "set_qlm": [_P, _D],
+    "vofrho": [_P, _D, _D, _D, _D, _D, _D],
 }
 OPTIONAL = {
     "set_async": [_P, C.c_int],
@@ -376,6 +380,48 @@ class Waves:
         self._chk(self._f["overlap_check"](self.h, _dptr(m), C.byref(x)), "overlap_check")
         return m, x.value
 
+    def set_rhoset(self):
+        """Loads the density G set and its tables (inputs key 'rhoset')."""
+        r = self.inp["rhoset"]
+        self._rk = dict(
+            igvec=np.ascontiguousarray(r["igvec"], dtype=np.int32),
+            gvec=np.ascontiguousarray(r["gvec"], dtype=np.float64),
+            g2=np.ascontiguousarray(r["g2"], dtype=np.float64),
+            lmrx=np.ascontiguousarray(r["lmrx"], dtype=np.int32),
+            ylm=np.ascontiguousarray(r["ylm"], dtype=np.float64),
+            g0=np.ascontiguousarray(r["g0"], dtype=np.float64),
+            v0=np.ascontiguousarray(r["v0"], dtype=np.float64),
+            pscore=np.ascontiguousarray(r["pscore"], dtype=np.float64),
+            vbar=np.ascontiguousarray(r["vbar"], dtype=np.float64),
+        )
+        k = self._rk
+        self._chk(self._f["set_rhoset"](self.h, int(len(k["g2"])), _iptr(k["igvec"]), _dptr(k["gvec"]),
+                                        _dptr(k["g2"]), int(r["lmrxx"]), _iptr(k["lmrx"]), _dptr(k["ylm"]),
+                                        _dptr(k["g0"]), _dptr(k["v0"]), _dptr(k["pscore"]), _dptr(k["vbar"])),
+                  "POTENTIAL_UPDATE")
+        self.set_qlm(r["qlm"])
+        return self
+
+    def set_qlm(self, qlm):
+        a = np.ascontiguousarray(qlm, dtype=np.float64)
+        self._chk(self._f["set_qlm"](self.h, _dptr(a)), "set_qlm")
+
+    def vofrho(self, rho=None, qlm=None):
+        """POTENTIAL$VOFRHO: (V as an (NR3, NR2, NR1) array, {EHARTREE, EXC, RHOB},
+        forces (NAT, 3), VQLM (NAT, LMRXX)); the handle's potential becomes V."""
+        d = self.dims
+        nr = d.nr1 * d.nr2 * d.nr3
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+        q = None if qlm is None else np.ascontiguousarray(qlm, dtype=np.float64)
+        v = np.empty(nr)
+        e = np.empty(3)
+        f = np.empty((self.nat, 3))
+        lmrxx = int(self.inp["rhoset"]["lmrxx"])
+        vq = np.empty((self.nat, lmrxx))
+        self._chk(self._f["vofrho"](self.h, _dptr(r), _dptr(q), _dptr(v), _dptr(e), _dptr(f), _dptr(vq)),
+                  "POTENTIAL$VOFRHO")
+        return v.reshape(d.nr3, d.nr2, d.nr1), dict(zip(("ehartree", "exc", "rhob"), e.tolist())), f, vq
+
     def set_async(self, flag: bool):
         if "set_async" in self._f:
             self._chk(self._f["set_async"](self.h, int(flag)), "set_async")
@@ -385,7 +431,7 @@ class Waves:
             self._chk(self._f["synchronize"](self.h), "synchronize")
 
     PHASES = ("reductions", "structure factors", "forces", "fft_vpsi", "addpro_propagate",
-              "projections", "gram", "ortho_solve", "rotate", "bookkeeping")
+              "projections", "gram", "ortho_solve", "rotate", "bookkeeping", "potential")
 
     def set_option(self, option: int, value: float):
         self._chk(self._f["set_option"](self.h, int(option), float(value)), "set_option")

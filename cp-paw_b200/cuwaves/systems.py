@@ -561,7 +561,69 @@ def build_inputs(sys: System, grid=None, seed: Optional[int] = None, psi_init: s
         v=v, dh=dh, dover=dover, occ=occ,
         psi=np.ascontiguousarray(psi), r0=np.ascontiguousarray(sys.pos), masses=masses,
         delt=sys.delt, annee=sys.annee, emass=emass, emasscg2=emasscg2,
+        rhoset=rhoset_inputs(sys, gbas, omega, grid, seed),
     )
+
+
+# Synthetic tables of the potential (the SETUP quantities that POTENTIAL_UPDATE
+# transforms to G space, src/paw_potential.f90:300-309), per species:
+# compensation Gaussian radius rcsm, the wider Gaussian rcbg of V0, pseudo-core
+# charge and radius, VADD well depth and width, valence charge.
+RHO_SETUP = {"Si": (0.55, 1.10, 0.30, 0.80, 0.50, 1.00, 4.0),
+             "O": (0.40, 0.80, 0.40, 0.55, 0.80, 0.70, 6.0),
+             "H": (0.30, 0.60, 0.00, 0.40, 0.30, 0.50, 1.0)}
+
+
+def rhoset_inputs(sys: System, gbas: np.ndarray, omega: float, grid, seed: int):
+    """The density G set of the potential and its tables (see
+    cuwaves_set_rhoset): the sphere 0.5|G|^2 <= 2 EPWPSI in PLANEWAVE_GETIG
+    order, reduced to one G of each +-G pair as PLANEWAVE$SUPFFT does
+    (MINUSG(IG) >= IG); YLMOFG = Y_lm(G)|G|^l for l <= 2; G0 and V0 of Gaussian
+    compensation charges, a Gaussian pseudo core and a Gaussian VADD well per
+    species, each normalised so that a factor Y0 recovers the charge per cell
+    volume at G = 0; QLM: minus the valence charge on the monopole plus small
+    seeded higher moments.  None when the grid cannot hold the sphere."""
+    full = get_ig(gbas, 2.0 * sys.epw_psi)
+    for d, n in enumerate(grid):
+        if 2 * np.abs(full[:, d]).max() >= n:
+            return None
+    mg = minus_g(full) - 1  # 0-based partner of each G
+    keep = mg >= np.arange(len(full))
+    igvec = np.ascontiguousarray(full[keep])
+    gvec = gvectors(gbas, igvec)
+    g2 = gvec[:, 0] ** 2 + gvec[:, 1] ** 2 + gvec[:, 2] ** 2
+    glen = np.sqrt(g2)
+    lmrxx = 9
+    ylm = real_ylm(gvec, lmrxx)
+    for lm in range(1, 4):
+        ylm[:, lm] *= glen
+    for lm in range(4, 9):
+        ylm[:, lm] *= g2
+    y0 = 1.0 / math.sqrt(4.0 * PI)
+    nsp = len(sys.species)
+    g0 = np.zeros((nsp, len(g2)))
+    v0 = np.zeros_like(g0)
+    pscore = np.zeros_like(g0)
+    vbar = np.zeros_like(g0)
+    gs = np.where(g2 > 1e-12, g2, 1.0)
+    for k, sp in enumerate(sys.species):
+        rcsm, rcbg, qcore, rcore, vb, sb, _ = RHO_SETUP[sp.name]
+        a = np.exp(-0.25 * g2 * rcsm ** 2)
+        b = np.exp(-0.25 * g2 * rcbg ** 2)
+        g0[k] = a / (omega * y0)
+        v0[k] = np.where(g2 > 1e-12, 4.0 * PI * (a - b) / gs, PI * (rcbg ** 2 - rcsm ** 2)) / (omega * y0)
+        pscore[k] = qcore * np.exp(-0.25 * g2 * rcore ** 2) / (omega * y0)
+        vbar[k] = -vb * (2.0 * PI * sb ** 2) ** 1.5 * np.exp(-0.5 * g2 * sb ** 2) / (omega * y0)
+    rng = np.random.default_rng(3000 + seed)
+    isp0 = np.asarray(sys.isp) - 1
+    qlm = np.zeros((sys.nat, lmrxx))
+    for a in range(sys.nat):
+        sp = sys.species[isp0[a]]
+        qlm[a, 0] = -(RHO_SETUP[sp.name][6] + RHO_SETUP[sp.name][2])
+        qlm[a, 1:] = 0.05 * rng.uniform(-1.0, 1.0, lmrxx - 1)
+    return dict(igvec=igvec, gvec=np.ascontiguousarray(gvec), g2=g2, lmrxx=lmrxx,
+                lmrx=np.full(nsp, lmrxx, dtype=np.int32), ylm=np.ascontiguousarray(ylm),
+                g0=g0, v0=v0, pscore=pscore, vbar=vbar, qlm=qlm)
 
 
 def named_system(name: str) -> System:

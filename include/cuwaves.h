@@ -171,7 +171,8 @@ int cuwaves_stop(cuw_handle* h);
  * R(-), R(0), R(+) on the device; otherwise R(+) is the one last set.  out[8]
  * receives: [0] total energy sum_n f_n <psi_n|H|psi_n>, [1] kinetic energy,
  * [2] fictitious kinetic energy 0.5*(EKIN1+EKIN2), [3] ionic kinetic energy,
- * [4] orthogonalisation iterations, [5..7] reserved.  force (3,NAT) may be NULL. */
+ * [4] orthogonalisation iterations, [5..7] zero, or with CUW_OPT_SELFCONSISTENT
+ * EHARTREE, EXC and int V rho.  force (3,NAT) may be NULL. */
 int cuwaves_cp_step(cuw_handle* h, int move_atoms, const double* mass,
                     int max_iter, double eps, double* out, double* force);
 /* Resets the nuclear history so that R(-) = R(0) (start from rest). */
@@ -181,6 +182,35 @@ int cuwaves_reset_atoms(cuw_handle* h, const double* r0);
  * (:4570-4739): out[0] = sum_n f_n <psi_n|H|psi_n>, out[1] = kinetic energy,
  * force (3*NAT, may be NULL).  Nothing is propagated. */
 int cuwaves_etot(cuw_handle* h, double* out, double* force);
+
+/* Local potential from the density: POTENTIAL$VOFRHO (src/paw_potential.f90:
+ * 324-485 with POTENTIAL_VOFRHO :487-895) at the Gamma point for one spin,
+ * LDA (DFT type 2: local exchange + Perdew-Wang local correlation), without
+ * stress, confining potential, pair potential or isolation.
+ *
+ * cuwaves_set_rhoset loads the density G set and the tables of
+ * POTENTIAL_UPDATE (:250-320): the NGLH G vectors that PLANEWAVE$SUPFFT keeps
+ * (one of each +-G pair, src/paw_fft.f90:1834-1838) as igvec(3,NGLH),
+ * gvec(3,NGLH) and g2(NGLH); ylm(LMRXX,NGLH) = Y_lm(G)|G|^l
+ * (POTENTIAL_YLMOFG, :1548-1616); g0, v0, pscore, vbar (NGLH,NSP) as
+ * SETUP$GETFOFG gives 'G0', 'V0', 'PSCORE', 'VADD' (:300-309); lmrx(NSP).
+ * The grid is the handle's FFT grid. */
+int cuwaves_set_rhoset(cuw_handle* h, int nglh, const int* igvec, const double* gvec, const double* g2,
+                       int lmrxx, const int* lmrx, const double* ylm, const double* g0, const double* v0,
+                       const double* pscore, const double* vbar);
+/* QLM(LMRXX,NAT): multipole moments of the one-centre densities (the QLM
+ * argument of POTENTIAL$VOFRHO), kept for cuwaves_vofrho and the
+ * self-consistent step. */
+int cuwaves_set_qlm(cuw_handle* h, const double* qlm);
+/* POTENTIAL$VOFRHO at R(0): from the pseudo density rho(NR1*NR2*NR3) (x
+ * fastest; NULL: the density of PSI0, formed on the device as
+ * cuwaves_density does) and QLM (NULL: the one last set), the local
+ * potential V(r), which becomes the handle's potential as POTENTIAL$VOFRHO
+ * overwrites RHO with it.  Outputs (each may be NULL): v(NR), e[3] =
+ * {EHARTREE, EXC, RHOB}, force(3,NAT) the Hartree and pseudo-core forces,
+ * vqlm(LMRXX,NAT) = dE/dQLM. */
+int cuwaves_vofrho(cuw_handle* h, const double* rho, const double* qlm, double* v, double* e, double* force,
+                   double* vqlm);
 
 /* Orthonormality test of WAVES$ORTHOGONALIZE (its TTEST block,
  * src/paw_waves2.f90:421-460) for PSI0 at R(0), e.g. after cuwaves_cp_step:
@@ -267,9 +297,10 @@ int cuwaves_server_destroy(cuw_server* s);
  * cuwaves_set_timing(h, 1) records CUDA events on the handle's stream at the
  * phase boundaries of cuwaves_cp_step and resets the accumulators;
  * cuwaves_get_timing returns the accumulated device time per phase in ms
- * (n <= 10: reductions, structure factors, forces, FFT/V.psi, H and O
+ * (n <= 11: reductions, structure factors, forces, FFT/V.psi, H and O
  * back-projection with propagation, projections at R(+), Gram products,
- * orthogonality solve, rotation by Lambda, bookkeeping), the number of kernels
+ * orthogonality solve, rotation by Lambda, bookkeeping, and the density with
+ * POTENTIAL$VOFRHO of a self-consistent step), the number of kernels
  * this handle has launched and the number of timed steps.
  * cuwaves_get_stream returns the handle's cudaStream_t. */
 int cuwaves_set_timing(cuw_handle* h, int enable);
@@ -298,6 +329,14 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
 /* CUW_OPT_LYAP_MAX_SWEEPS: sweeps of the Lyapunov fixed point before it counts
  * as failed and the solve is redone after a rediagonalisation (default 64). */
 #define CUW_OPT_LYAP_MAX_SWEEPS 3
+/* CUW_OPT_SELFCONSISTENT: 1 makes cuwaves_cp_step self-consistent in the order
+ * of TIMESTEP (src/paw_driver.f90:280-561): the density of PSI0 and
+ * POTENTIAL$VOFRHO (cuwaves_vofrho, with the QLM of cuwaves_set_qlm) give the
+ * potential of the step's H|psi> before the forces, which gain the Hartree and
+ * pseudo-core terms; out[0] becomes sum_n f_n <psi_n|H|psi_n> - int V rho +
+ * EHARTREE + EXC, and out[5..7] = EHARTREE, EXC, int V rho.  Needs
+ * cuwaves_set_rhoset and cuwaves_set_qlm first; 0 (default) keeps V fixed. */
+#define CUW_OPT_SELFCONSISTENT 4
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);

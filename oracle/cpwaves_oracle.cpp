@@ -217,6 +217,15 @@ struct orc_handle {
   std::vector<cplx> psi0, psim, hpsi, opsi, proj, rlam0, rlamm;
   bool have_hpsi = false, have_rlamm = false;
   double waveekin1 = 0.0, waveekin2 = 0.0;
+  // density G set of the potential (PLANEWAVE 'DENSITY' at the Gamma point:
+  // one G of each +-G pair, the NGLH vectors of PLANEWAVE$SUPFFT) with the
+  // tables of POTENTIAL_UPDATE (src/paw_potential.f90:250-320)
+  int nglh = 0, lmrxx = 0, ngamma = -1;
+  std::vector<int> rigvec, rplus, rminus, lmrx;  // grid offsets of +G and -G
+  std::vector<double> rgvec, rg2, rylm, rg0, rv0, rpscore, rvbar;
+  bool have_rhoset = false;
+  std::vector<double> qlm;    // (LMRXX, NAT) multipole moments of the one-centre densities
+  bool scf = false;           // cp_step forms V(r) from the density of PSI0 first
   std::string err;
   int nthreads = 0;
 };
@@ -1427,21 +1436,374 @@ int orc_etot(orc_handle* h, double* out, double* force) {
   return CUW_OK;
 }
 
+// ===========================================================================
+// POTENTIAL$VOFRHO (src/paw_potential.f90:324-485, POTENTIAL_VOFRHO :487-895)
+// at the Gamma point for one spin, without gradient corrections (LDA), stress,
+// confining potential, pair potential or isolation (those parts do not touch
+// the density); restated step by step.
+// ===========================================================================
+int orc_density(orc_handle* h, double* rho);
+
+// one 3-D transform of the full grid (x fastest): dir = -1 forward with 1/N
+// (PLANEWAVE_FFTRTOG), dir = +1 inverse unscaled (PLANEWAVE_FFTGTOR)
+static void grid_fft3(const orc_handle* h, std::vector<cplx>& f, int dir) {
+  const int n1 = h->d.nr1, n2 = h->d.nr2, n3 = h->d.nr3;
+  const FFTPlan& q1 = dir > 0 ? h->p1g : h->p1r;
+  const FFTPlan& q2 = dir > 0 ? h->p2g : h->p2r;
+  const FFTPlan& q3 = dir > 0 ? h->p3g : h->p3r;
+  std::vector<cplx> work;
+  for (int k = 0; k < n3; ++k)
+    for (int j = 0; j < n2; ++j) fft1d(q1, &f[(size_t)n1 * (j + (size_t)n2 * k)], 1, work);
+  for (int k = 0; k < n3; ++k)
+    for (int i = 0; i < n1; ++i) fft1d(q2, &f[i + (size_t)n1 * n2 * k], n1, work);
+  for (int j = 0; j < n2; ++j)
+    for (int i = 0; i < n1; ++i) fft1d(q3, &f[i + (size_t)n1 * j], n1 * n2, work);
+  if (dir < 0) {
+    const double sc = 1.0 / ((double)n1 * n2 * n3);
+    for (cplx& x : f) x *= sc;
+  }
+}
+
+// PLANEWAVE$SUPFFT('RTOG') of one real function (src/paw_fft.f90:1905-1937):
+// FOFG(IGH) = 0.5 (F(G) + conj F(-G))
+static void supfft_rtog(const orc_handle* h, const double* fofr, cplx* fofg) {
+  const size_t nr = (size_t)h->d.nr1 * h->d.nr2 * h->d.nr3;
+  std::vector<cplx> f(nr);
+  for (size_t i = 0; i < nr; ++i) f[i] = cplx(fofr[i], 0.0);
+  grid_fft3(h, f, -1);
+  for (int ig = 0; ig < h->nglh; ++ig) {
+    cplx f1 = f[h->rplus[ig]], f2 = std::conj(f[h->rminus[ig]]);
+    fofg[ig] = 0.5 * (f1 + f2);
+  }
+}
+
+// PLANEWAVE$SUPFFT('GTOR') of one real function (src/paw_fft.f90:1851-1886):
+// F(G) = FOFG(IGH), F(-G) = conj FOFG(IGH) (the second wins for G = 0)
+static void supfft_gtor(const orc_handle* h, const cplx* fofg, double* fofr) {
+  const size_t nr = (size_t)h->d.nr1 * h->d.nr2 * h->d.nr3;
+  std::vector<cplx> f(nr, cplx(0.0, 0.0));
+  for (int ig = 0; ig < h->nglh; ++ig) {
+    f[h->rplus[ig]] = fofg[ig];
+    f[h->rminus[ig]] = std::conj(fofg[ig]);
+  }
+  grid_fft3(h, f, +1);
+  for (size_t i = 0; i < nr; ++i) fofr[i] = f[i].real();
+}
+
+// PLANEWAVE$STRUCTUREFACTOR (src/paw_fft.f90:1597-1695) on the density set
+static void rho_structurefactor(const orc_handle* h, const double* R, cplx* eigr) {
+  const int nr[3] = {h->d.nr1, h->d.nr2, h->d.nr3};
+  int nrmax = std::max(nr[0], std::max(nr[1], nr[2]));
+  std::vector<cplx> w((size_t)(2 * nrmax + 1) * 3);
+  auto W = [&](int i, int dir) -> cplx& { return w[(size_t)(i + nrmax) + (size_t)(2 * nrmax + 1) * dir]; };
+  for (int dir = 0; dir < 3; ++dir) {
+    double gr = h->gbas[0 + 3 * dir] * R[0] + h->gbas[1 + 3 * dir] * R[1] + h->gbas[2 + 3 * dir] * R[2];
+    cplx cfacp(std::cos(gr), -std::sin(gr));
+    cplx csvarp(1.0, 0.0);
+    cplx cfacm = std::conj(cfacp), csvarm = csvarp;
+    for (int i = 1; i <= nr[dir]; ++i) {
+      W(i - 1, dir) = csvarp;
+      csvarp *= cfacp;
+      W(-i + 1, dir) = csvarm;
+      csvarm *= cfacm;
+    }
+  }
+  for (int ig = 0; ig < h->nglh; ++ig)
+    eigr[ig] = W(h->rigvec[3 * ig], 0) * W(h->rigvec[3 * ig + 1], 1) * W(h->rigvec[3 * ig + 2], 2);
+}
+
+// DFT (src/paw_dft.f90:780-967) for the LDA of functional type 2: local
+// exchange (EXCHANGE_X1, :2137-2236, EXFAC of EXCHANGE_INITIALIZE) plus the
+// Perdew-Wang local correlation of the unpolarised gas (PERDEWWANG91L$EPSVAL
+// with TSAFE, :4718-4834, PERDEWWANG91L_RHODEP1 :4521-4575; TSAFE is a
+// parameter .TRUE., :56, so no table is used); RHOTMIN = 1e-6 (:62)
+static double dft_lda(double rhot, double* vxc) {
+  const double rhotmin = 1e-6;
+  double val = rhot < rhotmin ? rhotmin : rhot;
+  const double kffac = std::pow(3.0 * PI * PI, 1.0 / 3.0);
+  const double exfac = -3.0 / (4.0 * PI) * kffac;
+  double ex = 0.0, ex_r = 0.0;
+  if (std::fabs(val) >= 1e-50) {
+    const double r13 = std::pow(val, 1.0 / 3.0), r23 = r13 * r13, r43 = r23 * r23;
+    ex = exfac * r43;
+    ex_r = ex * (4.0 / 3.0) / val;
+  }
+  // PERDEWWANG91L_RHODEP1 with the sigma = 0 parameters
+  const double au = 3.10907e-2, alpha1 = 2.1370e-1, beta1 = 7.5957, beta2 = 3.5876, beta3 = 1.6382,
+               beta4 = 4.9294e-1;
+  const double rsfac = std::pow(3.0 / (4.0 * PI), 1.0 / 3.0);
+  const double rs = rsfac / std::pow(val, 1.0 / 3.0);
+  const double sqrs = std::sqrt(rs), rssqrs = rs * sqrs;
+  const double sv1 = -2.0 * au * (1.0 + alpha1 * rs), dsv1 = -2.0 * au * alpha1;
+  const double sv2 = 2.0 * au * sqrs * (beta1 + beta2 * sqrs + beta3 * rs + beta4 * rssqrs);
+  const double dsv2 = au / sqrs * (beta1 + 2.0 * beta2 * sqrs + 3.0 * beta3 * rs + 4.0 * beta4 * rssqrs);
+  const double sv3 = 1.0 + 1.0 / sv2, dsv3 = -dsv2 / (sv2 * sv2);
+  const double sv4 = std::log(sv3), dsv4 = dsv3 / sv3;
+  double ecu = sv1 * sv4;
+  double decu = dsv1 * sv4 + sv1 * dsv4;
+  decu = decu * (-(1.0 / 3.0) * rs / val);
+  // PERDEWWANG91L$EVAL1 (:5152-5170)
+  const double ec = val * ecu, dec = val * decu + ecu;
+  double exc = ex + ec, dexc = ex_r + dec;
+  if (rhot < rhotmin) {  // wrap-up of DFT (:931-935)
+    dexc = exc / rhotmin;
+    exc = exc * rhot / rhotmin;
+  }
+  *vxc = dexc;
+  return exc;
+}
+
+// The density G set and its tables.  igvec(3,NGLH), gvec(3,NGLH), g2(NGLH),
+// ylm(LMRXX,NGLH) = Y_lm(G)|G|^l (POTENTIAL_YLMOFG, :1548-1616), g0, v0,
+// pscore, vbar (NGLH,NSP) as SETUP$GETFOFG gives them (:300-309), lmrx(NSP).
+int orc_set_rhoset(orc_handle* h, int nglh, const int* igvec, const double* gvec, const double* g2, int lmrxx,
+                   const int* lmrx, const double* ylm, const double* g0, const double* v0, const double* pscore,
+                   const double* vbar) {
+  OCHECK(h->have_gset, CUW_ERR_STATE, "gset not set");
+  OCHECK(nglh > 0 && lmrxx > 0 && igvec && gvec && g2 && lmrx && ylm && g0 && v0 && pscore && vbar, CUW_ERR_ARG,
+         "bad density set");
+  const int nsp = h->d.nsp;
+  const int n[3] = {h->d.nr1, h->d.nr2, h->d.nr3};
+  h->nglh = nglh;
+  h->lmrxx = lmrxx;
+  h->rigvec.assign(igvec, igvec + 3 * (size_t)nglh);
+  h->rplus.resize(nglh);
+  h->rminus.resize(nglh);
+  h->ngamma = -1;
+  for (int ig = 0; ig < nglh; ++ig) {
+    int p[3], m[3];
+    for (int k = 0; k < 3; ++k) {
+      const int i = igvec[3 * ig + k];
+      OCHECK(2 * std::abs(i) < n[k], CUW_ERR_ARG, "density G vector outside the grid");
+      p[k] = ((i % n[k]) + n[k]) % n[k];
+      m[k] = ((-i % n[k]) + n[k]) % n[k];
+    }
+    h->rplus[ig] = p[0] + n[0] * (p[1] + n[1] * p[2]);
+    h->rminus[ig] = m[0] + n[0] * (m[1] + n[1] * m[2]);
+    if (igvec[3 * ig] == 0 && igvec[3 * ig + 1] == 0 && igvec[3 * ig + 2] == 0) h->ngamma = ig;
+  }
+  h->rgvec.assign(gvec, gvec + 3 * (size_t)nglh);
+  h->rg2.assign(g2, g2 + nglh);
+  h->lmrx.assign(lmrx, lmrx + nsp);
+  for (int s = 0; s < nsp; ++s) OCHECK(lmrx[s] >= 1 && lmrx[s] <= lmrxx, CUW_ERR_ARG, "LMRX out of range");
+  h->rylm.assign(ylm, ylm + (size_t)lmrxx * nglh);
+  h->rg0.assign(g0, g0 + (size_t)nglh * nsp);
+  h->rv0.assign(v0, v0 + (size_t)nglh * nsp);
+  h->rpscore.assign(pscore, pscore + (size_t)nglh * nsp);
+  h->rvbar.assign(vbar, vbar + (size_t)nglh * nsp);
+  h->have_rhoset = true;
+  return CUW_OK;
+}
+
+int orc_set_qlm(orc_handle* h, const double* qlm) {
+  OCHECK(h->have_rhoset && qlm, CUW_ERR_STATE, "density set not loaded");
+  h->qlm.assign(qlm, qlm + (size_t)h->lmrxx * h->d.nat);
+  return CUW_OK;
+}
+
+int orc_set_option(orc_handle* h, int option, double value) {
+  if (option == CUW_OPT_SELFCONSISTENT) {
+    OCHECK(value == 0.0 || (h->have_rhoset && !h->qlm.empty()), CUW_ERR_STATE, "density set or QLM missing");
+    h->scf = value != 0.0;
+  }
+  return CUW_OK;  // the engine's tuning options do not apply to the oracle
+}
+
+// POTENTIAL_VOFRHO for RHOE = rho (pseudo density of the wave functions):
+// v = the potential on the grid; e[0] EHARTREE, e[1] EXC, e[2] RHOB;
+// force (3,NAT) Hartree + pseudo-core forces; vqlm (LMRXX,NAT)
+static int vofrho_core(orc_handle* h, const double* rho, double* v, double* e, double* force, double* vqlm) {
+  const int nglh = h->nglh, nat = h->d.nat, lmrxx = h->lmrxx;
+  const size_t nr = (size_t)h->d.nr1 * h->d.nr2 * h->d.nr3;
+  const double fpi = 4.0 * PI, y0 = 1.0 / std::sqrt(4.0 * PI);
+  const double cellvol = h->gweight;
+  const int lrxx = (int)std::sqrt((double)(lmrxx - 1) + 1e-5);
+  // RHOG = SUPFFT('RTOG', RHOE) (:600)
+  std::vector<cplx> rhog(nglh), eigr(nglh);
+  supfft_rtog(h, rho, rhog.data());
+  // POTENTIAL_ADDCORE (:1038-1066)
+  for (int a = 0; a < nat; ++a) {
+    const int s = h->isp[a];
+    rho_structurefactor(h, &h->r0[3 * a], eigr.data());
+    for (int ig = 0; ig < nglh; ++ig) rhog[ig] += h->rpscore[ig + (size_t)nglh * s] * y0 * eigr[ig];
+  }
+  // POTENTIAL_HARTREE (:1069-1336) without stress
+  std::vector<cplx> cfac(lmrxx);
+  {
+    int lm = 0;
+    cplx csvar(0.0, 1.0);
+    for (int l = 0; l <= lrxx; ++l) {
+      csvar = -csvar * CI / (double)(2 * l + 1);
+      for (int m = -l; m <= l; ++m)
+        if (lm < lmrxx) cfac[lm++] = csvar;
+    }
+  }
+  std::vector<cplx> rho2(rhog), pot(nglh, cplx(0.0, 0.0)), vg(nglh);
+  double vb = 0.0;
+  for (int a = 0; a < nat; ++a) {
+    const int s = h->isp[a];
+    rho_structurefactor(h, &h->r0[3 * a], eigr.data());
+    if (h->ngamma >= 0) vb += h->qlm[(size_t)lmrxx * a] * y0 * h->rv0[h->ngamma + (size_t)nglh * s];
+    for (int ig = 0; ig < nglh; ++ig) {
+      cplx c(0.0, 0.0);
+      for (int lm = 0; lm < h->lmrx[s]; ++lm)
+        c += cfac[lm] * h->qlm[lm + (size_t)lmrxx * a] * h->rylm[lm + (size_t)lmrxx * ig];
+      c *= eigr[ig];
+      rho2[ig] += c * h->rg0[ig + (size_t)nglh * s];
+      pot[ig] += c * h->rv0[ig + (size_t)nglh * s] + h->rvbar[ig + (size_t)nglh * s] * y0 * eigr[ig];
+    }
+  }
+  double rhob = 0.0;
+  if (h->ngamma >= 0) {
+    rhob = -rho2[h->ngamma].real();
+    rho2[h->ngamma] = 0.0;
+  }
+  cplx csum(0.0, 0.0);
+  for (int ig = 0; ig < nglh; ++ig) {
+    if (ig != h->ngamma) {
+      vg[ig] = rho2[ig] * fpi / h->rg2[ig];
+      csum += 0.5 * std::conj(rho2[ig]) * vg[ig] + std::conj(rhog[ig]) * pot[ig];
+      pot[ig] += vg[ig];
+    } else {
+      vg[ig] = -vb;
+      csum += 0.5 * (std::conj(rhog[ig]) * pot[ig] + rhob * vb);
+      pot[ig] += vg[ig];
+    }
+  }
+  double ehartree = csum.real();
+  // forces and VQLM (:1240-1319)
+  for (int ig = 0; ig < nglh; ++ig) rho2[ig] = rhog[ig];
+  if (h->ngamma >= 0) rho2[h->ngamma] += rhob;
+  std::vector<double> f(3 * (size_t)nat, 0.0), vq((size_t)lmrxx * nat, 0.0);
+  for (int a = 0; a < nat; ++a) {
+    const int s = h->isp[a];
+    rho_structurefactor(h, &h->r0[3 * a], eigr.data());
+    for (int ig = 0; ig < nglh; ++ig) {
+      const double g0 = h->rg0[ig + (size_t)nglh * s], v0 = h->rv0[ig + (size_t)nglh * s];
+      const double* y = &h->rylm[(size_t)lmrxx * ig];
+      if (ig == h->ngamma) {
+        cplx c0 = g0 * std::conj(vg[ig]) + v0 * std::conj(rho2[ig]);
+        cplx c = c0 * cfac[0] * y[0] * eigr[ig];
+        vq[(size_t)lmrxx * a] -= 0.5 * c.real();
+      }
+      cplx aval = (g0 * std::conj(vg[ig]) + v0 * std::conj(rho2[ig])) * eigr[ig];
+      cplx cs(0.0, 0.0);
+      for (int lm = 0; lm < h->lmrx[s]; ++lm) {
+        cplx c = cfac[lm] * y[lm];
+        vq[lm + (size_t)lmrxx * a] += (c * aval).real();
+        cs += h->qlm[lm + (size_t)lmrxx * a] * c;
+      }
+      cplx cval = h->rvbar[ig + (size_t)nglh * s] * y0 * eigr[ig] * std::conj(rhog[ig]);
+      const double sv = (cval + cs * aval).imag();
+      for (int k = 0; k < 3; ++k) f[3 * a + k] -= h->rgvec[3 * ig + k] * sv;
+    }
+  }
+  ehartree *= 2.0 * cellvol;
+  for (double& x : vq) x *= 2.0 * cellvol;
+  for (double& x : f) x *= 2.0 * cellvol;
+  // total pseudo density in real space (:747), XC (POTENTIAL_XC, :1339-1545)
+  std::vector<double> rt(nr);
+  supfft_gtor(h, rhog.data(), rt.data());
+  double sxc = 0.0, ssxc = 0.0;
+  for (size_t ir = 0; ir < nr; ++ir) {
+    double rhot = std::max(rt[ir], 1e-8);
+    double vt = 0.0;
+    sxc += dft_lda(rhot, &vt);
+    rt[ir] = vt;
+    if ((ir + 1) % 100 == 0) {
+      ssxc += sxc;
+      sxc = 0.0;
+    }
+  }
+  ssxc += sxc;
+  const double exc = ssxc * cellvol / (double)nr;
+  // V(G) = SUPFFT('RTOG', VXC) + VHARTREE (:778-800)
+  std::vector<cplx> vtot(nglh);
+  supfft_rtog(h, rt.data(), vtot.data());
+  for (int ig = 0; ig < nglh; ++ig) vtot[ig] += pot[ig];
+  // POTENTIAL_FPSCORE (:897-975)
+  for (int a = 0; a < nat; ++a) {
+    const int s = h->isp[a];
+    rho_structurefactor(h, &h->r0[3 * a], eigr.data());
+    double fa[3] = {0, 0, 0}, f1[3] = {0, 0, 0};
+    for (int ig = 0; ig < nglh; ++ig) {
+      cplx c = std::conj(vtot[ig]) * h->rpscore[ig + (size_t)nglh * s] * eigr[ig];
+      const double sv = -c.imag();
+      for (int k = 0; k < 3; ++k) f1[k] += sv * h->rgvec[3 * ig + k];
+      if ((ig + 1) % 100 == 0)
+        for (int k = 0; k < 3; ++k) {
+          fa[k] += f1[k];
+          f1[k] = 0.0;
+        }
+    }
+    for (int k = 0; k < 3; ++k) f[3 * a + k] += (fa[k] + f1[k]) * y0 * 2.0 * cellvol;
+  }
+  // V(r) (:890)
+  supfft_gtor(h, vtot.data(), v);
+  if (e) {
+    e[0] = ehartree;
+    e[1] = exc;
+    e[2] = rhob;
+  }
+  if (force) std::memcpy(force, f.data(), sizeof(double) * f.size());
+  if (vqlm) std::memcpy(vqlm, vq.data(), sizeof(double) * vq.size());
+  return CUW_OK;
+}
+
+// POTENTIAL$VOFRHO: the handle's potential becomes V[rho]; rho == NULL takes
+// the pseudo density of PSI0 (WAVES_DENSITY); v, e, force, vqlm may be NULL
+int orc_vofrho(orc_handle* h, const double* rho, const double* qlm, double* v, double* e, double* force,
+               double* vqlm) {
+  OCHECK(h->have_rhoset, CUW_ERR_STATE, "density set not loaded");
+  if (qlm) h->qlm.assign(qlm, qlm + (size_t)h->lmrxx * h->d.nat);
+  OCHECK(!h->qlm.empty(), CUW_ERR_STATE, "QLM not set");
+  const size_t nr = (size_t)h->d.nr1 * h->d.nr2 * h->d.nr3;
+  std::vector<double> r(nr), vv(nr);
+  if (rho) std::memcpy(r.data(), rho, sizeof(double) * nr);
+  else {
+    int st = orc_density(h, r.data());
+    if (st) return st;
+  }
+  int st = vofrho_core(h, r.data(), vv.data(), e, force, vqlm);
+  if (st) return st;
+  h->v = vv;
+  h->have_v = true;
+  if (v) std::memcpy(v, vv.data(), sizeof(double) * nr);
+  return CUW_OK;
+}
+
 int orc_cp_step(orc_handle* h, int move_atoms, const double* mass, int maxit, double eps,
                 double* out, double* force) {
   const int nb = h->d.nb, nat = h->d.nat;
   double ekin = 0.0, ekin1 = 0.0;
   int st = orc_ekin(h, &ekin);
   if (st) return st;
+  // self-consistent step: V(r) from the density of PSI0 at R(0) before H|psi>
+  // (the order of WAVES$ETOT -> POTENTIAL$VOFRHO -> WAVES$HPSI in TIMESTEP)
+  double epot[3] = {0.0, 0.0, 0.0}, edc = 0.0;
+  std::vector<double> fpot(3 * (size_t)nat, 0.0);
+  if (h->scf) {
+    const size_t nr = (size_t)h->d.nr1 * h->d.nr2 * h->d.nr3;
+    std::vector<double> rho(nr);
+    st = orc_density(h, rho.data());
+    if (st) return st;
+    st = vofrho_core(h, rho.data(), h->v.data(), epot, fpot.data(), nullptr);
+    if (st) return st;
+    // sum_n f_n <psi_n|V|psi_n> = int V rho, removed from the band energy
+    for (size_t ir = 0; ir < nr; ++ir) edc += h->v[ir] * rho[ir];
+    edc *= h->gweight / (double)nr;
+  }
   std::vector<double> f(3 * nat);
   st = orc_force(h, f.data());
   if (st) return st;
+  for (size_t i = 0; i < f.size(); ++i) f[i] += fpot[i];
   st = orc_hpsi(h);
   if (st) return st;
   std::vector<double> eig(nb);
   orc_expectation(h, eig.data());
   double etot = 0.0;
   for (int i = 0; i < nb; ++i) etot += h->occ[i] * eig[i];
+  if (h->scf) etot += epot[0] + epot[1] - edc;
   ekin1 = wavekinetic(h, nullptr);
   double eion = 0.0;
   if (move_atoms) {
@@ -1477,7 +1839,9 @@ int orc_cp_step(orc_handle* h, int move_atoms, const double* mass, int maxit, do
     out[2] = 0.5 * (ekin1 + ekin2);
     out[3] = eion;
     out[4] = iters;
-    out[5] = out[6] = out[7] = 0.0;
+    out[5] = epot[0];
+    out[6] = epot[1];
+    out[7] = edc;
   }
   if (force) std::memcpy(force, f.data(), sizeof(double) * 3 * nat);
   return CUW_OK;

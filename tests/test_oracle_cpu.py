@@ -310,3 +310,137 @@ def test_oracle_restart_records(oracle, tmp_path):
             u2.read_restart(tmp_path / name)
         assert np.array_equal(u2.download_psi(0), d["psi"][0])
 
+
+
+# ---------------------------------------------------------------------------
+# POTENTIAL$VOFRHO.  The reference checks this routine with its own self-tests
+# (POTENTIAL_VOFRHO, src/paw_potential.f90:619-650 and 860-880, SELFTEST
+# ITEST = 1, 2, 3): the potential is the derivative of EHARTREE + EXC with
+# respect to the density, VQLM the derivative with respect to QLM, the forces
+# minus the derivative with respect to the positions.  The same three checks
+# by central differences pin the oracle's restatement; a numpy restatement of
+# the formulas checks its arithmetic.
+# ---------------------------------------------------------------------------
+def _vofrho_case(oracle):
+    inp = systems.build_inputs(systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=15.0, name="Si8-15", disp=0.1))
+    w = oracle.open_oracle(inp).setup().initialize()
+    w.set_rhoset()
+    return inp, w
+
+
+def test_oracle_vofrho_selftests(oracle):
+    inp, w = _vofrho_case(oracle)
+    rho = w.density()
+    v, e, f, vq = w.vofrho(rho)
+    om, nr = inp["omega"], rho.size
+
+    def energy(r=rho, q=None):
+        _, ee, _, _ = w.vofrho(r, q)
+        return ee["ehartree"] + ee["exc"]
+
+    # ITEST 1: dE/drho along a seeded in-sphere direction equals int V drho
+    n = tuple(inp["grid"])
+    ig = inp["rhoset"]["igvec"]
+    mask = np.zeros(n, bool)
+    for sgn in (1, -1):
+        mask[(sgn * ig[:, 0]) % n[0], (sgn * ig[:, 1]) % n[1], (sgn * ig[:, 2]) % n[2]] = True
+    rng = np.random.default_rng(1)
+    spec = rng.normal(size=n) + 1j * rng.normal(size=n)
+    dr = np.fft.ifftn(np.where(mask, spec, 0)).real.transpose(2, 1, 0) * 100
+    d = 1e-4
+    fd = (energy(rho + d * dr) - energy(rho - d * dr)) / (2 * d)
+    assert abs(fd - (v * dr).sum() * om / nr) < 1e-6 * max(1.0, abs(fd))
+    # a single grid point
+    k = (5, 7, 3)
+    rp, rm = rho.copy(), rho.copy()
+    rp[k] += 1e-5
+    rm[k] -= 1e-5
+    assert abs((energy(rp) - energy(rm)) / 2e-5 / (om / nr) - v[k]) < 1e-6 * abs(v[k])
+    # ITEST 2: VQLM = dE/dQLM
+    q0 = inp["rhoset"]["qlm"].copy()
+    for a, lm in ((0, 0), (3, 2), (5, 7)):
+        qp, qm = q0.copy(), q0.copy()
+        qp[a, lm] += 1e-5
+        qm[a, lm] -= 1e-5
+        fdq = (energy(rho, qp) - energy(rho, qm)) / 2e-5
+        assert abs(fdq - vq[a, lm]) < 1e-6 * max(1e-2, abs(vq[a, lm])), (a, lm, fdq, vq[a, lm])
+    w.set_qlm(q0)
+    # ITEST 3: forces = -dE/dR
+    r0 = inp["r0"].copy()
+    for a, c in ((0, 0), (3, 2), (6, 1)):
+        rp = r0.copy()
+        rp[a, c] += 1e-5
+        w.set_atoms(rp, None)
+        ep = energy()
+        rm = r0.copy()
+        rm[a, c] -= 1e-5
+        w.set_atoms(rm, None)
+        em = energy()
+        assert abs(-(ep - em) / 2e-5 - f[a, c]) < 1e-6 * max(1.0, abs(f[a, c])), (a, c)
+    w.set_atoms(r0, None)
+
+
+def test_oracle_vofrho_matches_numpy(oracle):
+    """The potential formulas restated once more in numpy (full-grid FFTs,
+    direct structure factors)."""
+    inp, w = _vofrho_case(oracle)
+    rho = w.density()
+    v, e, _, _ = w.vofrho(rho)
+    R = inp["rhoset"]
+    n = tuple(inp["grid"])
+    om, N = inp["omega"], rho.size
+    ig, g, g2, y, q = R["igvec"], R["gvec"], R["g2"], R["ylm"], R["qlm"]
+    y0 = 1 / np.sqrt(4 * np.pi)
+    ip = tuple((ig[:, k] % n[k]) for k in range(3))
+    im = tuple((-ig[:, k] % n[k]) for k in range(3))
+
+    def rtog(f):
+        F = np.fft.fftn(f.transpose(2, 1, 0)) / N
+        return 0.5 * (F[ip] + np.conj(F[im]))
+
+    def gtor(c):
+        F = np.zeros(n, complex)
+        F[ip] = c
+        F[im] = np.conj(c)
+        return (np.fft.ifftn(F) * N).real.transpose(2, 1, 0)
+
+    cfac = np.array([1] + [-1j / 3] * 3 + [-1 / 15] * 5)
+    ng = int(np.nonzero((ig == 0).all(1))[0][0])
+    isp = inp["isp"] - 1
+    eig = [np.exp(-1j * (g @ r)) for r in inp["r0"]]
+    rhog = rtog(rho)
+    for a in range(len(eig)):
+        rhog = rhog + R["pscore"][isp[a]] * y0 * eig[a]
+    rho2, pot, vb = rhog.copy(), np.zeros_like(rhog), 0.0
+    for a in range(len(eig)):
+        s = isp[a]
+        c = (y * (cfac * q[a])[None, :]).sum(1) * eig[a]
+        vb += q[a, 0] * y0 * R["v0"][s][ng]
+        rho2 = rho2 + c * R["g0"][s]
+        pot = pot + c * R["v0"][s] + R["vbar"][s] * y0 * eig[a]
+    rhob = -rho2[ng].real
+    rho2[ng] = 0
+    gs = np.where(np.arange(len(g2)) == ng, 1, g2)
+    vg = rho2 * 4 * np.pi / gs
+    vg[ng] = -vb
+    terms = 0.5 * np.conj(rho2) * vg + np.conj(rhog) * pot
+    terms[ng] = 0.5 * (np.conj(rhog[ng]) * pot[ng] + rhob * vb)
+    eh = terms.sum().real * 2 * om
+    rt = np.maximum(gtor(rhog), 1e-8)
+    ex = -3 / (4 * np.pi) * (3 * np.pi ** 2) ** (1 / 3) * rt ** (4 / 3)
+    au, a1, b1, b2, b3, b4 = 3.10907e-2, 2.1370e-1, 7.5957, 3.5876, 1.6382, 4.9294e-1
+    rs = (3 / (4 * np.pi)) ** (1 / 3) / rt ** (1 / 3)
+    sq = np.sqrt(rs)
+    s1, ds1 = -2 * au * (1 + a1 * rs), -2 * au * a1
+    s2 = 2 * au * sq * (b1 + b2 * sq + b3 * rs + b4 * rs * sq)
+    ds2 = au / sq * (b1 + 2 * b2 * sq + 3 * b3 * rs + 4 * b4 * rs * sq)
+    s3 = 1 + 1 / s2
+    ecu = s1 * np.log(s3)
+    decu = (ds1 * np.log(s3) + s1 * (-ds2 / s2 ** 2) / s3) * (-rs / 3 / rt)
+    exc = (ex + rt * ecu).sum() * om / N
+    vxc = ex * 4 / 3 / rt + rt * decu + ecu
+    vnp = gtor(rtog(vxc) + pot + vg)
+    assert abs(eh - e["ehartree"]) < 1e-10 * abs(eh)
+    assert abs(exc - e["exc"]) < 1e-10 * abs(exc)
+    assert abs(rhob - e["rhob"]) < 1e-12
+    assert np.abs(vnp - v).max() < 1e-10 * np.abs(v).max()
