@@ -212,6 +212,7 @@ struct Handle {
   // inside the mixed path's own error.
   double lyap_tol = 0.0;
   int lyap_max_sweeps = 64;  // sweeps per Lyapunov solve before the fixed point counts as failed
+  bool ortho_panel = true;   // ORTHO_X by the panel-staged cluster kernel where it applies (64 < NB <= 128)
   bool tc_scope_open = false;
   const double* eigr_src = nullptr;  // position buffer (r0, rp or rm) that EIGR (and the fp32 table) was built from
   // potential: density G set size, LMRXX, index of G = 0 (-1: none), and
@@ -291,7 +292,7 @@ struct StepCoef {
 //   a = A[lane>>2][lane&3], b = B[lane&3][lane>>2],
 //   c[0..1] = C[lane>>2][2*(lane&3)+0..1]
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c[0]), "+d"(c[1])
                : "d"(a), "d"(b));
 }

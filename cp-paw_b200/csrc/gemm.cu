@@ -76,13 +76,20 @@ __device__ __forceinline__ void mma_slice(Acc& acc, const double* Ar, const doub
       br[ni] = Br[o];
       bi[ni] = Bi[o];
     }
+    // two passes over the 16 accumulators, so that the two products that
+    // add into one accumulator are 16 MMAs apart instead of back to back
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
       for (int ni = 0; ni < 2; ++ni) {
         dmma(acc.r[mi][ni], ar[mi], br[ni]);
-        dmma(acc.r[mi][ni], nai[mi], bi[ni]);
         dmma(acc.i[mi][ni], ar[mi], bi[ni]);
+      }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        dmma(acc.r[mi][ni], nai[mi], bi[ni]);
         dmma(acc.i[mi][ni], ai[mi], br[ni]);
       }
   }

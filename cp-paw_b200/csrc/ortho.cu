@@ -843,6 +843,303 @@ __global__ void __launch_bounds__(512) k_ortho_x(OrthoArgs a) {
   csync();
 }
 
+// ---------------------------------------------------------------------------
+// ORTHO_X for 64 < n <= 128 with equal occupations, as one cluster of 16 CTAs
+// in a 4 x 4 grid: CTA (ri, ci) owns the 32 x 32 tile (ri, ci) of every
+// product.  The matrices live in global memory (L2: 128 KB each); a product
+// tile op(A) op(B) stages its two operand panels (32 x n and n x 32) into
+// shared memory with 16-byte loads of whole column segments, each panel in
+// the one of two layouts that keeps the MMA fragment reads free of bank
+// conflicts for its orientation:
+//   row panel    rows i0..i0+31 of all columns k: [k][r], stride PR = 36
+//                (A, or B transposed: column segments of 32 elements)
+//   column panel columns j0..j0+31, all rows k:  [c][k], stride PC = 132
+//                (B, or A transposed: whole columns)
+// then multiplies on the FP64 tensor cores (m8n8k4), each warp one 8 x 8
+// block with two accumulation chains.  The elementwise operands of the
+// iteration (CHIPSI, PSIPSI, Gamma, the denominators, Lambda) stay in the
+// registers of the lanes that own the elements.  One cluster barrier ends
+// every phase (its release/acquire orders the global writes of a phase before
+// the next phase's reads, all through L2); the maxima of a phase are
+// exchanged through shared-memory slots of the cluster.  The arithmetic and
+// the phases are those of k_ortho_x with the same stopping rules.
+// ---------------------------------------------------------------------------
+namespace pnl {
+constexpr int T = 32, G = 4, KN = 128;
+constexpr int PR = T + 4;    // row panel stride ([k][r])
+constexpr int PC = KN + 4;   // column panel stride ([c][k])
+constexpr int RSZ = KN * PR, CSZ = T * PC;  // doubles of one row / column panel
+// two terms, each an A and a B panel of either kind (sized for the larger)
+constexpr int PSZ = RSZ > CSZ ? RSZ : CSZ;
+constexpr size_t kSmemBytes = sizeof(double) * ((size_t)4 * PSZ + 64);
+}  // namespace pnl
+
+// Stages op(M) as the A operand (rows i0.. of the product, all k) or as the B
+// operand (all k, columns j0..) of a product tile into dst.  M is n x n
+// column-major in global memory (n even, so column segments are 16-byte
+// aligned); elements outside n x n are zero.  Returns nothing; the caller
+// synchronises.
+__device__ __forceinline__ void pnl_stage(const double* __restrict__ M, int n, int off, bool row_panel,
+                                          double* __restrict__ dst) {
+  using namespace pnl;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (row_panel) {
+    // rows off..off+31 of every column k: 16 double2 per column
+    for (int t = tid; t < KN * (T / 2); t += nt) {
+      const int k = t / (T / 2), r2 = (t % (T / 2)) * 2;
+      double2 v = make_double2(0.0, 0.0);
+      if (k < n && off + r2 < n) v = __ldcg(reinterpret_cast<const double2*>(M + (size_t)n * k + off + r2));
+      *reinterpret_cast<double2*>(dst + k * PR + r2) = v;
+    }
+  } else {
+    // columns off..off+31, every row k: 64 double2 per column
+    for (int t = tid; t < T * (KN / 2); t += nt) {
+      const int c = t / (KN / 2), k2 = (t % (KN / 2)) * 2;
+      double2 v = make_double2(0.0, 0.0);
+      if (off + c < n && k2 < n) v = __ldcg(reinterpret_cast<const double2*>(M + (size_t)n * (off + c) + k2));
+      *reinterpret_cast<double2*>(dst + c * PC + k2) = v;
+    }
+  }
+}
+
+// One product term op(A) op(B) of a tile: the panels and how to read them.
+//   A normal: row panel of A at rows i0      -> element (i, k) at k*PR + i
+//   A transposed: column panel of A at cols i0 -> (i, k) = A(k, i) at i*PC + k
+//   B normal: column panel of B at cols j0   -> (k, j) at j*PC + k
+//   B transposed: row panel of B at rows j0  -> (k, j) = B(j, k) at k*PR + j
+struct PnlTerm {
+  const double* a;
+  bool ta;
+  const double* b;
+  bool tb;
+};
+
+__device__ __forceinline__ void pnl_stage_term(const PnlTerm& t, int n, int i0, int j0, double* sa, double* sb) {
+  pnl_stage(t.a, n, i0, !t.ta, sa);
+  pnl_stage(t.b, n, j0, t.tb, sb);
+}
+
+// acc (two chains) += op(A) op(B) for this warp's 8 x 8 block
+__device__ __forceinline__ void pnl_mma(const PnlTerm& t, int nk4, const double* sa, const double* sb, int r0,
+                                        int c0, double (&acc)[2], double (&acc2)[2]) {
+  using namespace pnl;
+  const int lane = threadIdx.x & 31, fr = lane >> 2, fk = lane & 3;
+  const double* pa = t.ta ? sa + (r0 + fr) * PC + fk : sa + fk * PR + r0 + fr;
+  const int as = t.ta ? 4 : 4 * PR;
+  const double* pb = t.tb ? sb + fk * PR + c0 + fr : sb + (c0 + fr) * PC + fk;
+  const int bs = t.tb ? 4 * PR : 4;
+#pragma unroll 4
+  for (int s = 0; s < nk4; s += 2) {
+    dmma(acc, pa[s * as], pb[s * bs]);
+    if (s + 1 < nk4) dmma(acc2, pa[(s + 1) * as], pb[(s + 1) * bs]);
+  }
+}
+
+__global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
+  using namespace pnl;
+  if (gate_closed(a.gate)) return;
+  extern __shared__ double sm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int ri = rank / G, ci = rank % G;
+  const int n = a.n, nk4 = (n + 3) / 4;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int fr = lane >> 2, fk = lane & 3;
+  const int r0 = (warp % 4) * 8, c0 = (warp / 4) * 8;  // this warp's 8 x 8 block of the tile
+  const int i0 = ri * T, j0 = ci * T;
+  double* sa0 = sm;
+  double* sb0 = sm + PSZ;
+  double* sa1 = sm + 2 * PSZ;
+  double* sb1 = sm + 3 * PSZ;
+  double* slotmax = sm + 4 * PSZ;  // [2 parities][x: 16 ranks, y: 16 ranks]
+  // this lane's two elements (gi, gj0 + e) of the tile
+  const int gi = i0 + r0 + fr, gjb = j0 + c0 + 2 * fk;
+  bool ok[2];
+  size_t gidx[2];
+  double cp[2], pp[2], lamv[2], den[2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int gj = gjb + e;
+    ok[e] = gi < n && gj < n;
+    gidx[e] = ok[e] ? (size_t)gi + (size_t)n * gj : 0;
+    cp[e] = ok[e] ? a.chipsi[gidx[e]] : 0.0;
+    pp[e] = ok[e] ? a.psipsi[min(gi, gj) + (size_t)n * max(gi, gj)] : 0.0;
+    lamv[e] = ok[e] ? __ldcg(&a.lam[gidx[e]]) : 0.0;
+    den[e] = ok[e] ? a.e[gi] + a.e[gj] : 1.0;
+  }
+  auto put = [&](double* M, const double (&v)[2]) {
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+      if (ok[e]) M[gidx[e]] = v[e];
+  };
+  // one product tile: stage both terms (the second may be absent), multiply
+  auto product = [&](const PnlTerm& t1, const PnlTerm* t2, double (&out)[2]) {
+    pnl_stage_term(t1, n, i0, j0, sa0, sb0);
+    if (t2) pnl_stage_term(*t2, n, i0, j0, sa1, sb1);
+    __syncthreads();
+    double acc[2] = {0.0, 0.0}, acc2[2] = {0.0, 0.0};
+    pnl_mma(t1, nk4, sa0, sb0, r0, c0, acc, acc2);
+    out[0] = acc[0] + acc2[0];
+    out[1] = acc[1] + acc2[1];
+    if (t2) {
+      double bcc[2] = {0.0, 0.0}, bcc2[2] = {0.0, 0.0};
+      pnl_mma(*t2, nk4, sa1, sb1, r0, c0, bcc, bcc2);
+      out[0] += bcc[0] + bcc2[0];
+      out[1] += bcc[1] + bcc2[1];
+    }
+    __syncthreads();  // the panels are free for the next stage
+  };
+  // cluster maxima of (x, y) through the shared-memory slots of parity par
+  __shared__ double red[64];
+  auto cmax2 = [&](double x, double y, int par, double& gx, double& gy) {
+    for (int o = 16; o > 0; o >>= 1) {
+      x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+      y = fmax(y, __shfl_xor_sync(0xffffffffu, y, o));
+    }
+    if (lane == 0) {
+      red[warp] = x;
+      red[32 + warp] = y;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double bx = red[0], by = red[32];
+      for (int w = 1; w < nt / 32; ++w) {
+        bx = fmax(bx, red[w]);
+        by = fmax(by, red[32 + w]);
+      }
+      slotmax[par * 32 + rank] = bx;
+      slotmax[par * 32 + 16 + rank] = by;
+    }
+    cl.sync();
+    const double* rs = cl.map_shared_rank(slotmax, lane & 15);
+    double vx = rs[par * 32 + (lane & 15)], vy = rs[par * 32 + 16 + (lane & 15)];
+    for (int o = 8; o > 0; o >>= 1) {
+      vx = fmax(vx, __shfl_xor_sync(0xffffffffu, vx, o));
+      vy = fmax(vy, __shfl_xor_sync(0xffffffffu, vy, o));
+    }
+    gx = vx;
+    gy = vy;
+  };
+  int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
+  double rho_known = 0.0;
+  int par = 0;
+  for (int iter = 1; iter <= a.max_iter; ++iter) {
+    double v[2];
+    // HAUX = CHICHI LAMBDA + CHIPSI
+    product({a.chichi, false, a.lam, false}, nullptr, v);
+    v[0] += cp[0];
+    v[1] += cp[1];
+    put(a.haux, v);
+    cl.sync();
+    // W = LAMBDA^T HAUX + CHIPSI^T LAMBDA + PSIPSI - 1, and its maximum
+    {
+      const PnlTerm t2{a.chipsi, true, a.lam, false};
+      product({a.lam, true, a.haux, false}, &t2, v);
+    }
+    double mx = 0.0;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      double w = v[e] + pp[e];
+      if (ok[e] && gi == gjb + e) w -= 1.0;
+      if (!ok[e]) w = 0.0;
+      v[e] = w;
+      mx = fmax(mx, fabs(w));
+      if (w != w) mx = INFINITY;
+    }
+    put(a.w, v);
+    double digam, unused;
+    cmax2(mx, 0.0, par, digam, unused);
+    par ^= 1;
+    if (digam < a.eps) {
+      status = CUW_OK;
+      iters = iter;
+      break;
+    }
+    if (!(digam <= 1e200)) {
+      status = CUW_ERR_DIVERGED;
+      iters = iter;
+      break;
+    }
+    // HAUX = U^T W
+    product({a.u, true, a.w, false}, nullptr, v);
+    put(a.haux, v);
+    cl.sync();
+    // GT = HAUX U ; X = GT / (e_i + e_j)
+    double gtv[2], xp[2], xq[2];
+    product({a.haux, false, a.u, false}, nullptr, gtv);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) xp[e] = xq[e] = ok[e] ? gtv[e] / den[e] : 0.0;
+    put(a.gamn, xp);
+    cl.sync();
+    double* xcur = a.gamn;
+    double* xnext = a.xb;
+    bool fp_failed = false;
+    if (a.use_e) {
+      // Lyapunov fixed point X <- (GT - E X - X E)/(e_i + e_j), Chebyshev
+      // accelerated as in lyap_fast
+      double prev = INFINITY, rho = rho_known, omega = 1.0;
+      const int cheb0 = rho > 0.0 ? 0 : 2;
+      for (int it2 = 0; it2 < a.max_inner; ++it2) {
+        double ex[2];
+        {
+          const PnlTerm t2{xcur, false, a.emat, false};
+          product({a.emat, false, xcur, false}, &t2, ex);
+        }
+        double dx = 0.0, xm = 0.0, xn[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          xn[e] = 0.0;
+          if (ok[e]) {
+            const double fx = (gtv[e] - ex[e]) / den[e];
+            xn[e] = omega * (fx - xq[e]) + xq[e];
+            dx = fmax(dx, fabs(xn[e] - xp[e]));
+            xm = fmax(xm, fabs(xn[e]));
+          }
+          xq[e] = xp[e];
+          xp[e] = xn[e];
+        }
+        put(xnext, xn);
+        double gdx, gxm;
+        cmax2(dx, xm, par, gdx, gxm);
+        par ^= 1;
+        double* t = xcur;
+        xcur = xnext;
+        xnext = t;
+        if (rank == 0 && tid == 0) a.inner[0] += 1;
+        const double ratio = gdx / prev;
+        if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, a.lyap_tol, fp_failed)) break;
+        if (it2 == cheb0) {
+          if (cheb0 == 2) rho_known = rho = fmin(0.9, fmax(0.05, 1.1 * ratio));
+          omega = 1.0 / (1.0 - 0.5 * rho * rho);
+        } else if (it2 > cheb0) {
+          omega = 1.0 / (1.0 - 0.25 * rho * rho * omega);
+        }
+      }
+    }
+    if (fp_failed) {
+      status = kFixedPointFailed;
+      iters = iter;
+      break;
+    }
+    // HAUX = U X
+    product({a.u, false, xcur, false}, nullptr, v);
+    put(a.haux, v);
+    cl.sync();
+    // LAMBDA -= HAUX U^T (equal occupations)
+    product({a.haux, false, a.u, true}, nullptr, v);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) lamv[e] -= v[e];
+    put(a.lam, lamv);
+    cl.sync();
+  }
+  if (rank == 0 && tid == 0) {
+    a.status[0] = status;
+    a.status[1] = iters;
+  }
+  // no CTA leaves while another may still read its shared-memory slots
+  cl.sync();
+}
+
 // C = op(A) op(B) for n x n matrices, one 32x32 tile per CTA
 __global__ void __launch_bounds__(256) k_small_gemm(const double* A, int tA, const double* B, int tB, int n, double* C,
                                                     const int* gate) {
@@ -1104,6 +1401,33 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, const 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   attr[0].id = cudaLaunchAttributeClusterDimension;
+  // 64 < NB <= 128 with equal occupations: the panel-staged cluster kernel
+  // (k_ortho_x_pnl)
+  if (a.occ_equal && n > 64 && n <= 128 && h->ortho_panel) {
+    bool ok = true;
+    if (!h->capturing && cudaFuncSetAttribute(k_ortho_x_pnl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                             cudaSuccess) {
+      cudaGetLastError();
+      ok = false;
+    }
+    if (ok && smem_allow((const void*)k_ortho_x_pnl, (int)pnl::kSmemBytes) != cudaSuccess) {
+      cudaGetLastError();
+      ok = false;
+    }
+    if (ok) {
+      cfg.gridDim = dim3(16);
+      cfg.dynamicSmemBytes = pnl::kSmemBytes;
+      attr[0].val.clusterDim.x = 16;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cudaError_t e = cudaLaunchKernelEx(&cfg, k_ortho_x_pnl, a);
+      if (e == cudaSuccess) {
+        ++h->launches;
+        return CUW_OK;
+      }
+      cudaGetLastError();
+    }
+  }
   int cs = 16;
   cudaError_t e = cudaSuccess;
   bool launched = false;
