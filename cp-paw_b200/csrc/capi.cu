@@ -389,7 +389,7 @@ static void free_all(Handle* h) {
                   g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1], g.bpre[0],
                   g.bpre[1], g.bsmall, g.jac_a, g.r_plus, g.r_minus, g.r_gx, g.r_gy, g.r_gz, g.r_g2, g.r_ylm,
                   g.r_g0, g.r_v0, g.r_pscore, g.r_vbar, g.r_lmrx, g.qlm, g.r_rhog, g.r_vg, g.r_pot, g.r_vtot,
-                  g.r_grid, g.r_part, g.fpot, g.vqlm, g.r_out};
+                  g.r_grid, g.r_part, g.fpot, g.vqlm, g.r_out, g.prox};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   h->g = Device();

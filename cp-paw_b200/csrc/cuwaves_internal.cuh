@@ -93,6 +93,7 @@ struct Device {
   double *mass = nullptr;        // (NAT)
   double2 *eigr = nullptr;       // (NGL, NAT) structure factors of the last position set
   float2 *pf = nullptr;          // (LDG, NPRO) mixed path: PRO(g,p) of the last position set in fp32, 0 for g >= NGL
+  double2 *prox = nullptr;       // (LDG, NPRO) FP64 path: PRO(g,p) of the last position set, 0 for g >= NGL
   double2 *xminus[2] = {nullptr, nullptr};  // (LDG, NBH) mixed path: X(-G) copies of wave-function arrays
   float *bpre[2] = {nullptr, nullptr};       // mixed path: wave-function arrays split into tf32 B tiles
   const double2 *bpre_src[2] = {nullptr, nullptr};  // arrays they hold (valid inside a solve scope)

@@ -210,6 +210,18 @@ __global__ void k_eigr(const double* __restrict__ gx, const double* __restrict__
   }
 }
 
+// PRO(g,p) of WAVES_EXPANDPRO for every projector of the present positions
+// into prox(LDG, NPRO), zero for NGL <= g < LDG (FP64 handles: the tile
+// loaders of the contractions then read whole columns)
+__global__ void k_pro_f64(int ngl, int ldg, int npro, const ProDesc* __restrict__ pdesc,
+                          const double* __restrict__ ylm, const double* __restrict__ pro,
+                          const double2* __restrict__ eigr, double2* __restrict__ prox) {
+  const int p = blockIdx.y;
+  const ProDesc d = pdesc[p];
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ldg; g += gridDim.x * blockDim.x)
+    prox[(size_t)g + (size_t)ldg * p] = g < ngl ? pro_value(g, ngl, d, ylm, pro, eigr) : make_double2(0.0, 0.0);
+}
+
 __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
 
 // ---------------------------------------------------------------------------
@@ -217,12 +229,15 @@ __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
 // for one or two operands X (psiA -> part, psiB -> part + dual_stride).
 // M = bands (blockIdx.y), N = projectors (blockIdx.x), K = g (blockIdx.z).
 // ---------------------------------------------------------------------------
-template <bool DUAL>
+// TAB: the projector functions come from the expanded table prox(LDG, NPRO)
+// of the present positions (FP64 handles) instead of being formed in the loader.
+template <bool DUAL, bool TAB>
 __global__ void __launch_bounds__(NT, 1) k_proj(const double2* __restrict__ psiA, const double2* __restrict__ psiB,
                                                 int ldg, int ngl, int nbh, int npro, int kchunk,
                                                 const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
                                                 const double* __restrict__ pro, const double2* __restrict__ eigr,
-                                                double2* __restrict__ part, size_t dual_stride) {
+                                                double2* __restrict__ part, size_t dual_stride,
+                                                const double2* __restrict__ prox = nullptr) {
   extern __shared__ double sm[];
   __shared__ ProDesc sd[BN];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
@@ -246,7 +261,10 @@ __global__ void __launch_bounds__(NT, 1) k_proj(const double2* __restrict__ psiA
   };
   auto fb0 = [&](int row, int g) {
     double2 v = zero2();
-    if (g < kend && n0 + row < npro) v = cconj(gen_pro(g, ngl, sd[row], ylm, pro, eigr));
+    if (g < kend && n0 + row < npro) {
+      if constexpr (TAB) v = cconj(prox[(size_t)g + (size_t)ldg * (n0 + row)]);
+      else v = cconj(gen_pro(g, ngl, sd[row], ylm, pro, eigr));
+    }
     return v;
   };
   if (DUAL) mainloop<MP21, true, true>(sm, kbeg, kend, fa0, fa1, fb0, fb0, acc, acc2);
@@ -289,14 +307,15 @@ __global__ void k_reduce_parts(const double2* __restrict__ part, int nz, size_t 
 // mode ADDPRO_OPSI : opsi  = (psi0 + PRO*C2) * dt^2/((1+annee) m_G)
 // mode ADDPRO_FUSED: both, then psim = a1 psi0 + a2 psim + a3/m_G hpsi
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, bool TAB>
 __global__ void __launch_bounds__(NT, 1) k_addpro(double2* __restrict__ hpsi, double2* __restrict__ opsi,
                                                   const double2* __restrict__ psi0, double2* __restrict__ psim,
                                                   const double* __restrict__ mpsi, int ldg, int ngl, int nbh,
                                                   int npro, const double2* __restrict__ c1,
                                                   const double2* __restrict__ c2, const ProDesc* __restrict__ pdesc,
                                                   const double* __restrict__ ylm, const double* __restrict__ pro,
-                                                  const double2* __restrict__ eigr, StepCoef sc) {
+                                                  const double2* __restrict__ eigr, StepCoef sc,
+                                                  const double2* __restrict__ prox) {
   constexpr bool USE_H = (MODE != ADDPRO_OPSI);
   constexpr bool USE_O = (MODE != ADDPRO_HPSI);
   extern __shared__ double sm[];
@@ -307,7 +326,9 @@ __global__ void __launch_bounds__(NT, 1) k_addpro(double2* __restrict__ hpsi, do
   acc2.zero();
   auto fa = [&](int row, int p) {
     int g = m0 + row;
-    return (g < ngl && p < npro) ? gen_pro(g, ngl, pdesc[p], ylm, pro, eigr) : zero2();
+    if (!(g < ngl && p < npro)) return zero2();
+    if constexpr (TAB) return prox[(size_t)g + (size_t)ldg * p];
+    else return gen_pro(g, ngl, pdesc[p], ylm, pro, eigr);
   };
   auto fb1 = [&](int row, int p) {
     int b = n0 + row;
@@ -497,12 +518,14 @@ __global__ void k_addoproj(double2* __restrict__ out, const double2* __restrict_
 // cancels in this sum (c(-G) = -conj(c(G)) for c = i Y P (-i)^l EIGR over the
 // full sphere), so it is not applied.
 // ---------------------------------------------------------------------------
+template <bool TAB>
 __global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi0, int ldg, int ngl, int nbh,
                                                  int npro, const double2* __restrict__ ded,
                                                  const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
                                                  const double* __restrict__ pro, const double2* __restrict__ eigr,
                                                  const double* __restrict__ gx, const double* __restrict__ gy,
-                                                 const double* __restrict__ gz, double* __restrict__ fpart) {
+                                                 const double* __restrict__ gz, double* __restrict__ fpart,
+                                                 const double2* __restrict__ prox) {
   extern __shared__ double sm[];
   __shared__ double fred[BN][3][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
@@ -534,13 +557,20 @@ __global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi
         acc_mn(wm, wn, lane, mi, ni, e, m, n);
         int g = m0 + m, p = n0 + n;
         if (g < ngl && p < npro) {
-          ProDesc d = pdesc[p];
-          double pr = pro[(size_t)g + (size_t)ngl * d.ibare];
-          double y = ylm[(size_t)g + (size_t)ngl * d.lm];
-          // cw = i * P * (-i)^l * EIGR
-          double2 cw = cmul(make_double2(0.0, pr), cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]));
           double2 dd = make_double2(acc.r[mi][ni][e], acc.i[mi][ni][e]);
-          double sv = (cw.x * dd.x + cw.y * dd.y) * y;  // Re(cw * conj(dd)) * Y
+          double sv;
+          if constexpr (TAB) {
+            // Re(i PRO(g,p) conj(dd))
+            const double2 pv = prox[(size_t)g + (size_t)ldg * p];
+            sv = -pv.y * dd.x + pv.x * dd.y;
+          } else {
+            ProDesc d = pdesc[p];
+            double pr = pro[(size_t)g + (size_t)ngl * d.ibare];
+            double y = ylm[(size_t)g + (size_t)ngl * d.lm];
+            // cw = i * P * (-i)^l * EIGR
+            double2 cw = cmul(make_double2(0.0, pr), cmul(mipow(d.l), eigr[(size_t)g + (size_t)ngl * d.iat]));
+            sv = (cw.x * dd.x + cw.y * dd.y) * y;  // Re(cw * conj(dd)) * Y
+          }
           f[ni][e][0] += sv * gx[g];
           f[ni][e][1] += sv * gy[g];
           f[ni][e][2] += sv * gz[g];
@@ -679,6 +709,16 @@ int eigr_compute(Handle* h, const double* r_dev) {
   k_eigr<<<grid, 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz, r_dev, h->d.ngl, h->d.nat, h->g.eigr);
   CUW_LAUNCH_CHECK("k_eigr");
   if (h->mixed()) CUW_RET(tc_pro_table(h));
+  else if (h->npro > 0) {
+    if (!h->g.prox) {
+      if (h->capturing) return h->fail(CUW_ERR_STATE, "projector table allocated during graph capture");
+      h->touch();
+      CUW_TRY(cudaMalloc(&h->g.prox, sizeof(double2) * (size_t)h->ldg * h->npro));
+    }
+    k_pro_f64<<<dim3(std::min(ceil_div(h->ldg, 256), 64), h->npro), 256, 0, h->stream>>>(
+        h->d.ngl, h->ldg, h->npro, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.prox);
+    CUW_LAUNCH_CHECK("k_pro_f64");
+  }
   if (pos) h->eigr_src = r_dev;
   return CUW_OK;
 }
@@ -698,12 +738,24 @@ int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* 
   const bool dual = (psiB != nullptr);
   CUW_RET(ensure_part(h, sizeof(double2) * one * (dual ? 2 : 1)));
   dim3 grid(tn, tm, ks);
-  if (dual)
-    k_proj<true><<<grid, NT, smem_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
-                                             h->g.pro, h->g.eigr, h->g.part, one);
+  // FP64 handles read the expanded projector table; the FP64 products of a
+  // mixed handle (start-up orthonormalisation, orthonormality test) form it
+  const bool tab = !h->mixed() && h->g.prox;
+  const Device& g = h->g;
+  if (dual && tab)
+    k_proj<true, true><<<grid, NT, smem_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk,
+                                                                   g.pdesc, g.ylm, g.pro, g.eigr, g.part, one,
+                                                                   g.prox);
+  else if (dual)
+    k_proj<true, false><<<grid, NT, smem_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk,
+                                                                    g.pdesc, g.ylm, g.pro, g.eigr, g.part, one);
+  else if (tab)
+    k_proj<false, true><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk,
+                                                                    g.pdesc, g.ylm, g.pro, g.eigr, g.part, 0,
+                                                                    g.prox);
   else
-    k_proj<false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk, h->g.pdesc, h->g.ylm,
-                                              h->g.pro, h->g.eigr, h->g.part, 0);
+    k_proj<false, false><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk,
+                                                                     g.pdesc, g.ylm, g.pro, g.eigr, g.part, 0);
   CUW_LAUNCH_CHECK("k_proj");
   const size_t n = (size_t)nbh * npro;
   const int rb = std::min(ceil_div((int)std::min<size_t>(n, 1 << 30), 256), 4 * h->nsm);
@@ -726,19 +778,20 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
   sc.oscale = h->delt * h->delt / (1.0 + h->annee);  // src/paw_waves2.f90:148-156
   if (h->tc_on()) return tc_addpro(h, mode, hpc, opc, sc);
   Device& g = h->g;
+  const bool tab = !h->mixed() && g.prox;
+#define CUW_ADDPRO(MODE_, MP_)                                                                                  \
+  (tab ? k_addpro<MODE_, true><<<grid, NT, smem_bytes<MP_>(), h->stream>>>(                                      \
+             g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro, hpc, opc, g.pdesc, g.ylm, g.pro,    \
+             g.eigr, sc, g.prox)                                                                                 \
+       : k_addpro<MODE_, false><<<grid, NT, smem_bytes<MP_>(), h->stream>>>(                                     \
+             g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro, hpc, opc, g.pdesc, g.ylm, g.pro,    \
+             g.eigr, sc, nullptr))
   switch (mode) {
-    case ADDPRO_HPSI:
-      k_addpro<ADDPRO_HPSI><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
-                                                         hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
-      break;
-    case ADDPRO_OPSI:
-      k_addpro<ADDPRO_OPSI><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro,
-                                                         hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
-      break;
-    default:
-      k_addpro<ADDPRO_FUSED><<<grid, NT, smem_bytes<MP12>(), h->stream>>>(g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh,
-                                                          npro, hpc, opc, g.pdesc, g.ylm, g.pro, g.eigr, sc);
+    case ADDPRO_HPSI: CUW_ADDPRO(ADDPRO_HPSI, MP11); break;
+    case ADDPRO_OPSI: CUW_ADDPRO(ADDPRO_OPSI, MP11); break;
+    default: CUW_ADDPRO(ADDPRO_FUSED, MP12);
   }
+#undef CUW_ADDPRO
   CUW_LAUNCH_CHECK("k_addpro");
   return CUW_OK;
 }
@@ -929,9 +982,14 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
   if (h->tc_on()) {
     CUW_RET(tc_force(h, ded, fpart, &tm));
   } else {
-    k_force<<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc,
-                                                                 h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
-                                                                 h->g.gz, fpart);
+    if (!h->mixed() && h->g.prox)
+      k_force<true><<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(
+          h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
+          h->g.gz, fpart, h->g.prox);
+    else
+      k_force<false><<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(
+          h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
+          h->g.gz, fpart, nullptr);
     CUW_LAUNCH_CHECK("k_force");
   }
   TabView t = tables(h);
@@ -943,15 +1001,21 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
 
 // dynamic shared memory above 48 KB for the pipelined contraction kernels
 int gemm_setup(Handle* h) {
-  CUW_TRY(smem_allow((const void*)k_proj<true>, (int)smem_bytes<MP21>()));
-  CUW_TRY(smem_allow((const void*)k_proj<false>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED>, (int)smem_bytes<MP12>()));
+  CUW_TRY(smem_allow((const void*)k_proj<true, false>, (int)smem_bytes<MP21>()));
+  CUW_TRY(smem_allow((const void*)k_proj<false, false>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_proj<true, true>, (int)smem_bytes<MP21>()));
+  CUW_TRY(smem_allow((const void*)k_proj<false, true>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI, false>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI, false>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED, false>, (int)smem_bytes<MP12>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI, true>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI, true>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED, true>, (int)smem_bytes<MP12>()));
   CUW_TRY(smem_allow((const void*)k_gram<true, true>, (int)smem_bytes<MPGRAM>()));
   CUW_TRY(smem_allow((const void*)k_gram<false, false>, (int)smem_bytes<MPGRAM>()));
   CUW_TRY(smem_allow((const void*)k_addx<true, true>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_force, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_force<false>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_force<true>, (int)smem_bytes<MP11>()));
   return CUW_OK;
 }
 
@@ -1028,7 +1092,7 @@ static int noalloc_scratch(double2** out) {
   if (!g_noalloc_ptr[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return CUW_ERR_CUDA;
-    if (cuw::smem_allow((const void*)cuw::k_proj<false>, (int)cuw::smem_bytes<cuw::MP11>()) != cudaSuccess)
+    if (cuw::smem_allow((const void*)cuw::k_proj<false, false>, (int)cuw::smem_bytes<cuw::MP11>()) != cudaSuccess)
       return CUW_ERR_CUDA;
     g_noalloc_ptr[dev] = static_cast<double2*>(p);
   }
@@ -1064,7 +1128,7 @@ extern "C" int cuwaves_projections_noalloc(int ngl, int ldg, int nbh, int nat, i
   // every partial sum that the reduction reads is written by k_proj in this
   // call, so nothing in the array has to start at zero; with no error pending
   // before the launches, cudaGetLastError reports only their own failures
-  k_proj<false><<<dim3(tn, tm, ks), NT, smem_bytes<MP11>(), st>>>(
+  k_proj<false, false><<<dim3(tn, tm, ks), NT, smem_bytes<MP11>(), st>>>(
       reinterpret_cast<const double2*>(psi), nullptr, ldg, ngl, nbh, npro, kchunk,
       reinterpret_cast<const ProDesc*>(pdesc), ylm, pro, reinterpret_cast<const double2*>(eigr), scratch, 0);
   if (cudaGetLastError() != cudaSuccess) return CUW_ERR_CUDA;

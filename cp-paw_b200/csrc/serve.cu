@@ -85,6 +85,7 @@ size_t estimate_bytes(const cuw_dims& d, const int* isp) {
   b += std::min(nbh * nr * 16, ((size_t)48 << 20) + nr * 16);  // FFT work grid
   b += (size_t)20 << 20;                               // split-K partials and small tables
   if (d.precision == CUW_PREC_MIXED) b += ldg * npro * 8;  // fp32 projector table
+  else b += ldg * npro * 16;                               // fp64 projector table
   return b;
 }
 
