@@ -185,6 +185,149 @@ __device__ __forceinline__ void mainloop(double* sm, int kbeg, int kend, FA0 fa0
   }
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous main loop for operands that are plain arrays (or gathers of
+// plain elements): every complex element of a K slice goes to shared memory
+// by one 16-byte cp.async straight from its address, NS2 slices in flight, so
+// no register staging and no load latency in the MMA warps' path.  Tiles
+// hold complex elements interleaved, [row][k] at a row stride of LD2 = 20
+// (16-byte words), which keeps the m8n8k4 fragment reads free of bank
+// conflicts and gives the real and imaginary part of a fragment in one load.
+//   pa0/pa1/pb0/pb1(row, k) -> address of the element, or nullptr for zero
+//   ca0(k)/ca1(k): conjugate A at global K index k in the product of acc0/acc1
+//   CB0/CB1: conjugate B in the product of acc0/acc1
+// ---------------------------------------------------------------------------
+constexpr int LD2 = 20;
+constexpr int LDR = BM + 2;      // [k][row] tiles (row contiguous in global memory)
+constexpr int TILE2 = BM * LD2;  // double2 of one operand tile (either layout fits)
+static_assert(BK * LDR <= TILE2, "tile layouts");
+// offset of element (row, k) of a tile: [row][k] when K is the contiguous
+// dimension of the operand in global memory (KF), else [k][row], so that
+// consecutive threads' 16-byte copies land in consecutive words either way
+template <bool KF>
+__device__ __forceinline__ int toff(int row, int k) {
+  if constexpr (KF) return row * LD2 + k;
+  else return k * LDR + row;
+}
+constexpr int NS2 = 3;           // K slices in flight
+
+__device__ const double2 g_zero2[1] = {{0.0, 0.0}};
+
+__device__ __forceinline__ void cpa16(double2* dst, const double2* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src ? src : g_zero2),
+               "r"(src ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <bool AKF, bool BKF, bool CB, class CA>
+__device__ __forceinline__ void mma_slice2(Acc& acc, const double2* A, const double2* B, int wm, int wn, int lane,
+                                           int k0, CA ca) {
+  const int r8 = lane >> 2, c4 = lane & 3;
+#pragma unroll
+  for (int ks = 0; ks < BK / 4; ++ks) {
+    const bool cj = ca(k0 + ks * 4 + c4);
+    double ar[4], ai[4], nai[4], br[2], bi[2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      const double2 v = A[toff<AKF>(wm * 32 + mi * 8 + r8, ks * 4 + c4)];
+      ar[mi] = v.x;
+      ai[mi] = cj ? -v.y : v.y;
+      nai[mi] = -ai[mi];
+    }
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni) {
+      const double2 w = B[toff<BKF>(wn * 16 + ni * 8 + r8, ks * 4 + c4)];
+      br[ni] = w.x;
+      bi[ni] = CB ? -w.y : w.y;
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        dmma(acc.r[mi][ni], ar[mi], br[ni]);
+        dmma(acc.i[mi][ni], ar[mi], bi[ni]);
+      }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        dmma(acc.r[mi][ni], nai[mi], bi[ni]);
+        dmma(acc.i[mi][ni], ai[mi], br[ni]);
+      }
+  }
+}
+
+struct NoConj {
+  __device__ __forceinline__ bool operator()(int) const { return false; }
+};
+struct AllConj {
+  __device__ __forceinline__ bool operator()(int) const { return true; }
+};
+
+template <int MODE, bool AKF, bool BKF, bool CB0, bool CB1, class PA0, class PA1, class PB0, class PB1, class CA0,
+          class CA1>
+__device__ __forceinline__ void mainloop2(double2* sm, int kbeg, int kend, PA0 pa0, PA1 pa1, PB0 pb0, PB1 pb1,
+                                          CA0 ca0, CA1 ca1, Acc& acc0, Acc& acc1) {
+  constexpr int NA = (MODE == MP21) ? 2 : 1;
+  constexpr int NBO = (MODE == MP12 || MODE == MPGRAM) ? 2 : 1;
+  constexpr int STAGE = TILE2 * (NA + NBO);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  if (kbeg >= kend) return;
+  const int nsl = (kend - kbeg + BK - 1) / BK;
+  auto issue = [&](int sl) {
+    double2* base = sm + (size_t)(sl % NS2) * STAGE;
+    const int k0 = kbeg + sl * BK;
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      int row, kk;
+      tile_rc<AKF>(tid + q * NT, row, kk);
+      cpa16(base + toff<AKF>(row, kk), pa0(row, k0 + kk));
+      if (NA == 2) cpa16(base + TILE2 + toff<AKF>(row, kk), pa1(row, k0 + kk));
+      tile_rc<BKF>(tid + q * NT, row, kk);
+      cpa16(base + NA * TILE2 + toff<BKF>(row, kk), pb0(row, k0 + kk));
+      if (NBO == 2) cpa16(base + (NA + 1) * TILE2 + toff<BKF>(row, kk), pb1(row, k0 + kk));
+    }
+  };
+#pragma unroll
+  for (int sl = 0; sl < NS2 - 1; ++sl) {
+    if (sl < nsl) issue(sl);
+    cpa_commit();
+  }
+  for (int sl = 0; sl < nsl; ++sl) {
+    cpa_wait<NS2 - 2>();
+    __syncthreads();
+    const double2* base = sm + (size_t)(sl % NS2) * STAGE;
+    const int k0 = kbeg + sl * BK;
+    const double2* A0 = base;
+    const double2* B0 = base + NA * TILE2;
+    if (MODE == MP11) {
+      mma_slice2<AKF, BKF, CB0>(acc0, A0, B0, wm, wn, lane, k0, ca0);
+    } else if (MODE == MP21) {
+      mma_slice2<AKF, BKF, CB0>(acc0, A0, B0, wm, wn, lane, k0, ca0);
+      mma_slice2<AKF, BKF, CB1>(acc1, A0 + TILE2, B0, wm, wn, lane, k0, ca1);
+    } else {
+      mma_slice2<AKF, BKF, CB0>(acc0, A0, B0, wm, wn, lane, k0, ca0);
+      mma_slice2<AKF, BKF, CB1>(acc1, A0, B0 + TILE2, wm, wn, lane, k0, ca1);
+    }
+    if (sl + NS2 - 1 < nsl) issue(sl + NS2 - 1);
+    cpa_commit();
+  }
+  cpa_wait<0>();
+  __syncthreads();
+}
+
+template <int MODE>
+constexpr size_t smem2_bytes() {
+  return sizeof(double2) * (size_t)NS2 * TILE2 *
+         (((MODE == MP21) ? 2 : 1) + ((MODE == MP12 || MODE == MPGRAM) ? 2 : 1));
+}
+
 template <int MODE>
 constexpr size_t smem_bytes() {
   return sizeof(double) * 2 * 2 * TILE * (((MODE == MP21) ? 2 : 1) + ((MODE == MP12 || MODE == MPGRAM) ? 2 : 1));
@@ -267,8 +410,25 @@ __global__ void __launch_bounds__(NT, 1) k_proj(const double2* __restrict__ psiA
     }
     return v;
   };
-  if (DUAL) mainloop<MP21, true, true>(sm, kbeg, kend, fa0, fa1, fb0, fb0, acc, acc2);
-  else mainloop<MP11, true, true>(sm, kbeg, kend, fa0, fa0, fb0, fb0, acc, acc2);
+  if constexpr (TAB) {
+    auto pa0 = [&](int row, int g) -> const double2* {
+      const int b = m0 + row;
+      return (g < kend && b < nbh) ? psiA + (size_t)g + (size_t)ldg * b : nullptr;
+    };
+    auto pa1 = [&](int row, int g) -> const double2* {
+      const int b = m0 + row;
+      return (DUAL && g < kend && b < nbh) ? psiB + (size_t)g + (size_t)ldg * b : nullptr;
+    };
+    auto pb0 = [&](int row, int g) -> const double2* {
+      return (g < kend && n0 + row < npro) ? prox + (size_t)g + (size_t)ldg * (n0 + row) : nullptr;
+    };
+    double2* sm2 = reinterpret_cast<double2*>(sm);
+    if (DUAL) mainloop2<MP21, true, true, true, true>(sm2, kbeg, kend, pa0, pa1, pb0, pb0, NoConj(), NoConj(), acc, acc2);
+    else mainloop2<MP11, true, true, true, true>(sm2, kbeg, kend, pa0, pa0, pb0, pb0, NoConj(), NoConj(), acc, acc2);
+  } else {
+    if (DUAL) mainloop<MP21, true, true>(sm, kbeg, kend, fa0, fa1, fb0, fb0, acc, acc2);
+    else mainloop<MP11, true, true>(sm, kbeg, kend, fa0, fa0, fb0, fb0, acc, acc2);
+  }
   double2* out = part + (size_t)blockIdx.z * nbh * npro;
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
@@ -338,9 +498,31 @@ __global__ void __launch_bounds__(NT, 1) k_addpro(double2* __restrict__ hpsi, do
     int b = n0 + row;
     return (b < nbh && p < npro) ? c2[(size_t)b + (size_t)nbh * p] : zero2();
   };
-  if (MODE == ADDPRO_FUSED) mainloop<MP12, false, false>(sm, 0, npro, fa, fa, fb1, fb2, acc, acc2);
-  else if (MODE == ADDPRO_HPSI) mainloop<MP11, false, false>(sm, 0, npro, fa, fa, fb1, fb1, acc, acc2);
-  else mainloop<MP11, false, false>(sm, 0, npro, fa, fa, fb2, fb2, acc2, acc);
+  if constexpr (TAB) {
+    auto pa = [&](int row, int p) -> const double2* {
+      const int g = m0 + row;
+      return (g < ngl && p < npro) ? prox + (size_t)g + (size_t)ldg * p : nullptr;
+    };
+    auto pb1 = [&](int row, int p) -> const double2* {
+      const int b = n0 + row;
+      return (b < nbh && p < npro) ? c1 + (size_t)b + (size_t)nbh * p : nullptr;
+    };
+    auto pb2 = [&](int row, int p) -> const double2* {
+      const int b = n0 + row;
+      return (b < nbh && p < npro) ? c2 + (size_t)b + (size_t)nbh * p : nullptr;
+    };
+    double2* sm2 = reinterpret_cast<double2*>(sm);
+    if (MODE == ADDPRO_FUSED)
+      mainloop2<MP12, false, false, false, false>(sm2, 0, npro, pa, pa, pb1, pb2, NoConj(), NoConj(), acc, acc2);
+    else if (MODE == ADDPRO_HPSI)
+      mainloop2<MP11, false, false, false, false>(sm2, 0, npro, pa, pa, pb1, pb1, NoConj(), NoConj(), acc, acc2);
+    else
+      mainloop2<MP11, false, false, false, false>(sm2, 0, npro, pa, pa, pb2, pb2, NoConj(), NoConj(), acc2, acc);
+  } else {
+    if (MODE == ADDPRO_FUSED) mainloop<MP12, false, false>(sm, 0, npro, fa, fa, fb1, fb2, acc, acc2);
+    else if (MODE == ADDPRO_HPSI) mainloop<MP11, false, false>(sm, 0, npro, fa, fa, fb1, fb1, acc, acc2);
+    else mainloop<MP11, false, false>(sm, 0, npro, fa, fa, fb2, fb2, acc2, acc);
+  }
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -401,21 +583,22 @@ __global__ void __launch_bounds__(NT, 1) k_gram(GramArgs a, const int* __restric
   Acc t1, t2;
   t1.zero();
   t2.zero();
-  auto fa = [&](int row, int k) {
+  auto pa = [&](int row, int k) -> const double2* {
     int m = m0 + row;
-    return (k < kend && m < a.nm) ? X[(size_t)k * a.sk + (size_t)m * a.sm] : zero2();
+    return (k < kend && m < a.nm) ? X + (size_t)k * a.sk + (size_t)m * a.sm : nullptr;
   };
-  auto fb = [&](int row, int k) {
+  auto pb = [&](int row, int k) -> const double2* {
     int n = n0 + row;
-    return (k < kend && n < a.nn) ? Y[(size_t)k * a.sk + (size_t)n * a.sm] : zero2();
+    return (k < kend && n < a.nn) ? Y + (size_t)k * a.sk + (size_t)n * a.sm : nullptr;
   };
-  auto fb2 = [&](int row, int k) {
+  auto pb2 = [&](int row, int k) -> const double2* {
     int n = n0 + row;
-    if (!(k < kend && n < a.nn)) return zero2();
+    if (!(k < kend && n < a.nn)) return nullptr;
     int kk = MINUS ? minusg[k] : k;
-    return Y[(size_t)kk * a.sk + (size_t)n * a.sm];
+    return Y + (size_t)kk * a.sk + (size_t)n * a.sm;
   };
-  mainloop<MPGRAM, KFAST, KFAST>(sm, kbeg, kend, fa, fa, fb, fb2, t1, t2);
+  mainloop2<MPGRAM, KFAST, KFAST, false, false>(reinterpret_cast<double2*>(sm), kbeg, kend, pa, pa, pb, pb2,
+                                                AllConj(), NoConj(), t1, t2);
   const size_t mn = (size_t)a.nm * a.nn;
   double2* o1 = part + ((size_t)blockIdx.z * 2 + 0) * mn;
   double2* o2 = part + ((size_t)blockIdx.z * 2 + 1) * mn;
@@ -459,19 +642,23 @@ __global__ void __launch_bounds__(NT, 1) k_addx(AddXArgs a, const int* __restric
   Acc acc, dummy;
   acc.zero();
   const int ktot = 2 * a.nk;
-  auto fa = [&](int row, int kg) {
+  // the second half of K takes conj(X(-g)): conjugated at the fragment read
+  auto pa = [&](int row, int kg) -> const double2* {
     int m = m0 + row;
-    if (!(m < a.nm && kg < ktot)) return zero2();
-    if (kg < a.nk) return a.x[(size_t)m * a.sxm + (size_t)kg * a.sxk];
+    if (!(m < a.nm && kg < ktot)) return nullptr;
+    if (kg < a.nk) return a.x + (size_t)m * a.sxm + (size_t)kg * a.sxk;
     int mm2 = XMINUS ? minusg[m] : m;
-    return cconj(a.x[(size_t)mm2 * a.sxm + (size_t)(kg - a.nk) * a.sxk]);
+    return a.x + (size_t)mm2 * a.sxm + (size_t)(kg - a.nk) * a.sxk;
   };
-  auto fb = [&](int row, int kg) {
+  auto pb = [&](int row, int kg) -> const double2* {
     int n = n0 + row;
-    if (!(n < a.nn && kg < ktot)) return zero2();
-    return kg < a.nk ? a.l1[(size_t)kg + (size_t)a.nk * n] : a.l2[(size_t)(kg - a.nk) + (size_t)a.nk * n];
+    if (!(n < a.nn && kg < ktot)) return nullptr;
+    return kg < a.nk ? a.l1 + (size_t)kg + (size_t)a.nk * n : a.l2 + (size_t)(kg - a.nk) + (size_t)a.nk * n;
   };
-  mainloop<MP11, !MFAST, true>(sm, 0, ktot, fa, fa, fb, fb, acc, dummy);
+  const int nk = a.nk;
+  auto second = [nk](int kg) { return kg >= nk; };
+  mainloop2<MP11, !MFAST, true, false, false>(reinterpret_cast<double2*>(sm), 0, ktot, pa, pa, pb, pb, second,
+                                              second, acc, dummy);
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -532,15 +719,16 @@ __global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   Acc acc, dummy;
   acc.zero();
-  auto fa = [&](int row, int b) {
+  auto pa = [&](int row, int b) -> const double2* {
     int g = m0 + row;
-    return (g < ngl && b < nbh) ? psi0[(size_t)g + (size_t)ldg * b] : zero2();
+    return (g < ngl && b < nbh) ? psi0 + (size_t)g + (size_t)ldg * b : nullptr;
   };
-  auto fb = [&](int row, int b) {
+  auto pb = [&](int row, int b) -> const double2* {
     int p = n0 + row;
-    return (b < nbh && p < npro) ? cconj(ded[(size_t)b + (size_t)nbh * p]) : zero2();
+    return (b < nbh && p < npro) ? ded + (size_t)b + (size_t)nbh * p : nullptr;
   };
-  mainloop<MP11, false, true>(sm, 0, nbh, fa, fa, fb, fb, acc, dummy);
+  mainloop2<MP11, false, true, true, true>(reinterpret_cast<double2*>(sm), 0, nbh, pa, pa, pb, pb, NoConj(),
+                                           NoConj(), acc, dummy);
   // epilogue: per (g, p) contribution, reduced over g
   double f[2][2][3];
 #pragma unroll
@@ -743,14 +931,14 @@ int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* 
   const bool tab = !h->mixed() && h->g.prox;
   const Device& g = h->g;
   if (dual && tab)
-    k_proj<true, true><<<grid, NT, smem_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk,
+    k_proj<true, true><<<grid, NT, smem2_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk,
                                                                    g.pdesc, g.ylm, g.pro, g.eigr, g.part, one,
                                                                    g.prox);
   else if (dual)
     k_proj<true, false><<<grid, NT, smem_bytes<MP21>(), h->stream>>>(psiA, psiB, h->ldg, ngl, nbh, npro, kchunk,
                                                                     g.pdesc, g.ylm, g.pro, g.eigr, g.part, one);
   else if (tab)
-    k_proj<false, true><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk,
+    k_proj<false, true><<<grid, NT, smem2_bytes<MP11>(), h->stream>>>(psiA, nullptr, h->ldg, ngl, nbh, npro, kchunk,
                                                                     g.pdesc, g.ylm, g.pro, g.eigr, g.part, 0,
                                                                     g.prox);
   else
@@ -780,7 +968,7 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
   Device& g = h->g;
   const bool tab = !h->mixed() && g.prox;
 #define CUW_ADDPRO(MODE_, MP_)                                                                                  \
-  (tab ? k_addpro<MODE_, true><<<grid, NT, smem_bytes<MP_>(), h->stream>>>(                                      \
+  (tab ? k_addpro<MODE_, true><<<grid, NT, smem2_bytes<MP_>(), h->stream>>>(                                      \
              g.hpsi, g.opsi, g.psi0, g.psim, g.mpsi, h->ldg, ngl, nbh, npro, hpc, opc, g.pdesc, g.ylm, g.pro,    \
              g.eigr, sc, g.prox)                                                                                 \
        : k_addpro<MODE_, false><<<grid, NT, smem_bytes<MP_>(), h->stream>>>(                                     \
@@ -921,8 +1109,8 @@ static int gram_run(Handle* h, const GramPair* pairs, int npair, bool minus, int
   const size_t mn = (size_t)nm * nm;
   CUW_RET(ensure_part(h, sizeof(double2) * mn * 2 * npair * ks));
   dim3 grid(ceil_div(nm, BN), ceil_div(nm, BM), ks * npair);
-  if (minus) k_gram<true, true><<<grid, NT, smem_bytes<MPGRAM>(), h->stream>>>(a, h->g.minusg, h->g.part);
-  else k_gram<false, false><<<grid, NT, smem_bytes<MPGRAM>(), h->stream>>>(a, h->g.minusg, h->g.part);
+  if (minus) k_gram<true, true><<<grid, NT, smem2_bytes<MPGRAM>(), h->stream>>>(a, h->g.minusg, h->g.part);
+  else k_gram<false, false><<<grid, NT, smem2_bytes<MPGRAM>(), h->stream>>>(a, h->g.minusg, h->g.part);
   CUW_LAUNCH_CHECK("k_gram");
   // reduce over splits: layout part[(split*npair+pair)*2+t] -> dst[(pair*2+t)]
   const size_t n = mn * 2 * npair;
@@ -955,7 +1143,7 @@ int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* 
   a.son = (size_t)h->ldg;
   if (h->tc_on()) return tc_addx(h, true, a.out, a.x, a.l1, a.l2, a.nm, a.nn, a.nk, a.sxm, a.sxk, a.som, a.son);
   dim3 grid(ceil_div(a.nm, BM), ceil_div(a.nn, BN));
-  k_addx<true, true><<<grid, NT, smem_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
+  k_addx<true, true><<<grid, NT, smem2_bytes<MP11>(), h->stream>>>(a, h->g.minusg);
   CUW_LAUNCH_CHECK("k_addx");
   return CUW_OK;
 }
@@ -983,11 +1171,11 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
     CUW_RET(tc_force(h, ded, fpart, &tm));
   } else {
     if (!h->mixed() && h->g.prox)
-      k_force<true><<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(
+      k_force<true><<<dim3(tm, tn), NT, smem2_bytes<MP11>(), h->stream>>>(
           h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
           h->g.gz, fpart, h->g.prox);
     else
-      k_force<false><<<dim3(tm, tn), NT, smem_bytes<MP11>(), h->stream>>>(
+      k_force<false><<<dim3(tm, tn), NT, smem2_bytes<MP11>(), h->stream>>>(
           h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.gx, h->g.gy,
           h->g.gz, fpart, nullptr);
     CUW_LAUNCH_CHECK("k_force");
@@ -1003,19 +1191,19 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
 int gemm_setup(Handle* h) {
   CUW_TRY(smem_allow((const void*)k_proj<true, false>, (int)smem_bytes<MP21>()));
   CUW_TRY(smem_allow((const void*)k_proj<false, false>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_proj<true, true>, (int)smem_bytes<MP21>()));
-  CUW_TRY(smem_allow((const void*)k_proj<false, true>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_proj<true, true>, (int)smem2_bytes<MP21>()));
+  CUW_TRY(smem_allow((const void*)k_proj<false, true>, (int)smem2_bytes<MP11>()));
   CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI, false>, (int)smem_bytes<MP11>()));
   CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI, false>, (int)smem_bytes<MP11>()));
   CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED, false>, (int)smem_bytes<MP12>()));
-  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI, true>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI, true>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED, true>, (int)smem_bytes<MP12>()));
-  CUW_TRY(smem_allow((const void*)k_gram<true, true>, (int)smem_bytes<MPGRAM>()));
-  CUW_TRY(smem_allow((const void*)k_gram<false, false>, (int)smem_bytes<MPGRAM>()));
-  CUW_TRY(smem_allow((const void*)k_addx<true, true>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_force<false>, (int)smem_bytes<MP11>()));
-  CUW_TRY(smem_allow((const void*)k_force<true>, (int)smem_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_HPSI, true>, (int)smem2_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_OPSI, true>, (int)smem2_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_addpro<ADDPRO_FUSED, true>, (int)smem2_bytes<MP12>()));
+  CUW_TRY(smem_allow((const void*)k_gram<true, true>, (int)smem2_bytes<MPGRAM>()));
+  CUW_TRY(smem_allow((const void*)k_gram<false, false>, (int)smem2_bytes<MPGRAM>()));
+  CUW_TRY(smem_allow((const void*)k_addx<true, true>, (int)smem2_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_force<false>, (int)smem2_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_force<true>, (int)smem2_bytes<MP11>()));
   return CUW_OK;
 }
 
