@@ -355,14 +355,31 @@ __global__ void k_eigr(const double* __restrict__ gx, const double* __restrict__
 
 // PRO(g,p) of WAVES_EXPANDPRO for every projector of the present positions
 // into prox(LDG, NPRO), zero for NGL <= g < LDG (FP64 handles: the tile
-// loaders of the contractions then read whole columns)
-__global__ void k_pro_f64(int ngl, int ldg, int npro, const ProDesc* __restrict__ pdesc,
-                          const double* __restrict__ ylm, const double* __restrict__ pro,
-                          const double2* __restrict__ eigr, double2* __restrict__ prox) {
-  const int p = blockIdx.y;
-  const ProDesc d = pdesc[p];
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ldg; g += gridDim.x * blockDim.x)
-    prox[(size_t)g + (size_t)ldg * p] = g < ngl ? pro_value(g, ngl, d, ylm, pro, eigr) : make_double2(0.0, 0.0);
+// loaders of the contractions then read whole columns), straight from the
+// positions: one thread per (g, atom) forms exp(-iG.R_a) as k_eigr does and
+// writes the atom's projectors, so no EIGR array is formed.
+__global__ void k_pro_f64_direct(int ngl, int ldg, const double* __restrict__ gx, const double* __restrict__ gy,
+                                 const double* __restrict__ gz, const double* __restrict__ r,
+                                 const int* __restrict__ ipro0, const int* __restrict__ nlmn,
+                                 const ProDesc* __restrict__ pdesc, const double* __restrict__ ylm,
+                                 const double* __restrict__ pro, double2* __restrict__ prox) {
+  const int a = blockIdx.y;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ldg) return;
+  const int p0 = ipro0[a], np = nlmn[a];
+  if (g >= ngl) {
+    for (int k = 0; k < np; ++k) prox[(size_t)g + (size_t)ldg * (p0 + k)] = make_double2(0.0, 0.0);
+    return;
+  }
+  double sn, cs;
+  sincos(gx[g] * r[3 * a] + gy[g] * r[3 * a + 1] + gz[g] * r[3 * a + 2], &sn, &cs);
+  const double2 ei = make_double2(cs, -sn);
+  for (int k = 0; k < np; ++k) {
+    const ProDesc d = pdesc[p0 + k];
+    const double sv = ylm[(size_t)g + (size_t)ngl * d.lm] * pro[(size_t)g + (size_t)ngl * d.ibare];
+    const double2 e = cmul(mipow(d.l), ei);
+    prox[(size_t)g + (size_t)ldg * (p0 + k)] = make_double2(sv * e.x, sv * e.y);
+  }
 }
 
 __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
@@ -893,19 +910,23 @@ int eigr_compute(Handle* h, const double* r_dev) {
   const bool pos = r_dev == h->g.r0 || r_dev == h->g.rp || r_dev == h->g.rm;
   if (pos && r_dev == h->eigr_src) return CUW_OK;
   h->eigr_src = nullptr;
-  dim3 grid(std::min(ceil_div(h->d.ngl, 256), 64), h->d.nat);
-  k_eigr<<<grid, 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz, r_dev, h->d.ngl, h->d.nat, h->g.eigr);
-  CUW_LAUNCH_CHECK("k_eigr");
-  if (h->mixed()) CUW_RET(tc_pro_table(h));
-  else if (h->npro > 0) {
+  if (!h->mixed() && h->npro > 0) {
+    // FP64 handles: the expanded projector table straight from the positions
+    // (the contractions read only the table, so EIGR is not formed)
     if (!h->g.prox) {
       if (h->capturing) return h->fail(CUW_ERR_STATE, "projector table allocated during graph capture");
       h->touch();
       CUW_TRY(cudaMalloc(&h->g.prox, sizeof(double2) * (size_t)h->ldg * h->npro));
     }
-    k_pro_f64<<<dim3(std::min(ceil_div(h->ldg, 256), 64), h->npro), 256, 0, h->stream>>>(
-        h->d.ngl, h->ldg, h->npro, h->g.pdesc, h->g.ylm, h->g.pro, h->g.eigr, h->g.prox);
-    CUW_LAUNCH_CHECK("k_pro_f64");
+    const Device& g = h->g;
+    k_pro_f64_direct<<<dim3(ceil_div(h->ldg, 256), h->d.nat), 256, 0, h->stream>>>(
+        h->d.ngl, h->ldg, g.gx, g.gy, g.gz, r_dev, g.t_ipro0, g.t_nlmn, g.pdesc, g.ylm, g.pro, g.prox);
+    CUW_LAUNCH_CHECK("k_pro_f64_direct");
+  } else {
+    dim3 grid(std::min(ceil_div(h->d.ngl, 256), 64), h->d.nat);
+    k_eigr<<<grid, 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz, r_dev, h->d.ngl, h->d.nat, h->g.eigr);
+    CUW_LAUNCH_CHECK("k_eigr");
+    if (h->mixed()) CUW_RET(tc_pro_table(h));
   }
   if (pos) h->eigr_src = r_dev;
   return CUW_OK;
