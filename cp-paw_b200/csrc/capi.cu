@@ -365,6 +365,11 @@ using namespace cuw;
 // extern "C" entry points
 // ---------------------------------------------------------------------------
 #define H(hp) Handle* h = reinterpret_cast<Handle*>(hp)
+#define CUW_BATCH_TRY(expr)                                                                 \
+  do {                                                                                      \
+    cudaError_t e__ = (expr);                                                               \
+    if (e__ != cudaSuccess) return b->fail(CUW_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
 #define NEED(cond, code, msg) \
   do {                        \
     if (!(cond)) return h->fail(code, msg); \
@@ -1195,6 +1200,269 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
       out[7] = hs[7];
     }
   }
+  return CUW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: many wave-function sets advanced by one CUDA graph launch.  The
+// graph holds two CP steps of every set (after two steps PSI0/PSIM are back in
+// their buffers, so the same graph serves every later pair), each set's
+// launches on its own stream, forked from and joined to the batch's stream:
+// the sets' kernels run concurrently on the device and the host issues one
+// launch per pair of steps for all of them.  Every set's launches and their
+// order are those of cuwaves_cp_step, so the results are bit-identical to
+// stepping each set alone.
+// ---------------------------------------------------------------------------
+struct cuw_batch {
+  std::vector<Handle*> hs;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t exec = nullptr;
+  struct Key {
+    const void* k[6];
+    long long epoch;
+    int rlamm;
+  };
+  std::vector<Key> keys;                  // host state of each set the graph was captured for
+  std::vector<const double*> eigr_after;  // EIGR source buffer of each set after a pair of steps
+  std::vector<long long> launches;        // kernels per set in the graph
+  int move = -1, max_iter = 0;
+  double eps = 0.0;
+  double* res = nullptr;  // device: [set][step][8] the outputs of cuwaves_cp_step (sc[0..7])
+  int* st = nullptr;      // device: [set][step][2] orthogonalisation status and iterations
+  std::string err;
+  long long replays = 0;
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+static cuw_batch::Key batch_key(const Handle* h) {
+  cuw_batch::Key k;
+  const Device& g = h->g;
+  const void* v[6] = {g.psi0, g.psim, g.r0, g.rm, g.rp, h->eigr_src};
+  std::memcpy(k.k, v, sizeof(v));
+  k.epoch = h->epoch;
+  k.rlamm = h->have_rlamm ? 1 : 0;
+  return k;
+}
+
+// Captures two steps of every set into b->exec; on failure every set's host
+// state is as before and nothing is enqueued.
+static int batch_capture(cuw_batch* b, int move, int max_iter, double eps) {
+  const int n = (int)b->hs.size();
+  std::vector<Device> saved(n);
+  std::vector<const double*> eigr_saved(n);
+  std::vector<long long> l0(n);
+  std::vector<cuw_batch::Key> keys(n);
+  for (int i = 0; i < n; ++i) {
+    Handle* h = b->hs[i];
+    saved[i] = h->g;
+    eigr_saved[i] = h->eigr_src;
+    l0[i] = h->launches;
+    keys[i] = batch_key(h);
+  }
+  if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return b->fail(CUW_ERR_CUDA, "batch: stream capture could not start");
+  }
+  int rc = CUW_OK;
+  cudaError_t e = cudaEventRecord(b->fork, b->stream);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    e = cudaStreamWaitEvent(b->hs[i]->stream, b->fork, 0);
+    b->hs[i]->capturing = true;
+  }
+  for (int s = 0; s < 2 && e == cudaSuccess && rc == CUW_OK; ++s)
+    for (int i = 0; i < n && rc == CUW_OK; ++i) {
+      Handle* h = b->hs[i];
+      h->nev = 0;
+      rc = step_body(h, move, max_iter, eps);
+      if (rc != CUW_OK) {
+        b->err = h->err;
+        break;
+      }
+      const size_t slot = (size_t)i * 2 + s;
+      e = cudaMemcpyAsync(b->res + slot * 8, h->g.scal, sizeof(double) * 8, cudaMemcpyDeviceToDevice, h->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->st + slot * 2, h->g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToDevice, h->stream);
+      if (e != cudaSuccess) rc = CUW_ERR_CUDA;
+    }
+  for (int i = 0; i < n; ++i) {
+    Handle* h = b->hs[i];
+    if (cudaEventRecord(b->join[i], h->stream) == cudaSuccess) cudaStreamWaitEvent(b->stream, b->join[i], 0);
+    h->capturing = false;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (rc == CUW_OK && e == cudaSuccess && ee == cudaSuccess && graph) ee = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (rc != CUW_OK || e != cudaSuccess || ee != cudaSuccess || !exec) {
+    cudaGetLastError();
+    for (int i = 0; i < n; ++i) {
+      Handle* h = b->hs[i];
+      h->g = saved[i];
+      h->eigr_src = eigr_saved[i];
+      h->launches = l0[i];
+      h->err.clear();
+    }
+    return b->fail(rc != CUW_OK ? rc : CUW_ERR_CUDA,
+                   "batch: the steps could not be captured" + (b->err.empty() ? std::string() : ": " + b->err));
+  }
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = exec;
+  b->keys = keys;
+  b->eigr_after.resize(n);
+  b->launches.resize(n);
+  for (int i = 0; i < n; ++i) {
+    b->eigr_after[i] = b->hs[i]->eigr_src;
+    b->launches[i] = b->hs[i]->launches - l0[i];
+  }
+  b->move = move;
+  b->max_iter = max_iter;
+  b->eps = eps;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_batch_create(cuw_handle* const* handles, int n, cuw_batch** out) {
+  if (!handles || n <= 0 || !out) return CUW_ERR_ARG;
+  *out = nullptr;
+  cuw_batch* b = new cuw_batch();
+  for (int i = 0; i < n; ++i) {
+    Handle* h = reinterpret_cast<Handle*>(handles[i]);
+    if (!h) {
+      delete b;
+      return CUW_ERR_ARG;
+    }
+    for (Handle* o : b->hs)
+      if (o == h) {
+        delete b;
+        return CUW_ERR_ARG;  // a set may appear once
+      }
+    b->hs.push_back(h);
+  }
+  int dev = b->hs[0]->device;
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess;
+  b->join.assign(n, nullptr);
+  for (int i = 0; i < n && ok; ++i) {
+    ok = b->hs[i]->device == dev && cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+  }
+  ok = ok && cudaMalloc(&b->res, sizeof(double) * 16 * (size_t)n) == cudaSuccess &&
+       cudaMalloc(&b->st, sizeof(int) * 4 * (size_t)n) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    cuwaves_batch_destroy(b);
+    return CUW_ERR_CUDA;
+  }
+  *out = b;
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_batch_step(cuw_batch* b, int move_atoms, const double* const* mass, int max_iter, double eps,
+                                  double* out) {
+  if (!b) return CUW_ERR_ARG;
+  const int n = (int)b->hs.size();
+  if (move_atoms && !mass) return b->fail(CUW_ERR_ARG, "masses required to move atoms");
+  for (int i = 0; i < n; ++i) {
+    Handle* h = b->hs[i];
+    if (!(h->have_gset && h->have_v && h->have_dh && h->have_do))
+      return b->fail(CUW_ERR_STATE, "batch: set " + std::to_string(i) + ": inputs not loaded");
+    if (!(h->have_u && h->have_rlamm))
+      return b->fail(CUW_ERR_STATE, "batch: set " + std::to_string(i) + ": take one cuwaves_cp_step first");
+    if (h->timing || h->async) return b->fail(CUW_ERR_STATE, "batch: timing or asynchronous mode is on");
+    if (move_atoms && !mass[i]) return b->fail(CUW_ERR_ARG, "batch: masses of set " + std::to_string(i));
+  }
+  for (int i = 0; i < n; ++i) {
+    Handle* h = b->hs[i];
+    CUW_BATCH_TRY(cudaStreamSynchronize(h->stream));
+    if (move_atoms)
+      CUW_BATCH_TRY(cudaMemcpyAsync(h->g.mass, mass[i], sizeof(double) * h->d.nat, cudaMemcpyHostToDevice, b->stream));
+  }
+  bool same = b->exec && b->move == move_atoms && b->max_iter == max_iter && b->eps == eps &&
+              (int)b->keys.size() == n;
+  for (int i = 0; i < n && same; ++i) {
+    const cuw_batch::Key k = batch_key(b->hs[i]);
+    same = std::memcmp(k.k, b->keys[i].k, sizeof(k.k)) == 0 && k.epoch == b->keys[i].epoch &&
+           k.rlamm == b->keys[i].rlamm;
+  }
+  if (same) {
+    CUW_BATCH_TRY(cudaGraphLaunch(b->exec, b->stream));
+    for (int i = 0; i < n; ++i) {
+      Handle* h = b->hs[i];
+      h->eigr_src = b->eigr_after[i];  // the PSI0/PSIM swaps of two steps cancel
+      h->launches += b->launches[i];
+      h->graph_replays += 2;
+    }
+    ++b->replays;
+  } else {
+    CUW_BATCH_TRY(cudaStreamSynchronize(b->stream));
+    const int rc = batch_capture(b, move_atoms, max_iter, eps);
+    if (rc != CUW_OK) return rc;
+    CUW_BATCH_TRY(cudaGraphLaunch(b->exec, b->stream));
+  }
+  for (Handle* h : b->hs) {
+    h->have_hpsi = false;
+    h->have_opsi = false;
+    h->have_rlamm = true;
+  }
+  std::vector<double> res((size_t)16 * n);
+  std::vector<int> st((size_t)4 * n);
+  CUW_BATCH_TRY(cudaMemcpyAsync(res.data(), b->res, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, b->stream));
+  CUW_BATCH_TRY(cudaMemcpyAsync(st.data(), b->st, sizeof(int) * st.size(), cudaMemcpyDeviceToHost, b->stream));
+  CUW_BATCH_TRY(cudaStreamSynchronize(b->stream));
+  int rc = CUW_OK;
+  for (int i = 0; i < n; ++i) {
+    Handle* h = b->hs[i];
+    int r = h->tc_status();
+    for (int s = 0; s < 2; ++s) {
+      const size_t slot = (size_t)i * 2 + s;
+      int iters = 0;
+      if (r == CUW_OK) r = ortho_result(h, &st[slot * 2], &iters);
+      if (out) {
+        const double* hs = &res[slot * 8];
+        double* o = out + slot * 8;
+        o[0] = hs[1];
+        o[1] = hs[0];
+        o[2] = 0.5 * (hs[2] + hs[3]);
+        o[3] = hs[4];
+        o[4] = iters;
+        o[5] = o[6] = o[7] = 0.0;
+        if (h->scf) {
+          o[0] = hs[1] - hs[7] + hs[5] + hs[6];
+          o[5] = hs[5];
+          o[6] = hs[6];
+          o[7] = hs[7];
+        }
+      }
+    }
+    if (r != CUW_OK && rc == CUW_OK) {
+      rc = r;
+      b->err = "set " + std::to_string(i) + ": " + h->err;
+    }
+  }
+  return rc;
+}
+
+extern "C" int cuwaves_batch_error(const cuw_batch* b, char* buf, int len) {
+  if (!b || !buf || len <= 0) return CUW_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", b->err.c_str());
+  return CUW_OK;
+}
+
+extern "C" int cuwaves_batch_destroy(cuw_batch* b) {
+  if (!b) return CUW_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (cudaEvent_t e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->res) cudaFree(b->res);
+  if (b->st) cudaFree(b->st);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
   return CUW_OK;
 }
 

@@ -101,6 +101,11 @@ OPTIONAL = {
     "get_graph_stats": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "autotune": [_P, _D, C.c_int],
     "tc_gemm_check": [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P],
+    # batches of sets stepped by one graph launch (no handle argument)
+    "batch_create": [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)],
+    "batch_step": [_P, C.c_int, C.POINTER(_D), C.c_int, C.c_double, _D],
+    "batch_error": [_P, C.c_char_p, C.c_int],
+    "batch_destroy": [_P],
     # device-pointer variant without allocation (no handle)
     "projections_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, _P, _P],
     "get_atoms": [_P, _D, _D, _D],
@@ -479,6 +484,45 @@ class Waves:
             self.gramschmidt(CUW_PSIM, r)
         self.projections()
         return self
+
+
+class Batch:
+    """Several wave-function sets advanced together by one CUDA graph launch
+    (cuwaves_batch_*): step() advances every set by two CP steps."""
+
+    def __init__(self, sets):
+        self.sets = list(sets)
+        self._f = self.sets[0]._f
+        arr = (C.c_void_p * len(self.sets))(*[w.h for w in self.sets])
+        b = C.c_void_p()
+        rc = self._f["batch_create"](arr, len(self.sets), C.byref(b))
+        if rc:
+            raise WavesError(rc, "batch_create", "")
+        self.b = b
+        self._masses = [np.ascontiguousarray(w.inp["masses"], dtype=np.float64) for w in self.sets]
+        self._mp = (_D * len(self.sets))(*[_dptr(m) for m in self._masses])
+
+    def step(self, move_atoms: bool = False, max_iter: int = 200, eps: float = 1e-8) -> np.ndarray:
+        """Two CP steps of every set; returns out[set, step, 8] as cuwaves_cp_step."""
+        out = np.zeros((len(self.sets), 2, 8))
+        rc = self._f["batch_step"](self.b, int(move_atoms), self._mp if move_atoms else None, max_iter, eps,
+                                   _dptr(out))
+        if rc:
+            buf = C.create_string_buffer(512)
+            self._f["batch_error"](self.b, buf, 512)
+            raise WavesError(rc, "batch_step", buf.value.decode(errors="replace"))
+        return out
+
+    def close(self):
+        if getattr(self, "b", None):
+            self._f["batch_destroy"](self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))

@@ -292,6 +292,31 @@ int cuwaves_server_stats(cuw_server* s, double* out, int n);
 /* Finishes the steps in flight, releases every set and stops the workers. */
 int cuwaves_server_destroy(cuw_server* s);
 
+/* Batches (no counterpart in the reference, which steps one set per program;
+ * its loops over sets, src/paw_waves1.f90:252-276 WAVES_SELECTWV, run them one
+ * after another): many sets, of any sizes, advanced together by one CUDA
+ * graph launch.  cuwaves_batch_step advances every set by TWO CP steps
+ * (cuwaves_cp_step with the same arguments; after two steps PSI0 and PSIM are
+ * back in their buffers, so one captured graph serves every later pair): each
+ * set's launches stay on its own stream, forked from and joined to the batch's
+ * stream, so the sets run concurrently on the device; the graph is captured
+ * at the first call and again whenever a set's host-side state or inputs
+ * changed.  Results are bit-identical to stepping each set alone.  Every set
+ * must have taken one cuwaves_cp_step first (the eigenbasis and Lagrange
+ * history exist), with timing and asynchronous mode off.  mass: one pointer
+ * (NAT masses) per set, or NULL with move_atoms = 0.  out (may be NULL):
+ * out[(i*2 + s)*8 + k] = output k of step s of set i, as cuwaves_cp_step.
+ * The call returns when both steps of every set are done; on a failed
+ * orthogonalisation it returns that set's status (cuwaves_batch_error tells
+ * which set).  A set may belong to one batch at a time and must not be used
+ * by another thread during cuwaves_batch_step. */
+typedef struct cuw_batch cuw_batch;
+int cuwaves_batch_create(cuw_handle* const* handles, int n, cuw_batch** out);
+int cuwaves_batch_step(cuw_batch* b, int move_atoms, const double* const* mass, int max_iter, double eps,
+                       double* out);
+int cuwaves_batch_error(const cuw_batch* b, char* buf, int len);
+int cuwaves_batch_destroy(cuw_batch* b);
+
 /* Measurement hooks (no counterpart in the reference, whose TIMING$CLOCKON/OFF
  * clocks, src/paw_timing.f90:121-192, play this role on the CPU).
  * cuwaves_set_timing(h, 1) records CUDA events on the handle's stream at the
