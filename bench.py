@@ -518,22 +518,35 @@ def run_serving(args):
 
 
 def run_batched(args):
-    """Batched workloads, mixed precision.
-    (1) Si64: `batched_si64` independent Si64 cells (different seeded
-        displacements), resident together, each stepped by its own host thread
-        on its own stream; aggregate CP steps/s after set-up and warm-up
-        (device-resident steady state).
-    (2) 64 independent small systems of uneven size (bulk Si2-Si16, Si2 and
-        H2O molecules in 20-bohr boxes) through the server, all admitted at
-        once, set-up included, against the same systems one at a time."""
-    import threading
-
-    import torch
+    """Batched workloads, mixed precision (and FP64 for the Si64 cells), every
+    batch advanced by one CUDA graph launch per two CP steps of all its sets
+    (cuwaves_batch_step: the sets' kernels run concurrently on the device, the
+    host issues one launch and reads the energies back per call):
+    (1) `batched_si64` independent Si64 cells (different seeded displacements);
+    (2) 64 independent small systems of uneven size: bulk Si2-Si16 cells and
+        Si2 / H2O molecules in 20-bohr boxes, 4-32 bands, grids 18^3 to 36^3
+        (the smallest holding each wave-function sphere), 30 Ry;
+        beside the same systems stepped one at a time.
+    Aggregate CP steps/s between synchronised start and end of the timed
+    batch calls (after warm-up calls that capture the graphs)."""
     import cuwaves
     from cuwaves import systems
-    from cuwaves.serve import Server
+
+    def timed_batch(ws, calls):
+        for w in ws:
+            w.cp_step(move_atoms=True)  # eigenbasis and Lagrange history
+        batch = cuwaves.Batch(ws)
+        for _ in range(max(2, args.warmup)):
+            batch.step(move_atoms=True)
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            batch.step(move_atoms=True)
+        dt = time.perf_counter() - t0
+        batch.close()
+        return len(ws) * 2 * calls / dt
 
     res = {}
+    calls = max(1, args.steps // 2)
     for prec, tag in ((cuwaves.CUW_PREC_MIXED, "mixed"), (cuwaves.CUW_PREC_FP64, "fp64")):
         ws = []
         for i in range(args.batched_si64):
@@ -542,58 +555,31 @@ def run_batched(args):
             ws.append(cuwaves.open_waves(inp, precision=prec).setup().initialize())
             if not args.no_autotune:
                 ws[-1].autotune()
-        for w in ws:
-            for _ in range(args.warmup):
-                w.cp_step(move_atoms=True)
-        bar = threading.Barrier(len(ws) + 1)
-
-        def body(w):
-            bar.wait()
-            for _ in range(args.steps):
-                w.cp_step(move_atoms=True)
-
-        th = [threading.Thread(target=body, args=(w,)) for w in ws]
-        for t in th:
-            t.start()
-        torch.cuda.synchronize()
-        bar.wait()
-        t0 = time.perf_counter()
-        for t in th:
-            t.join()
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
+        res[tag] = timed_batch(ws, calls)
         for w in ws:
             w.close()
-        res[tag] = len(ws) * args.steps / dt
-    inps = [systems.build_inputs(s) for s in systems.batched_mix(64)]
-    k = args.batched_steps
-    small = {}
-    for workers in (1, args.batched_workers):
-        srv = Server(hbm_budget=64 << 30, workers=workers)
-        for inp in inps[:4]:  # warm-up
-            srv.submit(inp, nsteps=1, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
-        srv.wait_all()
-        srv.close()
-        srv = Server(hbm_budget=64 << 30, workers=workers)
-        t0 = time.perf_counter()
-        for inp in inps:
-            srv.submit(inp, nsteps=k, move_atoms=True, precision=cuwaves.CUW_PREC_MIXED, borrow=True)
-        srv.wait_all()
-        dt = time.perf_counter() - t0
-        st = srv.stats()
-        srv.close()
-        small[workers] = (len(inps) * k / dt, st)
-    vb, stb = small[args.batched_workers]
+    inps = [systems.build_inputs(s) for s in systems.config_batch_mix(64)]
+    ws = [cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup().initialize() for inp in inps]
+    small = timed_batch(ws, args.batched_steps // 2)
+    # the same sets one at a time (each step a graph replay of its own)
+    for w in ws:
+        w.cp_step(move_atoms=True)
+    t0 = time.perf_counter()
+    nsteps = max(2, args.batched_steps // 2)
+    for w in ws:
+        for _ in range(nsteps):
+            w.cp_step(move_atoms=True)
+    alone = len(ws) * nsteps / (time.perf_counter() - t0)
+    for w in ws:
+        w.close()
     return {"value": round(res["mixed"], 2), "unit": "CP steps/s (all Si64 cells)", "precision": "mixed",
             "si64_cells": args.batched_si64, "fp64_same_batch": round(res["fp64"], 2),
-            "timing": "wall clock between a host barrier and the last thread's last step, with device "
-                      "synchronisation on both sides; every step ends in a host read of its energies",
-            "small_systems": {"value": round(vb, 2), "unit": "CP steps/s (all systems, set-up included)",
-                              "systems": len(inps), "steps_per_system": k, "workers": args.batched_workers,
-                              "one_at_a_time_value": round(small[1][0], 2),
-                              "mean_admitted_sets": round(stb["mean_admitted"], 2), "failed": int(stb["failed"]),
-                              "sizes": "Si2-Si16 bulk (4-32 bands, 28^3 / 28x28x56 grids), Si2 and H2O molecules "
-                                       "in 20-bohr boxes (56^3)"}}
+            "timing": "one CUDA graph launch per two CP steps of every set (cuwaves_batch_step), synchronised; "
+                      "wall clock over the timed calls after graph capture and warm-up",
+            "small_systems": {"value": round(small, 2), "unit": "CP steps/s (all systems)", "systems": len(ws),
+                              "one_at_a_time_value": round(alone, 2), "precision": "mixed",
+                              "sizes": "Si2-Si16 bulk (4-32 bands, 18^3 and 18x18x36 grids), Si2 and H2O molecules "
+                                       "in 20-bohr boxes (4 bands, 36^3), 30 Ry"}}
 
 
 def emit_cuda(args, res, world):
@@ -722,7 +708,7 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=int, default=48)
     ap.add_argument("--serve-seconds", type=float, default=25.0, help="arrival window of the sustained stream")
-    ap.add_argument("--batched-steps", type=int, default=10)
+    ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--batched-workers", type=int, default=16)
     ap.add_argument("--batched-si64", type=int, default=8)
     args = ap.parse_args()

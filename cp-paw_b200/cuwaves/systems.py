@@ -458,6 +458,37 @@ def batched_mix(count: int = 64, seed: int = 11) -> List[System]:
     return out
 
 
+# Batched workload of the benchmark configuration: 64 systems of uneven size,
+# bulk Si2..Si16 cells and Si2 / H2O molecules in 20-bohr boxes, 4-32 bands,
+# 30/60 Ry, each on the smallest FFT grid (16 to 40 points per axis) that
+# holds its wave-function sphere without aliasing.
+FFT_LENGTHS = (16, 18, 20, 24, 28, 30, 32, 36, 40)
+
+
+def psi_grid(sys: System):
+    gbas, _ = gbass(sys.rbas)
+    ig = get_ig(gbas, sys.epw_psi)
+    out = []
+    for d in range(3):
+        m = int(np.abs(ig[:, d]).max())
+        out.append(next(n for n in FFT_LENGTHS if 2 * m < n))
+    return tuple(out)
+
+
+def config_batch_mix(count: int = 64, seed: int = 11) -> List[System]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        k = int(rng.integers(0, 10))
+        if k < 8:
+            sy = si_small(int(2 * (k + 1)), seed=100 + i)  # Si2..Si16: 4..32 bands
+        else:
+            sy = molecule_box("Si2" if k == 8 else "H2O", box=20.0, seed=100 + i)
+        sy.grid = psi_grid(sy)
+        out.append(sy)
+    return out
+
+
 # Serving workload: perturbed bulk Si_n (n in 8..128) and water clusters of
 # 1-16 molecules, 30-40 Ry.
 SERVING_SI = {8: (1, 1, 1), 16: (1, 1, 2), 32: (1, 2, 2), 64: (2, 2, 2), 128: (2, 2, 4)}
