@@ -542,6 +542,33 @@ extern "C" int cuwaves_destroy(cuw_handle* hp) {
   return CUW_OK;
 }
 
+namespace cuw {
+// Returns a handle to the state of a freshly created one for the same G set
+// (the serving runtime reuses handles of finished requests): no eigenbasis,
+// no Lagrange history, no H|psi> or O|psi>, no EIGR, no step graphs.  Buffers
+// keep stale data, which every later call writes before it reads.
+int handle_recycle(cuw_handle* hp) {
+  Handle* h = reinterpret_cast<Handle*>(hp);
+  if (!h) return CUW_ERR_ARG;
+  CUW_TRY(cudaStreamSynchronize(h->stream));
+  // the Lagrange multipliers start from zero as in a new handle (the first
+  // ORTHO_X guess and the first forces read RLAM0)
+  const size_t nn = (size_t)h->d.nb * h->d.nb;
+  CUW_TRY(cudaMemset(h->g.rlam0, 0, sizeof(double2) * nn));
+  CUW_TRY(cudaMemset(h->g.rlamm, 0, sizeof(double2) * nn));
+  CUW_TRY(cudaMemset(h->g.lam, 0, sizeof(double) * nn));
+  h->have_hpsi = h->have_opsi = h->have_u = h->have_rlamm = false;
+  h->eigr_src = nullptr;
+  h->timing = false;
+  h->nev = 0;
+  h->scf = false;
+  h->drop_graphs();
+  h->touch();
+  h->err.clear();
+  return CUW_OK;
+}
+}  // namespace cuw
+
 extern "C" int cuwaves_last_error(const cuw_handle* hp, char* buf, int len) {
   if (!buf || len <= 0) return CUW_ERR_ARG;
   const Handle* h = reinterpret_cast<const Handle*>(hp);

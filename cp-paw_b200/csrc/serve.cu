@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <deque>
@@ -26,6 +27,10 @@
 #include <vector>
 
 #include "../../include/cuwaves.h"
+
+namespace cuw {
+int handle_recycle(cuw_handle* h);  // capi.cu
+}
 
 namespace {
 
@@ -49,6 +54,9 @@ struct Job {
   double gweight = 0.0, delt = 0.0, annee = 0.0;
   int lmnxx = 0, lnxx = 0, nsteps = 0, done_steps = 0;
   cuw_handle* h = nullptr;
+  bool reused = false;        // h came from the pool: same G set, set-up without cuwaves_set_gset
+  bool ready = false;         // set-up done
+  uint64_t gkey = 0;          // identity of the G set and sizes (pool key)
   size_t bytes = 0;
   bool busy = false, finished = false;
   int status = CUW_OK;
@@ -56,6 +64,29 @@ struct Job {
   double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> force;
   Clock::time_point t_submit, t_done;
+};
+
+// 64-bit hash of byte arrays, word by word (a key for pooled handles whose
+// G set and sizes equal a new request's)
+struct Hash64 {
+  uint64_t h = 0x9E3779B97F4A7C15ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+      uint64_t w;
+      std::memcpy(&w, b + i, 8);
+      mix(w);
+    }
+    uint64_t w = 0;
+    std::memcpy(&w, b + i, n - i);
+    mix(w ^ ((uint64_t)n << 56));
+  }
+  void mix(uint64_t w) {
+    h ^= w + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+  }
 };
 
 // projectors of the set (sum over atoms of 2l+1 per radial function)
@@ -111,6 +142,34 @@ struct cuw_server {
   double busy_integral = 0.0;  // time-weighted number of admitted systems
   Clock::time_point t_mark;
   std::vector<std::thread> workers;
+  // handles of finished requests, kept for requests of the same G set and
+  // sizes (no device allocation at their set-up); their bytes stay in in_use
+  std::multimap<uint64_t, std::pair<cuw_handle*, size_t>> pool;
+  std::deque<std::pair<uint64_t, cuw_handle*>> pool_order;  // oldest first
+  long long reused = 0;
+
+  void pool_drop(cuw_handle* h) {
+    for (auto it = pool_order.begin(); it != pool_order.end(); ++it)
+      if (it->second == h) {
+        pool_order.erase(it);
+        break;
+      }
+  }
+  // destroys the oldest pooled handle (false when the pool is empty)
+  bool evict_one() {
+    if (pool_order.empty()) return false;
+    const auto [key, h] = pool_order.front();
+    pool_order.pop_front();
+    auto r = pool.equal_range(key);
+    for (auto it = r.first; it != r.second; ++it)
+      if (it->second.first == h) {
+        in_use -= it->second.second;
+        pool.erase(it);
+        break;
+      }
+    cuwaves_destroy(h);
+    return true;
+  }
 
   void account(Clock::time_point now) {
     busy_integral += std::chrono::duration<double>(now - t_mark).count() * (double)active.size();
@@ -121,10 +180,24 @@ struct cuw_server {
   void admit() {
     while (!queue.empty()) {
       Job* j = queue.front();
-      if (in_use + j->bytes > budget || (int)active.size() >= max_active) break;
+      if ((int)active.size() >= max_active) break;
+      auto hit = pool.find(j->gkey);
+      if (hit != pool.end()) {
+        // a pooled handle of the same G set: its memory is already counted
+        j->h = hit->second.first;
+        j->bytes = hit->second.second;
+        j->reused = true;
+        pool_drop(j->h);
+        pool.erase(hit);
+        ++reused;
+      } else {
+        while (in_use + j->bytes > budget && evict_one()) {
+        }
+        if (in_use + j->bytes > budget) break;
+        in_use += j->bytes;
+      }
       queue.pop_front();
       account(Clock::now());
-      in_use += j->bytes;
       peak = std::max(peak, in_use);
       active.push_back(j);
     }
@@ -152,26 +225,39 @@ struct cuw_server {
   // one unit of work of job j, outside the lock
   static bool run_unit(Job* j) {
     int rc;
-    if (!j->h) {
+    if (!j->ready) {
       const Inputs& in = j->in;
-      j->dims.isp = in.isp;
-      if ((rc = cuwaves_create(&j->dims, &j->h)) != CUW_OK) {
-        j->h = nullptr;
-        fail(j, rc, "create");
-        return true;
+      j->ready = true;
+      if (j->h) {
+        // a pooled handle of the same G set: back to the state of a fresh one
+        if ((rc = cuw::handle_recycle(j->h)) != CUW_OK) {
+          fail(j, rc, "recycle");
+          return true;
+        }
+      } else {
+        j->dims.isp = in.isp;
+        if ((rc = cuwaves_create(&j->dims, &j->h)) != CUW_OK) {
+          j->h = nullptr;
+          fail(j, rc, "create");
+          return true;
+        }
+        if ((rc = cuwaves_set_gset(j->h, in.igvec, in.minusg, in.gbas, in.gvec, in.g2, in.pro, in.ylm, in.mpsi,
+                                   nullptr, j->gweight)) != CUW_OK) {
+          fail(j, rc, "set-up");
+          return true;
+        }
       }
       // Step graphs pay for their capture and instantiation (two per set)
       // only over long runs; on the serving mix of 20-step requests they
       // nearly halved the measured capacity (8.3 against 15-17 solves/s).
-      if (j->nsteps < kGraphSteps) cuwaves_set_option(j->h, CUW_OPT_GRAPHS, 0.0);
-      if ((rc = cuwaves_set_gset(j->h, in.igvec, in.minusg, in.gbas, in.gvec, in.g2, in.pro, in.ylm, in.mpsi, nullptr,
-                                 j->gweight)) ||
-          (rc = cuwaves_set_potential(j->h, in.v)) || (rc = cuwaves_set_dh(j->h, j->lmnxx, in.dh)) ||
+      cuwaves_set_option(j->h, CUW_OPT_GRAPHS, j->nsteps < kGraphSteps ? 0.0 : 1.0);
+      // PSIM starts equal to PSI0 (from rest): its Gram-Schmidt would repeat
+      // PSI0's bit for bit, so WAVES$STOP copies it instead
+      if ((rc = cuwaves_set_potential(j->h, in.v)) || (rc = cuwaves_set_dh(j->h, j->lmnxx, in.dh)) ||
           (rc = cuwaves_set_do(j->h, j->lnxx, in.dover)) || (rc = cuwaves_reset_atoms(j->h, in.r0)) ||
           (rc = cuwaves_set_occ(j->h, in.occ)) || (rc = cuwaves_set_dynamics(j->h, j->delt, j->annee)) ||
-          (rc = cuwaves_upload_psi(j->h, CUW_PSI0, in.psi)) || (rc = cuwaves_upload_psi(j->h, CUW_PSIM, in.psi)) ||
-          (rc = cuwaves_gramschmidt(j->h, CUW_PSI0, in.r0)) || (rc = cuwaves_gramschmidt(j->h, CUW_PSIM, in.r0)) ||
-          (rc = cuwaves_projections(j->h))) {
+          (rc = cuwaves_upload_psi(j->h, CUW_PSI0, in.psi)) || (rc = cuwaves_gramschmidt(j->h, CUW_PSI0, in.r0)) ||
+          (rc = cuwaves_stop(j->h)) || (rc = cuwaves_projections(j->h))) {
         fail(j, rc, "set-up");
         return true;
       }
@@ -203,7 +289,7 @@ struct cuw_server {
       j->busy = true;
       lk.unlock();
       const bool done = run_unit(j);
-      if (done && j->h) {
+      if (done && j->h && j->status != CUW_OK) {
         cuwaves_destroy(j->h);
         j->h = nullptr;
       }
@@ -217,7 +303,14 @@ struct cuw_server {
         t_last = now;
         active.erase(std::find(active.begin(), active.end(), j));
         if (rr > 0 && rr >= active.size()) rr = 0;
-        in_use -= j->bytes;
+        if (j->h) {
+          // into the pool; its bytes stay counted until it is evicted or reused
+          pool.emplace(j->gkey, std::make_pair(j->h, j->bytes));
+          pool_order.emplace_back(j->gkey, j->h);
+          j->h = nullptr;
+        } else {
+          in_use -= j->bytes;
+        }
         if (j->status == CUW_OK) {
           ++completed;
           latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - j->t_submit).count());
@@ -333,6 +426,27 @@ extern "C" int cuwaves_server_submit(cuw_server* s, const cuw_request* r, long l
   j->nsteps = r->nsteps;
   j->bytes = estimate_bytes(d, in.isp);
   if (j->bytes > s->budget) return CUW_ERR_NOMEM;  // could never be admitted
+  {
+    // sizes and G set: a pooled handle with the same key serves this request
+    Hash64 hk;
+    cuw_dims dk = d;
+    dk.isp = nullptr;
+    hk.add(&dk, sizeof(dk));
+    hk.add(in.isp, sizeof(int) * nat);
+    hk.add(in.igvec, sizeof(int) * 3 * ngl);
+    hk.add(in.minusg, sizeof(int) * ngl);
+    hk.add(in.gbas, sizeof(double) * 9);
+    hk.add(in.gvec, sizeof(double) * 3 * ngl);
+    hk.add(in.g2, sizeof(double) * ngl);
+    hk.add(in.pro, sizeof(double) * ngl * nbare);
+    hk.add(in.ylm, sizeof(double) * ngl * (size_t)d.lmx);
+    hk.add(in.mpsi, sizeof(double) * ngl);
+    const double gw = r->gweight;
+    const int lx[2] = {r->lmnxx, r->lnxx};
+    hk.add(&gw, sizeof(gw));
+    hk.add(lx, sizeof(lx));
+    j->gkey = hk.h;
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return CUW_ERR_STATE;
   j->id = s->next_id++;
@@ -418,6 +532,7 @@ extern "C" int cuwaves_server_destroy(cuw_server* s) {
   for (auto& t : s->workers) t.join();
   for (Job* j : s->active)
     if (j->h) cuwaves_destroy(j->h);
+  for (auto& kv : s->pool) cuwaves_destroy(kv.second.first);
   delete s;
   return CUW_OK;
 }
