@@ -874,11 +874,27 @@ constexpr int PSZ = RSZ > CSZ ? RSZ : CSZ;
 constexpr size_t kSmemBytes = sizeof(double) * ((size_t)4 * PSZ + 64);
 }  // namespace pnl
 
-// Stages op(M) as the A operand (rows i0.. of the product, all k) or as the B
-// operand (all k, columns j0..) of a product tile into dst.  M is n x n
-// column-major in global memory (n even, so column segments are 16-byte
-// aligned); elements outside n x n are zero.  Returns nothing; the caller
-// synchronises.
+// 16-byte asynchronous copy global -> shared through L2 (cp.async.cg: the
+// source may have been written by another CTA of the cluster in the previous
+// phase); a null source writes zeros.
+__device__ const double2 pnl_zero[1] = {{0.0, 0.0}};
+__device__ __forceinline__ void pnl_cp16(double* dst, const double* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d),
+               "l"(src ? src : reinterpret_cast<const double*>(pnl_zero)), "r"(src ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void pnl_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void pnl_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Issues the copies that stage op(M) as the A operand (rows i0.. of the
+// product, all k) or as the B operand (all k, columns j0..) of a product tile
+// into dst.  M is n x n column-major in global memory (n even, so column
+// segments are 16-byte aligned); elements outside n x n are zero.  Every
+// copy of the panel is in flight before the caller waits for them.
 __device__ __forceinline__ void pnl_stage(const double* __restrict__ M, int n, int off, bool row_panel,
                                           double* __restrict__ dst) {
   using namespace pnl;
@@ -887,17 +903,13 @@ __device__ __forceinline__ void pnl_stage(const double* __restrict__ M, int n, i
     // rows off..off+31 of every column k: 16 double2 per column
     for (int t = tid; t < KN * (T / 2); t += nt) {
       const int k = t / (T / 2), r2 = (t % (T / 2)) * 2;
-      double2 v = make_double2(0.0, 0.0);
-      if (k < n && off + r2 < n) v = __ldcg(reinterpret_cast<const double2*>(M + (size_t)n * k + off + r2));
-      *reinterpret_cast<double2*>(dst + k * PR + r2) = v;
+      pnl_cp16(dst + k * PR + r2, (k < n && off + r2 < n) ? M + (size_t)n * k + off + r2 : nullptr);
     }
   } else {
     // columns off..off+31, every row k: 64 double2 per column
     for (int t = tid; t < T * (KN / 2); t += nt) {
       const int c = t / (KN / 2), k2 = (t % (KN / 2)) * 2;
-      double2 v = make_double2(0.0, 0.0);
-      if (off + c < n && k2 < n) v = __ldcg(reinterpret_cast<const double2*>(M + (size_t)n * (off + c) + k2));
-      *reinterpret_cast<double2*>(dst + c * PC + k2) = v;
+      pnl_cp16(dst + c * PC + k2, (off + c < n && k2 < n) ? M + (size_t)n * (off + c) + k2 : nullptr);
     }
   }
 }
@@ -975,13 +987,22 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
   // one product tile: stage both terms (the second may be absent), multiply
   auto product = [&](const PnlTerm& t1, const PnlTerm* t2, double (&out)[2]) {
     pnl_stage_term(t1, n, i0, j0, sa0, sb0);
-    if (t2) pnl_stage_term(*t2, n, i0, j0, sa1, sb1);
+    pnl_commit();
+    if (t2) {
+      pnl_stage_term(*t2, n, i0, j0, sa1, sb1);
+      pnl_commit();
+      pnl_wait<1>();  // the first term's panels; the second's stay in flight
+    } else {
+      pnl_wait<0>();
+    }
     __syncthreads();
     double acc[2] = {0.0, 0.0}, acc2[2] = {0.0, 0.0};
     pnl_mma(t1, nk4, sa0, sb0, r0, c0, acc, acc2);
     out[0] = acc[0] + acc2[0];
     out[1] = acc[1] + acc2[1];
     if (t2) {
+      pnl_wait<0>();
+      __syncthreads();
       double bcc[2] = {0.0, 0.0}, bcc2[2] = {0.0, 0.0};
       pnl_mma(*t2, nk4, sa1, sb1, r0, c0, bcc, bcc2);
       out[0] += bcc[0] + bcc2[0];
