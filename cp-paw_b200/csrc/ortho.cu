@@ -871,7 +871,9 @@ constexpr int PC = KN + 4;   // column panel stride ([c][k])
 constexpr int RSZ = KN * PR, CSZ = T * PC;  // doubles of one row / column panel
 // two terms, each an A and a B panel of either kind (sized for the larger)
 constexpr int PSZ = RSZ > CSZ ? RSZ : CSZ;
-constexpr size_t kSmemBytes = sizeof(double) * ((size_t)4 * PSZ + 64);
+// four staging panels, the two resident panels of E (row panel at i0, column
+// panel at j0) and the maxima slots
+constexpr size_t kSmemBytes = sizeof(double) * ((size_t)4 * PSZ + RSZ + CSZ + 64);
 }  // namespace pnl
 
 // 16-byte asynchronous copy global -> shared through L2 (cp.async.cg: the
@@ -963,7 +965,9 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
   double* sb0 = sm + PSZ;
   double* sa1 = sm + 2 * PSZ;
   double* sb1 = sm + 3 * PSZ;
-  double* slotmax = sm + 4 * PSZ;  // [2 parities][x: 16 ranks, y: 16 ranks]
+  double* er = sm + 4 * PSZ;       // E rows i0..i0+31 (row panel), resident
+  double* ec = er + RSZ;           // E columns j0..j0+31 (column panel), resident
+  double* slotmax = ec + CSZ;      // [2 parities][x: 16 ranks, y: 16 ranks]
   // this lane's two elements (gi, gj0 + e) of the tile
   const int gi = i0 + r0 + fr, gjb = j0 + c0 + 2 * fk;
   bool ok[2];
@@ -1010,7 +1014,12 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
     }
     __syncthreads();  // the panels are free for the next stage
   };
-  // cluster maxima of (x, y) through the shared-memory slots of parity par
+  // Cluster maxima of (x, y).  Warp 0 reduces the CTA's warps and its lanes
+  // 0..15 store the CTA's pair into slot [par][rank] of every CTA of the
+  // cluster (remote stores, ordered by the barrier's release); after the
+  // barrier every CTA reduces its own 16 slots.  A slot of parity par is
+  // written again two calls later, after a barrier that every CTA reaches
+  // only once it has read it.
   __shared__ double red[64];
   auto cmax2 = [&](double x, double y, int par, double& gx, double& gy) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -1022,18 +1031,21 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
       red[32 + warp] = y;
     }
     __syncthreads();
-    if (tid == 0) {
-      double bx = red[0], by = red[32];
-      for (int w = 1; w < nt / 32; ++w) {
-        bx = fmax(bx, red[w]);
-        by = fmax(by, red[32 + w]);
+    if (warp == 0) {
+      const int nw = nt / 32;
+      double bx = lane < nw ? red[lane] : 0.0, by = lane < nw ? red[32 + lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) {
+        bx = fmax(bx, __shfl_xor_sync(0xffffffffu, bx, o));
+        by = fmax(by, __shfl_xor_sync(0xffffffffu, by, o));
       }
-      slotmax[par * 32 + rank] = bx;
-      slotmax[par * 32 + 16 + rank] = by;
+      if (lane < 16) {
+        double* rs = cl.map_shared_rank(slotmax, lane);
+        rs[par * 32 + rank] = bx;
+        rs[par * 32 + 16 + rank] = by;
+      }
     }
     cl.sync();
-    const double* rs = cl.map_shared_rank(slotmax, lane & 15);
-    double vx = rs[par * 32 + (lane & 15)], vy = rs[par * 32 + 16 + (lane & 15)];
+    double vx = slotmax[par * 32 + (lane & 15)], vy = slotmax[par * 32 + 16 + (lane & 15)];
     for (int o = 8; o > 0; o >>= 1) {
       vx = fmax(vx, __shfl_xor_sync(0xffffffffu, vx, o));
       vy = fmax(vy, __shfl_xor_sync(0xffffffffu, vy, o));
@@ -1041,9 +1053,32 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
     gx = vx;
     gy = vy;
   };
+  // E X + X E for a Lyapunov sweep: the E panels are resident, the X panels
+  // staged (both in flight before the first multiply)
+  auto sweep_product = [&](const double* x, double (&out)[2]) {
+    pnl_stage(x, n, j0, false, sb0);  // X columns j0.. (B of E X)
+    pnl_commit();
+    pnl_stage(x, n, i0, true, sa1);   // X rows i0.. (A of X E)
+    pnl_commit();
+    pnl_wait<1>();
+    __syncthreads();
+    double acc[2] = {0.0, 0.0}, acc2[2] = {0.0, 0.0};
+    pnl_mma({a.emat, false, x, false}, nk4, er, sb0, r0, c0, acc, acc2);
+    pnl_wait<0>();
+    __syncthreads();
+    pnl_mma({x, false, a.emat, false}, nk4, sa1, ec, r0, c0, acc, acc2);
+    out[0] = acc[0] + acc2[0];
+    out[1] = acc[1] + acc2[1];
+    __syncthreads();  // the staged panels are free for the next stage
+  };
+  if (a.use_e) {
+    pnl_stage(a.emat, n, i0, true, er);
+    pnl_stage(a.emat, n, j0, false, ec);
+    pnl_commit();  // waited for with the first product's copies
+  }
   int status = CUW_ERR_NOT_CONVERGED, iters = a.max_iter;
   double rho_known = 0.0;
-  int par = 0;
+  int par = 0, sweeps = 0;
   for (int iter = 1; iter <= a.max_iter; ++iter) {
     double v[2];
     // HAUX = CHICHI LAMBDA + CHIPSI
@@ -1102,10 +1137,7 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
       const int cheb0 = rho > 0.0 ? 0 : 2;
       for (int it2 = 0; it2 < a.max_inner; ++it2) {
         double ex[2];
-        {
-          const PnlTerm t2{xcur, false, a.emat, false};
-          product({a.emat, false, xcur, false}, &t2, ex);
-        }
+        sweep_product(xcur, ex);
         double dx = 0.0, xm = 0.0, xn[2];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
@@ -1126,7 +1158,7 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
         double* t = xcur;
         xcur = xnext;
         xnext = t;
-        if (rank == 0 && tid == 0) a.inner[0] += 1;
+        ++sweeps;
         const double ratio = gdx / prev;
         if (lyap_stop(gdx, gxm, prev, it2, a.max_inner, a.lyap_tol, fp_failed)) break;
         if (it2 == cheb0) {
@@ -1156,6 +1188,7 @@ __global__ void __launch_bounds__(512, 1) k_ortho_x_pnl(OrthoArgs a) {
   if (rank == 0 && tid == 0) {
     a.status[0] = status;
     a.status[1] = iters;
+    a.inner[0] += sweeps;
   }
   // no CTA leaves while another may still read its shared-memory slots
   cl.sync();
