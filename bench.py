@@ -169,6 +169,47 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
+def tf32_peak_tflops(torch):
+    """TF32 tensor throughput measured here: cuBLAS SGEMM with TF32 allowed
+    (torch.matmul float32, 8192^3), the denominator of the mixed path's
+    tensor-core roofline (MEASURED_PEAKS.json has BF16 only)."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e) * 1e-3)
+        del a, b
+        torch.cuda.empty_cache()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def fft_roofline(t_ms, fft_bytes, peaks, peak_src):
+    """HBM roofline of the V.psi transforms: one full-grid read and write per
+    transform (two transforms per super wave function), over the phase time."""
+    if not t_ms or t_ms <= 0:
+        return None
+    achieved = fft_bytes / (t_ms * 1e-3) / 1e9
+    peak = peaks.get("hbm_gbs")
+    return {"bound": "hbm", "kernels": "k_gtor_plane + k_zcol_v64 + k_rtog_plane", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if peak else None,
+            "peak_source": f"{peak_src} hbm_gbs (of measured)" if peak_src != "fallback" else "fallback",
+            "bytes_per_step": fft_bytes, "traffic": None}
+
+
 def load_ncu_traffic():
     """Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum,
     bytes) of the dominant FP64 kernels, from the committed ncu summaries: a
@@ -345,11 +386,30 @@ def run_mixed(args, local):
     _, l1, _ = w.get_timing()
     phases, nsteps = phase_pass(w, args.steps)
     w.close()
+    ph = {k: v / max(1, nsteps) for k, v in phases.items()}
+    # tensor-core roofline of the dominant tcgen05 phase: the split products
+    # issue three TF32 MMAs (hi*hi + hi*lo + lo*hi) per product of the model
+    fm = flops_model(inp)
+    cand = {"addpro_propagate": (ph.get("addpro_propagate", 0.0), fm["addpro_propagate_flops"], "k_tc_addpro<FUSED>"),
+            "projections": (ph.get("projections", 0.0), fm["projections_flops"], "k_tc_proj")}
+    name = max(cand, key=lambda k: cand[k][0])
+    t_ms, flops, kern = cand[name]
+    p32 = tf32_peak_tflops(torch)
+    tensor = 3.0 * flops / (t_ms * 1e-3) / 1e12 if t_ms > 0 else None
+    peaks, peak_src = measured_peaks()
     return {"value": round(args.steps / (ms * 1e-3), 4), "unit": "steps/s", "ms_per_step": round(ms / args.steps, 4),
             "dtype": "f32 FFT / tf32x3 tensor cores / f64 solve and sums",
             f"max_dE_per_atom_vs_fp64_{nacc}_steps": de, f"max_dF_vs_fp64_{nacc}_steps": df,
             "gpu_launches": l1 - l0, "autotune": tuned,
-            "phase_ms_per_step": {k: round(v / max(1, nsteps), 4) for k, v in phases.items()}}
+            "roofline": {"bound": "tensor", "kernel": kern, "phase": name,
+                         "achieved": round(tensor, 3) if tensor else None, "peak": round(p32, 3), "unit": "TFLOP/s",
+                         "frac": round(tensor / p32, 4) if tensor else None,
+                         "peak_source": "TF32 cuBLAS (torch.matmul float32 8192^3, TF32 allowed) measured in this run",
+                         "tensor_flops_per_step": 3.0 * flops, "model_flops_per_step": flops,
+                         "model_tflops": round(flops / (t_ms * 1e-3) / 1e12, 3) if t_ms > 0 else None,
+                         "traffic": None},
+            "roofline_fft": fft_roofline(ph.get("fft_vpsi"), fm["fft_bytes"] / 2, peaks, peak_src),
+            "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()}}
 
 
 def copy_state(src, dst):
@@ -614,6 +674,7 @@ def emit_cuda(args, res, world):
                      "peak_source": "FP64 cuBLAS DGEMM (torch.matmul float64 8192^3) measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "traffic": traffic, "flops_per_launch": flops},
+        "roofline_fft": fft_roofline(ph.get("fft_vpsi"), fm["fft_bytes"], *measured_peaks()),
         "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()},
         "ortho_solve": res.get("ortho"),
         "step_graphs": res.get("graphs"),

@@ -29,6 +29,15 @@ namespace cuw {
 namespace {
 
 constexpr int kMaxV = 8;   // complex values per thread per stage
+// Grids (NR1, NR2, NR3) with kernels compiled for their lengths: the cubic
+// grids of the benchmark systems, the grids the reference's rule picks for
+// Si8 and Si64 at 60 Ry (28^3, 56^3), and the bulk-Si, water and small-system
+// grids of the serving and batched workloads.
+#define CUW_FFT_GRIDS                                                                              \
+  CUW_FFT_GRID(18, 18, 18) CUW_FFT_GRID(18, 18, 36) CUW_FFT_GRID(24, 24, 24) CUW_FFT_GRID(28, 28, 28) \
+  CUW_FFT_GRID(28, 28, 56) CUW_FFT_GRID(28, 56, 56) CUW_FFT_GRID(32, 32, 32) CUW_FFT_GRID(36, 36, 36) \
+  CUW_FFT_GRID(48, 48, 48) CUW_FFT_GRID(56, 56, 56) CUW_FFT_GRID(56, 56, 110) CUW_FFT_GRID(64, 64, 64) \
+  CUW_FFT_GRID(72, 72, 72) CUW_FFT_GRID(80, 80, 80) CUW_FFT_GRID(96, 96, 96)
 constexpr int kPlaneThreads = 256;
 
 // The transforms are written once for double2 (FP64 path) and float2 (the FP32
@@ -411,7 +420,7 @@ __device__ __forceinline__ int row_of(int i, int nr1) {
 // ---------------------------------------------------------------------------
 // The kernels take the work-grid type C (double2 or float2); the sphere
 // coefficients psi/out stay FP64 and are converted at the gather/scatter.
-template <class C, int N>
+template <class C, int N1, int N2>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
                  const int* __restrict__ plane_g, const int* __restrict__ plane_pos, C* __restrict__ grid, int nzp,
@@ -431,25 +440,26 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x)
     plane[plane_pos[k]] = from_d2<C>(src[plane_g[k]]);
   __syncthreads();
-  xform<N>(plane, a1, nr2, ps, 1, false, tw1, (typename CT<C>::R)1);  // x lines
-  xform<N>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);  // y lines
+  xform<N1>(plane, a1, nr2, ps, 1, false, tw1, (typename CT<C>::R)1);  // x lines
+  xform<N2>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);  // y lines
   C* dst = grid + ((size_t)bl * nzp + p) * npl;
-  for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i + row_of<N>(i, nr1)];
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i + row_of<N1>(i, nr1)];
 }
 
 constexpr int kTX = 16;  // x columns per z-column block, generic kernels
-// x columns per z-column block for transforms of compile-time length N: a
-// whole x row up to 64, which amortises the block's fixed work (twiddles,
-// plane map, barriers) over 4x more columns
-template <int N>
-__host__ __device__ constexpr int tx_of() { return N == 0 ? kTX : (N < 64 ? N : 64); }
+// x columns per z-column block of a grid with compile-time lengths: a whole x
+// row up to 64 (fewer when the z lines are long, so that two blocks of the FP64
+// tile [N3][TX] still fit an SM), which amortises the block's fixed work
+// (twiddles, plane map, barriers) over more columns
+__host__ __device__ constexpr int tx_of(int n1, int n3) {
+  return n1 == 0 ? kTX : (n1 < 64 ? (n3 * n1 * 16 <= 100000 ? n1 : 32) : (n3 * 64 * 16 <= 100000 ? 64 : 56));
+}
 
-template <class C, int N>
+template <class C, int N, int TX>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_zcol_v(C* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot, int nzp, int nr1,
              int nr2, AxisArg a3, const double2* __restrict__ tw3g, double scale) {
   using T = typename CT<C>::R;
-  constexpr int TX = tx_of<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int nr3 = a3.n;
@@ -630,7 +640,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   }
 }
 
-template <class C, int N>
+template <class C, int N1, int N2>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_rtog_plane(const C* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
                  const int* __restrict__ plane_g, const int* __restrict__ plane_pos, double2* __restrict__ out,
@@ -645,12 +655,12 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   C* tw2 = tw1 + nr1;
   const int p = blockIdx.x, bl = blockIdx.y, b = b0 + bl;
   const C* srcp = grid + ((size_t)bl * nzp + p) * npl;
-  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i + row_of<N>(i, nr1)] = srcp[i];
+  for (int i = threadIdx.x; i < npl; i += blockDim.x) plane[i + row_of<N1>(i, nr1)] = srcp[i];
   load_tw(tw1, tw1g, nr1, -1.0);
   load_tw(tw2, tw2g, nr2, -1.0);
   __syncthreads();
-  xform<N>(plane, a2, nr1, 1, pst, false, tw2, (typename CT<C>::R)-1);  // y lines
-  xform<N>(plane, a1, nr2, pst, 1, false, tw1, (typename CT<C>::R)-1);  // x lines
+  xform<N2>(plane, a2, nr1, 1, pst, false, tw2, (typename CT<C>::R)-1);  // y lines
+  xform<N1>(plane, a1, nr2, pst, 1, false, tw1, (typename CT<C>::R)-1);  // x lines
   double2* dst = out + (size_t)ldg * b;
   const double2* ps = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
@@ -740,12 +750,12 @@ bool plan_axis(int n, AxisPlan& p) {
 }  // namespace
 
 // out = FFT_RTOG[ V * FFT_GTOR[psi] ] (+ 1/2 G^2 psi + bucket psi when add_kinetic)
-template <class C, int N>
+template <class C, int N1, int N2, int N3>
 static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
+  constexpr int TX = tx_of(N1, N3);
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
-  const size_t npl = (size_t)nr1 * nr2;
   const int smem_plane = (int)(((size_t)nr2 * plane_stride(nr1) + nr1 + nr2) * sizeof(C));
-  const int smem_z = (int)(((size_t)nr3 * tx_of<N>() + nr3) * sizeof(C));
+  const int smem_z = (int)(((size_t)nr3 * TX + nr3) * sizeof(C));
   const int tp = kPlaneThreads;
   const int tz = kPlaneThreads;
   AxisArg a1 = make_axis(h->ax[0]), a2 = make_axis(h->ax[1]), a3 = make_axis(h->ax[2]);
@@ -754,21 +764,21 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
   C* grid = reinterpret_cast<C*>(g.grid);
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
-    k_gtor_plane<C, N><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
-                                                                      g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
-                                                                      g.tw2);
+    k_gtor_plane<C, N1, N2><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
+                                                                           g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
+                                                                           g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
-    if constexpr (N == 64) {
+    if constexpr (N1 == 64 && N3 == 64) {
       k_zcol_v64<C><<<dim3(nr2, nb), tz, z64_smem_bytes<C>(), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
                                                                                  g.tw3, scale);
       CUW_LAUNCH_CHECK("k_zcol_v64");
     } else {
-      const int nxb = (nr1 + tx_of<N>() - 1) / tx_of<N>();
-      k_zcol_v<C, N><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3,
-                                                                  g.tw3, scale);
+      const int nxb = (nr1 + TX - 1) / TX;
+      k_zcol_v<C, N3, TX><<<dim3(nr2 * nxb, nb), tz, smem_z, h->stream>>>(grid, g.v, g.zslot, h->nzp, nr1, nr2, a3,
+                                                                       g.tw3, scale);
       CUW_LAUNCH_CHECK("k_zcol_v");
     }
-    k_rtog_plane<C, N><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
+    k_rtog_plane<C, N1, N2><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
                                                                       g.plane_pos, out, psi, h->ldg, b0, g.g2,
                                                                       g.bucket, add_kinetic ? 1 : 0, a1, a2,
                                                                       g.tw1, g.tw2);
@@ -780,7 +790,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
 
 // rho = sum over the bands of this set of f |psi(r)|^2 terms (WAVES_DENSITY
 // for TINV at Gamma), batch by batch through the work grid
-template <class C, int N>
+template <class C, int N1, int N2, int N3>
 static int fft_density_t(Handle* h, const double2* psi, double* rho) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   if (nr3 * kRhoTX > 8 * kPlaneThreads) return h->fail(CUW_ERR_UNSUPPORTED, "density: NR3 above 128");
@@ -792,10 +802,10 @@ static int fft_density_t(Handle* h, const double2* psi, double* rho) {
   const int nxb = (nr1 + kRhoTX - 1) / kRhoTX;
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
-    k_gtor_plane<C, N><<<dim3(h->nzp, nb), kPlaneThreads, smem_plane, h->stream>>>(
+    k_gtor_plane<C, N1, N2><<<dim3(h->nzp, nb), kPlaneThreads, smem_plane, h->stream>>>(
         psi, h->ldg, b0, g.plane_off, g.plane_g, g.plane_pos, grid, h->nzp, a1, a2, g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
-    k_zcol_rho<C, N><<<nr2 * nxb, kPlaneThreads, smem_rho, h->stream>>>(grid, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
+    k_zcol_rho<C, N3><<<nr2 * nxb, kPlaneThreads, smem_rho, h->stream>>>(grid, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
                                                                        g.occ, h->d.nb, b0, nb, rho, b0 == 0);
     CUW_LAUNCH_CHECK("k_zcol_rho");
   }
@@ -804,16 +814,17 @@ static int fft_density_t(Handle* h, const double2* psi, double* rho) {
 
 // kernels of work-grid type C and length N (0: any length): shared-memory
 // limits and the launcher
-template <class C, int N>
-static int fft_select(Handle* h, int smem_plane, int /*smem_z of the generic kernel*/) {
-  const int smem_z = (int)(((size_t)h->d.nr3 * tx_of<N>() + h->d.nr3) * sizeof(C));
-  CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N>, smem_plane));
-  CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N>, smem_plane));
-  CUW_TRY(smem_allow((const void*)k_zcol_v<C, N>, smem_z));
-  if constexpr (N == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, z64_smem_bytes<C>()));
-  CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
-  h->fft_run = &fft_vpsi_t<C, N>;
-  h->fft_rho = &fft_density_t<C, N>;
+template <class C, int N1, int N2, int N3>
+static int fft_select(Handle* h, int smem_plane) {
+  constexpr int TX = tx_of(N1, N3);
+  const int smem_z = (int)(((size_t)h->d.nr3 * TX + h->d.nr3) * sizeof(C));
+  CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N1, N2>, smem_plane));
+  CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N1, N2>, smem_plane));
+  if constexpr (N1 == 64 && N3 == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, z64_smem_bytes<C>()));
+  else CUW_TRY(smem_allow((const void*)k_zcol_v<C, N3, TX>, smem_z));
+  CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N3>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
+  h->fft_run = &fft_vpsi_t<C, N1, N2, N3>;
+  h->fft_rho = &fft_density_t<C, N1, N2, N3>;
   return CUW_OK;
 }
 
@@ -891,26 +902,20 @@ int fft_setup(Handle* h, const int* igvec) {
     CUW_TRY(cudaMemcpy(*tws[a], t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   }
   const int smem_plane = (int)(plane_elems * es);
-  const int smem_z = (int)(((size_t)nr3 * kTX + nr3) * es);
-  // cubic grids of a specialised length get kernels compiled for that length
-  const int nc = (nr1 == nr2 && nr2 == nr3) ? nr1 : 0;
+  // grids of the table get kernels compiled for their lengths (every index
+  // divisor and Stockham stage a constant); any other grid takes the kernels
+  // with run-time lengths
   int rc = CUW_OK;
-  switch (h->mixed() ? -nc - 1 : nc + 1) {
-#define CUW_FFT_CASE(LEN)                                                                  \
-  case LEN + 1: rc = fft_select<double2, LEN>(h, smem_plane, smem_z); break;               \
-  case -LEN - 1: rc = fft_select<float2, LEN>(h, smem_plane, smem_z); break;
-    CUW_FFT_CASE(24)
-    CUW_FFT_CASE(32)
-    CUW_FFT_CASE(48)
-    CUW_FFT_CASE(64)
-    CUW_FFT_CASE(72)
-    CUW_FFT_CASE(96)
-#undef CUW_FFT_CASE
-    default:
-      rc = h->mixed() ? fft_select<float2, 0>(h, smem_plane, smem_z) : fft_select<double2, 0>(h, smem_plane, smem_z);
+  bool found = false;
+#define CUW_FFT_GRID(A, B, Z)                                                                        \
+  if (!found && nr1 == A && nr2 == B && nr3 == Z) {                                                  \
+    found = true;                                                                                    \
+    rc = h->mixed() ? fft_select<float2, A, B, Z>(h, smem_plane) : fft_select<double2, A, B, Z>(h, smem_plane); \
   }
-  if (rc != CUW_OK) return rc;
-  return CUW_OK;
+  CUW_FFT_GRIDS
+#undef CUW_FFT_GRID
+  if (!found) rc = h->mixed() ? fft_select<float2, 0, 0, 0>(h, smem_plane) : fft_select<double2, 0, 0, 0>(h, smem_plane);
+  return rc;
 }
 
 // 3-D transform of a full FP64 complex grid (x fastest), in place and
