@@ -1251,17 +1251,41 @@ __global__ void k_switch_lambda(double2* __restrict__ rlam0, double2* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// WAVES_ORTHO_Y_C with PHIPHI = CHIPHI = CHICHI = S (real) and MAP = identity.
-// One CTA; A, B, C, ALPHA, X, WORK are n x n in global memory.
+// WAVES_ORTHO_Y_C with PHIPHI = CHIPHI = CHICHI = S (real) and MAP = identity
+// (src/paw_waves2.f90:1025-1338), as one cluster of kOyCS CTAs.  A, B, C,
+// ALPHA and X are n x n in global memory (L2).  Step nu of the sequential
+// orthogonalisation has three parts, each ended by a cluster barrier:
+//   1. CTA 0 forms the step's scalar and the column/row updates of X, A and B
+//      along index nu (vectors of n, block barriers only);
+//   2. every CTA copies what the rank-one updates read into its shared memory
+//      (row nu of B, columns nu of ALPHA and C, row nu of C) and forms the two
+//      coefficient vectors z1 (from column nu of A) and z2 (from column nu of
+//      B, which part 3 does not change);
+//   3. every CTA updates its share of the n x n elements of A, X, B, ALPHA
+//      and C from those copies.  The two B updates of an element are applied
+//      in the reference's order, the second with row nu of B as the first left
+//      it; the C update reads the copied row and column instead of a work array.
+// The arithmetic of each element is that of the one-CTA form.
 // ---------------------------------------------------------------------------
+constexpr int kOyCS = 8;
 __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, int n, double* A, double* B, double* C,
-                                                  double* AL, double* X, double* W, int* __restrict__ status) {
-  __shared__ double z[1024];
+                                                  double* AL, double* X, int* __restrict__ status) {
+  extern __shared__ double oysm[];
+  double* z1 = oysm;        // coefficients of the phi step
+  double* z2 = z1 + n;      // coefficients of the chi step
+  double* brow = z2 + n;    // B(nu, j) before part 3
+  double* brow2 = brow + n; // B(nu, j) after the first B update
+  double* alcol = brow2 + n;  // ALPHA(i, nu)
+  double* ccol = alcol + n;   // C(i, nu)
+  double* crow = ccol + n;    // C(nu, j)
   __shared__ double zn;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
   const int tid = threadIdx.x, nt = blockDim.x;
+  const size_t gt = (size_t)rank * nt + tid, gstride = (size_t)kOyCS * nt;
   const double r8small = 1e-10;
   const size_t nn = (size_t)n * n;
-  for (size_t k = tid; k < nn; k += nt) {
+  for (size_t k = gt; k < nn; k += gstride) {
     int i = (int)(k % n), j = (int)(k / n);
     A[k] = s[k] - (i == j ? 1.0 : 0.0);
     B[k] = s[k];
@@ -1269,81 +1293,76 @@ __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, 
     X[k] = 0.0;
     AL[k] = (i == j) ? 1.0 : 0.0;
   }
-  __syncthreads();
+  cl.sync();
   auto I = [n](int i, int j) { return (size_t)i + (size_t)n * j; };
   for (int nu = 0; nu < n; ++nu) {
     const int nn0 = nu;
-    if (tid == 0) {
-      double bnn = B[I(nn0, nn0)], ann = A[I(nn0, nn0)], cnn = C[I(nn0, nn0)];
-      double svar = bnn * bnn - ann * cnn;
-      double svar1 = -bnn, zz;
-      if (svar >= 0.0) {
-        double svar2 = sqrt(svar);
-        zz = (svar1 * svar2 >= 0.0) ? svar1 - svar2 : svar1 + svar2;
-      } else {
-        zz = svar1;
+    // ---- part 1: CTA 0
+    if (rank == 0) {
+      if (tid == 0) {
+        double bnn = B[I(nn0, nn0)], ann = A[I(nn0, nn0)], cnn = C[I(nn0, nn0)];
+        double svar = bnn * bnn - ann * cnn;
+        double svar1 = -bnn, zz;
+        if (svar >= 0.0) {
+          double svar2 = sqrt(svar);
+          zz = (svar1 * svar2 >= 0.0) ? svar1 - svar2 : svar1 + svar2;
+        } else {
+          zz = svar1;
+        }
+        zz = zz / (cnn + r8small);
+        if (svar != svar) status[0] = CUW_ERR_NAN;
+        zn = zz;
       }
-      zz = zz / (cnn + r8small);
-      if (svar != svar) status[0] = CUW_ERR_NAN;
-      zn = zz;
+      __syncthreads();
+      const double zz = zn;
+      for (int i = tid; i < n; i += nt) X[I(i, nn0)] += AL[I(i, nn0)] * zz;
+      for (int j = tid; j < n; j += nt) A[I(nn0, j)] += zz * B[I(nn0, j)];
+      __syncthreads();
+      for (int i = tid; i < n; i += nt) A[I(i, nn0)] += B[I(nn0, i)] * zz;
+      __syncthreads();
+      if (tid == 0) A[I(nn0, nn0)] += zz * C[I(nn0, nn0)] * zz;
+      __syncthreads();
+      for (int i = tid; i < n; i += nt) B[I(i, nn0)] += C[I(i, nn0)] * zz;
     }
-    __syncthreads();
-    const double zz = zn;
-    for (int i = tid; i < n; i += nt) X[I(i, nn0)] += AL[I(i, nn0)] * zz;
-    for (int j = tid; j < n; j += nt) A[I(nn0, j)] += zz * B[I(nn0, j)];
-    __syncthreads();
-    for (int i = tid; i < n; i += nt) A[I(i, nn0)] += B[I(nn0, i)] * zz;
-    __syncthreads();
-    if (tid == 0) A[I(nn0, nn0)] += zz * C[I(nn0, nn0)] * zz;
-    __syncthreads();
-    for (int i = tid; i < n; i += nt) B[I(i, nn0)] += C[I(i, nn0)] * zz;
-    __syncthreads();
-    // orthogonalise higher phis to this phi
+    cl.sync();
+    // ---- part 2: every CTA
     const double bnn = B[I(nn0, nn0)] + r8small;
-    for (int i = tid; i < n; i += nt) z[i] = (i > nu) ? -(A[I(i, nn0)] / bnn) : 0.0;
-    __syncthreads();
     const double cnn = C[I(nn0, nn0)];
-    for (size_t k = tid; k < nn; k += nt) {
-      int i = (int)(k % n), j = (int)(k / n);
-      if (j > nu) X[k] += AL[I(i, nn0)] * z[j];
+    for (int i = tid; i < n; i += nt) {
+      z1[i] = (i > nu) ? -(A[I(i, nn0)] / bnn) : 0.0;
+      z2[i] = (i > nu) ? -(B[I(i, nn0)] / bnn) : 0.0;
+      brow[i] = B[I(nn0, i)];
+      alcol[i] = AL[I(i, nn0)];
+      ccol[i] = C[I(i, nn0)];
+      crow[i] = C[I(nn0, i)];
+    }
+    __syncthreads();
+    for (int j = tid; j < n; j += nt) brow2[j] = (j > nu) ? brow[j] + ccol[nn0] * z1[j] : brow[j];
+    // every CTA has read the columns and rows before any CTA changes them
+    cl.sync();
+    // ---- part 3: the CTA's share of the n x n elements
+    for (size_t k = gt; k < nn; k += gstride) {
+      const int i = (int)(k % n), j = (int)(k / n);
+      // orthogonalise higher phis to this phi
+      if (j > nu) X[k] += alcol[i] * z1[j];
       double add = 0.0;
-      if (i > nu) add += z[i] * B[I(nn0, j)];
-      if (j > nu) add += B[I(nn0, i)] * z[j];
-      if (i > nu && j > nu) add += z[i] * cnn * z[j];
+      if (i > nu) add += z1[i] * brow[j];
+      if (j > nu) add += brow[i] * z1[j];
+      if (i > nu && j > nu) add += z1[i] * cnn * z1[j];
       A[k] += add;
-    }
-    __syncthreads();
-    for (size_t k = tid; k < nn; k += nt) {
-      int i = (int)(k % n), j = (int)(k / n);
-      if (j > nu) B[k] += C[I(i, nn0)] * z[j];
-    }
-    __syncthreads();
-    // orthogonalise higher chis to this phi
-    const double bnn2 = B[I(nn0, nn0)] + r8small;
-    __syncthreads();
-    for (int i = tid; i < n; i += nt) z[i] = (i > nu) ? -(B[I(i, nn0)] / bnn2) : 0.0;
-    __syncthreads();
-    for (size_t k = tid; k < nn; k += nt) {
-      int i = (int)(k % n), j = (int)(k / n);
-      if (j > nu) AL[k] += AL[I(i, nn0)] * z[j];
-    }
-    __syncthreads();
-    for (size_t k = tid; k < nn; k += nt) {
-      int i = (int)(k % n), j = (int)(k / n);
-      if (i > nu) B[k] += z[i] * B[I(nn0, j)];
-    }
-    const double cnn2 = C[I(nn0, nn0)];
-    for (size_t k = tid; k < nn; k += nt) {
-      int i = (int)(k % n), j = (int)(k / n);
+      double b = B[k];
+      if (j > nu) b += ccol[i] * z1[j];
+      // orthogonalise higher chis to this phi
+      if (j > nu) AL[k] += alcol[i] * z2[j];
+      if (i > nu) b += z2[i] * brow2[j];
+      B[k] = b;
       double wv = 0.0;
-      if (i > nu) wv += z[i] * C[I(nn0, j)];
-      if (j > nu) wv += C[I(i, nn0)] * z[j];
-      if (i > nu && j > nu) wv += z[i] * cnn2 * z[j];
-      W[k] = wv;
+      if (i > nu) wv += z2[i] * crow[j];
+      if (j > nu) wv += ccol[i] * z2[j];
+      if (i > nu && j > nu) wv += z2[i] * cnn * z2[j];
+      C[k] += wv;
     }
-    __syncthreads();
-    for (size_t k = tid; k < nn; k += nt) C[k] += W[k];
-    __syncthreads();
+    cl.sync();
   }
 }
 
@@ -1629,8 +1648,22 @@ int ortho_y_run(Handle* h, const double* s, double* x) {
   if (n > 1024) return h->fail(CUW_ERR_UNSUPPORTED, "Gram-Schmidt supports NB <= 1024");
   Device& g = h->g;
   CUW_TRY(cudaMemsetAsync(g.ostatus, 0, sizeof(int) * 2, h->stream));
-  // A, B, C, ALPHA, WORK in the NB x NB buffers that are free during start-up
-  k_ortho_y<<<1, 1024, 0, h->stream>>>(s, n, g.haux, g.gamn, g.work, g.lam2, x, g.lam, g.ostatus);
+  // A, B, C, ALPHA in the NB x NB buffers that are free during start-up
+  const int smem = (int)(sizeof(double) * 7 * (size_t)n);
+  CUW_TRY(smem_allow((const void*)k_ortho_y, smem));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kOyCS);
+  cfg.blockDim = dim3(1024);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kOyCS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CUW_TRY(cudaLaunchKernelEx(&cfg, k_ortho_y, s, n, g.haux, g.gamn, g.work, g.lam2, x, g.ostatus));
   CUW_LAUNCH_CHECK("k_ortho_y");
   return CUW_OK;
 }
