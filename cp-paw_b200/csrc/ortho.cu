@@ -214,6 +214,113 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ s_in
   if (tid == 0) info[0] = sweep;
 }
 
+// The same Jacobi iteration as one cluster of kJacCS CTAs for matrices whose
+// packed triangle does not fit one CTA's shared memory (A and V in global
+// memory, L2 resident).  Every CTA forms the rotations of a round itself (the
+// same arithmetic on the same data, so the CTAs agree on them and on the
+// convergence flag); a cluster barrier then separates those reads of A from
+// the round's updates, which the CTAs share, and a second one ends the round.
+constexpr int kJacCS = 8;
+__global__ void __launch_bounds__(1024) k_jacobi_cl(const double* __restrict__ s_in, int n, double* __restrict__ u_out,
+                                                    double* __restrict__ e_out, double* __restrict__ V,
+                                                    double* __restrict__ A, int max_sweeps, int* __restrict__ ost,
+                                                    const int* __restrict__ gate) {
+  extern __shared__ double sm[];
+  if (gate_closed(gate)) return;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int gt = rank * nt + tid, gs = kJacCS * nt;
+  if (rank == 0 && tid == 0) {
+    ++ost[kStRediag];
+    if (gate) ++ost[kStFallbacks];
+  }
+  int* info = ost + 4;
+  const int np = n / 2;
+  double* rc = sm;       // np cosines
+  double* rs = rc + np;  // np sines
+  int* pp = reinterpret_cast<int*>(rs + np);
+  int* pq = pp + np;
+  int* flag = pq + np;
+  int* pqtab = flag + 2;  // (P, Q) of every 2x2 block, P | Q << 16
+  for (int j = gt; j < n; j += gs)
+    for (int i = 0; i <= j; ++i) A[pk(i, j)] = s_in[i + (size_t)n * j];
+  for (int Q = tid; Q < np; Q += nt)
+    for (int P = 0; P <= Q; ++P) pqtab[Q * (Q + 1) / 2 + P] = P | (Q << 16);
+  cl.sync();  // V may alias s_in
+  for (size_t k = gt; k < (size_t)n * n; k += gs) {
+    int i = (int)(k % n), j = (int)(k / n);
+    V[k] = (i == j) ? 1.0 : 0.0;
+  }
+  cl.sync();
+  const int nblk = np * (np + 1) / 2;
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    if (tid == 0) *flag = 0;
+    __syncthreads();
+    for (int r = 0; r < n - 1; ++r) {
+      if (tid < np) {
+        int a, b;
+        if (tid == 0) { a = n - 1; b = r; }
+        else { a = (r + tid) % (n - 1); b = (r - tid + (n - 1)) % (n - 1); }
+        int p = min(a, b), q = max(a, b);
+        pp[tid] = p;
+        pq[tid] = q;
+        double apq = A[pk(p, q)], app = A[pk(p, p)], aqq = A[pk(q, q)];
+        double c = 1.0, s = 0.0;
+        if (apq != 0.0 && fabs(apq) > 1e-14 * sqrt(fabs(app * aqq))) {
+          double theta = (aqq - app) / (2.0 * apq);
+          double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          c = 1.0 / sqrt(t * t + 1.0);
+          s = t * c;
+          *flag = 1;
+        }
+        rc[tid] = c;
+        rs[tid] = s;
+      }
+      cl.sync();  // every CTA has read the round's pivots before any CTA rotates
+      for (int k = gt; k < nblk; k += gs) {
+        const int pqv = pqtab[k];
+        const int P = pqv & 0xffff, Q = pqv >> 16;
+        int p = pp[P], q = pq[P], r2 = pp[Q], s2 = pq[Q];
+        double cP = rc[P], sP = rs[P], cQ = rc[Q], sQ = rs[Q];
+        if (P == Q) {
+          double apq = A[pk(p, q)], app = A[pk(p, p)], aqq = A[pk(q, q)];
+          if (sP != 0.0) {
+            double t = sP / cP;
+            A[pk(p, p)] = app - t * apq;
+            A[pk(q, q)] = aqq + t * apq;
+            A[pk(p, q)] = 0.0;
+          }
+        } else {
+          double a_pr = A[pk(p, r2)], a_ps = A[pk(p, s2)], a_qr = A[pk(q, r2)], a_qs = A[pk(q, s2)];
+          double b_pr = cP * a_pr - sP * a_qr, b_ps = cP * a_ps - sP * a_qs;
+          double b_qr = sP * a_pr + cP * a_qr, b_qs = sP * a_ps + cP * a_qs;
+          A[pk(p, r2)] = cQ * b_pr - sQ * b_ps;
+          A[pk(p, s2)] = sQ * b_pr + cQ * b_ps;
+          A[pk(q, r2)] = cQ * b_qr - sQ * b_qs;
+          A[pk(q, s2)] = sQ * b_qr + cQ * b_qs;
+        }
+      }
+      for (int k = gt; k < np * n; k += gs) {
+        int P = k / n, row = k % n;
+        double c = rc[P], s = rs[P];
+        if (s == 0.0) continue;
+        int p = pp[P], q = pq[P];
+        double vp = V[row + (size_t)n * p], vq = V[row + (size_t)n * q];
+        V[row + (size_t)n * p] = c * vp - s * vq;
+        V[row + (size_t)n * q] = s * vp + c * vq;
+      }
+      cl.sync();  // the round's rotations are visible to every CTA
+    }
+    if (*flag == 0) break;
+    __syncthreads();  // every thread has read the flag before it is reset
+  }
+  for (int i = gt; i < n; i += gs) e_out[i] = A[pk(i, i)];
+  for (size_t k = gt; k < (size_t)n * n; k += gs) u_out[k] = V[k];
+  if (rank == 0 && tid == 0) info[0] = sweep;
+}
+
 // ---------------------------------------------------------------------------
 // WAVES_ORTHO_X iteration as one cluster of CS CTAs.  All matrices are real,
 // column-major n x n, in global memory (L2 resident).  The output tile of every
@@ -1400,11 +1507,29 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e, const int* 
     smem = base;
   }
   if (smem > 220 * 1024) {
-    // the packed matrix goes to global memory too
+    // the packed matrix goes to global memory too, and the rounds are shared
+    // by a cluster of CTAs
     smem = base - sizeof(double) * packed;
     if (smem > 220 * 1024) return h->fail(CUW_ERR_UNSUPPORTED, "NB too large for the eigensolver");
     if (!h->g.jac_a) CUW_TRY(cudaMalloc(&h->g.jac_a, sizeof(double) * packed));
     aglob = h->g.jac_a;
+    const size_t smem_cl = sizeof(double) * n + sizeof(int) * (n + 2) + tab;
+    CUW_TRY(smem_allow((const void*)k_jacobi_cl, (int)smem_cl));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kJacCS);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = smem_cl;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kJacCS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUW_TRY(cudaLaunchKernelEx(&cfg, k_jacobi_cl, s_dev, n, u, e, h->g.work, aglob, 40, h->g.ostatus, gate));
+    CUW_LAUNCH_CHECK("k_jacobi_cl");
+    return CUW_OK;
   }
   CUW_TRY(smem_allow((const void*)k_jacobi, (int)smem));
   k_jacobi<<<1, 1024, smem, h->stream>>>(s_dev, n, u, e, h->g.work, v_in_smem, aglob, 40, h->g.ostatus, gate);

@@ -217,6 +217,37 @@ def test_gramschmidt(oracle, inputs_cache):
     assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-10
 
 
+def test_large_band_count(oracle):
+    """NB = 256, beyond one CTA's shared memory: the cluster Gram-Schmidt, the
+    cluster Jacobi eigensolver of the first ORTHO_X call and the ORTHO_X
+    cluster kernel for NB > 128, against the oracle (Gram-Schmidt, then two
+    CP steps with moving atoms)."""
+    inp = systems.build_inputs(systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, nb=256, name="Si8-nb256"))
+    assert inp["nb"] == 256
+    gpu = cuwaves.open_waves(inp).setup()
+    cpu = oracle.open_oracle(inp).setup()
+    for which in (CUW_PSI0, CUW_PSIM):
+        for w in (gpu, cpu):
+            w.gramschmidt(which, inp["r0"])
+        # 256 sequential orthogonalisation steps from random vectors: the
+        # rounding of the two machines accumulates to a few 1e-10
+        assert rel(gpu.download_psi(which), cpu.download_psi(which)) < 1e-9
+    gpu.projections()
+    cpu.projections()
+    sync_state(gpu, cpu)
+    for step in range(2):
+        og, fg = gpu.cp_step(move_atoms=True)
+        oc, fc = cpu.cp_step(move_atoms=True)
+        assert og[4] == oc[4], f"step {step}: ortho iterations {og[4]} vs {oc[4]}"
+        tol = 1e-8 * max(1.0, abs(oc[0]) / 100)
+        assert abs(og[0] - oc[0]) < tol, f"step {step}: E {og[0]} vs {oc[0]}"
+        assert np.abs(fg - fc).max() < 1e-6
+    assert gpu.ortho_stats()["eigendecompositions"] >= 1
+    assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-8
+    gpu.close()
+    cpu.close()
+
+
 @pytest.mark.parametrize("name,nsteps,move", [("Si8-20Ry", 8, False), ("Si8", 5, True), ("H2O2", 5, True)])
 def test_cp_steps(name, nsteps, move, oracle, inputs_cache):
     """Full CP steps (TIMESTEP order) on both engines, compared step by step."""
