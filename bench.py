@@ -407,7 +407,7 @@ def run_mixed(args, local):
                          "peak_source": "TF32 cuBLAS (torch.matmul float32 8192^3, TF32 allowed) measured in this run",
                          "tensor_flops_per_step": 3.0 * flops, "model_flops_per_step": flops,
                          "model_tflops": round(flops / (t_ms * 1e-3) / 1e12, 3) if t_ms > 0 else None,
-                         "traffic": None},
+                         "traffic": load_ncu_traffic().get("tc_" + name)},
             "roofline_fft": fft_roofline(ph.get("fft_vpsi"), fm["fft_bytes"] / 2, peaks, peak_src),
             "phase_ms_per_step": {k: round(v, 4) for k, v in ph.items()}}
 
