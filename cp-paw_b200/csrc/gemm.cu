@@ -41,9 +41,15 @@ constexpr int EPT = BM * BK / NT;  // tile elements per thread and operand (4)
 // a pattern free of bank conflicts for the m8n8k4 fragments).
 // Warp (wm, wn) in a 2x4 layout owns a 32x16 block: 4 x 2 tiles of 8x8.
 // ---------------------------------------------------------------------------
+// Complex products by the three-multiplication (Gauss) form: with a = ar + i ai
+// and b = br + i bi, the main loops accumulate P1 = sum ar br (in r),
+// P2 = sum ai bi (in i) and P3 = sum (ar + ai)(br + bi) (in s), three real MMAs
+// per complex product instead of four; finish() turns them into
+// Re = P1 - P2 (r) and Im = P3 - P1 - P2 (i).
 struct Acc {
   double r[4][2][2];
   double i[4][2][2];
+  double s[4][2][2];
   __device__ void zero() {
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -51,7 +57,20 @@ struct Acc {
       for (int b = 0; b < 2; ++b) {
         r[a][b][0] = r[a][b][1] = 0.0;
         i[a][b][0] = i[a][b][1] = 0.0;
+        s[a][b][0] = s[a][b][1] = 0.0;
       }
+  }
+  __device__ void finish() {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const double p1 = r[a][b][e], p2 = i[a][b][e], p3 = s[a][b][e];
+          r[a][b][e] = p1 - p2;
+          i[a][b][e] = (p3 - p1) - p2;
+        }
   }
 };
 
@@ -61,37 +80,36 @@ __device__ __forceinline__ void mma_slice(Acc& acc, const double* Ar, const doub
   const int r8 = lane >> 2, c4 = lane & 3;
 #pragma unroll
   for (int ks = 0; ks < BK / 4; ++ks) {
-    double ar[4], ai[4], nai[4], br[2], bi[2];
+    double ar[4], ai[4], as[4], br[2], bi[2], bs[2];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
       const int o = (wm * 32 + mi * 8 + r8) * LDS + ks * 4 + c4;
       ar[mi] = Ar[o];
       double t = Ai[o];
       ai[mi] = CONJA ? -t : t;
-      nai[mi] = -ai[mi];
+      as[mi] = ar[mi] + ai[mi];
     }
 #pragma unroll
     for (int ni = 0; ni < 2; ++ni) {
       const int o = (wn * 16 + ni * 8 + r8) * LDS + ks * 4 + c4;
       br[ni] = Br[o];
       bi[ni] = Bi[o];
+      bs[ni] = br[ni] + bi[ni];
     }
-    // two passes over the 16 accumulators, so that the two products that
-    // add into one accumulator are 16 MMAs apart instead of back to back
+    // three passes over the 8 blocks: the products that add into one
+    // accumulator are 24 MMAs apart
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni) {
-        dmma(acc.r[mi][ni], ar[mi], br[ni]);
-        dmma(acc.i[mi][ni], ar[mi], bi[ni]);
-      }
+      for (int ni = 0; ni < 2; ++ni) dmma(acc.r[mi][ni], ar[mi], br[ni]);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni) {
-        dmma(acc.r[mi][ni], nai[mi], bi[ni]);
-        dmma(acc.i[mi][ni], ai[mi], br[ni]);
-      }
+      for (int ni = 0; ni < 2; ++ni) dmma(acc.i[mi][ni], ai[mi], bi[ni]);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) dmma(acc.s[mi][ni], as[mi], bs[ni]);
   }
 }
 
@@ -183,6 +201,8 @@ __device__ __forceinline__ void mainloop(double* sm, int kbeg, int kend, FA0 fa0
     __syncthreads();
     st ^= 1;
   }
+  acc0.finish();
+  acc1.finish();
 }
 
 // ---------------------------------------------------------------------------
@@ -232,34 +252,33 @@ __device__ __forceinline__ void mma_slice2(Acc& acc, const double2* A, const dou
 #pragma unroll
   for (int ks = 0; ks < BK / 4; ++ks) {
     const bool cj = ca(k0 + ks * 4 + c4);
-    double ar[4], ai[4], nai[4], br[2], bi[2];
+    double ar[4], ai[4], as[4], br[2], bi[2], bs[2];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
       const double2 v = A[toff<AKF>(wm * 32 + mi * 8 + r8, ks * 4 + c4)];
       ar[mi] = v.x;
       ai[mi] = cj ? -v.y : v.y;
-      nai[mi] = -ai[mi];
+      as[mi] = ar[mi] + ai[mi];
     }
 #pragma unroll
     for (int ni = 0; ni < 2; ++ni) {
       const double2 w = B[toff<BKF>(wn * 16 + ni * 8 + r8, ks * 4 + c4)];
       br[ni] = w.x;
       bi[ni] = CB ? -w.y : w.y;
+      bs[ni] = br[ni] + bi[ni];
     }
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni) {
-        dmma(acc.r[mi][ni], ar[mi], br[ni]);
-        dmma(acc.i[mi][ni], ar[mi], bi[ni]);
-      }
+      for (int ni = 0; ni < 2; ++ni) dmma(acc.r[mi][ni], ar[mi], br[ni]);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni) {
-        dmma(acc.r[mi][ni], nai[mi], bi[ni]);
-        dmma(acc.i[mi][ni], ai[mi], br[ni]);
-      }
+      for (int ni = 0; ni < 2; ++ni) dmma(acc.i[mi][ni], ai[mi], bi[ni]);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) dmma(acc.s[mi][ni], as[mi], bs[ni]);
   }
 }
 
@@ -320,6 +339,8 @@ __device__ __forceinline__ void mainloop2(double2* sm, int kbeg, int kend, PA0 p
   }
   cpa_wait<0>();
   __syncthreads();
+  acc0.finish();
+  acc1.finish();
 }
 
 template <int MODE>
