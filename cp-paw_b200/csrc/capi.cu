@@ -387,7 +387,7 @@ static int dev_alloc(Handle* h, void** p, size_t bytes) {
 static void free_all(Handle* h) {
   Device& g = h->g;
   void* ptrs[] = {g.rho, g.psi0, g.psim, g.hpsi, g.opsi, g.proj, g.oproj, g.hproj, g.pbuf, g.rlam0, g.rlamm, g.igvec,
-                  g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_off,
+                  g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_rows, g.plane_off,
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
                   g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,

@@ -79,6 +79,7 @@ struct Device {
   ProDesc *pdesc = nullptr;      // (NPRO)
   // FFT
   int *plane_iz = nullptr;       // (nzp) occupied z planes
+  int2 *plane_rows = nullptr;    // (nzp) first row and row count of the plane's G vectors
   int *plane_off = nullptr;      // (nzp+1) CSR offsets of the G lists
   int *plane_g = nullptr;        // (NGL) G index, grouped by plane
   int *plane_pos = nullptr;      // (NGL) ix + NR1*iy of that G

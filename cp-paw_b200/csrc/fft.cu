@@ -259,9 +259,16 @@ __host__ __device__ constexpr int chunk_lines(int N) {
   return lc;
 }
 
+// Line l of a transform lives at row (row0 + l) mod nrows of the buffer
+// (row0 = 0 and nrows above every line index: the identity).
+__device__ __forceinline__ int line_row(int l, int row0, int nrows) {
+  const int r = row0 + l;
+  return r >= nrows ? r - nrows : r;
+}
+
 template <int N, int R, int NS, int LC, class C>
 __device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, int es, bool jfast, const C* tw,
-                                            typename CT<C>::R sgn) {
+                                            typename CT<C>::R sgn, int row0, int nrows) {
   constexpr int BPT = bpt_of(R);
   constexpr int NQ = N / R;
   constexpr int TSTEP = N / (NS * R);
@@ -281,7 +288,7 @@ __device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, i
     const int k = j % NS;
     off_[t] = line * N + ((j / NS) * NS * R + k);  // (line, destination index) packed
     if (act[t]) {
-      C* base = buf + (size_t)(line0 + line) * ls;
+      C* base = buf + (size_t)line_row(line0 + line, row0, nrows) * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         C x = base[(size_t)(j + r * NQ) * es];
@@ -296,7 +303,7 @@ __device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, i
   for (int t = 0; t < BPT; ++t) {
     if (act[t]) {
       const int line = off_[t] / N, idxd = off_[t] % N;
-      C* base = buf + (size_t)(line0 + line) * ls;
+      C* base = buf + (size_t)line_row(line0 + line, row0, nrows) * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) base[(size_t)(idxd + r * NS) * es] = v[t][r];
     }
@@ -306,21 +313,22 @@ __device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, i
 
 template <int N, int S, int NS, int LC, class C>
 __device__ __forceinline__ void stages_fixed(C* buf, int line0, int nl, int ls, int es, bool jfast, const C* tw,
-                                             typename CT<C>::R sgn) {
+                                             typename CT<C>::R sgn, int row0, int nrows) {
   constexpr RadixList L = radices_of(N);
   if constexpr (S < L.n) {
     constexpr int R = L.r[S];
-    stage_fixed<N, R, NS, LC>(buf, line0, nl, ls, es, jfast, tw, sgn);
-    stages_fixed<N, S + 1, NS * R, LC>(buf, line0, nl, ls, es, jfast, tw, sgn);
+    stage_fixed<N, R, NS, LC>(buf, line0, nl, ls, es, jfast, tw, sgn, row0, nrows);
+    stages_fixed<N, S + 1, NS * R, LC>(buf, line0, nl, ls, es, jfast, tw, sgn, row0, nrows);
   }
 }
 
 template <int N, class C>
-__device__ void transform_fixed(C* buf, int nlines, int ls, int es, bool jfast, const C* tw, typename CT<C>::R sgn) {
+__device__ void transform_fixed(C* buf, int nlines, int ls, int es, bool jfast, const C* tw, typename CT<C>::R sgn,
+                                int row0 = 0, int nrows = 1 << 30) {
   constexpr int LC = chunk_lines(N);
   for (int l0 = 0; l0 < nlines; l0 += LC) {
     const int nl = min(LC, nlines - l0);
-    stages_fixed<N, 0, 1, LC>(buf, l0, nl, ls, es, jfast, tw, sgn);
+    stages_fixed<N, 0, 1, LC>(buf, l0, nl, ls, es, jfast, tw, sgn, row0, nrows);
   }
 }
 
@@ -383,6 +391,17 @@ __device__ __forceinline__ void xform(C* buf, const AxisArg& ax, int nlines, int
   else transform(buf, ax, nlines, ls, es, jfast, tw, sgn);
 }
 
+// The x lines of an xy plane restricted to the rows that hold G vectors:
+// rows (y0 + l) mod nr2 for l < ny (the plane's rows form one range of signed
+// y).  The other rows are zero before the G->R transform and are not read
+// after the R->G transform.  Kernels with run-time lengths transform every row.
+template <int N, class C>
+__device__ __forceinline__ void xform_rows(C* buf, const AxisArg& ax, int y0, int ny, int nr2, int ls,
+                                           const C* tw, typename CT<C>::R sgn) {
+  if constexpr (N > 0) transform_fixed<N>(buf, ny, ls, 1, false, tw, sgn, y0, nr2);
+  else transform(buf, ax, nr2, ls, 1, false, tw, sgn);
+}
+
 // load twiddles exp(sgn*2 pi i k/n) from the FP64 table exp(+2 pi i k/n)
 template <class C>
 __device__ void load_tw(C* dst, const double2* src, int n, double sgn) {
@@ -423,8 +442,9 @@ __device__ __forceinline__ int row_of(int i, int nr1) {
 template <class C, int N1, int N2>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
-                 const int* __restrict__ plane_g, const int* __restrict__ plane_pos, C* __restrict__ grid, int nzp,
-                 AxisArg a1, AxisArg a2, const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
+                 const int* __restrict__ plane_g, const int* __restrict__ plane_pos, const int2* __restrict__ plane_rows,
+                 C* __restrict__ grid, int nzp, AxisArg a1, AxisArg a2, const double2* __restrict__ tw1g,
+                 const double2* __restrict__ tw2g) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int nr1 = a1.n, nr2 = a2.n, npl = nr1 * nr2, ps = plane_stride(nr1);
@@ -440,8 +460,9 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x)
     plane[plane_pos[k]] = from_d2<C>(src[plane_g[k]]);
   __syncthreads();
-  xform<N1>(plane, a1, nr2, ps, 1, false, tw1, (typename CT<C>::R)1);  // x lines
-  xform<N2>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);  // y lines
+  const int2 rows = plane_rows[p];
+  xform_rows<N1>(plane, a1, rows.x, rows.y, nr2, ps, tw1, (typename CT<C>::R)1);  // x lines
+  xform<N2>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);               // y lines
   C* dst = grid + ((size_t)bl * nzp + p) * npl;
   for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i + row_of<N1>(i, nr1)];
 }
@@ -643,7 +664,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
 template <class C, int N1, int N2>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_rtog_plane(const C* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
-                 const int* __restrict__ plane_g, const int* __restrict__ plane_pos, double2* __restrict__ out,
+                 const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
+                 const int2* __restrict__ plane_rows, double2* __restrict__ out,
                  const double2* __restrict__ psi, int ldg, int b0, const double* __restrict__ g2,
                  const double* __restrict__ bucket, int add_kin, AxisArg a1, AxisArg a2,
                  const double2* __restrict__ tw1g, const double2* __restrict__ tw2g) {
@@ -660,7 +682,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   load_tw(tw2, tw2g, nr2, -1.0);
   __syncthreads();
   xform<N2>(plane, a2, nr1, 1, pst, false, tw2, (typename CT<C>::R)-1);  // y lines
-  xform<N1>(plane, a1, nr2, pst, 1, false, tw1, (typename CT<C>::R)-1);  // x lines
+  const int2 rows = plane_rows[p];
+  xform_rows<N1>(plane, a1, rows.x, rows.y, nr2, pst, tw1, (typename CT<C>::R)-1);  // x lines
   double2* dst = out + (size_t)ldg * b;
   const double2* ps = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
@@ -765,8 +788,8 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
     k_gtor_plane<C, N1, N2><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
-                                                                           g.plane_pos, grid, h->nzp, a1, a2, g.tw1,
-                                                                           g.tw2);
+                                                                           g.plane_pos, g.plane_rows, grid, h->nzp,
+                                                                           a1, a2, g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
     if constexpr (N1 == 64 && N3 == 64) {
       k_zcol_v64<C><<<dim3(nr2, nb), tz, z64_smem_bytes<C>(), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
@@ -779,7 +802,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
       CUW_LAUNCH_CHECK("k_zcol_v");
     }
     k_rtog_plane<C, N1, N2><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
-                                                                      g.plane_pos, out, psi, h->ldg, b0, g.g2,
+                                                                      g.plane_pos, g.plane_rows, out, psi, h->ldg, b0, g.g2,
                                                                       g.bucket, add_kinetic ? 1 : 0, a1, a2,
                                                                       g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_rtog_plane");
@@ -803,7 +826,7 @@ static int fft_density_t(Handle* h, const double2* psi, double* rho) {
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
     k_gtor_plane<C, N1, N2><<<dim3(h->nzp, nb), kPlaneThreads, smem_plane, h->stream>>>(
-        psi, h->ldg, b0, g.plane_off, g.plane_g, g.plane_pos, grid, h->nzp, a1, a2, g.tw1, g.tw2);
+        psi, h->ldg, b0, g.plane_off, g.plane_g, g.plane_pos, g.plane_rows, grid, h->nzp, a1, a2, g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
     k_zcol_rho<C, N3><<<nr2 * nxb, kPlaneThreads, smem_rho, h->stream>>>(grid, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
                                                                        g.occ, h->d.nb, b0, nb, rho, b0 == 0);
@@ -860,6 +883,22 @@ int fft_setup(Handle* h, const int* igvec) {
       off.push_back(off.back() + cnt[z]);
     }
   const int nzp = (int)plane_iz.size();
+  // signed row range of every occupied plane: rows (y0 + l) mod NR2, l < ny
+  std::vector<int> ylo(nzp, 1 << 30), yhi(nzp, -(1 << 30));
+  for (int gg = 0; gg < ngl; ++gg) {
+    const int s = zslot[iz_of[gg]];
+    int y = ((igvec[3 * gg + 1] % nr2) + nr2) % nr2;
+    if (y > nr2 / 2) y -= nr2;
+    ylo[s] = std::min(ylo[s], y);
+    yhi[s] = std::max(yhi[s], y);
+  }
+  std::vector<int2> rows(nzp);
+  for (int s = 0; s < nzp; ++s) {
+    int ny = yhi[s] - ylo[s] + 1;
+    int y0 = (ylo[s] + nr2) % nr2;
+    if (ny > nr2) { ny = nr2; y0 = 0; }
+    rows[s] = make_int2(y0, ny);
+  }
   std::vector<int> fill(off.begin(), off.end() - 1), pg(ngl), pp(ngl);
   for (int g = 0; g < ngl; ++g) {
     int s = zslot[iz_of[g]];
@@ -876,6 +915,7 @@ int fft_setup(Handle* h, const int* igvec) {
   Device& g = h->g;
   if (g.plane_off) {
     cudaFree(g.plane_off); cudaFree(g.plane_g); cudaFree(g.plane_pos); cudaFree(g.zslot); cudaFree(g.plane_iz);
+    cudaFree(g.plane_rows);
     cudaFree(g.grid); cudaFree(g.tw1); cudaFree(g.tw2); cudaFree(g.tw3);
   }
   CUW_TRY(cudaMalloc(&g.plane_off, sizeof(int) * (nzp + 1)));
@@ -883,6 +923,7 @@ int fft_setup(Handle* h, const int* igvec) {
   CUW_TRY(cudaMalloc(&g.plane_pos, sizeof(int) * ngl));
   CUW_TRY(cudaMalloc(&g.zslot, sizeof(int) * nr3));
   CUW_TRY(cudaMalloc(&g.plane_iz, sizeof(int) * nzp));
+  CUW_TRY(cudaMalloc(&g.plane_rows, sizeof(int2) * nzp));
   CUW_TRY(cudaMalloc(&g.grid, per_band * batch));
   h->grid_bands = batch;
   CUW_TRY(cudaMemcpy(g.plane_off, off.data(), sizeof(int) * (nzp + 1), cudaMemcpyHostToDevice));
@@ -890,6 +931,7 @@ int fft_setup(Handle* h, const int* igvec) {
   CUW_TRY(cudaMemcpy(g.plane_pos, pp.data(), sizeof(int) * ngl, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(g.zslot, zslot.data(), sizeof(int) * nr3, cudaMemcpyHostToDevice));
   CUW_TRY(cudaMemcpy(g.plane_iz, plane_iz.data(), sizeof(int) * nzp, cudaMemcpyHostToDevice));
+  CUW_TRY(cudaMemcpy(g.plane_rows, rows.data(), sizeof(int2) * nzp, cudaMemcpyHostToDevice));
   double2** tws[3] = {&g.tw1, &g.tw2, &g.tw3};
   for (int a = 0; a < 3; ++a) {
     int n = h->ax[a].n;
