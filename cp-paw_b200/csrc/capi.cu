@@ -1551,6 +1551,13 @@ extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
       h->use_graphs = value != 0.0;
       if (!h->use_graphs) h->drop_graphs();
       return CUW_OK;
+    case CUW_OPT_FFT_VARIANT: {
+      const int v = (int)value;
+      if ((double)v != value) return h->fail(CUW_ERR_ARG, "FFT_VARIANT must be an integer");
+      const int rc = fft_set_variant(h, v);
+      if (rc == CUW_ERR_UNSUPPORTED) return h->fail(rc, "FFT plan variant not available for this grid");
+      return rc;
+    }
     case CUW_OPT_SELFCONSISTENT:
       if (value != 0.0 && !(h->have_rhoset && h->have_qlm))
         return h->fail(CUW_ERR_STATE, "self-consistent steps need cuwaves_set_rhoset and cuwaves_set_qlm");

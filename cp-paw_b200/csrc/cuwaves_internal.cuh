@@ -163,6 +163,8 @@ struct Handle {
   AxisPlan ax[3];
   int (*fft_run)(Handle*, const double2*, double2*, bool) = nullptr;  // chosen by fft_setup
   int (*fft_rho)(Handle*, const double2*, double*) = nullptr;          // density, chosen by fft_setup
+  int fft_variant = 0;        // plan variant of the compiled FFT kernels (autotuner)
+  bool fft_compiled = false;  // the grid has kernels compiled for its lengths
   size_t nr = 0;
   std::vector<double> occ_h;
   double waveekin1 = 0.0, waveekin2 = 0.0;
@@ -304,6 +306,8 @@ int fft_setup(Handle* h, const int* igvec_host);
 int fft_vpsi(Handle* h, const double2* psi, double2* out, bool add_kinetic);
 int fft_density(Handle* h, const double2* psi, double* rho);
 int grid_fft(Handle* h, double2* grid, int dir);  // full-grid FP64 transform, unscaled
+int fft_set_variant(Handle* h, int v);  // FFT plan variant of the compiled kernels
+int fft_variants(const Handle* h);
 int vofrho_run(Handle* h, const double* rho_dev);  // POTENTIAL$VOFRHO on the device
 int denmat_run(Handle* h, int lmnxx, double2* denmat, double2* edenmat);
 int eigr_compute(Handle* h, const double* r_dev);

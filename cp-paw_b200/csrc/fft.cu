@@ -233,11 +233,18 @@ struct AxisArg {
 // the index arithmetic is a constant, the stages are inlined and the block
 // size is fixed (kPlaneThreads), so the lines per chunk are constant too.
 // ---------------------------------------------------------------------------
+//
+// Plan variants V (chosen per handle by the autotuner, src/paw_library.f90
+// LIB_FFTW3 leaves the same choice to FFTW's measured planning):
+//   bit 0: 16 instead of 8 complex values per thread and stage (more lines
+//          per pass, fewer barrier-separated passes, more registers);
+//   bit 1: the radix stages in ascending instead of descending order.
+// ---------------------------------------------------------------------------
 struct RadixList {
   int n;
   int r[8];
 };
-__host__ __device__ constexpr RadixList radices_of(int N) {
+__host__ __device__ constexpr RadixList radices_of(int N, int V = 0) {
   RadixList L{0, {0, 0, 0, 0, 0, 0, 0, 0}};
   int m = N;
   const int order[7] = {8, 4, 2, 3, 5, 7, 11};
@@ -246,18 +253,27 @@ __host__ __device__ constexpr RadixList radices_of(int N) {
       L.r[L.n++] = order[i];
       m /= order[i];
     }
+  if (V & 2)
+    for (int a = 0, b = L.n - 1; a < b; ++a, --b) {
+      const int t = L.r[a];
+      L.r[a] = L.r[b];
+      L.r[b] = t;
+    }
   return L;
 }
-__host__ __device__ constexpr int chunk_lines(int N) {
-  RadixList L = radices_of(N);
+__host__ __device__ constexpr int values_of(int V) { return (V & 1) ? 16 : kMaxV; }
+__host__ __device__ constexpr int bpt_v(int r, int mv) { return (mv / r) > 0 ? (mv / r) : 1; }
+__host__ __device__ constexpr int chunk_lines(int N, int V = 0) {
+  RadixList L = radices_of(N, V);
   int lc = 1 << 30;
   for (int s = 0; s < L.n; ++s) {
-    int cap = (kPlaneThreads * bpt_of(L.r[s]) * L.r[s]) / N;
+    int cap = (kPlaneThreads * bpt_v(L.r[s], values_of(V)) * L.r[s]) / N;
     if (cap < 1) cap = 1;
     lc = lc < cap ? lc : cap;
   }
   return lc;
 }
+constexpr int kFftVariants = 3;
 
 // Line l of a transform lives at row (row0 + l) mod nrows of the buffer
 // (row0 = 0 and nrows above every line index: the identity).
@@ -266,10 +282,10 @@ __device__ __forceinline__ int line_row(int l, int row0, int nrows) {
   return r >= nrows ? r - nrows : r;
 }
 
-template <int N, int R, int NS, int LC, class C>
+template <int N, int R, int NS, int LC, int MV, class C>
 __device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, int es, bool jfast, const C* tw,
                                             typename CT<C>::R sgn, int row0, int nrows) {
-  constexpr int BPT = bpt_of(R);
+  constexpr int BPT = bpt_v(R, MV);
   constexpr int NQ = N / R;
   constexpr int TSTEP = N / (NS * R);
   // jfast: index space nl*NQ (line = bf / NQ); otherwise the full chunk LC*NQ
@@ -311,24 +327,24 @@ __device__ __forceinline__ void stage_fixed(C* buf, int line0, int nl, int ls, i
   __syncthreads();
 }
 
-template <int N, int S, int NS, int LC, class C>
+template <int N, int S, int NS, int LC, int V, class C>
 __device__ __forceinline__ void stages_fixed(C* buf, int line0, int nl, int ls, int es, bool jfast, const C* tw,
                                              typename CT<C>::R sgn, int row0, int nrows) {
-  constexpr RadixList L = radices_of(N);
+  constexpr RadixList L = radices_of(N, V);
   if constexpr (S < L.n) {
     constexpr int R = L.r[S];
-    stage_fixed<N, R, NS, LC>(buf, line0, nl, ls, es, jfast, tw, sgn, row0, nrows);
-    stages_fixed<N, S + 1, NS * R, LC>(buf, line0, nl, ls, es, jfast, tw, sgn, row0, nrows);
+    stage_fixed<N, R, NS, LC, values_of(V)>(buf, line0, nl, ls, es, jfast, tw, sgn, row0, nrows);
+    stages_fixed<N, S + 1, NS * R, LC, V>(buf, line0, nl, ls, es, jfast, tw, sgn, row0, nrows);
   }
 }
 
-template <int N, class C>
+template <int N, int V = 0, class C>
 __device__ void transform_fixed(C* buf, int nlines, int ls, int es, bool jfast, const C* tw, typename CT<C>::R sgn,
                                 int row0 = 0, int nrows = 1 << 30) {
-  constexpr int LC = chunk_lines(N);
+  constexpr int LC = chunk_lines(N, V);
   for (int l0 = 0; l0 < nlines; l0 += LC) {
     const int nl = min(LC, nlines - l0);
-    stages_fixed<N, 0, 1, LC>(buf, l0, nl, ls, es, jfast, tw, sgn, row0, nrows);
+    stages_fixed<N, 0, 1, LC, V>(buf, l0, nl, ls, es, jfast, tw, sgn, row0, nrows);
   }
 }
 
@@ -384,10 +400,10 @@ __device__ void transform(C* buf, const AxisArg& ax, int nlines, int ls, int es,
 
 // N > 0: the transform of compile-time length N, inlined alone into the
 // kernel (its registers then fit without spills); N == 0: run-time dispatch.
-template <int N, class C>
+template <int N, int V = 0, class C>
 __device__ __forceinline__ void xform(C* buf, const AxisArg& ax, int nlines, int ls, int es, bool jfast,
                                       const C* tw, typename CT<C>::R sgn) {
-  if constexpr (N > 0) transform_fixed<N>(buf, nlines, ls, es, jfast, tw, sgn);
+  if constexpr (N > 0) transform_fixed<N, V>(buf, nlines, ls, es, jfast, tw, sgn);
   else transform(buf, ax, nlines, ls, es, jfast, tw, sgn);
 }
 
@@ -395,10 +411,10 @@ __device__ __forceinline__ void xform(C* buf, const AxisArg& ax, int nlines, int
 // rows (y0 + l) mod nr2 for l < ny (the plane's rows form one range of signed
 // y).  The other rows are zero before the G->R transform and are not read
 // after the R->G transform.  Kernels with run-time lengths transform every row.
-template <int N, class C>
+template <int N, int V = 0, class C>
 __device__ __forceinline__ void xform_rows(C* buf, const AxisArg& ax, int y0, int ny, int nr2, int ls,
                                            const C* tw, typename CT<C>::R sgn) {
-  if constexpr (N > 0) transform_fixed<N>(buf, ny, ls, 1, false, tw, sgn, y0, nr2);
+  if constexpr (N > 0) transform_fixed<N, V>(buf, ny, ls, 1, false, tw, sgn, y0, nr2);
   else transform(buf, ax, nr2, ls, 1, false, tw, sgn);
 }
 
@@ -439,7 +455,7 @@ __device__ __forceinline__ int row_of(int i, int nr1) {
 // ---------------------------------------------------------------------------
 // The kernels take the work-grid type C (double2 or float2); the sphere
 // coefficients psi/out stay FP64 and are converted at the gather/scatter.
-template <class C, int N1, int N2>
+template <class C, int N1, int N2, int V>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_gtor_plane(const double2* __restrict__ psi, int ldg, int b0, const int* __restrict__ plane_off,
                  const int* __restrict__ plane_g, const int* __restrict__ plane_pos, const int2* __restrict__ plane_rows,
@@ -461,8 +477,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
     plane[plane_pos[k]] = from_d2<C>(src[plane_g[k]]);
   __syncthreads();
   const int2 rows = plane_rows[p];
-  xform_rows<N1>(plane, a1, rows.x, rows.y, nr2, ps, tw1, (typename CT<C>::R)1);  // x lines
-  xform<N2>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);               // y lines
+  xform_rows<N1, V>(plane, a1, rows.x, rows.y, nr2, ps, tw1, (typename CT<C>::R)1);  // x lines
+  xform<N2, V>(plane, a2, nr1, 1, ps, false, tw2, (typename CT<C>::R)1);               // y lines
   C* dst = grid + ((size_t)bl * nzp + p) * npl;
   for (int i = threadIdx.x; i < npl; i += blockDim.x) dst[i] = plane[i + row_of<N1>(i, nr1)];
 }
@@ -661,7 +677,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   }
 }
 
-template <class C, int N1, int N2>
+template <class C, int N1, int N2, int V>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_rtog_plane(const C* __restrict__ grid, int nzp, const int* __restrict__ plane_off,
                  const int* __restrict__ plane_g, const int* __restrict__ plane_pos,
@@ -681,9 +697,9 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   load_tw(tw1, tw1g, nr1, -1.0);
   load_tw(tw2, tw2g, nr2, -1.0);
   __syncthreads();
-  xform<N2>(plane, a2, nr1, 1, pst, false, tw2, (typename CT<C>::R)-1);  // y lines
+  xform<N2, V>(plane, a2, nr1, 1, pst, false, tw2, (typename CT<C>::R)-1);  // y lines
   const int2 rows = plane_rows[p];
-  xform_rows<N1>(plane, a1, rows.x, rows.y, nr2, pst, tw1, (typename CT<C>::R)-1);  // x lines
+  xform_rows<N1, V>(plane, a1, rows.x, rows.y, nr2, pst, tw1, (typename CT<C>::R)-1);  // x lines
   double2* dst = out + (size_t)ldg * b;
   const double2* ps = psi + (size_t)ldg * b;
   for (int k = plane_off[p] + threadIdx.x; k < plane_off[p + 1]; k += blockDim.x) {
@@ -773,7 +789,7 @@ bool plan_axis(int n, AxisPlan& p) {
 }  // namespace
 
 // out = FFT_RTOG[ V * FFT_GTOR[psi] ] (+ 1/2 G^2 psi + bucket psi when add_kinetic)
-template <class C, int N1, int N2, int N3>
+template <class C, int N1, int N2, int N3, int V>
 static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kinetic) {
   constexpr int TX = tx_of(N1, N3);
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
@@ -787,7 +803,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
   C* grid = reinterpret_cast<C*>(g.grid);
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
-    k_gtor_plane<C, N1, N2><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
+    k_gtor_plane<C, N1, N2, V><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(psi, h->ldg, b0, g.plane_off, g.plane_g,
                                                                            g.plane_pos, g.plane_rows, grid, h->nzp,
                                                                            a1, a2, g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
@@ -801,7 +817,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
                                                                        g.tw3, scale);
       CUW_LAUNCH_CHECK("k_zcol_v");
     }
-    k_rtog_plane<C, N1, N2><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
+    k_rtog_plane<C, N1, N2, V><<<dim3(h->nzp, nb), tp, smem_plane, h->stream>>>(grid, h->nzp, g.plane_off, g.plane_g,
                                                                       g.plane_pos, g.plane_rows, out, psi, h->ldg, b0, g.g2,
                                                                       g.bucket, add_kinetic ? 1 : 0, a1, a2,
                                                                       g.tw1, g.tw2);
@@ -813,7 +829,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
 
 // rho = sum over the bands of this set of f |psi(r)|^2 terms (WAVES_DENSITY
 // for TINV at Gamma), batch by batch through the work grid
-template <class C, int N1, int N2, int N3>
+template <class C, int N1, int N2, int N3, int V>
 static int fft_density_t(Handle* h, const double2* psi, double* rho) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   if (nr3 * kRhoTX > 8 * kPlaneThreads) return h->fail(CUW_ERR_UNSUPPORTED, "density: NR3 above 128");
@@ -825,7 +841,7 @@ static int fft_density_t(Handle* h, const double2* psi, double* rho) {
   const int nxb = (nr1 + kRhoTX - 1) / kRhoTX;
   for (int b0 = 0; b0 < h->d.nbh; b0 += h->batch) {
     const int nb = std::min(h->batch, h->d.nbh - b0);
-    k_gtor_plane<C, N1, N2><<<dim3(h->nzp, nb), kPlaneThreads, smem_plane, h->stream>>>(
+    k_gtor_plane<C, N1, N2, V><<<dim3(h->nzp, nb), kPlaneThreads, smem_plane, h->stream>>>(
         psi, h->ldg, b0, g.plane_off, g.plane_g, g.plane_pos, g.plane_rows, grid, h->nzp, a1, a2, g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
     k_zcol_rho<C, N3><<<nr2 * nxb, kPlaneThreads, smem_rho, h->stream>>>(grid, g.zslot, h->nzp, nr1, nr2, a3, g.tw3,
@@ -837,18 +853,55 @@ static int fft_density_t(Handle* h, const double2* psi, double* rho) {
 
 // kernels of work-grid type C and length N (0: any length): shared-memory
 // limits and the launcher
-template <class C, int N1, int N2, int N3>
-static int fft_select(Handle* h, int smem_plane) {
+template <class C, int N1, int N2, int N3, int V>
+static int fft_select_v(Handle* h, int smem_plane) {
   constexpr int TX = tx_of(N1, N3);
   const int smem_z = (int)(((size_t)h->d.nr3 * TX + h->d.nr3) * sizeof(C));
-  CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N1, N2>, smem_plane));
-  CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N1, N2>, smem_plane));
+  CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N1, N2, V>, smem_plane));
+  CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N1, N2, V>, smem_plane));
   if constexpr (N1 == 64 && N3 == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, z64_smem_bytes<C>()));
   else CUW_TRY(smem_allow((const void*)k_zcol_v<C, N3, TX>, smem_z));
   CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N3>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
-  h->fft_run = &fft_vpsi_t<C, N1, N2, N3>;
-  h->fft_rho = &fft_density_t<C, N1, N2, N3>;
+  h->fft_run = &fft_vpsi_t<C, N1, N2, N3, V>;
+  h->fft_rho = &fft_density_t<C, N1, N2, N3, V>;
   return CUW_OK;
+}
+// the plan variant h->fft_variant of a grid with compiled lengths (variant 0
+// for the kernels with run-time lengths)
+template <class C, int N1, int N2, int N3>
+static int fft_select(Handle* h, int smem_plane) {
+  if constexpr (N1 > 0) {
+    switch (h->fft_variant) {
+      case 1: return fft_select_v<C, N1, N2, N3, 1>(h, smem_plane);
+      case 2: return fft_select_v<C, N1, N2, N3, 2>(h, smem_plane);
+      default: break;
+    }
+  }
+  return fft_select_v<C, N1, N2, N3, 0>(h, smem_plane);
+}
+
+// Kernels of the handle's grid and plan variant: grids of the table get
+// kernels compiled for their lengths (every index divisor and Stockham stage a
+// constant); any other grid takes the kernels with run-time lengths.
+static int fft_choose(Handle* h) {
+  const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
+  const size_t es = h->mixed() ? sizeof(float2) : sizeof(double2);
+  const int smem_plane = (int)(((size_t)nr2 * plane_stride(nr1) + nr1 + nr2) * es);
+  int rc = CUW_OK;
+  bool found = false;
+#define CUW_FFT_GRID(A, B, Z)                                                                        \
+  if (!found && nr1 == A && nr2 == B && nr3 == Z) {                                                  \
+    found = true;                                                                                    \
+    rc = h->mixed() ? fft_select<float2, A, B, Z>(h, smem_plane) : fft_select<double2, A, B, Z>(h, smem_plane); \
+  }
+  CUW_FFT_GRIDS
+#undef CUW_FFT_GRID
+  h->fft_compiled = found;
+  if (!found) {
+    h->fft_variant = 0;
+    rc = h->mixed() ? fft_select<float2, 0, 0, 0>(h, smem_plane) : fft_select<double2, 0, 0, 0>(h, smem_plane);
+  }
+  return rc;
 }
 
 int fft_setup(Handle* h, const int* igvec) {
@@ -943,21 +996,7 @@ int fft_setup(Handle* h, const int* igvec) {
     CUW_TRY(cudaMalloc(tws[a], sizeof(double2) * n));
     CUW_TRY(cudaMemcpy(*tws[a], t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   }
-  const int smem_plane = (int)(plane_elems * es);
-  // grids of the table get kernels compiled for their lengths (every index
-  // divisor and Stockham stage a constant); any other grid takes the kernels
-  // with run-time lengths
-  int rc = CUW_OK;
-  bool found = false;
-#define CUW_FFT_GRID(A, B, Z)                                                                        \
-  if (!found && nr1 == A && nr2 == B && nr3 == Z) {                                                  \
-    found = true;                                                                                    \
-    rc = h->mixed() ? fft_select<float2, A, B, Z>(h, smem_plane) : fft_select<double2, A, B, Z>(h, smem_plane); \
-  }
-  CUW_FFT_GRIDS
-#undef CUW_FFT_GRID
-  if (!found) rc = h->mixed() ? fft_select<float2, 0, 0, 0>(h, smem_plane) : fft_select<double2, 0, 0, 0>(h, smem_plane);
-  return rc;
+  return fft_choose(h);
 }
 
 // 3-D transform of a full FP64 complex grid (x fastest), in place and
@@ -989,5 +1028,16 @@ int fft_density(Handle* h, const double2* psi, double* rho) {
   if (!h->fft_rho) return h->fail(CUW_ERR_STATE, "FFT not set up");
   return h->fft_rho(h, psi, rho);
 }
+
+// plan variant v (0 .. fft_variants()-1) of the compiled kernels; grids with
+// run-time lengths have variant 0 only
+int fft_set_variant(Handle* h, int v) {
+  if (!h->fft_run) return h->fail(CUW_ERR_STATE, "FFT not set up");
+  if (v < 0 || v >= kFftVariants || (v != 0 && !h->fft_compiled)) return CUW_ERR_UNSUPPORTED;
+  h->fft_variant = v;
+  h->touch();
+  return fft_choose(h);
+}
+int fft_variants(const Handle* h) { return h->fft_compiled ? kFftVariants : 1; }
 
 }  // namespace cuw

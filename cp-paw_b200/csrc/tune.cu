@@ -1,7 +1,9 @@
 // Autotuner of the launch shapes (no counterpart in the reference, whose FFTW
 // plans are chosen by FFTW's own planner at start-up, src/paw_library.f90,
-// LIB_FFTW3 2635-2728).  Three parameters of a handle are picked by timing the
+// LIB_FFTW3 2635-2728).  Four parameters of a handle are picked by timing the
 // real operations on its own data, on its own stream:
+//   - the FFT plan variant of the plane transforms (values per thread and
+//     stage, radix order; grids with compiled lengths) together with
 //   - the FFT band batch (bands transformed per launch sequence; the work grid
 //     is reallocated when a larger batch wins);
 //   - the split-K factor of the projections <p|psi> (FP64 DMMA or tcgen05);
@@ -28,6 +30,7 @@ namespace {
 using Shape = std::array<long long, 8>;
 struct Choice {
   int batch;
+  int fft_variant;
   double split_proj, split_gram;
   double ms[3];
 };
@@ -94,6 +97,7 @@ int autotune(Handle* h, double* out, int n) {
   h->touch();
   if (cached) {
     CUW_RET(grid_room(h, c.batch));
+    CUW_RET(fft_set_variant(h, c.fft_variant));
   } else {
     CUW_RET(eigr_compute(h, g.r0));
     // FFT band batch: the L2 rule's batch and even splits of the bands
@@ -104,19 +108,28 @@ int autotune(Handle* h, double* out, int n) {
     std::sort(cand.begin(), cand.end());
     cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
     c.batch = h->batch;
+    c.fft_variant = 0;
     c.ms[0] = 1e30;
-    for (int b : cand) {
-      if (per_band * b > ((size_t)256 << 20) && b != h->batch) continue;
-      if (grid_room(h, b) != CUW_OK) continue;
-      h->batch = b;
-      double ms = 0.0;
-      CUW_RET(time_best(h, [&] { return fft_vpsi(h, g.psi0, g.hpsi, true); }, 3, &ms));
-      if (ms < c.ms[0]) {
-        c.ms[0] = ms;
-        c.batch = b;
+    const int nv = fft_variants(h);
+    for (int v = 0; v < nv; ++v) {
+      CUW_RET(fft_set_variant(h, v));
+      for (int b : cand) {
+        if (per_band * b > ((size_t)256 << 20) && b != h->batch) continue;
+        if (grid_room(h, b) != CUW_OK) continue;
+        const int keep = h->batch;
+        h->batch = b;
+        double ms = 0.0;
+        CUW_RET(time_best(h, [&] { return fft_vpsi(h, g.psi0, g.hpsi, true); }, 3, &ms));
+        if (ms < c.ms[0]) {
+          c.ms[0] = ms;
+          c.batch = b;
+          c.fft_variant = v;
+        }
+        h->batch = keep;
       }
     }
     h->batch = c.batch;
+    CUW_RET(fft_set_variant(h, c.fft_variant));
     h->have_hpsi = false;
     // split-K factors
     const double muls[] = {0.5, 1.0, 1.5, 2.0, 3.0};
@@ -148,8 +161,9 @@ int autotune(Handle* h, double* out, int n) {
   h->split_proj = c.split_proj;
   h->split_gram = c.split_gram;
   h->touch();
-  const double v[7] = {(double)c.batch, c.split_proj, c.split_gram, c.ms[0], c.ms[1], c.ms[2], cached ? 1.0 : 0.0};
-  for (int i = 0; i < n && i < 7; ++i) out[i] = v[i];
+  const double v[8] = {(double)c.batch, c.split_proj, c.split_gram, c.ms[0], c.ms[1], c.ms[2], cached ? 1.0 : 0.0,
+                       (double)c.fft_variant};
+  for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
   return h->sync();
 }
 

@@ -23,6 +23,7 @@ CUW_OPT_LYAP_TOL = 1
 CUW_OPT_GRAPHS = 2
 CUW_OPT_LYAP_MAX_SWEEPS = 3
 CUW_OPT_SELFCONSISTENT = 4
+CUW_OPT_FFT_VARIANT = 5
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
@@ -442,10 +443,10 @@ class Waves:
         self._chk(self._f["set_option"](self.h, int(option), float(value)), "set_option")
 
     def autotune(self) -> dict:
-        """Times and fixes the FFT band batch and the split-K factors."""
-        out = np.zeros(7)
+        """Times and fixes the FFT plan variant and band batch and the split-K factors."""
+        out = np.zeros(8)
         self._chk(self._f["autotune"](self.h, _dptr(out), len(out)), "autotune")
-        keys = ("fft_batch", "split_proj", "split_gram", "fft_ms", "proj_ms", "gram_ms", "cached")
+        keys = ("fft_batch", "split_proj", "split_gram", "fft_ms", "proj_ms", "gram_ms", "cached", "fft_variant")
         return dict(zip(keys, out.tolist()))
 
     def graph_stats(self) -> tuple:

@@ -362,17 +362,24 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * EHARTREE + EXC, and out[5..7] = EHARTREE, EXC, int V rho.  Needs
  * cuwaves_set_rhoset and cuwaves_set_qlm first; 0 (default) keeps V fixed. */
 #define CUW_OPT_SELFCONSISTENT 4
+/* CUW_OPT_FFT_VARIANT: plan variant of the FFT plane transforms, 0 (default),
+ * 1 (16 values per thread and stage) or 2 (radix stages in ascending order);
+ * grids without compiled kernels accept 0 only (CUW_ERR_UNSUPPORTED).  The
+ * autotuner picks it by timing. */
+#define CUW_OPT_FFT_VARIANT 5
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);
 /* Autotuner (no reference counterpart; FFTW's planner picks the reference's
- * FFT plans): times the FFT band batch and the split-K factors of the
- * projections and plane-wave Gram products on this handle's data (G set, V,
- * DH, DO and PSI0/PSIM loaded) and keeps the fastest, in a process-wide table
- * keyed by the shape so that later handles of the same shape reuse it.
- * out[0..6] (n values): batch, projection split factor, Gram split factor,
- * their best times in ms, 1 if the choice came from the table.  Results move
- * at rounding level (another summation order). */
+ * FFT plans, src/paw_library.f90:2694-2697): times the FFT plan variant of the
+ * plane transforms (values per thread and stage, radix order; grids with
+ * compiled lengths) together with the FFT band batch, and the split-K factors
+ * of the projections and plane-wave Gram products, on this handle's data (G
+ * set, V, DH, DO and PSI0/PSIM loaded) and keeps the fastest, in a
+ * process-wide table keyed by the shape so that later handles of the same
+ * shape reuse it.  out[0..7] (n values): batch, projection split factor, Gram
+ * split factor, their best times in ms, 1 if the choice came from the table,
+ * FFT plan variant.  Results move at rounding level (another summation order). */
 int cuwaves_autotune(cuw_handle* h, double* out, int n);
 /* Check of the split-precision tensor-core product (no reference
  * counterpart): C(M,N) = A(M,K) * B(N,K)^T on device buffers, FP64 row-major

@@ -33,3 +33,38 @@ def test_autotune_keeps_results_and_caches_by_shape(inputs, prec):
         assert abs(o0[0] - o1[0]) < tol_e and np.abs(f0 - f1).max() < tol_f
     for w in ws:
         w.close()
+
+
+@pytest.mark.parametrize("prec", [CUW_PREC_FP64, CUW_PREC_MIXED])
+def test_fft_plan_variants_agree(inputs, prec, oracle):
+    """Every FFT plan variant the autotuner can pick gives H|psi> of the
+    oracle (FP64: 1e-10 relative; FP32 transforms: 1e-5), on a grid with
+    compiled kernels; the tuner reports the variant it kept; a grid without
+    compiled kernels refuses variants other than 0."""
+    inp = inputs["H2O2"]
+    w = cuwaves.open_waves(inp, precision=prec).setup().initialize()
+    cpu = oracle.open_oracle(inp).setup()
+    for which in (cuwaves.CUW_PSI0, cuwaves.CUW_PSIM):
+        cpu.upload_psi(which, w.download_psi(which))
+    cpu.set_proj(w.get_proj())
+    cpu.hpsi()
+    ref = cpu.download_psi(cuwaves.CUW_HPSI)
+    tol = 1e-10 if prec == CUW_PREC_FP64 else 1e-5
+    for v in range(3):
+        w.set_option(cuwaves.CUW_OPT_FFT_VARIANT, v)
+        w.hpsi()
+        got = w.download_psi(cuwaves.CUW_HPSI)
+        err = float(np.abs(got - ref).max() / np.abs(ref).max())
+        assert err < tol, f"variant {v}: {err:.2e}"
+    t = w.autotune()
+    assert t["fft_variant"] in (0.0, 1.0, 2.0)
+    w.close()
+    cpu.close()
+    odd = systems.build_inputs(systems.water_box(2, box=10.0, lattice=(2, 1, 1), epw_psi_ry=25.0,
+                                                 grid=(30, 30, 30)))
+    w2 = cuwaves.open_waves(odd, precision=prec).setup()
+    w2.set_option(cuwaves.CUW_OPT_FFT_VARIANT, 0)
+    with pytest.raises(cuwaves.WavesError) as e:
+        w2.set_option(cuwaves.CUW_OPT_FFT_VARIANT, 1)
+    assert e.value.code == 6
+    w2.close()
