@@ -833,6 +833,123 @@ __global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi
   }
 }
 
+// Persistent form of k_force for the projector table and NBH <= 64: the
+// force contraction has a short K (the bands), so a CTA per output tile spends
+// most of its time filling its pipeline.  Here CTA (gi, pj) keeps the DEDPRO
+// tile of projector tile pj (all K) resident in shared memory and walks the G
+// tiles gi, gi + gstride, ...: the psi rows of the next G tile are copied
+// (16-byte cp.async) while the current one is multiplied and its epilogue
+// runs, and the G-weighted sums of every projector accumulate in registers
+// over all the CTA's tiles.  fpart(gi, p, c) then holds the CTA's partial sum.
+constexpr int kFpSlices = 4;                 // K slices of BK (NBH <= 64)
+constexpr int kFpASlice = BK * LDR;          // double2 of one [k][row] psi slice
+constexpr size_t kFpSmem = sizeof(double2) * ((size_t)kFpSlices * TILE2 + 2 * (size_t)kFpSlices * kFpASlice);
+__global__ void __launch_bounds__(NT, 1) k_force_p(const double2* __restrict__ psi0, int ldg, int ngl, int nbh,
+                                                   int npro, const double2* __restrict__ ded,
+                                                   const double* __restrict__ gx, const double* __restrict__ gy,
+                                                   const double* __restrict__ gz, double* __restrict__ fpart,
+                                                   const double2* __restrict__ prox, int gstride) {
+  extern __shared__ double sm[];
+  __shared__ double fred[BN][3][2];
+  double2* bsm = reinterpret_cast<double2*>(sm);  // [slice][TILE2], DEDPRO (row = projector, k = band)
+  double2* asm_ = bsm + kFpSlices * TILE2;        // [buffer][slice][kFpASlice], psi (k = band, row = G)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp >> 2, wn = warp & 3;
+  const int gi = blockIdx.x, n0 = blockIdx.y * BN;
+  const int tm = (ngl + BM - 1) / BM;
+  const int nsl = (nbh + BK - 1) / BK;
+  // resident DEDPRO tile
+  for (int sl = 0; sl < nsl; ++sl)
+#pragma unroll
+    for (int q = 0; q < EPT; ++q) {
+      int row, kk;
+      tile_rc<true>(tid + q * NT, row, kk);
+      const int b = sl * BK + kk, pr = n0 + row;
+      cpa16(bsm + sl * TILE2 + toff<true>(row, kk), (b < nbh && pr < npro) ? ded + b + (size_t)nbh * pr : nullptr);
+    }
+  auto issue_a = [&](int t, int buf) {
+    const int m0 = t * BM;
+    for (int sl = 0; sl < nsl; ++sl)
+#pragma unroll
+      for (int q = 0; q < EPT; ++q) {
+        int row, kk;
+        tile_rc<false>(tid + q * NT, row, kk);
+        const int g = m0 + row, b = sl * BK + kk;
+        cpa16(asm_ + ((size_t)buf * kFpSlices + sl) * kFpASlice + toff<false>(row, kk),
+              (g < ngl && b < nbh) ? psi0 + (size_t)g + (size_t)ldg * b : nullptr);
+      }
+  };
+  if (gi < tm) issue_a(gi, 0);
+  cpa_commit();
+  double f[2][2][3];
+#pragma unroll
+  for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) f[ni][e][0] = f[ni][e][1] = f[ni][e][2] = 0.0;
+  int buf = 0;
+  for (int t = gi; t < tm; t += gstride, buf ^= 1) {
+    if (t + gstride < tm) issue_a(t + gstride, buf ^ 1);
+    cpa_commit();
+    cpa_wait<1>();  // this tile's psi rows (and the DEDPRO tile) have landed
+    __syncthreads();
+    Acc acc;
+    acc.zero();
+    for (int sl = 0; sl < nsl; ++sl)
+      mma_slice2<false, true, true>(acc, asm_ + ((size_t)buf * kFpSlices + sl) * kFpASlice, bsm + sl * TILE2, wm,
+                                    wn, lane, sl * BK, NoConj());
+    acc.finish();
+    const int m0 = t * BM;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int m, n;
+          acc_mn(wm, wn, lane, mi, ni, e, m, n);
+          const int g = m0 + m, p = n0 + n;
+          if (g < ngl && p < npro) {
+            // Re(i PRO(g,p) conj(dd))
+            const double2 pv = prox[(size_t)g + (size_t)ldg * p];
+            const double sv = -pv.y * acc.r[mi][ni][e] + pv.x * acc.i[mi][ni][e];
+            f[ni][e][0] += sv * gx[g];
+            f[ni][e][1] += sv * gy[g];
+            f[ni][e][2] += sv * gz[g];
+          }
+        }
+    __syncthreads();  // the buffer is free for the copies of the tile after next
+  }
+  cpa_wait<0>();
+  // reduce across the 8 lanes that share (lane & 3) (different g rows)
+#pragma unroll
+  for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double v = f[ni][e][c];
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        f[ni][e][c] = v;
+      }
+  if (lane < 4) {
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int n = wn * 16 + ni * 8 + 2 * lane + e;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fred[n][c][wm] = f[ni][e][c];
+      }
+  }
+  __syncthreads();
+  for (int i = tid; i < BN * 3; i += NT) {
+    int n = i / 3, c = i % 3;
+    int p = n0 + n;
+    if (p < npro) fpart[((size_t)gi * npro + p) * 3 + c] = fred[n][c][0] + fred[n][c][1];
+  }
+}
+
 // force(c, iat) = 2 * Omega * sum over g tiles and projectors of atom iat;
 // one block per (component, atom), fixed-order tree reduction
 __global__ void k_force_final(const double* __restrict__ fpart, int ntile, int npro, const int* __restrict__ ipro0,
@@ -1211,6 +1328,13 @@ int force_gemm(Handle* h, const double2* ded, double* force_dev) {
   double* fpart = reinterpret_cast<double*>(h->g.part);
   if (h->tc_on()) {
     CUW_RET(tc_force(h, ded, fpart, &tm));
+  } else if (!h->mixed() && h->g.prox && nbh <= kFpSlices * BK) {
+    // persistent: about one CTA per SM, each walking every gstride-th G tile
+    const int gstride = std::max(1, std::min(tm, h->nsm / tn));
+    k_force_p<<<dim3(gstride, tn), NT, kFpSmem, h->stream>>>(h->g.psi0, h->ldg, ngl, nbh, npro, ded, h->g.gx,
+                                                               h->g.gy, h->g.gz, fpart, h->g.prox, gstride);
+    CUW_LAUNCH_CHECK("k_force_p");
+    tm = gstride;
   } else {
     if (!h->mixed() && h->g.prox)
       k_force<true><<<dim3(tm, tn), NT, smem2_bytes<MP11>(), h->stream>>>(
@@ -1246,6 +1370,7 @@ int gemm_setup(Handle* h) {
   CUW_TRY(smem_allow((const void*)k_addx<true, true>, (int)smem2_bytes<MP11>()));
   CUW_TRY(smem_allow((const void*)k_force<false>, (int)smem2_bytes<MP11>()));
   CUW_TRY(smem_allow((const void*)k_force<true>, (int)smem2_bytes<MP11>()));
+  CUW_TRY(smem_allow((const void*)k_force_p, (int)kFpSmem));
   return CUW_OK;
 }
 
