@@ -1558,6 +1558,25 @@ extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
       if (rc == CUW_ERR_UNSUPPORTED) return h->fail(rc, "FFT plan variant not available for this grid");
       return rc;
     }
+    case CUW_OPT_STREAM_PRIORITY: {
+      if (value != 0.0 && value != 1.0) return h->fail(CUW_ERR_ARG, "STREAM_PRIORITY must be 0 or 1");
+      const int want = value != 0.0 ? 1 : 0;
+      if (want == h->stream_prio) return CUW_OK;
+      int least = 0, greatest = 0;
+      CUW_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      cudaStream_t s = nullptr;
+      CUW_TRY(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, want ? greatest : least));
+      if (cudaError_t e = cudaStreamSynchronize(h->stream); e != cudaSuccess) {
+        cudaStreamDestroy(s);
+        return h->fail(CUW_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
+      }
+      cudaStreamDestroy(h->stream);
+      h->stream = s;
+      h->stream_prio = want;
+      h->drop_graphs();
+      h->touch();
+      return CUW_OK;
+    }
     case CUW_OPT_SELFCONSISTENT:
       if (value != 0.0 && !(h->have_rhoset && h->have_qlm))
         return h->fail(CUW_ERR_STATE, "self-consistent steps need cuwaves_set_rhoset and cuwaves_set_qlm");

@@ -164,6 +164,7 @@ struct Handle {
   int (*fft_run)(Handle*, const double2*, double2*, bool) = nullptr;  // chosen by fft_setup
   int (*fft_rho)(Handle*, const double2*, double*) = nullptr;          // density, chosen by fft_setup
   int fft_variant = 0;        // plan variant of the compiled FFT kernels (autotuner)
+  int stream_prio = 0;        // 1: the stream has the device's highest priority
   bool fft_compiled = false;  // the grid has kernels compiled for its lengths
   size_t nr = 0;
   std::vector<double> occ_h;

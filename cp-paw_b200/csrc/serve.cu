@@ -124,6 +124,7 @@ size_t estimate_bytes(const cuw_dims& d, const int* isp) {
 
 // requests with at least this many CP steps replay their steps as CUDA graphs
 constexpr int kGraphSteps = 64;
+constexpr double kLongWork = 1e8;  // bands x plane waves x steps of a long request
 
 struct cuw_server {
   size_t budget = 0;
@@ -251,6 +252,10 @@ struct cuw_server {
       // only over long runs; on the serving mix of 20-step requests they
       // nearly halved the measured capacity (8.3 against 15-17 solves/s).
       cuwaves_set_option(j->h, CUW_OPT_GRAPHS, j->nsteps < kGraphSteps ? 0.0 : 1.0);
+      // the longest requests (bands x plane waves x steps at least kLongWork)
+      // set the latency tail: their kernels go first when SMs free up
+      const double work = (double)j->dims.nb * j->dims.ngl * std::max(1, j->nsteps);
+      cuwaves_set_option(j->h, CUW_OPT_STREAM_PRIORITY, work >= kLongWork ? 1.0 : 0.0);
       // PSIM starts equal to PSI0 (from rest): its Gram-Schmidt would repeat
       // PSI0's bit for bit, so WAVES$STOP copies it instead
       if ((rc = cuwaves_set_potential(j->h, in.v)) || (rc = cuwaves_set_dh(j->h, j->lmnxx, in.dh)) ||

@@ -24,6 +24,7 @@ CUW_OPT_GRAPHS = 2
 CUW_OPT_LYAP_MAX_SWEEPS = 3
 CUW_OPT_SELFCONSISTENT = 4
 CUW_OPT_FFT_VARIANT = 5
+CUW_OPT_STREAM_PRIORITY = 6
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}

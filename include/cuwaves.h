@@ -367,6 +367,11 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * grids without compiled kernels accept 0 only (CUW_ERR_UNSUPPORTED).  The
  * autotuner picks it by timing. */
 #define CUW_OPT_FFT_VARIANT 5
+/* CUW_OPT_STREAM_PRIORITY: 0 (default) or 1: the handle's work runs on a
+ * stream of the device's lowest or highest scheduling priority (the stream is
+ * replaced after the work in flight; results do not change).  The serving
+ * runtime gives its longest requests the high priority. */
+#define CUW_OPT_STREAM_PRIORITY 6
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);

@@ -180,3 +180,26 @@ def test_concurrent_sets_match_alone():
             assert mixed[i] is not None, spec
             for step, ((oa, fa), (om, fm)) in enumerate(zip(alone[i], mixed[i])):
                 assert np.array_equal(oa, om) and np.array_equal(fa, fm), (spec, step)
+
+
+def test_stream_priority_keeps_results(inputs):
+    """CUW_OPT_STREAM_PRIORITY replaces the handle's stream (after the work in
+    flight) and retires its step graphs; the steps give bit for bit the same
+    energies and forces on the high- and the low-priority stream."""
+    inp = inputs["Si8-20Ry"]
+    outs = []
+    for prio in (0, 1):
+        w = cuwaves.open_waves(inp, precision=CUW_PREC_MIXED).setup().initialize()
+        w.cp_step(move_atoms=True)
+        w.set_option(cuwaves.CUW_OPT_STREAM_PRIORITY, prio)
+        res = [w.cp_step(move_atoms=True) for _ in range(3)]
+        w.set_option(cuwaves.CUW_OPT_STREAM_PRIORITY, 1 - prio)
+        res.append(w.cp_step(move_atoms=True))
+        outs.append(res)
+        w.close()
+    for (o0, f0), (o1, f1) in zip(outs[0], outs[1]):
+        assert np.array_equal(o0, o1) and np.array_equal(f0, f1)
+    w = cuwaves.open_waves(inp).setup()
+    with pytest.raises(cuwaves.WavesError):
+        w.set_option(cuwaves.CUW_OPT_STREAM_PRIORITY, 2)
+    w.close()
