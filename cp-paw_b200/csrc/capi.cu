@@ -464,7 +464,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     h->npro += h->lmnx[s];
   }
   h->ldg = ceil_div(d.ngl, 32) * 32;
-  h->lyap_tol = d.precision == CUW_PREC_MIXED ? 1e-2 : 1e-6;
+  h->lyap_tol = d.precision == CUW_PREC_MIXED ? 1e-2 : 1e-5;
   h->nr = (size_t)d.nr1 * d.nr2 * d.nr3;
   h->occ_h.assign(d.nb, 0.0);
   int rc = CUW_OK;

@@ -341,7 +341,7 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
 /* Tuning options (no reference counterpart).
  * CUW_OPT_LYAP_TOL: relative accuracy to which every ORTHO_X iteration solves
  * its Lyapunov equation S X + X S = Gamma (the reference solves it exactly by
- * diagonalising S).  0 = to rounding; default 1e-6 (FP64) and 1e-2 (mixed
+ * diagonalising S).  0 = to rounding; default 1e-5 (FP64) and 1e-2 (mixed
  * precision).  The ORTHO_X loop itself still stops on
  * max|<psi|O|psi> - 1| < eps, so a looser inner solve changes the iteration
  * path, not the constraint that the result satisfies. */
