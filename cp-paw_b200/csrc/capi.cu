@@ -38,10 +38,23 @@ namespace {
 // ---------------------------------------------------------------------------
 constexpr int RB = 256;
 constexpr int RG = 2048;  // g per block
+__device__ void energy_final_block(int mode, const double* __restrict__ part, int nblk, const double* __restrict__ occ,
+                                   int nbh, double gweight, double dt2, int tbucket, double* __restrict__ out,
+                                   double* __restrict__ scalar, double* sh);
+// The last block of a k_band_sums launch to finish (counted on `count`, which
+// it resets) forms the scalar results (energy_final_block).
+struct BandFinal {
+  const double* occ;
+  double gweight, dt2;
+  int tbucket;
+  double* out;
+  double* scalar;
+  unsigned* count;
+};
 
 __global__ void k_band_sums(int mode, const double2* __restrict__ x, const double2* __restrict__ y, int ldg, int ngl,
                             const double* __restrict__ w1, const double* __restrict__ w2,
-                            const int* __restrict__ minusg, double* __restrict__ part, int nblk) {
+                            const int* __restrict__ minusg, double* __restrict__ part, int nblk, BandFinal fin) {
   const int b = blockIdx.y, blk = blockIdx.x;
   const double2* xb = x + (size_t)ldg * b;
   const double2* yb = y ? y + (size_t)ldg * b : nullptr;
@@ -81,21 +94,35 @@ __global__ void k_band_sums(int mode, const double2* __restrict__ x, const doubl
     __syncthreads();
   }
   if (threadIdx.x < 4) part[((size_t)b * nblk + blk) * 4 + threadIdx.x] = red[threadIdx.x][0];
+  if (!fin.count) return;
+  __shared__ bool last;
+  __threadfence();  // this block's partials before its count
+  if (threadIdx.x == 0) last = atomicAdd(fin.count, 1u) == gridDim.x * gridDim.y - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  extern __shared__ double fsh[];
+  energy_final_block(mode, part, nblk, fin.occ, gridDim.y, fin.gweight, fin.dt2, fin.tbucket, fin.out, fin.scalar,
+                     fsh);
+  if (threadIdx.x == 0) *fin.count = 0u;
 }
 
-// scalar results from band sums and occupations: the block sums the block
+// scalar results from band sums and occupations (the last block of
+// k_band_sums): the block sums the block
 // partials of every band (the order of the former two-kernel form), forms the
 // per-band terms in parallel, and thread 0 adds them in band order
 //   out[0] EKIN or WAVEKINETIC energy; out[1 + i] per-band values
-__global__ void k_energy_final(int mode, const double* __restrict__ part, int nblk, const double* __restrict__ occ,
-                               int nbh, double gweight, double dt2, int tbucket, double* __restrict__ out) {
-  extern __shared__ double sh[];
+//   scalar (when not null) also receives out[0]
+// The partials are read through L2: other blocks of the same launch wrote them.
+__device__ void energy_final_block(int mode, const double* __restrict__ part, int nblk, const double* __restrict__ occ,
+                                   int nbh, double gweight, double dt2, int tbucket, double* __restrict__ out,
+                                   double* __restrict__ scalar, double* sh) {
   double* res = sh;            // [4 nbh]
   double* term = sh + 4 * nbh;  // [nbh]
   for (int i = threadIdx.x; i < 4 * nbh; i += blockDim.x) {
     const int b = i / 4, k = i % 4;
     double s = 0.0;
-    for (int t = 0; t < nblk; ++t) s += part[((size_t)b * nblk + t) * 4 + k];
+    for (int t = 0; t < nblk; ++t) s += __ldcg(&part[((size_t)b * nblk + t) * 4 + k]);
     res[i] = s;
   }
   __syncthreads();
@@ -138,6 +165,7 @@ __global__ void k_energy_final(int mode, const double* __restrict__ part, int nb
     double e = 0.0;
     for (int b = 0; b < nbh; ++b) e += term[b];
     out[0] = (mode == 2) ? e : e * gweight;
+    if (scalar) scalar[0] = out[0];
   }
 }
 
@@ -212,27 +240,31 @@ __global__ void k_copy_psi(const double2* __restrict__ src, double2* __restrict_
 // ---------------------------------------------------------------------------
 // band reductions: results in h->g.scal (device): [0] energy, [1..nb] per band
 // ---------------------------------------------------------------------------
-static int band_sums_run(Handle* h, int mode, const double2* x, const double2* y, const double* w1, const double* w2) {
+// the band sums of mode over G, then (by the launch's last block) the scalar
+// results: out_dev[0] the energy, out_dev[1..] per band, scalar[0] (when not
+// null) the energy again
+static int band_sums_run(Handle* h, int mode, const double2* x, const double2* y, const double* w1, const double* w2,
+                         double* out_dev, double* scalar) {
   const int nblk = ceil_div(h->d.ngl, RG);
-  k_band_sums<<<dim3(nblk, h->d.nbh), RB, 0, h->stream>>>(mode, x, y, h->ldg, h->d.ngl, w1, w2, h->g.minusg,
-                                                          h->g.red, nblk);
+  const size_t sm = sizeof(double) * 5 * (size_t)h->d.nbh;
+  if (sm > 48 * 1024) CUW_TRY(smem_allow((const void*)k_band_sums, (int)sm));
+  Device& g = h->g;
+  BandFinal fin{g.occ, h->gweight, h->delt * h->delt, h->tbucket ? 1 : 0, out_dev, scalar,
+                reinterpret_cast<unsigned*>(g.red + 4 * (size_t)h->d.nbh * (nblk + 1))};
+  k_band_sums<<<dim3(nblk, h->d.nbh), RB, sm, h->stream>>>(mode, x, y, h->ldg, h->d.ngl, w1, w2, g.minusg, g.red,
+                                                           nblk, fin);
   CUW_LAUNCH_CHECK("k_band_sums");
   return CUW_OK;
 }
 
-// mode: RED_EKIN / RED_WAVEKIN / RED_EXPECT; result vector at out_dev
-static int energy_run(Handle* h, int mode, double* out_dev) {
+// mode: RED_EKIN / RED_WAVEKIN / RED_EXPECT; result vector at out_dev, the
+// energy also at scalar (when not null)
+static int energy_run(Handle* h, int mode, double* out_dev, double* scalar = nullptr) {
   Device& g = h->g;
-  if (mode == RED_EKIN) CUW_RET(band_sums_run(h, 0, g.psi0, nullptr, g.g2, h->tbucket ? g.bucket : nullptr));
-  else if (mode == RED_WAVEKIN) CUW_RET(band_sums_run(h, 1, g.psi0, g.psim, g.mpsi, nullptr));
-  else CUW_RET(band_sums_run(h, 2, g.psi0, g.hpsi, nullptr, nullptr));
-  const size_t sm = sizeof(double) * 5 * (size_t)h->d.nbh;
-  if (sm > 48 * 1024) CUW_TRY(smem_allow((const void*)k_energy_final, (int)sm));
-  k_energy_final<<<1, 256, sm, h->stream>>>(mode == RED_EKIN ? 0 : (mode == RED_WAVEKIN ? 1 : 2), g.red,
-                                            ceil_div(h->d.ngl, RG), g.occ, h->d.nbh, h->gweight, h->delt * h->delt,
-                                            h->tbucket ? 1 : 0, out_dev);
-  CUW_LAUNCH_CHECK("k_energy_final");
-  return CUW_OK;
+  if (mode == RED_EKIN)
+    return band_sums_run(h, 0, g.psi0, nullptr, g.g2, h->tbucket ? g.bucket : nullptr, out_dev, scalar);
+  if (mode == RED_WAVEKIN) return band_sums_run(h, 1, g.psi0, g.psim, g.mpsi, nullptr, out_dev, scalar);
+  return band_sums_run(h, 2, g.psi0, g.hpsi, nullptr, nullptr, out_dev, scalar);
 }
 
 cudaError_t smem_allow(const void* fn, int bytes) {
@@ -1018,16 +1050,14 @@ extern "C" int cuwaves_etot(cuw_handle* hp, double* out, double* force) {
   double* sc = g.scal;
   double* tmpv = g.scal + 8;
   h->nev = 0;
-  CUW_RET(energy_run(h, RED_EKIN, tmpv));
-  CUW_TRY(cudaMemcpyAsync(sc + 0, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(energy_run(h, RED_EKIN, tmpv, sc + 0));
   CUW_RET(eigr_compute(h, g.r0));
   if (force) CUW_RET(force_dev_run(h, g.force));
   CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
   CUW_RET(hproj_compute(h, g.proj, g.hproj));
   CUW_RET(addpro_run(h, ADDPRO_HPSI, g.hproj, g.oproj));
   h->have_hpsi = true;
-  CUW_RET(energy_run(h, RED_EXPECT, tmpv));
-  CUW_TRY(cudaMemcpyAsync(sc + 1, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(energy_run(h, RED_EXPECT, tmpv, sc + 1));
   double hs[2];
   CUW_TRY(cudaMemcpyAsync(hs, sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
   if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
@@ -1045,10 +1075,8 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   double* sc = g.scal;  // [0] ekin [1] etot [2] ekin1 [3] ekin2 [4] eion ; per-band scratch after 8
   double* tmpv = g.scal + 8;
   CUW_RET(mark(h, PH_RED));
-  CUW_RET(energy_run(h, RED_EKIN, tmpv));
-  CUW_TRY(cudaMemcpyAsync(sc + 0, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
-  CUW_TRY(cudaMemcpyAsync(sc + 2, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(energy_run(h, RED_EKIN, tmpv, sc + 0));
+  CUW_RET(energy_run(h, RED_WAVEKIN, tmpv, sc + 2));
   CUW_RET(mark(h, PH_EIGR));
   CUW_RET(eigr_compute(h, g.r0));
   if (h->scf) {
@@ -1071,8 +1099,7 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   CUW_RET(oproj_compute(h, g.proj, g.oproj));
   CUW_RET(addpro_run(h, ADDPRO_FUSED, g.hproj, g.oproj));
   CUW_RET(mark(h, PH_RED));
-  CUW_RET(energy_run(h, RED_EXPECT, tmpv));
-  CUW_TRY(cudaMemcpyAsync(sc + 1, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(energy_run(h, RED_EXPECT, tmpv, sc + 1));
   CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
     if (h->eigr_src == g.rp) h->eigr_src = nullptr;  // R(+) is rewritten
@@ -1082,8 +1109,7 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   }
   CUW_RET(ortho_core(h, max_iter, eps));
   CUW_RET(mark(h, PH_RED));
-  CUW_RET(energy_run(h, RED_WAVEKIN, tmpv));
-  CUW_TRY(cudaMemcpyAsync(sc + 3, tmpv, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUW_RET(energy_run(h, RED_WAVEKIN, tmpv, sc + 3));
   CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
     k_ion_ekin<<<1, 128, sizeof(double) * 3 * h->d.nat, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
