@@ -23,6 +23,9 @@ int jacobi_run(Handle* h, const double* s_dev, double* u, double* e, const int* 
 int lambda_init_run(Handle* h);
 int store_lambda_run(Handle* h);
 int ortho_y_run(Handle* h, const double* s, double* x);
+int ortho_y_general(Handle* h, const double* s1, const double* s2, const double* s3, const int* map, double* x,
+                    bool clear_status);
+int smap_run(Handle* h);
 int fold_x_run(Handle* h, const double* x, double2* x1, double2* x2);
 
 namespace {
@@ -172,15 +175,38 @@ __device__ void energy_final_block(int mode, const double* __restrict__ part, in
 // WAVES$PROPAGATE (src/paw_waves1.f90:6575-6583)
 __global__ void k_propagate(const double2* __restrict__ psi0, double2* __restrict__ psim,
                             const double2* __restrict__ hpsi, const double* __restrict__ mpsi, int ldg, int ngl,
-                            int nbh, double a1, double a2, double a3) {
+                            int nbh, double a1, double a2, double a3, const double* __restrict__ fr, double dt2) {
   size_t n = (size_t)ldg * nbh;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     int g = (int)(k % ldg);
     if (g >= ngl) continue;
-    double c = a3 / mpsi[g];
+    double b1 = a1, b2 = a2, c = a3 / mpsi[g];
+    if (fr) {  // ARR1..ARR3 of ANNEEVEC (src/paw_waves1.f90:6536-6540)
+      const double an = 1.0 + fr[g];
+      b1 = 2.0 / an;
+      b2 = 1.0 - b1;
+      c = -dt2 / an / mpsi[g];
+    }
     double2 p0 = psi0[k], pm = psim[k], hv = hpsi[k];
-    psim[k] = make_double2(a1 * p0.x + a2 * pm.x + c * hv.x, a1 * p0.y + a2 * pm.y + c * hv.y);
+    psim[k] = make_double2(b1 * p0.x + b2 * pm.x + c * hv.x, b1 * p0.y + b2 * pm.y + c * hv.y);
   }
+}
+
+// ANNEEVEC(G) of WAVES_DMPSI with TSTRESS (src/paw_waves1.f90:6694-6709);
+// f = FRICMAT(3,3) in Fortran order
+struct Fric {
+  double f[9];
+};
+__global__ void k_anneevec(const double* __restrict__ gx, const double* __restrict__ gy,
+                           const double* __restrict__ gz, const double* __restrict__ dbucket, int ngl, Fric fm,
+                           double fac1, double fac2, double* __restrict__ anv) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngl) return;
+  const double* F = fm.f;
+  const double x = gx[g], y = gy[g], z = gz[g];
+  const double svar = F[0] * x * x + F[3] * 2.0 * x * y + F[6] * 2.0 * x * z + F[4] * y * y + F[7] * 2.0 * y * z +
+                      F[8] * z * z;
+  anv[g] = fac1 + fac2 * svar * (1.0 + (dbucket ? dbucket[g] : 0.0));
 }
 
 // DEDPROJ = F1 HPROJ + F2 conj(HPROJ) per super wave function (src/paw_waves1.f90:5644-5668)
@@ -292,10 +318,26 @@ int band_reduce(Handle* h, int what, double* out_host, double* eig_host) {
   return CUW_OK;
 }
 
+// ANNEEVEC of the cell friction for the present ANNEE and G set
+static int friction_update(Handle* h) {
+  if (!h->fric_on || !h->have_gset) return CUW_OK;
+  const double* F = h->fricmat;
+  const double fac1 = h->annee - 0.5 * (F[0] + F[4] + F[8]);
+  const double fac2 = -0.5 * h->emass * 2.0 * h->emasscg2;
+  Fric fm;
+  std::memcpy(fm.f, F, sizeof(fm.f));
+  k_anneevec<<<ceil_div(h->d.ngl, 256), 256, 0, h->stream>>>(h->g.gx, h->g.gy, h->g.gz,
+                                                             h->have_dbucket ? h->g.dbucket : nullptr, h->d.ngl,
+                                                             fm, fac1, fac2, h->g.anv);
+  CUW_LAUNCH_CHECK("k_anneevec");
+  return CUW_OK;
+}
+
 int propagate_run(Handle* h) {
   const double a1 = 2.0 / (1.0 + h->annee), a2 = 1.0 - a1, a3 = -h->delt * h->delt / (1.0 + h->annee);
   k_propagate<<<4 * h->nsm, 256, 0, h->stream>>>(h->g.psi0, h->g.psim, h->g.hpsi, h->g.mpsi, h->ldg, h->d.ngl,
-                                                 h->d.nbh, a1, a2, a3);
+                                                 h->d.nbh, a1, a2, a3, h->fric_on ? h->g.anv : nullptr,
+                                                 h->delt * h->delt);
   CUW_LAUNCH_CHECK("k_propagate");
   return CUW_OK;
 }
@@ -351,8 +393,17 @@ static int ortho_core(Handle* h, int max_iter, double eps) {
   guard.h = nullptr;
   CUW_RET(unravel_run(h, pw, oc, 3, g.mat, g.omat, g.oomat));
   CUW_RET(mark(h, 7));
-  CUW_RET(lambda_init_run(h));
-  CUW_RET(ortho_solve(h, max_iter, eps));
+  if (h->safeortho) {
+    CUW_RET(lambda_init_run(h));
+    CUW_RET(ortho_solve(h, max_iter, eps));
+  } else {
+    // SAFEORTHO = F (src/paw_waves2.f90:306-346, 384-386): WAVES_ORTHO_Y_C of
+    // MAT, OMAT, OOMAT gives LAMBDA directly (its X is INTENT(OUT), so the
+    // symmetrised and occupation-scaled RLAM0 of the other branch is unused);
+    // the state order SMAP follows the RLAM0 diagonal when SWAPSTATES = T
+    if (h->swapstates) CUW_RET(smap_run(h));
+    CUW_RET(ortho_y_general(h, g.mat, g.omat, g.oomat, h->swapstates ? g.smap : nullptr, g.lam, !h->swapstates));
+  }
   CUW_RET(mark(h, 8));
   CUW_RET(lambda12_run(h, g.lam, g.lam1c, g.lam2c));
   CUW_RET(addopsi_run(h, g.psim, g.opsi, g.lam1c, g.lam2c));
@@ -422,11 +473,11 @@ static void free_all(Handle* h) {
                   g.minusg, g.gx, g.gy, g.gz, g.g2, g.pro, g.ylm, g.mpsi, g.bucket, g.pdesc, g.plane_iz, g.plane_rows, g.plane_off,
                   g.plane_g, g.plane_pos, g.zslot, g.v, g.grid, g.tw1, g.tw2, g.tw3, g.r0, g.rp, g.rm, g.force, g.mass,
                   g.eigr, g.dh, g.dover, g.occ, g.mat, g.omat, g.oomat, g.lam, g.lam2, g.lam0, g.u, g.u2, g.eig, g.haux, g.gamn,
-                  g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
+                  g.work, g.wk2, g.smat, g.emat, g.gt, g.xb, g.tb, g.maxpart, g.ostatus, g.smap, g.lam1c, g.lam2c, g.part, g.red, g.scal, g.tmat, g.t_ipro0,
                   g.t_nlmn, g.t_isp, g.t_lnofp, g.t_mofp, g.t_lmn0ln, g.t_lox, g.pf, g.xminus[0], g.xminus[1], g.bpre[0],
                   g.bpre[1], g.bsmall, g.jac_a, g.r_plus, g.r_minus, g.r_gx, g.r_gy, g.r_gz, g.r_g2, g.r_ylm,
                   g.r_g0, g.r_v0, g.r_pscore, g.r_vbar, g.r_lmrx, g.qlm, g.r_rhog, g.r_vg, g.r_pot, g.r_vtot,
-                  g.r_grid, g.r_part, g.fpot, g.vqlm, g.r_out, g.prox};
+                  g.r_grid, g.r_part, g.fpot, g.vqlm, g.r_out, g.prox, g.anv, g.dbucket};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   h->g = Device();
@@ -535,7 +586,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
     TRYA(g.work, sizeof(double) * nn); TRYA(g.wk2, sizeof(double) * nn);
     TRYA(g.smat, sizeof(double) * nn); TRYA(g.emat, sizeof(double) * nn); TRYA(g.gt, sizeof(double) * nn);
     TRYA(g.xb, sizeof(double) * nn); TRYA(g.tb, sizeof(double) * nn);
-    TRYA(g.maxpart, sizeof(double) * 64); TRYA(g.ostatus, sizeof(int) * 16);
+    TRYA(g.maxpart, sizeof(double) * 64); TRYA(g.ostatus, sizeof(int) * 16); TRYA(g.smap, sizeof(int) * d.nb);
     TRYA(g.lam1c, sizeof(double2) * mn); TRYA(g.lam2c, sizeof(double2) * mn);
     TRYA(g.tmat, sizeof(double2) * 12 * mn);
     TRYA(g.red, sizeof(double) * (4 * (size_t)d.nbh * (ceil_div(d.ngl, RG) + 1) + 8));
@@ -664,7 +715,7 @@ extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* min
   }
   CUW_RET(fft_setup(h, igvec));
   h->have_gset = true;
-  return CUW_OK;
+  return friction_update(h);
 }
 
 extern "C" int cuwaves_set_potential(cuw_handle* hp, const double* v) {
@@ -751,7 +802,33 @@ extern "C" int cuwaves_set_dynamics(cuw_handle* hp, double delt, double annee) {
   NEED(delt > 0.0 && annee > -1.0, CUW_ERR_ARG, "DELT must be positive and ANNEE > -1");
   h->delt = delt;
   h->annee = annee;
-  return CUW_OK;
+  return friction_update(h);
+}
+
+extern "C" int cuwaves_set_cell_friction(cuw_handle* hp, const double* fricmat, double emass, double emasscg2,
+                                         const double* dbucket) {
+  H(hp);
+  h->touch();
+  NEED(h->have_gset, CUW_ERR_STATE, "cuwaves_set_gset first");
+  if (!fricmat) {
+    h->fric_on = false;
+    return CUW_OK;
+  }
+  for (int i = 0; i < 9; ++i) NEED(std::isfinite(fricmat[i]), CUW_ERR_ARG, "FRICMAT must be finite");
+  NEED(std::isfinite(emass) && std::isfinite(emasscg2), CUW_ERR_ARG, "EMASS and EMASSCG2 must be finite");
+  Device& g = h->g;
+  const size_t nb = sizeof(double) * h->d.ngl;
+  if (!g.anv) CUW_TRY(cudaMalloc(&g.anv, nb));
+  if (dbucket) {
+    if (!g.dbucket) CUW_TRY(cudaMalloc(&g.dbucket, nb));
+    CUW_TRY(cudaMemcpy(g.dbucket, dbucket, nb, cudaMemcpyHostToDevice));
+  }
+  h->have_dbucket = dbucket != nullptr;
+  std::memcpy(h->fricmat, fricmat, sizeof(h->fricmat));
+  h->emass = emass;
+  h->emasscg2 = emasscg2;
+  h->fric_on = true;
+  return friction_update(h);
 }
 
 static double2* psi_ptr(Handle* h, int which) {
@@ -1603,6 +1680,14 @@ extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
       h->touch();
       return CUW_OK;
     }
+    case CUW_OPT_SAFEORTHO:
+      if (value != 0.0 && value != 1.0) return h->fail(CUW_ERR_ARG, "SAFEORTHO must be 0 or 1");
+      h->safeortho = value != 0.0;
+      return CUW_OK;
+    case CUW_OPT_SWAPSTATES:
+      if (value != 0.0 && value != 1.0) return h->fail(CUW_ERR_ARG, "SWAPSTATES must be 0 or 1");
+      h->swapstates = value != 0.0;
+      return CUW_OK;
     case CUW_OPT_SELFCONSISTENT:
       if (value != 0.0 && !(h->have_rhoset && h->have_qlm))
         return h->fail(CUW_ERR_STATE, "self-consistent steps need cuwaves_set_rhoset and cuwaves_set_qlm");

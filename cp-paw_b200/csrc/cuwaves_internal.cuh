@@ -112,6 +112,8 @@ struct Device {
   double *smat = nullptr, *emat = nullptr, *gt = nullptr, *xb = nullptr, *tb = nullptr;
   double *maxpart = nullptr;
   int *ostatus = nullptr;        // [0] status, [1] iterations
+  int *smap = nullptr;           // (NB) state order of WAVES_ORTHO_Y_C (SAFEORTHO = F, SWAPSTATES = T)
+  double *anv = nullptr, *dbucket = nullptr;  // (NGL) ANNEEVEC and GSET%DBUCKET of the cell friction
   double2 *lam1c = nullptr, *lam2c = nullptr;  // (NBH, NBH) folded multipliers
   double2 *tmat = nullptr;       // 12 (NBH, NBH) reduced Gram products
   // scratch for split-K partial sums and band reductions
@@ -216,6 +218,14 @@ struct Handle {
   // (1e-8 Ha/atom) and the forces by 1e-8 Ha/bohr with 16% of the sweeps, far
   // inside the mixed path's own error.
   double lyap_tol = 0.0;
+  // WAVES$ORTHOGONALIZE branch (src/paw_waves1.f90:221-222): SAFEORTHO = T runs
+  // WAVES_ORTHO_X, F runs WAVES_ORTHO_Y_C, in the order of the RLAM0 diagonal
+  // when SWAPSTATES = T
+  bool safeortho = true, swapstates = false;
+  // cell friction of WAVES$PROPAGATE (cuwaves_set_cell_friction)
+  bool fric_on = false, have_dbucket = false;
+  double fricmat[9] = {0};
+  double emass = 0.0, emasscg2 = 0.0;
   int lyap_max_sweeps = 64;  // sweeps per Lyapunov solve before the fixed point counts as failed
   bool ortho_panel = true;   // ORTHO_X by the panel-staged cluster kernel where it applies (64 < NB <= 128)
   bool tc_scope_open = false;
@@ -291,6 +301,11 @@ __device__ __forceinline__ double2 pro_value(int g, int ngl, const ProDesc& d, c
 // coefficients of the fused ADDPRO epilogues (see k_addpro)
 struct StepCoef {
   double a1, a2, a3, oscale;
+  // G-dependent friction of a moving cell (ANNEEVEC(G), src/paw_waves1.f90:
+  // 6536-6540) or null; with it the propagation coefficients are formed per G
+  // from fr[g] and dt2 = DELT^2 instead of a1, a2, a3
+  const double* fr = nullptr;
+  double dt2 = 0.0;
 };
 
 // FP64 tensor-core MMA, m8n8k4, A row-major / B column-major fragments:

@@ -586,8 +586,14 @@ __global__ void __launch_bounds__(NT, 1) k_addpro(double2* __restrict__ hpsi, do
         }
         if (MODE == ADDPRO_FUSED) {
           double2 p0 = psi0[k], pm = psim[k];
-          double a3 = sc.a3 / mpsi[g];
-          psim[k] = make_double2(sc.a1 * p0.x + sc.a2 * pm.x + a3 * hv.x, sc.a1 * p0.y + sc.a2 * pm.y + a3 * hv.y);
+          double a1 = sc.a1, a2 = sc.a2, a3 = sc.a3 / mpsi[g];
+          if (sc.fr) {  // cell friction ANNEEVEC(G) (src/paw_waves1.f90:6536-6540)
+            const double an = 1.0 + sc.fr[g];
+            a1 = 2.0 / an;
+            a2 = 1.0 - a1;
+            a3 = -sc.dt2 / an / mpsi[g];
+          }
+          psim[k] = make_double2(a1 * p0.x + a2 * pm.x + a3 * hv.x, a1 * p0.y + a2 * pm.y + a3 * hv.y);
         }
       }
 }
@@ -1123,6 +1129,8 @@ int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc) {
   sc.a2 = 1.0 - sc.a1;
   sc.a3 = -h->delt * h->delt / (1.0 + h->annee);
   sc.oscale = h->delt * h->delt / (1.0 + h->annee);  // src/paw_waves2.f90:148-156
+  sc.fr = h->fric_on ? h->g.anv : nullptr;
+  sc.dt2 = h->delt * h->delt;
   if (h->tc_on()) return tc_addpro(h, mode, hpc, opc, sc);
   Device& g = h->g;
   const bool tab = !h->mixed() && g.prox;

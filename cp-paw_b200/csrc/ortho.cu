@@ -1358,25 +1358,34 @@ __global__ void k_switch_lambda(double2* __restrict__ rlam0, double2* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// WAVES_ORTHO_Y_C with PHIPHI = CHIPHI = CHICHI = S (real) and MAP = identity
-// (src/paw_waves2.f90:1025-1338), as one cluster of kOyCS CTAs.  A, B, C,
-// ALPHA and X are n x n in global memory (L2).  Step nu of the sequential
-// orthogonalisation has three parts, each ended by a cluster barrier:
+// WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338) for real (Gamma-point)
+// PHIPHI, CHIPHI, CHICHI and the state order MAP (identity when map is null),
+// as one cluster of kOyCS CTAs.  WAVES_GRAMSCHMIDT (:2025-2177) passes one
+// matrix S as all three; WAVES$ORTHOGONALIZE with SAFEORTHO = F (:361-386)
+// passes MAT, OMAT and OOMAT.  A, B, C, ALPHA and X are n x n in global
+// memory (L2).  pos[i] is the place of state i in MAP: "J > N in the order"
+// of the reference is pos[j] > nu.  Step nu (pivot N = MAP(nu)) of the
+// sequential orthogonalisation has three parts, each ended by a cluster
+// barrier:
 //   1. CTA 0 forms the step's scalar and the column/row updates of X, A and B
-//      along index nu (vectors of n, block barriers only);
+//      along index N (vectors of n, block barriers only);
 //   2. every CTA copies what the rank-one updates read into its shared memory
-//      (row nu of B, columns nu of ALPHA and C, row nu of C) and forms the two
-//      coefficient vectors z1 (from column nu of A) and z2 (from column nu of
+//      (row N of B, columns N of ALPHA and C, row N of C) and forms the two
+//      coefficient vectors z1 (from column N of A) and z2 (from column N of
 //      B, which part 3 does not change);
 //   3. every CTA updates its share of the n x n elements of A, X, B, ALPHA
 //      and C from those copies.  The two B updates of an element are applied
-//      in the reference's order, the second with row nu of B as the first left
+//      in the reference's order, the second with row N of B as the first left
 //      it; the C update reads the copied row and column instead of a work array.
 // The arithmetic of each element is that of the one-CTA form.
 // ---------------------------------------------------------------------------
 constexpr int kOyCS = 8;
-__global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, int n, double* A, double* B, double* C,
-                                                  double* AL, double* X, int* __restrict__ status) {
+// ostatus[0] of a state order that failed its check (mapped by ortho_result)
+constexpr int kStatusOrder = 100;
+__global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s1, const double* __restrict__ s2,
+                                                  const double* __restrict__ s3, const int* __restrict__ map,
+                                                  int n, double* A, double* B, double* C, double* AL, double* X,
+                                                  int* __restrict__ status) {
   extern __shared__ double oysm[];
   double* z1 = oysm;        // coefficients of the phi step
   double* z2 = z1 + n;      // coefficients of the chi step
@@ -1385,6 +1394,7 @@ __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, 
   double* alcol = brow2 + n;  // ALPHA(i, nu)
   double* ccol = alcol + n;   // C(i, nu)
   double* crow = ccol + n;    // C(nu, j)
+  int* pos = reinterpret_cast<int*>(crow + n);  // place of each state in MAP
   __shared__ double zn;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
@@ -1394,16 +1404,17 @@ __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, 
   const size_t nn = (size_t)n * n;
   for (size_t k = gt; k < nn; k += gstride) {
     int i = (int)(k % n), j = (int)(k / n);
-    A[k] = s[k] - (i == j ? 1.0 : 0.0);
-    B[k] = s[k];
-    C[k] = s[k];
+    A[k] = s1[k] - (i == j ? 1.0 : 0.0);
+    B[k] = s2[k];
+    C[k] = s3[k];
     X[k] = 0.0;
     AL[k] = (i == j) ? 1.0 : 0.0;
   }
+  for (int k = tid; k < n; k += nt) pos[map ? map[k] : k] = k;
   cl.sync();
   auto I = [n](int i, int j) { return (size_t)i + (size_t)n * j; };
   for (int nu = 0; nu < n; ++nu) {
-    const int nn0 = nu;
+    const int nn0 = map ? map[nu] : nu;
     // ---- part 1: CTA 0
     if (rank == 0) {
       if (tid == 0) {
@@ -1436,37 +1447,38 @@ __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s, 
     const double bnn = B[I(nn0, nn0)] + r8small;
     const double cnn = C[I(nn0, nn0)];
     for (int i = tid; i < n; i += nt) {
-      z1[i] = (i > nu) ? -(A[I(i, nn0)] / bnn) : 0.0;
-      z2[i] = (i > nu) ? -(B[I(i, nn0)] / bnn) : 0.0;
+      z1[i] = (pos[i] > nu) ? -(A[I(i, nn0)] / bnn) : 0.0;
+      z2[i] = (pos[i] > nu) ? -(B[I(i, nn0)] / bnn) : 0.0;
       brow[i] = B[I(nn0, i)];
       alcol[i] = AL[I(i, nn0)];
       ccol[i] = C[I(i, nn0)];
       crow[i] = C[I(nn0, i)];
     }
     __syncthreads();
-    for (int j = tid; j < n; j += nt) brow2[j] = (j > nu) ? brow[j] + ccol[nn0] * z1[j] : brow[j];
+    for (int j = tid; j < n; j += nt) brow2[j] = (pos[j] > nu) ? brow[j] + ccol[nn0] * z1[j] : brow[j];
     // every CTA has read the columns and rows before any CTA changes them
     cl.sync();
     // ---- part 3: the CTA's share of the n x n elements
     for (size_t k = gt; k < nn; k += gstride) {
       const int i = (int)(k % n), j = (int)(k / n);
+      const bool hi = pos[i] > nu, hj = pos[j] > nu;
       // orthogonalise higher phis to this phi
-      if (j > nu) X[k] += alcol[i] * z1[j];
+      if (hj) X[k] += alcol[i] * z1[j];
       double add = 0.0;
-      if (i > nu) add += z1[i] * brow[j];
-      if (j > nu) add += brow[i] * z1[j];
-      if (i > nu && j > nu) add += z1[i] * cnn * z1[j];
+      if (hi) add += z1[i] * brow[j];
+      if (hj) add += brow[i] * z1[j];
+      if (hi && hj) add += z1[i] * cnn * z1[j];
       A[k] += add;
       double b = B[k];
-      if (j > nu) b += ccol[i] * z1[j];
+      if (hj) b += ccol[i] * z1[j];
       // orthogonalise higher chis to this phi
-      if (j > nu) AL[k] += alcol[i] * z2[j];
-      if (i > nu) b += z2[i] * brow2[j];
+      if (hj) AL[k] += alcol[i] * z2[j];
+      if (hi) b += z2[i] * brow2[j];
       B[k] = b;
       double wv = 0.0;
-      if (i > nu) wv += z2[i] * crow[j];
-      if (j > nu) wv += ccol[i] * z2[j];
-      if (i > nu && j > nu) wv += z2[i] * cnn * z2[j];
+      if (hi) wv += z2[i] * crow[j];
+      if (hj) wv += ccol[i] * z2[j];
+      if (hi && hj) wv += z2[i] * cnn * z2[j];
       C[k] += wv;
     }
     cl.sync();
@@ -1742,6 +1754,8 @@ int ortho_result(Handle* h, const int* st, int* iters) {
   if (iters) *iters = st[1];
   if (st[0] == CUW_ERR_NOT_CONVERGED) return h->fail(st[0], "LOOP FOR ORTHOGONALIZATION IS NOT CONVERGED");
   if (st[0] == CUW_ERR_DIVERGED) return h->fail(st[0], "ITERATION LOOP FOR ORTHOGONALIZATION IS ABOUT TO DIVERGE");
+  if (st[0] == CUW_ERR_NAN) return h->fail(st[0], "NAN DETECTED in WAVES_ORTHO_Y_C");
+  if (st[0] == kStatusOrder) return h->fail(CUW_ERR_STATE, "STATE ORDERING FAILED");
   if (st[0] != CUW_OK) return h->fail(CUW_ERR_STATE, "orthogonalisation failed");
   return CUW_OK;
 }
@@ -1768,13 +1782,17 @@ int switch_lambda_run(Handle* h) {
   return CUW_OK;
 }
 
-int ortho_y_run(Handle* h, const double* s, double* x) {
+// WAVES_ORTHO_Y_C of s1 (PHIPHI), s2 (CHIPHI), s3 (CHICHI) in the state order
+// map (null: identity) into x; status word ostatus[0] becomes CUW_ERR_NAN on a
+// NaN.  clear_status = false keeps a status set earlier in the same solve.
+int ortho_y_general(Handle* h, const double* s1, const double* s2, const double* s3, const int* map, double* x,
+                    bool clear_status) {
   const int n = h->d.nb;
-  if (n > 1024) return h->fail(CUW_ERR_UNSUPPORTED, "Gram-Schmidt supports NB <= 1024");
+  if (n > 1024) return h->fail(CUW_ERR_UNSUPPORTED, "WAVES_ORTHO_Y_C supports NB <= 1024");
   Device& g = h->g;
-  CUW_TRY(cudaMemsetAsync(g.ostatus, 0, sizeof(int) * 2, h->stream));
-  // A, B, C, ALPHA in the NB x NB buffers that are free during start-up
-  const int smem = (int)(sizeof(double) * 7 * (size_t)n);
+  if (clear_status) CUW_TRY(cudaMemsetAsync(g.ostatus, 0, sizeof(int) * 2, h->stream));
+  // A, B, C, ALPHA in NB x NB buffers that ORTHO_X uses only inside its solve
+  const int smem = (int)(sizeof(double) * 7 * (size_t)n + sizeof(int) * (size_t)n);
   CUW_TRY(smem_allow((const void*)k_ortho_y, smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(kOyCS);
@@ -1788,8 +1806,93 @@ int ortho_y_run(Handle* h, const double* s, double* x) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CUW_TRY(cudaLaunchKernelEx(&cfg, k_ortho_y, s, n, g.haux, g.gamn, g.work, g.lam2, x, g.ostatus));
+  CUW_TRY(cudaLaunchKernelEx(&cfg, k_ortho_y, s1, s2, s3, map, n, g.haux, g.gamn, g.work, g.lam2, x, g.ostatus));
   CUW_LAUNCH_CHECK("k_ortho_y");
+  return CUW_OK;
+}
+
+int ortho_y_run(Handle* h, const double* s, double* x) { return ortho_y_general(h, s, s, s, nullptr, x, true); }
+
+// SMAP of WAVES$ORTHOGONALIZE with SAFEORTHO = F and SWAPSTATES = T
+// (src/paw_waves2.f90:306-346): the exchange sort of the states by the real
+// diagonal of LAMBDA (that of RLAM0: the hermitisation leaves the diagonal),
+// ascending, then the order check ("STATE ORDERING FAILED").  One warp: for
+// each place i the inner loop over j > i swaps the running minimum into place
+// i; the places where it swaps are those whose value is below every value
+// before them (a prefix minimum that keeps the first of equal values), and
+// each of them receives the element that held the minimum before it, so a
+// chunk of 32 places is done by one warp scan.
+static __global__ void k_smap(const double2* __restrict__ rlam0, int n, int* __restrict__ smap,
+                              int* __restrict__ status) {
+  extern __shared__ double smd[];
+  int* s = reinterpret_cast<int*>(smd + n);
+  const int lane = threadIdx.x;
+  for (int k = lane; k < n; k += 32) {
+    smd[k] = rlam0[(size_t)k + (size_t)n * k].x;
+    s[k] = k;
+  }
+  __syncwarp();
+  for (int i = 0; i < n; ++i) {
+    int cur = s[i];
+    double dc = smd[cur];
+    for (int j0 = i + 1; j0 < n; j0 += 32) {
+      const int j = j0 + lane;
+      const bool valid = j < n;
+      const int sj = valid ? s[j] : -1;
+      const double dj = valid ? smd[sj] : 0.0;
+      // inclusive scan over the lanes of (value, element), combine(a, b) =
+      // b if b.value < a.value else a (a earlier): the first strict minimum
+      double v = dj;
+      int e = sj;
+      bool has = valid && dj == dj;  // lanes past n and NaN values take no part (never below anything)
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const double vo = __shfl_up_sync(0xffffffffu, v, d);
+        const int eo = __shfl_up_sync(0xffffffffu, e, d);
+        const bool ho = __shfl_up_sync(0xffffffffu, has, d);
+        if (lane >= d && ho) {
+          if (!has || !(v < vo)) {
+            v = vo;
+            e = eo;
+          }
+          has = true;
+        }
+      }
+      // exclusive value and holder: the running minimum before place j
+      double ve = __shfl_up_sync(0xffffffffu, v, 1);
+      int ee = __shfl_up_sync(0xffffffffu, e, 1);
+      const bool he = __shfl_up_sync(0xffffffffu, has, 1);
+      if (lane == 0 || !he || !(ve < dc)) {
+        ve = dc;
+        ee = cur;
+      }
+      if (valid && dj < ve) s[j] = ee;
+      // running minimum after the chunk (lane 31 holds the chunk's scan)
+      const double vl = __shfl_sync(0xffffffffu, v, 31);
+      const int el = __shfl_sync(0xffffffffu, e, 31);
+      const bool hl = __shfl_sync(0xffffffffu, has, 31);
+      if (hl && vl < dc) {
+        dc = vl;
+        cur = el;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) s[i] = cur;
+    __syncwarp();
+  }
+  bool bad = false;
+  for (int k = lane; k + 1 < n; k += 32) bad |= smd[s[k]] > smd[s[k + 1]];
+  bad = __any_sync(0xffffffffu, bad);
+  for (int k = lane; k < n; k += 32) smap[k] = s[k];
+  if (lane == 0 && bad) status[0] = kStatusOrder;
+}
+
+int smap_run(Handle* h) {
+  const int n = h->d.nb;
+  Device& g = h->g;
+  CUW_TRY(cudaMemsetAsync(g.ostatus, 0, sizeof(int) * 2, h->stream));
+  k_smap<<<1, 32, (sizeof(double) + sizeof(int)) * (size_t)n, h->stream>>>(g.rlam0, n, g.smap, g.ostatus);
+  CUW_LAUNCH_CHECK("k_smap");
   return CUW_OK;
 }
 

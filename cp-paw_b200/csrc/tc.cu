@@ -280,9 +280,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           const double2 h2 = cadd(hv[q], v);
           hpsi[k[q]] = h2;
           if (MODE == ADDPRO_FUSED) {
-            const double a3 = sc.a3 * rm;
-            psim[k[q]] = make_double2(sc.a1 * p0v[q].x + sc.a2 * pm[q].x + a3 * h2.x,
-                                      sc.a1 * p0v[q].y + sc.a2 * pm[q].y + a3 * h2.y);
+            double a1 = sc.a1, a2 = sc.a2, a3 = sc.a3 * rm;
+            if (sc.fr) {  // cell friction ANNEEVEC(G) (src/paw_waves1.f90:6536-6540)
+              const double an = 1.0 + sc.fr[g];
+              a1 = 2.0 / an;
+              a2 = 1.0 - a1;
+              a3 = -sc.dt2 / an * rm;
+            }
+            psim[k[q]] = make_double2(a1 * p0v[q].x + a2 * pm[q].x + a3 * h2.x, a1 * p0v[q].y + a2 * pm[q].y + a3 * h2.y);
           }
         } else if (!hcol && USE_O) {
           const double s = sc.oscale * rm;

@@ -25,6 +25,8 @@ CUW_OPT_LYAP_MAX_SWEEPS = 3
 CUW_OPT_SELFCONSISTENT = 4
 CUW_OPT_FFT_VARIANT = 5
 CUW_OPT_STREAM_PRIORITY = 6
+CUW_OPT_SAFEORTHO = 7
+CUW_OPT_SWAPSTATES = 8
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
@@ -64,6 +66,7 @@ SIGNATURES = {
     "get_atoms": [_P, _D, _D, _D],
     "set_occ": [_P, _D],
     "set_dynamics": [_P, C.c_double, C.c_double],
+    "set_cell_friction": [_P, _D, C.c_double, C.c_double, _D],
     "upload_psi": [_P, C.c_int, _D],
     "download_psi": [_P, C.c_int, _D],
     "get_proj": [_P, _D],
@@ -257,6 +260,14 @@ class Waves:
 
     def set_dynamics(self, delt, annee=0.0):
         self._chk(self._f["set_dynamics"](self.h, float(delt), float(annee)), "set_dynamics")
+
+    def set_cell_friction(self, fricmat=None, emass=0.0, emasscg2=0.0, dbucket=None):
+        """G-dependent friction of a moving cell (WAVES_DMPSI with TSTRESS);
+        fricmat (3, 3) = PSIANNEMAT, None switches it off."""
+        f = None if fricmat is None else np.asfortranarray(fricmat, dtype=np.float64)
+        d = None if dbucket is None else np.ascontiguousarray(dbucket, dtype=np.float64)
+        self._chk(self._f["set_cell_friction"](self.h, _dptr(f), float(emass), float(emasscg2), _dptr(d)),
+                  "set_cell_friction")
 
     # -- data movement -------------------------------------------------------
     def upload_psi(self, which: int, psi):

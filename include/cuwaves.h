@@ -105,6 +105,18 @@ int cuwaves_get_atoms(cuw_handle* h, double* rm, double* r0, double* rp);
 int cuwaves_set_occ(cuw_handle* h, const double* occ);
 /* DELT and ANNEE (friction) of WAVES_MODULE (src/paw_waves1.f90:216-218). */
 int cuwaves_set_dynamics(cuw_handle* h, double delt, double annee);
+/* G-dependent friction of WAVES$PROPAGATE for a moving cell (TSTRESS,
+ * src/paw_waves1.f90:6524-6543, WAVES_DMPSI :6676-6711): fricmat(3,3) =
+ * CELL$GETR8A('PSIANNEMAT'), emass and emasscg2 = EMASS and EMASSCG2 of
+ * WAVES_MODULE, dbucket(NGL) = GSET%DBUCKET or NULL (zero).  The propagation
+ * (cuwaves_propagate and the one inside cuwaves_cp_step) then uses
+ * ANNEEVEC(G) = ANNEE - tr(FRICMAT)/2 - EMASS EMASSCG2 G.FRICMAT.G
+ * (1 + DBUCKET(G)) in place of ANNEE, recomputed when ANNEE or the G set
+ * change; the mass scaling of O|psi> in cuwaves_orthogonalize keeps ANNEE,
+ * as the reference does (src/paw_waves2.f90:148-156).  fricmat = NULL
+ * switches it off.  Needs cuwaves_set_gset first. */
+int cuwaves_set_cell_friction(cuw_handle* h, const double* fricmat, double emass, double emasscg2,
+                              const double* dbucket);
 
 int cuwaves_upload_psi(cuw_handle* h, int which, const double* psi);
 int cuwaves_download_psi(cuw_handle* h, int which, double* psi);
@@ -372,6 +384,17 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * replaced after the work in flight; results do not change).  The serving
  * runtime gives its longest requests the high priority. */
 #define CUW_OPT_STREAM_PRIORITY 6
+/* CUW_OPT_SAFEORTHO: SAFEORTHO of WAVES_MODULE (src/paw_waves1.f90:221, used
+ * in WAVES$ORTHOGONALIZE, src/paw_waves2.f90:306-386).  1 (default) solves the
+ * constraint with WAVES_ORTHO_X; 0 with WAVES_ORTHO_Y_C (:1025-1338) of the
+ * overlap matrices, which orthonormalises the states one after another and
+ * needs no iteration (cuwaves_orthogonalize reports 0 iterations).
+ * CUW_OPT_SWAPSTATES: SWAPSTATES (:222), 0 (default) or 1; with SAFEORTHO = 0
+ * the states are taken in the ascending order of the RLAM0 diagonal.  A NaN in
+ * ORTHO_Y_C returns CUW_ERR_NAN ("NAN DETECTED"), a failed state order
+ * CUW_ERR_STATE ("STATE ORDERING FAILED"). */
+#define CUW_OPT_SAFEORTHO 7
+#define CUW_OPT_SWAPSTATES 8
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);

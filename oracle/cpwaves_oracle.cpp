@@ -226,6 +226,13 @@ struct orc_handle {
   bool have_rhoset = false;
   std::vector<double> qlm;    // (LMRXX, NAT) multipole moments of the one-centre densities
   bool scf = false;           // cp_step forms V(r) from the density of PSI0 first
+  bool safeortho = true, swapstates = false;  // TSAFEORTHO, TSWAPSTATES (waves1:221-222)
+  // cell friction of WAVES$PROPAGATE with TSTRESS (waves1:6524-6543):
+  // FRICMAT = CELL 'PSIANNEMAT' (3,3), EMASS, EMASSCG2, GSET%DBUCKET
+  bool tstress = false;
+  double fricmat[9] = {0};
+  double emass = 0.0, emasscg2 = 0.0;
+  std::vector<double> dbucket;
   std::string err;
   int nthreads = 0;
 };
@@ -1092,9 +1099,57 @@ int orc_expectation(orc_handle* h, double* eig) {
 }
 
 // WAVES$PROPAGATE (src/paw_waves1.f90:6479-6592), no stress
+// WAVES_DMPSI (src/paw_waves1.f90:6676-6711): ANNEEVEC(G) = ANNEE without
+// TSTRESS, else ANNEE - tr(FRICMAT)/2 - EMASS*EMASSCG2 * G.FRICMAT.G *
+// (1 + DBUCKET(G)) (FRICMAT symmetric: its off-diagonal terms counted twice)
+static void dmpsi(const orc_handle* h, std::vector<double>& anneevec) {
+  const int ngl = h->d.ngl;
+  anneevec.assign(ngl, h->annee);
+  if (!h->tstress) return;
+  const double* F = h->fricmat;  // FRICMAT(i,j) = F[(i-1) + 3*(j-1)]
+  const double fac1 = h->annee - 0.5 * (F[0] + F[4] + F[8]);
+  const double fac2 = -0.5 * h->emass * 2.0 * h->emasscg2;
+  for (int ig = 0; ig < ngl; ++ig) {
+    const double* g = &h->gvec[3 * (size_t)ig];
+    const double svar = F[0] * g[0] * g[0] + F[3] * 2.0 * g[0] * g[1] + F[6] * 2.0 * g[0] * g[2] +
+                        F[4] * g[1] * g[1] + F[7] * 2.0 * g[1] * g[2] + F[8] * g[2] * g[2];
+    anneevec[ig] = fac1 + fac2 * svar * (1.0 + (h->dbucket.empty() ? 0.0 : h->dbucket[ig]));
+  }
+}
+
+int orc_set_cell_friction(orc_handle* h, const double* fricmat, double emass, double emasscg2,
+                          const double* dbucket) {
+  OCHECK(h->have_gset, CUW_ERR_STATE, "gset not set");
+  h->tstress = fricmat != nullptr;
+  if (fricmat) std::memcpy(h->fricmat, fricmat, sizeof(h->fricmat));
+  h->emass = emass;
+  h->emasscg2 = emasscg2;
+  if (dbucket) h->dbucket.assign(dbucket, dbucket + h->d.ngl);
+  else h->dbucket.clear();
+  return CUW_OK;
+}
+
 int orc_propagate(orc_handle* h) {
   OCHECK(h->have_hpsi, CUW_ERR_STATE, "HPSI NOT AVAILABLE");
   const int ngl = h->d.ngl, nbh = h->d.nbh;
+  if (h->tstress) {
+    // ARR1..ARR3 per G from ANNEEVEC (waves1:6536-6540)
+    std::vector<double> an, arr1(ngl), arr2(ngl), arr3(ngl);
+    dmpsi(h, an);
+    for (int ig = 0; ig < ngl; ++ig) {
+      arr1[ig] = 2.0 / (1.0 + an[ig]);
+      arr2[ig] = 1.0 - arr1[ig];
+      arr3[ig] = -h->delt * h->delt / (1.0 + an[ig]) / h->mpsi[ig];
+    }
+#pragma omp parallel for schedule(static)
+    for (int ib = 0; ib < nbh; ++ib)
+      for (int ig = 0; ig < ngl; ++ig) {
+        size_t k = PS(h, ig, ib);
+        h->psim[k] = arr1[ig] * h->psi0[k] + arr2[ig] * h->psim[k] + arr3[ig] * h->hpsi[k];
+      }
+    h->have_hpsi = false;
+    return CUW_OK;
+  }
   const double svar1 = 2.0 / (1.0 + h->annee), svar2 = 1.0 - svar1;
   const double svar3 = -h->delt * h->delt / (1.0 + h->annee);
 #pragma omp parallel for schedule(static)
@@ -1109,6 +1164,9 @@ int orc_propagate(orc_handle* h) {
 }
 
 // WAVES$ORTHOGONALIZE (src/paw_waves2.f90:11-494), TSAFEORTHO, TINV, no stress
+static int ortho_y_c(int nb, const cplx* phiphi, const cplx* chiphi, const cplx* chichi, cplx* x,
+                     const int* map = nullptr);
+
 int orc_orthogonalize(orc_handle* h, int maxit, double eps, int* iters) {
   OCHECK(h->have_gset && h->have_do, CUW_ERR_STATE, "gset/do not set");
   const int ngl = h->d.ngl, nbh = h->d.nbh, nb = h->d.nb, npro = h->npro;
@@ -1152,12 +1210,36 @@ int orc_orthogonalize(orc_handle* h, int maxit, double eps, int* iters) {
       lambda[i + (size_t)nb * j] = c;
       lambda[j + (size_t)nb * i] = std::conj(c);
     }
+  // SMAP (waves2:306-346): with SAFEORTHO = F the states are handled in the
+  // order MAP; SWAPSTATES = T sorts them by the real diagonal of LAMBDA with
+  // the reference's exchange loop, then checks the order
+  std::vector<int> smap(nb);
+  for (int i = 0; i < nb; ++i) smap[i] = i;
+  if (!h->safeortho && h->swapstates) {
+    auto dg = [&](int k) { return lambda[k + (size_t)nb * k].real(); };
+    for (int i = 0; i < nb; ++i)
+      for (int j = i + 1; j < nb; ++j)
+        if (dg(smap[j]) < dg(smap[i])) std::swap(smap[i], smap[j]);
+    for (int i = 0; i + 1 < nb; ++i)
+      OCHECK(!(dg(smap[i]) > dg(smap[i + 1])), CUW_ERR_STATE, "STATE ORDERING FAILED");
+  }
   for (int i = 0; i < nb; ++i)
     for (int j = 0; j < nb; ++j) {
       double occi = h->occ[i], occj = h->occ[j];
       if (occi + occj < 1e-12) occj = 1e-12;
       lambda[i + (size_t)nb * j] *= 0.5 * occi / (occi + occj);
     }
+  if (!h->safeortho) {
+    // WAVES_ORTHO_Y_C(NB, MAT, OMAT, OOMAT, LAMBDA, SMAP) (waves2:384-386)
+    OCHECK(ortho_y_c(nb, mat.data(), omat.data(), oomat.data(), lambda.data(), smap.data()) == CUW_OK, CUW_ERR_NAN,
+           "NAN DETECTED in WAVES_ORTHO_Y_C");
+    if (iters) *iters = 0;
+    addopsi(h, h->psim.data(), h->opsi.data(), lambda.data());
+    addoproj(h, npro, h->proj.data(), oproj.data(), lambda.data(), nbh);
+    h->rlam0 = lambda;
+    h->waveekin2 = wavekinetic(h, nullptr);
+    return CUW_OK;
+  }
   std::vector<double> rmat(nn), romat(nn), roomat(nn), rl(nn);
   for (size_t k = 0; k < nn; ++k) {
     rmat[k] = mat[k].real();
@@ -1229,8 +1311,12 @@ int orc_stop(orc_handle* h) {
   return CUW_OK;
 }
 
-// WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338) with MAP = identity
-static int ortho_y_c(int nb, const cplx* phiphi, const cplx* chiphi, const cplx* chichi, cplx* x) {
+// WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338); map = MAP (0-based), null
+// for the identity.  pos[i] is the place of state i in MAP, so "IU = NU+1, NB;
+// I = MAP(IU)" of the reference is every i with pos[i] > nu.
+static int ortho_y_c(int nb, const cplx* phiphi, const cplx* chiphi, const cplx* chichi, cplx* x, const int* map) {
+  std::vector<int> pos(nb);
+  for (int k = 0; k < nb; ++k) pos[map ? map[k] : k] = k;
   const size_t nn = (size_t)nb * nb;
   std::vector<cplx> A(nn), B(nn), C(nn), alpha(nn, 0.0), work(nn), z(nb);
   auto I = [nb](int i, int j) { return (size_t)i + (size_t)nb * j; };
@@ -1247,7 +1333,7 @@ static int ortho_y_c(int nb, const cplx* phiphi, const cplx* chiphi, const cplx*
     alpha[I(i, i)] = 1.0;
   }
   for (int nu = 0; nu < nb; ++nu) {
-    const int n = nu;
+    const int n = map ? map[nu] : nu;
     double svar = (std::pow(B[I(n, n)].real(), 2) - A[I(n, n)] * C[I(n, n)]).real();
     double svar1 = -B[I(n, n)].real();
     if (svar >= 0.0) {
@@ -1264,33 +1350,41 @@ static int ortho_y_c(int nb, const cplx* phiphi, const cplx* chiphi, const cplx*
     A[I(n, n)] += std::conj(z[n]) * C[I(n, n)] * z[n];
     for (int i = 0; i < nb; ++i) B[I(i, n)] += C[I(i, n)] * z[n];
     // orthogonalise higher phis to this phi
-    for (int iu = 0; iu <= nu; ++iu) z[iu] = 0.0;
-    for (int iu = nu + 1; iu < nb; ++iu) z[iu] = -std::conj(A[I(iu, n)] / (B[I(n, n)] + r8small));
-    const int nu0 = nu + 1;
-    for (int j = nu0; j < nb; ++j)
-      for (int i = 0; i < nb; ++i) x[I(i, j)] += alpha[I(i, n)] * z[j];
-    for (int i = nu0; i < nb; ++i)
-      for (int j = 0; j < nb; ++j) A[I(i, j)] += std::conj(z[i]) * B[I(n, j)];
+    for (int i = 0; i < nb; ++i) z[i] = pos[i] > nu ? -std::conj(A[I(i, n)] / (B[I(n, n)] + r8small)) : cplx(0.0);
+    auto hi = [&](int k) { return pos[k] > nu; };  // JU = NU0..NB, J = MAP(JU)
+    for (int j = 0; j < nb; ++j)
+      if (hi(j))
+        for (int i = 0; i < nb; ++i) x[I(i, j)] += alpha[I(i, n)] * z[j];
     for (int i = 0; i < nb; ++i)
-      for (int j = nu0; j < nb; ++j) A[I(i, j)] += std::conj(B[I(n, i)]) * z[j];
-    for (int i = nu0; i < nb; ++i)
-      for (int j = nu0; j < nb; ++j) A[I(i, j)] += std::conj(z[i]) * C[I(n, n)] * z[j];
+      if (hi(i))
+        for (int j = 0; j < nb; ++j) A[I(i, j)] += std::conj(z[i]) * B[I(n, j)];
     for (int i = 0; i < nb; ++i)
-      for (int j = nu0; j < nb; ++j) B[I(i, j)] += C[I(i, n)] * z[j];
+      for (int j = 0; j < nb; ++j)
+        if (hi(j)) A[I(i, j)] += std::conj(B[I(n, i)]) * z[j];
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j)
+        if (hi(i) && hi(j)) A[I(i, j)] += std::conj(z[i]) * C[I(n, n)] * z[j];
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j)
+        if (hi(j)) B[I(i, j)] += C[I(i, n)] * z[j];
     // orthogonalise higher chis to this phi
-    for (int iu = 0; iu <= nu; ++iu) z[iu] = 0.0;
-    for (int iu = nu + 1; iu < nb; ++iu) z[iu] = -std::conj(B[I(iu, n)] / (B[I(n, n)] + r8small));
+    for (int i = 0; i < nb; ++i) z[i] = pos[i] > nu ? -std::conj(B[I(i, n)] / (B[I(n, n)] + r8small)) : cplx(0.0);
     for (int i = 0; i < nb; ++i)
-      for (int j = nu0; j < nb; ++j) alpha[I(i, j)] += alpha[I(i, n)] * z[j];
-    for (int i = nu0; i < nb; ++i)
-      for (int j = 0; j < nb; ++j) B[I(i, j)] += std::conj(z[i]) * B[I(n, j)];
+      for (int j = 0; j < nb; ++j)
+        if (hi(j)) alpha[I(i, j)] += alpha[I(i, n)] * z[j];
+    for (int i = 0; i < nb; ++i)
+      if (hi(i))
+        for (int j = 0; j < nb; ++j) B[I(i, j)] += std::conj(z[i]) * B[I(n, j)];
     std::fill(work.begin(), work.end(), cplx(0.0));
-    for (int i = nu0; i < nb; ++i)
-      for (int j = 0; j < nb; ++j) work[I(i, j)] += std::conj(z[i]) * C[I(n, j)];
     for (int i = 0; i < nb; ++i)
-      for (int j = nu0; j < nb; ++j) work[I(i, j)] += C[I(i, n)] * z[j];
-    for (int i = nu0; i < nb; ++i)
-      for (int j = nu0; j < nb; ++j) work[I(i, j)] += std::conj(z[i]) * C[I(n, n)] * z[j];
+      if (hi(i))
+        for (int j = 0; j < nb; ++j) work[I(i, j)] += std::conj(z[i]) * C[I(n, j)];
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j)
+        if (hi(j)) work[I(i, j)] += C[I(i, n)] * z[j];
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j)
+        if (hi(i) && hi(j)) work[I(i, j)] += std::conj(z[i]) * C[I(n, n)] * z[j];
     for (size_t k = 0; k < nn; ++k) C[k] += work[k];
   }
   return CUW_OK;
@@ -1602,6 +1696,8 @@ int orc_set_qlm(orc_handle* h, const double* qlm) {
 }
 
 int orc_set_option(orc_handle* h, int option, double value) {
+  if (option == CUW_OPT_SAFEORTHO) h->safeortho = value != 0.0;
+  if (option == CUW_OPT_SWAPSTATES) h->swapstates = value != 0.0;
   if (option == CUW_OPT_SELFCONSISTENT) {
     OCHECK(value == 0.0 || (h->have_rhoset && !h->qlm.empty()), CUW_ERR_STATE, "density set or QLM missing");
     h->scf = value != 0.0;
@@ -2162,6 +2258,16 @@ int orc_initializerandom(int ng, int ndim, int nb, const double* g, double* psi_
 // PLANEWAVE_COUNTG + PLANEWAVE_GETIG (src/paw_fft.f90:1110-1327) at Gamma with
 // GBASS/BOXSPH (src/paw_generalpurpose.f90:72-180).  If igvec==NULL only the
 // count is returned in *ng.
+// WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338) on its own, for the tests:
+// complex NB x NB matrices as (re, im) pairs in Fortran order, map = MAP
+// (0-based) or null; returns CUW_ERR_NAN where the reference stops on a NaN.
+int orc_ortho_y_c(int nb, const double* phiphi, const double* chiphi, const double* chichi, double* x,
+                  const int* map) {
+  if (nb <= 0 || !phiphi || !chiphi || !chichi || !x) return CUW_ERR_ARG;
+  return ortho_y_c(nb, reinterpret_cast<const cplx*>(phiphi), reinterpret_cast<const cplx*>(chiphi),
+                   reinterpret_cast<const cplx*>(chichi), reinterpret_cast<cplx*>(x), map);
+}
+
 int orc_getig(const double* gbas, double epw, int* ng, int* igvec) {
   // BOXSPH(GBAS,0,0,0,RAD)
   const double* t1 = gbas;      // GBAS(:,1)

@@ -264,6 +264,90 @@ def test_cp_steps(name, nsteps, move, oracle, inputs_cache):
     assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-8
 
 
+@pytest.mark.parametrize("name,swap", [("Si8", 0), ("Si8", 1), ("H2O2", 1)])
+def test_cp_steps_safeortho_false(name, swap, oracle, inputs_cache):
+    """SAFEORTHO = F (src/paw_waves2.f90:306-386): inside the CP step the
+    cluster kernel of WAVES_ORTHO_Y_C replaces ORTHO_X, with the states in the
+    order of the RLAM0 diagonal when SWAPSTATES = T (the warp-scan exchange
+    sort); step by step against the oracle, from a state whose RLAM0 came from
+    ordinary steps."""
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    for w in (gpu, cpu):
+        w.cp_step(move_atoms=True)
+    sync_state(gpu, cpu)
+    d = np.diag(gpu.get_rlam0()).real
+    if swap:
+        assert not np.all(np.diff(d) >= 0)  # the order changes
+    for w in (gpu, cpu):
+        w.set_option(cuwaves.CUW_OPT_SWAPSTATES, swap)
+        w.set_option(cuwaves.CUW_OPT_SAFEORTHO, 0)
+    for step in range(4):
+        og, fg = gpu.cp_step(move_atoms=True)
+        oc, fc = cpu.cp_step(move_atoms=True)
+        assert og[4] == 0 and oc[4] == 0
+        for k in range(4):
+            assert abs(og[k] - oc[k]) < 1e-8, f"step {step}: out[{k}] {og[k]} vs {oc[k]}"
+        assert np.abs(fg - fc).max() < 1e-6
+    assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-8
+    assert np.abs(gpu.get_rlam0() - cpu.get_rlam0()).max() < 1e-8
+    gpu.close()
+    cpu.close()
+
+
+def _cell_friction(inp):
+    rng = np.random.default_rng(9)
+    return dict(fricmat=rng.normal(size=(3, 3)) * 0.01, emass=inp["emass"], emasscg2=inp["emasscg2"],
+                dbucket=rng.uniform(0.0, 0.2, size=inp["ngl"]))
+
+
+@pytest.mark.parametrize("name", ["Si8-20Ry", "H2O2"])
+def test_propagate_cell_friction(name, oracle, inputs_cache):
+    """WAVES$PROPAGATE with the G-dependent friction of a moving cell
+    (ANNEEVEC of WAVES_DMPSI, src/paw_waves1.f90:6524-6543, 6676-6711): the
+    standalone propagation and CP steps (the propagation fused into the
+    back-projection) against the oracle."""
+    inp, gpu, cpu = make_pair(name, oracle, inputs_cache)
+    fr = _cell_friction(inp)
+    for w in (gpu, cpu):
+        w.set_dynamics(inp["delt"], 0.02)
+        w.set_cell_friction(**fr)
+        w.hpsi()
+        w.propagate()
+    assert rel(gpu.download_psi(CUW_PSIM), cpu.download_psi(CUW_PSIM)) < 1e-10
+    sync_state(gpu, cpu)
+    for step in range(3):
+        og, fg = gpu.cp_step(move_atoms=True)
+        oc, fc = cpu.cp_step(move_atoms=True)
+        assert og[4] == oc[4]
+        for k in range(4):
+            assert abs(og[k] - oc[k]) < 1e-8, f"step {step}: out[{k}] {og[k]} vs {oc[k]}"
+        assert np.abs(fg - fc).max() < 1e-6
+    assert rel(gpu.download_psi(CUW_PSI0), cpu.download_psi(CUW_PSI0)) < 1e-8
+    gpu.close()
+    cpu.close()
+
+
+def test_cell_friction_mixed_path(oracle, inputs_cache):
+    """The friction in the tcgen05 back-projection epilogue of the mixed path:
+    one CP step agrees with the FP64 path under the same friction to the mixed
+    path's precision, and differs from a step without it."""
+    inp = systems.build_inputs(CASES["Si8"]())
+    fr = _cell_friction(inp)
+    res = {}
+    for prec, fric in ((cuwaves.CUW_PREC_FP64, True), (cuwaves.CUW_PREC_MIXED, True), (cuwaves.CUW_PREC_MIXED, False)):
+        w = cuwaves.open_waves(inp, precision=prec).setup().initialize()
+        w.set_dynamics(inp["delt"], 0.02)
+        if fric:
+            w.set_cell_friction(**fr)
+        w.cp_step(move_atoms=False)
+        res[(prec, fric)] = w.download_psi(CUW_PSI0)
+        w.close()
+    a, b = res[(cuwaves.CUW_PREC_FP64, True)], res[(cuwaves.CUW_PREC_MIXED, True)]
+    c = res[(cuwaves.CUW_PREC_MIXED, False)]
+    assert rel(b, a) < 1e-5
+    assert rel(c, a) > 10 * rel(b, a)
+
+
 def test_not_converged_status_and_recovery(oracle, inputs_cache):
     """A forced non-convergence (max_iter=1) is reported as a status and the
     handle stays usable (the reference stops the run instead)."""

@@ -444,3 +444,124 @@ def test_oracle_vofrho_matches_numpy(oracle):
     assert abs(exc - e["exc"]) < 1e-10 * abs(exc)
     assert abs(rhob - e["rhob"]) < 1e-12
     assert np.abs(vnp - v).max() < 1e-10 * np.abs(v).max()
+
+
+def _ortho_y_c(oracle, phiphi, chiphi, chichi, smap=None):
+    """orc_ortho_y_c: WAVES_ORTHO_Y_C of the oracle on complex NB x NB matrices."""
+    lib = oracle.library()
+    f = lib.orc_ortho_y_c
+    f.restype = C.c_int
+    f.argtypes = [C.c_int] + [C.c_void_p] * 5
+    nb = phiphi.shape[0]
+    mats = [np.asfortranarray(m, dtype=np.complex128) for m in (phiphi, chiphi, chichi)]
+    x = np.zeros((nb, nb), dtype=np.complex128, order="F")
+    mp = None if smap is None else np.ascontiguousarray(smap, dtype=np.int32)
+    rc = f(nb, *[m.ctypes.data for m in mats], x.ctypes.data, None if mp is None else mp.ctypes.data)
+    return rc, x
+
+
+@pytest.mark.parametrize("order", ["identity", "permuted"])
+@pytest.mark.parametrize("kind", ["complex", "real"])
+def test_oracle_ortho_y_c_self_test(oracle, order, kind):
+    """WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338) against the reference's
+    own TTEST checks of the routine (:1302-1336, TESTA :1343-1356): with
+    |phi'_I> = |phi_I> + sum_J |chi_J> X(J,I), PHIPHI + X^H CHIPHI + CHIPHI^H X
+    + X^H CHICHI X = 1 (the reference stops above TOL = 1e-10; its divisions
+    carry R8SMALL = 1e-10, :1058), and X(I,J) = 0 where I comes after J in
+    the order MAP (the states are orthonormalised one after another)."""
+    rng = np.random.default_rng(11)
+    nb, ng = 12, 300
+    cz = 1j if kind == "complex" else 0.0
+    q, _ = np.linalg.qr(rng.normal(size=(ng, nb)) + cz * rng.normal(size=(ng, nb)))
+    # columns of norm about 1 with perturbations of norm about 0.1 and 0.05
+    phi = q + 0.1 / np.sqrt(ng) * (rng.normal(size=(ng, nb)) + cz * rng.normal(size=(ng, nb)))
+    chi = q + 0.05 / np.sqrt(ng) * (rng.normal(size=(ng, nb)) + cz * rng.normal(size=(ng, nb)))
+    phiphi = phi.conj().T @ phi
+    chiphi = chi.conj().T @ phi  # CHIPHI(I,J) = <chi_I|phi_J>
+    chichi = chi.conj().T @ chi
+    smap = np.arange(nb) if order == "identity" else rng.permutation(nb)
+    rc, x = _ortho_y_c(oracle, phiphi, chiphi, chichi, None if order == "identity" else smap)
+    assert rc == 0
+    res = phiphi + x.conj().T @ chiphi + chiphi.conj().T @ x + x.conj().T @ chichi @ x - np.eye(nb)
+    assert np.abs(res).max() < 1e-9
+    new = phi + chi @ x
+    assert np.abs(new.conj().T @ new - np.eye(nb)).max() < 1e-9
+    pos = np.empty(nb, int)
+    pos[smap] = np.arange(nb)
+    later = pos[:, None] > pos[None, :]
+    assert np.all(x[later] == 0) and np.abs(x[~later]).max() > 0
+    if kind == "real":
+        assert np.all(x.imag == 0)
+
+
+def test_oracle_safeortho_false(oracle):
+    """WAVES$ORTHOGONALIZE with SAFEORTHO = F (src/paw_waves2.f90:306-386):
+    WAVES_ORTHO_Y_C of MAT, OMAT, OOMAT replaces WAVES_ORTHO_X, with SMAP
+    sorting the states by the RLAM0 diagonal when SWAPSTATES = T.  The CP
+    steps keep PSI orthonormal (O-metric) and report no iterations; the state
+    order changes the result."""
+    s = systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry")
+    inp = systems.build_inputs(s)
+    w = oracle.open_oracle(inp).setup().initialize()
+    for _ in range(3):
+        w.cp_step()
+    state = (w.download_psi(0), w.download_psi(1), w.get_proj(), w.get_rlam0())
+    d = np.diag(state[3]).real
+    assert not np.all(np.diff(d) >= 0)  # the sort has something to do
+    results = {}
+    for swap in (0, 1):
+        w.upload_psi(0, state[0])
+        w.upload_psi(1, state[1])
+        w.set_proj(state[2])
+        w.set_rlam0(state[3])
+        w.set_option(8, swap)  # CUW_OPT_SWAPSTATES
+        w.set_option(7, 0)  # CUW_OPT_SAFEORTHO = F
+        for _ in range(3):
+            out, _ = w.cp_step()
+            assert out[4] == 0
+            ov = _band_overlap(inp, w.download_psi(0), w.get_proj())
+            # R8SMALL = 1e-10 in the divisions of ORTHO_Y_C (waves2:1058), here
+            # against CHICHI = <O psi|O psi> (dt^2/m)^2 of order 1e-2
+            assert np.abs(ov - np.eye(inp["nb"])).max() < 1e-8
+        results[swap] = w.download_psi(0)
+    assert np.abs(results[0] - results[1]).max() > 1e-6
+    w.set_option(7, 1)
+    out, _ = w.cp_step()
+    assert out[4] > 0
+
+
+def test_oracle_cell_friction_propagate(oracle):
+    """WAVES$PROPAGATE with TSTRESS (src/paw_waves1.f90:6524-6543): the oracle's
+    per-G coefficients from WAVES_DMPSI (:6676-6711) against a numpy
+    restatement of the two routines (the reference reads the upper triangle of
+    FRICMAT, so a non-symmetric matrix checks the index order); switching the
+    friction off gives back the scalar path bit for bit."""
+    s = systems.si_cell(1, grid=(24, 24, 24), epw_psi_ry=20.0, name="Si8-20Ry")
+    inp = systems.build_inputs(s)
+    w = oracle.open_oracle(inp).setup().initialize()
+    rng = np.random.default_rng(4)
+    f = rng.normal(size=(3, 3)) * 0.01
+    db = rng.uniform(0.0, 0.2, size=inp["ngl"])
+    annee = 0.05
+    w.set_dynamics(inp["delt"], annee)
+    psi0, psim = w.download_psi(0), w.download_psi(1)
+    w.hpsi()
+    hp = w.download_psi(2)
+    x, y, z = inp["gvec"].T
+    svar = (f[0, 0] * x * x + 2 * f[0, 1] * x * y + 2 * f[0, 2] * x * z + f[1, 1] * y * y
+            + 2 * f[1, 2] * y * z + f[2, 2] * z * z)
+    an = annee - 0.5 * np.trace(f) - inp["emass"] * inp["emasscg2"] * svar * (1.0 + db)
+    want = (2.0 / (1.0 + an)) * psi0 + (1.0 - 2.0 / (1.0 + an)) * psim \
+        - inp["delt"] ** 2 / (1.0 + an) / inp["mpsi"] * hp
+    w.set_cell_friction(f, inp["emass"], inp["emasscg2"], db)
+    w.propagate()
+    got = w.download_psi(1)
+    assert np.abs(got - want).max() / np.abs(want).max() < 1e-13
+    # off again: the scalar ANNEE path
+    w.upload_psi(1, psim)
+    w.set_cell_friction(None)
+    w.hpsi()
+    w.propagate()
+    a1 = 2.0 / (1.0 + annee)
+    plain = a1 * psi0 + (1.0 - a1) * psim - inp["delt"] ** 2 / (1.0 + annee) / inp["mpsi"] * hp
+    assert np.abs(w.download_psi(1) - plain).max() / np.abs(plain).max() < 1e-13
