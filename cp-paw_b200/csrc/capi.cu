@@ -1680,6 +1680,11 @@ extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
       h->touch();
       return CUW_OK;
     }
+    case CUW_OPT_CONTRACTION_TILES:
+      if (value != 0.0 && value != 1.0) return h->fail(CUW_ERR_ARG, "CONTRACTION_TILES must be 0 or 1");
+      if (!h->mixed() && value == 0.0) return h->fail(CUW_ERR_ARG, "FP64 handles have DMMA tiles only");
+      h->dmma_tiles = value != 0.0;
+      return CUW_OK;
     case CUW_OPT_SAFEORTHO:
       if (value != 0.0 && value != 1.0) return h->fail(CUW_ERR_ARG, "SAFEORTHO must be 0 or 1");
       h->safeortho = value != 0.0;

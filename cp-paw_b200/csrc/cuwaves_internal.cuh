@@ -210,7 +210,11 @@ struct Handle {
   int nev = 0;
   bool mixed() const { return d.precision == CUW_PREC_MIXED; }
   bool fp64_only = false;  // contractions in FP64 even on the mixed path (start-up orthonormalisation)
-  bool tc_on() const { return mixed() && !fp64_only; }
+  // mixed path: the contractions on FP64 DMMA tiles (64 x 64, m8n8k4) instead
+  // of the split-tf32 tcgen05 tiles (128 x 128 x 8); set by the autotuner or
+  // CUW_OPT_CONTRACTION_TILES
+  bool dmma_tiles = false;
+  bool tc_on() const { return mixed() && !fp64_only && !dmma_tiles; }
   // relative accuracy to which each ORTHO_X iteration solves its Lyapunov
   // equation (0: to rounding).  Measured on Si64 over 40 CP steps against the
   // solve to rounding: 1e-6 moves the FP64 total energy by 3e-12 Ha and the

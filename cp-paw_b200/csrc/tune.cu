@@ -6,11 +6,17 @@
 //     stage, radix order; grids with compiled lengths) together with
 //   - the FFT band batch (bands transformed per launch sequence; the work grid
 //     is reallocated when a larger batch wins);
+//   - on mixed-precision handles, the tile family of the contractions:
+//     split-tf32 tcgen05 tiles (128 x 128 x 8) or FP64 DMMA tiles (64 x 64 x
+//     4), timed on the projections, the Gram products and the back-projection
+//     (the wide tiles waste most of their columns when there are few bands);
 //   - the split-K factor of the projections <p|psi> (FP64 DMMA or tcgen05);
 //   - the split-K factor of the plane-wave Gram products.
 // The choice is kept in a process-wide table keyed by the shape (precision,
 // NGL, NBH, NPRO, grid, SM count), so that further handles of the same shape
-// take it without timing.  A different split-K factor changes the summation
+// take it without timing.  The tile family changes the arithmetic (FP64
+// against split tf32), the split-K factors the summation order: results move
+// at the mixed path's precision or at rounding level.  A different split-K factor changes the summation
 // order of the contractions: results move at rounding level, which is why the
 // tuner runs only when asked.
 #include <cuda_runtime.h>
@@ -31,8 +37,9 @@ using Shape = std::array<long long, 8>;
 struct Choice {
   int batch;
   int fft_variant;
+  int dmma_tiles;
   double split_proj, split_gram;
-  double ms[3];
+  double ms[5];
 };
 std::mutex g_mu;
 std::map<Shape, Choice> g_table;
@@ -98,6 +105,7 @@ int autotune(Handle* h, double* out, int n) {
   if (cached) {
     CUW_RET(grid_room(h, c.batch));
     CUW_RET(fft_set_variant(h, c.fft_variant));
+    h->dmma_tiles = c.dmma_tiles != 0;
   } else {
     CUW_RET(eigr_compute(h, g.r0));
     // FFT band batch: the L2 rule's batch and even splits of the bands
@@ -131,6 +139,29 @@ int autotune(Handle* h, double* out, int n) {
     h->batch = c.batch;
     CUW_RET(fft_set_variant(h, c.fft_variant));
     h->have_hpsi = false;
+    // tile family of the contractions (mixed precision): projections, Gram
+    // products of the plane waves and the back-projection into HPSI, at the
+    // default split-K factors
+    c.dmma_tiles = h->dmma_tiles ? 1 : 0;
+    c.ms[3] = c.ms[4] = 0.0;
+    if (h->mixed()) {
+      const GramPair pq[3] = {{g.psi0, g.psi0}, {g.psim, g.psi0}, {g.psim, g.psim}};
+      h->split_proj = h->split_gram = 1.0;
+      for (int fam = 0; fam < 2; ++fam) {
+        h->dmma_tiles = fam == 1;
+        double ms = 0.0;
+        CUW_RET(time_best(h, [&] {
+          int rc = proj_compute(h, g.psi0, g.pbuf, nullptr, nullptr);
+          if (rc == CUW_OK) rc = gram_planewave(h, pq, 3, g.tmat);
+          if (rc == CUW_OK) rc = addpro_run(h, ADDPRO_HPSI, g.hproj, g.oproj);
+          return rc;
+        }, 3, &ms));
+        c.ms[3 + fam] = ms;
+      }
+      c.dmma_tiles = c.ms[4] < c.ms[3] ? 1 : 0;
+      h->dmma_tiles = c.dmma_tiles != 0;
+      h->have_hpsi = false;
+    }
     // split-K factors
     const double muls[] = {0.5, 1.0, 1.5, 2.0, 3.0};
     c.split_proj = c.split_gram = 1.0;
@@ -161,9 +192,9 @@ int autotune(Handle* h, double* out, int n) {
   h->split_proj = c.split_proj;
   h->split_gram = c.split_gram;
   h->touch();
-  const double v[8] = {(double)c.batch, c.split_proj, c.split_gram, c.ms[0], c.ms[1], c.ms[2], cached ? 1.0 : 0.0,
-                       (double)c.fft_variant};
-  for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
+  const double v[11] = {(double)c.batch, c.split_proj, c.split_gram, c.ms[0], c.ms[1], c.ms[2], cached ? 1.0 : 0.0,
+                        (double)c.fft_variant, (double)c.dmma_tiles, c.ms[3], c.ms[4]};
+  for (int i = 0; i < n && i < 11; ++i) out[i] = v[i];
   return h->sync();
 }
 

@@ -27,6 +27,7 @@ CUW_OPT_FFT_VARIANT = 5
 CUW_OPT_STREAM_PRIORITY = 6
 CUW_OPT_SAFEORTHO = 7
 CUW_OPT_SWAPSTATES = 8
+CUW_OPT_CONTRACTION_TILES = 9
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}
@@ -455,10 +456,12 @@ class Waves:
         self._chk(self._f["set_option"](self.h, int(option), float(value)), "set_option")
 
     def autotune(self) -> dict:
-        """Times and fixes the FFT plan variant and band batch and the split-K factors."""
-        out = np.zeros(8)
+        """Times and fixes the FFT plan variant and band batch, the tile family of
+        the contractions (mixed precision) and the split-K factors."""
+        out = np.zeros(11)
         self._chk(self._f["autotune"](self.h, _dptr(out), len(out)), "autotune")
-        keys = ("fft_batch", "split_proj", "split_gram", "fft_ms", "proj_ms", "gram_ms", "cached", "fft_variant")
+        keys = ("fft_batch", "split_proj", "split_gram", "fft_ms", "proj_ms", "gram_ms", "cached", "fft_variant",
+                "dmma_tiles", "tc_tiles_ms", "dmma_tiles_ms")
         return dict(zip(keys, out.tolist()))
 
     def graph_stats(self) -> tuple:

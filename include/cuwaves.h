@@ -395,19 +395,29 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * CUW_ERR_STATE ("STATE ORDERING FAILED"). */
 #define CUW_OPT_SAFEORTHO 7
 #define CUW_OPT_SWAPSTATES 8
+/* CUW_OPT_CONTRACTION_TILES (mixed precision only): tile family of the
+ * projector, Gram, rotation and force contractions, 0 (default) = split-tf32
+ * tcgen05 tiles of 128 x 128 x 8, 1 = FP64 DMMA tiles of 64 x 64 x 4 (more
+ * accurate; wins when few bands leave the wide tiles mostly empty).  The
+ * autotuner picks it by timing. */
+#define CUW_OPT_CONTRACTION_TILES 9
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);
 /* Autotuner (no reference counterpart; FFTW's planner picks the reference's
  * FFT plans, src/paw_library.f90:2694-2697): times the FFT plan variant of the
  * plane transforms (values per thread and stage, radix order; grids with
- * compiled lengths) together with the FFT band batch, and the split-K factors
- * of the projections and plane-wave Gram products, on this handle's data (G
- * set, V, DH, DO and PSI0/PSIM loaded) and keeps the fastest, in a
- * process-wide table keyed by the shape so that later handles of the same
- * shape reuse it.  out[0..7] (n values): batch, projection split factor, Gram
- * split factor, their best times in ms, 1 if the choice came from the table,
- * FFT plan variant.  Results move at rounding level (another summation order). */
+ * compiled lengths) together with the FFT band batch, on mixed-precision
+ * handles the tile family of the contractions (CUW_OPT_CONTRACTION_TILES),
+ * and the split-K factors of the projections and plane-wave Gram products, on
+ * this handle's data (G set, V, DH, DO and PSI0/PSIM loaded) and keeps the
+ * fastest, in a process-wide table keyed by the shape so that later handles of
+ * the same shape reuse it.  out[0..10] (n values): batch, projection split
+ * factor, Gram split factor, their best times in ms, 1 if the choice came from
+ * the table, FFT plan variant, tile family (1 = DMMA), the timed contraction
+ * set's ms on tcgen05 and on DMMA tiles (0 on FP64 handles).  Results move at
+ * rounding level (another summation order) or, with the tile family, at the
+ * mixed path's precision. */
 int cuwaves_autotune(cuw_handle* h, double* out, int n);
 /* Check of the split-precision tensor-core product (no reference
  * counterpart): C(M,N) = A(M,K) * B(N,K)^T on device buffers, FP64 row-major

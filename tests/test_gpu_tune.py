@@ -68,3 +68,37 @@ def test_fft_plan_variants_agree(inputs, prec, oracle):
         w2.set_option(cuwaves.CUW_OPT_FFT_VARIANT, 1)
     assert e.value.code == 6
     w2.close()
+
+
+def test_contraction_tile_families(inputs):
+    """The two tile families of the mixed path's contractions: split-tf32
+    tcgen05 tiles (128 x 128 x 8) and FP64 DMMA tiles (64 x 64 x 4).  A CP step
+    on either agrees with the FP64 handle within the mixed path's tolerance,
+    the DMMA tiles (FP64 products, FP32 transforms) closer than that; FP64
+    handles refuse the tcgen05 family; the autotuner times both and keeps the
+    faster."""
+    inp = inputs["H2O2"]
+    ref = cuwaves.open_waves(inp, precision=CUW_PREC_FP64).setup().initialize()
+    with pytest.raises(cuwaves.WavesError):
+        ref.set_option(cuwaves.CUW_OPT_CONTRACTION_TILES, 0)
+    ref.set_option(cuwaves.CUW_OPT_CONTRACTION_TILES, 1)
+    state = (ref.download_psi(cuwaves.CUW_PSI0), ref.download_psi(cuwaves.CUW_PSIM), ref.get_proj())
+    o_ref, f_ref = ref.cp_step(move_atoms=True)
+    errs = {}
+    for fam in (0, 1):
+        w = cuwaves.open_waves(inp, precision=CUW_PREC_MIXED).setup()
+        w.upload_psi(cuwaves.CUW_PSI0, state[0])
+        w.upload_psi(cuwaves.CUW_PSIM, state[1])
+        w.set_proj(state[2])
+        w.set_option(cuwaves.CUW_OPT_CONTRACTION_TILES, fam)
+        o, f = w.cp_step(move_atoms=True)
+        errs[fam] = (abs(o[0] - o_ref[0]) / inp["nat"], float(np.abs(f - f_ref).max()))
+        w.close()
+    for fam, (de, df) in errs.items():
+        assert de < 1e-6 and df < 1e-4, (fam, de, df)
+    w = cuwaves.open_waves(inp, precision=CUW_PREC_MIXED).setup().initialize()
+    t = w.autotune()
+    assert t["dmma_tiles"] in (0.0, 1.0) and t["tc_tiles_ms"] > 0 and t["dmma_tiles_ms"] > 0
+    assert t["dmma_tiles"] == float(t["dmma_tiles_ms"] < t["tc_tiles_ms"])
+    w.close()
+    ref.close()
