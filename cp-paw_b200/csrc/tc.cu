@@ -218,8 +218,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // ---------------------------------------------------------------------------
 // ADDPRO with the step epilogues (WAVES_ADDPRO, src/paw_waves1.f90:5908-6067,
-// and the epilogues of the FP64 k_addpro): 128 g x 32 bands per CTA, the tile
-// columns hold C1 (hproj) products for the bands, then C2 (oproj) products.
+// and the epilogues of the FP64 k_addpro): 128 g x 32 bands per CTA (band
+// tile blockIdx.x, G tile blockIdx.y), the tile columns hold C1 (hproj)
+// products for the bands, then C2 (oproj) products.
 // ---------------------------------------------------------------------------
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -229,13 +230,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                 int* __restrict__ err) {
   constexpr bool USE_H = (MODE != ADDPRO_OPSI);
   constexpr bool USE_O = (MODE != ADDPRO_HPSI);
-  const int g0 = blockIdx.x * 128, b0 = blockIdx.y * 32;
+  // the band tiles of one G tile are consecutive blocks (blockIdx.x), so the
+  // second read of the G tile's projector rows comes from L2
+  const int g0 = blockIdx.y * 128, b0 = blockIdx.x * 32;
   // raw slot: Pf box 8 p x 128 g (1 KB rows); zeros past NGL and NPRO.  B:
   // [C1 | C2] of bands b0..b0+31, split (k_bsplit, zero where unused)
   auto load = [&](int c, int lane, tc::Copier& cp) {
     if (lane == 0) cp.tensor(0, &tm_pf, 2 * g0, c * kCK, 8192);
   };
-  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, bc, nchk, blockIdx.y, c); };
+  auto load_b = [&](int c, int lane, tc::Copier& cp) { load_bsplit(cp, lane, bc, nchk, blockIdx.x, c); };
   auto a_row = [&](int c, const unsigned char* raw, int r, int kh, float (&v)[8]) {  // Pf(g, p), K = p
 #pragma unroll
     for (int i = 0; i < 4; ++i) a_put<false>(v, i, at<float2>(raw, (4 * kh + i) * 1024 + r * 8));
@@ -1059,7 +1062,7 @@ int tc_proj(Handle* h, const double2* psi, double2* proj) {
 
 int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const StepCoef& sc) {
   const int ngl = h->d.ngl, nbh = h->d.nbh, npro = h->npro;
-  const dim3 grid(ceil_div(ngl, 128), ceil_div(nbh, 32));
+  const dim3 grid(ceil_div(nbh, 32), ceil_div(ngl, 128));
   Device& g = h->g;
   CUtensorMap tpf;
   CUW_RET(make_map(h, &tpf, g.pf, false, 2ll * ngl, npro, 2ll * h->ldg, 256, 8, CU_TENSOR_MAP_SWIZZLE_NONE));
