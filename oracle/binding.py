@@ -27,6 +27,24 @@ def build(force: bool = False) -> str:
     return LIB
 
 
+def blas_path():
+    """The OpenBLAS bundled with scipy (its CBLAS ZGEMM), or None.  The
+    reference's fast build links a BLAS for the ZGEMMs of LIB$SCALARPRODUCTC8
+    and LIB$ADDPRODUCTC8; the oracle uses this one when it is there
+    (CPWAVES_ORACLE_BLAS=0 keeps the plain loops)."""
+    if os.environ.get("CPWAVES_ORACLE_BLAS", "1") == "0":
+        return None
+    import glob
+    import importlib.util
+
+    spec = importlib.util.find_spec("scipy")
+    if spec is None or not spec.submodule_search_locations:
+        return None
+    libs = os.path.join(os.path.dirname(list(spec.submodule_search_locations)[0]), "scipy.libs")
+    found = sorted(glob.glob(os.path.join(libs, "libscipy_openblas-*.so")))
+    return found[0] if found else None
+
+
 def library() -> C.CDLL:
     global _lib
     if _lib is None:
@@ -37,7 +55,17 @@ def library() -> C.CDLL:
         for name in ("orc_getig",):
             getattr(_lib, name).restype = C.c_int
         _lib.orc_max_threads.restype = C.c_int
+        _lib.orc_use_blas.argtypes = [C.c_char_p]
+        _lib.orc_use_blas.restype = C.c_int
+        _lib.orc_blas_in_use.restype = C.c_int
+        path = blas_path()
+        if path:
+            _lib.orc_use_blas(path.encode())
     return _lib
+
+
+def blas_in_use() -> bool:
+    return bool(library().orc_blas_in_use())
 
 
 def fns() -> dict:

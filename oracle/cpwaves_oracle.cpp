@@ -17,7 +17,10 @@
 // reference's boundary is restated here:
 //   FFTW3 fftw_plan_dft_1d (src/paw_library.f90:2635-2728) -> fft1d() below,
 //     same sign/scale convention (GTOR: +i, unscaled; RTOG: -i, 1/LEN);
-//   BLAS ZGEMM/ZHERK/DGEMM/DSYRK (src/paw_library.f90:2074-2260) -> plain loops;
+//   BLAS ZGEMM/ZHERK/DGEMM/DSYRK (src/paw_library.f90:2074-2260) -> ZGEMM of
+//     an OpenBLAS loaded at run time by orc_use_blas (the build bundled with
+//     scipy; the reference's fast build links a BLAS the same way), else plain
+//     loops;
 //   LAPACK DSYEV (src/paw_library.f90:1555-1620) -> cyclic Jacobi (jacobi_eig),
 //     whose eigenpairs agree with DSYEV up to order and sign; the only consumer
 //     (WAVES_ORTHO_X) is invariant under both.
@@ -26,6 +29,8 @@
 // identity here (src/paw_mpelib.f90:267 serial build).
 
 #include "../include/cuwaves.h"
+
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -252,6 +257,20 @@ static inline size_t PJ(const orc_handle* h, int ib, int ipro) {  // PROJ(1,ib,i
   return (size_t)ib + (size_t)h->d.nbh * ipro;
 }
 
+// ZGEMM of the BLAS that LIB$SCALARPRODUCTC8 and LIB$ADDPRODUCTC8 call
+// (src/paw_library.f90:2088-2141), through the CBLAS interface of a library
+// opened by orc_use_blas; null: the plain loops below.
+typedef void (*cblas_zgemm_t)(int order, int ta, int tb, int m, int n, int k, const void* alpha, const void* a,
+                              int lda, const void* b, int ldb, const void* beta, void* c, int ldc);
+typedef void (*blas_threads_t)(int);
+static cblas_zgemm_t g_zgemm = nullptr;
+static blas_threads_t g_blas_threads = nullptr;
+static void zgemm(char ta, char tb, int m, int n, int k, cplx alpha, const cplx* a, int lda, const cplx* b, int ldb,
+                  cplx beta, cplx* c, int ldc) {
+  auto op = [](char t) { return t == 'N' ? 111 : (t == 'T' ? 112 : 113); };  // CblasNoTrans/Trans/ConjTrans
+  g_zgemm(102 /* CblasColMajor */, op(ta), op(tb), m, n, k, &alpha, a, lda, b, ldb, &beta, c, ldc);
+}
+
 extern "C" {
 
 int orc_set_threads(orc_handle* h, int n) {
@@ -259,8 +278,29 @@ int orc_set_threads(orc_handle* h, int n) {
 #ifdef _OPENMP
   if (n > 0) omp_set_num_threads(n);
 #endif
+  if (n > 0 && g_blas_threads) g_blas_threads(n);
   return CUW_OK;
 }
+
+// Opens a BLAS with a CBLAS ZGEMM (symbols cblas_zgemm or, in scipy's bundled
+// OpenBLAS, scipy_cblas_zgemm); 0 when it is in use, else the loops stay.
+int orc_use_blas(const char* path) {
+  if (!path) {
+    g_zgemm = nullptr;
+    return CUW_OK;
+  }
+  void* lib = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+  if (!lib) return CUW_ERR_ARG;
+  void* f = dlsym(lib, "scipy_cblas_zgemm");
+  if (!f) f = dlsym(lib, "cblas_zgemm");
+  void* t = dlsym(lib, "scipy_openblas_set_num_threads");
+  if (!t) t = dlsym(lib, "openblas_set_num_threads");
+  if (!f) return CUW_ERR_ARG;
+  g_zgemm = reinterpret_cast<cblas_zgemm_t>(f);
+  g_blas_threads = reinterpret_cast<blas_threads_t>(t);
+  return CUW_OK;
+}
+int orc_blas_in_use(void) { return g_zgemm ? 1 : 0; }
 
 int orc_max_threads(void) {
 #ifdef _OPENMP
@@ -650,8 +690,32 @@ static void expandpro(const orc_handle* h, int iat, const cplx* eigr, cplx* pro)
 
 // WAVES_PROJECTIONS (src/paw_waves1.f90:5746-5905, unblocked branch):
 // PROPSI(1,IB,IPRO) = GWEIGHT * sum_G conj(PRO(G,LMN)) PSI(G,IB)
+// PRO(G, IPRO) of every atom at positions R (WAVES_EXPANDPRO per atom)
+static void expandpro_all(const orc_handle* h, const double* R, std::vector<cplx>& pro) {
+  const int ngl = h->d.ngl;
+  pro.resize((size_t)ngl * h->npro);
+#pragma omp parallel
+  {
+    std::vector<cplx> eigr(ngl);
+#pragma omp for schedule(dynamic)
+    for (int iat = 0; iat < h->d.nat; ++iat) {
+      structurefactor(h, R + 3 * iat, eigr.data());
+      expandpro(h, iat, eigr.data(), &pro[(size_t)ngl * h->p_ipro0[iat]]);
+    }
+  }
+}
+
 static void projections(const orc_handle* h, const double* R, const cplx* psi, cplx* propsi) {
   const int ngl = h->d.ngl, nbh = h->d.nbh;
+  if (g_zgemm && h->npro > 0) {
+    // ZGEMM('C','N') of LIB$SCALARPRODUCTC8 over all atoms at once
+    std::vector<cplx> pro, c((size_t)h->npro * nbh);
+    expandpro_all(h, R, pro);
+    zgemm('C', 'N', h->npro, nbh, ngl, h->gweight, pro.data(), ngl, psi, ngl, 0.0, c.data(), h->npro);
+    for (int ib = 0; ib < nbh; ++ib)
+      for (int ip = 0; ip < h->npro; ++ip) propsi[PJ(h, ib, ip)] = c[ip + (size_t)h->npro * ib];
+    return;
+  }
 #pragma omp parallel
   {
     std::vector<cplx> eigr(ngl), pro((size_t)ngl * h->lmnxx);
@@ -676,6 +740,13 @@ static void projections(const orc_handle* h, const double* R, const cplx* psi, c
 // WAVES_ADDPRO (src/paw_waves1.f90:5908-6067): PSI(G,IB) += sum PRO(G,LMN) PROPSI(1,IB,IPRO)
 static void addpro(const orc_handle* h, const double* R, cplx* psi, const cplx* propsi) {
   const int ngl = h->d.ngl, nbh = h->d.nbh;
+  if (g_zgemm && h->npro > 0) {
+    // ZGEMM('N','T') of LIB$ADDPRODUCTC8: PSI += PRO * PROPSI^T
+    std::vector<cplx> pro;
+    expandpro_all(h, R, pro);
+    zgemm('N', 'T', ngl, nbh, h->npro, 1.0, pro.data(), ngl, propsi, nbh, 1.0, psi, ngl);
+    return;
+  }
   std::vector<cplx> eigrall((size_t)ngl * h->d.nat);
 #pragma omp parallel for
   for (int iat = 0; iat < h->d.nat; ++iat) structurefactor(h, R + 3 * iat, &eigrall[(size_t)ngl * iat]);
@@ -804,6 +875,19 @@ int orc_vpsi_only(orc_handle* h) {
 static void scalarproduct(const orc_handle* h, char id, int n1, const cplx* f1, int n2,
                           const cplx* f2, cplx* mat) {
   const int ngl = h->d.ngl;
+  if (g_zgemm) {
+    if (id == '-') {
+      // sum_G F1(G) F2(-G): the gathered F2(-G) as the second operand
+      std::vector<cplx> f2m((size_t)ngl * n2);
+#pragma omp parallel for schedule(static)
+      for (int i2 = 0; i2 < n2; ++i2)
+        for (int ig = 0; ig < ngl; ++ig) f2m[ig + (size_t)ngl * i2] = f2[h->minusg[ig] + (size_t)ngl * i2];
+      zgemm('T', 'N', n1, n2, ngl, h->gweight, f1, ngl, f2m.data(), ngl, 0.0, mat, n1);
+    } else {
+      zgemm('C', 'N', n1, n2, ngl, h->gweight, f1, ngl, f2, ngl, 0.0, mat, n1);
+    }
+    return;
+  }
 #pragma omp parallel for collapse(2) schedule(static)
   for (int i2 = 0; i2 < n2; ++i2)
     for (int i1 = 0; i1 < n1; ++i1) {
@@ -981,6 +1065,16 @@ static void addopsi(const orc_handle* h, cplx* psibar, const cplx* opsi, const c
   const int ngl = h->d.ngl, nbh = h->d.nbh, nb = h->d.nb;
   std::vector<cplx> l1, l2;
   lambda12(nb, nbh, lambda, l1, l2);
+  if (g_zgemm) {
+    // PSIBAR += OPSI L1 + conj(OPSI(-G)) L2 (two ZGEMMs, waves2:597-610)
+    std::vector<cplx> om((size_t)ngl * nbh);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nbh; ++k)
+      for (int ig = 0; ig < ngl; ++ig) om[ig + (size_t)ngl * k] = std::conj(opsi[PS(h, h->minusg[ig], k)]);
+    zgemm('N', 'N', ngl, nbh, nbh, 1.0, opsi, ngl, l1.data(), nbh, 1.0, psibar, ngl);
+    zgemm('N', 'N', ngl, nbh, nbh, 1.0, om.data(), ngl, l2.data(), nbh, 1.0, psibar, ngl);
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (int ig = 0; ig < ngl; ++ig) {
     int mg = h->minusg[ig];
@@ -1460,6 +1554,15 @@ int orc_force(orc_handle* h, double* force) {
       lam[i + (size_t)nb * j] = -h->rlam0[i + (size_t)nb * j] * 0.5 * (h->occ[i] + h->occ[j]);
   addoproj(h, h->npro, dedproj.data(), oproj.data(), lam.data(), nbh);
   std::fill(force, force + 3 * nat, 0.0);
+  // with BLAS: DEDPRO(G,IPRO) = sum_IB PSI(G,IB) conj(DEDPROJ(IB,IPRO)) of all
+  // atoms by one ZGEMM (WAVES_DEDPRO, waves1:5694-5745)
+  std::vector<cplx> dall;
+  if (g_zgemm && h->npro > 0) {
+    std::vector<cplx> dc(dedproj.size());
+    for (size_t k = 0; k < dc.size(); ++k) dc[k] = std::conj(dedproj[k]);
+    dall.resize((size_t)ngl * h->npro);
+    zgemm('N', 'N', ngl, h->npro, nbh, 1.0, h->psi0.data(), ngl, dc.data(), nbh, 0.0, dall.data(), ngl);
+  }
 #pragma omp parallel
   {
     std::vector<cplx> dedpro((size_t)ngl * h->lmnxx), eigr(ngl), tmp(ngl);
@@ -1469,11 +1572,15 @@ int orc_force(orc_handle* h, double* force) {
       // DEDPRO(G,LMN) = sum_IB PSI(G,IB) conj(DEDPROJ(IB,LMN)), then TINV symmetrise
       for (int lmn = 0; lmn < lmnx; ++lmn) {
         cplx* d = &dedpro[(size_t)ngl * lmn];
-        for (int ig = 0; ig < ngl; ++ig) d[ig] = 0.0;
-        for (int ib = 0; ib < nbh; ++ib) {
-          cplx c = std::conj(dedproj[PJ(h, ib, i0 + lmn)]);
-          const cplx* p = &h->psi0[PS(h, 0, ib)];
-          for (int ig = 0; ig < ngl; ++ig) d[ig] += p[ig] * c;
+        if (!dall.empty()) {
+          std::copy(&dall[(size_t)ngl * (i0 + lmn)], &dall[(size_t)ngl * (i0 + lmn + 1)], d);
+        } else {
+          for (int ig = 0; ig < ngl; ++ig) d[ig] = 0.0;
+          for (int ib = 0; ib < nbh; ++ib) {
+            cplx c = std::conj(dedproj[PJ(h, ib, i0 + lmn)]);
+            const cplx* p = &h->psi0[PS(h, 0, ib)];
+            for (int ig = 0; ig < ngl; ++ig) d[ig] += p[ig] * c;
+          }
         }
         for (int ig = 0; ig < ngl; ++ig) tmp[ig] = std::conj(d[h->minusg[ig]]);
         for (int ig = 0; ig < ngl; ++ig) d[ig] = 0.5 * (d[ig] + tmp[ig]);
