@@ -14,7 +14,8 @@ not shard, one system per GPU); `e2e` is the same metric through the C ABI
 with per-step host buffers (V(r), DH and positions uploaded from pinned host
 memory, energies and forces read back).  --impl reference times the CPU
 restatement of the reference (the reference itself cannot be compiled in this
-image: no Fortran compiler, FFTW, BLAS or LAPACK) on all host cores.
+image: no Fortran compiler, FFTW or LAPACK) on all host cores, its ZGEMMs on the
+OpenBLAS that scipy bundles where the reference calls BLAS.
 """
 from __future__ import annotations
 
@@ -709,8 +710,9 @@ def cpu_baseline(args):
             break
     dt = time.perf_counter() - t0
     w.close()
+    gemm = "ZGEMM on the bundled OpenBLAS" if binding.blas_in_use() else "GEMMs as OpenMP loops"
     return {"value": round(n / dt, 5), "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"{n} CP steps of {args.system} after one warm-up step ({dt:.1f} s)"}
+            "sample": f"{n} CP steps of {args.system} after one warm-up step ({dt:.1f} s); {gemm}"}
 
 
 def run_reference(args):
@@ -741,7 +743,9 @@ def run_reference(args):
             "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": "port",
                              "sample": f"{args.steps} CP steps of {args.system} after {args.warmup} warm-up steps; "
                                        "the CPU restatement of the reference (the Fortran reference cannot be "
-                                       "built here: no Fortran compiler, FFTW, BLAS or LAPACK)"},
+                                       "built here: no Fortran compiler, FFTW or LAPACK); "
+                                       + ("its ZGEMMs on the OpenBLAS bundled with scipy, as the reference's "
+                                          "BLAS calls" if binding.blas_in_use() else "GEMMs as OpenMP loops")},
             "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -64,13 +64,19 @@ static inline cplx mipow(int l) {
 // 1-D mixed-radix DFT (stand-in for FFTW's fftw_plan_dft_1d).
 // dir=+1: y_k = sum_j x_j exp(+2 pi i jk/n)   (FFTW_BACKWARD, 'GTOR')
 // dir=-1: y_k = sum_j x_j exp(-2 pi i jk/n)   (FFTW_FORWARD,  'RTOG', unscaled)
-// Recursive decimation in time over the prime factors of n.
+// Iterative self-sorting (Stockham) form over the factors of n: stage s of
+// radix R, after the stages whose radices multiply to Ns, takes for every
+// j < n/R the R inputs in[j + r n/R], multiplies input r by
+// exp(dir 2 pi i r k / (Ns R)) with k = j mod Ns, does an R-point DFT and
+// stores output q at (j / Ns) Ns R + k + q Ns.  Twiddles are tabulated per
+// stage when the plan is made; radices 2, 3 and 4 have their own butterflies.
 // ---------------------------------------------------------------------------
 struct FFTPlan {
   int n = 0;
   int dir = 0;
   std::vector<int> factors;
-  std::vector<cplx> w;  // w[k] = exp(dir*2 pi i k/n)
+  std::vector<std::vector<cplx>> tw;  // per stage: (Ns, R-1) twiddles
+  std::vector<std::vector<cplx>> rt;  // per stage: R-th roots exp(dir 2 pi i q / R)
 };
 
 static void factorize(int n, std::vector<int>& f) {
@@ -87,50 +93,83 @@ static void factorize(int n, std::vector<int>& f) {
 static void plan_init(FFTPlan& P, int n, int dir) {
   P.n = n; P.dir = dir;
   factorize(n, P.factors);
-  P.w.resize(n);
-  for (int k = 0; k < n; ++k) {
-    double a = 2.0 * PI * (double)k / (double)n;
-    P.w[k] = cplx(std::cos(a), dir * std::sin(a));
+  P.tw.clear();
+  P.rt.clear();
+  int ns = 1;
+  for (int r : P.factors) {
+    std::vector<cplx> t((size_t)ns * (r - 1)), w(r);
+    for (int k = 0; k < ns; ++k)
+      for (int q = 1; q < r; ++q) {
+        const double a = 2.0 * PI * (double)q * (double)k / ((double)ns * r);
+        t[(size_t)k * (r - 1) + q - 1] = cplx(std::cos(a), dir * std::sin(a));
+      }
+    for (int q = 0; q < r; ++q) {
+      const double a = 2.0 * PI * (double)q / (double)r;
+      w[q] = cplx(std::cos(a), dir * std::sin(a));
+    }
+    P.tw.push_back(std::move(t));
+    P.rt.push_back(std::move(w));
+    ns *= r;
   }
 }
 
-// out[k*ostride] for k<n = DFT of in[j*istride], j<n, using factors[fi..]
-static void fft_rec(const FFTPlan& P, const cplx* in, cplx* out, int n, int istride,
-                    size_t fi, int wstride) {
-  if (n == 1) { out[0] = in[0]; return; }
-  int r = P.factors[fi];
-  int m = n / r;
-  // sub-transforms of length m on decimated inputs
-  for (int q = 0; q < r; ++q)
-    fft_rec(P, in + q * istride, out + q * m, m, istride * r, fi + 1, wstride * r);
-  // butterflies: out holds r blocks of length m: X_q[k]
-  cplx tmp[64];
-  for (int k = 0; k < m; ++k) {
-    for (int q = 0; q < r; ++q) {
-      // twiddle W_n^{qk}
-      cplx t = out[q * m + k];
-      if (q && k) t *= P.w[(size_t)((long)wstride * q * k % P.n)];
-      tmp[q] = t;
-    }
-    for (int s = 0; s < r; ++s) {
-      cplx acc = 0.0;
-      for (int q = 0; q < r; ++q) {
-        long idx = (long)wstride * m * ((long)q * s % r) % P.n;
-        acc += tmp[q] * P.w[idx];
+static void fft_stages(const FFTPlan& P, cplx* a, cplx* b) {
+  const int n = P.n;
+  const double sd = (double)P.dir;
+  cplx* in = a;
+  cplx* out = b;
+  int ns = 1;
+  for (size_t st = 0; st < P.factors.size(); ++st) {
+    const int r = P.factors[st], nr = n / r;
+    const cplx* tw = P.tw[st].data();
+    const cplx* rt = P.rt[st].data();
+    for (int j = 0; j < nr; ++j) {
+      const int k = j % ns;
+      const size_t o = (size_t)(j / ns) * ns * r + k;
+      cplx v[64];
+      v[0] = in[j];
+      for (int q = 1; q < r; ++q) v[q] = in[j + (size_t)q * nr] * tw[(size_t)k * (r - 1) + q - 1];
+      if (r == 2) {
+        out[o] = v[0] + v[1];
+        out[o + ns] = v[0] - v[1];
+      } else if (r == 4) {
+        const cplx s0 = v[0] + v[2], s1 = v[0] - v[2], s2 = v[1] + v[3];
+        const cplx d = v[1] - v[3];
+        const cplx s3(-sd * d.imag(), sd * d.real());  // dir * i * (v1 - v3)
+        out[o] = s0 + s2;
+        out[o + ns] = s1 + s3;
+        out[o + 2 * (size_t)ns] = s0 - s2;
+        out[o + 3 * (size_t)ns] = s1 - s3;
+      } else if (r == 3) {
+        const cplx s = v[1] + v[2], d = v[1] - v[2];
+        const cplx m = v[0] - 0.5 * s;
+        const double c = sd * 0.86602540378443864676;  // dir * sin(2 pi / 3)
+        const cplx id(-c * d.imag(), c * d.real());
+        out[o] = v[0] + s;
+        out[o + ns] = m + id;
+        out[o + 2 * (size_t)ns] = m - id;
+      } else {
+        for (int q = 0; q < r; ++q) {
+          cplx acc = v[0];
+          for (int p = 1; p < r; ++p) acc += v[p] * rt[(size_t)(p * q) % r];
+          out[o + (size_t)q * ns] = acc;
+        }
       }
-      out[s * m + k] = acc;
     }
+    std::swap(in, out);
+    ns *= r;
   }
+  if (in != a) std::copy(in, in + n, a);
 }
 
 static void fft1d(const FFTPlan& P, cplx* data, int stride, std::vector<cplx>& work) {
   int n = P.n;
   work.resize(2 * n);
-  cplx* in = work.data();
-  cplx* out = work.data() + n;
-  for (int j = 0; j < n; ++j) in[j] = data[(size_t)j * stride];
-  fft_rec(P, in, out, n, 1, 0, 1);
-  for (int j = 0; j < n; ++j) data[(size_t)j * stride] = out[j];
+  cplx* a = work.data();
+  cplx* b = work.data() + n;
+  for (int j = 0; j < n; ++j) a[j] = data[(size_t)j * stride];
+  fft_stages(P, a, b);
+  for (int j = 0; j < n; ++j) data[(size_t)j * stride] = a[j];
 }
 
 // ---------------------------------------------------------------------------
@@ -232,6 +271,7 @@ struct orc_handle {
   std::vector<double> qlm;    // (LMRXX, NAT) multipole moments of the one-centre densities
   bool scf = false;           // cp_step forms V(r) from the density of PSI0 first
   bool safeortho = true, swapstates = false;  // TSAFEORTHO, TSWAPSTATES (waves1:221-222)
+  mutable std::vector<cplx> protab;  // work table PRO(G, IPRO) of the ZGEMM path (kept to reuse its pages)
   // cell friction of WAVES$PROPAGATE with TSTRESS (waves1:6524-6543):
   // FRICMAT = CELL 'PSIANNEMAT' (3,3), EMASS, EMASSCG2, GSET%DBUCKET
   bool tstress = false;
@@ -262,8 +302,11 @@ static inline size_t PJ(const orc_handle* h, int ib, int ipro) {  // PROJ(1,ib,i
 // opened by orc_use_blas; null: the plain loops below.
 typedef void (*cblas_zgemm_t)(int order, int ta, int tb, int m, int n, int k, const void* alpha, const void* a,
                               int lda, const void* b, int ldb, const void* beta, void* c, int ldc);
+typedef void (*cblas_dgemm_t)(int order, int ta, int tb, int m, int n, int k, double alpha, const double* a, int lda,
+                              const double* b, int ldb, double beta, double* c, int ldc);
 typedef void (*blas_threads_t)(int);
 static cblas_zgemm_t g_zgemm = nullptr;
+static cblas_dgemm_t g_dgemm = nullptr;
 static blas_threads_t g_blas_threads = nullptr;
 static void zgemm(char ta, char tb, int m, int n, int k, cplx alpha, const cplx* a, int lda, const cplx* b, int ldb,
                   cplx beta, cplx* c, int ldc) {
@@ -287,6 +330,7 @@ int orc_set_threads(orc_handle* h, int n) {
 int orc_use_blas(const char* path) {
   if (!path) {
     g_zgemm = nullptr;
+    g_dgemm = nullptr;
     return CUW_OK;
   }
   void* lib = dlopen(path, RTLD_NOW | RTLD_LOCAL);
@@ -295,8 +339,11 @@ int orc_use_blas(const char* path) {
   if (!f) f = dlsym(lib, "cblas_zgemm");
   void* t = dlsym(lib, "scipy_openblas_set_num_threads");
   if (!t) t = dlsym(lib, "openblas_set_num_threads");
+  void* d = dlsym(lib, "scipy_cblas_dgemm");
+  if (!d) d = dlsym(lib, "cblas_dgemm");
   if (!f) return CUW_ERR_ARG;
   g_zgemm = reinterpret_cast<cblas_zgemm_t>(f);
+  g_dgemm = reinterpret_cast<cblas_dgemm_t>(d);
   g_blas_threads = reinterpret_cast<blas_threads_t>(t);
   return CUW_OK;
 }
@@ -693,7 +740,7 @@ static void expandpro(const orc_handle* h, int iat, const cplx* eigr, cplx* pro)
 // PRO(G, IPRO) of every atom at positions R (WAVES_EXPANDPRO per atom)
 static void expandpro_all(const orc_handle* h, const double* R, std::vector<cplx>& pro) {
   const int ngl = h->d.ngl;
-  pro.resize((size_t)ngl * h->npro);
+  if (pro.size() != (size_t)ngl * h->npro) pro.resize((size_t)ngl * h->npro);
 #pragma omp parallel
   {
     std::vector<cplx> eigr(ngl);
@@ -709,7 +756,8 @@ static void projections(const orc_handle* h, const double* R, const cplx* psi, c
   const int ngl = h->d.ngl, nbh = h->d.nbh;
   if (g_zgemm && h->npro > 0) {
     // ZGEMM('C','N') of LIB$SCALARPRODUCTC8 over all atoms at once
-    std::vector<cplx> pro, c((size_t)h->npro * nbh);
+    std::vector<cplx>& pro = h->protab;
+    std::vector<cplx> c((size_t)h->npro * nbh);
     expandpro_all(h, R, pro);
     zgemm('C', 'N', h->npro, nbh, ngl, h->gweight, pro.data(), ngl, psi, ngl, 0.0, c.data(), h->npro);
     for (int ib = 0; ib < nbh; ++ib)
@@ -742,7 +790,7 @@ static void addpro(const orc_handle* h, const double* R, cplx* psi, const cplx* 
   const int ngl = h->d.ngl, nbh = h->d.nbh;
   if (g_zgemm && h->npro > 0) {
     // ZGEMM('N','T') of LIB$ADDPRODUCTC8: PSI += PRO * PROPSI^T
-    std::vector<cplx> pro;
+    std::vector<cplx>& pro = h->protab;
     expandpro_all(h, R, pro);
     zgemm('N', 'T', ngl, nbh, h->npro, 1.0, pro.data(), ngl, propsi, nbh, 1.0, psi, ngl);
     return;
@@ -969,7 +1017,15 @@ static void onecoverlap(const orc_handle* h, const cplx* proj1, const cplx* proj
 }
 
 // plain real matrix helpers (column-major n x n)
+// LIB$MATMULR8 / LIB$SCALARPRODUCTR8 / LIB$DYADSUMR8 (DGEMM in the reference,
+// src/paw_library.f90:2161-2218): the loaded BLAS, else loops
+static bool dgemm_nn(char ta, char tb, int n, const double* a, const double* b, double* c) {
+  if (!g_dgemm) return false;
+  g_dgemm(102, ta == 'T' ? 112 : 111, tb == 'T' ? 112 : 111, n, n, n, 1.0, a, n, b, n, 0.0, c, n);
+  return true;
+}
 static void matmul(int n, const double* a, const double* b, double* c) {  // C = A B
+  if (dgemm_nn('N', 'N', n, a, b, c)) return;
   for (int j = 0; j < n; ++j)
     for (int i = 0; i < n; ++i) {
       double s = 0;
@@ -978,6 +1034,7 @@ static void matmul(int n, const double* a, const double* b, double* c) {  // C =
     }
 }
 static void matmul_tn(int n, const double* a, const double* b, double* c) {  // C = A^T B
+  if (dgemm_nn('T', 'N', n, a, b, c)) return;
   for (int j = 0; j < n; ++j)
     for (int i = 0; i < n; ++i) {
       double s = 0;
@@ -986,6 +1043,7 @@ static void matmul_tn(int n, const double* a, const double* b, double* c) {  // 
     }
 }
 static void matmul_nt(int n, const double* a, const double* b, double* c) {  // C = A B^T
+  if (dgemm_nn('N', 'T', n, a, b, c)) return;
   for (int j = 0; j < n; ++j)
     for (int i = 0; i < n; ++i) {
       double s = 0;
@@ -1556,7 +1614,8 @@ int orc_force(orc_handle* h, double* force) {
   std::fill(force, force + 3 * nat, 0.0);
   // with BLAS: DEDPRO(G,IPRO) = sum_IB PSI(G,IB) conj(DEDPROJ(IB,IPRO)) of all
   // atoms by one ZGEMM (WAVES_DEDPRO, waves1:5694-5745)
-  std::vector<cplx> dall;
+  std::vector<cplx>& dall = h->protab;  // the work table of the ZGEMM path
+  dall.clear();
   if (g_zgemm && h->npro > 0) {
     std::vector<cplx> dc(dedproj.size());
     for (size_t k = 0; k < dc.size(); ++k) dc[k] = std::conj(dedproj[k]);
