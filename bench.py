@@ -621,6 +621,11 @@ def run_batched(args):
             w.close()
     inps = [systems.build_inputs(s) for s in systems.config_batch_mix(64)]
     ws = [cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup().initialize() for inp in inps]
+    tiles = []
+    if not args.no_autotune:
+        # launch shapes and contraction tile family per shape (the table keeps
+        # one choice per shape, so repeated shapes are not timed again)
+        tiles = [w.autotune()["dmma_tiles"] for w in ws]
     small = timed_batch(ws, args.batched_steps // 2)
     # the same sets one at a time (each step a graph replay of its own)
     for w in ws:
@@ -639,6 +644,7 @@ def run_batched(args):
                       "wall clock over the timed calls after graph capture and warm-up",
             "small_systems": {"value": round(small, 2), "unit": "CP steps/s (all systems)", "systems": len(ws),
                               "one_at_a_time_value": round(alone, 2), "precision": "mixed",
+                              "dmma_tile_sets": int(sum(tiles)) if tiles else None,
                               "sizes": "Si2-Si16 bulk (4-32 bands, 18^3 and 18x18x36 grids), Si2 and H2O molecules "
                                        "in 20-bohr boxes (4 bands, 36^3), 30 Ry"}}
 

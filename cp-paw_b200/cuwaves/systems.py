@@ -669,6 +669,8 @@ def named_system(name: str) -> System:
         return si_cell(2, a=10.26, disp=0.05, seed=1, name="Si64")
     if name == "H2O32":
         return water_box(32, grid=(72, 72, 72))
+    if name == "Si128":  # the largest system of the serving mix (256 bands)
+        return serving_system("Si", 128, 1)
     if name.startswith("Si") and name[2:].isdigit():
         return si_small(int(name[2:]))
     raise ValueError(name)
