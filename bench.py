@@ -774,6 +774,7 @@ def main():
     ap.add_argument("--quench-steps", type=int, default=300)
     ap.add_argument("--quench-friction", type=float, default=0.1)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving and batched runs")
+    ap.add_argument("--no-serving-stream", action="store_true", help="skip the serving streams, keep the batched runs")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-workers", type=int, default=8)
@@ -798,7 +799,7 @@ def main():
         if world == 1 and not args.no_precision:
             res["precision"] = run_precision(args)
     if not args.no_serving and world == 1:
-        res["serving"] = run_serving(args)
+        res["serving"] = None if args.no_serving_stream else run_serving(args)
         res["batched"] = run_batched(args)
     if rank == 0:
         if world > 1 or args.no_cpu:
