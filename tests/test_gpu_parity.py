@@ -208,6 +208,29 @@ def test_orthogonalize(name, oracle, inputs_cache):
     assert np.abs(gpu.get_rlam0() - cpu.get_rlam0()).max() < 1e-8
 
 
+@pytest.mark.parametrize("name", ["Si8", "H2O2"])
+def test_lyapunov_tolerance(name, oracle, inputs_cache):
+    """The inner Lyapunov solve of ORTHO_X at its default accuracy (1e-2 while
+    the residual is far from EPS, 1e-5 in the last iterations) against the
+    solve to rounding (CUW_OPT_LYAP_TOL = 0), from one state over six CP steps
+    with moving atoms: the same ORTHO_X iteration counts, energies within
+    1e-9 Ha and forces within 1e-8 Ha/bohr, with fewer fixed-point sweeps."""
+    inp, ref, cpu = make_pair(name, oracle, inputs_cache)
+    cpu.close()
+    ref.set_option(cuwaves.CUW_OPT_LYAP_TOL, 0.0)
+    w = cuwaves.open_waves(inp).setup()
+    sync_state(ref, w)
+    s0 = (ref.ortho_stats()["fixed_point_sweeps"], w.ortho_stats()["fixed_point_sweeps"])
+    for step in range(6):
+        (oa, fa), (ob, fb) = ref.cp_step(move_atoms=True), w.cp_step(move_atoms=True)
+        assert oa[4] == ob[4], f"step {step}: iterations {oa[4]} vs {ob[4]}"
+        assert abs(oa[0] - ob[0]) < 1e-9 and np.abs(fa - fb).max() < 1e-8
+    s1 = (ref.ortho_stats()["fixed_point_sweeps"], w.ortho_stats()["fixed_point_sweeps"])
+    assert s1[1] - s0[1] < s1[0] - s0[0]
+    ref.close()
+    w.close()
+
+
 def test_gramschmidt(oracle, inputs_cache):
     inp = systems.build_inputs(CASES["Si8-20Ry"]())
     gpu = cuwaves.open_waves(inp).setup()
