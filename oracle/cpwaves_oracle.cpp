@@ -589,12 +589,13 @@ int orc_set_rlam0(orc_handle* h, const double* r) {
 static void fft_gtor(const orc_handle* h, const cplx* fofg, cplx* fofr) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   const int ns = h->nstripe;
-  std::vector<cplx> work;
-  std::vector<cplx> fofg1((size_t)nr1 * ns, 0.0);
+  // work arrays kept per thread (no fresh pages on every transform)
+  static thread_local std::vector<cplx> work, fofg1, f;
+  fofg1.assign((size_t)nr1 * ns, 0.0);
   for (int ig = 0; ig < h->d.ngl; ++ig) fofg1[h->igtostripe[ig]] = fofg[ig];
   for (int s = 0; s < ns; ++s) fft1d(h->p1g, &fofg1[(size_t)nr1 * s], 1, work);
   // distribute onto FOFR(NR2,NR3,NR1L) (fft:2096-2118)
-  std::vector<cplx> f((size_t)nr1 * nr2 * nr3, 0.0);
+  f.assign((size_t)nr1 * nr2 * nr3, 0.0);
   const int imid = nr3 / 2;
   int nr3end1 = 1, nr3end2 = nr3;
   const size_t stride2 = (size_t)nr2 * nr3;
@@ -626,9 +627,10 @@ static void fft_gtor(const orc_handle* h, const cplx* fofg, cplx* fofr) {
 static void fft_rtog(const orc_handle* h, const cplx* fofr, cplx* fofg) {
   const int nr1 = h->d.nr1, nr2 = h->d.nr2, nr3 = h->d.nr3;
   const int ns = h->nstripe;
-  std::vector<cplx> work;
+  // work arrays kept per thread (no fresh pages on every transform)
+  static thread_local std::vector<cplx> work, f1, f2, fofg1;
   // FOFR1(IR3,IR2,IR1) = FOFR(IR1,IR2,IR3); z-lines
-  std::vector<cplx> f1((size_t)nr1 * nr2 * nr3);
+  f1.resize((size_t)nr1 * nr2 * nr3);
   for (int ir1 = 0; ir1 < nr1; ++ir1)
     for (int ir2 = 0; ir2 < nr2; ++ir2)
       for (int ir3 = 0; ir3 < nr3; ++ir3)
@@ -649,7 +651,7 @@ static void fft_rtog(const orc_handle* h, const cplx* fofr, cplx* fofg) {
   }
   if (nr3end1 == nr3end2) nr3end2 = nr3end2 + 1;
   // FOFR2(IR2,IR3,IR1) restricted to occupied z (fft:2262-2280)
-  std::vector<cplx> f2((size_t)nr1 * nr2 * nr3, 0.0);
+  f2.assign((size_t)nr1 * nr2 * nr3, 0.0);
   for (int ir1 = 0; ir1 < nr1; ++ir1)
     for (int ir2 = 0; ir2 < nr2; ++ir2) {
       for (int ir3 = 1; ir3 <= nr3end1; ++ir3)
@@ -671,7 +673,7 @@ static void fft_rtog(const orc_handle* h, const cplx* fofr, cplx* fofg) {
       for (int k = 0; k < nr2; ++k) p[k] *= sc2;
     }
   }
-  std::vector<cplx> fofg1((size_t)nr1 * ns, 0.0);
+  fofg1.assign((size_t)nr1 * ns, 0.0);
   for (int s = 0; s < ns; ++s) {
     int i23 = h->istripetoyz[s];
     for (int ir1 = 0; ir1 < nr1; ++ir1)
