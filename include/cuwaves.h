@@ -431,8 +431,7 @@ int cuwaves_tc_gemm_check(int M, int N, int K, const double* A, const double* B,
  * conj(PRO(G,p)) psi(G,b), the contraction of cuwaves_projections, for callers
  * that cannot call cudaMalloc (memory handed out only by a host pool, code
  * running under another program's memory cap or inside its stream capture).
- * There is no counterpart in the reference; WAVES_PROJECTIONS
- * (src/paw_waves1.f90:5746-5905) computes the same numbers on the host.
+ * There is no counterpart in the reference.
  * Every argument is a device pointer the caller owns:
  *   psi(ldg,nbh) complex, pdesc(4,npro) int (0-based atom, column of pro, LM, L
  *   of each projector), ylm(ngl,LMX), pro(ngl,NBAREPRO), eigr(ngl,nat) complex
