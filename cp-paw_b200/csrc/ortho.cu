@@ -1360,7 +1360,8 @@ __global__ void k_switch_lambda(double2* __restrict__ rlam0, double2* __restrict
 // ---------------------------------------------------------------------------
 // WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338) for real (Gamma-point)
 // PHIPHI, CHIPHI, CHICHI and the state order MAP (identity when map is null),
-// as one cluster of kOyCS CTAs.  WAVES_GRAMSCHMIDT (:2025-2177) passes one
+// as one cluster of kOyCS CTAs (one CTA for NB <= kOySmall, where a cluster
+// barrier costs more than a step's updates).  WAVES_GRAMSCHMIDT (:2025-2177) passes one
 // matrix S as all three; WAVES$ORTHOGONALIZE with SAFEORTHO = F (:361-386)
 // passes MAT, OMAT and OOMAT.  A, B, C, ALPHA and X are n x n in global
 // memory (L2).  pos[i] is the place of state i in MAP: "J > N in the order"
@@ -1379,7 +1380,7 @@ __global__ void k_switch_lambda(double2* __restrict__ rlam0, double2* __restrict
 //      it; the C update reads the copied row and column instead of a work array.
 // The arithmetic of each element is that of the one-CTA form.
 // ---------------------------------------------------------------------------
-constexpr int kOyCS = 8;
+constexpr int kOyCS = 8, kOySmall = 64;
 // ostatus[0] of a state order that failed its check (mapped by ortho_result)
 constexpr int kStatusOrder = 100;
 __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s1, const double* __restrict__ s2,
@@ -1399,7 +1400,7 @@ __global__ void __launch_bounds__(1024) k_ortho_y(const double* __restrict__ s1,
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const int tid = threadIdx.x, nt = blockDim.x;
-  const size_t gt = (size_t)rank * nt + tid, gstride = (size_t)kOyCS * nt;
+  const size_t gt = (size_t)rank * nt + tid, gstride = (size_t)cl.num_blocks() * nt;
   const double r8small = 1e-10;
   const size_t nn = (size_t)n * n;
   for (size_t k = gt; k < nn; k += gstride) {
@@ -1638,7 +1639,10 @@ static int ortho_x_launch(Handle* h, int use_e, int max_iter, double eps, const 
       cudaGetLastError();
     }
   }
-  int cs = 16;
+  // NB <= 32: one CTA holds every tile (products of at most 32^3 take it well
+  // under a microsecond, less than one cluster barrier), which also leaves the
+  // other SMs to the other sets of a batch; larger NB start from 16 CTAs
+  int cs = n <= 32 ? 1 : 16;
   cudaError_t e = cudaSuccess;
   bool launched = false;
   for (; cs >= 1 && !launched; cs /= 2) {
@@ -1795,13 +1799,14 @@ int ortho_y_general(Handle* h, const double* s1, const double* s2, const double*
   const int smem = (int)(sizeof(double) * 7 * (size_t)n + sizeof(int) * (size_t)n);
   CUW_TRY(smem_allow((const void*)k_ortho_y, smem));
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kOyCS);
+  const int cs = n <= kOySmall ? 1 : kOyCS;
+  cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(1024);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = h->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kOyCS;
+  attr[0].val.clusterDim.x = cs;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
