@@ -606,6 +606,17 @@ def run_batched(args):
         batch.close()
         return len(ws) * 2 * calls / dt
 
+    import torch
+
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+
+    def share(nsets):
+        # SMs each set's launch shapes assume (CUW_OPT_SM_SHARE): the sets of
+        # a batch share the device, so each launches fewer split-K blocks; in
+        # measurements, max(16, SMs / sets) did best for 8 Si64 cells (18) and
+        # for the 64 small systems (16), 3 % and 16 % above the whole device
+        return max(16, nsm // max(1, nsets))
+
     res = {}
     calls = max(1, args.steps // 2)
     for prec, tag in ((cuwaves.CUW_PREC_MIXED, "mixed"), (cuwaves.CUW_PREC_FP64, "fp64")):
@@ -614,6 +625,7 @@ def run_batched(args):
             inp = systems.build_inputs(systems.si_cell(2, a=10.26, disp=0.05, seed=1 + i, grid=(64, 64, 64),
                                                        name="Si64"))
             ws.append(cuwaves.open_waves(inp, precision=prec).setup().initialize())
+            ws[-1].set_option(cuwaves.CUW_OPT_SM_SHARE, share(args.batched_si64))
             if not args.no_autotune:
                 ws[-1].autotune()
         res[tag] = timed_batch(ws, calls)
@@ -621,14 +633,18 @@ def run_batched(args):
             w.close()
     inps = [systems.build_inputs(s) for s in systems.config_batch_mix(64)]
     ws = [cuwaves.open_waves(inp, precision=cuwaves.CUW_PREC_MIXED).setup().initialize() for inp in inps]
+    for w in ws:
+        w.set_option(cuwaves.CUW_OPT_SM_SHARE, share(len(ws)))
     tiles = []
     if not args.no_autotune:
         # launch shapes and contraction tile family per shape (the table keeps
         # one choice per shape, so repeated shapes are not timed again)
         tiles = [w.autotune()["dmma_tiles"] for w in ws]
     small = timed_batch(ws, args.batched_steps // 2)
-    # the same sets one at a time (each step a graph replay of its own)
+    # the same sets one at a time (each step a graph replay of its own), each
+    # with the whole device again
     for w in ws:
+        w.set_option(cuwaves.CUW_OPT_SM_SHARE, 0)
         w.cp_step(move_atoms=True)
     t0 = time.perf_counter()
     nsteps = max(2, args.batched_steps // 2)
@@ -640,11 +656,13 @@ def run_batched(args):
         w.close()
     return {"value": round(res["mixed"], 2), "unit": "CP steps/s (all Si64 cells)", "precision": "mixed",
             "si64_cells": args.batched_si64, "fp64_same_batch": round(res["fp64"], 2),
+            "sm_share_per_set": share(args.batched_si64),
             "timing": "one CUDA graph launch per two CP steps of every set (cuwaves_batch_step), synchronised; "
                       "wall clock over the timed calls after graph capture and warm-up",
             "small_systems": {"value": round(small, 2), "unit": "CP steps/s (all systems)", "systems": len(ws),
                               "one_at_a_time_value": round(alone, 2), "precision": "mixed",
                               "dmma_tile_sets": int(sum(tiles)) if tiles else None,
+                              "sm_share_per_set": share(len(ws)),
                               "sizes": "Si2-Si16 bulk (4-32 bands, 18^3 and 18x18x36 grids), Si2 and H2O molecules "
                                        "in 20-bohr boxes (4 bands, 36^3), 30 Ry"}}
 

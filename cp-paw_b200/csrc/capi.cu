@@ -510,6 +510,7 @@ extern "C" int cuwaves_create(const cuw_dims* dims, cuw_handle** out) {
   h->d.isp = nullptr;
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
+  h->nsm_dev = h->nsm;
   h->isp.resize(d.nat);
   for (int a = 0; a < d.nat; ++a) {
     h->isp[a] = dims->isp[a] - 1;
@@ -1678,6 +1679,13 @@ extern "C" int cuwaves_set_option(cuw_handle* hp, int option, double value) {
       h->stream_prio = want;
       h->drop_graphs();
       h->touch();
+      return CUW_OK;
+    }
+    case CUW_OPT_SM_SHARE: {
+      const int v = (int)value;
+      if ((double)v != value || v < 0) return h->fail(CUW_ERR_ARG, "SM_SHARE must be a non-negative integer");
+      h->nsm = v == 0 ? h->nsm_dev : std::min(v, h->nsm_dev);
+      h->drop_graphs();
       return CUW_OK;
     }
     case CUW_OPT_CONTRACTION_TILES:

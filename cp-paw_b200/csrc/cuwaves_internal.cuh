@@ -172,7 +172,9 @@ struct Handle {
   std::vector<double> occ_h;
   double waveekin1 = 0.0, waveekin2 = 0.0;
   cudaStream_t stream = nullptr;
-  int device = 0, nsm = 148;
+  // nsm: SMs the launch shapes assume (the device's nsm_dev, or the share of a
+  // set that runs beside others, CUW_OPT_SM_SHARE)
+  int device = 0, nsm = 148, nsm_dev = 148;
   // CUDA graphs of cuwaves_cp_step.  A step's launches depend on host-side
   // state only through the PSI0/PSIM swap, the buffer EIGR was built from,
   // the Lagrange history flag and the arguments; one graph is kept per such

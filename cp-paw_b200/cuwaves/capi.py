@@ -28,6 +28,7 @@ CUW_OPT_STREAM_PRIORITY = 6
 CUW_OPT_SAFEORTHO = 7
 CUW_OPT_SWAPSTATES = 8
 CUW_OPT_CONTRACTION_TILES = 9
+CUW_OPT_SM_SHARE = 10
 
 ERRORS = {1: "CUW_ERR_ARG", 2: "CUW_ERR_CUDA", 3: "CUW_ERR_STATE", 4: "CUW_ERR_NOT_CONVERGED",
           5: "CUW_ERR_DIVERGED", 6: "CUW_ERR_UNSUPPORTED", 7: "CUW_ERR_NAN", 8: "CUW_ERR_NOMEM"}

@@ -401,6 +401,14 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * accurate; wins when few bands leave the wide tiles mostly empty).  The
  * autotuner picks it by timing. */
 #define CUW_OPT_CONTRACTION_TILES 9
+/* CUW_OPT_SM_SHARE: the number of SMs that this set's launch shapes assume
+ * (the split-K factors of the contractions, the persistent force kernel, the
+ * grid-stride loops); 0 (default) = every SM of the device.  A set stepped in
+ * a batch of k sets can take about (SM count)/k, so that the sets' kernels
+ * share the device instead of each launching enough blocks to fill it.  Other
+ * split-K factors change summation orders at rounding level; the autotuner
+ * keeps its choices per share. */
+#define CUW_OPT_SM_SHARE 10
 int cuwaves_set_option(cuw_handle* h, int option, double value);
 /* Step graphs held now and graph replays so far (CUW_OPT_GRAPHS). */
 int cuwaves_get_graph_stats(cuw_handle* h, long long* graphs, long long* replays);

@@ -18,12 +18,14 @@ MIX = [
 ]
 
 
-def pairs(precision):
+def pairs(precision, share=0):
     out = []
     for make in MIX:
         inp = systems.build_inputs(make())
         a = cuwaves.open_waves(inp, precision=precision).setup().initialize()
         b = cuwaves.open_waves(inp, precision=precision).setup()
+        for w in (a, b):
+            w.set_option(cuwaves.CUW_OPT_SM_SHARE, share)
         for which in (CUW_PSI0, CUW_PSIM):
             b.upload_psi(which, a.download_psi(which))
         b.set_proj(a.get_proj())
@@ -34,9 +36,12 @@ def pairs(precision):
     return out
 
 
-@pytest.mark.parametrize("precision", [CUW_PREC_FP64, CUW_PREC_MIXED])
-def test_batch_equals_sets_alone(precision):
-    ps = pairs(precision)
+@pytest.mark.parametrize("precision,share", [(CUW_PREC_FP64, 0), (CUW_PREC_MIXED, 0), (CUW_PREC_FP64, 4),
+                                             (CUW_PREC_MIXED, 4)])
+def test_batch_equals_sets_alone(precision, share):
+    """share: CUW_OPT_SM_SHARE of every set (0: the whole device), the same for
+    the set in the batch and its twin stepped alone."""
+    ps = pairs(precision, share)
     batch = cuwaves.Batch([a for _, a, _ in ps])
     for rep in range(3):  # the first call captures, the others replay
         out = batch.step(move_atoms=True)
@@ -65,3 +70,26 @@ def test_batch_refuses_fresh_set():
         batch.step()
     assert e.value.code == 3
     batch.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(CUW_PREC_FP64, 1e-11), (CUW_PREC_MIXED, 1e-6)])
+def test_sm_share_changes_rounding_only(precision, tol):
+    """A set whose launch shapes assume 4 SMs (CUW_OPT_SM_SHARE) takes other
+    split-K factors and persistent grids than one that assumes the whole
+    device: the same CP steps to rounding level (relative to the energy)."""
+    inp = systems.build_inputs(MIX[0]())
+    a = cuwaves.open_waves(inp, precision=precision).setup().initialize()
+    b = cuwaves.open_waves(inp, precision=precision).setup()
+    for which in (CUW_PSI0, CUW_PSIM):
+        b.upload_psi(which, a.download_psi(which))
+    b.set_proj(a.get_proj())
+    b.set_option(cuwaves.CUW_OPT_SM_SHARE, 4)
+    for _ in range(3):
+        (oa, fa), (ob, fb) = a.cp_step(move_atoms=True), b.cp_step(move_atoms=True)
+        assert oa[4] == ob[4]
+        assert abs(oa[0] - ob[0]) <= tol * abs(oa[0])
+        assert np.abs(fa - fb).max() < 1e-6
+    with pytest.raises(cuwaves.WavesError):
+        b.set_option(cuwaves.CUW_OPT_SM_SHARE, -1)
+    a.close()
+    b.close()
