@@ -1361,9 +1361,9 @@ __global__ void k_switch_lambda(double2* __restrict__ rlam0, double2* __restrict
 // WAVES_ORTHO_Y_C (src/paw_waves2.f90:1025-1338) for real (Gamma-point)
 // PHIPHI, CHIPHI, CHICHI and the state order MAP (identity when map is null),
 // as one cluster of kOyCS CTAs (one CTA for NB <= kOySmall, where a cluster
-// barrier costs more than a step's updates).  WAVES_GRAMSCHMIDT (:2025-2177) passes one
-// matrix S as all three; WAVES$ORTHOGONALIZE with SAFEORTHO = F (:361-386)
-// passes MAT, OMAT and OOMAT.  A, B, C, ALPHA and X are n x n in global
+// barrier costs more than a step's updates).  WAVES_GRAMSCHMIDT (:2025-2177)
+// passes one matrix S as all three; WAVES$ORTHOGONALIZE with SAFEORTHO = F
+// (:361-386) passes MAT, OMAT and OOMAT.  A, B, C, ALPHA and X are n x n in global
 // memory (L2).  pos[i] is the place of state i in MAP: "J > N in the order"
 // of the reference is pos[j] > nu.  Step nu (pivot N = MAP(nu)) of the
 // sequential orthogonalisation has three parts, each ended by a cluster
