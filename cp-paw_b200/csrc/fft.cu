@@ -238,7 +238,10 @@ struct AxisArg {
 // LIB_FFTW3 leaves the same choice to FFTW's measured planning):
 //   bit 0: 16 instead of 8 complex values per thread and stage (more lines
 //          per pass, fewer barrier-separated passes, more registers);
-//   bit 1: the radix stages in ascending instead of descending order.
+//   bit 1: the radix stages in ascending instead of descending order;
+//   bit 2: on 64^3 grids, the z transforms exchange values between the lanes
+//          of a column by warp shuffles instead of shared memory (k_zcol_v64).
+// Variants 0, 1 and 2 are V = 0, 1, 2; variant 3 is V = 4 (64^3 grids only).
 // ---------------------------------------------------------------------------
 struct RadixList {
   int n;
@@ -273,7 +276,7 @@ __host__ __device__ constexpr int chunk_lines(int N, int V = 0) {
   }
   return lc;
 }
-constexpr int kFftVariants = 3;
+constexpr int kFftVariants = 4;
 
 // Line l of a transform lives at row (row0 + l) mod nrows of the buffer
 // (row0 = 0 and nrows above every line index: the identity).
@@ -555,23 +558,66 @@ constexpr int kZ64Smem = 64 * kZ64Ld + 2 * 64;  // elements: tile and two twiddl
 template <class C>
 constexpr int z64_smem_bytes() { return kZ64Smem * (int)sizeof(C) + 64 * kZ64Ld * (int)sizeof(typename CT<C>::R); }
 
-// on entry a[r] = x[t + 8r]; on exit a[k] = X[t + 8k], X[k] = sum_n x[n] tw[nk mod 64]
-// with tw[k] = exp(sgn 2 pi i k/64); col[q * kZ64Ld] are the column's slots
+// b[j] = a[(j + sh) & 7] (sh = +-t) for a run-time shift, by three stages of
+// selects: the register indices stay compile-time constants
 template <class C>
+__device__ __forceinline__ void rot8(C (&a)[8], int sh) {
+#pragma unroll
+  for (int bit = 1; bit < 8; bit <<= 1) {
+    const bool on = (sh & bit) != 0;
+    C b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = on ? a[(j + bit) & 7] : a[j];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = b[j];
+  }
+}
+__device__ __forceinline__ float2 shfl_c(float2 v, int src) {
+  return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+__device__ __forceinline__ double2 shfl_c(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// on entry a[r] = x[t + 8r]; on exit a[k] = X[t + 8k], X[k] = sum_n x[n] tw[nk mod 64]
+// with tw[k] = exp(sgn 2 pi i k/64).  Between the two radix-8 DFTs the 8 x 8
+// transpose among the column's lanes (lane t then holds element t of every
+// lane): through the column's shared-memory slots col[q * kZ64Ld], or (SHFL)
+// by warp shuffles among the 8 lanes, which are `lane0 + 4 t` of the warp:
+// round r sends element (t - r) mod 8 to lane (t - r) mod 8 and receives
+// element t of lane (t + r) mod 8; the array is rotated by t before and after
+// so that every round uses a fixed register.
+template <class C, bool SHFL>
 __device__ __forceinline__ void z64(C (&a)[8], C* col, int t, const C* tw, typename CT<C>::R sgn) {
   Bfly<8>::run(a, sgn, tw, 64);
 #pragma unroll
   for (int k1 = 1; k1 < 8; ++k1) a[k1] = cmul(a[k1], tw[t * k1]);
-  __syncwarp();  // the lanes' earlier reads of the slots are done
+  if constexpr (SHFL) {
+    const int lane = threadIdx.x & 31, l0 = lane & 3;
+    rot8(a, t);  // a[j] = old a[(j + t) mod 8]
+    C b[8];
 #pragma unroll
-  for (int k1 = 0; k1 < 8; ++k1) col[(k1 * 8 + ((t + k1) & 7)) * kZ64Ld] = a[k1];
-  __syncwarp();
+    for (int r = 0; r < 8; ++r) {
+      // send old a[(t - r) mod 8] = rotated a[(-r) mod 8]
+      const C v = a[(8 - r) & 7];
+      b[r] = shfl_c(v, l0 + 4 * ((t + r) & 7));  // element t of lane (t + r) mod 8
+    }
+    // b[r] holds element t of lane (t + r) mod 8: a[n1] = b[(n1 - t) mod 8]
 #pragma unroll
-  for (int n1 = 0; n1 < 8; ++n1) a[n1] = col[(t * 8 + ((n1 + t) & 7)) * kZ64Ld];
+    for (int j = 0; j < 8; ++j) a[j] = b[j];
+    rot8(a, 8 - t);
+  } else {
+    __syncwarp();  // the lanes' earlier reads of the slots are done
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) col[(k1 * 8 + ((t + k1) & 7)) * kZ64Ld] = a[k1];
+    __syncwarp();
+#pragma unroll
+    for (int n1 = 0; n1 < 8; ++n1) a[n1] = col[(t * 8 + ((n1 + t) & 7)) * kZ64Ld];
+  }
   Bfly<8>::run(a, sgn, tw, 64);
 }
 
-template <class C>
+template <class C, bool SHFL>
 __global__ void __launch_bounds__(kPlaneThreads, 2)
     k_zcol_v64(C* __restrict__ grid, const double* __restrict__ v, const int* __restrict__ zslot, int nzp, int nr2,
                const double2* __restrict__ tw3g, double scale) {
@@ -601,10 +647,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
     C a[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) a[r] = col[(t + 8 * r) * kZ64Ld];
-    z64(a, col, t, twp, (T)1);
+    z64<C, SHFL>(a, col, t, twp, (T)1);
 #pragma unroll
     for (int k = 0; k < 8; ++k) a[k] = cscale(a[k], vrow[(t + 8 * k) * kZ64Ld + x]);
-    z64(a, col, t, twm, (T)-1);
+    z64<C, SHFL>(a, col, t, twm, (T)-1);
     __syncwarp();  // the transpose reads are done before the slots take the result
 #pragma unroll
     for (int k = 0; k < 8; ++k) col[(t + 8 * k) * kZ64Ld] = a[k];
@@ -808,7 +854,7 @@ static int fft_vpsi_t(Handle* h, const double2* psi, double2* out, bool add_kine
                                                                            a1, a2, g.tw1, g.tw2);
     CUW_LAUNCH_CHECK("k_gtor_plane");
     if constexpr (N1 == 64 && N3 == 64) {
-      k_zcol_v64<C><<<dim3(nr2, nb), tz, z64_smem_bytes<C>(), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
+      k_zcol_v64<C, (V & 4) != 0><<<dim3(nr2, nb), tz, z64_smem_bytes<C>(), h->stream>>>(grid, g.v, g.zslot, h->nzp, nr2,
                                                                                  g.tw3, scale);
       CUW_LAUNCH_CHECK("k_zcol_v64");
     } else {
@@ -859,7 +905,8 @@ static int fft_select_v(Handle* h, int smem_plane) {
   const int smem_z = (int)(((size_t)h->d.nr3 * TX + h->d.nr3) * sizeof(C));
   CUW_TRY(smem_allow((const void*)k_gtor_plane<C, N1, N2, V>, smem_plane));
   CUW_TRY(smem_allow((const void*)k_rtog_plane<C, N1, N2, V>, smem_plane));
-  if constexpr (N1 == 64 && N3 == 64) CUW_TRY(smem_allow((const void*)k_zcol_v64<C>, z64_smem_bytes<C>()));
+  if constexpr (N1 == 64 && N3 == 64)
+    CUW_TRY(smem_allow((const void*)k_zcol_v64<C, (V & 4) != 0>, z64_smem_bytes<C>()));
   else CUW_TRY(smem_allow((const void*)k_zcol_v<C, N3, TX>, smem_z));
   CUW_TRY(smem_allow((const void*)k_zcol_rho<C, N3>, (int)(((size_t)h->d.nr3 * kRhoTX + h->d.nr3) * sizeof(C))));
   h->fft_run = &fft_vpsi_t<C, N1, N2, N3, V>;
@@ -874,6 +921,9 @@ static int fft_select(Handle* h, int smem_plane) {
     switch (h->fft_variant) {
       case 1: return fft_select_v<C, N1, N2, N3, 1>(h, smem_plane);
       case 2: return fft_select_v<C, N1, N2, N3, 2>(h, smem_plane);
+      case 3:
+        if constexpr (N1 == 64 && N3 == 64) return fft_select_v<C, N1, N2, N3, 4>(h, smem_plane);
+        break;
       default: break;
     }
   }
@@ -1031,13 +1081,15 @@ int fft_density(Handle* h, const double2* psi, double* rho) {
 
 // plan variant v (0 .. fft_variants()-1) of the compiled kernels; grids with
 // run-time lengths have variant 0 only
+// the shuffle variant (3) changes only the 64-point z kernel
+static bool z64_grid(const Handle* h) { return h->d.nr1 == 64 && h->d.nr2 == 64 && h->d.nr3 == 64; }
+int fft_variants(const Handle* h) { return !h->fft_compiled ? 1 : (z64_grid(h) ? kFftVariants : kFftVariants - 1); }
 int fft_set_variant(Handle* h, int v) {
   if (!h->fft_run) return h->fail(CUW_ERR_STATE, "FFT not set up");
-  if (v < 0 || v >= kFftVariants || (v != 0 && !h->fft_compiled)) return CUW_ERR_UNSUPPORTED;
+  if (v < 0 || v >= fft_variants(h)) return CUW_ERR_UNSUPPORTED;
   h->fft_variant = v;
   h->touch();
   return fft_choose(h);
 }
-int fft_variants(const Handle* h) { return h->fft_compiled ? kFftVariants : 1; }
 
 }  // namespace cuw

@@ -374,10 +374,11 @@ int cuwaves_get_ortho_stats(cuw_handle* h, double* out, int n);
  * EHARTREE + EXC, and out[5..7] = EHARTREE, EXC, int V rho.  Needs
  * cuwaves_set_rhoset and cuwaves_set_qlm first; 0 (default) keeps V fixed. */
 #define CUW_OPT_SELFCONSISTENT 4
-/* CUW_OPT_FFT_VARIANT: plan variant of the FFT plane transforms, 0 (default),
- * 1 (16 values per thread and stage) or 2 (radix stages in ascending order);
- * grids without compiled kernels accept 0 only (CUW_ERR_UNSUPPORTED).  The
- * autotuner picks it by timing. */
+/* CUW_OPT_FFT_VARIANT: plan variant of the FFT transforms, 0 (default),
+ * 1 (16 values per thread and stage), 2 (radix stages in ascending order) or,
+ * on 64^3 grids, 3 (the z transforms exchange values between lanes by warp
+ * shuffles instead of shared memory); grids without compiled kernels accept 0
+ * only (CUW_ERR_UNSUPPORTED).  The autotuner picks it by timing. */
 #define CUW_OPT_FFT_VARIANT 5
 /* CUW_OPT_STREAM_PRIORITY: 0 (default) or 1: the handle's work runs on a
  * stream of the device's lowest or highest scheduling priority (the stream is

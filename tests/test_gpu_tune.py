@@ -102,3 +102,40 @@ def test_contraction_tile_families(inputs):
     assert t["dmma_tiles"] == float(t["dmma_tiles_ms"] < t["tc_tiles_ms"])
     w.close()
     ref.close()
+
+
+@pytest.mark.parametrize("prec", [CUW_PREC_FP64, CUW_PREC_MIXED])
+def test_fft_shuffle_variant(prec, oracle):
+    """Plan variant 3 (64^3 grids): the 8 x 8 exchange of the 64-point z
+    transforms by warp shuffles among a column's lanes instead of shared
+    memory gives H|psi> of the oracle (FP64: 1e-10 relative; FP32 transforms:
+    1e-5), the same as variant 0 to rounding; a grid of another size refuses
+    it."""
+    inp = systems.build_inputs(systems.si_cell(1, grid=(64, 64, 64), epw_psi_ry=30.0, name="Si8-64"))
+    w = cuwaves.open_waves(inp, precision=prec).setup().initialize()
+    cpu = oracle.open_oracle(inp).setup()
+    for which in (cuwaves.CUW_PSI0, cuwaves.CUW_PSIM):
+        cpu.upload_psi(which, w.download_psi(which))
+    cpu.set_proj(w.get_proj())
+    cpu.hpsi()
+    ref = cpu.download_psi(cuwaves.CUW_HPSI)
+    tol = 1e-10 if prec == CUW_PREC_FP64 else 1e-5
+    got = {}
+    for v in (0, 3):
+        w.set_option(cuwaves.CUW_OPT_FFT_VARIANT, v)
+        w.hpsi()
+        got[v] = w.download_psi(cuwaves.CUW_HPSI)
+        err = float(np.abs(got[v] - ref).max() / np.abs(ref).max())
+        assert err < tol, f"variant {v}: {err:.2e}"
+    assert float(np.abs(got[3] - got[0]).max() / np.abs(ref).max()) < tol
+    w.close()
+    cpu.close()
+    small = cuwaves.open_waves(inputs_h2o2(), precision=prec).setup()
+    with pytest.raises(cuwaves.WavesError) as e:
+        small.set_option(cuwaves.CUW_OPT_FFT_VARIANT, 3)
+    assert e.value.code == 6
+    small.close()
+
+
+def inputs_h2o2():
+    return systems.build_inputs(systems.water_box(2, box=10.0, lattice=(2, 1, 1), epw_psi_ry=25.0, grid=(32, 32, 32)))
