@@ -40,11 +40,16 @@ constexpr int kRawGram = 16384;   // X, X(-k): 64 rows of 8 k (128B swizzle), or
 constexpr int kRawAddx = 32768;   // X, second-half X: 8 k x 128 m (2 KB rows) or 128 m x 8 k (128B swizzle)
 constexpr int kRawForce = 16384;  // psi0 8 b x 128 g (2 KB rows)
 constexpr int kRawGemm = 36864;   // A, B 128 rows x 16 doubles (144-byte rows, element copies)
-using ProjPipe = tc::Pipe<kNSplit, 8, kRawProj>;
-using AddproPipe = tc::Pipe<kNSplit, 8, kRawAddpro>;
-using GramPipe = tc::Pipe<kNSplit, 6, kRawGram>;
-using AddxPipe = tc::Pipe<6, 4, kRawAddx>;
-using ForcePipe = tc::Pipe<kNSplit, 6, kRawForce>;
+// Chunks travel in pairs through the copy and conversion hand-overs (the last
+// template argument): each hand-over costs several hundred cycles whatever it
+// carries, and pairs took 10-20 % off these kernels on B200 (Si64 and Si128
+// projections, back-projection, Gram; more raw slots than listed here gained
+// nothing).  Stage and slot counts below count pairs.
+using ProjPipe = tc::Pipe<4, 4, kRawProj, true, 2, 2, 2>;
+using AddproPipe = tc::Pipe<4, 4, kRawAddpro, true, 2, 2, 2>;
+using GramPipe = tc::Pipe<4, 2, kRawGram, true, 2, 2, 2>;
+using AddxPipe = tc::Pipe<3, 2, kRawAddx, true, 2, 2, 2>;
+using ForcePipe = tc::Pipe<4, 2, kRawForce, true, 2, 2, 2>;
 using GemmPipe = tc::Pipe<kNSplit, 2, kRawGemm, false>;
 constexpr int kThreads = ProjPipe::kThreads;
 constexpr int kNC = ProjPipe::kCols / 2;  // complex output columns per drain thread
@@ -56,7 +61,7 @@ static_assert(ProjPipe::kSmem <= 232448 && GramPipe::kSmem <= 232448 && AddxPipe
 // padded to an odd number of doubles so that the column stores of a warp (one
 // row per lane) spread over the banks
 constexpr int kSvLd = 65;
-static_assert(ForcePipe::kSplitBytes + 6 * kRawForce >= sizeof(double) * (128 * kSvLd + 4 * 128 + 4 * 192),
+static_assert(ForcePipe::kSplitBytes + ForcePipe::kNRaw * ForcePipe::kG * kRawForce >= sizeof(double) * (128 * kSvLd + 4 * 128 + 4 * 192),
               "stage area too small");
 
 // offset of 16-byte chunk e of row r in a box with 128-byte (64-byte) rows

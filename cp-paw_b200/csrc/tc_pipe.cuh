@@ -27,17 +27,20 @@
 // shared-memory bandwidth bounds a tf32 product of this shape.
 //
 // TMEM columns: [0, 128 NREG) accumulator regions, [128 NREG + 32 s, +32) A of
-// stage s (hi: 16 columns, lo: 16 columns).  Two regions and eight stages keep
+// stage place s (hi: 16 columns, lo: 16 columns).  Chunks move in units of G
+// through the copies and the conversion (one raw slot and one stage hold G
+// chunks, one hand-over per unit).  Two regions and eight stage places keep
 // four regions' worth of chunks in flight: the hand-overs between converters,
-// MMA thread and drain each take several hundred cycles.  The copies run up to NRAW chunks ahead of
-// the conversion; converted operands sit in NSPLIT stages, so copies,
-// conversion, MMAs and drains of different chunks overlap.  Every hand-over is
-// an mbarrier: rawfull[slot] (copies landed), rawempty[slot] (converters done
-// with the raw slot), sfull[s] (operands converted), sfree[s] (MMAs done with
-// stage s), bfull[r] (run r accumulated), bempty[r] (run r drained).  Every
-// wait is bounded; a wait that runs out raises the CTA's abort flag and *err,
-// every role then leaves its loop (its own waits run out too), copies in
-// flight are waited for, and TMEM is released on the common exit path.
+// MMA thread and drain each take several hundred cycles, whatever they carry.
+// The copies run up to NRAW units ahead of the conversion; converted operands
+// sit in NSPLIT stages, so copies, conversion, MMAs and drains of different
+// units overlap.  Every hand-over is an mbarrier: rawfull[slot] (copies
+// landed), rawempty[slot] (converters done with the raw slot), sfull[s]
+// (operands converted), sfree[s] (MMAs done with stage s), bfull[r] (run r
+// accumulated), bempty[r] (run r drained).  Every wait is bounded; a wait
+// that runs out raises the CTA's abort flag and *err, every role then leaves
+// its loop (its own waits run out too), copies in flight are waited for, and
+// TMEM is released on the common exit path.
 #pragma once
 
 #include "tc_sm100.cuh"
@@ -50,9 +53,11 @@ constexpr long long kWaitCycles = 1ll << 31;  // about one second at 2 GHz
 // 2^-23 relative to the binade of the accumulated value
 constexpr float kLossPerStep = 0.25f * 1.1920928955078125e-7f;
 
-template <int NSPLIT, int NRAW, int RAWB, bool BPRE = true, int CPR = 2, int NREG = 2>
+template <int NSPLIT, int NRAW, int RAWB, bool BPRE = true, int CPR = 2, int NREG = 2, int G = 1>
 struct Pipe {
-  static_assert(NRAW >= 2 && NSPLIT >= 2 * CPR, "stage counts");
+  // G chunks travel together through every hand-over but the drain's: one raw
+  // slot holds G chunks' raw data, one stage G chunks' converted operands.
+  static_assert(NRAW >= 2 && NSPLIT * G >= 2 * CPR && CPR % G == 0, "stage counts");
   // The two converter groups take alternate chunks.  With an even slot count
   // every raw slot belongs to one group, whose waits on it are never more than
   // one phase ahead of the barrier.  With an odd count a group can wait on
@@ -61,7 +66,7 @@ struct Pipe {
   // on phase k.  (Stages need no such rule: the MMAs that free them complete
   // in issue order.)
   static_assert(NRAW % 2 == 0, "raw slot count must be even");
-  static_assert(128 * NREG + 32 * NSPLIT <= 512, "TMEM: accumulator regions and A stages");
+  static_assert(128 * NREG + 32 * G * NSPLIT <= 512, "TMEM: accumulator regions and A stages");
   static_assert(RAWB % 1024 == 0, "raw slots keep the 1024-byte alignment of swizzled TMA boxes");
   static constexpr int kRows = 128;                 // A rows = TMEM lanes = B rows (N)
   static constexpr int kBK = 16;                    // real K values per chunk
@@ -82,8 +87,9 @@ struct Pipe {
   static constexpr int kRawBytes = RAWB;
   static constexpr int kNRaw = NRAW;
   static constexpr int kNSplit = NSPLIT;
-  static constexpr size_t kSplitBytes = sizeof(float) * NSPLIT * kStage;
-  static constexpr size_t kSmem = kSplitBytes + (size_t)NRAW * RAWB + 1024 + 512;
+  static constexpr int kG = G;                      // chunks per raw slot and per stage
+  static constexpr size_t kSplitBytes = sizeof(float) * NSPLIT * G * kStage;
+  static constexpr size_t kSmem = kSplitBytes + (size_t)NRAW * G * RAWB + 1024 + 512;
 };
 
 // Copies of one chunk issued by one lane of the copy warp into a raw slot:
@@ -156,7 +162,7 @@ __device__ __forceinline__ float untruncate(float y, float h) {
 }
 
 // load(c, lane, cp): lane `lane` of the copy warp issues its copies of chunk
-// c through `cp` (offsets within the raw slot, at most RAWB bytes).  Rows the
+// c through `cp` (offsets within the chunk's raw space, at most RAWB bytes).  Rows the
 // copies leave out hold stale data: a_row and convert_b mask them.
 // a_row(c, raw, row, kh, v): the eight real K values 8kh .. 8kh+7 of A row
 // `row` (0..127) of chunk c, from the raw slot.
@@ -173,9 +179,10 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
   constexpr int NRAW = P::kNRaw;
   constexpr int RAWB = P::kRawBytes;
   constexpr int CPR = P::kCPR;
+  constexpr int G = P::kG;
   float* st = pipe_stage_base();
   unsigned char* raw0 = reinterpret_cast<unsigned char*>(st) + P::kSplitBytes;
-  uint64_t* rawfull = reinterpret_cast<uint64_t*>(raw0 + (size_t)NRAW * RAWB);
+  uint64_t* rawfull = reinterpret_cast<uint64_t*>(raw0 + (size_t)NRAW * G * RAWB);
   constexpr int NR = P::kRegions;
   uint64_t* rawempty = rawfull + NRAW;
   uint64_t* sfull = rawempty + NRAW;
@@ -210,6 +217,7 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
   fence_after_sync();
   const uint32_t tmem = *tslot;
   const int nreg = (nchunk + CPR - 1) / CPR;  // accumulation regions
+  const int ngrp = (nchunk + G - 1) / G;      // hand-over units of G chunks
   auto raise = [&]() {
     *abort_flag = 1;
     atomicExch(err, 1);
@@ -229,8 +237,9 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
       int last = -1;  // last region issued
       for (int u = 0; u < nreg && !*abort_flag; ++u) {
         const int r = u % NR, c0 = u * CPR, nc = min(CPR, nchunk - c0);
+        const int q0 = c0 / G, nq = (nc + G - 1) / G;  // the region's hand-over units
         bool ok = u < NR || mbar_wait(&bempty[r], ((u / NR) - 1) & 1, kWaitCycles);
-        for (int i = 0; i < nc && ok; ++i) ok = mbar_wait(&sfull[(c0 + i) % NSPLIT], ((c0 + i) / NSPLIT) & 1, kWaitCycles);
+        for (int i = 0; i < nq && ok; ++i) ok = mbar_wait(&sfull[(q0 + i) % NSPLIT], ((q0 + i) / NSPLIT) & 1, kWaitCycles);
         if (!ok) {
           raise();
           break;
@@ -243,7 +252,8 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
 #pragma unroll
           for (int i = 0; i < CPR; ++i) {
             if (i >= nc) continue;
-            const int s = (c0 + i) % NSPLIT;
+            // stage of chunk c0 + i: sub-stage (c0 + i) % G of unit (c0 + i) / G
+            const int s = ((c0 + i) / G) % NSPLIT * G + (c0 + i) % G;
             const uint32_t bu = st0 + (uint32_t)s * kStageU;
             const uint32_t ta = tmem + (uint32_t)(P::kACol + 32 * s);
 #pragma unroll
@@ -259,7 +269,7 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
             }
           }
         mma_commit(&bfull[r]);
-        for (int i = 0; i < nc; ++i) mma_commit(&sfree[(c0 + i) % NSPLIT]);
+        for (int i = 0; i < nq; ++i) mma_commit(&sfree[(q0 + i) % NSPLIT]);
         last = u;
       }
       // let the MMAs in flight finish before TMEM is released
@@ -268,11 +278,11 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
   } else if (warp == 1) {
     // raw A (and unsplit B) data, up to NRAW chunks ahead of the converters
     int issued = 0;
-    for (int c = 0; c < nchunk; ++c) {
-      const int slot = c % NRAW;
+    for (int q = 0; q < ngrp; ++q) {
+      const int slot = q % NRAW;
       bool ok = true;
       if (lane == 0) {
-        if (c >= NRAW) ok = mbar_wait(&rawempty[slot], ((c / NRAW) - 1) & 1, kWaitCycles);
+        if (q >= NRAW) ok = mbar_wait(&rawempty[slot], ((q / NRAW) - 1) & 1, kWaitCycles);
         ok = ok && !*abort_flag;
       }
       ok = __shfl_sync(0xffffffffu, ok, 0);  // one decision for the whole warp
@@ -280,30 +290,39 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
         if (lane == 0) raise();
         break;
       }
-      Copier cp{raw0 + (size_t)slot * RAWB, &rawfull[slot], 0u};
-      load(c, lane, cp);
+      uint32_t bytes = 0;
+      bool async = false;
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int c = q * G + j;
+        if (c >= nchunk) break;
+        Copier cp{raw0 + (size_t)(slot * G + j) * RAWB, &rawfull[slot], 0u};
+        load(c, lane, cp);
+        bytes += cp.bytes;
+        async = async || cp.async;
+      }
       // (an arrival per lane with element copies: many arrivals on one
       // mbarrier serialise, so lanes without any skip it)
-      if (cp.async) cp_async_mbar_arrive(&rawfull[slot]);
+      if (async) cp_async_mbar_arrive(&rawfull[slot]);
       __syncwarp();
-      const uint32_t total = __reduce_add_sync(0xffffffffu, cp.bytes);
+      const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
       if (lane == 0) mbar_arrive_expect_tx(&rawfull[slot], total);
-      issued = c + 1;
+      issued = q + 1;
     }
     cp_async_wait_all();
     if (*abort_flag && lane == 0) {
-      // copies of chunks nobody consumed complete before the CTA ends
-      for (int c = max(0, issued - NRAW); c < issued; ++c) mbar_wait(&rawfull[c % NRAW], (c / NRAW) & 1, kWaitCycles);
+      // copies of units nobody consumed complete before the CTA ends
+      for (int q = max(0, issued - NRAW); q < issued; ++q) mbar_wait(&rawfull[q % NRAW], (q / NRAW) & 1, kWaitCycles);
     }
   } else if (warp == 2) {
     // split B tiles straight into their stages, once the MMAs are done with them
     if (P::kBPre) {
       int issued = 0;
-      for (int c = 0; c < nchunk; ++c) {
-        const int s = c % NSPLIT;
+      for (int q = 0; q < ngrp; ++q) {
+        const int s = q % NSPLIT;
         bool ok = true;
         if (lane == 0) {
-          if (c >= NSPLIT) ok = mbar_wait(&sfree[s], ((c / NSPLIT) - 1) & 1, kWaitCycles);
+          if (q >= NSPLIT) ok = mbar_wait(&sfree[s], ((q / NSPLIT) - 1) & 1, kWaitCycles);
           ok = ok && !*abort_flag;
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);  // one decision for the whole warp
@@ -311,51 +330,63 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
           if (lane == 0) raise();
           break;
         }
-        Copier cb{reinterpret_cast<unsigned char*>(st + s * P::kStage), &sfull[s], 0u};
-        load_b(c, lane, cb);
-        const uint32_t tb = __reduce_add_sync(0xffffffffu, cb.bytes);
+        uint32_t bytes = 0;
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const int c = q * G + j;
+          if (c >= nchunk) break;
+          Copier cb{reinterpret_cast<unsigned char*>(st + (s * G + j) * P::kStage), &sfull[s], 0u};
+          load_b(c, lane, cb);
+          bytes += cb.bytes;
+        }
+        const uint32_t tb = __reduce_add_sync(0xffffffffu, bytes);
         if (lane == 0) mbar_arrive_expect_tx(&sfull[s], tb);
-        issued = c + 1;
+        issued = q + 1;
       }
       if (*abort_flag && lane == 0)
-        for (int c = max(0, issued - NSPLIT); c < issued; ++c) mbar_wait(&sfull[c % NSPLIT], (c / NSPLIT) & 1, kWaitCycles);
+        for (int q = max(0, issued - NSPLIT); q < issued; ++q) mbar_wait(&sfull[q % NSPLIT], (q / NSPLIT) & 1, kWaitCycles);
     }
   } else if (warp < 3 + P::kConvWarps) {
-    // group grp converts chunks grp, grp + 2, ...; each thread owns one A row
+    // group grp converts units grp, grp + 2, ...; each thread owns one A row
     // (its TMEM lane) and converts both K halves (MMA steps) of it
     const int grp = (warp - 3) >> 2, gt = tid - 96 - grp * P::kGroup;
     const int arow = 32 * (warp & 3) + lane;
     const uint32_t tlane = (uint32_t)(32 * (warp & 3)) << 16;
-    for (int c = grp; c < nchunk; c += 2) {
-      const int s = c % NSPLIT, slot = c % NRAW;
-      bool ok = mbar_wait(&rawfull[slot], (c / NRAW) & 1, kWaitCycles);
-      if (ok && c >= NSPLIT) ok = mbar_wait(&sfree[s], ((c / NSPLIT) - 1) & 1, kWaitCycles);
+    for (int q = grp; q < ngrp; q += 2) {
+      const int s = q % NSPLIT, slot = q % NRAW;
+      bool ok = mbar_wait(&rawfull[slot], (q / NRAW) & 1, kWaitCycles);
+      if (ok && q >= NSPLIT) ok = mbar_wait(&sfree[s], ((q / NSPLIT) - 1) & 1, kWaitCycles);
       ok = __all_sync(0xffffffffu, ok && !*abort_flag);  // one decision for the whole warp
       if (!ok) {
         if (lane == 0) raise();
         break;
       }
       fence_after_sync();
-      const unsigned char* raw = raw0 + (size_t)slot * RAWB;
 #pragma unroll
-      for (int kh = 0; kh < 2; ++kh) {
-        float v[8];
-        a_row(c, raw, arow, kh, v);
-        uint32_t hi[8], lo[8];
+      for (int j = 0; j < G; ++j) {
+        const int c = q * G + j;
+        if (c >= nchunk) break;
+        const unsigned char* raw = raw0 + (size_t)(slot * G + j) * RAWB;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          float h, l;
-          split_tf32f(v[i], h, l);
-          hi[i] = __float_as_uint(h);
-          lo[i] = __float_as_uint(l);
+        for (int kh = 0; kh < 2; ++kh) {
+          float v[8];
+          a_row(c, raw, arow, kh, v);
+          uint32_t hi[8], lo[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            float h, l;
+            split_tf32f(v[i], h, l);
+            hi[i] = __float_as_uint(h);
+            lo[i] = __float_as_uint(l);
+          }
+          const uint32_t ta = tmem + tlane + (uint32_t)(P::kACol + 32 * (s * G + j) + 8 * kh);
+          tmem_st8(ta, hi);
+          tmem_st8(ta + 16, lo);
         }
-        const uint32_t ta = tmem + tlane + (uint32_t)(P::kACol + 32 * s + 8 * kh);
-        tmem_st8(ta, hi);
-        tmem_st8(ta + 16, lo);
-      }
-      if (!P::kBPre) {
-        float* bhi = st + s * P::kStage;
-        convert_b(c, raw, gt, bhi, bhi + P::kTile);
+        if (!P::kBPre) {
+          float* bhi = st + (s * G + j) * P::kStage;
+          convert_b(c, raw, gt, bhi, bhi + P::kTile);
+        }
       }
       tmem_wait_st();
       if (!P::kBPre) fence_async_smem();

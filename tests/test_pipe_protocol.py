@@ -60,8 +60,10 @@ def check(cond, what):
         raise Violation(what)
 
 
-def simulate(nsplit, nraw, bpre, cpr, nreg, nchunk, seed, conv_warps=2, drain_warps=2):
-    """One random interleaving; raises Violation on a protocol error."""
+def simulate(nsplit, nraw, bpre, cpr, nreg, nchunk, seed, conv_warps=2, drain_warps=2, g=1):
+    """One random interleaving; raises Violation on a protocol error.  g
+    chunks travel together as one unit through a raw slot and a stage (each
+    of g chunk places), with one hand-over per unit."""
     rng = random.Random(seed)
     rawfull = [Bar(1) for _ in range(nraw)]
     # the warps of one converter group (conv_warps of them) all arrive for the
@@ -71,55 +73,73 @@ def simulate(nsplit, nraw, bpre, cpr, nreg, nchunk, seed, conv_warps=2, drain_wa
     sfree = [Bar(1) for _ in range(nsplit)]
     bfull = [Bar(1) for _ in range(nreg)]
     bempty = [Bar(drain_warps) for _ in range(nreg)]
-    raw = [None] * nraw
-    sa = [None] * nsplit
-    sb = [None] * nsplit
+    raw = [None] * (nraw * g)
+    sa = [None] * (nsplit * g)
+    sb = [None] * (nsplit * g)
     region = [None] * nreg
     drained = [-1] * drain_warps
     copies = []  # landing events, any order
     mmas = []  # completion events, issue order
     nregions = (nchunk + cpr - 1) // cpr
+    nunits = (nchunk + g - 1) // g
+    assert cpr % g == 0
 
-    def land_raw(slot, c):
-        raw[slot] = c
-        rawfull[slot].complete_tx(1)
+    def chunks(q):
+        return range(q * g, min(nchunk, (q + 1) * g))
 
-    def land_b(s, c):
-        sb[s] = c
-        sfull[s].complete_tx(1)
+    def place(q, c, n):  # chunk c's place in the slot or stage of unit q (n of them)
+        return (q % n) * g + c - q * g
+
+    def land_raw(i, c):
+        raw[i] = c
+        rawfull[i // g].complete_tx(1)
+
+    def land_b(i, c):
+        sb[i] = c
+        sfull[i // g].complete_tx(1)
 
     def copy_a():
-        for c in range(nchunk):
-            slot = c % nraw
-            if c >= nraw:
-                yield rawempty[slot], ((c // nraw) - 1) & 1
-            copies.append((land_raw, slot, c))
+        for q in range(nunits):
+            slot = q % nraw
+            if q >= nraw:
+                yield rawempty[slot], ((q // nraw) - 1) & 1
+            for c in chunks(q):
+                copies.append((land_raw, place(q, c, nraw), c))
             yield None
-            rawfull[slot].arrive(expect_tx=1)
+            rawfull[slot].arrive(expect_tx=len(chunks(q)))
 
     def copy_b():
-        for c in range(nchunk):
-            s = c % nsplit
-            if c >= nsplit:
-                yield sfree[s], ((c // nsplit) - 1) & 1
-            copies.append((land_b, s, c))
+        for q in range(nunits):
+            s = q % nsplit
+            if q >= nsplit:
+                yield sfree[s], ((q // nsplit) - 1) & 1
+            for c in chunks(q):
+                copies.append((land_b, place(q, c, nsplit), c))
             yield None
-            sfull[s].arrive(expect_tx=1)
+            sfull[s].arrive(expect_tx=len(chunks(q)))
 
     def converter(grp):
-        for c in range(grp, nchunk, 2):
-            s, slot = c % nsplit, c % nraw
-            yield rawfull[slot], (c // nraw) & 1
-            if c >= nsplit:
-                yield sfree[s], ((c // nsplit) - 1) & 1
-            check(raw[slot] == c, f"converter of chunk {c} reads raw slot {slot} holding {raw[slot]}")
+        for q in range(grp, nunits, 2):
+            s, slot = q % nsplit, q % nraw
+            yield rawfull[slot], (q // nraw) & 1
+            if q >= nsplit:
+                yield sfree[s], ((q // nsplit) - 1) & 1
+            for c in chunks(q):
+                i = place(q, c, nraw)
+                check(raw[i] == c, f"converter of chunk {c} reads raw place {i} holding {raw[i]}")
             yield None
-            sa[s] = c
-            if not bpre:
-                sb[s] = c
-            check(raw[slot] == c, f"raw slot {slot} overwritten while chunk {c} converts")
+            for c in chunks(q):
+                sa[place(q, c, nsplit)] = c
+                if not bpre:
+                    sb[place(q, c, nsplit)] = c
+                i = place(q, c, nraw)
+                check(raw[i] == c, f"raw place {i} overwritten while chunk {c} converts")
             sfull[s].arrive()
             rawempty[slot].arrive()
+
+    def units(u):  # the units of region u
+        c0 = u * cpr
+        return range(c0 // g, (min(nchunk, c0 + cpr) + g - 1) // g)
 
     def mma():
         for u in range(nregions):
@@ -128,27 +148,24 @@ def simulate(nsplit, nraw, bpre, cpr, nreg, nchunk, seed, conv_warps=2, drain_wa
             if u >= nreg:
                 yield bempty[r], ((u // nreg) - 1) & 1
             check(all(d >= u - nreg for d in drained), f"region {u} issued before region {u - nreg} drained")
-            for i in range(nc):
-                c = c0 + i
-                yield sfull[c % nsplit], (c // nsplit) & 1
-            for i in range(nc):
-                c = c0 + i
-                s = c % nsplit
-                check(sa[s] == c and sb[s] == c, f"MMA of chunk {c} issued on stage {s} holding {sa[s]}/{sb[s]}")
+            for q in units(u):
+                yield sfull[q % nsplit], (q // nsplit) & 1
+            for c in range(c0, c0 + nc):
+                s = place(c // g, c, nsplit)
+                check(sa[s] == c and sb[s] == c, f"MMA of chunk {c} issued on stage place {s} holding {sa[s]}/{sb[s]}")
             mmas.append(u)
             yield None
 
     def mma_done(u):
         r, c0 = u % nreg, u * cpr
         nc = min(cpr, nchunk - c0)
-        for i in range(nc):
-            c = c0 + i
-            s = c % nsplit
-            check(sa[s] == c and sb[s] == c, f"stage {s} overwritten before the MMA of chunk {c} completed")
+        for c in range(c0, c0 + nc):
+            s = place(c // g, c, nsplit)
+            check(sa[s] == c and sb[s] == c, f"stage place {s} overwritten before the MMA of chunk {c} completed")
         region[r] = u
         bfull[r].arrive()
-        for i in range(nc):
-            sfree[(c0 + i) % nsplit].arrive()
+        for q in units(u):
+            sfree[q % nsplit].arrive()
 
     def drain(w):
         for u in range(nregions):
@@ -204,7 +221,8 @@ def pipe_configs():
         bpre = bool(vals[3]) if len(vals) > 3 else True
         cpr = vals[4] if len(vals) > 4 else 2
         nreg = vals[5] if len(vals) > 5 else 2
-        out[name] = (nsplit, nraw, bpre, cpr, nreg)
+        g = vals[6] if len(vals) > 6 else 1
+        out[name] = (nsplit, nraw, bpre, cpr, nreg, g)
     return out
 
 
@@ -218,23 +236,31 @@ def test_configs_found():
 
 @pytest.mark.parametrize("name", sorted(CONFIGS))
 def test_protocol_holds_under_random_interleavings(name):
-    nsplit, nraw, bpre, cpr, nreg = CONFIGS[name]
+    nsplit, nraw, bpre, cpr, nreg, g = CONFIGS[name]
     for nchunk in NCHUNKS:
         for seed in range(40):
-            simulate(nsplit, nraw, bpre, cpr, nreg, nchunk, seed)
+            simulate(nsplit, nraw, bpre, cpr, nreg, nchunk, seed, g=g)
+
+
+@pytest.mark.parametrize("nsplit,nraw,cpr,g", [(4, 4, 2, 2), (4, 2, 4, 2), (2, 4, 4, 4)])
+def test_protocol_holds_with_units_of_several_chunks(nsplit, nraw, cpr, g):
+    for nchunk in NCHUNKS:
+        for seed in range(20):
+            simulate(nsplit, nraw, True, cpr, 2, nchunk, seed, g=g)
 
 
 def test_model_finds_an_odd_raw_slot_count():
     """Planted mistake in the model: three raw slots shared by the two
     converter groups let a group pass a parity wait one phase early."""
-    found = False
-    for seed in range(400):
-        try:
-            simulate(8, 3, True, 2, 2, 40, seed)
-        except Violation:
-            found = True
-            break
-    assert found
+    for g in (1, 2):
+        found = False
+        for seed in range(400):
+            try:
+                simulate(8 // g, 3, True, 2, 2, 40, seed, g=g)
+            except Violation:
+                found = True
+                break
+        assert found, g
 
 
 def simulate_force(nchk, w0, w1, tn, nstage, seed, conv_warps=2, drain_warps=2, plant=None):
