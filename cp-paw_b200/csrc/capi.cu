@@ -621,6 +621,7 @@ extern "C" int cuwaves_destroy(cuw_handle* hp) {
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   h->drop_graphs();
   free_all(h);
+  if (h->res_h) cudaFreeHost(h->res_h);
   cudaStreamDestroy(h->stream);
   delete h;
   return CUW_OK;
@@ -677,6 +678,7 @@ extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* min
                                 const double* gvec, const double* g2, const double* pro, const double* ylm,
                                 const double* mpsi, const double* bucket, double gweight) {
   H(hp);
+  CUW_TRY(h->settle());
   h->touch();
   h->eigr_src = nullptr;
   NEED(igvec && minusg && gbas && gvec && g2 && pro && ylm && mpsi, CUW_ERR_ARG, "null argument");
@@ -722,7 +724,7 @@ extern "C" int cuwaves_set_gset(cuw_handle* hp, const int* igvec, const int* min
 extern "C" int cuwaves_set_potential(cuw_handle* hp, const double* v) {
   H(hp);
   NEED(v, CUW_ERR_ARG, "null potential");
-  CUW_TRY(cudaMemcpy(h->g.v, v, sizeof(double) * h->nr, cudaMemcpyHostToDevice));
+  CUW_TRY(h->h2d(h->g.v, v, sizeof(double) * h->nr));
   h->have_v = true;
   return CUW_OK;
 }
@@ -738,7 +740,7 @@ extern "C" int cuwaves_set_dh(cuw_handle* hp, int lmnxx, const double* dh) {
         size_t src = 2 * ((size_t)i + (size_t)lmnxx * (j + (size_t)lmnxx * a));
         t[i + (size_t)L * (j + (size_t)L * a)] = make_double2(dh[src], dh[src + 1]);
       }
-  CUW_TRY(cudaMemcpy(h->g.dh, t.data(), sizeof(double2) * t.size(), cudaMemcpyHostToDevice));
+  CUW_TRY(h->h2d(h->g.dh, t.data(), sizeof(double2) * t.size()));
   h->have_dh = true;
   return CUW_OK;
 }
@@ -752,7 +754,7 @@ extern "C" int cuwaves_set_do(cuw_handle* hp, int lnxx, const double* dover) {
   for (int s = 0; s < nsp; ++s)
     for (int j = 0; j < L; ++j)
       for (int i = 0; i < L; ++i) t[i + (size_t)L * (j + (size_t)L * s)] = dover[i + (size_t)lnxx * (j + (size_t)lnxx * s)];
-  CUW_TRY(cudaMemcpy(h->g.dover, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+  CUW_TRY(h->h2d(h->g.dover, t.data(), sizeof(double) * t.size()));
   h->have_do = true;
   return CUW_OK;
 }
@@ -761,8 +763,8 @@ extern "C" int cuwaves_set_atoms(cuw_handle* hp, const double* r0, const double*
   H(hp);
   const size_t n = sizeof(double) * 3 * h->d.nat;
   h->eigr_src = nullptr;
-  if (r0) CUW_TRY(cudaMemcpy(h->g.r0, r0, n, cudaMemcpyHostToDevice));
-  if (rp) CUW_TRY(cudaMemcpy(h->g.rp, rp, n, cudaMemcpyHostToDevice));
+  if (r0) CUW_TRY(h->h2d(h->g.r0, r0, n));
+  if (rp) CUW_TRY(h->h2d(h->g.rp, rp, n));
   return CUW_OK;
 }
 
@@ -772,9 +774,9 @@ extern "C" int cuwaves_reset_atoms(cuw_handle* hp, const double* r0) {
   NEED(r0, CUW_ERR_ARG, "null positions");
   const size_t n = sizeof(double) * 3 * h->d.nat;
   h->eigr_src = nullptr;
-  CUW_TRY(cudaMemcpy(h->g.r0, r0, n, cudaMemcpyHostToDevice));
-  CUW_TRY(cudaMemcpy(h->g.rp, r0, n, cudaMemcpyHostToDevice));
-  CUW_TRY(cudaMemcpy(h->g.rm, r0, n, cudaMemcpyHostToDevice));
+  CUW_TRY(h->h2d(h->g.r0, r0, n));
+  CUW_TRY(h->h2d(h->g.rp, r0, n));
+  CUW_TRY(h->h2d(h->g.rm, r0, n));
   return CUW_OK;
 }
 
@@ -793,7 +795,7 @@ extern "C" int cuwaves_set_occ(cuw_handle* hp, const double* occ) {
   h->touch();
   NEED(occ, CUW_ERR_ARG, "null occupations");
   h->occ_h.assign(occ, occ + h->d.nb);
-  CUW_TRY(cudaMemcpy(h->g.occ, occ, sizeof(double) * h->d.nb, cudaMemcpyHostToDevice));
+  CUW_TRY(h->h2d(h->g.occ, occ, sizeof(double) * h->d.nb));
   return CUW_OK;
 }
 
@@ -809,6 +811,7 @@ extern "C" int cuwaves_set_dynamics(cuw_handle* hp, double delt, double annee) {
 extern "C" int cuwaves_set_cell_friction(cuw_handle* hp, const double* fricmat, double emass, double emasscg2,
                                          const double* dbucket) {
   H(hp);
+  CUW_TRY(h->settle());
   h->touch();
   NEED(h->have_gset, CUW_ERR_STATE, "cuwaves_set_gset first");
   if (!fricmat) {
@@ -1305,13 +1308,17 @@ extern "C" int cuwaves_cp_step(cuw_handle* hp, int move_atoms, const double* mas
                        step_graph(h, move_atoms, max_iter, eps, &rc);
   if (!graphed) rc = step_body(h, move_atoms, max_iter, eps);
   if (rc != CUW_OK) return rc;
-  double hs[8];
-  int st[2];
-  CUW_TRY(cudaMemcpyAsync(hs, g.scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
-  CUW_TRY(cudaMemcpyAsync(st, g.ostatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
-  if (force) CUW_TRY(cudaMemcpyAsync(force, g.force, sizeof(double) * 3 * h->d.nat, cudaMemcpyDeviceToHost, h->stream));
+  // results through one page-locked block: three copies, one wait
+  const size_t nf = (size_t)3 * h->d.nat;
+  if (!h->res_h) CUW_TRY(cudaMallocHost(&h->res_h, sizeof(double) * (16 + std::max<size_t>(nf, 1))));
+  double* hs = h->res_h;
+  const int* st = reinterpret_cast<const int*>(h->res_h + 8);  // ostatus[0..15]
+  CUW_TRY(cudaMemcpyAsync(h->res_h, g.scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUW_TRY(cudaMemcpyAsync(h->res_h + 8, g.ostatus, sizeof(int) * 16, cudaMemcpyDeviceToHost, h->stream));
+  if (force && nf) CUW_TRY(cudaMemcpyAsync(h->res_h + 16, g.force, sizeof(double) * nf, cudaMemcpyDeviceToHost, h->stream));
   CUW_TRY(cudaStreamSynchronize(h->stream));
-  CUW_RET(h->tc_status());
+  if (force && nf) std::memcpy(force, h->res_h + 16, sizeof(double) * nf);
+  CUW_RET(h->tc_flag(st[12]));
   int iters = 0;
   CUW_RET(ortho_result(h, st, &iters));
   CUW_RET(collect_marks(h));

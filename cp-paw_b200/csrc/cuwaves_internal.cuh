@@ -156,6 +156,9 @@ struct Handle {
   bool have_hpsi = false, have_rlamm = false, have_opsi = false, have_u = false;
   bool tbucket = false;
   bool async = false;
+  // page-locked host block of cuwaves_cp_step's results (8 sums, the 16 status
+  // words, the forces): one copy each and one wait per step
+  double* res_h = nullptr;
   int nzp = 0;                   // occupied z planes
   int batch = 0;                 // bands per FFT batch
   int grid_bands = 0;            // bands the FFT work grid has room for
@@ -259,9 +262,24 @@ struct Handle {
     int f = 0;
     cudaError_t e = cudaMemcpy(&f, g.ostatus + 12, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(CUW_ERR_CUDA, std::string("status: ") + cudaGetErrorString(e));
-    if (f) return fail(CUW_ERR_CUDA, "tensor-core pipeline: a bounded wait ran out");
+    return tc_flag(f);
+  }
+  int tc_flag(int f) {
+    if (mixed() && f) return fail(CUW_ERR_CUDA, "tensor-core pipeline: a bounded wait ran out");
     return CUW_OK;
   }
+  // Copy of n bytes of caller input to the device, ordered on the handle's
+  // stream after the work enqueued before it.  Synchronous mode waits for it;
+  // asynchronous mode only enqueues (the runtime stages a pageable buffer
+  // before the call returns; a page-locked one is read when the stream gets
+  // there, so the caller keeps it unchanged until cuwaves_synchronize).
+  cudaError_t h2d(void* dst, const void* src, size_t n) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && !async) e = cudaStreamSynchronize(stream);
+    return e;
+  }
+  // set-up calls (new G set, new buffers) wait for the work in flight first
+  cudaError_t settle() { return async ? cudaStreamSynchronize(stream) : cudaSuccess; }
 };
 
 // ---------------------------------------------------------------------------

@@ -76,7 +76,11 @@ int cuwaves_destroy(cuw_handle* h);
 /* Copies the last error message (NUL-terminated, truncated to len); with
  * h == NULL, the message of the calling thread's last failed cuwaves_create. */
 int cuwaves_last_error(const cuw_handle* h, char* buf, int len);
-/* 0: every call waits for its work (default); 1: calls only enqueue. */
+/* 0: every call waits for its work (default); 1: calls only enqueue, input
+ * copies included (they run in stream order after the work enqueued before
+ * them; a page-locked input buffer is read when the stream gets there, so it
+ * stays unchanged until cuwaves_synchronize).  cuwaves_set_gset and
+ * cuwaves_set_cell_friction wait for the work in flight in either mode. */
 int cuwaves_set_async(cuw_handle* h, int async);
 int cuwaves_synchronize(cuw_handle* h);
 

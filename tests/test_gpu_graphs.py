@@ -77,3 +77,33 @@ def test_rediagonalisation_inside_graphs(inputs):
     assert sa["fixed_point_fallbacks"] >= 6 and sa == sb
     ga.close()
     gb.close()
+
+
+@pytest.mark.parametrize("prec", [CUW_PREC_FP64, CUW_PREC_MIXED])
+def test_async_input_copies_follow_enqueued_work(inputs, prec):
+    """In asynchronous mode a new potential is copied in stream order: H|psi>
+    calls enqueued before cuwaves_set_potential still see the old V(r), and
+    the next one sees the new V(r); in both cases bit for bit what synchronous
+    calls give."""
+    inp = inputs["Si8-20Ry"]
+    w = cuwaves.open_waves(inp, precision=prec).setup().initialize()
+    v1 = np.ascontiguousarray(inp["v"], dtype=np.float64)
+    v2 = v1 * 1.25 + 0.05
+    w.set_potential(v2)
+    w.projections()
+    w.hpsi()
+    want2 = w.expectation()
+    w.set_potential(v1)
+    w.hpsi()
+    want1 = w.expectation()
+    assert not np.array_equal(want1, want2)
+    w.set_async(True)
+    for _ in range(6):  # several milliseconds of queued work ahead of the copy
+        w.hpsi()
+    w.set_potential(v2)
+    w.set_async(False)
+    w.synchronize()
+    assert np.array_equal(w.expectation(), want1)
+    w.hpsi()
+    assert np.array_equal(w.expectation(), want2)
+    w.close()
