@@ -236,12 +236,17 @@ __global__ void k_atoms_verlet(const double* __restrict__ r0, const double* __re
   rp[i] = 2.0 * r0[i] - rm[i] + dt2 * f[i] / mass[i / 3];
 }
 
-__global__ void k_ion_ekin(const double* __restrict__ rp, const double* __restrict__ rm,
-                           const double* __restrict__ mass, int nat, double dt, double* __restrict__ out) {
+// Ionic kinetic energy from R(+) and R(-), then ATOMS$SWITCH by copies:
+// R(-) <- R(0), R(0) <- R(+) (one block; each thread rewrites only the
+// coordinates it has read)
+__global__ void k_ion_ekin_switch(const double* __restrict__ rp, double* __restrict__ rm, double* __restrict__ r0,
+                                  const double* __restrict__ mass, int nat, double dt, double* __restrict__ out) {
   extern __shared__ double term[];  // [3 nat]; summed by thread 0 in index order
   for (int i = threadIdx.x; i < 3 * nat; i += blockDim.x) {
     const double v = (rp[i] - rm[i]) / (2.0 * dt);
     term[i] = 0.5 * mass[i / 3] * v * v;
+    rm[i] = r0[i];
+    r0[i] = rp[i];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -249,6 +254,15 @@ __global__ void k_ion_ekin(const double* __restrict__ rp, const double* __restri
     for (int i = 0; i < 3 * nat; ++i) e += term[i];
     out[0] = e;
   }
+}
+
+// a set's step results into the batch's result slots: the 8 sums and the two
+// status words
+__global__ void k_batch_out(const double* __restrict__ scal, const int* __restrict__ status, double* __restrict__ res,
+                            int* __restrict__ st) {
+  const int t = threadIdx.x;
+  if (t < 8) res[t] = scal[t];
+  if (t < 2) st[t] = status[t];
 }
 
 __global__ void k_add_vec(double* __restrict__ a, const double* __restrict__ b, int n) {
@@ -1193,15 +1207,13 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   CUW_RET(energy_run(h, RED_WAVEKIN, tmpv, sc + 3));
   CUW_RET(mark(h, PH_MISC));
   if (move_atoms) {
-    k_ion_ekin<<<1, 128, sizeof(double) * 3 * h->d.nat, h->stream>>>(g.rp, g.rm, g.mass, h->d.nat, h->delt, sc + 4);
-    CUW_LAUNCH_CHECK("k_ion_ekin");
-    // ATOMS$SWITCH: R(-) <- R(0), R(0) <- R(+) by copies (the buffers keep
-    // their roles, so a step's launches see the same pointers every time);
-    // R(+) keeps R(0) until the next Verlet step, and EIGR of R(+) is now
-    // EIGR of R(0)
-    const size_t nb3 = sizeof(double) * 3 * h->d.nat;
-    CUW_TRY(cudaMemcpyAsync(g.rm, g.r0, nb3, cudaMemcpyDeviceToDevice, h->stream));
-    CUW_TRY(cudaMemcpyAsync(g.r0, g.rp, nb3, cudaMemcpyDeviceToDevice, h->stream));
+    // ATOMS$SWITCH in the same launch: R(-) <- R(0), R(0) <- R(+) by copies
+    // (the buffers keep their roles, so a step's launches see the same
+    // pointers every time); R(+) keeps R(0) until the next Verlet step, and
+    // EIGR of R(+) is now EIGR of R(0)
+    k_ion_ekin_switch<<<1, 128, sizeof(double) * 3 * h->d.nat, h->stream>>>(g.rp, g.rm, g.r0, g.mass, h->d.nat,
+                                                                             h->delt, sc + 4);
+    CUW_LAUNCH_CHECK("k_ion_ekin_switch");
     h->eigr_src = h->eigr_src == g.rp ? g.r0 : nullptr;
   } else {
     CUW_TRY(cudaMemsetAsync(sc + 4, 0, sizeof(double), h->stream));
@@ -1422,9 +1434,9 @@ static int batch_capture(cuw_batch* b, int move, int max_iter, double eps) {
         break;
       }
       const size_t slot = (size_t)i * 2 + s;
-      e = cudaMemcpyAsync(b->res + slot * 8, h->g.scal, sizeof(double) * 8, cudaMemcpyDeviceToDevice, h->stream);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b->st + slot * 2, h->g.ostatus, sizeof(int) * 2, cudaMemcpyDeviceToDevice, h->stream);
+      k_batch_out<<<1, 32, 0, h->stream>>>(h->g.scal, h->g.ostatus, b->res + slot * 8, b->st + slot * 2);
+      ++h->launches;
+      e = cudaGetLastError();
       if (e != cudaSuccess) rc = CUW_ERR_CUDA;
     }
   for (int i = 0; i < n; ++i) {

@@ -88,11 +88,15 @@ __global__ void k_lambda_init(const double2* __restrict__ rlam0, const double* _
 }
 
 // 0.5*(A + A^T)
-__global__ void k_symmetrize(const double* __restrict__ a, int n, double* __restrict__ s) {
+// s = sym(a); with lam non-null also lam0 = lam (the saved Lambda that a
+// rediagonalised ORTHO_X restarts from), in the same launch
+__global__ void k_symmetrize(const double* __restrict__ a, int n, double* __restrict__ s,
+                             const double* __restrict__ lam, double* __restrict__ lam0) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n * n) return;
   int i = idx % n, j = idx / n;
   s[idx] = 0.5 * (a[i + (size_t)n * j] + a[j + (size_t)n * i]);
+  if (lam) lam0[idx] = lam[idx];
 }
 
 // ---------------------------------------------------------------------------
@@ -1562,9 +1566,14 @@ __global__ void k_split_diag(const double* __restrict__ b, int n, double* __rest
   }
 }
 
-__global__ void k_copy_gated(const double* __restrict__ src, double* __restrict__ dst, int n, const int* gate) {
+// dst1 = src1 and dst2 = src2 (n elements each) unless the gate is closed
+__global__ void k_copy_gated(const double* __restrict__ src1, double* __restrict__ dst1,
+                             const double* __restrict__ src2, double* __restrict__ dst2, int n, const int* gate) {
   if (gate_closed(gate)) return;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) dst[k] = src[k];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    dst1[k] = src1[k];
+    dst2[k] = src2[k];
+  }
 }
 
 // One launch of the ORTHO_X iteration (k_ortho_x) with the eigenbasis in
@@ -1726,21 +1735,19 @@ int ortho_solve(Handle* h, int max_iter, double eps) {
   Device& g = h->g;
   const int nn = n * n;
   const dim3 tg(ceil_div(n, 32), ceil_div(n, 32));
-  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.smat);
+  // with an eigenbasis, Lambda is saved to lam0 in the same launch
+  k_symmetrize<<<ceil_div(n * n, 256), 256, 0, h->stream>>>(g.omat, n, g.smat, h->have_u ? g.lam : nullptr, g.lam0);
   CUW_LAUNCH_CHECK("k_symmetrize");
   if (h->have_u) {
     const int* gate = g.ostatus;  // status of the first launch
     const int cb = std::min(ceil_div(nn, 256), 2 * h->nsm);
     CUW_RET(rotate_to_basis(h, nullptr));
-    CUW_TRY(cudaMemcpyAsync(g.lam0, g.lam, sizeof(double) * nn, cudaMemcpyDeviceToDevice, h->stream));
     CUW_RET(ortho_x_launch(h, 1, max_iter, eps, nullptr));
     CUW_RET(rotate_to_basis(h, gate));  // g.work was overwritten by the iteration
     CUW_RET(jacobi_run(h, g.work, g.wk2, g.eig, gate));
     k_small_gemm<<<tg, 256, 0, h->stream>>>(g.u, 0, g.wk2, 0, n, g.u2, gate);
     CUW_LAUNCH_CHECK("k_small_gemm");
-    k_copy_gated<<<cb, 256, 0, h->stream>>>(g.u2, g.u, nn, gate);
-    CUW_LAUNCH_CHECK("k_copy_gated");
-    k_copy_gated<<<cb, 256, 0, h->stream>>>(g.lam0, g.lam, nn, gate);
+    k_copy_gated<<<cb, 256, 0, h->stream>>>(g.u2, g.u, g.lam0, g.lam, nn, gate);
     CUW_LAUNCH_CHECK("k_copy_gated");
     CUW_RET(ortho_x_launch(h, 0, max_iter, eps, gate));
   } else {
