@@ -624,7 +624,7 @@ __device__ __forceinline__ bool lyap_stop(double gdx, double gxm, double& prev, 
 template <int MR, int MC>
 __device__ double* lyap_fast(const OrthoArgs& a, int cs, int rank, int i0, int i1, int j0, int j1, double* sm,
                              double* red, double* xcur, double* xnext, bool& failed, double& rho_io) {
-  constexpr int RA = 16 * MR, RB = 16 * MC, LDA = RA + 4, LDB = RB + 4;
+  constexpr int RA = 16 * MR, RB = 16 * MC, LDA = RA + 4;
   constexpr int TR = RA / 8, TC = RB / 8, NTILE = TR * TC, TPW = (NTILE + 7) / 8;
   // the slices always hold KN = 128 rows of k (zero past n), so that every
   // divisor of the staging index arithmetic is a compile-time constant

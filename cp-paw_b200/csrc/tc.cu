@@ -1088,7 +1088,8 @@ int tc_addpro(Handle* h, int mode, const double2* hpc, const double2* opc, const
 
 int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int nm, size_t sk, size_t sm,
             double scale, double2* dst) {
-  TcGramArgs a;
+  if (npair < 1 || npair > 3) return h->fail(CUW_ERR_ARG, "Gram product: one to three pairs");
+  TcGramArgs a{};
   a.npair = npair;
   a.nk = nk;
   a.nm = nm;
@@ -1096,7 +1097,7 @@ int tc_gram(Handle* h, const GramPair* pairs, int npair, bool minus, int nk, int
   a.nchk = ceil_div(nk, kCK);
   if (!a.kfast && sm != 1) return h->fail(CUW_ERR_UNSUPPORTED, "Gram product with neither index contiguous");
   if (minus && !a.kfast) return h->fail(CUW_ERR_UNSUPPORTED, "X(-k) Gram product of projections");
-  TcGramMaps tm;
+  TcGramMaps tm{};
   // X(-k) copies of the distinct X arrays (at most two: PSIBAR and OPSI)
   const double2* src[2] = {nullptr, nullptr};
   const double2* mcopy[2] = {nullptr, nullptr};
