@@ -162,8 +162,8 @@ __device__ __forceinline__ float untruncate(float y, float h) {
 }
 
 // load(c, lane, cp): lane `lane` of the copy warp issues its copies of chunk
-// c through `cp` (offsets within the chunk's raw space, at most RAWB bytes).  Rows the
-// copies leave out hold stale data: a_row and convert_b mask them.
+// c through `cp` (offsets within the chunk's raw space, at most RAWB bytes).
+// Rows the copies leave out hold stale data: a_row and convert_b mask them.
 // a_row(c, raw, row, kh, v): the eight real K values 8kh .. 8kh+7 of A row
 // `row` (0..127) of chunk c, from the raw slot.
 // load_b(c, lane, cp) (P::kBPre): lane `lane` issues the bulk copy of chunk
@@ -276,7 +276,7 @@ __device__ __forceinline__ void pipe_run(int nchunk, Load& load, LoadB& load_b, 
       if (last >= 0) mbar_wait(&bfull[last % NR], (last / NR) & 1, kWaitCycles);
     }
   } else if (warp == 1) {
-    // raw A (and unsplit B) data, up to NRAW chunks ahead of the converters
+    // raw A (and unsplit B) data, up to NRAW units ahead of the converters
     int issued = 0;
     for (int q = 0; q < ngrp; ++q) {
       const int slot = q % NRAW;
