@@ -771,6 +771,22 @@ __global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi
     int p = n0 + row;
     return (b < nbh && p < npro) ? ded + (size_t)b + (size_t)nbh * p : nullptr;
   };
+  // with the projector table, its values for this tile's outputs are loaded
+  // before the products so that their latency overlaps the MMAs
+  double2 pvt[4][2][2];
+  if constexpr (TAB) {
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int m, n;
+          acc_mn(wm, wn, lane, mi, ni, e, m, n);
+          const int g = m0 + m, p = n0 + n;
+          pvt[mi][ni][e] = (g < ngl && p < npro) ? prox[(size_t)g + (size_t)ldg * p] : make_double2(0.0, 0.0);
+        }
+  }
   mainloop2<MP11, false, true, true, true>(reinterpret_cast<double2*>(sm), 0, nbh, pa, pa, pb, pb, NoConj(),
                                            NoConj(), acc, dummy);
   // epilogue: per (g, p) contribution, reduced over g
@@ -793,7 +809,7 @@ __global__ void __launch_bounds__(NT, 1) k_force(const double2* __restrict__ psi
           double sv;
           if constexpr (TAB) {
             // Re(i PRO(g,p) conj(dd))
-            const double2 pv = prox[(size_t)g + (size_t)ldg * p];
+            const double2 pv = pvt[mi][ni][e];
             sv = -pv.y * dd.x + pv.x * dd.y;
           } else {
             ProDesc d = pdesc[p];
@@ -897,13 +913,27 @@ __global__ void __launch_bounds__(NT, 1) k_force_p(const double2* __restrict__ p
     cpa_commit();
     cpa_wait<1>();  // this tile's psi rows (and the DEDPRO tile) have landed
     __syncthreads();
+    const int m0 = t * BM;
+    // the projector-table values of this tile's outputs, loaded before the
+    // products so that their latency overlaps the MMAs
+    double2 pvt[4][2][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int m, n;
+          acc_mn(wm, wn, lane, mi, ni, e, m, n);
+          const int g = m0 + m, p = n0 + n;
+          pvt[mi][ni][e] = (g < ngl && p < npro) ? prox[(size_t)g + (size_t)ldg * p] : make_double2(0.0, 0.0);
+        }
     Acc acc;
     acc.zero();
     for (int sl = 0; sl < nsl; ++sl)
       mma_slice2<false, true, true>(acc, asm_ + ((size_t)buf * kFpSlices + sl) * kFpASlice, bsm + sl * TILE2, wm,
                                     wn, lane, sl * BK, NoConj());
     acc.finish();
-    const int m0 = t * BM;
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -915,7 +945,7 @@ __global__ void __launch_bounds__(NT, 1) k_force_p(const double2* __restrict__ p
           const int g = m0 + m, p = n0 + n;
           if (g < ngl && p < npro) {
             // Re(i PRO(g,p) conj(dd))
-            const double2 pv = prox[(size_t)g + (size_t)ldg * p];
+            const double2 pv = pvt[mi][ni][e];
             const double sv = -pv.y * acc.r[mi][ni][e] + pv.x * acc.i[mi][ni][e];
             f[ni][e][0] += sv * gx[g];
             f[ni][e][1] += sv * gy[g];
