@@ -701,6 +701,21 @@ __global__ void __launch_bounds__(NT, 1) k_addx(AddXArgs a, const int* __restric
   };
   const int nk = a.nk;
   auto second = [nk](int kg) { return kg >= nk; };
+  // the outputs' old values (out is not an operand), loaded before the
+  // products so that their latency overlaps the MMAs
+  double2 old[4][2][2];
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int m, n;
+        acc_mn(wm, wn, lane, mi, ni, e, m, n);
+        m += m0;
+        n += n0;
+        old[mi][ni][e] = (m < a.nm && n < a.nn) ? a.out[(size_t)m * a.som + (size_t)n * a.son] : make_double2(0.0, 0.0);
+      }
   mainloop2<MP11, !MFAST, true, false, false>(reinterpret_cast<double2*>(sm), 0, ktot, pa, pa, pb, pb, second,
                                               second, acc, dummy);
 #pragma unroll
@@ -715,30 +730,50 @@ __global__ void __launch_bounds__(NT, 1) k_addx(AddXArgs a, const int* __restric
         n += n0;
         if (m < a.nm && n < a.nn) {
           size_t k = (size_t)m * a.som + (size_t)n * a.son;
-          double2 o = a.out[k];
+          const double2 o = old[mi][ni][e];
           a.out[k] = make_double2(o.x + acc.r[mi][ni][e], o.y + acc.i[mi][ni][e]);
         }
       }
 }
 
 // out(b,p) += sum_k x(k,p) l1(k,b) + conj(x(k,p)) l2(k,b) for (NBH, NPRO)
-// arrays with the band index fastest; thread t = b + NBH p
+// arrays with the band index fastest.  A block of 256 threads forms 64 bands
+// x 4 projectors, one output per thread with K in order; L1, L2 and x pass
+// through shared memory kAopK values of k at a time, copied along k (the
+// contiguous index), so that no warp reads L1 or L2 at a stride of NBH.
+constexpr int kAopK = 16;
 __global__ void k_addoproj(double2* __restrict__ out, const double2* __restrict__ x, const double2* __restrict__ l1,
                            const double2* __restrict__ l2, int npro, int nbh) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npro * nbh) return;
-  const int b = t % nbh, p = t / nbh;
-  const double2* xp = x + (size_t)p * nbh;
-  const double2* a = l1 + (size_t)nbh * b;
-  const double2* c = l2 + (size_t)nbh * b;
+  __shared__ double2 s1[64][kAopK + 1], s2[64][kAopK + 1], sx[4][kAopK];
+  const int tb = threadIdx.x & 63, tp = threadIdx.x >> 6;
+  const int b0 = blockIdx.y * 64, p0 = blockIdx.x * 4;
+  const int b = b0 + tb, p = p0 + tp;
   double sr = 0.0, si = 0.0;
-  for (int k = 0; k < nbh; ++k) {
-    const double2 xv = xp[k], av = a[k], cv = c[k];
-    sr += xv.x * av.x - xv.y * av.y + xv.x * cv.x + xv.y * cv.y;
-    si += xv.x * av.y + xv.y * av.x + xv.x * cv.y - xv.y * cv.x;
+  for (int k0 = 0; k0 < nbh; k0 += kAopK) {
+    __syncthreads();  // the previous chunk is consumed
+    for (int i = threadIdx.x; i < 64 * kAopK; i += blockDim.x) {
+      const int kk = i % kAopK, bb = i / kAopK, k = k0 + kk, bg = b0 + bb;
+      const bool ok = k < nbh && bg < nbh;
+      s1[bb][kk] = ok ? l1[(size_t)k + (size_t)nbh * bg] : make_double2(0.0, 0.0);
+      s2[bb][kk] = ok ? l2[(size_t)k + (size_t)nbh * bg] : make_double2(0.0, 0.0);
+    }
+    if (threadIdx.x < 4 * kAopK) {
+      const int pp = threadIdx.x / kAopK, kk = threadIdx.x % kAopK, k = k0 + kk, pg = p0 + pp;
+      sx[pp][kk] = (k < nbh && pg < npro) ? x[(size_t)pg * nbh + k] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int kn = min(kAopK, nbh - k0);
+    for (int kk = 0; kk < kn; ++kk) {
+      const double2 xv = sx[tp][kk], av = s1[tb][kk], cv = s2[tb][kk];
+      sr += xv.x * av.x - xv.y * av.y + xv.x * cv.x + xv.y * cv.y;
+      si += xv.x * av.y + xv.y * av.x + xv.x * cv.y - xv.y * cv.x;
+    }
   }
-  const double2 o = out[t];
-  out[t] = make_double2(o.x + sr, o.y + si);
+  if (b < nbh && p < npro) {
+    const size_t t = (size_t)b + (size_t)nbh * p;
+    const double2 o = out[t];
+    out[t] = make_double2(o.x + sr, o.y + si);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1353,7 +1388,8 @@ int addopsi_run(Handle* h, double2* psibar, const double2* opsi, const double2* 
 int addoproj_run(Handle* h, double2* proj, const double2* oproj, const double2* l1, const double2* l2) {
   const int n = h->npro * h->d.nbh;
   if (n == 0) return CUW_OK;
-  k_addoproj<<<ceil_div(n, 128), 128, 0, h->stream>>>(proj, oproj, l1, l2, h->npro, h->d.nbh);
+  k_addoproj<<<dim3(ceil_div(h->npro, 4), ceil_div(h->d.nbh, 64)), 256, 0, h->stream>>>(proj, oproj, l1, l2, h->npro,
+                                                                                        h->d.nbh);
   CUW_LAUNCH_CHECK("k_addoproj");
   return CUW_OK;
 }
