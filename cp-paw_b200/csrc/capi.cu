@@ -777,8 +777,9 @@ extern "C" int cuwaves_set_atoms(cuw_handle* hp, const double* r0, const double*
   H(hp);
   const size_t n = sizeof(double) * 3 * h->d.nat;
   h->eigr_src = nullptr;
-  if (r0) CUW_TRY(h->h2d(h->g.r0, r0, n));
-  if (rp) CUW_TRY(h->h2d(h->g.rp, rp, n));
+  if (r0) CUW_TRY(h->h2d(h->g.r0, r0, n, false));
+  if (rp) CUW_TRY(h->h2d(h->g.rp, rp, n, false));
+  CUW_TRY(h->h2d_done());
   return CUW_OK;
 }
 
@@ -788,9 +789,10 @@ extern "C" int cuwaves_reset_atoms(cuw_handle* hp, const double* r0) {
   NEED(r0, CUW_ERR_ARG, "null positions");
   const size_t n = sizeof(double) * 3 * h->d.nat;
   h->eigr_src = nullptr;
-  CUW_TRY(h->h2d(h->g.r0, r0, n));
-  CUW_TRY(h->h2d(h->g.rp, r0, n));
-  CUW_TRY(h->h2d(h->g.rm, r0, n));
+  CUW_TRY(h->h2d(h->g.r0, r0, n, false));
+  CUW_TRY(h->h2d(h->g.rp, r0, n, false));
+  CUW_TRY(h->h2d(h->g.rm, r0, n, false));
+  CUW_TRY(h->h2d_done());
   return CUW_OK;
 }
 

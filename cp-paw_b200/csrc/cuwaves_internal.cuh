@@ -273,11 +273,13 @@ struct Handle {
   // asynchronous mode only enqueues (the runtime stages a pageable buffer
   // before the call returns; a page-locked one is read when the stream gets
   // there, so the caller keeps it unchanged until cuwaves_synchronize).
-  cudaError_t h2d(void* dst, const void* src, size_t n) {
+  cudaError_t h2d(void* dst, const void* src, size_t n, bool wait = true) {
     cudaError_t e = cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess && !async) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && wait && !async) e = cudaStreamSynchronize(stream);
     return e;
   }
+  // the wait of synchronous mode after copies enqueued with h2d(..., false)
+  cudaError_t h2d_done() { return async ? cudaSuccess : cudaStreamSynchronize(stream); }
   // set-up calls (new G set, new buffers) wait for the work in flight first
   cudaError_t settle() { return async ? cudaStreamSynchronize(stream) : cudaSuccess; }
 };

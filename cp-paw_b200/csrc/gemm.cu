@@ -489,7 +489,18 @@ __global__ void k_reduce_parts(const double2* __restrict__ part, int nz, size_t 
                                double2* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     double2 s = make_double2(0.0, 0.0);
-    for (int z = 0; z < nz; ++z) {
+    int z = 0;
+    for (; z + 8 <= nz; z += 8) {  // eight loads in flight, added in split order
+      double2 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = part[(size_t)(z + j) * stride + i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        s.x += v[j].x;
+        s.y += v[j].y;
+      }
+    }
+    for (; z < nz; ++z) {
       double2 v = part[(size_t)z * stride + i];
       s.x += v.x;
       s.y += v.y;

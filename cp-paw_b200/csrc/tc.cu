@@ -151,7 +151,18 @@ __global__ void k_tc_reduce(const float2* __restrict__ part, int nz, size_t n, d
                             double2* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     double sx = 0.0, sy = 0.0;
-    for (int z = 0; z < nz; ++z) {
+    int z = 0;
+    for (; z + 8 <= nz; z += 8) {  // eight loads in flight, added in split order
+      float2 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = part[(size_t)(z + j) * n + i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        sx += (double)v[j].x;
+        sy += (double)v[j].y;
+      }
+    }
+    for (; z < nz; ++z) {
       const float2 v = part[(size_t)z * n + i];
       sx += (double)v.x;
       sy += (double)v.y;
