@@ -40,7 +40,7 @@ namespace {
 //   q0 + i q1 = sum conj(x) y, q2 + i q3 = sum x(g) y(-g)
 // ---------------------------------------------------------------------------
 constexpr int RB = 256;
-constexpr int RG = 2048;  // g per block
+constexpr int RG = 2048;  // G values per block at most when blocks are plentiful (sizes g.red)
 __device__ void energy_final_block(int mode, const double* __restrict__ part, int nblk, const double* __restrict__ occ,
                                    int nbh, double gweight, double dt2, int tbucket, double* __restrict__ out,
                                    double* __restrict__ scalar, double* sh);
@@ -57,12 +57,13 @@ struct BandFinal {
 
 __global__ void k_band_sums(int mode, const double2* __restrict__ x, const double2* __restrict__ y, int ldg, int ngl,
                             const double* __restrict__ w1, const double* __restrict__ w2,
-                            const int* __restrict__ minusg, double* __restrict__ part, int nblk, BandFinal fin) {
+                            const int* __restrict__ minusg, double* __restrict__ part, int nblk, int rg,
+                            BandFinal fin) {
   const int b = blockIdx.y, blk = blockIdx.x;
   const double2* xb = x + (size_t)ldg * b;
   const double2* yb = y ? y + (size_t)ldg * b : nullptr;
   double q[4] = {0.0, 0.0, 0.0, 0.0};
-  const int g0 = blk * RG, g1 = min(ngl, g0 + RG);
+  const int g0 = blk * rg, g1 = min(ngl, g0 + rg);
   for (int g = g0 + threadIdx.x; g < g1; g += RB) {
     int mg = minusg[g];
     if (mode == 0) {
@@ -285,14 +286,24 @@ __global__ void k_copy_psi(const double2* __restrict__ src, double2* __restrict_
 // null) the energy again
 static int band_sums_run(Handle* h, int mode, const double2* x, const double2* y, const double* w1, const double* w2,
                          double* out_dev, double* scalar) {
-  const int nblk = ceil_div(h->d.ngl, RG);
+  const int nmax = ceil_div(h->d.ngl, RG);  // partial slots per band in g.red
   const size_t sm = sizeof(double) * 5 * (size_t)h->d.nbh;
   if (sm > 48 * 1024) CUW_TRY(smem_allow((const void*)k_band_sums, (int)sm));
+  if (h->band_bps == 0) {
+    int bps = 0;
+    CUW_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_band_sums, RB, sm));
+    h->band_bps = std::max(1, bps);
+  }
+  // one wave of blocks on the SMs the set may use (a second, nearly empty
+  // wave would double the time): G ranges of a multiple of RB per block
+  int nblk = std::min(nmax, std::max(1, h->nsm * h->band_bps / h->d.nbh));
+  const int rg = ceil_div(ceil_div(h->d.ngl, nblk), RB) * RB;
+  nblk = ceil_div(h->d.ngl, rg);
   Device& g = h->g;
   BandFinal fin{g.occ, h->gweight, h->delt * h->delt, h->tbucket ? 1 : 0, out_dev, scalar,
-                reinterpret_cast<unsigned*>(g.red + 4 * (size_t)h->d.nbh * (nblk + 1))};
+                reinterpret_cast<unsigned*>(g.red + 4 * (size_t)h->d.nbh * (nmax + 1))};
   k_band_sums<<<dim3(nblk, h->d.nbh), RB, sm, h->stream>>>(mode, x, y, h->ldg, h->d.ngl, w1, w2, g.minusg, g.red,
-                                                           nblk, fin);
+                                                           nblk, rg, fin);
   CUW_LAUNCH_CHECK("k_band_sums");
   return CUW_OK;
 }

@@ -159,6 +159,7 @@ struct Handle {
   // page-locked host block of cuwaves_cp_step's results (8 sums, the 16 status
   // words, the forces): one copy each and one wait per step
   double* res_h = nullptr;
+  int band_bps = 0;  // resident blocks per SM of the band-sum kernel (0: not yet queried)
   int nzp = 0;                   // occupied z planes
   int batch = 0;                 // bands per FFT batch
   int grid_bands = 0;            // bands the FFT work grid has room for
