@@ -1203,8 +1203,7 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   CUW_RET(mark(h, PH_FFT));
   CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
   CUW_RET(mark(h, PH_ADDPRO));
-  CUW_RET(hproj_compute(h, g.proj, g.hproj));
-  CUW_RET(oproj_compute(h, g.proj, g.oproj));
+  CUW_RET(hoproj_compute(h, g.proj, g.hproj, g.oproj));
   CUW_RET(addpro_run(h, ADDPRO_FUSED, g.hproj, g.oproj));
   CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_EXPECT, tmpv, sc + 1));

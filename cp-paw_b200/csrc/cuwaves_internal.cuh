@@ -358,6 +358,7 @@ int proj_compute(Handle* h, const double2* psiA, double2* projA, const double2* 
 int addpro_run(Handle* h, int mode, const double2* hpc, const double2* opc);
 int hproj_compute(Handle* h, const double2* proj, double2* out);
 int oproj_compute(Handle* h, const double2* proj, double2* out);
+int hoproj_compute(Handle* h, const double2* proj, double2* hout, double2* oout);
 int gram_overlaps(Handle* h, double2* projP, double2* projO);
 int ortho_solve(Handle* h, int max_iter, double eps);
 int ortho_result(Handle* h, const int* st, int* iters);

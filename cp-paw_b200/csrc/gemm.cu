@@ -1059,11 +1059,10 @@ __global__ void k_force_final(const double* __restrict__ fpart, int ntile, int n
 // HPROJ = DH * PROJ per atom (WAVES_HPROJ, src/paw_waves1.f90:4919-4973)
 // OPROJ = DO * PROJ per atom (WAVES_OPROJ, src/paw_waves2.f90:497-544)
 // ---------------------------------------------------------------------------
-__global__ void k_hproj(const double2* __restrict__ proj, const double2* __restrict__ dh, int lmnxx,
-                        const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0,
-                        const int* __restrict__ nlmn, int nbh, int npro, double2* __restrict__ out) {
-  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= (size_t)nbh * npro) return;
+// HPROJ(b,p) = sum_l2 DH(l1,l2,atom) PROJ(b, atom's l2) for output i = b + NBH p
+__device__ __forceinline__ void hproj_at(size_t i, const double2* __restrict__ proj, const double2* __restrict__ dh,
+                                         int lmnxx, const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0,
+                                         const int* __restrict__ nlmn, int nbh, double2* __restrict__ out) {
   int b = (int)(i % nbh), p = (int)(i / nbh);
   int a = pdesc[p].iat;
   int l1 = p - ipro0[a];
@@ -1076,12 +1075,20 @@ __global__ void k_hproj(const double2* __restrict__ proj, const double2* __restr
   out[i] = s;
 }
 
-__global__ void k_oproj(const double2* __restrict__ proj, const double* __restrict__ dover, int lnxx,
-                        const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0, const int* __restrict__ isp,
-                        const int* __restrict__ lnofp, const int* __restrict__ mofp, const int* __restrict__ lmn0ln,
-                        const int* __restrict__ lox, int maxln, int nbh, int npro, double2* __restrict__ out) {
+__global__ void k_hproj(const double2* __restrict__ proj, const double2* __restrict__ dh, int lmnxx,
+                        const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0,
+                        const int* __restrict__ nlmn, int nbh, int npro, double2* __restrict__ out) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= (size_t)nbh * npro) return;
+  hproj_at(i, proj, dh, lmnxx, pdesc, ipro0, nlmn, nbh, out);
+}
+
+// OPROJ(b,p) = sum over the atom's projectors of equal l and m of DO(ln1,ln2) PROJ
+__device__ __forceinline__ void oproj_at(size_t i, const double2* __restrict__ proj, const double* __restrict__ dover,
+                                         int lnxx, const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0,
+                                         const int* __restrict__ isp, const int* __restrict__ lnofp,
+                                         const int* __restrict__ mofp, const int* __restrict__ lmn0ln,
+                                         const int* __restrict__ lox, int maxln, int nbh, double2* __restrict__ out) {
   int b = (int)(i % nbh), p = (int)(i / nbh);
   int a = pdesc[p].iat, s = isp[a];
   int ln1 = lnofp[p], m = mofp[p], l1 = pdesc[p].l;
@@ -1096,6 +1103,29 @@ __global__ void k_oproj(const double2* __restrict__ proj, const double* __restri
     acc.y += dv * c.y;
   }
   out[i] = acc;
+}
+
+__global__ void k_oproj(const double2* __restrict__ proj, const double* __restrict__ dover, int lnxx,
+                        const ProDesc* __restrict__ pdesc, const int* __restrict__ ipro0, const int* __restrict__ isp,
+                        const int* __restrict__ lnofp, const int* __restrict__ mofp, const int* __restrict__ lmn0ln,
+                        const int* __restrict__ lox, int maxln, int nbh, int npro, double2* __restrict__ out) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)nbh * npro) return;
+  oproj_at(i, proj, dover, lnxx, pdesc, ipro0, isp, lnofp, mofp, lmn0ln, lox, maxln, nbh, out);
+}
+
+// HPROJ and OPROJ of the same PROJ in one launch (the step's back-projection
+// needs both)
+__global__ void k_hoproj(const double2* __restrict__ proj, const double2* __restrict__ dh, int lmnxx,
+                         const double* __restrict__ dover, int lnxx, const ProDesc* __restrict__ pdesc,
+                         const int* __restrict__ ipro0, const int* __restrict__ nlmn, const int* __restrict__ isp,
+                         const int* __restrict__ lnofp, const int* __restrict__ mofp, const int* __restrict__ lmn0ln,
+                         const int* __restrict__ lox, int maxln, int nbh, int npro, double2* __restrict__ hout,
+                         double2* __restrict__ oout) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)nbh * npro) return;
+  hproj_at(i, proj, dh, lmnxx, pdesc, ipro0, nlmn, nbh, hout);
+  oproj_at(i, proj, dover, lnxx, pdesc, ipro0, isp, lnofp, mofp, lmn0ln, lox, maxln, nbh, oout);
 }
 
 }  // namespace
@@ -1319,6 +1349,16 @@ int hproj_compute(Handle* h, const double2* proj, double2* out) {
   k_hproj<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(proj, h->g.dh, h->lmnxx, h->g.pdesc, t.ipro0, t.nlmn,
                                                               h->d.nbh, h->npro, out);
   CUW_LAUNCH_CHECK("k_hproj");
+  return CUW_OK;
+}
+
+int hoproj_compute(Handle* h, const double2* proj, double2* hout, double2* oout) {
+  TabView t = tables(h);
+  size_t n = (size_t)h->d.nbh * h->npro;
+  k_hoproj<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(proj, h->g.dh, h->lmnxx, h->g.dover, h->lnxx, h->g.pdesc,
+                                                               t.ipro0, t.nlmn, t.isp, t.lnofp, t.mofp, t.lmn0ln, t.lox,
+                                                               CUW_MAXLN, h->d.nbh, h->npro, hout, oout);
+  CUW_LAUNCH_CHECK("k_hoproj");
   return CUW_OK;
 }
 
