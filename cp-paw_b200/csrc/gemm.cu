@@ -1148,7 +1148,9 @@ int ensure_part(Handle* h, size_t bytes) {
 }
 
 static int choose_split(Handle* h, int tiles, int nk, int minchunk, double mul) {
-  int want = std::max(1, (int)std::ceil(2.0 * h->nsm * mul / std::max(1, tiles)));
+  // at most 2 mul waves of one CTA per SM (rounded down: a CTA past a whole
+  // wave would cost a wave of its own)
+  int want = std::max(1, (int)std::floor(2.0 * h->nsm * mul / std::max(1, tiles)));
   int maxs = std::max(1, ceil_div(nk, minchunk));
   return std::min(want, maxs);
 }

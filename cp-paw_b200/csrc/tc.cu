@@ -914,7 +914,9 @@ static int* tc_err(Handle* h) { return h->g.ostatus + 12; }
 
 // number of K splits so that tiles * splits fills the GPU once (one CTA per SM)
 static int tc_splits(Handle* h, int tiles, int nk, double mul) {
-  const int want = std::max(1, (int)std::ceil(h->nsm * mul / std::max(1, tiles)));
+  // at most mul waves of one CTA per SM (rounded down: a CTA past a whole
+  // wave would cost a wave of its own)
+  const int want = std::max(1, (int)std::floor(h->nsm * mul / std::max(1, tiles)));
   return std::max(1, std::min(want, ceil_div(nk, 4 * kCK)));
 }
 
