@@ -6,7 +6,7 @@ Workload: Si64 (2x2x2 supercell of cubic diamond Si, a=20.52 bohr, seeded
 moving.  Synthetic setups, V_loc and DH (no dataset is involved).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--precision fp64]
+                  [--system NAME] [--no-mixed] [--no-precision] [--no-serving] ...
 
 One JSON line is printed by rank 0.  `value` is whole-job steps/s with every
 array resident in HBM (N independent replicas with --gpus N: the path does
@@ -39,6 +39,19 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def max_over_ranks(vals, world, device="cuda"):
+    """Element-wise maximum of every rank's timings (ms) over all ranks: the
+    job's time is that of its slowest replica.  One collective, taken by every
+    rank in the same order."""
+    if world == 1:
+        return [float(v) for v in vals]
+    import torch
+
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t]
 
 
 class ClockSampler:
@@ -328,11 +341,7 @@ def run_cuda(args, rank, world, local):
     ms_e2e = ev2.elapsed_time(ev3)
     h2d = v_h.numel() * 8 + dh_h.numel() * 8 + r_h.numel() * 8 + m_h.numel() * 8
     d2h = out_h.numel() * 8 // 8 * 5 + f_h.numel() * 8
-    # max over ranks
-    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], world)
     # roofline of the dominant phase
     fm = flops_model(inp)
     peaks, peak_src = measured_peaks()
