@@ -371,8 +371,7 @@ int propagate_run(Handle* h) {
 static int force_dev_run(Handle* h, double* force_dev) {
   Device& g = h->g;
   const int nbh = h->d.nbh, npro = h->npro, nb = h->d.nb;
-  CUW_RET(hproj_compute(h, g.proj, g.hproj));
-  CUW_RET(oproj_compute(h, g.proj, g.oproj));
+  CUW_RET(hoproj_compute(h, g.proj, g.hproj, g.oproj));
   size_t n = (size_t)nbh * npro;
   k_dedproj<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(g.hproj, g.occ, nbh, npro);
   CUW_LAUNCH_CHECK("k_dedproj");
@@ -1203,7 +1202,9 @@ static int step_body(Handle* h, int move_atoms, int max_iter, double eps) {
   CUW_RET(mark(h, PH_FFT));
   CUW_RET(fft_vpsi(h, g.psi0, g.hpsi, true));
   CUW_RET(mark(h, PH_ADDPRO));
-  CUW_RET(hoproj_compute(h, g.proj, g.hproj, g.oproj));
+  // OPROJ of this PROJ is still in g.oproj from the forces (which turned
+  // g.hproj into DEDPRO): only HPROJ is formed again
+  CUW_RET(hproj_compute(h, g.proj, g.hproj));
   CUW_RET(addpro_run(h, ADDPRO_FUSED, g.hproj, g.oproj));
   CUW_RET(mark(h, PH_RED));
   CUW_RET(energy_run(h, RED_EXPECT, tmpv, sc + 1));
